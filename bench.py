@@ -1,0 +1,346 @@
+#!/usr/bin/env python
+"""Benchmark: sweep unknowns/s of the B200 transport sweep on the 256x256, Q2 (9 dofs/cell), S16
+(144 ordinates) heterogeneous steady problem (log-normal sigma_t, median 1, log-sd 1; scattering
+ratio U[0.5, 0.999]; unit isotropic source; seeded synthetic data).
+
+One step = one application of L^{-1} (Omega.grad + sigma_t)^{-1} to the problem's angular source: the
+out-of-place sweep source -> psi with the scalar flux phi = P psi fused in, on HBM-resident arrays.
+The headline `value` is the FP32-cell-solve + FP64-refinement sweep; the plain FP64 sweep is timed
+beside it (`fp64`).  `e2e` times the same step through the C ABI with pinned HOST buffers (host ->
+device copy of the source and device -> host copy of psi and phi inside the timed region).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference solver's own CPU sweep (SweepOperator::Apply, compiled from the
+reference's sources into oracle/_ref/libidcref.so) on all host cores, same workload and metric.
+Under torchrun (N > 1) every rank sweeps its own independent problem (seed = rank; no collective on
+the data path, weak scaling); rank 0 prints the line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, "idc-transport-solver_b200")
+for _p in (REPO, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+NX, P_DEG, SN = 256, 2, 16
+METRIC = "sweep unknowns/s"
+UNIT = "unknowns/s"
+WORKLOAD = "256x256 Q2 S16 log-normal steady sweep (FP32 cell solves + FP64 refinement)"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def problem(seed: int):
+    from idcsweep.problems import lognormal
+    return lognormal(NX, P_DEG, SN, seed=seed, median=1.0, log_sd=1.0, c_range=(0.5, 0.999), source="uniform")
+
+
+def algorithmic_bytes(P) -> int:
+    """Per launch: read the FP64 angular source and write FP64 psi (16 B per unknown), read sigma_t and
+    write the N phi moments once per cell."""
+    cells = P.nx * P.ny
+    return 16 * P.unknowns_per_sweep + cells * (8 + 8 * P.N)
+
+
+def hbm_peak():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def measured_traffic():
+    """dram read+write bytes per launch of the headline sweep kernel from the committed ncu summary."""
+    path = os.path.join(REPO, "profiles", "sweep_traffic.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["dram_bytes_per_launch"])
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.dev)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out = ""
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        if not getattr(self, "lines", None):
+            return None
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        loaded = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def emit(d):
+    print(json.dumps(d), flush=True)
+
+
+# ----------------------------------------------------------------------------------------------------
+# reference arm: the reference's own CPU sweep
+# ----------------------------------------------------------------------------------------------------
+
+def time_reference_cpu(P, reps: int):
+    """SweepOperator::Apply of the reference (oracle/_ref), OpenMP on all host cores.  Returns
+    (seconds per sweep, threads, psi of the last sweep)."""
+    from oracle.bindings import Problem as OP, Reference
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    ref = Reference()
+    o = OP(P.nx, P.ny, P.p, P.xi, P.eta, P.w, P.quad, P.sigma_t, P.sigma_s, P.ax, P.bx, P.ay, P.by)
+    with ref.open(o, P.dt) as h:
+        psi = h.sweep(P.source, P.dt)            # warm-up, and the oracle result
+        sec = h.time_sweeps(P.source, P.dt, reps)
+        phi = h.pmv(psi)
+    return sec / reps, int(os.environ.get("OMP_NUM_THREADS", threads)), phi
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    P = problem(0)
+    steps = max(1, args.steps)
+    reps = max(1, min(steps, 3))
+    t0 = time.time()
+    sec, threads, _ = time_reference_cpu(P, reps)
+    value = P.unknowns_per_sweep / sec
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+        "steps": reps, "warmup": 1, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "256x256 Q2 S16 log-normal steady sweep (reference CPU, FP64 GE)",
+                   "nx": NX, "ny": NX, "p": P_DEG, "nq": P.nq, "unknowns_per_step": P.unknowns_per_sweep},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"{reps} full sweeps of the workload after 1 warm-up sweep"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": time.time() - t0,
+    }
+    emit(line)
+    return 0
+
+
+# ----------------------------------------------------------------------------------------------------
+# our arm
+# ----------------------------------------------------------------------------------------------------
+
+def run_ours(args):
+    import torch
+    from idcsweep import abi
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = local if world > 1 else 0
+    torch.cuda.set_device(dev)
+
+    P = problem(rank)
+    ctx = abi.SweepContext(P.nx, P.ny, P.p, P.ax, P.bx, P.ay, P.by, device=dev)
+    ctx.set_ordinates(P.xi, P.eta, P.w, P.quad)
+    ctx.set_sigma(P.sigma_t, P.sigma_s)
+
+    src = torch.from_numpy(P.source).to(f"cuda:{dev}")
+    out = torch.empty_like(src)
+    phi = torch.zeros(P.phi_shape(), dtype=torch.float64, device=f"cuda:{dev}")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def timed(prec, steps, warmup, sampler=False):
+        for _ in range(warmup):
+            ctx.sweep_out(src.data_ptr(), out.data_ptr(), P.dt, phi.data_ptr(), prec, loc=abi.LOC_DEVICE)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        kernel_ms, launches = [], 0
+        stream = torch.cuda.current_stream()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        clocks = ClockSampler(dev) if sampler else None
+        if clocks:
+            clocks.__enter__()
+        ev0.record(stream)
+        for _ in range(steps):
+            # each call is synchronous (it checks the device error word), so host wall time and events
+            # on the current stream bracket exactly the K sweeps
+            ctx.sweep_out(src.data_ptr(), out.data_ptr(), P.dt, phi.data_ptr(), prec, loc=abi.LOC_DEVICE)
+            ms, n = ctx.last_timing()
+            kernel_ms.append(ms)
+            launches += n
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        if clocks:
+            clocks.__exit__()
+        total_ms = ev0.elapsed_time(ev1)
+        if dist is not None:
+            t = torch.tensor([total_ms], device=f"cuda:{dev}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total_ms = float(t.item())
+        return total_ms / steps, statistics.mean(kernel_ms), launches, (clocks.summary() if clocks else None)
+
+    warm = max(3, args.warmup)
+    ms64, k64, _, _ = timed(abi.PREC_FP64, args.steps, warm)
+    phi64 = phi.clone()
+    ms32, k32, launches, clocks = timed(abi.PREC_FP32_REFINED, args.steps, warm, sampler=(rank == 0))
+    phi32 = phi.clone()
+
+    # end to end through the C ABI with pinned host buffers
+    h_src = torch.from_numpy(P.source).pin_memory()
+    h_out = torch.empty_like(h_src).pin_memory()
+    h_phi = torch.zeros(P.phi_shape(), dtype=torch.float64).pin_memory()
+    hs, ho, hp = h_src.numpy(), h_out.numpy(), h_phi.numpy()
+    e2e_steps = max(1, min(args.steps, 10))
+    ctx.sweep_out(hs, ho, P.dt, hp, abi.PREC_FP32_REFINED, loc=abi.LOC_HOST)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        ctx.sweep_out(hs, ho, P.dt, hp, abi.PREC_FP32_REFINED, loc=abi.LOC_HOST)
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if dist is not None:
+        t = torch.tensor([e2e_s], device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_phi_err = float(np.abs(hp - phi32.cpu().numpy()).max() / np.abs(hp).max())
+
+    unknowns = P.unknowns_per_sweep
+    alg = algorithmic_bytes(P)
+    peak, peak_kind = hbm_peak()
+    traffic = measured_traffic()
+    err_fp32_vs_fp64 = float(((phi32 - phi64).abs().max() / phi64.abs().max()).item())
+
+    if rank != 0:
+        ctx.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
+
+    line = {
+        "metric": METRIC,
+        "value": world * unknowns / (ms32 * 1e-3),
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": warm,
+        "ms_per_step": ms32,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32+f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "nx": NX, "ny": NX, "p": P_DEG, "nq": P.nq,
+                   "unknowns_per_step": unknowns, "parallelism": f"replicas{world}" if world > 1 else "single",
+                   "l2": "inputs larger than L2 (source 690 MB, psi 690 MB per step); no flush"},
+        "roofline": {"bound": "hbm", "achieved": alg / (k32 * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": alg / (k32 * 1e-3) / 1e9 / peak, "traffic": traffic,
+                     "algorithmic_bytes": alg, "kernel_ms": k32, "peak_kind": peak_kind},
+        "fp64": {"value": world * unknowns / (ms64 * 1e-3), "ms_per_step": ms64, "kernel_ms": k64,
+                 "roofline_frac": alg / (k64 * 1e-3) / 1e9 / peak},
+        "speedup_fp32_refined_vs_fp64": ms64 / ms32,
+        "err_phi_fp32_refined_vs_fp64_gpu": err_fp32_vs_fp64,
+        "e2e": {"value": world * unknowns / e2e_s, "unit": UNIT,
+                "h2d_bytes_per_step": int(hs.nbytes), "d2h_bytes_per_step": int(P.nx * P.ny * P.nq * P.N * 8 + hp.nbytes),
+                "ms_per_step": e2e_s * 1e3, "phi_rel_diff_vs_device_run": e2e_phi_err},
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+
+    if not args.no_cpu_baseline and world == 1:
+        try:
+            sec, threads, phi_ref = time_reference_cpu(P, reps=2)
+            line["cpu_baseline"] = {"value": unknowns / sec, "unit": UNIT, "cores": threads, "kind": "reference",
+                                    "sample": "2 full sweeps of the workload after 1 warm-up sweep"}
+            scale = np.abs(phi_ref).max()
+            line["err_phi_vs_oracle"] = {
+                "fp64": float(np.abs(phi64.cpu().numpy() - phi_ref).max() / scale),
+                "fp32_refined": float(np.abs(phi32.cpu().numpy() - phi_ref).max() / scale)}
+        except Exception as e:  # the reference library may be absent where it was never built
+            line["cpu_baseline"] = None
+            line["cpu_baseline_error"] = str(e)[:200]
+    emit(line)
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

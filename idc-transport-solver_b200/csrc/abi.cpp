@@ -1,0 +1,301 @@
+// The extern "C" boundary declared in include/idcsweep.h: argument checks, host <-> device staging,
+// status codes.  Nothing here throws across the boundary.
+#include "context.hpp"
+#include "idcsweep.h"
+
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+
+struct idc_ctx {
+    idc::Context impl;
+    explicit idc_ctx(const idc_problem_desc &d) : impl(d) {}
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(const idc::Status &s) {
+    g_last_error = s.msg;
+    return s.code;
+}
+
+int fail(int code, const char *msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define ABI_TRY(expr)                        \
+    do {                                     \
+        idc::Status s_ = (expr);             \
+        if (!s_.good()) return fail(s_);     \
+    } while (0)
+
+#define ABI_TRY_CUDA(expr) ABI_TRY(idc::cuda_status((expr), #expr))
+
+#define ABI_GUARD_BEGIN try {
+#define ABI_GUARD_END                                                      \
+    }                                                                      \
+    catch (const std::bad_alloc &) { return fail(IDC_ERR_NOMEM, "host allocation failed"); } \
+    catch (...) { return fail(IDC_ERR_CUDA, "unexpected exception in idcsweep"); }
+
+bool valid_loc(int loc) { return loc == IDC_LOC_HOST || loc == IDC_LOC_DEVICE; }
+
+}  // namespace
+
+extern "C" {
+
+const char *idc_strerror(int status) {
+    switch (status) {
+        case IDC_OK: return "ok";
+        case IDC_ERR_ARG: return "invalid argument";
+        case IDC_ERR_UNSUPPORTED: return "unsupported configuration";
+        case IDC_ERR_CUDA: return "CUDA error";
+        case IDC_ERR_TIMEOUT: return "device-side wait timed out";
+        case IDC_ERR_NOT_CONVERGED: return "iterative solve did not converge";
+        case IDC_ERR_STATE: return "call made in the wrong state";
+        case IDC_ERR_NOMEM: return "out of memory";
+        default: return "unknown status";
+    }
+}
+
+const char *idc_last_error_message(void) { return g_last_error.c_str(); }
+
+int idc_ctx_create(const idc_problem_desc *desc, idc_ctx **out) {
+    ABI_GUARD_BEGIN
+    if (!desc || !out) return fail(IDC_ERR_ARG, "idc_ctx_create: null argument");
+    *out = nullptr;
+    if (desc->nx < 1 || desc->ny < 1) return fail(IDC_ERR_ARG, "idc_ctx_create: nx and ny must be >= 1");
+    if (desc->nx > (1 << 20) || desc->ny > (1 << 20)) return fail(IDC_ERR_ARG, "idc_ctx_create: grid too large");
+    if (!(desc->bx > desc->ax) || !(desc->by > desc->ay) || !std::isfinite(desc->bx - desc->ax) ||
+        !std::isfinite(desc->by - desc->ay))
+        return fail(IDC_ERR_ARG, "idc_ctx_create: empty or non-finite domain");
+    if (desc->dg_degree < 0) return fail(IDC_ERR_ARG, "idc_ctx_create: negative DG degree");
+    if (desc->dg_degree > 2) return fail(IDC_ERR_UNSUPPORTED, "idc_ctx_create: DG degree > 2 not implemented");
+    if (desc->sigma_degree != 0)
+        return fail(IDC_ERR_UNSUPPORTED, "idc_ctx_create: only piecewise-constant cross sections are implemented");
+    if (desc->flags != 0) return fail(IDC_ERR_ARG, "idc_ctx_create: flags must be 0");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(IDC_ERR_CUDA, "idc_ctx_create: no CUDA device available");
+    if (desc->device < 0 || desc->device >= ndev) return fail(IDC_ERR_ARG, "idc_ctx_create: bad device ordinal");
+    auto *c = new idc_ctx(*desc);
+    idc::Status s = c->impl.init();
+    if (!s.good()) {
+        delete c;
+        return fail(s);
+    }
+    *out = c;
+    return IDC_OK;
+    ABI_GUARD_END
+}
+
+int idc_ctx_destroy(idc_ctx *ctx) {
+    ABI_GUARD_BEGIN
+    delete ctx;
+    return IDC_OK;
+    ABI_GUARD_END
+}
+
+int idc_set_ordinates(idc_ctx *ctx, int64_t nq, const double *xi, const double *eta, const double *w,
+                      const int64_t quad_bounds[5]) {
+    ABI_GUARD_BEGIN
+    if (!ctx) return fail(IDC_ERR_ARG, "null context");
+    ABI_TRY(ctx->impl.set_ordinates(nq, xi, eta, w, quad_bounds));
+    return IDC_OK;
+    ABI_GUARD_END
+}
+
+int idc_set_sigma(idc_ctx *ctx, const double *sigma_t, const double *sigma_s, int loc) {
+    ABI_GUARD_BEGIN
+    if (!ctx) return fail(IDC_ERR_ARG, "null context");
+    if (!valid_loc(loc)) return fail(IDC_ERR_ARG, "bad loc");
+    ABI_TRY(ctx->impl.set_sigma(sigma_t, sigma_s, loc));
+    return IDC_OK;
+    ABI_GUARD_END
+}
+
+int idc_set_tiling(idc_ctx *ctx, int32_t ordinates_per_block, int32_t rows_per_block) {
+    ABI_GUARD_BEGIN
+    if (!ctx) return fail(IDC_ERR_ARG, "null context");
+    if (ordinates_per_block > 320 || rows_per_block > 320 ||
+        (int64_t)ordinates_per_block * rows_per_block > 320)
+        return fail(IDC_ERR_ARG, "idc_set_tiling: more than 320 threads per block");
+    ABI_TRY(ctx->impl.set_tiling(ordinates_per_block, rows_per_block));
+    return IDC_OK;
+    ABI_GUARD_END
+}
+
+int idc_sweep(idc_ctx *ctx, double *psi_inout, double dt, double *phi_out, int precision, int loc) {
+    ABI_GUARD_BEGIN
+    if (!ctx || !psi_inout) return fail(IDC_ERR_ARG, "idc_sweep: null argument");
+    if (!valid_loc(loc)) return fail(IDC_ERR_ARG, "bad loc");
+    idc::Context &c = ctx->impl;
+    if (!c.have_ordinates) return fail(IDC_ERR_STATE, "idc_sweep before idc_set_ordinates");
+    ABI_TRY_CUDA(cudaSetDevice(c.device));
+    c.launches = 0;
+    if (loc == IDC_LOC_DEVICE) {
+        ABI_TRY(c.sweep(psi_inout, psi_inout, dt, phi_out, precision));
+        ABI_TRY(c.check_device_error());
+    } else {
+        ABI_TRY(c.ensure_psi_buffers(1));
+        ABI_TRY(c.ensure_phi_buffers(3));
+        double *d_psi = c.psi_buf(0);
+        double *d_phi = phi_out ? c.phi_buf(2) : nullptr;
+        ABI_TRY_CUDA(cudaMemcpyAsync(d_psi, psi_inout, sizeof(double) * c.psi_len(), cudaMemcpyHostToDevice, c.stream));
+        ABI_TRY(c.sweep(d_psi, d_psi, dt, d_phi, precision));
+        ABI_TRY_CUDA(cudaMemcpyAsync(psi_inout, d_psi, sizeof(double) * c.psi_len(), cudaMemcpyDeviceToHost, c.stream));
+        if (phi_out)
+            ABI_TRY_CUDA(cudaMemcpyAsync(phi_out, d_phi, sizeof(double) * c.phi_len(), cudaMemcpyDeviceToHost, c.stream));
+        ABI_TRY(c.check_device_error());
+    }
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, c.ev0, c.ev1) == cudaSuccess) c.last_sweep_ms = ms;
+    return IDC_OK;
+    ABI_GUARD_END
+}
+
+int idc_sweep_out(idc_ctx *ctx, const double *source, double *result, double dt, double *phi_out, int precision,
+                  int loc) {
+    ABI_GUARD_BEGIN
+    if (!ctx || !source || !result) return fail(IDC_ERR_ARG, "idc_sweep_out: null argument");
+    if (!valid_loc(loc)) return fail(IDC_ERR_ARG, "bad loc");
+    idc::Context &c = ctx->impl;
+    if (!c.have_ordinates) return fail(IDC_ERR_STATE, "idc_sweep_out before idc_set_ordinates");
+    ABI_TRY_CUDA(cudaSetDevice(c.device));
+    c.launches = 0;
+    if (loc == IDC_LOC_DEVICE) {
+        ABI_TRY(c.sweep(source, result, dt, phi_out, precision));
+        ABI_TRY(c.check_device_error());
+    } else {
+        ABI_TRY(c.ensure_psi_buffers(2));
+        ABI_TRY(c.ensure_phi_buffers(3));
+        double *d_src = c.psi_buf(1), *d_res = c.psi_buf(0);
+        double *d_phi = phi_out ? c.phi_buf(2) : nullptr;
+        ABI_TRY_CUDA(cudaMemcpyAsync(d_src, source, sizeof(double) * c.psi_len(), cudaMemcpyHostToDevice, c.stream));
+        ABI_TRY(c.sweep(d_src, d_res, dt, d_phi, precision));
+        // interior cells only; the caller's ghost cells of result stay as they were
+        const size_t cell = (size_t)c.nq * c.N;
+        for (int64_t i = 1; i <= c.nx; ++i) {
+            const size_t off = ((size_t)i * (c.ny + 2) + 1) * cell;
+            ABI_TRY_CUDA(cudaMemcpyAsync(result + off, d_res + off, sizeof(double) * cell * c.ny,
+                                         cudaMemcpyDeviceToHost, c.stream));
+        }
+        if (phi_out)
+            ABI_TRY_CUDA(cudaMemcpyAsync(phi_out, d_phi, sizeof(double) * c.phi_len(), cudaMemcpyDeviceToHost, c.stream));
+        ABI_TRY(c.check_device_error());
+    }
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, c.ev0, c.ev1) == cudaSuccess) c.last_sweep_ms = ms;
+    return IDC_OK;
+    ABI_GUARD_END
+}
+
+// Operators: stage through the context's buffers when loc is host.
+int idc_pmv(idc_ctx *ctx, double alpha, double beta, const double *psi, double *phi, int loc) {
+    ABI_GUARD_BEGIN
+    if (!ctx || !psi || !phi) return fail(IDC_ERR_ARG, "idc_pmv: null argument");
+    if (!valid_loc(loc)) return fail(IDC_ERR_ARG, "bad loc");
+    idc::Context &c = ctx->impl;
+    if (!c.have_ordinates) return fail(IDC_ERR_STATE, "idc_pmv before idc_set_ordinates");
+    ABI_TRY_CUDA(cudaSetDevice(c.device));
+    c.launches = 0;
+    if (loc == IDC_LOC_DEVICE) {
+        ABI_TRY(c.pmv(alpha, beta, psi, phi));
+    } else {
+        ABI_TRY(c.ensure_psi_buffers(1));
+        ABI_TRY(c.ensure_phi_buffers(3));
+        ABI_TRY_CUDA(cudaMemcpyAsync(c.psi_buf(0), psi, sizeof(double) * c.psi_len(), cudaMemcpyHostToDevice, c.stream));
+        ABI_TRY_CUDA(cudaMemcpyAsync(c.phi_buf(2), phi, sizeof(double) * c.phi_len(), cudaMemcpyHostToDevice, c.stream));
+        ABI_TRY(c.pmv(alpha, beta, c.psi_buf(0), c.phi_buf(2)));
+        ABI_TRY_CUDA(cudaMemcpyAsync(phi, c.phi_buf(2), sizeof(double) * c.phi_len(), cudaMemcpyDeviceToHost, c.stream));
+    }
+    ABI_TRY_CUDA(cudaStreamSynchronize(c.stream));
+    return IDC_OK;
+    ABI_GUARD_END
+}
+
+int idc_smv(idc_ctx *ctx, double alpha, double beta, const double *phi, double *psi, int loc) {
+    ABI_GUARD_BEGIN
+    if (!ctx || !psi || !phi) return fail(IDC_ERR_ARG, "idc_smv: null argument");
+    if (!valid_loc(loc)) return fail(IDC_ERR_ARG, "bad loc");
+    idc::Context &c = ctx->impl;
+    if (!c.have_ordinates) return fail(IDC_ERR_STATE, "idc_smv before idc_set_ordinates");
+    ABI_TRY_CUDA(cudaSetDevice(c.device));
+    c.launches = 0;
+    if (loc == IDC_LOC_DEVICE) {
+        ABI_TRY(c.smv(alpha, beta, phi, psi));
+    } else {
+        ABI_TRY(c.ensure_psi_buffers(1));
+        ABI_TRY(c.ensure_phi_buffers(3));
+        ABI_TRY_CUDA(cudaMemcpyAsync(c.psi_buf(0), psi, sizeof(double) * c.psi_len(), cudaMemcpyHostToDevice, c.stream));
+        ABI_TRY_CUDA(cudaMemcpyAsync(c.phi_buf(2), phi, sizeof(double) * c.phi_len(), cudaMemcpyHostToDevice, c.stream));
+        ABI_TRY(c.smv(alpha, beta, c.phi_buf(2), c.psi_buf(0)));
+        ABI_TRY_CUDA(cudaMemcpyAsync(psi, c.psi_buf(0), sizeof(double) * c.psi_len(), cudaMemcpyDeviceToHost, c.stream));
+    }
+    ABI_TRY_CUDA(cudaStreamSynchronize(c.stream));
+    return IDC_OK;
+    ABI_GUARD_END
+}
+
+int idc_lmv(idc_ctx *ctx, double alpha, double beta, const double *x, double *y, int loc) {
+    ABI_GUARD_BEGIN
+    if (!ctx || !x || !y) return fail(IDC_ERR_ARG, "idc_lmv: null argument");
+    if (!valid_loc(loc)) return fail(IDC_ERR_ARG, "bad loc");
+    idc::Context &c = ctx->impl;
+    if (!c.have_ordinates) return fail(IDC_ERR_STATE, "idc_lmv before idc_set_ordinates");
+    if (x == y) return fail(IDC_ERR_ARG, "idc_lmv: x and y must not alias");
+    ABI_TRY_CUDA(cudaSetDevice(c.device));
+    c.launches = 0;
+    if (loc == IDC_LOC_DEVICE) {
+        ABI_TRY(c.lmv(alpha, beta, x, y));
+    } else {
+        ABI_TRY(c.ensure_psi_buffers(2));
+        ABI_TRY_CUDA(cudaMemcpyAsync(c.psi_buf(0), x, sizeof(double) * c.psi_len(), cudaMemcpyHostToDevice, c.stream));
+        ABI_TRY_CUDA(cudaMemcpyAsync(c.psi_buf(1), y, sizeof(double) * c.psi_len(), cudaMemcpyHostToDevice, c.stream));
+        ABI_TRY(c.lmv(alpha, beta, c.psi_buf(0), c.psi_buf(1)));
+        ABI_TRY_CUDA(cudaMemcpyAsync(y, c.psi_buf(1), sizeof(double) * c.psi_len(), cudaMemcpyDeviceToHost, c.stream));
+    }
+    ABI_TRY_CUDA(cudaStreamSynchronize(c.stream));
+    return IDC_OK;
+    ABI_GUARD_END
+}
+
+int idc_source_iteration(idc_ctx *ctx, double *source_inout, double dt, double abs_tol, int64_t max_its, int precision,
+                         int loc, int64_t *iters, double *final_err) {
+    ABI_GUARD_BEGIN
+    if (!ctx || !source_inout) return fail(IDC_ERR_ARG, "idc_source_iteration: null argument");
+    if (!valid_loc(loc)) return fail(IDC_ERR_ARG, "bad loc");
+    if (max_its < 0 || !(abs_tol >= 0)) return fail(IDC_ERR_ARG, "idc_source_iteration: bad tolerance");
+    idc::Context &c = ctx->impl;
+    ABI_TRY_CUDA(cudaSetDevice(c.device));
+    c.launches = 0;
+    ABI_TRY(c.ensure_psi_buffers(2));
+    double *d_src = c.psi_buf(1), *d_psi = c.psi_buf(0);
+    const cudaMemcpyKind in = loc == IDC_LOC_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    const cudaMemcpyKind out = loc == IDC_LOC_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    ABI_TRY_CUDA(cudaMemcpyAsync(d_src, source_inout, sizeof(double) * c.psi_len(), in, c.stream));
+    // psi starts as the source so that its ghost cells hold the inflow values (SISolver copies
+    // Interior|Boundary from the source every iteration, SISolver.cpp:226)
+    ABI_TRY_CUDA(cudaMemcpyAsync(d_psi, d_src, sizeof(double) * c.psi_len(), cudaMemcpyDeviceToDevice, c.stream));
+    int64_t its = 0;
+    double err = 0;
+    ABI_TRY(c.source_iteration(d_src, d_psi, dt, abs_tol, max_its, precision, &its, &err));
+    ABI_TRY_CUDA(cudaMemcpyAsync(source_inout, d_psi, sizeof(double) * c.psi_len(), out, c.stream));
+    ABI_TRY_CUDA(cudaStreamSynchronize(c.stream));
+    if (iters) *iters = its;
+    if (final_err) *final_err = err;
+    return IDC_OK;
+    ABI_GUARD_END
+}
+
+int idc_last_timing(idc_ctx *ctx, double *sweep_kernel_ms, int64_t *kernels_launched) {
+    if (!ctx) return fail(IDC_ERR_ARG, "null context");
+    if (sweep_kernel_ms) *sweep_kernel_ms = ctx->impl.last_sweep_ms;
+    if (kernels_launched) *kernels_launched = ctx->impl.launches;
+    return IDC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,347 @@
+// C++ host layer, see context.hpp.
+#include "context.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace idc {
+
+Status cuda_status(cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return Status::ok();
+    Status s;
+    s.code = (e == cudaErrorMemoryAllocation) ? IDC_ERR_NOMEM : IDC_ERR_CUDA;
+    s.msg = std::string(what) + ": " + cudaGetErrorString(e);
+    return s;
+}
+
+#define IDC_TRY_CUDA(expr)                                   \
+    do {                                                     \
+        cudaError_t e_ = (expr);                             \
+        if (e_ != cudaSuccess) return cuda_status(e_, #expr); \
+    } while (0)
+
+#define IDC_TRY(expr)                     \
+    do {                                  \
+        Status s_ = (expr);               \
+        if (!s_.good()) return s_;        \
+    } while (0)
+
+static Status bad(int code, const std::string &m) {
+    Status s;
+    s.code = code;
+    s.msg = m;
+    return s;
+}
+
+Context::Context(const idc_problem_desc &d) : desc(d) {}
+
+Context::~Context() {
+    if (device >= 0) cudaSetDevice(device);
+    for (double *p : psi_bufs_) cudaFree(p);
+    for (double *p : phi_bufs_) cudaFree(p);
+    cudaFree(d_scalar_);
+    cudaFree(d_xi);
+    cudaFree(d_eta);
+    cudaFree(d_w);
+    cudaFree(d_sigma_t);
+    cudaFree(d_sigma_s);
+    cudaFree(d_items);
+    cudaFree(d_sync);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+Status Context::init() {
+    nx = desc.nx;
+    ny = desc.ny;
+    P = (int)desc.dg_degree + 1;
+    N = P * P;
+    dx = (desc.bx - desc.ax) / (double)nx;
+    dy = (desc.by - desc.ay) / (double)ny;
+    device = desc.device;
+    IDC_TRY_CUDA(cudaSetDevice(device));
+    IDC_TRY_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
+    IDC_TRY_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    IDC_TRY_CUDA(cudaEventCreate(&ev0));
+    IDC_TRY_CUDA(cudaEventCreate(&ev1));
+    IDC_TRY_CUDA(cudaMalloc(&d_scalar_, sizeof(double) * 4));
+    return Status::ok();
+}
+
+Status Context::set_ordinates(int64_t nq_in, const double *xi, const double *eta, const double *w,
+                              const int64_t qb[5]) {
+    if (nq_in <= 0 || !xi || !eta || !w || !qb) return bad(IDC_ERR_ARG, "set_ordinates: null or empty input");
+    if (qb[0] != 0 || qb[4] != nq_in) return bad(IDC_ERR_ARG, "set_ordinates: quad_bounds must run 0..nq");
+    for (int k = 0; k < 4; ++k)
+        if (qb[k + 1] < qb[k]) return bad(IDC_ERR_ARG, "set_ordinates: quad_bounds not monotone");
+    // every ordinate must lie strictly inside its quadrant (OrdinateSet::SetSigns, OrdinateSet.cpp:658-700)
+    for (int k = 0; k < 4; ++k)
+        for (int64_t q = qb[k]; q < qb[k + 1]; ++q) {
+            const bool xneg = k >= 2, yneg = (k & 1) != 0;
+            if (!(std::isfinite(xi[q]) && std::isfinite(eta[q]) && std::isfinite(w[q])))
+                return bad(IDC_ERR_ARG, "set_ordinates: non-finite ordinate");
+            if ((xneg ? !(xi[q] < 0) : !(xi[q] > 0)) || (yneg ? !(eta[q] < 0) : !(eta[q] > 0)))
+                return bad(IDC_ERR_ARG, "set_ordinates: ordinate " + std::to_string(q) + " outside quadrant " +
+                                            std::to_string(k));
+        }
+    IDC_TRY_CUDA(cudaSetDevice(device));
+    cudaFree(d_xi);
+    cudaFree(d_eta);
+    cudaFree(d_w);
+    d_xi = d_eta = d_w = nullptr;
+    IDC_TRY_CUDA(cudaMalloc(&d_xi, sizeof(double) * nq_in));
+    IDC_TRY_CUDA(cudaMalloc(&d_eta, sizeof(double) * nq_in));
+    IDC_TRY_CUDA(cudaMalloc(&d_w, sizeof(double) * nq_in));
+    IDC_TRY_CUDA(cudaMemcpy(d_xi, xi, sizeof(double) * nq_in, cudaMemcpyHostToDevice));
+    IDC_TRY_CUDA(cudaMemcpy(d_eta, eta, sizeof(double) * nq_in, cudaMemcpyHostToDevice));
+    IDC_TRY_CUDA(cudaMemcpy(d_w, w, sizeof(double) * nq_in, cudaMemcpyHostToDevice));
+    if (nq_in != nq) {
+        // psi-sized buffers depend on nq
+        for (double *p : psi_bufs_) cudaFree(p);
+        psi_bufs_.clear();
+    }
+    nq = nq_in;
+    for (int k = 0; k < 5; ++k) quad[k] = qb[k];
+    have_ordinates = true;
+    n_items = 0;   // schedule rebuilt lazily
+    occupancy_precision = -1;
+    return Status::ok();
+}
+
+Status Context::set_sigma(const double *sigma_t, const double *sigma_s, int loc) {
+    if (!sigma_t) return bad(IDC_ERR_ARG, "set_sigma: sigma_t is null");
+    IDC_TRY_CUDA(cudaSetDevice(device));
+    if (!d_sigma_t) IDC_TRY_CUDA(cudaMalloc(&d_sigma_t, sizeof(double) * sig_len()));
+    if (!d_sigma_s) IDC_TRY_CUDA(cudaMalloc(&d_sigma_s, sizeof(double) * sig_len()));
+    const cudaMemcpyKind kind = loc == IDC_LOC_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    IDC_TRY_CUDA(cudaMemcpy(d_sigma_t, sigma_t, sizeof(double) * sig_len(), kind));
+    if (sigma_s)
+        IDC_TRY_CUDA(cudaMemcpy(d_sigma_s, sigma_s, sizeof(double) * sig_len(), kind));
+    else
+        IDC_TRY_CUDA(cudaMemset(d_sigma_s, 0, sizeof(double) * sig_len()));
+    have_sigma = true;
+    return Status::ok();
+}
+
+Status Context::set_tiling(int G, int R) {
+    if (G < 0 || R < 0) return bad(IDC_ERR_ARG, "set_tiling: negative tile size");
+    user_G = G;
+    user_R = R;
+    n_items = 0;
+    occupancy_precision = -1;
+    return Status::ok();
+}
+
+Status Context::ensure_psi_buffers(int count) {
+    IDC_TRY_CUDA(cudaSetDevice(device));
+    while ((int)psi_bufs_.size() < count) {
+        double *p = nullptr;
+        IDC_TRY_CUDA(cudaMalloc(&p, sizeof(double) * psi_len()));
+        psi_bufs_.push_back(p);
+    }
+    return Status::ok();
+}
+
+Status Context::ensure_phi_buffers(int count) {
+    IDC_TRY_CUDA(cudaSetDevice(device));
+    while ((int)phi_bufs_.size() < count) {
+        double *p = nullptr;
+        IDC_TRY_CUDA(cudaMalloc(&p, sizeof(double) * phi_len()));
+        IDC_TRY_CUDA(cudaMemset(p, 0, sizeof(double) * phi_len()));
+        phi_bufs_.push_back(p);
+    }
+    return Status::ok();
+}
+
+// Work items in row-block-major order: (row block, quadrant, ordinate chunk).
+Status Context::build_schedule(int precision) {
+    if (n_items > 0 && occupancy_precision == precision) return Status::ok();
+    int qmax = 0;
+    for (int k = 0; k < 4; ++k) qmax = std::max<int>(qmax, (int)(quad[k + 1] - quad[k]));
+    if (qmax == 0) return bad(IDC_ERR_ARG, "no ordinates");
+    const int max_threads = 320;
+    int G = user_G > 0 ? user_G : std::min(qmax, P == 3 ? 36 : 64);
+    if (G > max_threads) G = max_threads;
+    int R = user_R > 0 ? user_R : std::max(1, std::min(16, max_threads / G));
+    if (G * R > max_threads) R = std::max(1, max_threads / G);
+    if (R > ny) R = (int)ny;
+    tiling.G = G;
+    tiling.R = R;
+    const int nrb = (int)((ny + R - 1) / R);
+
+    std::vector<SweepItem> items;
+    // chunks of each quadrant, balanced: ceil(count / G) chunks of near-equal size
+    std::vector<std::vector<std::pair<int, int>>> chunks(4);
+    for (int k = 0; k < 4; ++k) {
+        const int cnt = (int)(quad[k + 1] - quad[k]);
+        if (cnt == 0) continue;
+        const int nch = (cnt + G - 1) / G;
+        int beg = (int)quad[k];
+        for (int c = 0; c < nch; ++c) {
+            const int sz = cnt / nch + (c < cnt % nch ? 1 : 0);
+            chunks[k].push_back({beg, sz});
+            beg += sz;
+        }
+    }
+    std::vector<int> prev_index;   // index of the same (quadrant, chunk) in the previous row block
+    for (int rb = 0; rb < nrb; ++rb) {
+        std::vector<int> cur_index;
+        int slot = 0;
+        for (int k = 0; k < 4; ++k)
+            for (auto &ch : chunks[k]) {
+                SweepItem it;
+                it.quadrant = k;
+                it.q_begin = ch.first;
+                it.q_count = ch.second;
+                it.row_block = rb;
+                it.dep = rb == 0 ? -1 : prev_index[slot];
+                cur_index.push_back((int)items.size());
+                items.push_back(it);
+                ++slot;
+            }
+        prev_index = cur_index;
+    }
+    n_items = (int)items.size();
+
+    IDC_TRY_CUDA(cudaSetDevice(device));
+    cudaFree(d_items);
+    cudaFree(d_sync);
+    d_items = nullptr;
+    d_sync = nullptr;
+    IDC_TRY_CUDA(cudaMalloc(&d_items, sizeof(SweepItem) * items.size()));
+    IDC_TRY_CUDA(cudaMemcpy(d_items, items.data(), sizeof(SweepItem) * items.size(), cudaMemcpyHostToDevice));
+    IDC_TRY_CUDA(cudaMalloc(&d_sync, sizeof(int) * (2 + items.size())));
+    IDC_TRY_CUDA(cudaMemset(d_sync, 0, sizeof(int) * (2 + items.size())));
+
+    block = ((G * R + 31) / 32) * 32;
+    smem = sweep_smem_bytes(P, R, G);
+    int per_sm = 0;
+    IDC_TRY_CUDA(sweep_occupancy(P, precision, block, smem, &per_sm));
+    if (per_sm < 1) return bad(IDC_ERR_UNSUPPORTED, "sweep kernel does not fit on an SM with this tiling");
+    grid = std::min(n_items, per_sm * num_sms);
+    occupancy_precision = precision;
+    return Status::ok();
+}
+
+Status Context::check_device_error() {
+    int err = 0;
+    IDC_TRY_CUDA(cudaMemcpyAsync(&err, d_sync + 1, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    IDC_TRY_CUDA(cudaStreamSynchronize(stream));
+    if (err != kDevOk) {
+        IDC_TRY_CUDA(cudaMemsetAsync(d_sync + 1, 0, sizeof(int), stream));
+        IDC_TRY_CUDA(cudaStreamSynchronize(stream));
+        return bad(IDC_ERR_TIMEOUT, "a device-side wait gave up (bounded spin); the sweep was abandoned");
+    }
+    return Status::ok();
+}
+
+Status Context::sweep(const double *src, double *out, double dt, double *phi, int precision,
+                      const double *phi_scatter, double scatter_scale) {
+    if (!have_ordinates) return bad(IDC_ERR_STATE, "sweep before idc_set_ordinates");
+    if (!have_sigma) return bad(IDC_ERR_STATE, "sweep before idc_set_sigma");
+    if (precision < 0 || precision > 2) return bad(IDC_ERR_ARG, "unknown precision");
+    if (!(dt > 0)) return bad(IDC_ERR_ARG, "dt must be positive (+inf for steady state)");
+    IDC_TRY(build_schedule(precision));
+    IDC_TRY_CUDA(cudaSetDevice(device));
+
+    SweepArgs a{};
+    a.src = src;
+    a.out = out;
+    a.sigma_t = d_sigma_t;
+    a.sigma_s = d_sigma_s;
+    a.phi_scatter = phi_scatter;
+    a.scatter_scale = scatter_scale;
+    a.phi = phi;
+    a.xi = d_xi;
+    a.eta = d_eta;
+    a.w = d_w;
+    a.nx = (int)nx;
+    a.ny = (int)ny;
+    a.nq = (int)nq;
+    a.dx = dx;
+    a.dy = dy;
+    a.inv_dt = 1.0 / dt;
+    a.items = d_items;
+    a.n_items = n_items;
+    a.R = tiling.R;
+    a.G = tiling.G;
+    a.n_refine = 1;
+    a.next_item = d_sync;
+    a.error = d_sync + 1;
+    a.progress = d_sync + 2;
+    a.spin_limit = spin_limit;
+
+    // queue head and progress flags start at zero; the error word is kept until checked
+    IDC_TRY_CUDA(cudaMemsetAsync(d_sync, 0, sizeof(int), stream));
+    IDC_TRY_CUDA(cudaMemsetAsync(d_sync + 2, 0, sizeof(int) * n_items, stream));
+    if (phi) IDC_TRY_CUDA(cudaMemsetAsync(phi, 0, sizeof(double) * phi_len(), stream));
+    IDC_TRY_CUDA(cudaEventRecord(ev0, stream));
+    IDC_TRY_CUDA(launch_sweep(P, precision, a, grid, block, smem, stream));
+    IDC_TRY_CUDA(cudaEventRecord(ev1, stream));
+    launches += 1;
+    return Status::ok();
+}
+
+Status Context::pmv(double alpha, double beta, const double *psi, double *phi) {
+    if (!have_ordinates) return bad(IDC_ERR_STATE, "pmv before idc_set_ordinates");
+    IDC_TRY_CUDA(cudaSetDevice(device));
+    IDC_TRY_CUDA(launch_pmv(dims(), alpha, beta, d_w, psi, phi, stream));
+    launches += 1;
+    return Status::ok();
+}
+
+Status Context::smv(double alpha, double beta, const double *phi, double *psi) {
+    if (!have_ordinates) return bad(IDC_ERR_STATE, "smv before idc_set_ordinates");
+    if (!have_sigma) return bad(IDC_ERR_STATE, "smv before idc_set_sigma");
+    IDC_TRY_CUDA(cudaSetDevice(device));
+    IDC_TRY_CUDA(launch_smv(dims(), alpha, beta, d_sigma_s, phi, psi, stream));
+    launches += 1;
+    return Status::ok();
+}
+
+Status Context::lmv(double alpha, double beta, const double *x, double *y) {
+    if (!have_ordinates) return bad(IDC_ERR_STATE, "lmv before idc_set_ordinates");
+    if (!have_sigma) return bad(IDC_ERR_STATE, "lmv before idc_set_sigma");
+    IDC_TRY_CUDA(cudaSetDevice(device));
+    IDC_TRY_CUDA(launch_lmv(dims(), alpha, beta, d_sigma_t, d_xi, d_eta, x, y, stream));
+    launches += 1;
+    return Status::ok();
+}
+
+Status Context::l2dist(const double *a, const double *b, double *out_host) {
+    IDC_TRY_CUDA(launch_l2dist2(dims(), a, b, d_scalar_, stream));
+    launches += 1;
+    double v = 0;
+    IDC_TRY_CUDA(cudaMemcpyAsync(&v, d_scalar_, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    IDC_TRY_CUDA(cudaStreamSynchronize(stream));
+    *out_host = std::sqrt(v);
+    return Status::ok();
+}
+
+// SISolver::Solve, linear_solvers/Abstract/ImplicitSolver/SISolver.cpp:190-254.  The copy of the
+// source into psi, Smv(1, 1, sigma_s, phi_last -> psi) and Pmv(1, 0, psi -> phi) of each iteration are
+// fused into the sweep (source read + scattering term on the fly, moments in the epilogue).
+Status Context::source_iteration(const double *src, double *psi_out, double dt, double abs_tol, int64_t max_its,
+                                 int precision, int64_t *iters, double *err) {
+    IDC_TRY(ensure_phi_buffers(2));
+    double *phi_cur = phi_buf(0), *phi_last = phi_buf(1);
+    IDC_TRY_CUDA(cudaMemsetAsync(phi_cur, 0, sizeof(double) * phi_len(), stream));
+    IDC_TRY_CUDA(cudaMemsetAsync(phi_last, 0, sizeof(double) * phi_len(), stream));
+    int64_t it = 0;
+    double e = INFINITY;
+    while (it < max_its && e > abs_tol) {
+        ++it;
+        std::swap(phi_cur, phi_last);
+        IDC_TRY(sweep(src, psi_out, dt, phi_cur, precision, phi_last, 1.0));
+        IDC_TRY(l2dist(phi_cur, phi_last, &e));
+        IDC_TRY(check_device_error());
+    }
+    // Like the reference, reaching max_its is not an error: the caller reads *err.
+    if (iters) *iters = it;
+    if (err) *err = e;
+    return Status::ok();
+}
+
+}  // namespace idc

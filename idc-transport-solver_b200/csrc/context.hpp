@@ -1,0 +1,93 @@
+// C++ host layer: the device-resident counterpart of the reference's SweepOperator / TransportOperator /
+// SISolver objects for one grid on one GPU.  The C ABI (abi.cpp) validates arguments, moves host data in
+// and out, and calls these methods with device pointers.
+#pragma once
+
+#include "idc_internal.hpp"
+#include "idcsweep.h"
+
+#include <string>
+#include <vector>
+
+namespace idc {
+
+// Status carries an IDC_* code and a message.
+struct Status {
+    int code = IDC_OK;
+    std::string msg;
+    static Status ok() { return {}; }
+    bool good() const { return code == IDC_OK; }
+};
+
+Status cuda_status(cudaError_t e, const char *what);
+
+class Context {
+public:
+    explicit Context(const idc_problem_desc &d);
+    ~Context();
+    Status init();
+
+    // ---- configuration (SweepOperator construction / SetParameters) ----
+    Status set_ordinates(int64_t nq, const double *xi, const double *eta, const double *w, const int64_t qb[5]);
+    Status set_sigma(const double *sigma_t, const double *sigma_s, int loc);
+    Status set_tiling(int G, int R);   // 0 = automatic
+
+    // ---- operators on device pointers ----
+    // Sweep: out <- L^{-1} (src [+ scale * S phi_scatter]); phi (nullable) <- P out.  src may equal out.
+    Status sweep(const double *src, double *out, double dt, double *phi, int precision,
+                 const double *phi_scatter = nullptr, double scatter_scale = 1.0);
+    Status pmv(double alpha, double beta, const double *psi, double *phi);
+    Status smv(double alpha, double beta, const double *phi, double *psi);
+    Status lmv(double alpha, double beta, const double *x, double *y);
+    Status l2dist(const double *a, const double *b, double *out_host);
+    Status source_iteration(const double *src, double *psi_out, double dt, double abs_tol, int64_t max_its,
+                            int precision, int64_t *iters, double *err);
+
+    // ---- buffers ----
+    Status ensure_psi_buffers(int count);   // device scratch psi-sized buffers
+    Status ensure_phi_buffers(int count);
+    double *psi_buf(int k) { return psi_bufs_[k]; }
+    double *phi_buf(int k) { return phi_bufs_[k]; }
+    Status check_device_error();   // reads and clears the device error word
+
+    size_t psi_len() const { return (size_t)(nx + 2) * (ny + 2) * (size_t)nq * N; }
+    size_t phi_len() const { return (size_t)(nx + 2) * (ny + 2) * (size_t)N; }
+    size_t sig_len() const { return (size_t)(nx + 2) * (ny + 2); }
+    GridDims dims() const { return GridDims{(int)nx, (int)ny, (int)nq, P, dx, dy}; }
+
+    idc_problem_desc desc;
+    int64_t nx = 0, ny = 0;
+    int P = 0, N = 0;
+    double dx = 0, dy = 0;
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+    int64_t nq = 0;
+    int64_t quad[5] = {0, 0, 0, 0, 0};
+    double *d_xi = nullptr, *d_eta = nullptr, *d_w = nullptr;
+    double *d_sigma_t = nullptr, *d_sigma_s = nullptr;
+    bool have_ordinates = false, have_sigma = false;
+
+    // sweep schedule
+    SweepTiling tiling;
+    int user_G = 0, user_R = 0;
+    SweepItem *d_items = nullptr;
+    int n_items = 0;
+    int *d_sync = nullptr;        // [0] queue head, [1] error word, [2..] progress per item
+    int grid = 0, block = 0;
+    size_t smem = 0;
+    int occupancy_precision = -1;
+
+    float last_sweep_ms = 0.f;
+    int64_t launches = 0;
+    long long spin_limit = 1ll << 22;
+
+private:
+    Status build_schedule(int precision);
+    std::vector<double *> psi_bufs_, phi_bufs_;
+    double *d_scalar_ = nullptr;
+};
+
+}  // namespace idc

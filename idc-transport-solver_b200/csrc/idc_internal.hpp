@@ -1,0 +1,79 @@
+// Internal declarations shared by the CUDA kernels, the C++ host layer and the C ABI.
+#pragma once
+
+#include <cstdint>
+#include <cstddef>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+namespace idc {
+
+// Device-side error codes written to the context's error word.
+enum DeviceError : int {
+    kDevOk = 0,
+    kDevTimeout = 1,        // a bounded spin on another CTA's progress flag ran out
+};
+
+// One unit of work of the persistent wavefront kernel: R consecutive rows (in sweep order) of one
+// quadrant, for a chunk of that quadrant's ordinates, swept across all columns.  `dep` is the item
+// that owns the R rows just upwind in y (same quadrant and chunk, previous row block), or -1.
+struct SweepItem {
+    int quadrant;
+    int q_begin;
+    int q_count;
+    int row_block;
+    int dep;
+};
+
+struct SweepArgs {
+    const double *src;         // angular source (read); ghost cells carry the inflow values
+    double *out;               // psi (written); may equal src (in-place sweep)
+    const double *sigma_t;     // (nx+2)(ny+2), piecewise constant
+    const double *sigma_s;     // (nx+2)(ny+2) or null: fused isotropic scattering source
+    const double *phi_scatter; // phi used by the fused scattering source, or null
+    double *phi;               // fused moment output (atomically accumulated, pre-zeroed), or null
+    const double *xi, *eta, *w;
+    int nx, ny, nq;
+    double dx, dy, inv_dt;
+    double scatter_scale;      // multiplies sigma_s*phi/(4 pi) in the fused source
+    const SweepItem *items;
+    int n_items;
+    int R;                     // rows per item
+    int G;                     // ordinate slots per CTA (>= every item's q_count)
+    int n_refine;              // FP64 refinement steps of the FP32 cell solve
+    int *progress;             // per item: columns finished by its last row
+    int *next_item;            // dynamic work queue head
+    int *error;                // device error word
+    long long spin_limit;      // polls before a wait gives up
+};
+
+// Launch geometry picked by the host (autotuner or defaults).
+struct SweepTiling {
+    int G = 0;   // ordinates per CTA
+    int R = 0;   // rows per CTA
+};
+
+// Kernel launchers (sweep_kernels.cu).  `precision` is one of the IDC_PREC_* values.
+cudaError_t launch_sweep(int P, int precision, const SweepArgs &args, int grid, int block, size_t smem,
+                         cudaStream_t stream);
+cudaError_t sweep_occupancy(int P, int precision, int block, size_t smem, int *blocks_per_sm);
+size_t sweep_smem_bytes(int P, int R, int G);
+
+// Operator kernels (ops_kernels.cu).
+struct GridDims {
+    int nx, ny, nq, P;
+    double dx, dy;
+};
+cudaError_t launch_pmv(const GridDims &g, double alpha, double beta, const double *w, const double *psi,
+                       double *phi, cudaStream_t s);
+cudaError_t launch_smv(const GridDims &g, double alpha, double beta, const double *sigma_s, const double *phi,
+                       double *psi, cudaStream_t s);
+cudaError_t launch_lmv(const GridDims &g, double alpha, double beta, const double *sigma_t, const double *xi,
+                       const double *eta, const double *x, double *y, cudaStream_t s);
+cudaError_t launch_zero_ghost_phi(const GridDims &g, double *phi, cudaStream_t s);
+// sum over interior cells of (a - b)^2 into *out (device double, pre-zeroed by the launcher)
+cudaError_t launch_l2dist2(const GridDims &g, const double *a, const double *b, double *out, cudaStream_t s);
+
+}  // namespace idc

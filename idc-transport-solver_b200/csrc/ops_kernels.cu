@@ -1,0 +1,210 @@
+// Streaming transport operators on the reference's layouts (operators/RKDG/TransportOperator.cpp):
+// Pmv (moment reduction), Smv (isotropic scattering source), Lmv (explicit advection-absorption), plus
+// the l2 distance used by source iteration.  All of them touch interior cells only, as the reference
+// does with OpDomain::Interior.  HBM-bound streaming kernels: one pass over psi, coalesced.
+#include "cell_solve.cuh"
+#include "idc_internal.hpp"
+
+namespace idc {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+inline int blocks_for(size_t n, int threads = kThreads) {
+    size_t b = (n + threads - 1) / threads;
+    if (b > (size_t)148 * 32) b = (size_t)148 * 32;   // grid-stride beyond 32 waves of 148 SMs
+    return (int)(b == 0 ? 1 : b);
+}
+
+// phi(i,j,k) <- beta*phi + alpha * sum_q w_q psi(q,i,j,k): TransportOperator::Pmv, :140-158.
+// One thread per (interior cell, dof).
+__global__ void pmv_kernel(GridDims g, double alpha, double beta, const double *__restrict__ w,
+                           const double *__restrict__ psi, double *__restrict__ phi) {
+    const int N = g.P * g.P;
+    const size_t total = (size_t)g.nx * g.ny * N;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const int k = (int)(t % N);
+        const size_t cell = t / N;
+        const int i = 1 + (int)(cell / g.ny), j = 1 + (int)(cell % g.ny);
+        const size_t cidx = (size_t)i * (g.ny + 2) + j;
+        const double *ps = psi + cidx * (size_t)g.nq * N + k;
+        double acc = phi[cidx * N + k] * beta;
+        for (int q = 0; q < g.nq; ++q) acc += alpha * w[q] * ps[(size_t)q * N];
+        phi[cidx * N + k] = acc;
+    }
+}
+
+// psi(q,i,j,k) <- beta*psi + alpha*sigma_s(i,j)*phi(i,j,k)/(4 pi): TransportOperator::Smv, :317-400.
+__global__ void smv_kernel(GridDims g, double alpha, double beta, const double *__restrict__ sigma_s,
+                           const double *__restrict__ phi, double *__restrict__ psi) {
+    const int N = g.P * g.P;
+    const size_t per_cell = (size_t)g.nq * N;
+    const size_t total = (size_t)g.nx * g.ny * per_cell;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const size_t cell = t / per_cell;
+        const size_t within = t - cell * per_cell;
+        const int k = (int)(within % N);
+        const int i = 1 + (int)(cell / g.ny), j = 1 + (int)(cell % g.ny);
+        const size_t cidx = (size_t)i * (g.ny + 2) + j;
+        const double v = (sigma_s[cidx] * phi[cidx * N + k] / (4.0 * M_PI)) * alpha;
+        const size_t idx = cidx * per_cell + within;
+        psi[idx] = beta * psi[idx] + v;
+    }
+}
+
+// y <- beta*y + alpha*(Omega.grad + sigma_t) x: TransportOperator::Lmv, :1215-1480 (piecewise-constant
+// sigma).  One thread per (interior cell, ordinate).
+template <int P>
+__global__ void lmv_kernel(GridDims g, double alpha, double beta, const double *__restrict__ sigma_t,
+                           const double *__restrict__ xi_a, const double *__restrict__ eta_a,
+                           const double *__restrict__ x, double *__restrict__ y) {
+    constexpr int N = P * P;
+    const size_t plane = (size_t)g.nq * N;
+    const size_t istride = (size_t)(g.ny + 2) * plane;
+    const size_t total = (size_t)g.nx * g.ny * g.nq;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const int q = (int)(t % g.nq);
+        const size_t cell = t / g.nq;
+        const int i = 1 + (int)(cell / g.ny), j = 1 + (int)(cell % g.ny);
+        const double xi = xi_a[q], eta = eta_a[q];
+        const bool xneg = xi <= 0.0, yneg = eta <= 0.0;
+        const size_t base = (size_t)i * istride + (size_t)j * plane + (size_t)q * N;
+        const double *X0 = x + base;
+        const double *X1 = x + base + (xneg ? (ptrdiff_t)istride : -(ptrdiff_t)istride);
+        const double *X2 = x + base + (yneg ? (ptrdiff_t)plane : -(ptrdiff_t)plane);
+        double x0[N], x1[N], x2[N], x3[N];
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            x0[k] = X0[k];
+            x1[k] = X1[k];
+            x2[k] = X2[k];
+        }
+        const double s = sigma_t[(size_t)i * (g.ny + 2) + j];
+#pragma unroll
+        for (int k = 0; k < N; ++k) x3[k] = s * x0[k];
+        double cv = xi / g.dx;
+#pragma unroll
+        for (int d = 0; d < P; ++d)
+#pragma unroll
+            for (int a = 0; a < P; ++a)
+#pragma unroll
+                for (int e = 0; e < P; ++e) {
+                    const double f = xneg ? (neg1pow(a) * x1[e + P * a] + neg1pow(d + a + 1) * x0[e + P * a])
+                                          : (x0[e + P * a] + neg1pow(d + 1) * x1[e + P * a]);
+                    x3[e + P * d] += cv * double(2 * d + 1) * f;
+                }
+#pragma unroll
+        for (int d = 0; d < P; ++d)
+#pragma unroll
+            for (int a = d - 1; a >= 0; a -= 2)
+#pragma unroll
+                for (int e = 0; e < P; ++e) x3[e + P * d] -= double(2 * (2 * d + 1)) * cv * x0[e + P * a];
+        cv = eta / g.dy;
+#pragma unroll
+        for (int d = 0; d < P; ++d)
+#pragma unroll
+            for (int e = 0; e < P; ++e)
+#pragma unroll
+                for (int b = 0; b < P; ++b) {
+                    const double f = yneg ? (neg1pow(b) * x2[b + P * d] + neg1pow(e + b + 1) * x0[b + P * d])
+                                          : (x0[b + P * d] + neg1pow(e + 1) * x2[b + P * d]);
+                    x3[e + P * d] += cv * double(2 * e + 1) * f;
+                }
+#pragma unroll
+        for (int d = 0; d < P; ++d)
+#pragma unroll
+            for (int e = 0; e < P; ++e)
+#pragma unroll
+                for (int b = e - 1; b >= 0; b -= 2) x3[e + P * d] -= double(2 * (2 * e + 1)) * cv * x0[b + P * d];
+        double *Y = y + base;
+#pragma unroll
+        for (int k = 0; k < N; ++k) Y[k] = beta * Y[k] + alpha * x3[k];
+    }
+}
+
+__global__ void zero_ghost_phi_kernel(GridDims g, double *phi) {
+    const int N = g.P * g.P;
+    const int nxg = g.nx + 2, nyg = g.ny + 2;
+    const size_t perim = (size_t)2 * nyg + (size_t)2 * g.nx;   // ghost cells
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < perim * N; t += (size_t)gridDim.x * blockDim.x) {
+        const size_t c = t / N;
+        const int k = (int)(t % N);
+        int i, j;
+        if (c < (size_t)nyg) { i = 0; j = (int)c; }
+        else if (c < (size_t)2 * nyg) { i = nxg - 1; j = (int)(c - nyg); }
+        else if (c < (size_t)2 * nyg + g.nx) { i = 1 + (int)(c - 2 * nyg); j = 0; }
+        else { i = 1 + (int)(c - 2 * nyg - g.nx); j = nyg - 1; }
+        phi[((size_t)i * nyg + j) * N + k] = 0.0;
+    }
+}
+
+__global__ void l2dist2_kernel(GridDims g, const double *__restrict__ a, const double *__restrict__ b,
+                               double *__restrict__ out) {
+    const int N = g.P * g.P;
+    const size_t total = (size_t)g.nx * g.ny * N;
+    double acc = 0.0;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const int k = (int)(t % N);
+        const size_t cell = t / N;
+        const int i = 1 + (int)(cell / g.ny), j = 1 + (int)(cell % g.ny);
+        const size_t idx = ((size_t)i * (g.ny + 2) + j) * N + k;
+        const double d = a[idx] - b[idx];
+        acc += d * d;
+    }
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    __shared__ double warp_sums[kThreads / 32];
+    if ((threadIdx.x & 31) == 0) warp_sums[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        acc = threadIdx.x < (blockDim.x >> 5) ? warp_sums[threadIdx.x] : 0.0;
+        for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+        if (threadIdx.x == 0) atomicAdd(out, acc);
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_pmv(const GridDims &g, double alpha, double beta, const double *w, const double *psi, double *phi,
+                       cudaStream_t s) {
+    const size_t n = (size_t)g.nx * g.ny * g.P * g.P;
+    pmv_kernel<<<blocks_for(n), kThreads, 0, s>>>(g, alpha, beta, w, psi, phi);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_smv(const GridDims &g, double alpha, double beta, const double *sigma_s, const double *phi,
+                       double *psi, cudaStream_t s) {
+    const size_t n = (size_t)g.nx * g.ny * g.nq * g.P * g.P;
+    smv_kernel<<<blocks_for(n), kThreads, 0, s>>>(g, alpha, beta, sigma_s, phi, psi);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_lmv(const GridDims &g, double alpha, double beta, const double *sigma_t, const double *xi,
+                       const double *eta, const double *x, double *y, cudaStream_t s) {
+    const size_t n = (size_t)g.nx * g.ny * g.nq;
+    switch (g.P) {
+        case 1: lmv_kernel<1><<<blocks_for(n), kThreads, 0, s>>>(g, alpha, beta, sigma_t, xi, eta, x, y); break;
+        case 2: lmv_kernel<2><<<blocks_for(n), kThreads, 0, s>>>(g, alpha, beta, sigma_t, xi, eta, x, y); break;
+        case 3: lmv_kernel<3><<<blocks_for(n), kThreads, 0, s>>>(g, alpha, beta, sigma_t, xi, eta, x, y); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_zero_ghost_phi(const GridDims &g, double *phi, cudaStream_t s) {
+    const size_t n = ((size_t)2 * (g.ny + 2) + (size_t)2 * g.nx) * g.P * g.P;
+    zero_ghost_phi_kernel<<<blocks_for(n), kThreads, 0, s>>>(g, phi);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_l2dist2(const GridDims &g, const double *a, const double *b, double *out, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(double), s);
+    if (e != cudaSuccess) return e;
+    const size_t n = (size_t)g.nx * g.ny * g.P * g.P;
+    int blocks = blocks_for(n);
+    if (blocks > 148 * 4) blocks = 148 * 4;
+    l2dist2_kernel<<<blocks, kThreads, 0, s>>>(g, a, b, out);
+    return cudaGetLastError();
+}
+
+}  // namespace idc

@@ -1,0 +1,202 @@
+"""ctypes binding of the C ABI in include/idcsweep.h (libidcsweep.so).
+
+This is the host-side mirror of the reference's sweep/operator interface for Python callers (tests,
+bench).  Arrays are numpy float64 host arrays (``loc=HOST``) or raw device pointers (``loc=DEVICE``,
+e.g. ``torch.Tensor.data_ptr()``), always in the reference's halo-padded layouts.
+
+The library is loaded from the package's build directory; if it is missing the import fails loudly
+(there is no CPU fallback).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(HERE), "build", "libidcsweep.so")
+
+IDC_OK = 0
+IDC_ERR_ARG = 1
+IDC_ERR_UNSUPPORTED = 2
+IDC_ERR_CUDA = 3
+IDC_ERR_TIMEOUT = 4
+IDC_ERR_NOT_CONVERGED = 5
+IDC_ERR_STATE = 6
+IDC_ERR_NOMEM = 7
+
+LOC_HOST = 0
+LOC_DEVICE = 1
+
+PREC_FP64 = 0
+PREC_FP32_REFINED = 1
+PREC_FP32 = 2
+
+# Every symbol include/idcsweep.h declares (checked by tests/test_abi_symbols.py).
+EXPORTED_SYMBOLS = (
+    "idc_ctx_create", "idc_ctx_destroy", "idc_set_ordinates", "idc_set_sigma", "idc_sweep", "idc_pmv",
+    "idc_smv", "idc_lmv", "idc_source_iteration", "idc_strerror", "idc_last_error_message", "idc_last_timing",
+    "idc_set_tiling", "idc_sweep_out",
+)
+
+
+class IdcError(RuntimeError):
+    def __init__(self, code: int, where: str, msg: str):
+        super().__init__(f"{where}: status {code} ({msg})")
+        self.code = code
+
+
+class ProblemDesc(C.Structure):
+    _fields_ = [("nx", C.c_int64), ("ny", C.c_int64), ("ax", C.c_double), ("bx", C.c_double),
+                ("ay", C.c_double), ("by", C.c_double), ("dg_degree", C.c_int64), ("sigma_degree", C.c_int64),
+                ("device", C.c_int32), ("flags", C.c_int32)]
+
+
+_dp = C.POINTER(C.c_double)
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Loads libidcsweep.so (once) and declares the prototypes."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} not built: run __graft_entry__.build() or make -C csrc")
+    lib = C.CDLL(path)
+    vp = C.c_void_p
+    lib.idc_ctx_create.argtypes = [C.POINTER(ProblemDesc), C.POINTER(vp)]
+    lib.idc_ctx_destroy.argtypes = [vp]
+    lib.idc_set_ordinates.argtypes = [vp, C.c_int64, vp, vp, vp, vp]
+    lib.idc_set_sigma.argtypes = [vp, vp, vp, C.c_int]
+    lib.idc_sweep.argtypes = [vp, vp, C.c_double, vp, C.c_int, C.c_int]
+    lib.idc_pmv.argtypes = [vp, C.c_double, C.c_double, vp, vp, C.c_int]
+    lib.idc_smv.argtypes = [vp, C.c_double, C.c_double, vp, vp, C.c_int]
+    lib.idc_lmv.argtypes = [vp, C.c_double, C.c_double, vp, vp, C.c_int]
+    lib.idc_source_iteration.argtypes = [vp, vp, C.c_double, C.c_double, C.c_int64, C.c_int, C.c_int,
+                                         C.POINTER(C.c_int64), _dp]
+    lib.idc_strerror.argtypes = [C.c_int]
+    lib.idc_strerror.restype = C.c_char_p
+    lib.idc_last_error_message.argtypes = []
+    lib.idc_last_error_message.restype = C.c_char_p
+    lib.idc_last_timing.argtypes = [vp, _dp, C.POINTER(C.c_int64)]
+    lib.idc_set_tiling.argtypes = [vp, C.c_int32, C.c_int32]
+    lib.idc_sweep_out.argtypes = [vp, vp, vp, C.c_double, vp, C.c_int, C.c_int]
+    for name in EXPORTED_SYMBOLS:
+        if name not in ("idc_strerror", "idc_last_error_message"):
+            getattr(lib, name).restype = C.c_int
+    _lib = lib
+    return lib
+
+
+def _check(rc: int, where: str):
+    if rc != IDC_OK:
+        lib = load_library()
+        msg = lib.idc_last_error_message().decode(errors="replace")
+        raise IdcError(rc, where, msg or lib.idc_strerror(rc).decode())
+
+
+def _host_ptr(a: np.ndarray):
+    if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
+        raise TypeError("arrays must be C-contiguous float64")
+    return C.c_void_p(a.ctypes.data)
+
+
+def _ptr(a, loc: int):
+    if a is None:
+        return None
+    if loc == LOC_DEVICE:
+        return C.c_void_p(int(a))
+    return _host_ptr(a)
+
+
+class SweepContext:
+    """One grid on one GPU: the device-side counterpart of SweepOperator<RKDG::OrdinateFlux> plus the
+    TransportOperator and SISolver routines that operate on its arrays."""
+
+    def __init__(self, nx: int, ny: int, p: int, ax=0.0, bx=1.0, ay=0.0, by=1.0, device: int = 0):
+        lib = load_library()
+        self._lib = lib
+        self.nx, self.ny, self.p = int(nx), int(ny), int(p)
+        self.N = (self.p + 1) ** 2
+        desc = ProblemDesc(self.nx, self.ny, ax, bx, ay, by, self.p, 0, device, 0)
+        h = C.c_void_p()
+        _check(lib.idc_ctx_create(C.byref(desc), C.byref(h)), "idc_ctx_create")
+        self._h = h
+        self.nq = 0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.idc_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- configuration --
+    def set_ordinates(self, xi, eta, w, quad_bounds):
+        self._ord = [np.ascontiguousarray(a, np.float64) for a in (xi, eta, w)]
+        self._qb = np.ascontiguousarray(quad_bounds, np.int64)
+        _check(self._lib.idc_set_ordinates(self._h, int(self._ord[0].size), *[_host_ptr(a) for a in self._ord],
+                                           C.c_void_p(self._qb.ctypes.data)), "idc_set_ordinates")
+        self.nq = int(self._ord[0].size)
+
+    def set_sigma(self, sigma_t, sigma_s=None, loc: int = LOC_HOST):
+        if loc == LOC_HOST:
+            sigma_t = np.ascontiguousarray(sigma_t, np.float64)
+            sigma_s = None if sigma_s is None else np.ascontiguousarray(sigma_s, np.float64)
+        _check(self._lib.idc_set_sigma(self._h, _ptr(sigma_t, loc), _ptr(sigma_s, loc), loc), "idc_set_sigma")
+
+    def set_tiling(self, ordinates_per_block: int = 0, rows_per_block: int = 0):
+        _check(self._lib.idc_set_tiling(self._h, int(ordinates_per_block), int(rows_per_block)), "idc_set_tiling")
+
+    # -- operators --
+    def psi_shape(self):
+        return (self.nx + 2, self.ny + 2, self.nq, self.p + 1, self.p + 1)
+
+    def phi_shape(self):
+        return (self.nx + 2, self.ny + 2, self.p + 1, self.p + 1)
+
+    def sweep(self, psi, dt=np.inf, phi=None, precision=PREC_FP64, loc=LOC_HOST):
+        """In place: psi <- L^{-1} psi; phi (if given) <- P psi."""
+        _check(self._lib.idc_sweep(self._h, _ptr(psi, loc), float(dt), _ptr(phi, loc), int(precision), loc),
+               "idc_sweep")
+
+    def sweep_out(self, source, result, dt=np.inf, phi=None, precision=PREC_FP64, loc=LOC_HOST):
+        """result <- L^{-1} source (interior cells); phi (if given) <- P result."""
+        _check(self._lib.idc_sweep_out(self._h, _ptr(source, loc), _ptr(result, loc), float(dt), _ptr(phi, loc),
+                                       int(precision), loc), "idc_sweep_out")
+
+    def pmv(self, alpha, beta, psi, phi, loc=LOC_HOST):
+        _check(self._lib.idc_pmv(self._h, alpha, beta, _ptr(psi, loc), _ptr(phi, loc), loc), "idc_pmv")
+
+    def smv(self, alpha, beta, phi, psi, loc=LOC_HOST):
+        _check(self._lib.idc_smv(self._h, alpha, beta, _ptr(phi, loc), _ptr(psi, loc), loc), "idc_smv")
+
+    def lmv(self, alpha, beta, x, y, loc=LOC_HOST):
+        _check(self._lib.idc_lmv(self._h, alpha, beta, _ptr(x, loc), _ptr(y, loc), loc), "idc_lmv")
+
+    def source_iteration(self, source, dt=np.inf, abs_tol=1e-10, max_its=500, precision=PREC_FP64, loc=LOC_HOST):
+        """In place: source <- psi of the converged source iteration.  Returns (iterations, last change)."""
+        its = C.c_int64()
+        err = C.c_double()
+        _check(self._lib.idc_source_iteration(self._h, _ptr(source, loc), float(dt), float(abs_tol), int(max_its),
+                                              int(precision), loc, C.byref(its), C.byref(err)),
+               "idc_source_iteration")
+        return int(its.value), float(err.value)
+
+    def last_timing(self):
+        ms = C.c_double()
+        n = C.c_int64()
+        _check(self._lib.idc_last_timing(self._h, C.byref(ms), C.byref(n)), "idc_last_timing")
+        return float(ms.value), int(n.value)

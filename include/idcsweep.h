@@ -1,0 +1,143 @@
+/*
+ * idcsweep — B200 (sm_100a) implementation of the 2-D upwind-DG discrete-ordinates transport sweep of
+ * crockatt/idc-transport-solver, behind a plain C ABI.
+ *
+ * Every entry point takes plain pointers and sizes, returns an int status (IDC_OK == 0) and never
+ * aborts.  Arrays use the reference's layouts, halo cells included, so a caller holding the
+ * reference's objects passes PointerAtCell(0,0) of each one directly:
+ *
+ *   psi   [i][j][q][d][e]  (nx+2)*(ny+2)*nq*N doubles   RKDG::OrdinateFlux::Index,   objects/RKDG/OrdinateFlux.hpp:639-700
+ *   phi   [i][j][d][e]     (nx+2)*(ny+2)*N doubles      RKDG::DensityFunction::Index, objects/RKDG/DensityFunction.hpp
+ *   sigma [i][j]           (nx+2)*(ny+2) doubles        RKDG::CrossSection with DG degree 0 (piecewise constant)
+ *
+ * with i the x index (0 and nx+1 are ghost cells), j the y index, N = (p+1)^2 for DG degree p, and
+ * ordinates sorted into the reference's quadrant ranges (Quadrants(k), utils/Quadrule/OrdinateSet.hpp:352):
+ * quadrant 0 xi>0,eta>0; 1 xi>0,eta<0; 2 xi<0,eta>0; 3 xi<0,eta<0.
+ *
+ * Pointers marked "loc" are host pointers when loc == IDC_LOC_HOST (the library copies them to and from
+ * its own device buffers inside the call) and device pointers on the context's GPU when
+ * loc == IDC_LOC_DEVICE (the call works on them in place).  Calls are synchronous: when one returns, its
+ * results are in place.  A context is not re-entrant: use one context per host thread.
+ */
+#ifndef IDCSWEEP_H
+#define IDCSWEEP_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------------------------------- */
+enum {
+    IDC_OK = 0,
+    IDC_ERR_ARG = 1,            /* invalid argument (null pointer, bad size, unsorted ordinates, ...)   */
+    IDC_ERR_UNSUPPORTED = 2,    /* valid for the reference but not implemented here (e.g. p > 2)        */
+    IDC_ERR_CUDA = 3,           /* a CUDA runtime call failed; idc_last_error_message() has the text     */
+    IDC_ERR_TIMEOUT = 4,        /* a device-side wait gave up (bounded spin); results are not valid      */
+    IDC_ERR_NOT_CONVERGED = 5,  /* an iterative solve stopped at its iteration limit                     */
+    IDC_ERR_STATE = 6,          /* call order violated (e.g. sweep before idc_set_ordinates)             */
+    IDC_ERR_NOMEM = 7           /* device allocation failed                                              */
+};
+
+enum { IDC_LOC_HOST = 0, IDC_LOC_DEVICE = 1 };
+
+/* Arithmetic of a sweep.  IDC_PREC_FP64 restates the reference's FP64 Gaussian elimination.
+ * IDC_PREC_FP32_REFINED factors and solves each cell system in FP32 and refines the solution with
+ * FP64 residuals of the same cell system (all inputs, outputs and inter-cell traces stay FP64).
+ * IDC_PREC_FP32 is the unrefined FP32 solve (for error studies). */
+enum { IDC_PREC_FP64 = 0, IDC_PREC_FP32_REFINED = 1, IDC_PREC_FP32 = 2 };
+
+typedef struct idc_ctx idc_ctx;
+
+typedef struct idc_problem_desc {
+    int64_t nx, ny;          /* interior cells in x and y (DomainDecomposition nx(0), nx(1))            */
+    double ax, bx, ay, by;   /* domain [ax,bx] x [ay,by]; dx = (bx-ax)/nx, dy = (by-ay)/ny              */
+    int64_t dg_degree;       /* DG degree p of psi and phi (Global::DG_degree); 0..2 supported          */
+    int64_t sigma_degree;    /* DG degree of the cross sections; 0 (piecewise constant) supported       */
+    int32_t device;          /* CUDA device ordinal                                                     */
+    int32_t flags;           /* reserved, must be 0                                                     */
+} idc_problem_desc;
+
+/* ---- context --------------------------------------------------------------------------------------- */
+
+/* Creates a context for one grid on one GPU.  Replaces the construction of
+ * SweepOperator<RKDG::OrdinateFlux> (linear_solvers/Abstract/SweepOperator.cpp:25-49) for the
+ * "gpu-wavefront" sweep pattern. */
+int idc_ctx_create(const idc_problem_desc *desc, idc_ctx **out);
+
+/* Releases every device resource of the context.  Accepts NULL. */
+int idc_ctx_destroy(idc_ctx *ctx);
+
+/* Installs the ordinate set: nq ordinates (xi, eta, w) sorted into the four quadrant ranges
+ * quad_bounds[0..4] (quad_bounds[0] = 0, quad_bounds[4] = nq).  Replaces the angular part of the
+ * SweepOperator set-up, i.e. the per-ordinate matrices of SweepLinearSolveSpec::ComputeMatrices
+ * (linear_solvers/RKDG/SweepCellSolve/SweepLinearSolveSpec.cpp:98-158). */
+int idc_set_ordinates(idc_ctx *ctx, int64_t nq, const double *xi, const double *eta, const double *w,
+                      const int64_t quad_bounds[5]);
+
+/* Installs piecewise-constant sigma_t and sigma_s on the halo-padded cell grid (loc as above).
+ * sigma_s may be NULL (treated as zero).  These are the CrossSection arguments of
+ * SweepOperator::Apply and ImplicitSolver::Solve. */
+int idc_set_sigma(idc_ctx *ctx, const double *sigma_t, const double *sigma_s, int loc);
+
+/* Tile shape of the persistent sweep kernel: G ordinates x R rows per thread block (0 = automatic).
+ * A tuning knob only: results do not depend on it.  No reference counterpart (the reference's
+ * closest knob is the compile-time SIMD block length, utils/SIMD.hpp). */
+int idc_set_tiling(idc_ctx *ctx, int32_t ordinates_per_block, int32_t rows_per_block);
+
+/* ---- the sweep ------------------------------------------------------------------------------------- */
+
+/* In-place transport sweep psi <- (Omega.grad + sigma_t + 1/dt)^{-1} psi over the interior cells,
+ * ghost cells of psi_inout carrying the inflow boundary values (they are read, never written).
+ * dt = +INFINITY is steady state.  If phi_out is not NULL it receives phi = sum_q w_q psi_q on the
+ * interior cells (the fused TransportOperator::Pmv(1, 0, psi, phi)); its ghost cells are zeroed.
+ * Replaces SweepOperator<RKDG::OrdinateFlux>::Apply (linear_solvers/Abstract/SweepOperator.cpp:118-135)
+ * with SweepPatternUniCartWavefront::Sweep (.../SweepPattern/SweepPatternUniCartWavefront.cpp:121-332). */
+int idc_sweep(idc_ctx *ctx, double *psi_inout, double dt, double *phi_out, int precision, int loc);
+
+/* Out-of-place form: result <- (Omega.grad + sigma_t + 1/dt)^{-1} source on the interior cells, the
+ * inflow values read from the ghost cells of `source`; result's ghost cells are not written; source is
+ * not modified (it must not overlap result unless they are the same pointer).  The shape of
+ * SweepPattern::Sweep(source, result, sigma, initial) (.../SweepPattern/SweepPattern.hpp:117-122), of
+ * which SweepOperator::Apply is the source == result case. */
+int idc_sweep_out(idc_ctx *ctx, const double *source, double *result, double dt, double *phi_out, int precision,
+                  int loc);
+
+/* ---- transport operators (operators/RKDG/TransportOperator.hpp:25-43), interior cells ------------ */
+
+/* phi <- beta*phi + alpha * sum_q w_q psi_q.              TransportOperator::Pmv, TransportOperator.cpp:140-158 */
+int idc_pmv(idc_ctx *ctx, double alpha, double beta, const double *psi, double *phi, int loc);
+
+/* psi_q <- beta*psi_q + alpha * sigma_s phi / (4 pi).    TransportOperator::Smv, TransportOperator.cpp:317-400 */
+int idc_smv(idc_ctx *ctx, double alpha, double beta, const double *phi, double *psi, int loc);
+
+/* y <- beta*y + alpha * (Omega.grad + sigma_t) x.        TransportOperator::Lmv, TransportOperator.cpp:1215-1689 */
+int idc_lmv(idc_ctx *ctx, double alpha, double beta, const double *x, double *y, int loc);
+
+/* ---- implicit solvers (linear_solvers/Abstract/ImplicitSolver.hpp:116-122) ------------------------- */
+
+/* Source iteration from a zero initial guess: source_inout holds Q on entry and psi on return.
+ * Stops when the absolute l2 change of phi over interior cells is <= abs_tol or after max_its.
+ * Replaces SISolver::Solve (linear_solvers/Abstract/ImplicitSolver/SISolver.cpp:190-254).
+ * *iters and *final_err (either may be NULL) report the iteration count and last change. */
+int idc_source_iteration(idc_ctx *ctx, double *source_inout, double dt, double abs_tol, int64_t max_its,
+                         int precision, int loc, int64_t *iters, double *final_err);
+
+/* ---- diagnostics ----------------------------------------------------------------------------------- */
+
+/* Text for a status code (static storage). */
+const char *idc_strerror(int status);
+
+/* Text of the most recent error on this thread (static per-thread storage). */
+const char *idc_last_error_message(void);
+
+/* Device time in milliseconds of the last sweep kernel launched by the context (CUDA events on the
+ * launching stream), and the number of kernels the last idc_* call launched. */
+int idc_last_timing(idc_ctx *ctx, double *sweep_kernel_ms, int64_t *kernels_launched);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* IDCSWEEP_H */

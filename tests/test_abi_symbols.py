@@ -1,0 +1,62 @@
+"""The C-ABI library loads and exports every entry point include/idcsweep.h declares; argument checks
+that need no GPU behave like the reference's (errors are status codes, never aborts)."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+from conftest import REPO, gpu_available
+from idcsweep import abi
+
+HEADER = os.path.join(REPO, "include", "idcsweep.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(idc_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_header_declares_what_the_binding_lists():
+    assert declared_functions() == sorted(abi.EXPORTED_SYMBOLS)
+
+
+def test_library_exports_every_declared_symbol():
+    lib = abi.load_library()
+    for name in declared_functions():
+        assert hasattr(lib, name), name
+
+
+def test_strerror_and_null_arguments():
+    lib = abi.load_library()
+    assert lib.idc_strerror(abi.IDC_OK) == b"ok"
+    assert lib.idc_strerror(abi.IDC_ERR_TIMEOUT) == b"device-side wait timed out"
+    assert lib.idc_strerror(12345) == b"unknown status"
+    assert lib.idc_ctx_create(None, None) == abi.IDC_ERR_ARG
+    assert lib.idc_sweep(None, None, 1.0, None, 0, 0) == abi.IDC_ERR_ARG
+    assert lib.idc_pmv(None, 1.0, 0.0, None, None, 0) == abi.IDC_ERR_ARG
+    assert lib.idc_ctx_destroy(None) == abi.IDC_OK
+    assert b"null" in lib.idc_last_error_message()
+
+
+def test_descriptor_validation_before_device():
+    lib = abi.load_library()
+    h = C.c_void_p()
+    bad = abi.ProblemDesc(0, 4, 0.0, 1.0, 0.0, 1.0, 1, 0, 0, 0)
+    assert lib.idc_ctx_create(C.byref(bad), C.byref(h)) == abi.IDC_ERR_ARG
+    p3 = abi.ProblemDesc(4, 4, 0.0, 1.0, 0.0, 1.0, 3, 0, 0, 0)
+    assert lib.idc_ctx_create(C.byref(p3), C.byref(h)) == abi.IDC_ERR_UNSUPPORTED
+    hi = abi.ProblemDesc(4, 4, 0.0, 1.0, 0.0, 1.0, 1, 1, 0, 0)
+    assert lib.idc_ctx_create(C.byref(hi), C.byref(h)) == abi.IDC_ERR_UNSUPPORTED
+    empty = abi.ProblemDesc(4, 4, 1.0, 1.0, 0.0, 1.0, 1, 0, 0, 0)
+    assert lib.idc_ctx_create(C.byref(empty), C.byref(h)) == abi.IDC_ERR_ARG
+
+
+@pytest.mark.skipif(gpu_available(), reason="checks the no-GPU path")
+def test_no_device_is_a_status_not_a_crash():
+    lib = abi.load_library()
+    h = C.c_void_p()
+    ok = abi.ProblemDesc(4, 4, 0.0, 1.0, 0.0, 1.0, 1, 0, 0, 0)
+    assert lib.idc_ctx_create(C.byref(ok), C.byref(h)) == abi.IDC_ERR_CUDA
+    assert not h.value
