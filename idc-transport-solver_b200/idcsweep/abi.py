@@ -37,7 +37,7 @@ PREC_FP32 = 2
 EXPORTED_SYMBOLS = (
     "idc_ctx_create", "idc_ctx_destroy", "idc_set_ordinates", "idc_set_sigma", "idc_sweep", "idc_pmv",
     "idc_smv", "idc_lmv", "idc_source_iteration", "idc_strerror", "idc_last_error_message", "idc_last_timing",
-    "idc_set_tiling", "idc_sweep_out",
+    "idc_set_tiling", "idc_sweep_out", "idc_sweep_noalloc",
 )
 
 
@@ -83,6 +83,8 @@ def load_library(path: str = LIB_PATH):
     lib.idc_last_timing.argtypes = [vp, _dp, C.POINTER(C.c_int64)]
     lib.idc_set_tiling.argtypes = [vp, C.c_int32, C.c_int32]
     lib.idc_sweep_out.argtypes = [vp, vp, vp, C.c_double, vp, C.c_int, C.c_int]
+    lib.idc_sweep_noalloc.argtypes = [C.POINTER(ProblemDesc), C.c_int64, vp, vp, vp, vp, vp, vp, vp, C.c_double, vp,
+                                      C.c_int, vp]
     for name in EXPORTED_SYMBOLS:
         if name not in ("idc_strerror", "idc_last_error_message"):
             getattr(lib, name).restype = C.c_int
@@ -200,3 +202,16 @@ class SweepContext:
         n = C.c_int64()
         _check(self._lib.idc_last_timing(self._h, C.byref(ms), C.byref(n)), "idc_last_timing")
         return float(ms.value), int(n.value)
+
+
+def sweep_noalloc(nx, ny, p, ax, bx, ay, by, xi_ptr, eta_ptr, w_ptr, nq, quad_bounds, sigma_t_ptr, source_ptr,
+                  result_ptr, dt=np.inf, phi_ptr=None, precision=PREC_FP64, device=0, stream=None):
+    """idc_sweep_noalloc: the allocation-free out-of-place sweep.  Every array argument is a device
+    pointer (int) the caller owns; quad_bounds is host data.  Returns the status code."""
+    lib = load_library()
+    desc = ProblemDesc(int(nx), int(ny), ax, bx, ay, by, int(p), 0, int(device), 0)
+    qb = np.ascontiguousarray(quad_bounds, np.int64)
+    v = lambda x: None if x is None else C.c_void_p(int(x))
+    return lib.idc_sweep_noalloc(C.byref(desc), int(nq), v(xi_ptr), v(eta_ptr), v(w_ptr), C.c_void_p(qb.ctypes.data),
+                                 v(sigma_t_ptr), v(source_ptr), v(result_ptr), float(dt), v(phi_ptr), int(precision),
+                                 v(stream))

@@ -124,6 +124,33 @@ int idc_lmv(idc_ctx *ctx, double alpha, double beta, const double *x, double *y,
 int idc_source_iteration(idc_ctx *ctx, double *source_inout, double dt, double abs_tol, int64_t max_its,
                          int precision, int loc, int64_t *iters, double *final_err);
 
+/* ---- allocation-free sweep ------------------------------------------------------------------------- */
+
+#define IDC_NOALLOC_MAX_ITEMS 4096      /* work items (row blocks x ordinate chunks) one call can schedule */
+#define IDC_NOALLOC_MAX_ORDINATES 1024  /* ordinates one call accepts                                      */
+
+/* The out-of-place sweep of idc_sweep_out for callers that cannot allocate device memory: a host code that
+ * owns the whole GPU through its own memory arena, or a loop that cannot pay for cudaMalloc/cudaFree,
+ * which may synchronise the device and fail once the memory is reserved.  No counterpart in the
+ * reference (its sweep allocates per-thread work space with malloc on every call,
+ * SweepPatternUniCartWavefront.cpp:147-170).
+ *
+ * Everything is passed in: xi, eta, w (nq each), sigma_t, source, result and phi_out (nullable) are DEVICE
+ * pointers on desc->device; quad_bounds is a host array.  The call makes no cudaMalloc/cudaFree and uses
+ * no context.  The sweep's own scratch (work-queue head, error word, progress flags, work-item list) is
+ * one fixed file-scope device array of about 96 KiB that every GPU loading the library keeps until the
+ * process exits; problems needing more than IDC_NOALLOC_MAX_ITEMS work items, or more than
+ * IDC_NOALLOC_MAX_ORDINATES ordinates, are rejected with IDC_ERR_ARG (use idc_sweep_out for those).
+ * The first call on a device looks up that array's device address (cudaGetSymbolAddress); make that
+ * first call before any stream capture.  All calls share the array and it keeps the last call's
+ * contents; each call clears the parts that must start at zero.  Calls whose kernels overlap on the GPU
+ * would race on it: calls from one process are serialised by a lock, and the call returns only after its
+ * work on `stream` (a cudaStream_t, NULL for the default stream) has finished.  The caller's current
+ * device is restored on return. */
+int idc_sweep_noalloc(const idc_problem_desc *desc, int64_t nq, const double *xi, const double *eta, const double *w,
+                      const int64_t quad_bounds[5], const double *sigma_t, const double *source, double *result,
+                      double dt, double *phi_out, int precision, void *stream);
+
 /* ---- diagnostics ----------------------------------------------------------------------------------- */
 
 /* Text for a status code (static storage). */
