@@ -35,16 +35,17 @@ for _p in (REPO, PKG):
     if _p not in sys.path:
         sys.path.insert(0, _p)
 
-NX, P_DEG, SN = 256, 2, 16
+P_DEG, SN = 2, 16
+NX = 256
 METRIC = "sweep unknowns/s"
 UNIT = "unknowns/s"
 WORKLOAD = "256x256 Q2 S16 log-normal steady sweep (FP32 cell solves + FP64 refinement)"
 FALLBACK_HBM_GBS = 6650.0
 
 
-def problem(seed: int):
+def problem(seed: int, nx: int | None = None):
     from idcsweep.problems import lognormal
-    return lognormal(NX, P_DEG, SN, seed=seed, median=1.0, log_sd=1.0, c_range=(0.5, 0.999), source="uniform")
+    return lognormal(nx or NX, P_DEG, SN, seed=seed, median=1.0, log_sd=1.0, c_range=(0.5, 0.999), source="uniform")
 
 
 def algorithmic_bytes(P) -> int:
@@ -198,7 +199,7 @@ def run_ours(args):
     dev = local if world > 1 else 0
     torch.cuda.set_device(dev)
 
-    P = problem(rank)
+    P = problem(rank, args.nx)
     ctx = abi.SweepContext(P.nx, P.ny, P.p, P.ax, P.bx, P.ay, P.by, device=dev)
     ctx.set_ordinates(P.xi, P.eta, P.w, P.quad)
     ctx.set_sigma(P.sigma_t, P.sigma_s)
@@ -255,18 +256,20 @@ def run_ours(args):
     h_out = torch.empty_like(h_src).pin_memory()
     h_phi = torch.zeros(P.phi_shape(), dtype=torch.float64).pin_memory()
     hs, ho, hp = h_src.numpy(), h_out.numpy(), h_phi.numpy()
-    e2e_steps = max(1, min(args.steps, 10))
-    ctx.sweep_out(hs, ho, P.dt, hp, abi.PREC_FP32_REFINED, loc=abi.LOC_HOST)
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
+    e2e_s, e2e_phi_err = float("nan"), None
+    if not args.no_e2e:
+        e2e_steps = max(1, min(args.steps, 10))
         ctx.sweep_out(hs, ho, P.dt, hp, abi.PREC_FP32_REFINED, loc=abi.LOC_HOST)
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
-    if dist is not None:
-        t = torch.tensor([e2e_s], device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_phi_err = float(np.abs(hp - phi32.cpu().numpy()).max() / np.abs(hp).max())
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            ctx.sweep_out(hs, ho, P.dt, hp, abi.PREC_FP32_REFINED, loc=abi.LOC_HOST)
+        e2e_s = (time.perf_counter() - t0) / e2e_steps
+        if dist is not None:
+            t = torch.tensor([e2e_s], device=f"cuda:{dev}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e_phi_err = float(np.abs(hp - phi32.cpu().numpy()).max() / np.abs(hp).max())
 
     unknowns = P.unknowns_per_sweep
     alg = algorithmic_bytes(P)
@@ -293,7 +296,8 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "f32+f64",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "nx": NX, "ny": NX, "p": P_DEG, "nq": P.nq,
+        "config": {"workload": WORKLOAD if P.nx == NX else WORKLOAD.replace("256x256", f"{P.nx}x{P.nx}"),
+                   "nx": P.nx, "ny": P.ny, "p": P_DEG, "nq": P.nq,
                    "unknowns_per_step": unknowns, "parallelism": f"replicas{world}" if world > 1 else "single",
                    "l2": "inputs larger than L2 (source 690 MB, psi 690 MB per step); no flush"},
         "roofline": {"bound": "hbm", "achieved": alg / (k32 * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
@@ -303,9 +307,10 @@ def run_ours(args):
                  "roofline_frac": alg / (k64 * 1e-3) / 1e9 / peak},
         "speedup_fp32_refined_vs_fp64": ms64 / ms32,
         "err_phi_fp32_refined_vs_fp64_gpu": err_fp32_vs_fp64,
-        "e2e": {"value": world * unknowns / e2e_s, "unit": UNIT,
-                "h2d_bytes_per_step": int(hs.nbytes), "d2h_bytes_per_step": int(P.nx * P.ny * P.nq * P.N * 8 + hp.nbytes),
-                "ms_per_step": e2e_s * 1e3, "phi_rel_diff_vs_device_run": e2e_phi_err},
+        "e2e": None if args.no_e2e else {
+            "value": world * unknowns / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(hs.nbytes),
+            "d2h_bytes_per_step": int(P.nx * P.ny * P.nq * P.N * 8 + hp.nbytes), "ms_per_step": e2e_s * 1e3,
+            "phi_rel_diff_vs_device_run": e2e_phi_err},
         "gpu_launches": launches,
         "clocks": clocks,
     }
@@ -336,6 +341,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg (profiling runs)")
+    ap.add_argument("--nx", type=int, default=NX, help="grid side (default: the benchmark's 256; smaller for ncu)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
