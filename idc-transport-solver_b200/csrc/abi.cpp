@@ -291,6 +291,33 @@ int idc_source_iteration(idc_ctx *ctx, double *source_inout, double dt, double a
     ABI_GUARD_END
 }
 
+int idc_gmres_solve(idc_ctx *ctx, double *source_inout, double dt, double abs_tol, int32_t restart, int64_t max_its,
+                    int precision, int loc, int64_t *iters, double *final_resid) {
+    ABI_GUARD_BEGIN
+    if (!ctx || !source_inout) return fail(IDC_ERR_ARG, "idc_gmres_solve: null argument");
+    if (!valid_loc(loc)) return fail(IDC_ERR_ARG, "bad loc");
+    if (max_its < 0 || !(abs_tol >= 0)) return fail(IDC_ERR_ARG, "idc_gmres_solve: bad tolerance");
+    idc::Context &c = ctx->impl;
+    ABI_TRY_CUDA(cudaSetDevice(c.device));
+    c.launches = 0;
+    ABI_TRY(c.ensure_psi_buffers(2));
+    double *d_src = c.psi_buf(1), *d_psi = c.psi_buf(0);
+    const cudaMemcpyKind in = loc == IDC_LOC_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    const cudaMemcpyKind out = loc == IDC_LOC_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    ABI_TRY_CUDA(cudaMemcpyAsync(d_src, source_inout, sizeof(double) * c.psi_len(), in, c.stream));
+    ABI_TRY_CUDA(cudaMemcpyAsync(d_psi, d_src, sizeof(double) * c.psi_len(), cudaMemcpyDeviceToDevice, c.stream));
+    int64_t its = 0;
+    double res = 0;
+    idc::Status st = c.gmres_peierls(d_src, d_psi, dt, abs_tol, restart, max_its, precision, &its, &res);
+    if (iters) *iters = its;
+    if (final_resid) *final_resid = res;
+    if (!st.good()) return fail(st);
+    ABI_TRY_CUDA(cudaMemcpyAsync(source_inout, d_psi, sizeof(double) * c.psi_len(), out, c.stream));
+    ABI_TRY_CUDA(cudaStreamSynchronize(c.stream));
+    return IDC_OK;
+    ABI_GUARD_END
+}
+
 int idc_last_timing(idc_ctx *ctx, double *sweep_kernel_ms, int64_t *kernels_launched) {
     if (!ctx) return fail(IDC_ERR_ARG, "null context");
     if (sweep_kernel_ms) *sweep_kernel_ms = ctx->impl.last_sweep_ms;

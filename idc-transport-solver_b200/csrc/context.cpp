@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 namespace idc {
@@ -48,6 +49,10 @@ Context::~Context() {
     cudaFree(d_sigma_s);
     cudaFree(d_items);
     cudaFree(d_sync);
+    cudaFree(d_phi_part);
+    cudaFree(d_trace);
+    cudaFree(d_krylov);
+    cudaFree(d_small);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);
@@ -67,6 +72,8 @@ Status Context::init() {
     IDC_TRY_CUDA(cudaEventCreate(&ev0));
     IDC_TRY_CUDA(cudaEventCreate(&ev1));
     IDC_TRY_CUDA(cudaMalloc(&d_scalar_, sizeof(double) * 4));
+    // tuning knob (results do not depend on it): IDC_SWEEP_KERNEL=rowsync selects the row-synchronous kernel
+    if (const char *k = std::getenv("IDC_SWEEP_KERNEL")) use_warp_kernel = std::string(k) != "rowsync";
     return Status::ok();
 }
 
@@ -155,18 +162,58 @@ Status Context::ensure_phi_buffers(int count) {
     return Status::ok();
 }
 
+// Tile shape of the warp kernel: ordinates of a quadrant are split into nch chunks of at most G
+// ordinates, each chunk on a row segment of `seg` lanes (a power of two); a warp holds 32/seg rows and a
+// CTA wn compute warps (at most 7, plus the helper warp).
+static void choose_warp_tiling(int qmax, int user_G, int user_rows, int max_wn, int *G_out, int *seg_out,
+                               int *wn_out) {
+    int seg = 16, G = 0;
+    if (user_G > 0) {
+        G = std::min(user_G, 32);
+        seg = 1;
+        while (seg < G) seg <<= 1;
+        seg = std::max(seg, 1);
+    } else {
+        // from wide to narrow: a narrower segment must use its lanes clearly better (> 10 points) to win,
+        // since every extra chunk adds moment atomics and work items
+        double best = -1.0;
+        for (int cand : {32, 16, 8, 4}) {
+            const int nch = (qmax + cand - 1) / cand;
+            const int g = (qmax + nch - 1) / nch;
+            const double eff = (double)qmax / (nch * cand);
+            if (eff > best + 0.1) {
+                best = eff;
+                seg = cand;
+                G = g;
+            }
+        }
+    }
+    const int rw = 32 / seg;
+    int wn = user_rows > 0 ? std::max(1, user_rows / rw) : 7;
+    wn = std::min(wn, max_wn);
+    *G_out = G;
+    *seg_out = seg;
+    *wn_out = wn;
+}
+
 // Work items in row-block-major order: (row block, quadrant, ordinate chunk).
 Status Context::build_schedule(int precision) {
     if (n_items > 0 && occupancy_precision == precision) return Status::ok();
     int qmax = 0;
     for (int k = 0; k < 4; ++k) qmax = std::max<int>(qmax, (int)(quad[k + 1] - quad[k]));
     if (qmax == 0) return bad(IDC_ERR_ARG, "no ordinates");
-    const int max_threads = 320;
-    int G = user_G > 0 ? user_G : std::min(qmax, P == 3 ? 36 : 64);
-    if (G > max_threads) G = max_threads;
-    int R = user_R > 0 ? user_R : std::max(1, std::min(16, max_threads / G));
-    if (G * R > max_threads) R = std::max(1, max_threads / G);
-    if (R > ny) R = (int)ny;
+    int G = 0, R = 0;
+    if (use_warp_kernel) {
+        choose_warp_tiling(qmax, user_G, user_R, 7, &G, &seg, &wn);
+        R = wn * (32 / seg);
+    } else {
+        const int max_threads = 320;
+        G = user_G > 0 ? user_G : std::min(qmax, P == 3 ? 36 : 64);
+        if (G > max_threads) G = max_threads;
+        R = user_R > 0 ? user_R : std::max(1, std::min(16, max_threads / G));
+        if (G * R > max_threads) R = std::max(1, max_threads / G);
+        if (R > ny) R = (int)ny;
+    }
     tiling.G = G;
     tiling.R = R;
     const int nrb = (int)((ny + R - 1) / R);
@@ -204,6 +251,7 @@ Status Context::build_schedule(int precision) {
         prev_index = cur_index;
     }
     n_items = (int)items.size();
+    items_per_rb = n_items / nrb;
 
     IDC_TRY_CUDA(cudaSetDevice(device));
     cudaFree(d_items);
@@ -215,10 +263,26 @@ Status Context::build_schedule(int precision) {
     IDC_TRY_CUDA(cudaMalloc(&d_sync, sizeof(int) * (2 + items.size())));
     IDC_TRY_CUDA(cudaMemset(d_sync, 0, sizeof(int) * (2 + items.size())));
 
-    block = ((G * R + 31) / 32) * 32;
-    smem = sweep_smem_bytes(P, R, G);
+    if (use_warp_kernel) {
+        cudaFree(d_trace);
+        d_trace = nullptr;
+        const size_t tl = (size_t)n_items * nx * G * N;
+        IDC_TRY_CUDA(cudaMalloc(&d_trace, sizeof(double) * tl));
+        trace_len = tl;
+        IDC_TRY_CUDA(launch_fill_u64(reinterpret_cast<unsigned long long *>(d_trace), tl, kTraceSentinel, stream));
+        IDC_TRY_CUDA(cudaStreamSynchronize(stream));
+    }
+
     int per_sm = 0;
-    IDC_TRY_CUDA(sweep_occupancy(P, precision, block, smem, &per_sm));
+    if (use_warp_kernel) {
+        block = (wn + 1) * 32;
+        smem = sweep_warp_smem_bytes(P, wn, G, seg);
+        IDC_TRY_CUDA(sweep_warp_occupancy(P, precision, block, smem, &per_sm));
+    } else {
+        block = ((G * R + 31) / 32) * 32;
+        smem = sweep_smem_bytes(P, R, G);
+        IDC_TRY_CUDA(sweep_occupancy(P, precision, block, smem, &per_sm));
+    }
     if (per_sm < 1) return bad(IDC_ERR_UNSUPPORTED, "sweep kernel does not fit on an SM with this tiling");
     grid = std::min(n_items, per_sm * num_sms);
     occupancy_precision = precision;
@@ -231,6 +295,8 @@ Status Context::check_device_error() {
     IDC_TRY_CUDA(cudaStreamSynchronize(stream));
     if (err != kDevOk) {
         IDC_TRY_CUDA(cudaMemsetAsync(d_sync + 1, 0, sizeof(int), stream));
+        if (d_trace)
+            IDC_TRY_CUDA(launch_fill_u64(reinterpret_cast<unsigned long long *>(d_trace), trace_len, kTraceSentinel, stream));
         IDC_TRY_CUDA(cudaStreamSynchronize(stream));
         return bad(IDC_ERR_TIMEOUT, "a device-side wait gave up (bounded spin); the sweep was abandoned");
     }
@@ -243,6 +309,8 @@ Status Context::sweep(const double *src, double *out, double dt, double *phi, in
     if (!have_sigma) return bad(IDC_ERR_STATE, "sweep before idc_set_sigma");
     if (precision < 0 || precision > 2) return bad(IDC_ERR_ARG, "unknown precision");
     if (!(dt > 0)) return bad(IDC_ERR_ARG, "dt must be positive (+inf for steady state)");
+    if ((!src || !out) && !use_warp_kernel)
+        return bad(IDC_ERR_UNSUPPORTED, "a sweep without source or output array needs the warp-pipelined kernel");
     IDC_TRY(build_schedule(precision));
     IDC_TRY_CUDA(cudaSetDevice(device));
 
@@ -268,19 +336,46 @@ Status Context::sweep(const double *src, double *out, double dt, double *phi, in
     a.R = tiling.R;
     a.G = tiling.G;
     a.n_refine = 1;
+    a.seg = seg;
+    a.wn = wn;
+    a.trace = d_trace;
+    a.trace_stride = (size_t)nx * tiling.G * N;
     a.next_item = d_sync;
     a.error = d_sync + 1;
     a.progress = d_sync + 2;
     a.spin_limit = spin_limit;
 
+    // the warp kernel writes per-chunk partial moments, summed afterwards in a fixed order
+    if (use_warp_kernel && phi) {
+        const size_t need = (size_t)items_per_rb * phi_len();
+        if (phi_part_len < need) {
+            cudaFree(d_phi_part);
+            d_phi_part = nullptr;
+            phi_part_len = 0;
+            IDC_TRY_CUDA(cudaMalloc(&d_phi_part, sizeof(double) * need));
+            phi_part_len = need;
+        }
+        a.phi = nullptr;
+        a.phi_part = d_phi_part;
+        a.phi_slots = items_per_rb;
+        a.phi_slot_stride = phi_len();
+    }
+
     // queue head and progress flags start at zero; the error word is kept until checked
     IDC_TRY_CUDA(cudaMemsetAsync(d_sync, 0, sizeof(int), stream));
     IDC_TRY_CUDA(cudaMemsetAsync(d_sync + 2, 0, sizeof(int) * n_items, stream));
-    if (phi) IDC_TRY_CUDA(cudaMemsetAsync(phi, 0, sizeof(double) * phi_len(), stream));
+    if (a.phi) IDC_TRY_CUDA(cudaMemsetAsync(phi, 0, sizeof(double) * phi_len(), stream));
     IDC_TRY_CUDA(cudaEventRecord(ev0, stream));
-    IDC_TRY_CUDA(launch_sweep(P, precision, a, grid, block, smem, stream));
+    if (use_warp_kernel)
+        IDC_TRY_CUDA(launch_sweep_warp(P, precision, a, grid, smem, stream));
+    else
+        IDC_TRY_CUDA(launch_sweep(P, precision, a, grid, block, smem, stream));
     IDC_TRY_CUDA(cudaEventRecord(ev1, stream));
     launches += 1;
+    if (a.phi_part) {
+        IDC_TRY_CUDA(launch_reduce_phi_partials(dims(), d_phi_part, items_per_rb, phi_len(), phi, stream));
+        launches += 1;
+    }
     return Status::ok();
 }
 

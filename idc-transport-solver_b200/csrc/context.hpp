@@ -42,6 +42,10 @@ public:
     Status l2dist(const double *a, const double *b, double *out_host);
     Status source_iteration(const double *src, double *psi_out, double dt, double abs_tol, int64_t max_its,
                             int precision, int64_t *iters, double *err);
+    Status gmres_peierls(const double *src, double *psi_out, double dt, double abs_tol, int restart, int64_t max_its,
+                         int precision, int64_t *iters, double *resid);
+    Status apply_peierls(const double *x, double *y, double *tmp_phi, double dt, int precision);
+    Status dot_host(const double *x, const double *y, size_t n, double *out);
 
     // ---- buffers ----
     Status ensure_psi_buffers(int count);   // device scratch psi-sized buffers
@@ -76,6 +80,13 @@ public:
     SweepItem *d_items = nullptr;
     int n_items = 0;
     int *d_sync = nullptr;        // [0] queue head, [1] error word, [2..] progress per item
+    bool use_warp_kernel = true;   // warp-pipelined kernel (sweep_warp.cu) vs row-synchronous (sweep_kernels.cu)
+    int seg = 0, wn = 0;           // warp kernel tiling
+    double *d_trace = nullptr;     // warp kernel: per-item last-row traces (sentinel-armed)
+    size_t trace_len = 0;
+    int items_per_rb = 0;          // work items per row block (= ordinate chunks over all quadrants)
+    double *d_phi_part = nullptr;  // warp kernel: per-chunk partial moments
+    size_t phi_part_len = 0;
     int grid = 0, block = 0;
     size_t smem = 0;
     int occupancy_precision = -1;
@@ -83,6 +94,10 @@ public:
     float last_sweep_ms = 0.f;
     int64_t launches = 0;
     long long spin_limit = 1ll << 22;
+
+    double *d_krylov = nullptr;    // GMRES basis, (restart + 1) phi-sized vectors
+    size_t krylov_len = 0;
+    double *d_small = nullptr;     // GMRES Hessenberg column / coefficients (device)
 
 private:
     Status build_schedule(int precision);

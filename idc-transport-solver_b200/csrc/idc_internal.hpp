@@ -28,12 +28,16 @@ struct SweepItem {
 };
 
 struct SweepArgs {
-    const double *src;         // angular source (read); ghost cells carry the inflow values
-    double *out;               // psi (written); may equal src (in-place sweep)
+    const double *src;         // angular source (read); ghost cells carry the inflow values.  Warp kernel:
+                               // null means zero source and vacuum inflow
+    double *out;               // psi (written); may equal src (in-place sweep).  Warp kernel: null = not stored
     const double *sigma_t;     // (nx+2)(ny+2), piecewise constant
     const double *sigma_s;     // (nx+2)(ny+2) or null: fused isotropic scattering source
     const double *phi_scatter; // phi used by the fused scattering source, or null
     double *phi;               // fused moment output (atomically accumulated, pre-zeroed), or null
+    double *phi_part;          // warp kernel: per-chunk partial moments [phi_slots][stride], or null
+    int phi_slots;             // warp kernel: ordinate chunks per row block (items per row block)
+    size_t phi_slot_stride;    // warp kernel: doubles per partial-moment slot = (nx+2)(ny+2)N
     const double *xi, *eta, *w;
     int nx, ny, nq;
     double dx, dy, inv_dt;
@@ -43,6 +47,10 @@ struct SweepArgs {
     int R;                     // rows per item
     int G;                     // ordinate slots per CTA (>= every item's q_count)
     int n_refine;              // FP64 refinement steps of the FP32 cell solve
+    int seg;                   // warp kernel: lanes per row segment (power of two >= G); rows per warp = 32/seg
+    int wn;                    // warp kernel: compute warps per CTA (rows per CTA = wn * 32/seg)
+    double *trace;             // warp kernel: per-item last-row traces [n_items][nx][G][N], sentinel-armed
+    size_t trace_stride;       // warp kernel: doubles per item in `trace` = nx * G * N
     int *progress;             // per item: columns finished by its last row
     int *next_item;            // dynamic work queue head
     int *error;                // device error word
@@ -61,6 +69,16 @@ cudaError_t launch_sweep(int P, int precision, const SweepArgs &args, int grid, 
 cudaError_t sweep_occupancy(int P, int precision, int block, size_t smem, int *blocks_per_sm);
 size_t sweep_smem_bytes(int P, int R, int G);
 
+// Warp-pipelined sweep kernel (sweep_warp.cu): same arguments, with seg/wn set and R = wn * 32/seg.
+cudaError_t launch_sweep_warp(int P, int precision, const SweepArgs &args, int grid, size_t smem, cudaStream_t stream);
+cudaError_t sweep_warp_occupancy(int P, int precision, int threads, size_t smem, int *blocks_per_sm);
+size_t sweep_warp_smem_bytes(int P, int wn, int G, int seg);
+constexpr int kWarpRingSlots = 8;
+// Bit pattern of an unwritten trace slot: a signalling-NaN payload that floating-point arithmetic never
+// produces (arithmetic returns quiet NaNs).
+constexpr unsigned long long kTraceSentinel = 0x7FF4DEADBEEFCAFEull;
+cudaError_t launch_fill_u64(unsigned long long *p, size_t n, unsigned long long value, cudaStream_t s);
+
 // Operator kernels (ops_kernels.cu).
 struct GridDims {
     int nx, ny, nq, P;
@@ -73,6 +91,14 @@ cudaError_t launch_smv(const GridDims &g, double alpha, double beta, const doubl
 cudaError_t launch_lmv(const GridDims &g, double alpha, double beta, const double *sigma_t, const double *xi,
                        const double *eta, const double *x, double *y, cudaStream_t s);
 cudaError_t launch_zero_ghost_phi(const GridDims &g, double *phi, cudaStream_t s);
+// phi = sum over `slots` partial-moment arrays (interior cells, fixed order); ghost cells of phi zeroed
+cudaError_t launch_reduce_phi_partials(const GridDims &g, const double *part, int slots, size_t stride, double *phi,
+                                       cudaStream_t s);
+// Krylov helpers on flat FP64 vectors of length n (device pointers; `out` arrays are device memory)
+cudaError_t launch_multidot(const double *V, int nv, size_t ld, const double *w, size_t n, double *out, cudaStream_t s);
+cudaError_t launch_multiaxpy(double *w, const double *V, int nv, size_t ld, const double *c, size_t n, cudaStream_t s);
+cudaError_t launch_axpby(double a, const double *x, double b, double *y, size_t n, cudaStream_t s);
+cudaError_t launch_dot(const double *x, const double *y, size_t n, double *out, cudaStream_t s);
 // sum over interior cells of (a - b)^2 into *out (device double, pre-zeroed by the launcher)
 cudaError_t launch_l2dist2(const GridDims &g, const double *a, const double *b, double *out, cudaStream_t s);
 

@@ -139,6 +139,27 @@ __global__ void zero_ghost_phi_kernel(GridDims g, double *phi) {
     }
 }
 
+// phi(cell, k) = sum_{slot} part[slot](cell, k) for interior cells, ghosts zero; one thread per
+// (cell, dof), slots summed in index order.
+__global__ void reduce_phi_partials_kernel(GridDims g, const double *__restrict__ part, int slots, size_t stride,
+                                           double *__restrict__ phi) {
+    const int N = g.P * g.P;
+    const size_t total = (size_t)(g.nx + 2) * (g.ny + 2) * N;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const size_t cell = t / N;
+        const int i = (int)(cell / (g.ny + 2)), j = (int)(cell % (g.ny + 2));
+        double acc = 0.0;
+        if (i >= 1 && i <= g.nx && j >= 1 && j <= g.ny)
+            for (int sl = 0; sl < slots; ++sl) acc += part[(size_t)sl * stride + t];
+        phi[t] = acc;
+    }
+}
+
+__global__ void fill_u64_kernel(unsigned long long *p, size_t n, unsigned long long v) {
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x)
+        p[t] = v;
+}
+
 __global__ void l2dist2_kernel(GridDims g, const double *__restrict__ a, const double *__restrict__ b,
                                double *__restrict__ out) {
     const int N = g.P * g.P;
@@ -163,7 +184,98 @@ __global__ void l2dist2_kernel(GridDims g, const double *__restrict__ a, const d
     }
 }
 
+// out[k] += sum_i V[k*ld + i] * w[i], k < nv (nv <= kMaxKrylov + 1); out pre-zeroed by the launcher.
+constexpr int kMaxDots = 64;
+__global__ void multidot_kernel(const double *__restrict__ V, int nv, size_t ld, const double *__restrict__ w, size_t n,
+                                double *__restrict__ out) {
+    __shared__ double red[kMaxDots][kThreads / 32];
+    double acc[kMaxDots];
+#pragma unroll
+    for (int k = 0; k < kMaxDots; ++k) acc[k] = 0.0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const double wi = w[i];
+#pragma unroll
+        for (int k = 0; k < kMaxDots; ++k)
+            if (k < nv) acc[k] += V[(size_t)k * ld + i] * wi;
+    }
+#pragma unroll
+    for (int k = 0; k < kMaxDots; ++k) {
+        if (k >= nv) break;
+        double v = acc[k];
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if ((threadIdx.x & 31) == 0) red[k][threadIdx.x >> 5] = v;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < nv; k += blockDim.x) {
+        double v = 0.0;
+        for (int t = 0; t < (int)(blockDim.x >> 5); ++t) v += red[k][t];
+        atomicAdd(out + k, v);
+    }
+}
+
+// w[i] -= sum_k c[k] V[k*ld + i]
+__global__ void multiaxpy_kernel(double *__restrict__ w, const double *__restrict__ V, int nv, size_t ld,
+                                 const double *__restrict__ c, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        double acc = w[i];
+        for (int k = 0; k < nv; ++k) acc -= c[k] * V[(size_t)k * ld + i];
+        w[i] = acc;
+    }
+}
+
+// y = a*x + b*y
+__global__ void axpby_kernel(double a, const double *__restrict__ x, double b, double *__restrict__ y, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        y[i] = a * x[i] + b * y[i];
+}
+
+// out[0] += sum x*y
+__global__ void dot_kernel(const double *__restrict__ x, const double *__restrict__ y, size_t n, double *__restrict__ out) {
+    double acc = 0.0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        acc += x[i] * y[i];
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    __shared__ double ws[kThreads / 32];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        acc = threadIdx.x < (blockDim.x >> 5) ? ws[threadIdx.x] : 0.0;
+        for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+        if (threadIdx.x == 0) atomicAdd(out, acc);
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_multidot(const double *V, int nv, size_t ld, const double *w, size_t n, double *out,
+                            cudaStream_t s) {
+    if (nv > kMaxDots) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(double) * nv, s);
+    if (e != cudaSuccess) return e;
+    int blocks = blocks_for(n);
+    if (blocks > 148 * 2) blocks = 148 * 2;
+    multidot_kernel<<<blocks, kThreads, 0, s>>>(V, nv, ld, w, n, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_multiaxpy(double *w, const double *V, int nv, size_t ld, const double *c, size_t n, cudaStream_t s) {
+    multiaxpy_kernel<<<blocks_for(n), kThreads, 0, s>>>(w, V, nv, ld, c, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_axpby(double a, const double *x, double b, double *y, size_t n, cudaStream_t s) {
+    axpby_kernel<<<blocks_for(n), kThreads, 0, s>>>(a, x, b, y, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dot(const double *x, const double *y, size_t n, double *out, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(double), s);
+    if (e != cudaSuccess) return e;
+    int blocks = blocks_for(n);
+    if (blocks > 148 * 4) blocks = 148 * 4;
+    dot_kernel<<<blocks, kThreads, 0, s>>>(x, y, n, out);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_pmv(const GridDims &g, double alpha, double beta, const double *w, const double *psi, double *phi,
                        cudaStream_t s) {
@@ -194,6 +306,18 @@ cudaError_t launch_lmv(const GridDims &g, double alpha, double beta, const doubl
 cudaError_t launch_zero_ghost_phi(const GridDims &g, double *phi, cudaStream_t s) {
     const size_t n = ((size_t)2 * (g.ny + 2) + (size_t)2 * g.nx) * g.P * g.P;
     zero_ghost_phi_kernel<<<blocks_for(n), kThreads, 0, s>>>(g, phi);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_phi_partials(const GridDims &g, const double *part, int slots, size_t stride, double *phi,
+                                       cudaStream_t s) {
+    const size_t n = (size_t)(g.nx + 2) * (g.ny + 2) * g.P * g.P;
+    reduce_phi_partials_kernel<<<blocks_for(n), kThreads, 0, s>>>(g, part, slots, stride, phi);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fill_u64(unsigned long long *p, size_t n, unsigned long long value, cudaStream_t s) {
+    fill_u64_kernel<<<blocks_for(n), kThreads, 0, s>>>(p, n, value);
     return cudaGetLastError();
 }
 

@@ -1,0 +1,171 @@
+// Krylov solver on the GPU: the reference's Peierls-form GMRES (PETScPeierlsSolver,
+// linear_solvers/Abstract/ImplicitSolver/PETScPeierlsSolver.cpp:423-572) with the operator application
+// done by the fused sweep and the Arnoldi process, Hessenberg least squares and all vectors in FP64.
+#include "context.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+namespace idc {
+
+#define IDC_TRY_CUDA(expr)                                    \
+    do {                                                      \
+        cudaError_t e_ = (expr);                              \
+        if (e_ != cudaSuccess) return cuda_status(e_, #expr); \
+    } while (0)
+
+#define IDC_TRY(expr)              \
+    do {                           \
+        Status s_ = (expr);        \
+        if (!s_.good()) return s_; \
+    } while (0)
+
+namespace {
+
+Status bad(int code, const std::string &m) {
+    Status s;
+    s.code = code;
+    s.msg = m;
+    return s;
+}
+
+}  // namespace
+
+Status Context::dot_host(const double *x, const double *y, size_t n, double *out) {
+    IDC_TRY_CUDA(launch_dot(x, y, n, d_scalar_, stream));
+    launches += 1;
+    IDC_TRY_CUDA(cudaMemcpyAsync(out, d_scalar_, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    IDC_TRY_CUDA(cudaStreamSynchronize(stream));
+    return Status::ok();
+}
+
+// y = x - P L^{-1} S x  (IPLS, PETScPeierlsSolver.cpp:529-572): one sweep with no angular source and
+// vacuum inflow, the scattering source built from x on the fly, psi not stored.
+Status Context::apply_peierls(const double *x, double *y, double *tmp_phi, double dt, int precision) {
+    IDC_TRY(sweep(nullptr, nullptr, dt, tmp_phi, precision, x, 1.0));
+    IDC_TRY_CUDA(launch_axpby(1.0, x, 0.0, y, phi_len(), stream));
+    IDC_TRY_CUDA(launch_axpby(-1.0, tmp_phi, 1.0, y, phi_len(), stream));
+    launches += 2;
+    return Status::ok();
+}
+
+// GMRES(restart) from a zero initial guess on (I - P L^{-1} S) phi = P L^{-1} Q, stopping when the
+// residual 2-norm (the Arnoldi estimate, as PETSc reports it) is <= abs_tol, then
+// psi = L^{-1}(S phi + Q).  Classical Gram-Schmidt with one re-orthogonalisation pass (CGS2), Givens
+// rotations on the host.  PETSc's LGMRES adds error-approximation vectors to the restart; it converges
+// to the same fixed point, so iteration counts may differ but the solution does not.
+Status Context::gmres_peierls(const double *src, double *psi_out, double dt, double abs_tol, int restart,
+                              int64_t max_its, int precision, int64_t *iters_out, double *resid_out) {
+    if (!use_warp_kernel) return bad(IDC_ERR_UNSUPPORTED, "GMRES needs the warp-pipelined sweep kernel");
+    if (restart < 1 || restart > 60) return bad(IDC_ERR_ARG, "gmres restart must be in 1..60");
+    const size_t n = phi_len();
+    const int m = restart;
+    IDC_TRY(ensure_phi_buffers(6));
+    double *b = phi_buf(3), *x = phi_buf(4), *tmp = phi_buf(5);
+    if (krylov_len < (size_t)(m + 1) * n) {
+        cudaFree(d_krylov);
+        d_krylov = nullptr;
+        krylov_len = 0;
+        IDC_TRY_CUDA(cudaMalloc(&d_krylov, sizeof(double) * (size_t)(m + 1) * n));
+        krylov_len = (size_t)(m + 1) * n;
+    }
+    if (!d_small) IDC_TRY_CUDA(cudaMalloc(&d_small, sizeof(double) * 128));
+    double *V = d_krylov;
+    auto Vc = [&](int k) { return V + (size_t)k * n; };
+
+    // right-hand side b = P L^{-1} Q (PETScPeierlsSolver.cpp:461-466)
+    IDC_TRY(sweep(src, nullptr, dt, b, precision));
+    IDC_TRY_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, stream));
+
+    // r = b - A x = b for the zero initial guess
+    IDC_TRY_CUDA(cudaMemcpyAsync(Vc(0), b, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream));
+    double beta = 0.0;
+    IDC_TRY(dot_host(Vc(0), Vc(0), n, &beta));
+    beta = std::sqrt(beta);
+
+    std::vector<double> H((size_t)(m + 1) * m, 0.0), cs(m), sn(m), g(m + 1), h(m + 1), h2(m + 1), yv(m);
+    int64_t its = 0;
+    double resid = beta;
+    bool converged = resid <= abs_tol;
+    while (!converged && its < max_its) {
+        IDC_TRY_CUDA(launch_axpby(0.0, Vc(0), 1.0 / beta, Vc(0), n, stream));
+        std::fill(g.begin(), g.end(), 0.0);
+        g[0] = beta;
+        int k = 0;   // columns built in this cycle
+        for (int j = 0; j < m && its < max_its; ++j) {
+            IDC_TRY(apply_peierls(Vc(j), Vc(j + 1), tmp, dt, precision));
+            // CGS2: h = V^T w, w -= V h, twice
+            IDC_TRY_CUDA(launch_multidot(V, j + 1, n, Vc(j + 1), n, d_small, stream));
+            IDC_TRY_CUDA(cudaMemcpyAsync(h.data(), d_small, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost, stream));
+            IDC_TRY_CUDA(launch_multiaxpy(Vc(j + 1), V, j + 1, n, d_small, n, stream));
+            IDC_TRY_CUDA(launch_multidot(V, j + 1, n, Vc(j + 1), n, d_small + 64, stream));
+            IDC_TRY_CUDA(cudaMemcpyAsync(h2.data(), d_small + 64, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost,
+                                         stream));
+            IDC_TRY_CUDA(launch_multiaxpy(Vc(j + 1), V, j + 1, n, d_small + 64, n, stream));
+            launches += 4;
+            double hn = 0.0;
+            IDC_TRY(dot_host(Vc(j + 1), Vc(j + 1), n, &hn));   // synchronises: h, h2 are on the host now
+            hn = std::sqrt(hn);
+            for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = h[i] + h2[i];
+            H[(size_t)(j + 1) * m + j] = hn;
+            if (hn > 0.0) {
+                IDC_TRY_CUDA(launch_axpby(0.0, Vc(j + 1), 1.0 / hn, Vc(j + 1), n, stream));
+                launches += 1;
+            }
+            // apply the previous rotations to the new column, then a new one
+            for (int i = 0; i < j; ++i) {
+                const double a = H[(size_t)i * m + j], c = H[(size_t)(i + 1) * m + j];
+                H[(size_t)i * m + j] = cs[i] * a + sn[i] * c;
+                H[(size_t)(i + 1) * m + j] = -sn[i] * a + cs[i] * c;
+            }
+            const double a = H[(size_t)j * m + j], c = H[(size_t)(j + 1) * m + j];
+            const double r = std::hypot(a, c);
+            cs[j] = r > 0.0 ? a / r : 1.0;
+            sn[j] = r > 0.0 ? c / r : 0.0;
+            H[(size_t)j * m + j] = r;
+            H[(size_t)(j + 1) * m + j] = 0.0;
+            g[j + 1] = -sn[j] * g[j];
+            g[j] = cs[j] * g[j];
+            resid = std::fabs(g[j + 1]);
+            ++its;
+            k = j + 1;
+            IDC_TRY(check_device_error());
+            if (resid <= abs_tol || hn == 0.0) break;
+        }
+        // y = H^{-1} g, x += V y
+        for (int i = k - 1; i >= 0; --i) {
+            double sum = g[i];
+            for (int l = i + 1; l < k; ++l) sum -= H[(size_t)i * m + l] * yv[l];
+            yv[i] = sum / H[(size_t)i * m + i];
+        }
+        for (int i = 0; i < k; ++i) yv[i] = -yv[i];   // multiaxpy subtracts
+        IDC_TRY_CUDA(cudaMemcpyAsync(d_small, yv.data(), sizeof(double) * k, cudaMemcpyHostToDevice, stream));
+        IDC_TRY_CUDA(launch_multiaxpy(x, V, k, n, d_small, n, stream));
+        launches += 1;
+        if (resid <= abs_tol) {
+            converged = true;
+            break;
+        }
+        // restart from the true residual r = b - A x
+        IDC_TRY(apply_peierls(x, Vc(0), tmp, dt, precision));
+        IDC_TRY_CUDA(launch_axpby(1.0, b, -1.0, Vc(0), n, stream));
+        launches += 1;
+        IDC_TRY(dot_host(Vc(0), Vc(0), n, &beta));
+        beta = std::sqrt(beta);
+        resid = beta;
+        converged = resid <= abs_tol;
+        if (beta == 0.0) break;
+    }
+    // psi = L^{-1} (S phi + Q)  (PETScPeierlsSolver.cpp:504-505)
+    IDC_TRY(sweep(src, psi_out, dt, nullptr, precision, x, 1.0));
+    IDC_TRY(check_device_error());
+    if (iters_out) *iters_out = its;
+    if (resid_out) *resid_out = resid;
+    if (!converged)
+        return bad(IDC_ERR_NOT_CONVERGED, "GMRES transport solve failed to converge (max_its reached, residual " +
+                                              std::to_string(resid) + ")");
+    return Status::ok();
+}
+
+}  // namespace idc

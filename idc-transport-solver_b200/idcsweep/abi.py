@@ -37,7 +37,7 @@ PREC_FP32 = 2
 EXPORTED_SYMBOLS = (
     "idc_ctx_create", "idc_ctx_destroy", "idc_set_ordinates", "idc_set_sigma", "idc_sweep", "idc_pmv",
     "idc_smv", "idc_lmv", "idc_source_iteration", "idc_strerror", "idc_last_error_message", "idc_last_timing",
-    "idc_set_tiling", "idc_sweep_out", "idc_sweep_noalloc",
+    "idc_set_tiling", "idc_sweep_out", "idc_sweep_noalloc", "idc_gmres_solve",
 )
 
 
@@ -83,6 +83,8 @@ def load_library(path: str = LIB_PATH):
     lib.idc_last_timing.argtypes = [vp, _dp, C.POINTER(C.c_int64)]
     lib.idc_set_tiling.argtypes = [vp, C.c_int32, C.c_int32]
     lib.idc_sweep_out.argtypes = [vp, vp, vp, C.c_double, vp, C.c_int, C.c_int]
+    lib.idc_gmres_solve.argtypes = [vp, vp, C.c_double, C.c_double, C.c_int32, C.c_int64, C.c_int, C.c_int,
+                                    C.POINTER(C.c_int64), _dp]
     lib.idc_sweep_noalloc.argtypes = [C.POINTER(ProblemDesc), C.c_int64, vp, vp, vp, vp, vp, vp, vp, C.c_double, vp,
                                       C.c_int, vp]
     for name in EXPORTED_SYMBOLS:
@@ -196,6 +198,16 @@ class SweepContext:
                                               int(precision), loc, C.byref(its), C.byref(err)),
                "idc_source_iteration")
         return int(its.value), float(err.value)
+
+    def gmres_solve(self, source, dt=np.inf, abs_tol=1e-8, restart=30, max_its=3000, precision=PREC_FP64,
+                    loc=LOC_HOST):
+        """In place: source <- psi of the Peierls-form GMRES solve.  Returns (iterations, final residual)."""
+        its = C.c_int64()
+        res = C.c_double()
+        _check(self._lib.idc_gmres_solve(self._h, _ptr(source, loc), float(dt), float(abs_tol), int(restart),
+                                         int(max_its), int(precision), loc, C.byref(its), C.byref(res)),
+               "idc_gmres_solve")
+        return int(its.value), float(res.value)
 
     def last_timing(self):
         ms = C.c_double()

@@ -151,6 +151,16 @@ int idc_sweep_noalloc(const idc_problem_desc *desc, int64_t nq, const double *xi
                       const int64_t quad_bounds[5], const double *sigma_t, const double *source, double *result,
                       double dt, double *phi_out, int precision, void *stream);
 
+/* GMRES(restart) on the scalar flux, the Peierls form (I - P L^{-1} S) phi = P L^{-1} Q, from a zero
+ * initial guess; stops when the residual 2-norm is <= abs_tol (absolute, the reference's default criterion),
+ * then psi = L^{-1}(S phi + Q) is returned in source_inout (Q on entry).  Arnoldi (CGS2), Hessenberg least
+ * squares and all vectors are FP64; `precision` selects the sweep arithmetic.  Replaces
+ * PETScPeierlsSolver::Solve with IPLS (linear_solvers/Abstract/ImplicitSolver/PETScPeierlsSolver.cpp:423-572);
+ * PETSc's LGMRES augmentation is not reproduced (same fixed point, different iteration counts).  Returns
+ * IDC_ERR_NOT_CONVERGED after max_its iterations, as the reference throws. */
+int idc_gmres_solve(idc_ctx *ctx, double *source_inout, double dt, double abs_tol, int32_t restart, int64_t max_its,
+                    int precision, int loc, int64_t *iters, double *final_resid);
+
 /* ---- diagnostics ----------------------------------------------------------------------------------- */
 
 /* Text for a status code (static storage). */
