@@ -51,6 +51,7 @@ Context::~Context() {
     cudaFree(d_sync);
     cudaFree(d_phi_part);
     cudaFree(d_trace);
+    cudaFree(d_inflow);
     cudaFree(d_krylov);
     cudaFree(d_small);
     if (ev0) cudaEventDestroy(ev0);
@@ -72,8 +73,12 @@ Status Context::init() {
     IDC_TRY_CUDA(cudaEventCreate(&ev0));
     IDC_TRY_CUDA(cudaEventCreate(&ev1));
     IDC_TRY_CUDA(cudaMalloc(&d_scalar_, sizeof(double) * 4));
-    // tuning knob (results do not depend on it): IDC_SWEEP_KERNEL=rowsync selects the row-synchronous kernel
-    if (const char *k = std::getenv("IDC_SWEEP_KERNEL")) use_warp_kernel = std::string(k) != "rowsync";
+    // IDC_SWEEP_KERNEL=warp|rowsync selects one of the elimination kernels instead of the modal one
+    if (const char *k = std::getenv("IDC_SWEEP_KERNEL")) {
+        const std::string v(k);
+        kernel = v == "rowsync" ? kRowSync : v == "warp" ? kWarp : kModal;
+    }
+    use_warp_kernel = kernel != kRowSync;
     return Status::ok();
 }
 
@@ -162,17 +167,16 @@ Status Context::ensure_phi_buffers(int count) {
     return Status::ok();
 }
 
-// Tile shape of the warp kernel: ordinates of a quadrant are split into nch chunks of at most G
-// ordinates, each chunk on a row segment of `seg` lanes (a power of two); a warp holds 32/seg rows and a
-// CTA wn compute warps (at most 7, plus the helper warp).
+// Tile shape of the warp and modal kernels: ordinates of a quadrant are split into nch chunks of at most
+// G ordinates, each chunk on a row segment of `seg` lanes (a power of two, at least 4); a warp holds
+// 32/seg rows and a CTA wn compute warps (at most 7, plus the helper warp).
 static void choose_warp_tiling(int qmax, int user_G, int user_rows, int max_wn, int *G_out, int *seg_out,
                                int *wn_out) {
     int seg = 16, G = 0;
     if (user_G > 0) {
         G = std::min(user_G, 32);
-        seg = 1;
+        seg = 4;
         while (seg < G) seg <<= 1;
-        seg = std::max(seg, 1);
     } else {
         // from wide to narrow: a narrower segment must use its lanes clearly better (> 10 points) to win,
         // since every extra chunk adds moment atomics and work items
@@ -266,7 +270,7 @@ Status Context::build_schedule(int precision) {
     if (use_warp_kernel) {
         cudaFree(d_trace);
         d_trace = nullptr;
-        const size_t tl = (size_t)n_items * nx * G * N;
+        const size_t tl = (size_t)n_items * nx * G * (kernel == kModal ? P : N);
         IDC_TRY_CUDA(cudaMalloc(&d_trace, sizeof(double) * tl));
         trace_len = tl;
         IDC_TRY_CUDA(launch_fill_u64(reinterpret_cast<unsigned long long *>(d_trace), tl, kTraceSentinel, stream));
@@ -274,7 +278,11 @@ Status Context::build_schedule(int precision) {
     }
 
     int per_sm = 0;
-    if (use_warp_kernel) {
+    if (kernel == kModal) {
+        block = (wn + 1) * 32;
+        smem = sweep_modal_smem_bytes(P, wn, G, seg);
+        IDC_TRY_CUDA(sweep_modal_occupancy(P, precision, seg, block, smem, &per_sm));
+    } else if (kernel == kWarp) {
         block = (wn + 1) * 32;
         smem = sweep_warp_smem_bytes(P, wn, G, seg);
         IDC_TRY_CUDA(sweep_warp_occupancy(P, precision, block, smem, &per_sm));
@@ -339,7 +347,7 @@ Status Context::sweep(const double *src, double *out, double dt, double *phi, in
     a.seg = seg;
     a.wn = wn;
     a.trace = d_trace;
-    a.trace_stride = (size_t)nx * tiling.G * N;
+    a.trace_stride = (size_t)nx * tiling.G * (kernel == kModal ? P : N);
     a.next_item = d_sync;
     a.error = d_sync + 1;
     a.progress = d_sync + 2;
@@ -366,7 +374,23 @@ Status Context::sweep(const double *src, double *out, double dt, double *phi, in
     IDC_TRY_CUDA(cudaMemsetAsync(d_sync + 2, 0, sizeof(int) * n_items, stream));
     if (a.phi) IDC_TRY_CUDA(cudaMemsetAsync(phi, 0, sizeof(double) * phi_len(), stream));
     IDC_TRY_CUDA(cudaEventRecord(ev0, stream));
-    if (use_warp_kernel)
+    if (kernel == kModal) {
+        if (src) {   // inflow traces of the ghost cells (packed modal, or physical for the refined mode)
+            const size_t need = (size_t)(nx + ny) * nq * P;
+            if (inflow_len < need) {
+                cudaFree(d_inflow);
+                d_inflow = nullptr;
+                inflow_len = 0;
+                IDC_TRY_CUDA(cudaMalloc(&d_inflow, sizeof(double) * need));
+                inflow_len = need;
+            }
+            IDC_TRY_CUDA(launch_inflow_traces(P, precision != IDC_PREC_FP32_REFINED, src, d_xi, d_eta, (int)nx,
+                                              (int)ny, (int)nq, d_inflow, stream));
+            launches += 1;
+            a.inflow = d_inflow;
+        }
+        IDC_TRY_CUDA(launch_sweep_modal(P, precision, a, grid, smem, stream));
+    } else if (kernel == kWarp)
         IDC_TRY_CUDA(launch_sweep_warp(P, precision, a, grid, smem, stream));
     else
         IDC_TRY_CUDA(launch_sweep(P, precision, a, grid, block, smem, stream));

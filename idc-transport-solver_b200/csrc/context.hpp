@@ -80,9 +80,15 @@ public:
     SweepItem *d_items = nullptr;
     int n_items = 0;
     int *d_sync = nullptr;        // [0] queue head, [1] error word, [2..] progress per item
-    bool use_warp_kernel = true;   // warp-pipelined kernel (sweep_warp.cu) vs row-synchronous (sweep_kernels.cu)
+    // sweep kernel: modal (sweep_modal.cu, default), warp-pipelined with elimination (sweep_warp.cu) or
+    // row-synchronous (sweep_kernels.cu)
+    enum Kernel { kRowSync = 0, kWarp = 1, kModal = 2 };
+    int kernel = kModal;
+    bool use_warp_kernel = true;   // kernel is kWarp or kModal (same schedule and trace protocol)
     int seg = 0, wn = 0;           // warp kernel tiling
-    double *d_trace = nullptr;     // warp kernel: per-item last-row traces (sentinel-armed)
+    double *d_trace = nullptr;     // warp / modal kernel: per-item last-row traces (sentinel-armed)
+    double *d_inflow = nullptr;    // modal kernel: inflow traces of the ghost cells
+    size_t inflow_len = 0;
     size_t trace_len = 0;
     int items_per_rb = 0;          // work items per row block (= ordinate chunks over all quadrants)
     double *d_phi_part = nullptr;  // warp kernel: per-chunk partial moments

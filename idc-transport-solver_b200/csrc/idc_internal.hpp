@@ -28,8 +28,9 @@ struct SweepItem {
 };
 
 struct SweepArgs {
-    const double *src;         // angular source (read); ghost cells carry the inflow values.  Warp kernel:
-                               // null means zero source and vacuum inflow
+    const double *src;         // angular source (read); ghost cells carry the inflow values.  Warp and modal
+                               // kernels: null means zero source and vacuum inflow
+    const double *inflow;      // modal kernel: inflow traces of the ghost cells [nx + ny][nq][P], or null
     double *out;               // psi (written); may equal src (in-place sweep).  Warp kernel: null = not stored
     const double *sigma_t;     // (nx+2)(ny+2), piecewise constant
     const double *sigma_s;     // (nx+2)(ny+2) or null: fused isotropic scattering source
@@ -49,8 +50,9 @@ struct SweepArgs {
     int n_refine;              // FP64 refinement steps of the FP32 cell solve
     int seg;                   // warp kernel: lanes per row segment (power of two >= G); rows per warp = 32/seg
     int wn;                    // warp kernel: compute warps per CTA (rows per CTA = wn * 32/seg)
-    double *trace;             // warp kernel: per-item last-row traces [n_items][nx][G][N], sentinel-armed
-    size_t trace_stride;       // warp kernel: doubles per item in `trace` = nx * G * N
+    double *trace;             // warp / modal kernel: per-item last-row traces [n_items][nx][G][V], V = N (warp)
+                               // or P (modal), sentinel-armed
+    size_t trace_stride;       // doubles per item in `trace` = nx * G * V
     int *progress;             // per item: columns finished by its last row
     int *next_item;            // dynamic work queue head
     int *error;                // device error word
@@ -74,6 +76,16 @@ cudaError_t launch_sweep_warp(int P, int precision, const SweepArgs &args, int g
 cudaError_t sweep_warp_occupancy(int P, int precision, int threads, size_t smem, int *blocks_per_sm);
 size_t sweep_warp_smem_bytes(int P, int wn, int G, int seg);
 constexpr int kWarpRingSlots = 8;
+
+// Modal sweep kernel (sweep_modal.cu): same arguments as the warp kernel plus `inflow`, traces of P values.
+cudaError_t launch_sweep_modal(int P, int precision, const SweepArgs &args, int grid, size_t smem, cudaStream_t stream);
+cudaError_t sweep_modal_occupancy(int P, int precision, int seg, int threads, size_t smem, int *blocks_per_sm);
+size_t sweep_modal_smem_bytes(int P, int wn, int G, int seg);
+// Inflow traces of the ghost cells of `src` for the modal kernel: out[(k * nq + q) * P + m], k < nx the
+// ghost row below column k, k >= nx the ghost column left of row k - nx (sweep order); packed modal
+// coefficients if `modal`, else sign-flipped physical traces.
+cudaError_t launch_inflow_traces(int P, bool modal, const double *src, const double *xi, const double *eta, int nx,
+                                 int ny, int nq, double *out, cudaStream_t stream);
 // Bit pattern of an unwritten trace slot: a signalling-NaN payload that floating-point arithmetic never
 // produces (arithmetic returns quiet NaNs).
 constexpr unsigned long long kTraceSentinel = 0x7FF4DEADBEEFCAFEull;
