@@ -318,6 +318,88 @@ int idc_gmres_solve(idc_ctx *ctx, double *source_inout, double dt, double abs_to
     ABI_GUARD_END
 }
 
+int idc_sweep_adjoint(idc_ctx *ctx, const double *source, double *result, double dt, double *moments_out, int precision,
+                      int loc) {
+    ABI_GUARD_BEGIN
+    if (!ctx || !source || !result) return fail(IDC_ERR_ARG, "idc_sweep_adjoint: null argument");
+    if (!valid_loc(loc)) return fail(IDC_ERR_ARG, "bad loc");
+    idc::Context &c = ctx->impl;
+    if (!c.have_ordinates) return fail(IDC_ERR_STATE, "idc_sweep_adjoint before idc_set_ordinates");
+    ABI_TRY_CUDA(cudaSetDevice(c.device));
+    c.launches = 0;
+    if (loc == IDC_LOC_DEVICE) {
+        ABI_TRY(c.sweep(source, result, dt, moments_out, precision, nullptr, 1.0, true));
+        ABI_TRY(c.check_device_error());
+    } else {
+        ABI_TRY(c.ensure_psi_buffers(2));
+        ABI_TRY(c.ensure_phi_buffers(3));
+        double *d_src = c.psi_buf(1), *d_res = c.psi_buf(0);
+        double *d_mom = moments_out ? c.phi_buf(2) : nullptr;
+        ABI_TRY_CUDA(cudaMemcpyAsync(d_src, source, sizeof(double) * c.psi_len(), cudaMemcpyHostToDevice, c.stream));
+        ABI_TRY(c.sweep(d_src, d_res, dt, d_mom, precision, nullptr, 1.0, true));
+        const size_t cell = (size_t)c.nq * c.N;
+        for (int64_t i = 1; i <= c.nx; ++i) {
+            const size_t off = ((size_t)i * (c.ny + 2) + 1) * cell;
+            ABI_TRY_CUDA(cudaMemcpyAsync(result + off, d_res + off, sizeof(double) * cell * c.ny,
+                                         cudaMemcpyDeviceToHost, c.stream));
+        }
+        if (moments_out)
+            ABI_TRY_CUDA(cudaMemcpyAsync(moments_out, d_mom, sizeof(double) * c.phi_len(), cudaMemcpyDeviceToHost,
+                                         c.stream));
+        ABI_TRY(c.check_device_error());
+    }
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, c.ev0, c.ev1) == cudaSuccess) c.last_sweep_ms = ms;
+    return IDC_OK;
+    ABI_GUARD_END
+}
+
+int idc_adjoint_grad(idc_ctx *ctx, const double *psi, const double *detector, double dt, double abs_tol,
+                     int32_t restart, int64_t max_its, int precision, double *dsigma_t, double *dsigma_s,
+                     double *dsource, int loc, int64_t *iters, double *final_resid) {
+    ABI_GUARD_BEGIN
+    if (!ctx || !psi || !detector) return fail(IDC_ERR_ARG, "idc_adjoint_grad: null argument");
+    if (!valid_loc(loc)) return fail(IDC_ERR_ARG, "bad loc");
+    if (max_its < 0 || !(abs_tol >= 0)) return fail(IDC_ERR_ARG, "idc_adjoint_grad: bad tolerance");
+    idc::Context &c = ctx->impl;
+    if (!c.have_ordinates || !c.have_sigma) return fail(IDC_ERR_STATE, "idc_adjoint_grad before ordinates and sigma");
+    ABI_TRY_CUDA(cudaSetDevice(c.device));
+    c.launches = 0;
+    ABI_TRY(c.ensure_psi_buffers(2));
+    ABI_TRY(c.ensure_phi_buffers(14));
+    const double *d_psi = psi;
+    double *d_det = c.phi_buf(10);
+    double *d_gt = dsigma_t, *d_gs = dsigma_s, *d_gq = dsource;
+    const cudaMemcpyKind in = loc == IDC_LOC_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    if (loc == IDC_LOC_HOST) {
+        ABI_TRY_CUDA(cudaMemcpyAsync(c.psi_buf(1), psi, sizeof(double) * c.psi_len(), in, c.stream));
+        d_psi = c.psi_buf(1);
+        d_gt = dsigma_t ? c.phi_buf(11) : nullptr;   // sigma-sized results fit a moment-sized buffer
+        d_gs = dsigma_s ? c.phi_buf(12) : nullptr;
+        d_gq = dsource ? c.phi_buf(13) : nullptr;
+    }
+    ABI_TRY_CUDA(cudaMemcpyAsync(d_det, detector, sizeof(double) * c.phi_len(), in, c.stream));
+    ABI_TRY_CUDA(idc::launch_zero_ghost_phi(c.dims(), d_det, c.stream));
+    int64_t its = 0;
+    double res = 0;
+    idc::Status st = c.adjoint_gradient(d_psi, d_det, dt, abs_tol, restart, max_its, precision, d_gt, d_gs, d_gq, &its,
+                                        &res);
+    if (iters) *iters = its;
+    if (final_resid) *final_resid = res;
+    if (!st.good()) return fail(st);
+    if (loc == IDC_LOC_HOST) {
+        if (dsigma_t)
+            ABI_TRY_CUDA(cudaMemcpyAsync(dsigma_t, d_gt, sizeof(double) * c.sig_len(), cudaMemcpyDeviceToHost, c.stream));
+        if (dsigma_s)
+            ABI_TRY_CUDA(cudaMemcpyAsync(dsigma_s, d_gs, sizeof(double) * c.sig_len(), cudaMemcpyDeviceToHost, c.stream));
+        if (dsource)
+            ABI_TRY_CUDA(cudaMemcpyAsync(dsource, d_gq, sizeof(double) * c.phi_len(), cudaMemcpyDeviceToHost, c.stream));
+    }
+    ABI_TRY_CUDA(cudaStreamSynchronize(c.stream));
+    return IDC_OK;
+    ABI_GUARD_END
+}
+
 int idc_last_timing(idc_ctx *ctx, double *sweep_kernel_ms, int64_t *kernels_launched) {
     if (!ctx) return fail(IDC_ERR_ARG, "null context");
     if (sweep_kernel_ms) *sweep_kernel_ms = ctx->impl.last_sweep_ms;

@@ -312,13 +312,15 @@ Status Context::check_device_error() {
 }
 
 Status Context::sweep(const double *src, double *out, double dt, double *phi, int precision,
-                      const double *phi_scatter, double scatter_scale) {
+                      const double *phi_scatter, double scatter_scale, bool adjoint) {
     if (!have_ordinates) return bad(IDC_ERR_STATE, "sweep before idc_set_ordinates");
     if (!have_sigma) return bad(IDC_ERR_STATE, "sweep before idc_set_sigma");
     if (precision < 0 || precision > 2) return bad(IDC_ERR_ARG, "unknown precision");
     if (!(dt > 0)) return bad(IDC_ERR_ARG, "dt must be positive (+inf for steady state)");
     if ((!src || !out) && !use_warp_kernel)
         return bad(IDC_ERR_UNSUPPORTED, "a sweep without source or output array needs the warp-pipelined kernel");
+    if (adjoint && (kernel != kModal || precision == IDC_PREC_FP32))
+        return bad(IDC_ERR_UNSUPPORTED, "the transposed sweep needs the modal kernel in FP64 or refined precision");
     IDC_TRY(build_schedule(precision));
     IDC_TRY_CUDA(cudaSetDevice(device));
 
@@ -352,6 +354,7 @@ Status Context::sweep(const double *src, double *out, double dt, double *phi, in
     a.error = d_sync + 1;
     a.progress = d_sync + 2;
     a.spin_limit = spin_limit;
+    a.adjoint = adjoint ? 1 : 0;
 
     // the warp kernel writes per-chunk partial moments, summed afterwards in a fixed order
     if (use_warp_kernel && phi) {
@@ -375,7 +378,7 @@ Status Context::sweep(const double *src, double *out, double dt, double *phi, in
     if (a.phi) IDC_TRY_CUDA(cudaMemsetAsync(phi, 0, sizeof(double) * phi_len(), stream));
     if (kernel != kModal) IDC_TRY_CUDA(cudaEventRecord(ev0, stream));
     if (kernel == kModal) {
-        if (src) {   // inflow traces of the ghost cells (packed modal, or physical for the refined mode)
+        if (src && !adjoint) {   // inflow traces of the ghost cells (packed modal, or physical for the refined mode)
             const size_t need = (size_t)(nx + ny) * nq * P;
             if (inflow_len < need) {
                 cudaFree(d_inflow);

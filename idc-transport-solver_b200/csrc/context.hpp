@@ -35,7 +35,7 @@ public:
     // ---- operators on device pointers ----
     // Sweep: out <- L^{-1} (src [+ scale * S phi_scatter]); phi (nullable) <- P out.  src may equal out.
     Status sweep(const double *src, double *out, double dt, double *phi, int precision,
-                 const double *phi_scatter = nullptr, double scatter_scale = 1.0);
+                 const double *phi_scatter = nullptr, double scatter_scale = 1.0, bool adjoint = false);
     Status pmv(double alpha, double beta, const double *psi, double *phi);
     Status smv(double alpha, double beta, const double *phi, double *psi);
     Status lmv(double alpha, double beta, const double *x, double *y);
@@ -45,6 +45,18 @@ public:
     Status gmres_peierls(const double *src, double *psi_out, double dt, double abs_tol, int restart, int64_t max_its,
                          int precision, int64_t *iters, double *resid);
     Status apply_peierls(const double *x, double *y, double *tmp_phi, double dt, int precision);
+    // GMRES(restart) from x = 0 on A x = b for an operator on moment-sized vectors; *converged reports
+    // whether the residual reached abs_tol (the caller decides whether that is an error)
+    template <typename Op>
+    Status gmres(Op apply, const double *b, double *x, double abs_tol, int restart, int64_t max_its, int64_t *iters,
+                 double *resid, bool *converged);
+    // transposed (adjoint) problem: (L - S P)^T lam = P^T c, via (I - S^T L^{-T} P^T) mu = c
+    Status apply_peierls_adjoint(const double *x, double *y, double *tmp_phi, double dt, int precision);
+    Status adjoint_solve(const double *detector, double *lam_out, double *Lam_out, double dt, double abs_tol,
+                         int restart, int64_t max_its, int precision, int64_t *iters, double *resid);
+    Status adjoint_gradient(const double *psi, const double *detector, double dt, double abs_tol, int restart,
+                            int64_t max_its, int precision, double *dsig_t, double *dsig_s, double *dq,
+                            int64_t *iters, double *resid);
     Status dot_host(const double *x, const double *y, size_t n, double *out);
 
     // ---- buffers ----

@@ -57,6 +57,8 @@ struct SweepArgs {
     int *next_item;            // dynamic work queue head
     int *error;                // device error word
     long long spin_limit;      // polls before a wait gives up
+    int adjoint;               // modal kernel: 1 = transposed sweep (reverse order; phi_scatter is mu and the
+                               // fused source is w_q mu; the moments are unweighted sums over ordinates)
 };
 
 // Launch geometry picked by the host (autotuner or defaults).
@@ -111,6 +113,13 @@ cudaError_t launch_multidot(const double *V, int nv, size_t ld, const double *w,
 cudaError_t launch_multiaxpy(double *w, const double *V, int nv, size_t ld, const double *c, size_t n, cudaStream_t s);
 cudaError_t launch_axpby(double a, const double *x, double b, double *y, size_t n, cudaStream_t s);
 cudaError_t launch_dot(const double *x, const double *y, size_t n, double *out, cudaStream_t s);
+// adjoint Peierls operator: y = x - sigma_s/(4 pi) lam on interior cells, y = x on ghost cells
+cudaError_t launch_adjoint_scatter(const GridDims &g, const double *sigma_s, const double *x, const double *lam,
+                                   double *y, cudaStream_t s);
+// per-cell gradients of J = c . phi from the forward psi, phi and the adjoint lam, Lam = sum_q lam_q
+// (outputs on the halo layouts, interior cells written, any of them nullable)
+cudaError_t launch_adjoint_gradient(const GridDims &g, const double *psi, const double *lam, const double *phi,
+                                    const double *Lam, double *dsig_t, double *dsig_s, double *dq, cudaStream_t s);
 // sum over interior cells of (a - b)^2 into *out (device double, pre-zeroed by the launcher)
 cudaError_t launch_l2dist2(const GridDims &g, const double *a, const double *b, double *out, cudaStream_t s);
 

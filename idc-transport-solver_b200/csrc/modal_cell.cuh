@@ -18,6 +18,12 @@
 // x' = Vp Z Vp^T is needed only for the stored psi and the moments.  The recurrence from cell to
 // cell is therefore a handful of fused multiply-adds deep, and the dense transforms are off it.
 //
+// The transposed (adjoint) sweep solves A'^T lam = r + ax 1 (x) ft + ay gt (x) 1 with the outgoing traces
+// ft(e) = sum_d u_d lam(d,e), gt(d) = sum_e u_e lam(d,e) (the transpose of the rank-one coupling), in
+// reverse traversal order.  M^T = Vp_T blockdiag Wp_T with Vp_T = Wp^T J, Wp_T = J Vp^T,
+// J = diag(+1 for Re and real indices, -1 for Im indices), so the same block solve applies, with the
+// coupling vector t (instead of uh) and the trace weights J uh (instead of t).  Templates take ADJ.
+//
 // Index conventions: a cell array v[e + P*d] holds Legendre degree d in x and e in y (the psi layout);
 // a modal array Z[b + P*a] holds packed x-mode a and y-mode b.
 #pragma once
@@ -33,6 +39,36 @@ __host__ __device__ constexpr double flip_sign(int d) {
     return (NEG && (d & 1)) ? -1.0 : 1.0;
 }
 
+// J of the transposed basis: -1 on the Im index of each complex pair.
+template <int P>
+__host__ __device__ constexpr double jsign(int k) {
+    return (k < 2 * ModalTable<P>::kPairs && (k & 1)) ? -1.0 : 1.0;
+}
+// Trace weight t_k of packed index k: column sums of Vp (1 for a pair's Re index and the real index).
+template <int P>
+__host__ __device__ constexpr double tweight(int k) {
+    return (k < 2 * ModalTable<P>::kPairs && (k & 1)) ? 0.0 : 1.0;
+}
+// Basis of the forward (ADJ = false) or transposed (ADJ = true) cell operator: packed coefficients
+// out = Wb v Wb^T, cell values v = Vb Z Vb^T; coupling vector of the incoming traces and weights of the
+// outgoing traces.
+template <int P, bool ADJ>
+__host__ __device__ constexpr double basis_w(int a, int d) {
+    return ADJ ? jsign<P>(a) * ModalTable<P>::V(d, a) : ModalTable<P>::W(a, d);
+}
+template <int P, bool ADJ>
+__host__ __device__ constexpr double basis_v(int d, int a) {
+    return ADJ ? ModalTable<P>::W(a, d) * jsign<P>(a) : ModalTable<P>::V(d, a);
+}
+template <int P, bool ADJ>
+__host__ __device__ constexpr double couple_w(int k) {
+    return ADJ ? tweight<P>(k) : ModalTable<P>::uh(k);
+}
+template <int P, bool ADJ>
+__host__ __device__ constexpr double trace_w(int k) {
+    return ADJ ? jsign<P>(k) * ModalTable<P>::uh(k) : tweight<P>(k);
+}
+
 // Per-ordinate constants of the modal cell step (compute type T).
 template <int P, typename T>
 struct ModalOrdinate {
@@ -43,7 +79,7 @@ struct ModalOrdinate {
     T pp_re, pp_im_p, pp_im_m, pr_re, pr_im, rp_re, rp_im, rr_re;
 };
 
-template <int P, typename T>
+template <int P, typename T, bool ADJ = false>
 __device__ __forceinline__ ModalOrdinate<P, T> modal_ordinate(double axd, double ayd) {
     using Tab = ModalTable<P>;
     ModalOrdinate<P, T> o{};
@@ -51,8 +87,8 @@ __device__ __forceinline__ ModalOrdinate<P, T> modal_ordinate(double axd, double
     o.ay = T(ayd);
 #pragma unroll
     for (int k = 0; k < P; ++k) {
-        o.cx[k] = T(axd * Tab::uh(k));
-        o.cy[k] = T(ayd * Tab::uh(k));
+        o.cx[k] = T(axd * couple_w<P, ADJ>(k));
+        o.cy[k] = T(ayd * couple_w<P, ADJ>(k));
     }
     if constexpr (Tab::kPairs > 0) {
         o.pp_re = T((axd + ayd) * Tab::mu(0));
@@ -146,51 +182,49 @@ __device__ __forceinline__ ModalRecip<P, T> modal_recip(const ModalOrdinate<P, T
 
 // out(a,b) = sum_{d,e} Wp(a,d) sx^d Wp(b,e) sy^e v(d,e): packed modal coefficients of a (sign-flipped)
 // cell array.
-template <int P, bool XN, bool YN, typename T>
+template <int P, bool XN, bool YN, typename T, bool ADJ = false>
 __device__ __forceinline__ void modal_forward(T (&out)[P * P], const T (&v)[P * P]) {
-    using Tab = ModalTable<P>;
     T t[P * P];
 #pragma unroll
     for (int a = 0; a < P; ++a)
 #pragma unroll
         for (int e = 0; e < P; ++e) {
-            T acc = v[e] * T(Tab::W(a, 0));
+            T acc = v[e] * T(basis_w<P, ADJ>(a, 0));
 #pragma unroll
-            for (int d = 1; d < P; ++d) acc = fma(T(Tab::W(a, d) * flip_sign<XN>(d)), v[e + P * d], acc);
+            for (int d = 1; d < P; ++d) acc = fma(T(basis_w<P, ADJ>(a, d) * flip_sign<XN>(d)), v[e + P * d], acc);
             t[e + P * a] = acc;
         }
 #pragma unroll
     for (int a = 0; a < P; ++a)
 #pragma unroll
         for (int b = 0; b < P; ++b) {
-            T acc = t[P * a] * T(Tab::W(b, 0));
+            T acc = t[P * a] * T(basis_w<P, ADJ>(b, 0));
 #pragma unroll
-            for (int e = 1; e < P; ++e) acc = fma(T(Tab::W(b, e) * flip_sign<YN>(e)), t[e + P * a], acc);
+            for (int e = 1; e < P; ++e) acc = fma(T(basis_w<P, ADJ>(b, e) * flip_sign<YN>(e)), t[e + P * a], acc);
             out[b + P * a] = acc;
         }
 }
 
 // v(d,e) = sx^d sy^e sum_{a,b} Vp(d,a) Vp(e,b) Z(a,b): the cell array (unflipped) of modal coefficients.
-template <int P, bool XN, bool YN, typename T>
+template <int P, bool XN, bool YN, typename T, bool ADJ = false>
 __device__ __forceinline__ void modal_backward(T (&v)[P * P], const T (&Z)[P * P]) {
-    using Tab = ModalTable<P>;
-    T t[P * P];   // t(d, b) = sx^d sum_a Vp(d,a) Z(a,b)
+    T t[P * P];   // t(d, b) = sx^d sum_a Vb(d,a) Z(a,b)
 #pragma unroll
     for (int d = 0; d < P; ++d)
 #pragma unroll
         for (int b = 0; b < P; ++b) {
-            T acc = Z[b] * T(Tab::V(d, 0) * flip_sign<XN>(d));
+            T acc = Z[b] * T(basis_v<P, ADJ>(d, 0) * flip_sign<XN>(d));
 #pragma unroll
-            for (int a = 1; a < P; ++a) acc = fma(T(Tab::V(d, a) * flip_sign<XN>(d)), Z[b + P * a], acc);
+            for (int a = 1; a < P; ++a) acc = fma(T(basis_v<P, ADJ>(d, a) * flip_sign<XN>(d)), Z[b + P * a], acc);
             t[b + P * d] = acc;
         }
 #pragma unroll
     for (int d = 0; d < P; ++d)
 #pragma unroll
         for (int e = 0; e < P; ++e) {
-            T acc = t[P * d] * T(Tab::V(e, 0) * flip_sign<YN>(e));
+            T acc = t[P * d] * T(basis_v<P, ADJ>(e, 0) * flip_sign<YN>(e));
 #pragma unroll
-            for (int b = 1; b < P; ++b) acc = fma(T(Tab::V(e, b) * flip_sign<YN>(e)), t[b + P * d], acc);
+            for (int b = 1; b < P; ++b) acc = fma(T(basis_v<P, ADJ>(e, b) * flip_sign<YN>(e)), t[b + P * d], acc);
             v[e + P * d] = acc;
         }
 }
@@ -222,59 +256,63 @@ __device__ __forceinline__ void modal_block_solve(T (&Y)[P * P], const ModalReci
     if constexpr (Tab::kHasReal) Y[P * P - 1] *= r.rr;
 }
 
-// Trace weight of packed index k: column sums of Vp (1 for a pair's Re index and the real index).
-template <int P>
-__host__ __device__ constexpr bool trace_weight(int k) {
-    return !(k < 2 * ModalTable<P>::kPairs && (k & 1));
+// Sum of v[k] * w(k) over k with compile-time weights (zero weights skipped, unit weights added).
+template <int P, typename T, typename W>
+__device__ __forceinline__ T weighted_sum(const T *v, int stride, W w) {
+    T acc = T(0);
+    bool first = true;
+#pragma unroll
+    for (int k = 0; k < P; ++k) {
+        const double c = w(k);
+        if (c == 0.0) continue;
+        const T term = v[k * stride];
+        if (first)
+            acc = (c == 1.0) ? term : T(c) * term;
+        else
+            acc = (c == 1.0) ? acc + term : fma(T(c), term, acc);
+        first = false;
+    }
+    return acc;
 }
 
-// One modal cell step: Z from the cell's packed source S, the incoming packed traces fh (from the
-// x-upwind cell) and gh (from the y-upwind cell); then fh <- outgoing x trace, gh_out <- outgoing y trace.
-template <int P, typename T>
+// One modal cell step: Z from the cell's packed source S, the incoming packed traces fh (x-upwind cell)
+// and gh (y-upwind cell); then fh <- outgoing x trace, gh_out <- outgoing y trace.  Coupling terms with
+// a zero coupling weight are skipped at compile time.
+template <int P, typename T, bool ADJ = false>
 __device__ __forceinline__ void modal_step(T (&Z)[P * P], const T (&S)[P * P], T (&fh)[P], const T (&gh)[P],
                                            T (&gh_out)[P], const ModalOrdinate<P, T> &o, const ModalRecip<P, T> &r) {
 #pragma unroll
     for (int a = 0; a < P; ++a)
 #pragma unroll
-        for (int b = 0; b < P; ++b) Z[b + P * a] = fma(o.cx[a], fh[b], fma(o.cy[b], gh[a], S[b + P * a]));
+        for (int b = 0; b < P; ++b) {
+            T z = S[b + P * a];
+            if (couple_w<P, ADJ>(b) != 0.0) z = fma(o.cy[b], gh[a], z);
+            if (couple_w<P, ADJ>(a) != 0.0) z = fma(o.cx[a], fh[b], z);
+            Z[b + P * a] = z;
+        }
     modal_block_solve<P, T>(Z, r);
 #pragma unroll
-    for (int b = 0; b < P; ++b) {
-        T acc = T(0);
-        bool first = true;
+    for (int b = 0; b < P; ++b) fh[b] = weighted_sum<P, T>(Z + b, P, [](int k) { return trace_w<P, ADJ>(k); });
 #pragma unroll
-        for (int a = 0; a < P; ++a)
-            if (trace_weight<P>(a)) {
-                acc = first ? Z[b + P * a] : acc + Z[b + P * a];
-                first = false;
-            }
-        fh[b] = acc;
-    }
-#pragma unroll
-    for (int a = 0; a < P; ++a) {
-        T acc = T(0);
-        bool first = true;
-#pragma unroll
-        for (int b = 0; b < P; ++b)
-            if (trace_weight<P>(b)) {
-                acc = first ? Z[b + P * a] : acc + Z[b + P * a];
-                first = false;
-            }
-        gh_out[a] = acc;
-    }
+    for (int a = 0; a < P; ++a) gh_out[a] = weighted_sum<P, T>(Z + P * a, 1, [](int k) { return trace_w<P, ADJ>(k); });
 }
 
 // Physical-basis solve x = A'^-1 B (flipped, scaled frame) through the modal basis, in type T.
-template <int P, typename T>
+template <int P, typename T, bool ADJ = false>
 __device__ __forceinline__ void modal_solve_phys(T (&x)[P * P], const T (&B)[P * P], const ModalRecip<P, T> &r) {
     T Z[P * P];
-    modal_forward<P, false, false, T>(Z, B);
+    modal_forward<P, false, false, T, ADJ>(Z, B);
     modal_block_solve<P, T>(Z, r);
-    modal_backward<P, false, false, T>(x, Z);
+    modal_backward<P, false, false, T, ADJ>(x, Z);
 }
 
-// r = B - A' x in FP64, A' = ax (M (x) I) + ay (I (x) M) + s I, M(d,a) = (2d+1)(1 - 2[a < d, d - a odd]).
-template <int P>
+// Entry (d, a) of the 1-D upwind matrix M (xi > 0): (2d+1)(1 - 2[a < d, d - a odd]).
+__host__ __device__ constexpr double upwind_m(int d, int a) {
+    return (a < d && ((d - a) & 1)) ? -double(2 * d + 1) : double(2 * d + 1);
+}
+
+// r = B - A' x in FP64, A' = ax (M (x) I) + ay (I (x) M) + s I, or its transpose (ADJ).
+template <int P, bool ADJ = false>
 __device__ __forceinline__ void phys_residual(double (&res)[P * P], const double (&B)[P * P], const double (&x)[P * P],
                                               double ax, double ay, double s) {
 #pragma unroll
@@ -283,15 +321,9 @@ __device__ __forceinline__ void phys_residual(double (&res)[P * P], const double
         for (int e = 0; e < P; ++e) {
             double mx = 0.0, my = 0.0;
 #pragma unroll
-            for (int a = 0; a < P; ++a) {
-                const double c = (a < d && ((d - a) & 1)) ? -double(2 * d + 1) : double(2 * d + 1);
-                mx = fma(c, x[e + P * a], mx);
-            }
+            for (int a = 0; a < P; ++a) mx = fma(ADJ ? upwind_m(a, d) : upwind_m(d, a), x[e + P * a], mx);
 #pragma unroll
-            for (int b = 0; b < P; ++b) {
-                const double c = (b < e && ((e - b) & 1)) ? -double(2 * e + 1) : double(2 * e + 1);
-                my = fma(c, x[b + P * d], my);
-            }
+            for (int b = 0; b < P; ++b) my = fma(ADJ ? upwind_m(b, e) : upwind_m(e, b), x[b + P * d], my);
             res[e + P * d] = B[e + P * d] - fma(ax, mx, fma(ay, my, s * x[e + P * d]));
         }
 }

@@ -245,6 +245,54 @@ __global__ void dot_kernel(const double *__restrict__ x, const double *__restric
     }
 }
 
+
+// ---- adjoint helpers ----
+
+// y = x - sigma_s / (4 pi) * lam on interior cells, y = x on ghost cells: the adjoint Peierls operator
+// (I - S^T L^{-T} P^T) applied to x, given lam = sum_q (L^{-T} P^T x)_q.
+__global__ void adjoint_scatter_kernel(GridDims g, const double *__restrict__ sigma_s, const double *__restrict__ x,
+                                       const double *__restrict__ lam, double *__restrict__ y) {
+    const int N = g.P * g.P;
+    const size_t total = (size_t)(g.nx + 2) * (g.ny + 2) * N;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const size_t cidx = t / N;
+        const int i = (int)(cidx / (g.ny + 2)), j = (int)(cidx % (g.ny + 2));
+        const bool interior = i >= 1 && i <= g.nx && j >= 1 && j <= g.ny;
+        y[t] = interior ? x[t] - sigma_s[cidx] / (4.0 * M_PI) * lam[t] : x[t];
+    }
+}
+
+// Gradients of J = c . phi per interior cell (one warp per cell; the cell's nq*N values are contiguous):
+// dJ/dsigma_t = -sum_{q,k} lam psi, dJ/dsigma_s = sum_k Lam_k phi_k / (4 pi), dJ/dq_k = Lam_k / (4 pi),
+// with Lam = sum_q lam_q and q the isotropic source moments (angular source q / (4 pi)).
+__global__ void adjoint_gradient_kernel(GridDims g, const double *__restrict__ psi, const double *__restrict__ lam,
+                                        const double *__restrict__ phi, const double *__restrict__ Lam,
+                                        double *__restrict__ dsig_t, double *__restrict__ dsig_s, double *__restrict__ dq) {
+    const int N = g.P * g.P;
+    const int lane = threadIdx.x & 31;
+    const size_t warps = (size_t)gridDim.x * (blockDim.x / 32);
+    const size_t cells = (size_t)g.nx * g.ny;
+    for (size_t c = blockIdx.x * (size_t)(blockDim.x / 32) + (threadIdx.x >> 5); c < cells; c += warps) {
+        const int i = 1 + (int)(c / g.ny), j = 1 + (int)(c % g.ny);
+        const size_t cidx = (size_t)i * (g.ny + 2) + j;
+        const size_t base = cidx * (size_t)g.nq * N;
+        double acc = 0.0;
+        for (int t = lane; t < g.nq * N; t += 32) acc = fma(lam[base + t], psi[base + t], acc);
+        for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+        double accs = 0.0;
+        if (lane < N) {
+            const double L = Lam[cidx * N + lane];
+            accs = L * phi[cidx * N + lane];
+            if (dq) dq[cidx * N + lane] = L / (4.0 * M_PI);
+        }
+        for (int off = 16; off > 0; off >>= 1) accs += __shfl_xor_sync(0xffffffffu, accs, off);
+        if (lane == 0) {
+            if (dsig_t) dsig_t[cidx] = -acc;
+            if (dsig_s) dsig_s[cidx] = accs / (4.0 * M_PI);
+        }
+    }
+}
+
 }  // namespace
 
 cudaError_t launch_multidot(const double *V, int nv, size_t ld, const double *w, size_t n, double *out,
@@ -328,6 +376,20 @@ cudaError_t launch_l2dist2(const GridDims &g, const double *a, const double *b, 
     int blocks = blocks_for(n);
     if (blocks > 148 * 4) blocks = 148 * 4;
     l2dist2_kernel<<<blocks, kThreads, 0, s>>>(g, a, b, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adjoint_scatter(const GridDims &g, const double *sigma_s, const double *x, const double *lam,
+                                   double *y, cudaStream_t s) {
+    const size_t n = (size_t)(g.nx + 2) * (g.ny + 2) * g.P * g.P;
+    adjoint_scatter_kernel<<<blocks_for(n), kThreads, 0, s>>>(g, sigma_s, x, lam, y);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adjoint_gradient(const GridDims &g, const double *psi, const double *lam, const double *phi,
+                                    const double *Lam, double *dsig_t, double *dsig_s, double *dq, cudaStream_t s) {
+    const size_t warps = (size_t)g.nx * g.ny;
+    adjoint_gradient_kernel<<<blocks_for(warps * 32), kThreads, 0, s>>>(g, psi, lam, phi, Lam, dsig_t, dsig_s, dq);
     return cudaGetLastError();
 }
 

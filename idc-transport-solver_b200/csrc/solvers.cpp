@@ -50,19 +50,17 @@ Status Context::apply_peierls(const double *x, double *y, double *tmp_phi, doubl
     return Status::ok();
 }
 
-// GMRES(restart) from a zero initial guess on (I - P L^{-1} S) phi = P L^{-1} Q, stopping when the
-// residual 2-norm (the Arnoldi estimate, as PETSc reports it) is <= abs_tol, then
-// psi = L^{-1}(S phi + Q).  Classical Gram-Schmidt with one re-orthogonalisation pass (CGS2), Givens
-// rotations on the host.  PETSc's LGMRES adds error-approximation vectors to the restart; it converges
-// to the same fixed point, so iteration counts may differ but the solution does not.
-Status Context::gmres_peierls(const double *src, double *psi_out, double dt, double abs_tol, int restart,
-                              int64_t max_its, int precision, int64_t *iters_out, double *resid_out) {
-    if (!use_warp_kernel) return bad(IDC_ERR_UNSUPPORTED, "GMRES needs the warp-pipelined sweep kernel");
+// GMRES(restart) from a zero initial guess on A x = b (moment-sized vectors), stopping when the residual
+// 2-norm (the Arnoldi estimate, as PETSc reports it) is <= abs_tol.  Classical Gram-Schmidt with one
+// re-orthogonalisation pass (CGS2), Givens rotations on the host, restarts from the true residual.
+// PETSc's LGMRES adds error-approximation vectors to the restart; it converges to the same solution, so
+// iteration counts may differ but the solution does not.
+template <typename Op>
+Status Context::gmres(Op apply, const double *b, double *x, double abs_tol, int restart, int64_t max_its,
+                      int64_t *iters_out, double *resid_out, bool *converged_out) {
     if (restart < 1 || restart > 60) return bad(IDC_ERR_ARG, "gmres restart must be in 1..60");
     const size_t n = phi_len();
     const int m = restart;
-    IDC_TRY(ensure_phi_buffers(6));
-    double *b = phi_buf(3), *x = phi_buf(4), *tmp = phi_buf(5);
     if (krylov_len < (size_t)(m + 1) * n) {
         cudaFree(d_krylov);
         d_krylov = nullptr;
@@ -74,10 +72,7 @@ Status Context::gmres_peierls(const double *src, double *psi_out, double dt, dou
     double *V = d_krylov;
     auto Vc = [&](int k) { return V + (size_t)k * n; };
 
-    // right-hand side b = P L^{-1} Q (PETScPeierlsSolver.cpp:461-466)
-    IDC_TRY(sweep(src, nullptr, dt, b, precision));
     IDC_TRY_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, stream));
-
     // r = b - A x = b for the zero initial guess
     IDC_TRY_CUDA(cudaMemcpyAsync(Vc(0), b, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream));
     double beta = 0.0;
@@ -94,7 +89,7 @@ Status Context::gmres_peierls(const double *src, double *psi_out, double dt, dou
         g[0] = beta;
         int k = 0;   // columns built in this cycle
         for (int j = 0; j < m && its < max_its; ++j) {
-            IDC_TRY(apply_peierls(Vc(j), Vc(j + 1), tmp, dt, precision));
+            IDC_TRY(apply(Vc(j), Vc(j + 1)));
             // CGS2: h = V^T w, w -= V h, twice
             IDC_TRY_CUDA(launch_multidot(V, j + 1, n, Vc(j + 1), n, d_small, stream));
             IDC_TRY_CUDA(cudaMemcpyAsync(h.data(), d_small, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost, stream));
@@ -148,7 +143,7 @@ Status Context::gmres_peierls(const double *src, double *psi_out, double dt, dou
             break;
         }
         // restart from the true residual r = b - A x
-        IDC_TRY(apply_peierls(x, Vc(0), tmp, dt, precision));
+        IDC_TRY(apply(x, Vc(0)));
         IDC_TRY_CUDA(launch_axpby(1.0, b, -1.0, Vc(0), n, stream));
         launches += 1;
         IDC_TRY(dot_host(Vc(0), Vc(0), n, &beta));
@@ -157,14 +152,78 @@ Status Context::gmres_peierls(const double *src, double *psi_out, double dt, dou
         converged = resid <= abs_tol;
         if (beta == 0.0) break;
     }
+    if (iters_out) *iters_out = its;
+    if (resid_out) *resid_out = resid;
+    if (converged_out) *converged_out = converged;
+    return Status::ok();
+}
+
+// (I - P L^{-1} S) phi = P L^{-1} Q (PETScPeierlsSolver.cpp:423-572), then psi = L^{-1}(S phi + Q).
+Status Context::gmres_peierls(const double *src, double *psi_out, double dt, double abs_tol, int restart,
+                              int64_t max_its, int precision, int64_t *iters_out, double *resid_out) {
+    if (!use_warp_kernel) return bad(IDC_ERR_UNSUPPORTED, "GMRES needs the warp-pipelined sweep kernel");
+    IDC_TRY(ensure_phi_buffers(6));
+    double *b = phi_buf(3), *x = phi_buf(4), *tmp = phi_buf(5);
+    // right-hand side b = P L^{-1} Q (PETScPeierlsSolver.cpp:461-466)
+    IDC_TRY(sweep(src, nullptr, dt, b, precision));
+    bool converged = false;
+    double resid = 0.0;
+    auto op = [&](const double *in, double *out) { return apply_peierls(in, out, tmp, dt, precision); };
+    IDC_TRY(gmres(op, b, x, abs_tol, restart, max_its, iters_out, &resid, &converged));
     // psi = L^{-1} (S phi + Q)  (PETScPeierlsSolver.cpp:504-505)
     IDC_TRY(sweep(src, psi_out, dt, nullptr, precision, x, 1.0));
     IDC_TRY(check_device_error());
-    if (iters_out) *iters_out = its;
     if (resid_out) *resid_out = resid;
     if (!converged)
         return bad(IDC_ERR_NOT_CONVERGED, "GMRES transport solve failed to converge (max_its reached, residual " +
                                               std::to_string(resid) + ")");
+    return Status::ok();
+}
+
+// y = x - S^T L^{-T} P^T x: one transposed sweep with the fused source w_q x, no psi stored, the unweighted
+// moment sums scaled by sigma_s / (4 pi).
+Status Context::apply_peierls_adjoint(const double *x, double *y, double *tmp_phi, double dt, int precision) {
+    IDC_TRY(sweep(nullptr, nullptr, dt, tmp_phi, precision, x, 1.0, true));
+    IDC_TRY_CUDA(launch_adjoint_scatter(dims(), d_sigma_s, x, tmp_phi, y, stream));
+    launches += 1;
+    return Status::ok();
+}
+
+// The discrete adjoint of the steady (or implicit-step) transport problem F = L' psi - Q - S P psi = 0
+// with the functional J = c . P psi: (L' - S P)^T lam = P^T c.  With mu = c + S^T lam the equation reads
+// (I - S^T L'^{-T} P^T) mu = c (GMRES), then lam = L'^{-T} P^T mu (one more transposed sweep).
+// lam_out (psi-sized, nullable) and Lam_out = sum_q lam_q (moment-sized) are device arrays.
+Status Context::adjoint_solve(const double *detector, double *lam_out, double *Lam_out, double dt, double abs_tol,
+                              int restart, int64_t max_its, int precision, int64_t *iters, double *resid_out) {
+    if (kernel != kModal) return bad(IDC_ERR_UNSUPPORTED, "the adjoint needs the modal sweep kernel");
+    IDC_TRY(ensure_phi_buffers(8));
+    double *mu = phi_buf(6), *tmp = phi_buf(7);
+    bool converged = false;
+    double resid = 0.0;
+    auto op = [&](const double *in, double *out) { return apply_peierls_adjoint(in, out, tmp, dt, precision); };
+    IDC_TRY(gmres(op, detector, mu, abs_tol, restart, max_its, iters, &resid, &converged));
+    IDC_TRY(sweep(nullptr, lam_out, dt, Lam_out, precision, mu, 1.0, true));
+    IDC_TRY(check_device_error());
+    if (resid_out) *resid_out = resid;
+    if (!converged)
+        return bad(IDC_ERR_NOT_CONVERGED, "adjoint GMRES failed to converge (max_its reached, residual " +
+                                              std::to_string(resid) + ")");
+    return Status::ok();
+}
+
+Status Context::adjoint_gradient(const double *psi, const double *detector, double dt, double abs_tol, int restart,
+                                 int64_t max_its, int precision, double *dsig_t, double *dsig_s, double *dq,
+                                 int64_t *iters, double *resid) {
+    IDC_TRY(ensure_psi_buffers(1));
+    IDC_TRY(ensure_phi_buffers(10));
+    double *lam = psi_buf(0), *Lam = phi_buf(8), *phi = phi_buf(9);
+    IDC_TRY(adjoint_solve(detector, lam, Lam, dt, abs_tol, restart, max_its, precision, iters, resid));
+    IDC_TRY(pmv(1.0, 0.0, psi, phi));
+    if (dsig_t) IDC_TRY_CUDA(cudaMemsetAsync(dsig_t, 0, sizeof(double) * sig_len(), stream));
+    if (dsig_s) IDC_TRY_CUDA(cudaMemsetAsync(dsig_s, 0, sizeof(double) * sig_len(), stream));
+    if (dq) IDC_TRY_CUDA(cudaMemsetAsync(dq, 0, sizeof(double) * phi_len(), stream));
+    IDC_TRY_CUDA(launch_adjoint_gradient(dims(), psi, lam, phi, Lam, dsig_t, dsig_s, dq, stream));
+    launches += 1;
     return Status::ok();
 }
 

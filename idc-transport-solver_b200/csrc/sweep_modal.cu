@@ -1,477 +1,20 @@
-// Modal persistent wavefront sweep for sm_100a.
-//
-// Replaces SweepPatternUniCartWavefront::Sweep (linear_solvers/Abstract/SweepPattern/
-// SweepPatternUniCartWavefront.cpp:121-332) with the per-cell CalcB / CalcA / GE / StoreResult of
-// SweepCellSolveBase::ConstructAndSolve (linear_solvers/RKDG/SweepCellSolve/SweepCellSolve.hpp:312-353),
-// solving each (cell, ordinate) system in the packed modal basis of modal_cell.cuh.  What travels from
-// a cell to its downwind neighbours is its face trace (P values per ordinate and face), not its N dofs.
-//
-//   * a compute warp owns Rw = 32/seg consecutive rows; lane (rr, o) = (lane / seg, lane % seg) owns
-//     ordinate q_begin + o on row rr.  Row rr runs one column behind row rr-1; its y trace is row rr-1's
-//     outgoing trace of the previous step, moved by __shfl_up.  The x trace stays in the lane.
-//   * the Wn compute warps of a CTA are stacked in y; warp w's last row hands its outgoing y traces to
-//     warp w+1 through a ring of kWarpRingSlots shared-memory slots guarded by full/empty mbarriers.
-//   * between CTAs: the CTA's last warp writes its last row's traces, column by column, into the item's
-//     trace buffer with relaxed stores, and the helper warp of the item below polls the values
-//     themselves (a slot holds a NaN-payload sentinel that arithmetic never produces; 8-byte accesses
-//     are single-copy atomic), copies ready columns into ring 0 and re-arms the slots.  The first row
-//     block's helper copies the inflow traces of the ghost row (inflow_traces_kernel) instead.
-//   * each lane prefetches its next cells' source with cp.async (lane o == 0 of a row also sigma_t and
-//     the fused scattering source), prefetch_depth(P) cells ahead, into a per-warp stage ring.
-//   * the loop over columns is instantiated per quadrant, so the quadrant's sign flips are constants.
-//   * the fused moments phi = sum_q w_q psi_q: a row segment's weighted values meet in shared memory and
-//     one partial moment per (cell, dof, ordinate chunk) is stored; reduce_phi_partials (ops_kernels.cu)
-//     adds the chunks in a fixed order, so phi is bitwise reproducible.
-//
-// Precision: MODE 0 computes in FP64.  MODE 2 computes the modal step in FP32 (traces in FP32).
-// MODE 1 keeps FP64 physical traces and right-hand sides and solves each cell by FP32 modal solves
-// with FP64 residual corrections (iterative refinement per cell).
-//
-// Work items (row blocks x quadrant x ordinate chunk) are dequeued in row-block order from an atomic
-// counter, so every item's producer is held by a CTA that is already running.  Every wait (mbarrier or
-// trace poll) is bounded; on expiry the warp records kDevTimeout in the device error word and leaves,
-// and every other warp leaves as soon as it sees the word.  After an error the trace buffer may hold
-// values instead of sentinels; the host re-arms it before the next sweep.
-#include "device_sync.cuh"
-#include "idc_internal.hpp"
-#include "modal_cell.cuh"
+// Modal sweep: host-side dispatch over degree, precision, row-segment width and direction, the shared-
+// memory size, and the inflow-trace kernel.  The kernels are in sweep_modal_impl.cuh.
+#include "sweep_modal_impl.cuh"
 
-#include <cstdint>
-#include <type_traits>
+IDC_MODAL_LAUNCHERS(extern, 0, false)
+IDC_MODAL_LAUNCHERS(extern, 0, true)
+IDC_MODAL_LAUNCHERS(extern, 1, false)
+IDC_MODAL_LAUNCHERS(extern, 1, true)
+IDC_MODAL_LAUNCHERS(extern, 2, false)
 
 namespace idc {
 
 namespace {
 
-constexpr int kS = kWarpRingSlots;
-constexpr int kMaxWarps = 8;   // up to 7 compute warps + 1 helper
-
-__device__ __forceinline__ int T_steps(int nx, int Rw) { return nx + Rw - 1; }
-
-// Source prefetch depth (cells ahead per lane) within the shared-memory budget.
-__host__ __device__ constexpr int prefetch_depth(int P) { return P == 3 ? 4 : 8; }
-
-struct Layout {
-    uint64_t *full, *empty;   // [Wn+1][kS]
-    double *ring;             // [Wn+1][kS][G][P]: y traces
-    double *src;              // [Wn][D][32][N]: each lane's cell source dofs
-    double *cellst;           // [Wn][D][32/seg][N+2]: per row: sigma_t, sigma_s, phi_scatter[N]
-    double *w;                // [G]
-    double *red;              // [2][Wn][32][N]: per-lane weighted values for the moment reduction
-};
-
-__device__ __forceinline__ Layout carve(unsigned char *raw, int wn, int G, int P, int D, int rw) {
-    const int N = P * P;
-    Layout L;
-    L.full = reinterpret_cast<uint64_t *>(raw);
-    L.empty = L.full + (wn + 1) * kS;
-    L.ring = reinterpret_cast<double *>(L.empty + (wn + 1) * kS);
-    L.src = L.ring + (size_t)(wn + 1) * kS * G * P;
-    L.cellst = L.src + (size_t)wn * D * 32 * N;
-    L.w = L.cellst + (size_t)wn * D * rw * (N + 2);
-    L.red = L.w + ((G + 1) & ~1);
-    return L;
-}
-
-// Inputs of one cell step prepared ahead of the step.  MODE 0 / 2: packed modal source and reciprocal
-// denominators.  MODE 1: the sign-flipped physical source, FP32 reciprocals and s = sigma_t + 1/dt.
-template <int P, int MODE>
-struct CellIn {
-    using TS = std::conditional_t<MODE == 0, double, float>;
-    std::conditional_t<MODE == 1, double, TS> v[P * P];
-    ModalRecip<P, TS> r;
-    double s;
-};
-
-template <int P, int MODE, bool XN, bool YN>
-__device__ __forceinline__ void prep_cell(CellIn<P, MODE> &in, const double *sp, const double *cp, const SweepArgs &a,
-                                          const ModalOrdinate<P, typename CellIn<P, MODE>::TS> &od) {
-    constexpr int N = P * P;
-    using TS = typename CellIn<P, MODE>::TS;
-    double src[N];
-#pragma unroll
-    for (int k = 0; k < N; ++k) src[k] = a.src ? sp[k] : 0.0;
-    if (a.phi_scatter) {   // fused TransportOperator::Smv(scale, 1, sigma_s, phi -> src)
-        const double sv = cp[1];
-#pragma unroll
-        for (int k = 0; k < N; ++k) src[k] += a.scatter_scale * (sv * cp[2 + k] / (4.0 * M_PI));
-    }
-    in.s = cp[0] + a.inv_dt;
-    in.r = modal_recip<P, TS>(od, TS(in.s));
-    if constexpr (MODE != 1) {
-        TS v[N];
-#pragma unroll
-        for (int k = 0; k < N; ++k) v[k] = TS(src[k]);
-        modal_forward<P, XN, YN, TS>(in.v, v);
-    } else {
-#pragma unroll
-        for (int d = 0; d < P; ++d)
-#pragma unroll
-            for (int e = 0; e < P; ++e) in.v[e + P * d] = flip_sign<XN>(d) * flip_sign<YN>(e) * src[e + P * d];
-    }
-}
-
-// MODE 1 cell step in the flipped physical frame: B = src' + ax u (x) f + ay g (x) u in FP64, solved by an
-// FP32 modal solve and n_refine FP64 residual corrections; f <- outgoing x trace, g_out <- outgoing y trace.
-template <int P>
-__device__ __forceinline__ void refined_step(double (&xp)[P * P], const CellIn<P, 1> &in, double (&f)[P],
-                                             const double (&g)[P], double (&g_out)[P], double axd, double ayd,
-                                             int n_refine) {
-    constexpr int N = P * P;
-    double B[N], res[N];
-    float bf[N], xf[N];
-#pragma unroll
-    for (int d = 0; d < P; ++d)
-#pragma unroll
-        for (int e = 0; e < P; ++e) {
-            const double ud = (d & 1) ? -double(2 * d + 1) : double(2 * d + 1);
-            const double ue = (e & 1) ? -double(2 * e + 1) : double(2 * e + 1);
-            B[e + P * d] = fma(axd * ud, f[e], fma(ayd * ue, g[d], in.v[e + P * d]));
-        }
-#pragma unroll
-    for (int k = 0; k < N; ++k) bf[k] = float(B[k]);
-    modal_solve_phys<P, float>(xf, bf, in.r);
-#pragma unroll
-    for (int k = 0; k < N; ++k) xp[k] = double(xf[k]);
-    for (int it = 0; it < n_refine; ++it) {
-        phys_residual<P>(res, B, xp, axd, ayd, in.s);
-#pragma unroll
-        for (int k = 0; k < N; ++k) bf[k] = float(res[k]);
-        modal_solve_phys<P, float>(xf, bf, in.r);
-#pragma unroll
-        for (int k = 0; k < N; ++k) xp[k] += double(xf[k]);
-    }
-#pragma unroll
-    for (int e = 0; e < P; ++e) {
-        double acc = xp[e];
-#pragma unroll
-        for (int d = 1; d < P; ++d) acc += xp[e + P * d];
-        f[e] = acc;
-    }
-#pragma unroll
-    for (int d = 0; d < P; ++d) {
-        double acc = xp[P * d];
-#pragma unroll
-        for (int e = 1; e < P; ++e) acc += xp[e + P * d];
-        g_out[d] = acc;
-    }
-}
-
-// Compute warp.  Per column step s the loop runs: receive the y trace, the cell step (the only part on
-// the cell-to-cell dependency chain), send the outgoing y trace, then prepare the next cell (modal
-// source, reciprocals) and finish this one (cell dofs, psi store, moments), whose instructions fill the
-// step's latency.  Lanes without a cell this step compute on stale stage data and store nothing.
-template <int P, int MODE, int SEG, bool XN, bool YN>
-__device__ __forceinline__ void modal_rows(const SweepArgs &a, const SweepItem &item, const Layout &L, int w,
-                                           int lane, bool has_consumer, int it_index) {
-    constexpr int N = P * P;
-    using TS = std::conditional_t<MODE == 0, double, float>;   // modal solve type
-    using TR = std::conditional_t<MODE == 2, float, double>;   // trace type
-    using TZ = std::conditional_t<MODE == 1, double, TS>;      // step result (modal Z, or MODE 1 dofs)
-    constexpr int seg = SEG, Rw = 32 / SEG;
-    const int G = a.G, rows_cta = a.wn * Rw;
-    const int rr = lane / seg, o = lane - rr * seg;
-    const int row_w = item.row_block * rows_cta + w * Rw;   // the warp's first row in sweep order
-    const int row = row_w + rr;
-    const bool row_valid = row < a.ny;
-    const bool act = (o < item.q_count) && row_valid;
-    const int q = item.q_begin + (act ? o : 0);
-    const int j = YN ? (a.ny - row) : (1 + row);
-    const size_t plane = (size_t)a.nq * N;
-    const size_t istride = (size_t)(a.ny + 2) * plane;
-    const bool last_warp = w == a.wn - 1;
-
-    double axd = 0.0, ayd = 0.0, wq = 0.0;
-    TR f[P];   // x trace (modal, or physical in MODE 1) entering the next cell of this row
-#pragma unroll
-    for (int m = 0; m < P; ++m) f[m] = TR(0);
-    if (act) {
-        axd = fabs(a.xi[q]) / a.dx;
-        ayd = fabs(a.eta[q]) / a.dy;
-        wq = L.w[o];
-        if (a.inflow) {
-            const double *in = a.inflow + ((size_t)(a.nx + row) * a.nq + q) * P;
-#pragma unroll
-            for (int m = 0; m < P; ++m) f[m] = TR(in[m]);
-        }
-    }
-    const ModalOrdinate<P, TS> od = modal_ordinate<P, TS>(axd, ayd);
-    TR gprev[P];   // this lane's outgoing y trace of the previous step
-#pragma unroll
-    for (int m = 0; m < P; ++m) gprev[m] = TR(0);
-
-    constexpr int D = prefetch_depth(P);
-    constexpr int NC = N + 2;
-    const int phi_slot = a.phi_slots > 0 ? it_index % a.phi_slots : 0;
-    double *my_src = L.src + ((size_t)w * D * 32 + lane) * N;     // stage b at + b*32*N
-    double *my_cell = L.cellst + ((size_t)w * D * Rw + rr) * NC;  // stage b at + b*Rw*NC
-
-    // One cp.async group per step (possibly empty), D - 1 steps in flight ahead of the current one.
-    auto prefetch = [&](int s) {
-        const int c = s - rr;
-        if (s < T_steps(a.nx, Rw) && row_valid && c >= 0 && c < a.nx) {
-            const int i = XN ? a.nx - c : 1 + c;
-            if (act && a.src) {
-                const double *g = a.src + (size_t)i * istride + (size_t)j * plane + (size_t)q * N;
-                double *d = my_src + (size_t)(s % D) * 32 * N;
-#pragma unroll
-                for (int k = 0; k < N; ++k) cp_async8(d + k, g + k);
-            }
-            if (o == 0) {
-                const size_t cidx = (size_t)i * (a.ny + 2) + j;
-                double *d = my_cell + (size_t)(s % D) * Rw * NC;
-                cp_async8(d, a.sigma_t + cidx);
-                if (a.phi_scatter) {
-                    cp_async8(d + 1, a.sigma_s + cidx);
-#pragma unroll
-                    for (int k = 0; k < N; ++k) cp_async8(d + 2 + k, a.phi_scatter + cidx * N + k);
-                }
-            }
-        }
-        cp_commit();
-    };
-
-    const int T = T_steps(a.nx, Rw);
-#pragma unroll
-    for (int s = 0; s < D - 1; ++s) prefetch(s);
-    CellIn<P, MODE> cur;
-    cp_wait<D - 2>();
-    __syncwarp();
-    prep_cell<P, MODE, XN, YN>(cur, my_src, my_cell, a, od);
-
-    for (int s = 0; s < T; ++s) {
-        prefetch(s + D - 1);
-        cp_wait<D - 2>();   // stage s + 1 has landed
-        __syncwarp();       // lane o == 0's cell-data copies are visible to its row segment
-        const int c = s - rr;
-        const bool valid = act && c >= 0 && c < a.nx;
-
-        // y trace: rows rr > 0 from the lane seg below in the warp (previous step), row 0 from the ring
-        TR g[P];
-#pragma unroll
-        for (int m = 0; m < P; ++m) g[m] = __shfl_up_sync(kFullMask, gprev[m], seg);
-        if (s < a.nx) {   // warp-uniform: row 0 needs column s
-            const int slot = s % kS;
-            if (!mbar_wait(L.full + w * kS + slot, (uint32_t)((s / kS) & 1), a.error, a.spin_limit)) break;
-            if (rr == 0 && o < G) {
-                const double *rp = L.ring + (((size_t)w * kS + slot) * G + o) * P;
-#pragma unroll
-                for (int m = 0; m < P; ++m) g[m] = TR(rp[m]);
-            }
-            __syncwarp();
-            mbar_arrive(L.empty + w * kS + slot);
-        }
-
-        // the cell step: the dependency chain from cell to cell
-        TZ Z[N];
-        TR fn[P], gout[P];
-#pragma unroll
-        for (int m = 0; m < P; ++m) fn[m] = f[m];
-        if constexpr (MODE != 1)
-            modal_step<P, TS>(Z, cur.v, fn, g, gout, od, cur.r);
-        else
-            refined_step<P>(Z, cur, fn, g, gout, axd, ayd, a.n_refine);
-#pragma unroll
-        for (int m = 0; m < P; ++m) {
-            f[m] = valid ? fn[m] : f[m];
-            gout[m] = valid ? gout[m] : TR(0);
-            gprev[m] = gout[m];
-        }
-
-        // last row (column s - (Rw-1)): its y traces to ring w+1, or, from the CTA's last warp, to the
-        // item's trace buffer that the item below polls (relaxed stores, no fence: each value is its flag)
-        const int cout = s - (Rw - 1);
-        if (last_warp) {
-            if (has_consumer && rr == Rw - 1 && o < item.q_count && cout >= 0 && cout < a.nx) {
-                double *tp = a.trace + (size_t)it_index * a.trace_stride + ((size_t)cout * G + o) * P;
-#pragma unroll
-                for (int m = 0; m < P; ++m) st_relaxed_f64(tp + m, double(gout[m]));
-            }
-        } else if (cout >= 0 && cout < a.nx) {   // warp-uniform
-            const int slot = cout % kS;
-            uint64_t *emp = L.empty + (w + 1) * kS + slot;
-            if (!mbar_wait(emp, (uint32_t)(((cout / kS) & 1) ^ 1), a.error, a.spin_limit)) break;
-            if (rr == Rw - 1 && o < G) {
-                double *rp = L.ring + (((size_t)(w + 1) * kS + slot) * G + o) * P;
-#pragma unroll
-                for (int m = 0; m < P; ++m) rp[m] = double(gout[m]);
-            }
-            __syncwarp();
-            mbar_arrive(L.full + (w + 1) * kS + slot);
-        }
-
-        // next cell's inputs (stage s + 1; stale for lanes without a next cell, never stored)
-        prep_cell<P, MODE, XN, YN>(cur, my_src + (size_t)((s + 1) % D) * 32 * N,
-                                   my_cell + (size_t)((s + 1) % D) * Rw * NC, a, od);
-
-        // this cell's dofs, psi and moments
-        double x[N];
-        if constexpr (MODE != 1) {
-            TS xv[N];
-            modal_backward<P, XN, YN, TS>(xv, Z);
-#pragma unroll
-            for (int k = 0; k < N; ++k) x[k] = double(xv[k]);
-        } else {
-#pragma unroll
-            for (int d = 0; d < P; ++d)
-#pragma unroll
-                for (int e = 0; e < P; ++e) x[e + P * d] = flip_sign<XN>(d) * flip_sign<YN>(e) * Z[e + P * d];
-        }
-        const size_t cell = (size_t)(XN ? a.nx - c : 1 + c) * istride + (size_t)j * plane + (size_t)q * N;
-        if (a.out && valid) {
-            double *op = a.out + cell;
-#pragma unroll
-            for (int k = 0; k < N; ++k) op[k] = x[k];
-        }
-        // moments: the warp's weighted values meet in shared memory (two buffers by step parity, so one
-        // __syncwarp per step orders the writes against the previous step's reads); the warp's Rw x N
-        // (row, dof) sums over each row segment's ordinates are spread over the lanes, each a fixed
-        // pairwise tree, and stored into this chunk's partial moments
-        if (a.phi_part) {
-            double *red = L.red + ((size_t)(s & 1) * a.wn + w) * 32 * N;
-#pragma unroll
-            for (int k = 0; k < N; ++k) red[lane * N + k] = valid ? wq * x[k] : 0.0;
-            __syncwarp();
-            constexpr int kSums = Rw * N;
-#pragma unroll
-            for (int m = 0; m < (kSums + 31) / 32; ++m) {
-                const int t = lane + 32 * m;
-                const int r2 = t / N, k = t - (t / N) * N;
-                const int c2 = s - r2, row2 = row_w + r2;
-                if (t < kSums && row2 < a.ny && c2 >= 0 && c2 < a.nx) {
-                    const double *sr = red + (size_t)r2 * SEG * N + k;
-                    double v[SEG];
-#pragma unroll
-                    for (int oo = 0; oo < SEG; ++oo) v[oo] = sr[oo * N];
-#pragma unroll
-                    for (int h = 1; h < SEG; h <<= 1)
-#pragma unroll
-                        for (int oo = 0; oo < SEG; oo += 2 * h) v[oo] += v[oo + h];
-                    const int i2 = XN ? a.nx - c2 : 1 + c2, j2 = YN ? (a.ny - row2) : (1 + row2);
-                    a.phi_part[(size_t)phi_slot * a.phi_slot_stride + ((size_t)i2 * (a.ny + 2) + j2) * N + k] = v[0];
-                }
-            }
-        }
-    }
-    cp_wait<0>();
-}
-
-// Helper warp: feeds ring 0 with the y traces entering the item's first row -- the ghost row's inflow
-// traces for the first row block, otherwise the traces the item above writes column by column (ready
-// when none of a column's values is the sentinel; the helper writes the sentinel back for the next
-// sweep).  The helper blocks in the barrier unit until the ring slot of its next column is free, then
-// loads that column and every further column with a free slot (up to kS): lane l holds values
-// l, l + 32, l + 64 of each column, all loads issued before any value is used.
-template <int P>
-__device__ void modal_helper(const SweepArgs &a, const SweepItem &item, const Layout &L, int lane) {
-    constexpr int kV = (32 * P + 31) / 32;   // values per lane and column: chunk <= 32 P
-    const int G = a.G;
-    const bool has_dep = item.dep >= 0;
-    const int chunk = item.q_count * P;   // values per column
-    const size_t col_stride = has_dep ? (size_t)G * P : (size_t)a.nq * P;
-    double *trace = has_dep ? a.trace + (size_t)item.dep * a.trace_stride : nullptr;
-    const double *src = has_dep ? trace : (a.inflow ? a.inflow + (size_t)item.q_begin * P : nullptr);
-
-    int fetch = 0;
-    long long idle = 0;
-    while (fetch < a.nx) {
-        // block (bounded, in the barrier unit) until the slot of column `fetch` is free, then count the
-        // free slots after it without blocking
-        if (!mbar_wait(L.empty + fetch % kS, (uint32_t)(((fetch / kS) & 1) ^ 1), a.error, a.spin_limit)) break;
-        int n = 1;
-        if (lane == 0)
-            while (n < kS && fetch + n < a.nx &&
-                   mbar_test(L.empty + (fetch + n) % kS, (uint32_t)((((fetch + n) / kS) & 1) ^ 1)))
-                ++n;
-        n = __shfl_sync(kFullMask, n, 0);
-
-        double v[kS][kV];
-        unsigned col_ok = (1u << n) - 1u;   // bit t: column fetch + t complete in this lane
-#pragma unroll
-        for (int t = 0; t < kS; ++t)
-#pragma unroll
-            for (int k = 0; k < kV; ++k) {
-                const int e = lane + 32 * k;
-                v[t][k] = 0.0;
-                if (t < n && e < chunk && src) {
-                    const double *p = src + (size_t)(fetch + t) * col_stride + e;
-                    if (has_dep) {
-                        v[t][k] = ld_relaxed_f64(p);
-                        if (is_sentinel(v[t][k])) col_ok &= ~(1u << t);
-                    } else {
-                        v[t][k] = *p;
-                    }
-                }
-            }
-        // leading columns that every lane has complete
-        const unsigned all_ok = __reduce_and_sync(kFullMask, col_ok);
-        int ready = __ffs(~all_ok) - 1;
-        if (ready < 0 || ready > n) ready = n;
-#pragma unroll
-        for (int t = 0; t < kS; ++t)
-#pragma unroll
-            for (int k = 0; k < kV; ++k) {
-                const int e = lane + 32 * k;
-                if (t < ready && e < chunk) {
-                    L.ring[(size_t)((fetch + t) % kS) * G * P + e] = v[t][k];
-                    if (has_dep) st_relaxed_f64(trace + (size_t)(fetch + t) * col_stride + e, sentinel_value());
-                }
-            }
-        if (ready > 0) {
-            __syncwarp();
-            for (int t = 0; t < ready; ++t) mbar_arrive(L.full + (fetch + t) % kS);
-            fetch += ready;
-        } else {   // the item above has not written column `fetch` yet: poll again (each poll is an L2
-                   // round trip), bounded
-            if (((++idle) & 63) == 0 && ld_relaxed(a.error) != kDevOk) break;
-            if (idle > a.spin_limit) {
-                if (lane == 0) atomicCAS(a.error, kDevOk, kDevTimeout);
-                break;
-            }
-        }
-    }
-}
-
-template <int P, int MODE, int SEG>
-__global__ void __launch_bounds__(kMaxWarps * 32, 1) sweep_modal_kernel(const SweepArgs a) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ int s_item;
-    __shared__ int s_stop;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const Layout L = carve(smem_raw, a.wn, a.G, P, prefetch_depth(P), 32 / SEG);
-    const int rows_cta = a.wn * (32 / SEG);
-
-    for (;;) {
-        if (threadIdx.x == 0) {
-            const int it = atomicAdd(a.next_item, 1);
-            s_item = it;
-            s_stop = (it >= a.n_items) || (ld_relaxed(a.error) != kDevOk);
-            if (!s_stop)
-                for (int b = 0; b < (a.wn + 1) * kS; ++b) {
-                    mbar_init(L.full + b, 32);
-                    mbar_init(L.empty + b, 32);
-                }
-        }
-        __syncthreads();
-        const int it = s_item;
-        if (s_stop) return;
-        const SweepItem item = a.items[it];
-        if ((int)threadIdx.x < item.q_count) L.w[threadIdx.x] = a.w[item.q_begin + threadIdx.x];
-        __syncthreads();
-        const bool has_consumer = (item.row_block + 1) * rows_cta < a.ny;
-        if (warp < a.wn) {
-            switch (item.quadrant) {
-                case 0: modal_rows<P, MODE, SEG, false, false>(a, item, L, warp, lane, has_consumer, it); break;
-                case 1: modal_rows<P, MODE, SEG, false, true>(a, item, L, warp, lane, has_consumer, it); break;
-                case 2: modal_rows<P, MODE, SEG, true, false>(a, item, L, warp, lane, has_consumer, it); break;
-                default: modal_rows<P, MODE, SEG, true, true>(a, item, L, warp, lane, has_consumer, it); break;
-            }
-        } else {
-            modal_helper<P>(a, item, L, lane);
-        }
-        __syncthreads();
-    }
-}
+using modal::kS;
+using modal::kMaxWarps;
+using modal::prefetch_depth;
 
 // Inflow traces of the ghost cells, one thread per (boundary position k, ordinate q):
 // k < nx: the y trace g(d) = sum_e x'(d,e) of the ghost cell below column k (sweep order);
@@ -522,41 +65,32 @@ __global__ void inflow_traces_kernel(const double *src, const double *xi, const 
     }
 }
 
-template <int P, int MODE, int SEG>
-cudaError_t launch_seg(const SweepArgs &args, int grid, size_t smem, cudaStream_t stream) {
-    auto kern = sweep_modal_kernel<P, MODE, SEG>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    kern<<<grid, (args.wn + 1) * 32, smem, stream>>>(args);
-    return cudaGetLastError();
-}
-
-template <int P, int MODE, int SEG>
-cudaError_t occ_seg(int threads, size_t smem, int *n) {
-    auto kern = sweep_modal_kernel<P, MODE, SEG>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, kern, threads, smem);
-}
-
-template <int P, int MODE>
-cudaError_t launch_t(const SweepArgs &args, int grid, size_t smem, cudaStream_t stream) {
+template <int P, int MODE, bool ADJ>
+cudaError_t launch_dir(const SweepArgs &args, int grid, size_t smem, cudaStream_t stream) {
     switch (args.seg) {
-        case 4: return launch_seg<P, MODE, 4>(args, grid, smem, stream);
-        case 8: return launch_seg<P, MODE, 8>(args, grid, smem, stream);
-        case 16: return launch_seg<P, MODE, 16>(args, grid, smem, stream);
-        case 32: return launch_seg<P, MODE, 32>(args, grid, smem, stream);
+        case 4: return modal::launch_seg<P, MODE, 4, ADJ>(args, grid, smem, stream);
+        case 8: return modal::launch_seg<P, MODE, 8, ADJ>(args, grid, smem, stream);
+        case 16: return modal::launch_seg<P, MODE, 16, ADJ>(args, grid, smem, stream);
+        case 32: return modal::launch_seg<P, MODE, 32, ADJ>(args, grid, smem, stream);
         default: return cudaErrorInvalidValue;
     }
+}
+
+// The transposed sweep exists for the FP64 and refined modes.
+template <int P, int MODE>
+cudaError_t launch_t(const SweepArgs &args, int grid, size_t smem, cudaStream_t stream) {
+    if (!args.adjoint) return launch_dir<P, MODE, false>(args, grid, smem, stream);
+    if constexpr (MODE == 2) return cudaErrorInvalidValue;
+    else return launch_dir<P, MODE, true>(args, grid, smem, stream);
 }
 
 template <int P, int MODE>
 cudaError_t occ_t(int seg, int threads, size_t smem, int *n) {
     switch (seg) {
-        case 4: return occ_seg<P, MODE, 4>(threads, smem, n);
-        case 8: return occ_seg<P, MODE, 8>(threads, smem, n);
-        case 16: return occ_seg<P, MODE, 16>(threads, smem, n);
-        case 32: return occ_seg<P, MODE, 32>(threads, smem, n);
+        case 4: return modal::occ_seg<P, MODE, 4, false>(threads, smem, n);
+        case 8: return modal::occ_seg<P, MODE, 8, false>(threads, smem, n);
+        case 16: return modal::occ_seg<P, MODE, 16, false>(threads, smem, n);
+        case 32: return modal::occ_seg<P, MODE, 32, false>(threads, smem, n);
         default: return cudaErrorInvalidValue;
     }
 }

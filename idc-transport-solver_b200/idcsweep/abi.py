@@ -37,7 +37,8 @@ PREC_FP32 = 2
 EXPORTED_SYMBOLS = (
     "idc_ctx_create", "idc_ctx_destroy", "idc_set_ordinates", "idc_set_sigma", "idc_sweep", "idc_pmv",
     "idc_smv", "idc_lmv", "idc_source_iteration", "idc_strerror", "idc_last_error_message", "idc_last_timing",
-    "idc_set_tiling", "idc_sweep_out", "idc_sweep_noalloc", "idc_gmres_solve",
+    "idc_set_tiling", "idc_sweep_out", "idc_sweep_noalloc", "idc_gmres_solve", "idc_sweep_adjoint",
+    "idc_adjoint_grad",
 )
 
 
@@ -83,6 +84,9 @@ def load_library(path: str = LIB_PATH):
     lib.idc_last_timing.argtypes = [vp, _dp, C.POINTER(C.c_int64)]
     lib.idc_set_tiling.argtypes = [vp, C.c_int32, C.c_int32]
     lib.idc_sweep_out.argtypes = [vp, vp, vp, C.c_double, vp, C.c_int, C.c_int]
+    lib.idc_sweep_adjoint.argtypes = [vp, vp, vp, C.c_double, vp, C.c_int, C.c_int]
+    lib.idc_adjoint_grad.argtypes = [vp, vp, vp, C.c_double, C.c_double, C.c_int32, C.c_int64, C.c_int, vp, vp, vp,
+                                     C.c_int, C.POINTER(C.c_int64), _dp]
     lib.idc_gmres_solve.argtypes = [vp, vp, C.c_double, C.c_double, C.c_int32, C.c_int64, C.c_int, C.c_int,
                                     C.POINTER(C.c_int64), _dp]
     lib.idc_sweep_noalloc.argtypes = [C.POINTER(ProblemDesc), C.c_int64, vp, vp, vp, vp, vp, vp, vp, C.c_double, vp,
@@ -207,6 +211,23 @@ class SweepContext:
         _check(self._lib.idc_gmres_solve(self._h, _ptr(source, loc), float(dt), float(abs_tol), int(restart),
                                          int(max_its), int(precision), loc, C.byref(its), C.byref(res)),
                "idc_gmres_solve")
+        return int(its.value), float(res.value)
+
+    def sweep_adjoint(self, source, result, dt=np.inf, moments=None, precision=PREC_FP64, loc=LOC_HOST):
+        """result <- L^{-T} source (interior cells, transposed sweep); moments (if given) <- sum_q result_q."""
+        _check(self._lib.idc_sweep_adjoint(self._h, _ptr(source, loc), _ptr(result, loc), float(dt),
+                                           _ptr(moments, loc), int(precision), loc), "idc_sweep_adjoint")
+
+    def adjoint_grad(self, psi, detector, dsigma_t=None, dsigma_s=None, dsource=None, dt=np.inf, abs_tol=1e-12,
+                     restart=30, max_its=3000, precision=PREC_FP64, loc=LOC_HOST):
+        """Gradients of J = detector . phi(psi) w.r.t. sigma_t, sigma_s (halo cell layout) and the isotropic
+        source moments (phi layout), written into the given arrays.  Returns (iterations, final residual)."""
+        its = C.c_int64()
+        res = C.c_double()
+        _check(self._lib.idc_adjoint_grad(self._h, _ptr(psi, loc), _ptr(detector, loc), float(dt), float(abs_tol),
+                                          int(restart), int(max_its), int(precision), _ptr(dsigma_t, loc),
+                                          _ptr(dsigma_s, loc), _ptr(dsource, loc), loc, C.byref(its), C.byref(res)),
+               "idc_adjoint_grad")
         return int(its.value), float(res.value)
 
     def last_timing(self):

@@ -192,3 +192,16 @@ def random_problem(nx: int, ny: int, p: int, sn: int, seed: int, dt: float = mat
     return Problem(nx, ny, p, xi, eta, w, qb, np.ascontiguousarray(st.ravel()), np.ascontiguousarray(ss.ravel()),
                    np.ascontiguousarray(src), 0.0, 1.0 * nx / max(nx, ny) * 2.0, 0.0, 1.0 * ny / max(nx, ny) * 2.0,
                    dt, {"kind": "random", "sn": sn, "seed": seed})
+
+
+def detector_window(P: Problem, cells: int = 16, cx: float = 2.0 / 3.0, cy: float = 0.5) -> np.ndarray:
+    """Detector weights c (phi layout) of J = c . phi = the integrated scalar flux over a cells x cells window
+    centred at (cx L, cy L): c = dx dy on the (0, 0) moment of the window's cells (the cell integral of the
+    Legendre expansion), zero elsewhere."""
+    dx, dy = (P.bx - P.ax) / P.nx, (P.by - P.ay) / P.ny
+    m = min(cells, P.nx, P.ny)
+    i0 = min(max(0, int(round(cx * P.nx - m / 2.0))), P.nx - m)
+    j0 = min(max(0, int(round(cy * P.ny - m / 2.0))), P.ny - m)
+    c = np.zeros(P.phi_shape())
+    c[1 + i0:1 + i0 + m, 1 + j0:1 + j0 + m, 0, 0] = dx * dy
+    return c

@@ -161,6 +161,30 @@ int idc_sweep_noalloc(const idc_problem_desc *desc, int64_t nq, const double *xi
 int idc_gmres_solve(idc_ctx *ctx, double *source_inout, double dt, double abs_tol, int32_t restart, int64_t max_its,
                     int precision, int loc, int64_t *iters, double *final_resid);
 
+/* ---- discrete adjoint --------------------------------------------------------------------------------- */
+
+/* Transposed sweep: result = L^{-T} source on interior cells, where L^{-1} is the sweep of idc_sweep_out
+ * (psi = L^{-1} q with the cell systems divided by dx*dy, so that L^{-T} is the exact transpose of that
+ * linear map on interior cells with zero inflow).  Cells are processed downwind-first per quadrant with
+ * the transposed cell matrices and face couplings; the source's ghost cells are not read.  moments_out
+ * (nullable) receives sum_q result_q (unweighted, interior cells; ghost cells zero).  FP64 and
+ * FP32_REFINED only.  No counterpart in the reference (it has no adjoint); it is the transpose of
+ * SweepOperator::Apply (linear_solvers/Abstract/SweepOperator.cpp:118-135) restated per cell from
+ * SweepLinearSolveSpec.cpp:98-158, 267-321, 473-598. */
+int idc_sweep_adjoint(idc_ctx *ctx, const double *source, double *result, double dt, double *moments_out, int precision,
+                      int loc);
+
+/* Gradients of the detector response J = sum_{cells, dofs} detector * phi of the transport problem
+ * (L - S P) psi = q (the problem idc_gmres_solve solves; psi is its solution, halo layout) with respect to
+ * the per-cell sigma_t, sigma_s (halo layout, ghost entries zero) and the isotropic source moments
+ * dsource (phi layout; the angular source is dsource-moment / (4 pi) on every ordinate).  The adjoint
+ * problem (L - S P)^T lam = P^T detector is solved by GMRES on (I - S^T L^{-T} P^T) mu = detector, then
+ * lam = L^{-T} P^T mu; dJ/dsigma_t = -sum_{q,k} lam psi, dJ/dsigma_s = sum_k (sum_q lam)_k phi_k / (4 pi),
+ * dJ/dq_k = (sum_q lam)_k / (4 pi) per cell.  Outputs are nullable.  No counterpart in the reference. */
+int idc_adjoint_grad(idc_ctx *ctx, const double *psi, const double *detector, double dt, double abs_tol,
+                     int32_t restart, int64_t max_its, int precision, double *dsigma_t, double *dsigma_s,
+                     double *dsource, int loc, int64_t *iters, double *final_resid);
+
 /* ---- diagnostics ----------------------------------------------------------------------------------- */
 
 /* Text for a status code (static storage). */
