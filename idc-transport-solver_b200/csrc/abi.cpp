@@ -318,6 +318,14 @@ int idc_gmres_solve(idc_ctx *ctx, double *source_inout, double dt, double abs_to
     ABI_GUARD_END
 }
 
+int idc_set_preconditioner(idc_ctx *ctx, int kind, int32_t inner_steps) {
+    ABI_GUARD_BEGIN
+    if (!ctx) return fail(IDC_ERR_ARG, "null context");
+    ABI_TRY(ctx->impl.set_preconditioner(kind, inner_steps));
+    return IDC_OK;
+    ABI_GUARD_END
+}
+
 int idc_sweep_adjoint(idc_ctx *ctx, const double *source, double *result, double dt, double *moments_out, int precision,
                       int loc) {
     ABI_GUARD_BEGIN

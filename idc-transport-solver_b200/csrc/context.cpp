@@ -54,6 +54,7 @@ Context::~Context() {
     cudaFree(d_inflow);
     cudaFree(d_krylov);
     cudaFree(d_small);
+    cudaFree(d_dsa_ws);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);

@@ -49,7 +49,8 @@ public:
     // whether the residual reached abs_tol (the caller decides whether that is an error)
     template <typename Op>
     Status gmres(Op apply, const double *b, double *x, double abs_tol, int restart, int64_t max_its, int64_t *iters,
-                 double *resid, bool *converged);
+                 double *resid, bool *converged, bool dsa = false);
+    Status set_preconditioner(int kind, int inner_steps);   // 0 none, 1 DSA
     // transposed (adjoint) problem: (L - S P)^T lam = P^T c, via (I - S^T L^{-T} P^T) mu = c
     Status apply_peierls_adjoint(const double *x, double *y, double *tmp_phi, double dt, int precision);
     Status adjoint_solve(const double *detector, double *lam_out, double *Lam_out, double dt, double abs_tol,
@@ -113,7 +114,11 @@ public:
     int64_t launches = 0;
     long long spin_limit = 1ll << 22;
 
-    double *d_krylov = nullptr;    // GMRES basis, (restart + 1) phi-sized vectors
+    double *d_krylov = nullptr;    // GMRES basis, (restart + 1) phi-sized vectors (+ restart for flexible GMRES)
+    int precond_kind = 0;          // 0 none, 1 DSA (right preconditioner of the forward Peierls GMRES)
+    int dsa_steps = 30;            // Jacobi-PCG steps per DSA application
+    double *d_dsa_ws = nullptr;    // DSA workspace
+    size_t dsa_ws_len = 0;
     size_t krylov_len = 0;
     double *d_small = nullptr;     // GMRES Hessenberg column / coefficients (device)
 

@@ -120,6 +120,12 @@ cudaError_t launch_adjoint_scatter(const GridDims &g, const double *sigma_s, con
 // (outputs on the halo layouts, interior cells written, any of them nullable)
 cudaError_t launch_adjoint_gradient(const GridDims &g, const double *psi, const double *lam, const double *phi,
                                     const double *Lam, double *dsig_t, double *dsig_s, double *dq, cudaStream_t s);
+// DSA preconditioner (dsa_kernels.cu): workspace size, coefficient setup from the cross sections, and
+// out = v + C^{-1}(sigma_s v_00) on the (0,0) moment by cg_steps Jacobi-PCG steps (out may alias v)
+size_t dsa_workspace_doubles(int nx, int ny);
+cudaError_t dsa_setup(const GridDims &g, const double *sigma_t, const double *sigma_s, double *ws, cudaStream_t s);
+cudaError_t dsa_apply(const GridDims &g, const double *sigma_s, const double *v, double *out, int cg_steps, double *ws,
+                      cudaStream_t s, int *launches);
 // sum over interior cells of (a - b)^2 into *out (device double, pre-zeroed by the launcher)
 cudaError_t launch_l2dist2(const GridDims &g, const double *a, const double *b, double *out, cudaStream_t s);
 

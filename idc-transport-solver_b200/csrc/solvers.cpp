@@ -54,23 +54,39 @@ Status Context::apply_peierls(const double *x, double *y, double *tmp_phi, doubl
 // 2-norm (the Arnoldi estimate, as PETSc reports it) is <= abs_tol.  Classical Gram-Schmidt with one
 // re-orthogonalisation pass (CGS2), Givens rotations on the host, restarts from the true residual.
 // PETSc's LGMRES adds error-approximation vectors to the restart; it converges to the same solution, so
-// iteration counts may differ but the solution does not.
+// iteration counts may differ but the solution does not.  With `dsa`, flexible GMRES with the DSA right
+// preconditioner M: the basis Z_j = M V_j is kept (M is a fixed number of CG steps, so it is not exactly
+// linear) and x = Z y.
 template <typename Op>
 Status Context::gmres(Op apply, const double *b, double *x, double abs_tol, int restart, int64_t max_its,
-                      int64_t *iters_out, double *resid_out, bool *converged_out) {
+                      int64_t *iters_out, double *resid_out, bool *converged_out, bool dsa) {
     if (restart < 1 || restart > 60) return bad(IDC_ERR_ARG, "gmres restart must be in 1..60");
     const size_t n = phi_len();
     const int m = restart;
-    if (krylov_len < (size_t)(m + 1) * n) {
+    const size_t need = (size_t)(dsa ? 2 * m + 1 : m + 1) * n;
+    if (krylov_len < need) {
         cudaFree(d_krylov);
         d_krylov = nullptr;
         krylov_len = 0;
-        IDC_TRY_CUDA(cudaMalloc(&d_krylov, sizeof(double) * (size_t)(m + 1) * n));
-        krylov_len = (size_t)(m + 1) * n;
+        IDC_TRY_CUDA(cudaMalloc(&d_krylov, sizeof(double) * need));
+        krylov_len = need;
     }
     if (!d_small) IDC_TRY_CUDA(cudaMalloc(&d_small, sizeof(double) * 128));
     double *V = d_krylov;
     auto Vc = [&](int k) { return V + (size_t)k * n; };
+    auto Zc = [&](int k) { return V + (size_t)(m + 1 + k) * n; };
+    if (dsa) {
+        const size_t wl = dsa_workspace_doubles((int)nx, (int)ny);
+        if (dsa_ws_len < wl) {
+            cudaFree(d_dsa_ws);
+            d_dsa_ws = nullptr;
+            dsa_ws_len = 0;
+            IDC_TRY_CUDA(cudaMalloc(&d_dsa_ws, sizeof(double) * wl));
+            dsa_ws_len = wl;
+        }
+        IDC_TRY_CUDA(dsa_setup(dims(), d_sigma_t, d_sigma_s, d_dsa_ws, stream));
+        launches += 2;
+    }
 
     IDC_TRY_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, stream));
     // r = b - A x = b for the zero initial guess
@@ -89,7 +105,14 @@ Status Context::gmres(Op apply, const double *b, double *x, double abs_tol, int 
         g[0] = beta;
         int k = 0;   // columns built in this cycle
         for (int j = 0; j < m && its < max_its; ++j) {
-            IDC_TRY(apply(Vc(j), Vc(j + 1)));
+            if (dsa) {
+                int nl = 0;
+                IDC_TRY_CUDA(dsa_apply(dims(), d_sigma_s, Vc(j), Zc(j), dsa_steps, d_dsa_ws, stream, &nl));
+                launches += nl;
+                IDC_TRY(apply(Zc(j), Vc(j + 1)));
+            } else {
+                IDC_TRY(apply(Vc(j), Vc(j + 1)));
+            }
             // CGS2: h = V^T w, w -= V h, twice
             IDC_TRY_CUDA(launch_multidot(V, j + 1, n, Vc(j + 1), n, d_small, stream));
             IDC_TRY_CUDA(cudaMemcpyAsync(h.data(), d_small, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost, stream));
@@ -136,7 +159,7 @@ Status Context::gmres(Op apply, const double *b, double *x, double abs_tol, int 
         }
         for (int i = 0; i < k; ++i) yv[i] = -yv[i];   // multiaxpy subtracts
         IDC_TRY_CUDA(cudaMemcpyAsync(d_small, yv.data(), sizeof(double) * k, cudaMemcpyHostToDevice, stream));
-        IDC_TRY_CUDA(launch_multiaxpy(x, V, k, n, d_small, n, stream));
+        IDC_TRY_CUDA(launch_multiaxpy(x, dsa ? Zc(0) : V, k, n, d_small, n, stream));
         launches += 1;
         if (resid <= abs_tol) {
             converged = true;
@@ -169,7 +192,7 @@ Status Context::gmres_peierls(const double *src, double *psi_out, double dt, dou
     bool converged = false;
     double resid = 0.0;
     auto op = [&](const double *in, double *out) { return apply_peierls(in, out, tmp, dt, precision); };
-    IDC_TRY(gmres(op, b, x, abs_tol, restart, max_its, iters_out, &resid, &converged));
+    IDC_TRY(gmres(op, b, x, abs_tol, restart, max_its, iters_out, &resid, &converged, precond_kind == 1));
     // psi = L^{-1} (S phi + Q)  (PETScPeierlsSolver.cpp:504-505)
     IDC_TRY(sweep(src, psi_out, dt, nullptr, precision, x, 1.0));
     IDC_TRY(check_device_error());
@@ -177,6 +200,14 @@ Status Context::gmres_peierls(const double *src, double *psi_out, double dt, dou
     if (!converged)
         return bad(IDC_ERR_NOT_CONVERGED, "GMRES transport solve failed to converge (max_its reached, residual " +
                                               std::to_string(resid) + ")");
+    return Status::ok();
+}
+
+Status Context::set_preconditioner(int kind, int inner_steps) {
+    if (kind < 0 || kind > 1) return bad(IDC_ERR_ARG, "unknown preconditioner");
+    if (kind == 1 && (inner_steps < 1 || inner_steps > 10000)) return bad(IDC_ERR_ARG, "DSA steps must be in 1..10000");
+    precond_kind = kind;
+    if (kind == 1) dsa_steps = inner_steps;
     return Status::ok();
 }
 

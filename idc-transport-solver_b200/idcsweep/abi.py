@@ -18,6 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(os.path.dirname(HERE), "build", "libidcsweep.so")
 
 IDC_OK = 0
+PRECOND_NONE, PRECOND_DSA = 0, 1
 IDC_ERR_ARG = 1
 IDC_ERR_UNSUPPORTED = 2
 IDC_ERR_CUDA = 3
@@ -38,7 +39,7 @@ EXPORTED_SYMBOLS = (
     "idc_ctx_create", "idc_ctx_destroy", "idc_set_ordinates", "idc_set_sigma", "idc_sweep", "idc_pmv",
     "idc_smv", "idc_lmv", "idc_source_iteration", "idc_strerror", "idc_last_error_message", "idc_last_timing",
     "idc_set_tiling", "idc_sweep_out", "idc_sweep_noalloc", "idc_gmres_solve", "idc_sweep_adjoint",
-    "idc_adjoint_grad",
+    "idc_adjoint_grad", "idc_set_preconditioner",
 )
 
 
@@ -85,6 +86,7 @@ def load_library(path: str = LIB_PATH):
     lib.idc_set_tiling.argtypes = [vp, C.c_int32, C.c_int32]
     lib.idc_sweep_out.argtypes = [vp, vp, vp, C.c_double, vp, C.c_int, C.c_int]
     lib.idc_sweep_adjoint.argtypes = [vp, vp, vp, C.c_double, vp, C.c_int, C.c_int]
+    lib.idc_set_preconditioner.argtypes = [vp, C.c_int, C.c_int32]
     lib.idc_adjoint_grad.argtypes = [vp, vp, vp, C.c_double, C.c_double, C.c_int32, C.c_int64, C.c_int, vp, vp, vp,
                                      C.c_int, C.POINTER(C.c_int64), _dp]
     lib.idc_gmres_solve.argtypes = [vp, vp, C.c_double, C.c_double, C.c_int32, C.c_int64, C.c_int, C.c_int,
@@ -212,6 +214,10 @@ class SweepContext:
                                          int(max_its), int(precision), loc, C.byref(its), C.byref(res)),
                "idc_gmres_solve")
         return int(its.value), float(res.value)
+
+    def set_preconditioner(self, kind: int, inner_steps: int = 30):
+        """Right preconditioner of gmres_solve: PRECOND_NONE or PRECOND_DSA (inner_steps CG steps)."""
+        _check(self._lib.idc_set_preconditioner(self._h, int(kind), int(inner_steps)), "idc_set_preconditioner")
 
     def sweep_adjoint(self, source, result, dt=np.inf, moments=None, precision=PREC_FP64, loc=LOC_HOST):
         """result <- L^{-T} source (interior cells, transposed sweep); moments (if given) <- sum_q result_q."""

@@ -161,6 +161,14 @@ int idc_sweep_noalloc(const idc_problem_desc *desc, int64_t nq, const double *xi
 int idc_gmres_solve(idc_ctx *ctx, double *source_inout, double dt, double abs_tol, int32_t restart, int64_t max_its,
                     int precision, int loc, int64_t *iters, double *final_resid);
 
+/* Right preconditioner of idc_gmres_solve: 0 = none, 1 = diffusion synthetic acceleration (DSA): a 2-D
+ * cell-centred diffusion solve on the cell-average moment, -div(1/(3 sigma_t) grad e) + sigma_a e =
+ * sigma_s r_00 with Marshak vacuum boundaries, by inner_steps Jacobi-preconditioned CG steps; GMRES then
+ * runs in its flexible form.  The reference has DSA only in 1-D (SIP-DG inside its PETSc Peierls solver,
+ * linear_solvers/RKDG/ImplicitSolver/PETScPeierlsSolver.cpp:27-376); the converged solution does not
+ * depend on the preconditioner. */
+int idc_set_preconditioner(idc_ctx *ctx, int kind, int32_t inner_steps);
+
 /* ---- discrete adjoint --------------------------------------------------------------------------------- */
 
 /* Transposed sweep: result = L^{-T} source on interior cells, where L^{-1} is the sweep of idc_sweep_out

@@ -76,3 +76,42 @@ def test_sweep_out_matches_in_place():
     assert np.array_equal(a[interior], b[interior])
     assert np.all(b[0] == 7.0) and np.all(b[:, -1] == 7.0)    # result ghosts untouched
     assert np.array_equal(pa, pb)                               # fixed-order moment reduction
+
+
+@pytest.mark.parametrize("path", GOLDEN[:4], ids=[os.path.basename(p) for p in GOLDEN[:4]])
+def test_gmres_dsa_reaches_reference_si_fixed_point(path):
+    z = np.load(path)
+    with abi.SweepContext(int(z["nx"]), int(z["ny"]), int(z["p"]), float(z["ax"]), float(z["bx"]), float(z["ay"]),
+                          float(z["by"])) as ctx:
+        ctx.set_ordinates(z["xi"], z["eta"], z["w"], z["quad"])
+        ctx.set_sigma(z["sigma_t"], z["sigma_s"])
+        ctx.set_preconditioner(abi.PRECOND_DSA, 30)
+        psi = z["source"].copy()
+        its, res = ctx.gmres_solve(psi, float(z["dt"]), abs_tol=1e-13, restart=30, max_its=500)
+        assert res <= 1e-13
+        assert rel_err(psi, z["si_psi"]) < 1e-10
+
+
+@pytest.mark.parametrize("p,sn,c", [(1, 8, (0.95, 0.999)), (2, 8, (0.5, 0.999))])
+def test_dsa_reduces_gmres_iterations(p, sn, c):
+    """Scattering-dominated log-normal media: the DSA-preconditioned flexible GMRES converges to the same
+    solution in fewer iterations."""
+    P = lognormal(64, p, sn, seed=2, c_range=c)
+    out = {}
+    for kind in (abi.PRECOND_NONE, abi.PRECOND_DSA):
+        with context_for(P) as ctx:
+            ctx.set_preconditioner(kind, 30)
+            psi = P.source.copy()
+            its, res = ctx.gmres_solve(psi, P.dt, abs_tol=1e-10, restart=30, max_its=3000)
+            out[kind] = (its, psi)
+    assert out[abi.PRECOND_DSA][0] < out[abi.PRECOND_NONE][0]
+    assert rel_err(out[abi.PRECOND_DSA][1], out[abi.PRECOND_NONE][1]) < 1e-8
+
+
+def test_set_preconditioner_rejects_bad_arguments():
+    P = lognormal(8, 1, 4, seed=1)
+    with context_for(P) as ctx:
+        with pytest.raises(abi.IdcError):
+            ctx.set_preconditioner(7, 30)
+        with pytest.raises(abi.IdcError):
+            ctx.set_preconditioner(abi.PRECOND_DSA, 0)
