@@ -326,6 +326,38 @@ int idc_set_preconditioner(idc_ctx *ctx, int kind, int32_t inner_steps) {
     ABI_GUARD_END
 }
 
+int idc_idc_integrate(idc_ctx *ctx, double *psi_inout, const double *source, double dt, int64_t steps,
+                      int32_t num_nodes, int32_t num_corrections, int scattering, int precision, double abs_tol,
+                      int32_t restart, int64_t max_its, int use_graph, int loc, int64_t *sweeps) {
+    ABI_GUARD_BEGIN
+    if (!ctx || !psi_inout || !source) return fail(IDC_ERR_ARG, "idc_idc_integrate: null argument");
+    if (!valid_loc(loc)) return fail(IDC_ERR_ARG, "bad loc");
+    idc::Context &c = ctx->impl;
+    ABI_TRY_CUDA(cudaSetDevice(c.device));
+    c.launches = 0;
+    double *d_psi = psi_inout;
+    const double *d_src = source;
+    if (loc == IDC_LOC_HOST) {
+        ABI_TRY(c.ensure_psi_buffers(2));
+        ABI_TRY_CUDA(cudaMemcpyAsync(c.psi_buf(0), psi_inout, sizeof(double) * c.psi_len(), cudaMemcpyHostToDevice,
+                                     c.stream));
+        ABI_TRY_CUDA(cudaMemcpyAsync(c.psi_buf(1), source, sizeof(double) * c.psi_len(), cudaMemcpyHostToDevice,
+                                     c.stream));
+        d_psi = c.psi_buf(0);
+        d_src = c.psi_buf(1);
+    }
+    int64_t n_sweeps = 0;
+    idc::Status st = c.idc_integrate(d_psi, d_src, dt, steps, num_nodes, num_corrections, scattering, precision,
+                                     abs_tol, restart, max_its, use_graph != 0, &n_sweeps);
+    if (sweeps) *sweeps = n_sweeps;
+    if (!st.good()) return fail(st);
+    if (loc == IDC_LOC_HOST)
+        ABI_TRY_CUDA(cudaMemcpyAsync(psi_inout, d_psi, sizeof(double) * c.psi_len(), cudaMemcpyDeviceToHost, c.stream));
+    ABI_TRY_CUDA(cudaStreamSynchronize(c.stream));
+    return IDC_OK;
+    ABI_GUARD_END
+}
+
 int idc_sweep_adjoint(idc_ctx *ctx, const double *source, double *result, double dt, double *moments_out, int precision,
                       int loc) {
     ABI_GUARD_BEGIN

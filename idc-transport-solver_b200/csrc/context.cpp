@@ -41,6 +41,8 @@ Context::~Context() {
     if (device >= 0) cudaSetDevice(device);
     for (double *p : psi_bufs_) cudaFree(p);
     for (double *p : phi_bufs_) cudaFree(p);
+    for (double *p : idc_psi_) cudaFree(p);
+    for (double *p : idc_phi_) cudaFree(p);
     cudaFree(d_scalar_);
     cudaFree(d_xi);
     cudaFree(d_eta);
@@ -377,7 +379,7 @@ Status Context::sweep(const double *src, double *out, double dt, double *phi, in
     IDC_TRY_CUDA(cudaMemsetAsync(d_sync, 0, sizeof(int), stream));
     IDC_TRY_CUDA(cudaMemsetAsync(d_sync + 2, 0, sizeof(int) * n_items, stream));
     if (a.phi) IDC_TRY_CUDA(cudaMemsetAsync(phi, 0, sizeof(double) * phi_len(), stream));
-    if (kernel != kModal) IDC_TRY_CUDA(cudaEventRecord(ev0, stream));
+    if (kernel != kModal && !capturing) IDC_TRY_CUDA(cudaEventRecord(ev0, stream));
     if (kernel == kModal) {
         if (src && !adjoint) {   // inflow traces of the ghost cells (packed modal, or physical for the refined mode)
             const size_t need = (size_t)(nx + ny) * nq * P;
@@ -393,13 +395,13 @@ Status Context::sweep(const double *src, double *out, double dt, double *phi, in
             launches += 1;
             a.inflow = d_inflow;
         }
-        IDC_TRY_CUDA(cudaEventRecord(ev0, stream));   // the timing covers the sweep kernel alone
+        if (!capturing) IDC_TRY_CUDA(cudaEventRecord(ev0, stream));   // the timing covers the sweep kernel alone
         IDC_TRY_CUDA(launch_sweep_modal(P, precision, a, grid, smem, stream));
     } else if (kernel == kWarp)
         IDC_TRY_CUDA(launch_sweep_warp(P, precision, a, grid, smem, stream));
     else
         IDC_TRY_CUDA(launch_sweep(P, precision, a, grid, block, smem, stream));
-    IDC_TRY_CUDA(cudaEventRecord(ev1, stream));
+    if (!capturing) IDC_TRY_CUDA(cudaEventRecord(ev1, stream));
     launches += 1;
     if (a.phi_part) {
         IDC_TRY_CUDA(launch_reduce_phi_partials(dims(), d_phi_part, items_per_rb, phi_len(), phi, stream));

@@ -51,6 +51,12 @@ public:
     Status gmres(Op apply, const double *b, double *x, double abs_tol, int restart, int64_t max_its, int64_t *iters,
                  double *resid, bool *converged, bool dsa = false);
     Status set_preconditioner(int kind, int inner_steps);   // 0 none, 1 DSA
+    // IDC time integration (idc.cpp): psi (device, in/out) advanced `steps` steps of size dt with M
+    // Gauss-Lobatto nodes and K corrections; scattering 0 = explicit (IMEX, one sweep per substep, CUDA
+    // graph when use_graph), 1 = implicit (GMRES per substep)
+    Status idc_integrate(double *psi, const double *Q, double dt, int64_t steps, int M, int K, int scattering,
+                         int precision, double abs_tol, int restart, int64_t max_its, bool use_graph,
+                         int64_t *sweeps);
     // transposed (adjoint) problem: (L - S P)^T lam = P^T c, via (I - S^T L^{-T} P^T) mu = c
     Status apply_peierls_adjoint(const double *x, double *y, double *tmp_phi, double dt, int precision);
     Status adjoint_solve(const double *detector, double *lam_out, double *Lam_out, double dt, double abs_tol,
@@ -111,6 +117,7 @@ public:
     int occupancy_precision = -1;
 
     float last_sweep_ms = 0.f;
+    bool capturing = false;   // a CUDA graph capture is open on `stream`: no timing events, no host syncs
     int64_t launches = 0;
     long long spin_limit = 1ll << 22;
 
@@ -125,6 +132,7 @@ public:
 private:
     Status build_schedule(int precision);
     std::vector<double *> psi_bufs_, phi_bufs_;
+    std::vector<double *> idc_psi_, idc_phi_;
     double *d_scalar_ = nullptr;
 };
 

@@ -1,0 +1,300 @@
+// IDC (integral deferred correction) time stepping of the transport equation on the GPU:
+//     d psi / dt = -(L - S P) psi + Q,
+// non-hybrid, "update" form (IDCIntegrator::Step_Nonhybrid and ComputeResiduals / ComputeSource,
+// time_integrators/RKDG/idc.cpp:846-955, 1657-1740), on Gauss-Lobatto nodes (SetNodes, :2305-2381).
+//
+// Two treatments of scattering:
+//  * implicit (the reference's): every substep solves (1/(h dt) + L - S P) psi_n = src_n with the GPU
+//    GMRES (Peierls form); the prediction is implicit Euler, and a correction's source is
+//    src_n = sum_l (delta_nl - W(n,l)/h) res_l + psi_{n-1}/(h dt) + Q,  res_l = (L - S P) psi_l.
+//  * explicit (IMEX): every substep is one sweep, (1/(h dt) + L) psi_n = src_n + S phi_s, with the
+//    scattering lagged to the previous node: the prediction uses phi_s = phi_{n-1}; a correction uses
+//    src_n = psi_{n-1}^new/(h dt) + Q + res_n^old - (1/h) sum_l W(n,l) res_l^old and
+//    phi_s = phi_{n-1}^new - phi_{n-1}^old + phi_n^old, so that the implicit part L psi_n and the
+//    explicit part S P psi_{n-1} are both corrected against the previous level (IMEX deferred correction).
+//    A whole IMEX step is a fixed sequence of kernels with no host synchronisation, so it is captured once
+//    as a CUDA graph and replayed.
+// The quadrature sums, residuals and sources are FP64; `precision` selects the sweep arithmetic.
+#include "context.hpp"
+
+#include <cmath>
+#include <vector>
+
+namespace idc {
+
+#define IDC_TRY_CUDA(expr)                                    \
+    do {                                                      \
+        cudaError_t e_ = (expr);                              \
+        if (e_ != cudaSuccess) return cuda_status(e_, #expr); \
+    } while (0)
+
+#define IDC_TRY(expr)              \
+    do {                           \
+        Status s_ = (expr);        \
+        if (!s_.good()) return s_; \
+    } while (0)
+
+namespace {
+
+Status bad(int code, const std::string &m) {
+    Status s;
+    s.code = code;
+    s.msg = m;
+    return s;
+}
+
+// Legendre P_n(x) and P_n'(x).
+void legendre(int n, double x, double *p, double *dp) {
+    double p0 = 1.0, p1 = x;
+    if (n == 0) {
+        *p = 1.0;
+        *dp = 0.0;
+        return;
+    }
+    for (int k = 2; k <= n; ++k) {
+        const double pk = ((2 * k - 1) * x * p1 - (k - 1) * p0) / k;
+        p0 = p1;
+        p1 = pk;
+    }
+    *p = p1;
+    *dp = (std::fabs(x) < 1.0) ? n * (x * p1 - p0) / (x * x - 1.0) : 0.5 * n * (n + 1) * (x > 0 ? 1.0 : ((n & 1) ? 1.0 : -1.0));
+}
+
+// Gauss-Legendre nodes / weights on [-1, 1] (Newton on P_m).
+void gauss_legendre(int m, std::vector<double> &x, std::vector<double> &w) {
+    x.assign(m, 0.0);
+    w.assign(m, 0.0);
+    for (int k = 0; k < m; ++k) {
+        double z = std::cos(M_PI * (k + 0.75) / (m + 0.5));
+        for (int it = 0; it < 100; ++it) {
+            double p, dp;
+            legendre(m, z, &p, &dp);
+            const double dz = p / dp;
+            z -= dz;
+            if (std::fabs(dz) < 1e-16) break;
+        }
+        double p, dp;
+        legendre(m, z, &p, &dp);
+        x[k] = z;
+        w[k] = 2.0 / ((1.0 - z * z) * dp * dp);
+    }
+}
+
+// Gauss-Lobatto nodes on [0, 1] (M >= 2): the endpoints and the roots of P'_{M-1}.
+std::vector<double> lobatto_nodes(int M) {
+    std::vector<double> t(M);
+    const int n = M - 1;
+    t[0] = 0.0;
+    t[M - 1] = 1.0;
+    for (int k = 1; k < n; ++k) {
+        double z = -std::cos(M_PI * k / n);
+        for (int it = 0; it < 100; ++it) {
+            double p, dp;
+            legendre(n, z, &p, &dp);
+            const double d2p = (2.0 * z * dp - n * (n + 1) * p) / (1.0 - z * z);
+            const double dz = dp / d2p;
+            z -= dz;
+            if (std::fabs(dz) < 1e-16) break;
+        }
+        t[k] = 0.5 * (z + 1.0);
+    }
+    return t;
+}
+
+// W[i][j] = integral over [t_{i-1}, t_i] (i >= 1) or [0, 1] (i = 0) of the Lagrange basis l_j of the nodes.
+std::vector<double> integration_weights(const std::vector<double> &t) {
+    const int M = (int)t.size();
+    std::vector<double> gx, gw, W((size_t)M * M, 0.0);
+    gauss_legendre(M, gx, gw);   // exact for degree 2M-1 >= M-1
+    for (int i = 0; i < M; ++i) {
+        const double a = i == 0 ? 0.0 : t[i - 1], b = i == 0 ? 1.0 : t[i];
+        for (int j = 0; j < M; ++j) {
+            double acc = 0.0;
+            for (int q = 0; q < M; ++q) {
+                const double x = 0.5 * (a + b) + 0.5 * (b - a) * gx[q];
+                double l = 1.0;
+                for (int m = 0; m < M; ++m)
+                    if (m != j) l *= (x - t[m]) / (t[j] - t[m]);
+                acc += gw[q] * l;
+            }
+            W[(size_t)i * M + j] = 0.5 * (b - a) * acc;
+        }
+    }
+    return W;
+}
+
+}  // namespace
+
+void idc_nodes_and_weights(int M, std::vector<double> &t, std::vector<double> &W) {
+    t = lobatto_nodes(M);
+    W = integration_weights(t);
+}
+
+Status Context::idc_integrate(double *psi, const double *Q, double dt, int64_t steps, int M, int K, int scattering,
+                              int precision, double abs_tol, int restart, int64_t max_its, bool use_graph,
+                              int64_t *sweeps_out) {
+    if (!have_ordinates || !have_sigma) return bad(IDC_ERR_STATE, "IDC before ordinates and sigma");
+    if (M < 2 || M > 8) return bad(IDC_ERR_ARG, "IDC nodes must be in 2..8");
+    if (K < 0 || K > 16) return bad(IDC_ERR_ARG, "IDC corrections must be in 0..16");
+    if (!(dt > 0) || !std::isfinite(dt)) return bad(IDC_ERR_ARG, "IDC needs a finite positive dt");
+    if (steps < 0) return bad(IDC_ERR_ARG, "negative step count");
+    if (scattering != 0 && scattering != 1) return bad(IDC_ERR_ARG, "scattering must be 0 (explicit) or 1 (implicit)");
+    if (kernel != kModal) return bad(IDC_ERR_UNSUPPORTED, "IDC needs the modal sweep kernel");
+    std::vector<double> t, W;
+    idc_nodes_and_weights(M, t, W);
+
+    // buffers: M stages, M residuals, one source (psi-sized); M moments, M previous-level moments, one
+    // scattering combination (moment-sized)
+    const size_t np = psi_len(), nm = phi_len();
+    const int need_psi = 2 * M + 1, need_phi = 2 * M + 1;
+    IDC_TRY_CUDA(cudaSetDevice(device));
+    while ((int)idc_psi_.size() < need_psi) {
+        double *p = nullptr;
+        IDC_TRY_CUDA(cudaMalloc(&p, sizeof(double) * np));
+        idc_psi_.push_back(p);
+    }
+    while ((int)idc_phi_.size() < need_phi) {
+        double *p = nullptr;
+        IDC_TRY_CUDA(cudaMalloc(&p, sizeof(double) * nm));
+        IDC_TRY_CUDA(cudaMemset(p, 0, sizeof(double) * nm));
+        idc_phi_.push_back(p);
+    }
+    auto stage = [&](int l) { return idc_psi_[l]; };
+    auto res = [&](int l) { return idc_psi_[M + l]; };
+    double *src = idc_psi_[2 * M];
+    auto phi = [&](int l) { return idc_phi_[l]; };
+    auto phi_old = [&](int l) { return idc_phi_[M + l]; };
+    double *phi_s = idc_phi_[2 * M];
+    int64_t sweeps = 0;
+
+    auto residual = [&](int l) -> Status {   // res_l = (L - S P) psi_l  (ComputeResiduals, idc.cpp:1657-1667)
+        IDC_TRY(pmv(1.0, 0.0, stage(l), phi(l)));
+        IDC_TRY(lmv(1.0, 0.0, stage(l), res(l)));
+        IDC_TRY(smv(-1.0, 1.0, phi(l), res(l)));
+        return Status::ok();
+    };
+    auto source = [&](int n, bool correction, bool imex) -> Status {
+        const double h = t[n] - t[n - 1];
+        IdcTerms tm{};
+        tm.n = 0;
+        tm.a[tm.n] = stage(n - 1);
+        tm.c[tm.n++] = 1.0 / (h * dt);
+        if (correction) {
+            for (int l = 0; l < M; ++l) {
+                tm.a[tm.n] = res(l);
+                tm.c[tm.n++] = (n == l ? 1.0 : 0.0) - W[(size_t)n * M + l] / h;
+            }
+        }
+        (void)imex;
+        IDC_TRY_CUDA(launch_idc_source(dims(), tm, Q, src, stream));
+        launches += 1;
+        return Status::ok();
+    };
+
+    // one IMEX step: only stream work, so it can be captured
+    auto imex_step = [&]() -> Status {
+        IDC_TRY(pmv(1.0, 0.0, stage(0), phi(0)));
+        for (int n = 1; n < M; ++n) {   // prediction: IMEX Euler
+            const double h = t[n] - t[n - 1];
+            IDC_TRY(source(n, false, true));
+            IDC_TRY(sweep(src, stage(n), h * dt, phi(n), precision, phi(n - 1), 1.0));
+            ++sweeps;
+        }
+        for (int p = 0; p < K; ++p) {
+            for (int l = 0; l < M; ++l) {
+                IDC_TRY(lmv(1.0, 0.0, stage(l), res(l)));
+                IDC_TRY(smv(-1.0, 1.0, phi(l), res(l)));
+                IDC_TRY_CUDA(cudaMemcpyAsync(phi_old(l), phi(l), sizeof(double) * nm, cudaMemcpyDeviceToDevice, stream));
+            }
+            for (int n = 1; n < M; ++n) {
+                const double h = t[n] - t[n - 1];
+                IDC_TRY(source(n, true, true));
+                IDC_TRY_CUDA(launch_phi_combine(nm, phi(n - 1), phi_old(n - 1), phi_old(n), phi_s, stream));
+                launches += 1;
+                IDC_TRY(sweep(src, stage(n), h * dt, phi(n), precision, phi_s, 1.0));
+                ++sweeps;
+            }
+        }
+        IDC_TRY_CUDA(cudaMemcpyAsync(stage(0), stage(M - 1), sizeof(double) * np, cudaMemcpyDeviceToDevice, stream));
+        return Status::ok();
+    };
+
+    // stage ghost cells hold the inflow values (Q's ghost cells), as the reference's in-place solves leave
+    // them; the sweeps write interior cells only, so they stay.  Lmv reads them for the boundary residuals.
+    IDC_TRY_CUDA(cudaMemcpyAsync(stage(0), psi, sizeof(double) * np, cudaMemcpyDeviceToDevice, stream));
+    for (int l = 1; l < M; ++l)
+        IDC_TRY_CUDA(cudaMemcpyAsync(stage(l), Q, sizeof(double) * np, cudaMemcpyDeviceToDevice, stream));
+    if (scattering == 0) {
+        if (use_graph && steps > 0) {
+            // first step uncaptured (builds the sweep schedule, allocates nothing inside the capture), then
+            // capture one step and replay it
+            IDC_TRY(imex_step());
+            IDC_TRY(check_device_error());
+            if (steps > 1) {
+                cudaGraph_t graph = nullptr;
+                cudaGraphExec_t exec = nullptr;
+                capturing = true;
+                const int64_t s0 = sweeps, l0 = launches;
+                IDC_TRY_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+                Status st = imex_step();
+                cudaError_t ce = cudaStreamEndCapture(stream, &graph);
+                capturing = false;
+                if (!st.good()) {
+                    if (graph) cudaGraphDestroy(graph);
+                    return st;
+                }
+                IDC_TRY_CUDA(ce);
+                const int64_t per_sweeps = sweeps - s0, per_launch = launches - l0;
+                sweeps = s0;
+                launches = l0;
+                ce = cudaGraphInstantiate(&exec, graph, 0);
+                if (ce != cudaSuccess) {
+                    cudaGraphDestroy(graph);
+                    return cuda_status(ce, "cudaGraphInstantiate");
+                }
+                for (int64_t s = 1; s < steps; ++s) {
+                    ce = cudaGraphLaunch(exec, stream);
+                    if (ce != cudaSuccess) break;
+                    sweeps += per_sweeps;
+                    launches += per_launch;
+                }
+                cudaGraphExecDestroy(exec);
+                cudaGraphDestroy(graph);
+                IDC_TRY_CUDA(ce);
+            }
+        } else {
+            for (int64_t s = 0; s < steps; ++s) IDC_TRY(imex_step());
+        }
+        IDC_TRY(check_device_error());
+    } else {
+        // implicit: GMRES per substep (host-driven; the reference's Step_Nonhybrid, update form)
+        for (int64_t s = 0; s < steps; ++s) {
+            for (int n = 1; n < M; ++n) {
+                const double h = t[n] - t[n - 1];
+                IDC_TRY(source(n, false, false));
+                int64_t its = 0;
+                double r = 0;
+                IDC_TRY(gmres_peierls(src, stage(n), h * dt, abs_tol, restart, max_its, precision, &its, &r));
+                sweeps += its + 2;
+            }
+            for (int p = 0; p < K; ++p) {
+                for (int l = 0; l < M; ++l) IDC_TRY(residual(l));
+                for (int n = 1; n < M; ++n) {
+                    const double h = t[n] - t[n - 1];
+                    IDC_TRY(source(n, true, false));
+                    int64_t its = 0;
+                    double r = 0;
+                    IDC_TRY(gmres_peierls(src, stage(n), h * dt, abs_tol, restart, max_its, precision, &its, &r));
+                    sweeps += its + 2;
+                }
+            }
+            IDC_TRY_CUDA(cudaMemcpyAsync(stage(0), stage(M - 1), sizeof(double) * np, cudaMemcpyDeviceToDevice, stream));
+        }
+    }
+    IDC_TRY_CUDA(cudaMemcpyAsync(psi, stage(0), sizeof(double) * np, cudaMemcpyDeviceToDevice, stream));
+    IDC_TRY_CUDA(cudaStreamSynchronize(stream));
+    if (sweeps_out) *sweeps_out = sweeps;
+    return Status::ok();
+}
+
+}  // namespace idc

@@ -120,6 +120,15 @@ cudaError_t launch_adjoint_scatter(const GridDims &g, const double *sigma_s, con
 // (outputs on the halo layouts, interior cells written, any of them nullable)
 cudaError_t launch_adjoint_gradient(const GridDims &g, const double *psi, const double *lam, const double *phi,
                                     const double *Lam, double *dsig_t, double *dsig_s, double *dq, cudaStream_t s);
+// IDC (ops_kernels.cu): out = sum_k c_k A_k + Q on interior cells, Q on ghost cells (Q nullable = 0)
+struct IdcTerms {
+    static constexpr int kMax = 10;
+    int n;
+    const double *a[kMax];
+    double c[kMax];
+};
+cudaError_t launch_idc_source(const GridDims &g, const IdcTerms &t, const double *Q, double *out, cudaStream_t s);
+cudaError_t launch_phi_combine(size_t n, const double *a, const double *b, const double *c, double *out, cudaStream_t s);
 // DSA preconditioner (dsa_kernels.cu): workspace size, coefficient setup from the cross sections, and
 // out = v + C^{-1}(sigma_s v_00) on the (0,0) moment by cg_steps Jacobi-PCG steps (out may alias v)
 size_t dsa_workspace_doubles(int nx, int ny);

@@ -246,6 +246,31 @@ __global__ void dot_kernel(const double *__restrict__ x, const double *__restric
 }
 
 
+
+// ---- IDC helpers ----
+
+// out = sum_k c_k A_k + Q on interior cells, out = Q on ghost cells (the inflow values), psi layout:
+// the FP64 source of an IDC substep (IDCIntegrator::ComputeSource, time_integrators/RKDG/idc.cpp:1691-1740).
+__global__ void idc_source_kernel(GridDims g, IdcTerms t, const double *__restrict__ Q, double *__restrict__ out) {
+    const size_t cell = (size_t)g.nq * g.P * g.P;
+    const size_t total = (size_t)(g.nx + 2) * (g.ny + 2) * cell;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const size_t c = e / cell;
+        const int i = (int)(c / (g.ny + 2)), j = (int)(c % (g.ny + 2));
+        double v = Q ? Q[e] : 0.0;
+        if (i >= 1 && i <= g.nx && j >= 1 && j <= g.ny)
+            for (int k = 0; k < t.n; ++k) v = fma(t.c[k], t.a[k][e], v);
+        out[e] = v;
+    }
+}
+
+// out = a - b + c (moment arrays, all cells)
+__global__ void phi_combine_kernel(size_t n, const double *__restrict__ a, const double *__restrict__ b,
+                                   const double *__restrict__ c, double *__restrict__ out) {
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+        out[e] = a[e] - b[e] + c[e];
+}
+
 // ---- adjoint helpers ----
 
 // y = x - sigma_s / (4 pi) * lam on interior cells, y = x on ghost cells: the adjoint Peierls operator
@@ -390,6 +415,18 @@ cudaError_t launch_adjoint_gradient(const GridDims &g, const double *psi, const 
                                     const double *Lam, double *dsig_t, double *dsig_s, double *dq, cudaStream_t s) {
     const size_t warps = (size_t)g.nx * g.ny;
     adjoint_gradient_kernel<<<blocks_for(warps * 32), kThreads, 0, s>>>(g, psi, lam, phi, Lam, dsig_t, dsig_s, dq);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_idc_source(const GridDims &g, const IdcTerms &t, const double *Q, double *out, cudaStream_t s) {
+    if (t.n < 0 || t.n > IdcTerms::kMax) return cudaErrorInvalidValue;
+    const size_t n = (size_t)(g.nx + 2) * (g.ny + 2) * g.nq * g.P * g.P;
+    idc_source_kernel<<<blocks_for(n), kThreads, 0, s>>>(g, t, Q, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_phi_combine(size_t n, const double *a, const double *b, const double *c, double *out, cudaStream_t s) {
+    phi_combine_kernel<<<blocks_for(n), kThreads, 0, s>>>(n, a, b, c, out);
     return cudaGetLastError();
 }
 

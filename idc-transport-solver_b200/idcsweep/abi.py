@@ -19,6 +19,7 @@ LIB_PATH = os.path.join(os.path.dirname(HERE), "build", "libidcsweep.so")
 
 IDC_OK = 0
 PRECOND_NONE, PRECOND_DSA = 0, 1
+SCATTER_EXPLICIT, SCATTER_IMPLICIT = 0, 1
 IDC_ERR_ARG = 1
 IDC_ERR_UNSUPPORTED = 2
 IDC_ERR_CUDA = 3
@@ -39,7 +40,7 @@ EXPORTED_SYMBOLS = (
     "idc_ctx_create", "idc_ctx_destroy", "idc_set_ordinates", "idc_set_sigma", "idc_sweep", "idc_pmv",
     "idc_smv", "idc_lmv", "idc_source_iteration", "idc_strerror", "idc_last_error_message", "idc_last_timing",
     "idc_set_tiling", "idc_sweep_out", "idc_sweep_noalloc", "idc_gmres_solve", "idc_sweep_adjoint",
-    "idc_adjoint_grad", "idc_set_preconditioner",
+    "idc_adjoint_grad", "idc_set_preconditioner", "idc_idc_integrate",
 )
 
 
@@ -87,6 +88,8 @@ def load_library(path: str = LIB_PATH):
     lib.idc_sweep_out.argtypes = [vp, vp, vp, C.c_double, vp, C.c_int, C.c_int]
     lib.idc_sweep_adjoint.argtypes = [vp, vp, vp, C.c_double, vp, C.c_int, C.c_int]
     lib.idc_set_preconditioner.argtypes = [vp, C.c_int, C.c_int32]
+    lib.idc_idc_integrate.argtypes = [vp, vp, vp, C.c_double, C.c_int64, C.c_int32, C.c_int32, C.c_int, C.c_int,
+                                      C.c_double, C.c_int32, C.c_int64, C.c_int, C.c_int, C.POINTER(C.c_int64)]
     lib.idc_adjoint_grad.argtypes = [vp, vp, vp, C.c_double, C.c_double, C.c_int32, C.c_int64, C.c_int, vp, vp, vp,
                                      C.c_int, C.POINTER(C.c_int64), _dp]
     lib.idc_gmres_solve.argtypes = [vp, vp, C.c_double, C.c_double, C.c_int32, C.c_int64, C.c_int, C.c_int,
@@ -214,6 +217,16 @@ class SweepContext:
                                          int(max_its), int(precision), loc, C.byref(its), C.byref(res)),
                "idc_gmres_solve")
         return int(its.value), float(res.value)
+
+    def idc_integrate(self, psi, source, dt, steps, num_nodes=4, num_corrections=3, scattering=SCATTER_EXPLICIT,
+                      precision=PREC_FP64, abs_tol=1e-12, restart=30, max_its=2000, use_graph=True, loc=LOC_HOST):
+        """In place: psi <- psi after `steps` IDC steps of size dt with the constant source.  Returns sweeps."""
+        sw = C.c_int64()
+        _check(self._lib.idc_idc_integrate(self._h, _ptr(psi, loc), _ptr(source, loc), float(dt), int(steps),
+                                           int(num_nodes), int(num_corrections), int(scattering), int(precision),
+                                           float(abs_tol), int(restart), int(max_its), int(bool(use_graph)), loc,
+                                           C.byref(sw)), "idc_idc_integrate")
+        return int(sw.value)
 
     def set_preconditioner(self, kind: int, inner_steps: int = 30):
         """Right preconditioner of gmres_solve: PRECOND_NONE or PRECOND_DSA (inner_steps CG steps)."""

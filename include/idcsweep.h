@@ -169,6 +169,25 @@ int idc_gmres_solve(idc_ctx *ctx, double *source_inout, double dt, double abs_to
  * depend on the preconditioner. */
 int idc_set_preconditioner(idc_ctx *ctx, int kind, int32_t inner_steps);
 
+/* ---- time integration ------------------------------------------------------------------------------- */
+
+enum { IDC_SCATTER_EXPLICIT = 0, IDC_SCATTER_IMPLICIT = 1 };
+
+/* IDC time integration of d psi/dt = -(L - S P) psi + q: `steps` steps of size dt from psi_inout (its ghost
+ * cells are the inflow values of the initial state) with `source` q constant in time (its ghost cells are
+ * the inflow values during the steps).  num_nodes Gauss-Lobatto nodes, num_corrections corrections,
+ * non-hybrid update form: IDCIntegrator::Step_Nonhybrid, ComputeResiduals, ComputeSource
+ * (time_integrators/RKDG/idc.cpp:846-955, 1657-1740) and SetNodes (:2305-2381).
+ * scattering = IDC_SCATTER_IMPLICIT: every substep solves (1/(h dt) + L - S P) with the GPU GMRES
+ * (abs_tol, restart, max_its), as the reference does with its implicit solver.
+ * scattering = IDC_SCATTER_EXPLICIT (IMEX): every substep is one sweep with the scattering lagged to the
+ * previous node and corrected by the deferred-correction iterations; with use_graph a step is captured
+ * once as a CUDA graph and replayed.  Quadrature sums and residuals are FP64; `precision` selects the
+ * sweep arithmetic.  *sweeps receives the number of sweeps performed. */
+int idc_idc_integrate(idc_ctx *ctx, double *psi_inout, const double *source, double dt, int64_t steps,
+                      int32_t num_nodes, int32_t num_corrections, int scattering, int precision, double abs_tol,
+                      int32_t restart, int64_t max_its, int use_graph, int loc, int64_t *sweeps);
+
 /* ---- discrete adjoint --------------------------------------------------------------------------------- */
 
 /* Transposed sweep: result = L^{-T} source on interior cells, where L^{-1} is the sweep of idc_sweep_out

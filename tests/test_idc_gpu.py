@@ -1,0 +1,85 @@
+"""IDC time stepping on the GPU against the restated reference IDC (tests/idc_ref.py) on the oracle's
+operators, graph replay against plain launches, and the temporal order of accuracy."""
+import numpy as np
+import pytest
+
+from conftest import rel_err, to_oracle
+from idc_ref import idc_steps
+from idcsweep import abi
+from idcsweep.problems import lattice, random_problem
+
+pytestmark = pytest.mark.gpu
+
+
+def context_for(P):
+    ctx = abi.SweepContext(P.nx, P.ny, P.p, P.ax, P.bx, P.ay, P.by)
+    ctx.set_ordinates(P.xi, P.eta, P.w, P.quad)
+    ctx.set_sigma(P.sigma_t, P.sigma_s)
+    return ctx
+
+
+def _problem(n=10, p=1):
+    P = lattice(n, p, 4, dt=0.01)
+    psi0 = np.zeros(P.psi_shape())
+    return P, psi0
+
+
+@pytest.mark.parametrize("use_graph", [False, True])
+@pytest.mark.parametrize("prec,tol", [(abi.PREC_FP64, 1e-12), (abi.PREC_FP32_REFINED, 1e-9)])
+def test_imex_idc_matches_restated_reference(restatement, use_graph, prec, tol):
+    P, psi0 = _problem()
+    want = idc_steps(restatement, to_oracle(P), psi0, P.source, P.dt, 3, M=4, K=3, scattering="explicit")
+    with context_for(P) as ctx:
+        psi = psi0.copy()
+        sweeps = ctx.idc_integrate(psi, P.source, P.dt, 3, 4, 3, abi.SCATTER_EXPLICIT, prec, use_graph=use_graph)
+    assert sweeps == 3 * 3 * 4
+    assert rel_err(psi[1:-1, 1:-1], want[1:-1, 1:-1]) < tol
+
+
+def test_implicit_idc_matches_restated_reference(restatement):
+    P, psi0 = _problem(n=8)
+    want = idc_steps(restatement, to_oracle(P), psi0, P.source, P.dt, 2, M=3, K=2, scattering="implicit")
+    with context_for(P) as ctx:
+        psi = psi0.copy()
+        ctx.idc_integrate(psi, P.source, P.dt, 2, 3, 2, abi.SCATTER_IMPLICIT, abi.PREC_FP64, abs_tol=1e-14)
+    assert rel_err(psi[1:-1, 1:-1], want[1:-1, 1:-1]) < 1e-10
+
+
+def test_graph_replay_is_bitwise_plain_launches():
+    P = lattice(32, 1, 8, dt=0.005)
+    out = []
+    for g in (False, True):
+        with context_for(P) as ctx:
+            psi = np.zeros(P.psi_shape())
+            ctx.idc_integrate(psi, P.source, P.dt, 5, 4, 3, abi.SCATTER_EXPLICIT, abi.PREC_FP64, use_graph=g)
+            out.append(psi)
+    assert np.array_equal(out[0], out[1])
+
+
+@pytest.mark.parametrize("scattering", [abi.SCATTER_EXPLICIT, abi.SCATTER_IMPLICIT])
+def test_idc_fourth_order_in_time(scattering):
+    """4 Lobatto nodes + 3 corrections: the error at T against a 16x finer run falls ~16x per halving of dt."""
+    P = random_problem(4, 4, 1, 4, seed=9, inflow=True, sigma_range=(0.5, 2.0))
+    T = 0.4
+    src = P.source.copy()
+    psi0 = P.source.copy()   # ghost cells: the same inflow as the source (no jump in time at t = 0)
+    psi0[1:-1, 1:-1] = 0.1
+    sols = {}
+    with context_for(P) as ctx:
+        for m in (2, 4, 8, 64):
+            psi = psi0.copy()
+            ctx.idc_integrate(psi, src, T / m, m, 4, 3, scattering, abi.PREC_FP64, abs_tol=1e-14)
+            sols[m] = psi[1:-1, 1:-1]
+    e = [np.abs(sols[m] - sols[64]).max() for m in (2, 4, 8)]
+    orders = [np.log2(e[k] / e[k + 1]) for k in range(2)]
+    assert orders[-1] > 3.5 and min(orders) > 3.0, (e, orders)
+
+
+def test_idc_rejects_bad_arguments():
+    P, psi0 = _problem(n=6)
+    with context_for(P) as ctx:
+        for kw in ({"dt": np.inf}, {"num_nodes": 1}, {"scattering": 5}):
+            args = dict(dt=P.dt, num_nodes=4, scattering=abi.SCATTER_EXPLICIT)
+            args.update(kw)
+            with pytest.raises(abi.IdcError):
+                ctx.idc_integrate(psi0.copy(), P.source, args["dt"], 1, args["num_nodes"], 3, args["scattering"])
