@@ -40,7 +40,8 @@ EXPORTED_SYMBOLS = (
     "idc_ctx_create", "idc_ctx_destroy", "idc_set_ordinates", "idc_set_sigma", "idc_sweep", "idc_pmv",
     "idc_smv", "idc_lmv", "idc_source_iteration", "idc_strerror", "idc_last_error_message", "idc_last_timing",
     "idc_set_tiling", "idc_sweep_out", "idc_sweep_noalloc", "idc_gmres_solve", "idc_sweep_adjoint",
-    "idc_adjoint_grad", "idc_set_preconditioner", "idc_idc_integrate",
+    "idc_adjoint_grad", "idc_set_preconditioner", "idc_idc_integrate", "idc_write_sd2", "idc_read_sd2",
+    "idc_write_af2", "idc_read_af2",
 )
 
 

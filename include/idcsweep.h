@@ -212,6 +212,25 @@ int idc_adjoint_grad(idc_ctx *ctx, const double *psi, const double *detector, do
                      int32_t restart, int64_t max_its, int precision, double *dsigma_t, double *dsigma_s,
                      double *dsource, int loc, int64_t *iters, double *final_resid);
 
+/* ---- binary files ------------------------------------------------------------------------------------ */
+
+/* The reference's serial 2-D binary formats, on the halo layouts of this ABI (no GPU involved).
+ * .sd2 (scalar flux): SpatialDomain::WriteToDisk (objects/SpatialDomain.cpp:385-411) then
+ * DensityFunction::WriteToDisk (objects/RKDG/DensityFunction.cpp:2228-2400): [nx ax bx][ny ay by],
+ * dg_degree, byte size, count, density.  .af2 (angular flux): OrdinateFlux::WriteToDisk and ReadFromDisk
+ * (objects/RKDG/OrdinateFlux.cpp:2553-2620, 2720-2930): the domain block, the ordinate type name
+ * (null-terminated, "#R" appended for symmetric-reduced sets) and ang_order, then dg_degree, byte size,
+ * count, density.  Readers with density == NULL return the header only; `count` is the number of doubles. */
+int idc_write_sd2(const char *path, int64_t nx, int64_t ny, double ax, double bx, double ay, double by,
+                  int64_t dg_degree, const double *density);
+int idc_read_sd2(const char *path, int64_t *nx, int64_t *ny, double *ax, double *bx, double *ay, double *by,
+                 int64_t *dg_degree, double *density, int64_t capacity, int64_t *count);
+int idc_write_af2(const char *path, int64_t nx, int64_t ny, double ax, double bx, double ay, double by,
+                  const char *ordinate_type, int64_t ang_order, int64_t dg_degree, int64_t nq, const double *density);
+int idc_read_af2(const char *path, int64_t *nx, int64_t *ny, double *ax, double *bx, double *ay, double *by,
+                 char *ordinate_type, int64_t type_capacity, int64_t *ang_order, int64_t *dg_degree, double *density,
+                 int64_t capacity, int64_t *count);
+
 /* ---- diagnostics ----------------------------------------------------------------------------------- */
 
 /* Text for a status code (static storage). */

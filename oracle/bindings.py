@@ -156,7 +156,10 @@ class Reference:
         lib.ref_smv.argtypes = [C.c_void_p, C.c_double, C.c_double, _dp, _dp]
         lib.ref_lmv.argtypes = [C.c_void_p, C.c_double, C.c_double, _dp, _dp]
         lib.ref_si_solve.argtypes = [C.c_void_p, _dp, C.c_double, C.POINTER(C.c_int64), _dp]
-        for f in ("ref_apply", "ref_apply_timed", "ref_pmv", "ref_smv", "ref_lmv", "ref_si_solve"):
+        lib.ref_write_sd.argtypes = [C.c_void_p, _dp, C.c_char_p]
+        lib.ref_write_af.argtypes = [C.c_void_p, _dp, C.c_char_p]
+        for f in ("ref_apply", "ref_apply_timed", "ref_pmv", "ref_smv", "ref_lmv", "ref_si_solve", "ref_write_sd",
+                  "ref_write_af"):
             getattr(lib, f).restype = C.c_int
         self.lib = lib
 
@@ -210,6 +213,14 @@ class _RefHandle:
         out = np.zeros(self.P.psi_shape()) if y is None else np.ascontiguousarray(y, np.float64).copy()
         assert self.lib.ref_lmv(self.h, alpha, beta, _p(np.ascontiguousarray(x, np.float64)), _p(out)) == 0
         return out
+
+    def write_sd(self, phi, path: str):
+        """The reference's DensityFunction::WriteToDisk of phi (halo layout)."""
+        assert self.lib.ref_write_sd(self.h, _p(np.ascontiguousarray(phi, np.float64)), path.encode()) == 0
+
+    def write_af(self, psi, path: str):
+        """The reference's OrdinateFlux::WriteToDisk of psi (halo layout)."""
+        assert self.lib.ref_write_af(self.h, _p(np.ascontiguousarray(psi, np.float64)), path.encode()) == 0
 
     def source_iteration(self, source, dt=np.inf):
         psi = np.ascontiguousarray(source, np.float64).copy()

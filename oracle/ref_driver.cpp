@@ -255,4 +255,26 @@ int ref_si_solve ( void * h, double * source_inout, double dt, int64_t * iters, 
     } catch ( std::exception & e ) { std::fprintf( stderr, "ref_si_solve: %s\n", e.what() ); return 1; }
 }
 
+// DensityFunction::WriteToDisk (objects/RKDG/DensityFunction.cpp:2228-2400) of a scalar flux given on the
+// halo layout: the reference's .sd2 file.
+int ref_write_sd ( void * h, const double * phi, const char * path ) {
+    auto * P = static_cast<RefProblem *>(h);
+    try {
+        CopyIn( *P->phi, phi, P->phi_len() );
+        P->phi->WriteToDisk( std::string( path ) );
+        return 0;
+    } catch ( std::exception & e ) { std::fprintf( stderr, "ref_write_sd: %s\n", e.what() ); return 1; }
+}
+
+// OrdinateFlux::WriteToDisk (objects/RKDG/OrdinateFlux.cpp:2720-2930) of an angular flux given on the halo
+// layout: the reference's .af2 file.
+int ref_write_af ( void * h, const double * psi, const char * path ) {
+    auto * P = static_cast<RefProblem *>(h);
+    try {
+        CopyIn( *P->psi, psi, P->psi_len() );
+        P->psi->WriteToDisk( std::string( path ) );
+        return 0;
+    } catch ( std::exception & e ) { std::fprintf( stderr, "ref_write_af: %s\n", e.what() ); return 1; }
+}
+
 } // extern "C"
