@@ -358,6 +358,22 @@ int idc_idc_integrate(idc_ctx *ctx, double *psi_inout, const double *source, dou
     ABI_GUARD_END
 }
 
+int idc_sweep_fused(idc_ctx *ctx, const double *source, double *result, double dt, const double *phi_scatter,
+                    double scatter_scale, double *phi_out, int precision, int loc) {
+    ABI_GUARD_BEGIN
+    if (!ctx) return fail(IDC_ERR_ARG, "idc_sweep_fused: null context");
+    if (loc != IDC_LOC_DEVICE) return fail(IDC_ERR_ARG, "idc_sweep_fused takes device pointers only");
+    idc::Context &c = ctx->impl;
+    ABI_TRY_CUDA(cudaSetDevice(c.device));
+    c.launches = 0;
+    ABI_TRY(c.sweep(source, result, dt, phi_out, precision, phi_scatter, scatter_scale));
+    ABI_TRY(c.check_device_error());
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, c.ev0, c.ev1) == cudaSuccess) c.last_sweep_ms = ms;
+    return IDC_OK;
+    ABI_GUARD_END
+}
+
 int idc_sweep_adjoint(idc_ctx *ctx, const double *source, double *result, double dt, double *moments_out, int precision,
                       int loc) {
     ABI_GUARD_BEGIN

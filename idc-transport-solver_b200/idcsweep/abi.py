@@ -41,7 +41,7 @@ EXPORTED_SYMBOLS = (
     "idc_smv", "idc_lmv", "idc_source_iteration", "idc_strerror", "idc_last_error_message", "idc_last_timing",
     "idc_set_tiling", "idc_sweep_out", "idc_sweep_noalloc", "idc_gmres_solve", "idc_sweep_adjoint",
     "idc_adjoint_grad", "idc_set_preconditioner", "idc_idc_integrate", "idc_write_sd2", "idc_read_sd2",
-    "idc_write_af2", "idc_read_af2",
+    "idc_write_af2", "idc_read_af2", "idc_sweep_fused",
 )
 
 
@@ -89,6 +89,7 @@ def load_library(path: str = LIB_PATH):
     lib.idc_sweep_out.argtypes = [vp, vp, vp, C.c_double, vp, C.c_int, C.c_int]
     lib.idc_sweep_adjoint.argtypes = [vp, vp, vp, C.c_double, vp, C.c_int, C.c_int]
     lib.idc_set_preconditioner.argtypes = [vp, C.c_int, C.c_int32]
+    lib.idc_sweep_fused.argtypes = [vp, vp, vp, C.c_double, vp, C.c_double, vp, C.c_int, C.c_int]
     lib.idc_idc_integrate.argtypes = [vp, vp, vp, C.c_double, C.c_int64, C.c_int32, C.c_int32, C.c_int, C.c_int,
                                       C.c_double, C.c_int32, C.c_int64, C.c_int, C.c_int, C.POINTER(C.c_int64)]
     lib.idc_adjoint_grad.argtypes = [vp, vp, vp, C.c_double, C.c_double, C.c_int32, C.c_int64, C.c_int, vp, vp, vp,
@@ -228,6 +229,13 @@ class SweepContext:
                                            float(abs_tol), int(restart), int(max_its), int(bool(use_graph)), loc,
                                            C.byref(sw)), "idc_idc_integrate")
         return int(sw.value)
+
+    def sweep_fused(self, source_ptr, result_ptr, dt, phi_scatter_ptr, scatter_scale, phi_ptr, precision=PREC_FP64):
+        """Device pointers (int or None): result <- L^{-1}(source + scale S phi_scatter), phi <- P result."""
+        v = lambda x: None if x is None else C.c_void_p(int(x))
+        _check(self._lib.idc_sweep_fused(self._h, v(source_ptr), v(result_ptr), float(dt), v(phi_scatter_ptr),
+                                         float(scatter_scale), v(phi_ptr), int(precision), LOC_DEVICE),
+               "idc_sweep_fused")
 
     def set_preconditioner(self, kind: int, inner_steps: int = 30):
         """Right preconditioner of gmres_solve: PRECOND_NONE or PRECOND_DSA (inner_steps CG steps)."""

@@ -188,6 +188,15 @@ int idc_idc_integrate(idc_ctx *ctx, double *psi_inout, const double *source, dou
                       int32_t num_nodes, int32_t num_corrections, int scattering, int precision, double abs_tol,
                       int32_t restart, int64_t max_its, int use_graph, int loc, int64_t *sweeps);
 
+/* Out-of-place sweep with the fused isotropic scattering source: result = L^{-1}(source +
+ * scatter_scale * sigma_s * phi_scatter / (4 pi)) on interior cells, phi_out = P result.  source may be
+ * NULL (zero source, vacuum inflow), result may be NULL (not stored), phi_scatter may be NULL (no
+ * scattering term); DEVICE pointers only (loc must be IDC_LOC_DEVICE).  The fused form of
+ * SISolver::Solve's per-iteration Smv + Apply + Pmv (linear_solvers/Abstract/ImplicitSolver/SISolver.cpp:
+ * 190-254) for callers that drive their own iteration, e.g. across GPUs holding disjoint ordinate sets. */
+int idc_sweep_fused(idc_ctx *ctx, const double *source, double *result, double dt, const double *phi_scatter,
+                    double scatter_scale, double *phi_out, int precision, int loc);
+
 /* ---- discrete adjoint --------------------------------------------------------------------------------- */
 
 /* Transposed sweep: result = L^{-T} source on interior cells, where L^{-1} is the sweep of idc_sweep_out
