@@ -1,5 +1,6 @@
 // The extern "C" boundary declared in include/idcsweep.h: argument checks, host <-> device staging,
 // status codes.  Nothing here throws across the boundary.
+#include "batch.hpp"
 #include "context.hpp"
 #include "idcsweep.h"
 
@@ -7,6 +8,10 @@
 #include <cstring>
 #include <new>
 #include <string>
+
+struct idc_batch {
+    idc::Batch impl;
+};
 
 struct idc_ctx {
     idc::Context impl;
@@ -372,6 +377,72 @@ int idc_sweep_fused(idc_ctx *ctx, const double *source, double *result, double d
     if (cudaEventElapsedTime(&ms, c.ev0, c.ev1) == cudaSuccess) c.last_sweep_ms = ms;
     return IDC_OK;
     ABI_GUARD_END
+}
+
+int idc_set_tile_shape(idc_ctx *ctx, int32_t seg, int32_t warps) {
+    ABI_GUARD_BEGIN
+    if (!ctx) return fail(IDC_ERR_ARG, "null context");
+    ABI_TRY(ctx->impl.set_tile_shape(seg, warps));
+    return IDC_OK;
+    ABI_GUARD_END
+}
+
+int idc_autotune(idc_ctx *ctx, const double *source, double dt, int precision, int32_t *seg, int32_t *warps) {
+    ABI_GUARD_BEGIN
+    if (!ctx || !source) return fail(IDC_ERR_ARG, "idc_autotune: null argument");
+    idc::Context &c = ctx->impl;
+    ABI_TRY_CUDA(cudaSetDevice(c.device));
+    int s = 0, w = 0;
+    ABI_TRY(c.autotune(source, dt, precision, &s, &w));
+    if (seg) *seg = s;
+    if (warps) *warps = w;
+    return IDC_OK;
+    ABI_GUARD_END
+}
+
+int idc_batch_create(idc_batch **out) {
+    ABI_GUARD_BEGIN
+    if (!out) return fail(IDC_ERR_ARG, "idc_batch_create: null argument");
+    *out = new (std::nothrow) idc_batch();
+    if (!*out) return fail(IDC_ERR_NOMEM, "idc_batch_create: out of host memory");
+    return IDC_OK;
+    ABI_GUARD_END
+}
+
+int idc_batch_add(idc_batch *b, idc_ctx *ctx) {
+    ABI_GUARD_BEGIN
+    if (!b || !ctx) return fail(IDC_ERR_ARG, "idc_batch_add: null argument");
+    ABI_TRY(b->impl.add(&ctx->impl));
+    return IDC_OK;
+    ABI_GUARD_END
+}
+
+int idc_batch_sweep(idc_batch *b, const double *const *sources, double *const *results, double *const *phi_out,
+                    double dt, int precision) {
+    ABI_GUARD_BEGIN
+    if (!b) return fail(IDC_ERR_ARG, "idc_batch_sweep: null batch");
+    ABI_TRY(b->impl.sweep(sources, results, nullptr, 1.0, phi_out, dt, precision));
+    return IDC_OK;
+    ABI_GUARD_END
+}
+
+int idc_batch_autotune(idc_batch *b, const double *const *sources, double *const *results, double dt, int precision) {
+    ABI_GUARD_BEGIN
+    if (!b) return fail(IDC_ERR_ARG, "idc_batch_autotune: null batch");
+    ABI_TRY(b->impl.autotune(sources, results, dt, precision));
+    return IDC_OK;
+    ABI_GUARD_END
+}
+
+int idc_batch_last_timing(idc_batch *b, double *ms) {
+    if (!b) return fail(IDC_ERR_ARG, "null batch");
+    if (ms) *ms = b->impl.last_ms;
+    return IDC_OK;
+}
+
+int idc_batch_destroy(idc_batch *b) {
+    delete b;
+    return IDC_OK;
 }
 
 int idc_sweep_adjoint(idc_ctx *ctx, const double *source, double *result, double dt, double *moments_out, int precision,

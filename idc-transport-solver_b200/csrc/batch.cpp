@@ -1,0 +1,292 @@
+// Batched sweeps: several independent problems (contexts on one GPU) in one persistent launch per DG
+// degree, and the tile-shape autotuner for a batch.
+//
+// The problems of a degree share the launch's tile shape (row-segment width seg, compute warps wn) and
+// item queue.  Each problem keeps its own arrays, chunks its quadrants' ordinates by seg, and gets its
+// own trace buffer, partial-moment slots and inflow traces; its descriptor (a SweepArgs)
+// sits in a device table that the kernel reads per item.  Row blocks of all problems are interleaved in
+// the queue (row block 0 of every problem, then row block 1, ...), so every problem's wavefront starts at
+// once and every dependency is dequeued before its consumer.
+#include "batch.hpp"
+
+#include <algorithm>
+#include <cmath>
+
+namespace idc {
+
+#define IDC_TRY_CUDA(expr)                                    \
+    do {                                                      \
+        cudaError_t e_ = (expr);                              \
+        if (e_ != cudaSuccess) return cuda_status(e_, #expr); \
+    } while (0)
+
+#define IDC_TRY(expr)              \
+    do {                           \
+        Status s_ = (expr);        \
+        if (!s_.good()) return s_; \
+    } while (0)
+
+namespace {
+
+Status bad(int code, const std::string &m) {
+    Status s;
+    s.code = code;
+    s.msg = m;
+    return s;
+}
+
+// Default shape: the widest segment whose lane use is within 10 points of the best (fewer chunks and
+// items), 7 compute warps.
+void default_shape(int qmax, int *seg, int *wn) {
+    double best = -1.0;
+    for (int cand : {32, 16, 8, 4}) {
+        const int nch = (qmax + cand - 1) / cand;
+        const double eff = (double)qmax / (nch * cand);
+        if (eff > best + 0.1) {
+            best = eff;
+            *seg = cand;
+        }
+    }
+    *wn = 7;
+}
+
+int qmax_of(const Context &c) {
+    int q = 0;
+    for (int k = 0; k < 4; ++k) q = std::max<int>(q, (int)(c.quad[k + 1] - c.quad[k]));
+    return q;
+}
+
+}  // namespace
+
+Batch::~Batch() { release(); }
+
+void Batch::release() {
+    for (auto &g : groups) {
+        cudaFree(g.d_items);
+        cudaFree(g.d_sync);
+        cudaFree(g.d_table);
+        for (double *p : g.trace) cudaFree(p);
+        for (double *p : g.phi_part) cudaFree(p);
+        for (double *p : g.inflow) cudaFree(p);
+    }
+    groups.clear();
+}
+
+Status Batch::add(Context *c) {
+    if (!c) return bad(IDC_ERR_ARG, "null context");
+    if (!c->have_ordinates || !c->have_sigma) return bad(IDC_ERR_STATE, "batch member without ordinates or sigma");
+    if (c->kernel != Context::kModal) return bad(IDC_ERR_UNSUPPORTED, "batched sweeps need the modal kernel");
+    if (!members.empty() && c->device != members[0]->device) return bad(IDC_ERR_ARG, "batch members on different GPUs");
+    members.push_back(c);
+    release();
+    return Status::ok();
+}
+
+Status Batch::build_group(Group &g, int precision) {
+    Context &c0 = *members[g.members[0]];
+    const int seg = g.seg, wn = g.wn, rw = 32 / seg, rows_cta = wn * rw;
+    g.G = seg;
+    std::vector<std::vector<SweepItem>> per(g.members.size());
+    std::vector<int> nrb(g.members.size()), ipr(g.members.size());
+    for (size_t m = 0; m < g.members.size(); ++m) {
+        const Context &c = *members[g.members[m]];
+        // chunks of each quadrant (near-equal, at most seg ordinates)
+        std::vector<int> qk, qb, qc;
+        for (int k = 0; k < 4; ++k) {
+            const int cnt = (int)(c.quad[k + 1] - c.quad[k]);
+            if (!cnt) continue;
+            const int nch = (cnt + seg - 1) / seg;
+            int beg = (int)c.quad[k];
+            for (int h = 0; h < nch; ++h) {
+                const int sz = cnt / nch + (h < cnt % nch ? 1 : 0);
+                qk.push_back(k);
+                qb.push_back(beg);
+                qc.push_back(sz);
+                beg += sz;
+            }
+        }
+        ipr[m] = (int)qk.size();
+        nrb[m] = (int)((c.ny + rows_cta - 1) / rows_cta);
+        for (int rb = 0; rb < nrb[m]; ++rb)
+            for (int s = 0; s < ipr[m]; ++s)
+                per[m].push_back(
+                    SweepItem{qk[s], qb[s], qc[s], rb, rb == 0 ? -1 : (rb - 1) * ipr[m] + s, (int)m, rb * ipr[m] + s});
+    }
+    // interleave row blocks (items keep their problem-local index and local dependency)
+    std::vector<SweepItem> items;
+    const int max_rb = *std::max_element(nrb.begin(), nrb.end());
+    for (int rb = 0; rb < max_rb; ++rb)
+        for (size_t m = 0; m < g.members.size(); ++m)
+            if (rb < nrb[m])
+                for (int s = 0; s < ipr[m]; ++s) items.push_back(per[m][(size_t)rb * ipr[m] + s]);
+    g.n_items = (int)items.size();
+    g.items_per_rb = ipr;
+    IDC_TRY_CUDA(cudaSetDevice(c0.device));
+    IDC_TRY_CUDA(cudaMalloc(&g.d_items, sizeof(SweepItem) * items.size()));
+    IDC_TRY_CUDA(cudaMemcpy(g.d_items, items.data(), sizeof(SweepItem) * items.size(), cudaMemcpyHostToDevice));
+    IDC_TRY_CUDA(cudaMalloc(&g.d_sync, sizeof(int) * 2));
+    IDC_TRY_CUDA(cudaMemset(g.d_sync, 0, sizeof(int) * 2));
+    IDC_TRY_CUDA(cudaMalloc(&g.d_table, sizeof(SweepArgs) * g.members.size()));
+    g.trace.assign(g.members.size(), nullptr);
+    g.trace_len.assign(g.members.size(), 0);
+    g.phi_part.assign(g.members.size(), nullptr);
+    g.inflow.assign(g.members.size(), nullptr);
+    for (size_t m = 0; m < g.members.size(); ++m) {
+        const Context &c = *members[g.members[m]];
+        const size_t tl = per[m].size() * (size_t)c.nx * g.G * c.P;   // one trace row per item of the member
+        IDC_TRY_CUDA(cudaMalloc(&g.trace[m], sizeof(double) * tl));
+        g.trace_len[m] = tl;
+        IDC_TRY_CUDA(launch_fill_u64(reinterpret_cast<unsigned long long *>(g.trace[m]), tl, kTraceSentinel, c0.stream));
+        IDC_TRY_CUDA(cudaMalloc(&g.phi_part[m], sizeof(double) * (size_t)ipr[m] * c.phi_len()));
+        IDC_TRY_CUDA(cudaMalloc(&g.inflow[m], sizeof(double) * (size_t)(c.nx + c.ny) * c.nq * c.P));
+    }
+    int per_sm = 0;
+    g.smem = sweep_modal_smem_bytes(c0.P, wn, g.G, seg);
+    IDC_TRY_CUDA(sweep_modal_occupancy(c0.P, precision, seg, (wn + 1) * 32, g.smem, &per_sm));
+    if (per_sm < 1) return bad(IDC_ERR_UNSUPPORTED, "batched sweep kernel does not fit on an SM");
+    g.grid = std::min(g.n_items, per_sm * c0.num_sms);
+    g.precision = precision;
+    IDC_TRY_CUDA(cudaStreamSynchronize(c0.stream));
+    return Status::ok();
+}
+
+Status Batch::launch_group(Group &g, const double *const *srcs, double *const *outs, const double *const *phi_sc,
+                           double scale, double *const *phis, double dt) {
+    Context &c0 = *members[g.members[0]];
+    cudaStream_t st = c0.stream;
+    std::vector<SweepArgs> table(g.members.size());
+    for (size_t m = 0; m < g.members.size(); ++m) {
+        const int p = g.members[m];
+        Context &c = *members[p];
+        SweepArgs &a = table[m];
+        a = SweepArgs{};
+        a.src = srcs ? srcs[p] : nullptr;
+        a.out = outs ? outs[p] : nullptr;
+        a.sigma_t = c.d_sigma_t;
+        a.sigma_s = c.d_sigma_s;
+        a.phi_scatter = phi_sc ? phi_sc[p] : nullptr;
+        a.scatter_scale = scale;
+        a.xi = c.d_xi;
+        a.eta = c.d_eta;
+        a.w = c.d_w;
+        a.nx = (int)c.nx;
+        a.ny = (int)c.ny;
+        a.nq = (int)c.nq;
+        a.dx = c.dx;
+        a.dy = c.dy;
+        a.inv_dt = 1.0 / dt;
+        a.items = g.d_items;
+        a.n_items = g.n_items;
+        a.G = g.G;
+        a.n_refine = 1;
+        a.seg = g.seg;
+        a.wn = g.wn;
+        a.R = g.wn * (32 / g.seg);
+        a.trace = g.trace[m];
+        a.trace_stride = (size_t)c.nx * g.G * c.P;
+        a.next_item = g.d_sync;
+        a.error = g.d_sync + 1;
+        a.spin_limit = c.spin_limit;
+        if (phis && phis[p]) {
+            a.phi_part = g.phi_part[m];
+            a.phi_slots = g.items_per_rb[m];
+            a.phi_slot_stride = c.phi_len();
+        }
+        if (a.src) {
+            IDC_TRY_CUDA(launch_inflow_traces(c.P, g.precision != IDC_PREC_FP32_REFINED, a.src, c.d_xi, c.d_eta, (int)c.nx,
+                                              (int)c.ny, (int)c.nq, g.inflow[m], st));
+            a.inflow = g.inflow[m];
+        }
+    }
+    SweepArgs launch = table[0];   // the launch-wide fields (items, queue, error, tile shape) are common
+    IDC_TRY_CUDA(cudaMemcpyAsync(g.d_table, table.data(), sizeof(SweepArgs) * table.size(), cudaMemcpyHostToDevice, st));
+    IDC_TRY_CUDA(cudaMemsetAsync(g.d_sync, 0, sizeof(int), st));
+    IDC_TRY_CUDA(launch_sweep_modal_batched(c0.P, g.precision, launch, g.d_table, g.grid, g.smem, st));
+    for (size_t m = 0; m < g.members.size(); ++m) {
+        const int p = g.members[m];
+        if (phis && phis[p]) {
+            Context &c = *members[p];
+            IDC_TRY_CUDA(launch_reduce_phi_partials(c.dims(), g.phi_part[m], g.items_per_rb[m], c.phi_len(), phis[p], st));
+        }
+    }
+    return Status::ok();
+}
+
+Status Batch::sweep(const double *const *srcs, double *const *outs, const double *const *phi_sc, double scale,
+                    double *const *phis, double dt, int precision) {
+    if (members.empty()) return bad(IDC_ERR_STATE, "empty batch");
+    if (precision != IDC_PREC_FP64 && precision != IDC_PREC_FP32_REFINED)
+        return bad(IDC_ERR_UNSUPPORTED, "batched sweeps run in FP64 or refined precision");
+    if (!(dt > 0)) return bad(IDC_ERR_ARG, "dt must be positive");
+    Context &c0 = *members[0];
+    IDC_TRY_CUDA(cudaSetDevice(c0.device));
+    if (groups.empty() || groups[0].precision != precision) {
+        release();
+        for (int P : {1, 2, 3}) {
+            Group g;
+            for (size_t m = 0; m < members.size(); ++m)
+                if (members[m]->P == P) g.members.push_back((int)m);
+            if (g.members.empty()) continue;
+            g.P = P;
+            int qmax = 0;
+            for (int m : g.members) qmax = std::max(qmax, qmax_of(*members[m]));
+            const auto key = std::make_pair(P, precision);
+            if (tuned.count(key)) {
+                g.seg = tuned[key].first;
+                g.wn = tuned[key].second;
+            } else {
+                default_shape(qmax, &g.seg, &g.wn);
+            }
+            g.precision = precision;
+            groups.push_back(g);
+        }
+        for (auto &g : groups) IDC_TRY(build_group(g, precision));
+    }
+    IDC_TRY_CUDA(cudaEventRecord(c0.ev0, c0.stream));
+    for (auto &g : groups) IDC_TRY(launch_group(g, srcs, outs, phi_sc, scale, phis, dt));
+    IDC_TRY_CUDA(cudaEventRecord(c0.ev1, c0.stream));
+    IDC_TRY_CUDA(cudaStreamSynchronize(c0.stream));
+    for (auto &g : groups) {
+        int err = 0;
+        IDC_TRY_CUDA(cudaMemcpy(&err, g.d_sync + 1, sizeof(int), cudaMemcpyDeviceToHost));
+        if (err != kDevOk) {
+            IDC_TRY_CUDA(cudaMemset(g.d_sync + 1, 0, sizeof(int)));
+            for (size_t m = 0; m < g.members.size(); ++m)
+                IDC_TRY_CUDA(launch_fill_u64(reinterpret_cast<unsigned long long *>(g.trace[m]), g.trace_len[m],
+                                             kTraceSentinel, c0.stream));
+            IDC_TRY_CUDA(cudaStreamSynchronize(c0.stream));
+            return bad(IDC_ERR_TIMEOUT, "a device-side wait gave up in a batched sweep");
+        }
+    }
+    float ms = 0.f;
+    IDC_TRY_CUDA(cudaEventElapsedTime(&ms, c0.ev0, c0.ev1));
+    last_ms = ms;
+    return Status::ok();
+}
+
+Status Batch::autotune(const double *const *srcs, double *const *outs, double dt, int precision) {
+    if (members.empty()) return bad(IDC_ERR_STATE, "empty batch");
+    for (int P : {1, 2, 3}) {
+        bool any = false;
+        for (auto *c : members) any |= c->P == P;
+        if (!any) continue;
+        float best = 1e30f;
+        std::pair<int, int> bsh{0, 0};
+        for (int cs : {4, 8, 16, 32})
+            for (int cw : {3, 5, 7}) {
+                tuned[std::make_pair(P, precision)] = {cs, cw};
+                release();
+                for (int rep = 0; rep < 2; ++rep) IDC_TRY(sweep(srcs, outs, nullptr, 1.0, nullptr, dt, precision));
+                // the timing covers every degree's launch; the other degrees' shapes stay fixed meanwhile
+                if (last_ms < best) {
+                    best = last_ms;
+                    bsh = {cs, cw};
+                }
+            }
+        tuned[std::make_pair(P, precision)] = bsh;
+        release();
+    }
+    return Status::ok();
+}
+
+}  // namespace idc

@@ -1,0 +1,45 @@
+// Batched sweeps of independent problems in one persistent launch per DG degree (batch.cpp).
+#pragma once
+
+#include "context.hpp"
+
+#include <map>
+#include <utility>
+#include <vector>
+
+namespace idc {
+
+class Batch {
+public:
+    ~Batch();
+    Status add(Context *c);
+    // per problem p (arrays indexed like `members`, entries nullable): outs[p] <- L^{-1}(srcs[p] +
+    // scale S phi_sc[p]), phis[p] <- P outs[p]; device pointers
+    Status sweep(const double *const *srcs, double *const *outs, const double *const *phi_sc, double scale,
+                 double *const *phis, double dt, int precision);
+    // times the candidate tile shapes per degree on the given inputs and keeps the fastest
+    Status autotune(const double *const *srcs, double *const *outs, double dt, int precision);
+
+    std::vector<Context *> members;
+    std::map<std::pair<int, int>, std::pair<int, int>> tuned;   // (P, precision) -> (seg, wn)
+    float last_ms = 0.f;
+
+private:
+    struct Group {
+        int P = 0, seg = 0, wn = 0, G = 0, precision = -1, n_items = 0, grid = 0;
+        size_t smem = 0;
+        std::vector<int> members, items_per_rb;
+        SweepItem *d_items = nullptr;
+        int *d_sync = nullptr;
+        SweepArgs *d_table = nullptr;
+        std::vector<double *> trace, phi_part, inflow;
+        std::vector<size_t> trace_len;
+    };
+    Status build_group(Group &g, int precision);
+    Status launch_group(Group &g, const double *const *srcs, double *const *outs, const double *const *phi_sc,
+                        double scale, double *const *phis, double dt);
+    void release();
+    std::vector<Group> groups;
+};
+
+}  // namespace idc

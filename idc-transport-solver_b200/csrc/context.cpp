@@ -149,6 +149,48 @@ Status Context::set_tiling(int G, int R) {
     return Status::ok();
 }
 
+Status Context::set_tile_shape(int s, int w) {
+    if (s == 0 && w == 0) {
+        tune_seg = tune_wn = 0;
+    } else {
+        if ((s != 4 && s != 8 && s != 16 && s != 32) || w < 1 || w > 7)
+            return bad(IDC_ERR_ARG, "tile shape: seg must be 4, 8, 16 or 32 and wn in 1..7");
+        tune_seg = s;
+        tune_wn = w;
+    }
+    n_items = 0;
+    occupancy_precision = -1;
+    return Status::ok();
+}
+
+// Candidate tile shapes, timed with CUDA events on this problem (second of two sweeps each).
+Status Context::autotune(const double *src, double dt, int precision, int *seg_out, int *wn_out) {
+    if (kernel != kModal) return bad(IDC_ERR_UNSUPPORTED, "the autotuner tunes the modal kernel");
+    IDC_TRY(ensure_psi_buffers(1));
+    IDC_TRY(ensure_phi_buffers(1));
+    float best = 1e30f;
+    int bs = 0, bw = 0;
+    for (int cs : {4, 8, 16, 32})
+        for (int cw : {3, 5, 7}) {
+            IDC_TRY(set_tile_shape(cs, cw));
+            float ms = 0.f;
+            for (int rep = 0; rep < 2; ++rep) {
+                IDC_TRY(sweep(src, psi_buf(0), dt, phi_buf(0), precision));
+                IDC_TRY(check_device_error());
+                IDC_TRY_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+            }
+            if (ms < best) {
+                best = ms;
+                bs = cs;
+                bw = cw;
+            }
+        }
+    IDC_TRY(set_tile_shape(bs, bw));
+    if (seg_out) *seg_out = bs;
+    if (wn_out) *wn_out = bw;
+    return Status::ok();
+}
+
 Status Context::ensure_psi_buffers(int count) {
     IDC_TRY_CUDA(cudaSetDevice(device));
     while ((int)psi_bufs_.size() < count) {
@@ -210,7 +252,13 @@ Status Context::build_schedule(int precision) {
     for (int k = 0; k < 4; ++k) qmax = std::max<int>(qmax, (int)(quad[k + 1] - quad[k]));
     if (qmax == 0) return bad(IDC_ERR_ARG, "no ordinates");
     int G = 0, R = 0;
-    if (use_warp_kernel) {
+    if (use_warp_kernel && tune_seg > 0) {
+        seg = tune_seg;
+        wn = tune_wn;
+        const int nch = (qmax + seg - 1) / seg;
+        G = (qmax + nch - 1) / nch;
+        R = wn * (32 / seg);
+    } else if (use_warp_kernel) {
         choose_warp_tiling(qmax, user_G, user_R, 7, &G, &seg, &wn);
         R = wn * (32 / seg);
     } else {

@@ -31,6 +31,11 @@ public:
     Status set_ordinates(int64_t nq, const double *xi, const double *eta, const double *w, const int64_t qb[5]);
     Status set_sigma(const double *sigma_t, const double *sigma_s, int loc);
     Status set_tiling(int G, int R);   // 0 = automatic
+    // fixed tile shape of the modal kernel (segment width seg in {4,8,16,32}, compute warps per CTA wn),
+    // set by the autotuner; 0 = the default heuristic
+    Status set_tile_shape(int seg, int wn);
+    // times the candidate tile shapes on this problem with `src` (device psi array) and keeps the fastest
+    Status autotune(const double *src, double dt, int precision, int *seg_out, int *wn_out);
 
     // ---- operators on device pointers ----
     // Sweep: out <- L^{-1} (src [+ scale * S phi_scatter]); phi (nullable) <- P out.  src may equal out.
@@ -96,6 +101,7 @@ public:
     // sweep schedule
     SweepTiling tiling;
     int user_G = 0, user_R = 0;
+    int tune_seg = 0, tune_wn = 0;
     SweepItem *d_items = nullptr;
     int n_items = 0;
     int *d_sync = nullptr;        // [0] queue head, [1] error word, [2..] progress per item

@@ -25,6 +25,9 @@ struct SweepItem {
     int q_count;
     int row_block;
     int dep;
+    int problem;   // batched modal launch: index into the launch's problem table (0 otherwise)
+    int local;     // batched modal launch: the item's index within its problem (trace buffer and moment
+                   // slot; `dep` is then a local index too)
 };
 
 struct SweepArgs {
@@ -81,6 +84,13 @@ constexpr int kWarpRingSlots = 8;
 
 // Modal sweep kernel (sweep_modal.cu): same arguments as the warp kernel plus `inflow`, traces of P values.
 cudaError_t launch_sweep_modal(int P, int precision, const SweepArgs &args, int grid, size_t smem, cudaStream_t stream);
+// Batched modal launch: one persistent kernel over the items of several problems of the same degree P.
+// `launch` carries the shared item list, queue head, error word and tile shape (G, seg, wn); `table`
+// (device) holds one SweepArgs per problem (its arrays, sizes, trace buffer); items carry their problem
+// and problem-local index.  Forward sweeps,
+// FP64 or refined precision.
+cudaError_t launch_sweep_modal_batched(int P, int precision, const SweepArgs &launch, const SweepArgs *table, int grid,
+                                       size_t smem, cudaStream_t stream);
 cudaError_t sweep_modal_occupancy(int P, int precision, int seg, int threads, size_t smem, int *blocks_per_sm);
 size_t sweep_modal_smem_bytes(int P, int wn, int G, int seg);
 // Inflow traces of the ghost cells of `src` for the modal kernel: out[(k * nq + q) * P + m], k < nx the

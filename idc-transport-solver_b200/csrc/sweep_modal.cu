@@ -7,6 +7,8 @@ IDC_MODAL_LAUNCHERS(extern, 0, true)
 IDC_MODAL_LAUNCHERS(extern, 1, false)
 IDC_MODAL_LAUNCHERS(extern, 1, true)
 IDC_MODAL_LAUNCHERS(extern, 2, false)
+IDC_MODAL_BATCHED(extern, 0)
+IDC_MODAL_BATCHED(extern, 1)
 
 namespace idc {
 
@@ -105,6 +107,18 @@ cudaError_t inflow_t(const double *src, const double *xi, const double *eta, int
     return cudaGetLastError();
 }
 
+template <int P, int MODE>
+cudaError_t launch_batched_t(const SweepArgs &launch, const SweepArgs *table, int grid, size_t smem,
+                             cudaStream_t stream) {
+    switch (launch.seg) {
+        case 4: return modal::launch_seg_batched<P, MODE, 4>(launch, table, grid, smem, stream);
+        case 8: return modal::launch_seg_batched<P, MODE, 8>(launch, table, grid, smem, stream);
+        case 16: return modal::launch_seg_batched<P, MODE, 16>(launch, table, grid, smem, stream);
+        case 32: return modal::launch_seg_batched<P, MODE, 32>(launch, table, grid, smem, stream);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 }  // namespace
 
 size_t sweep_modal_smem_bytes(int P, int wn, int G, int seg) {
@@ -132,6 +146,23 @@ cudaError_t launch_sweep_modal(int P, int precision, const SweepArgs &args, int 
         case 1: IDC_MDISPATCH(1, launch_t, args, grid, smem, stream);
         case 2: IDC_MDISPATCH(2, launch_t, args, grid, smem, stream);
         case 3: IDC_MDISPATCH(3, launch_t, args, grid, smem, stream);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_sweep_modal_batched(int P, int precision, const SweepArgs &launch, const SweepArgs *table, int grid,
+                                       size_t smem, cudaStream_t stream) {
+    if (launch.wn < 1 || launch.wn + 1 > kMaxWarps || launch.seg < 4 || launch.seg > 32 || (launch.seg & (launch.seg - 1)) ||
+        launch.G > launch.seg || !table || launch.adjoint)
+        return cudaErrorInvalidValue;
+    if (precision != 0 && precision != 1) return cudaErrorInvalidValue;
+    switch (P) {
+        case 1: return precision == 0 ? launch_batched_t<1, 0>(launch, table, grid, smem, stream)
+                                      : launch_batched_t<1, 1>(launch, table, grid, smem, stream);
+        case 2: return precision == 0 ? launch_batched_t<2, 0>(launch, table, grid, smem, stream)
+                                      : launch_batched_t<2, 1>(launch, table, grid, smem, stream);
+        case 3: return precision == 0 ? launch_batched_t<3, 0>(launch, table, grid, smem, stream)
+                                      : launch_batched_t<3, 1>(launch, table, grid, smem, stream);
         default: return cudaErrorInvalidValue;
     }
 }

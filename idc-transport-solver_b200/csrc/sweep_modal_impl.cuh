@@ -448,22 +448,24 @@ __device__ void modal_helper(const SweepArgs &a, const SweepItem &item, const La
     }
 }
 
-template <int P, int MODE, int SEG, bool ADJ>
-__global__ void __launch_bounds__(kMaxWarps * 32, 1) sweep_modal_kernel(const SweepArgs a) {
+template <int P, int MODE, int SEG, bool ADJ, bool BATCHED>
+__global__ void __launch_bounds__(kMaxWarps * 32, 1) sweep_modal_kernel(const SweepArgs a0,
+                                                                        const SweepArgs *__restrict__ table) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_item;
     __shared__ int s_stop;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const Layout L = carve(smem_raw, a.wn, a.G, P, prefetch_depth(P), 32 / SEG);
-    const int rows_cta = a.wn * (32 / SEG);
+    const Layout L = carve(smem_raw, a0.wn, a0.G, P, prefetch_depth(P), 32 / SEG);
+    const int rows_cta = a0.wn * (32 / SEG);
+    __shared__ __align__(16) SweepArgs s_args;   // batched: the current item's problem descriptor
 
     for (;;) {
         if (threadIdx.x == 0) {
-            const int it = atomicAdd(a.next_item, 1);
+            const int it = atomicAdd(a0.next_item, 1);
             s_item = it;
-            s_stop = (it >= a.n_items) || (ld_relaxed(a.error) != kDevOk);
+            s_stop = (it >= a0.n_items) || (ld_relaxed(a0.error) != kDevOk);
             if (!s_stop)
-                for (int b = 0; b < (a.wn + 1) * kS; ++b) {
+                for (int b = 0; b < (a0.wn + 1) * kS; ++b) {
                     mbar_init(L.full + b, 32);
                     mbar_init(L.empty + b, 32);
                 }
@@ -471,16 +473,25 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 1) sweep_modal_kernel(const Sw
         __syncthreads();
         const int it = s_item;
         if (s_stop) return;
-        const SweepItem item = a.items[it];
+        const SweepItem item = a0.items[it];
+        if constexpr (BATCHED) {
+            const unsigned long long *sw = reinterpret_cast<const unsigned long long *>(table + item.problem);
+            unsigned long long *dw = reinterpret_cast<unsigned long long *>(&s_args);
+            for (int k = threadIdx.x; k < (int)(sizeof(SweepArgs) / 8); k += blockDim.x) dw[k] = sw[k];
+            __syncthreads();
+        }
+        const SweepArgs &a = BATCHED ? s_args : a0;
+        // the item's index within its problem (its trace buffer and partial-moment slot)
+        const int local = BATCHED ? item.local : it;
         if ((int)threadIdx.x < item.q_count) L.w[threadIdx.x] = a.w[item.q_begin + threadIdx.x];
         __syncthreads();
         const bool has_consumer = (item.row_block + 1) * rows_cta < a.ny;
-        if (warp < a.wn) {
+        if (warp < a0.wn) {
             switch (item.quadrant) {
-                case 0: modal_rows<P, MODE, SEG, false, false, ADJ>(a, item, L, warp, lane, has_consumer, it); break;
-                case 1: modal_rows<P, MODE, SEG, false, true, ADJ>(a, item, L, warp, lane, has_consumer, it); break;
-                case 2: modal_rows<P, MODE, SEG, true, false, ADJ>(a, item, L, warp, lane, has_consumer, it); break;
-                default: modal_rows<P, MODE, SEG, true, true, ADJ>(a, item, L, warp, lane, has_consumer, it); break;
+                case 0: modal_rows<P, MODE, SEG, false, false, ADJ>(a, item, L, warp, lane, has_consumer, local); break;
+                case 1: modal_rows<P, MODE, SEG, false, true, ADJ>(a, item, L, warp, lane, has_consumer, local); break;
+                case 2: modal_rows<P, MODE, SEG, true, false, ADJ>(a, item, L, warp, lane, has_consumer, local); break;
+                default: modal_rows<P, MODE, SEG, true, true, ADJ>(a, item, L, warp, lane, has_consumer, local); break;
             }
         } else {
             modal_helper<P>(a, item, L, lane);
@@ -491,16 +502,26 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 1) sweep_modal_kernel(const Sw
 
 template <int P, int MODE, int SEG, bool ADJ>
 cudaError_t launch_seg(const SweepArgs &args, int grid, size_t smem, cudaStream_t stream) {
-    auto kern = sweep_modal_kernel<P, MODE, SEG, ADJ>;
+    auto kern = sweep_modal_kernel<P, MODE, SEG, ADJ, false>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    kern<<<grid, (args.wn + 1) * 32, smem, stream>>>(args);
+    kern<<<grid, (args.wn + 1) * 32, smem, stream>>>(args, nullptr);
+    return cudaGetLastError();
+}
+
+template <int P, int MODE, int SEG>
+cudaError_t launch_seg_batched(const SweepArgs &launch, const SweepArgs *table, int grid, size_t smem,
+                               cudaStream_t stream) {
+    auto kern = sweep_modal_kernel<P, MODE, SEG, false, true>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    kern<<<grid, (launch.wn + 1) * 32, smem, stream>>>(launch, table);
     return cudaGetLastError();
 }
 
 template <int P, int MODE, int SEG, bool ADJ>
 cudaError_t occ_seg(int threads, size_t smem, int *n) {
-    auto kern = sweep_modal_kernel<P, MODE, SEG, ADJ>;
+    auto kern = sweep_modal_kernel<P, MODE, SEG, ADJ, false>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, kern, threads, smem);
@@ -536,3 +557,17 @@ cudaError_t occ_seg(int threads, size_t smem, int *n) {
     DECL template cudaError_t idc::modal::occ_seg<3, MODE, 8, ADJ>(int, size_t, int *);                             \
     DECL template cudaError_t idc::modal::occ_seg<3, MODE, 16, ADJ>(int, size_t, int *);                            \
     DECL template cudaError_t idc::modal::occ_seg<3, MODE, 32, ADJ>(int, size_t, int *);
+
+#define IDC_MODAL_BATCHED(DECL, MODE)                                                                              \
+    DECL template cudaError_t idc::modal::launch_seg_batched<1, MODE, 4>(const idc::SweepArgs &, const idc::SweepArgs *, int, size_t, cudaStream_t);  \
+    DECL template cudaError_t idc::modal::launch_seg_batched<1, MODE, 8>(const idc::SweepArgs &, const idc::SweepArgs *, int, size_t, cudaStream_t);  \
+    DECL template cudaError_t idc::modal::launch_seg_batched<1, MODE, 16>(const idc::SweepArgs &, const idc::SweepArgs *, int, size_t, cudaStream_t); \
+    DECL template cudaError_t idc::modal::launch_seg_batched<1, MODE, 32>(const idc::SweepArgs &, const idc::SweepArgs *, int, size_t, cudaStream_t); \
+    DECL template cudaError_t idc::modal::launch_seg_batched<2, MODE, 4>(const idc::SweepArgs &, const idc::SweepArgs *, int, size_t, cudaStream_t);  \
+    DECL template cudaError_t idc::modal::launch_seg_batched<2, MODE, 8>(const idc::SweepArgs &, const idc::SweepArgs *, int, size_t, cudaStream_t);  \
+    DECL template cudaError_t idc::modal::launch_seg_batched<2, MODE, 16>(const idc::SweepArgs &, const idc::SweepArgs *, int, size_t, cudaStream_t); \
+    DECL template cudaError_t idc::modal::launch_seg_batched<2, MODE, 32>(const idc::SweepArgs &, const idc::SweepArgs *, int, size_t, cudaStream_t); \
+    DECL template cudaError_t idc::modal::launch_seg_batched<3, MODE, 4>(const idc::SweepArgs &, const idc::SweepArgs *, int, size_t, cudaStream_t);  \
+    DECL template cudaError_t idc::modal::launch_seg_batched<3, MODE, 8>(const idc::SweepArgs &, const idc::SweepArgs *, int, size_t, cudaStream_t);  \
+    DECL template cudaError_t idc::modal::launch_seg_batched<3, MODE, 16>(const idc::SweepArgs &, const idc::SweepArgs *, int, size_t, cudaStream_t); \
+    DECL template cudaError_t idc::modal::launch_seg_batched<3, MODE, 32>(const idc::SweepArgs &, const idc::SweepArgs *, int, size_t, cudaStream_t);

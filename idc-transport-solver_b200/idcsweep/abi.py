@@ -41,7 +41,8 @@ EXPORTED_SYMBOLS = (
     "idc_smv", "idc_lmv", "idc_source_iteration", "idc_strerror", "idc_last_error_message", "idc_last_timing",
     "idc_set_tiling", "idc_sweep_out", "idc_sweep_noalloc", "idc_gmres_solve", "idc_sweep_adjoint",
     "idc_adjoint_grad", "idc_set_preconditioner", "idc_idc_integrate", "idc_write_sd2", "idc_read_sd2",
-    "idc_write_af2", "idc_read_af2", "idc_sweep_fused",
+    "idc_write_af2", "idc_read_af2", "idc_sweep_fused", "idc_set_tile_shape", "idc_autotune", "idc_batch_create",
+    "idc_batch_add", "idc_batch_sweep", "idc_batch_autotune", "idc_batch_last_timing", "idc_batch_destroy",
 )
 
 
@@ -90,6 +91,14 @@ def load_library(path: str = LIB_PATH):
     lib.idc_sweep_adjoint.argtypes = [vp, vp, vp, C.c_double, vp, C.c_int, C.c_int]
     lib.idc_set_preconditioner.argtypes = [vp, C.c_int, C.c_int32]
     lib.idc_sweep_fused.argtypes = [vp, vp, vp, C.c_double, vp, C.c_double, vp, C.c_int, C.c_int]
+    lib.idc_set_tile_shape.argtypes = [vp, C.c_int32, C.c_int32]
+    lib.idc_autotune.argtypes = [vp, vp, C.c_double, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+    lib.idc_batch_create.argtypes = [C.POINTER(vp)]
+    lib.idc_batch_add.argtypes = [vp, vp]
+    lib.idc_batch_sweep.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.c_double, C.c_int]
+    lib.idc_batch_autotune.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), C.c_double, C.c_int]
+    lib.idc_batch_last_timing.argtypes = [vp, _dp]
+    lib.idc_batch_destroy.argtypes = [vp]
     lib.idc_idc_integrate.argtypes = [vp, vp, vp, C.c_double, C.c_int64, C.c_int32, C.c_int32, C.c_int, C.c_int,
                                       C.c_double, C.c_int32, C.c_int64, C.c_int, C.c_int, C.POINTER(C.c_int64)]
     lib.idc_adjoint_grad.argtypes = [vp, vp, vp, C.c_double, C.c_double, C.c_int32, C.c_int64, C.c_int, vp, vp, vp,
@@ -237,6 +246,16 @@ class SweepContext:
                                          float(scatter_scale), v(phi_ptr), int(precision), LOC_DEVICE),
                "idc_sweep_fused")
 
+    def set_tile_shape(self, seg: int, warps: int):
+        _check(self._lib.idc_set_tile_shape(self._h, int(seg), int(warps)), "idc_set_tile_shape")
+
+    def autotune(self, source_ptr, dt=np.inf, precision=PREC_FP64):
+        """Times every tile shape on this problem (device source pointer); keeps and returns (seg, warps)."""
+        sg, wp = C.c_int32(), C.c_int32()
+        _check(self._lib.idc_autotune(self._h, C.c_void_p(int(source_ptr)), float(dt), int(precision), C.byref(sg),
+                                      C.byref(wp)), "idc_autotune")
+        return int(sg.value), int(wp.value)
+
     def set_preconditioner(self, kind: int, inner_steps: int = 30):
         """Right preconditioner of gmres_solve: PRECOND_NONE or PRECOND_DSA (inner_steps CG steps)."""
         _check(self._lib.idc_set_preconditioner(self._h, int(kind), int(inner_steps)), "idc_set_preconditioner")
@@ -263,6 +282,52 @@ class SweepContext:
         n = C.c_int64()
         _check(self._lib.idc_last_timing(self._h, C.byref(ms), C.byref(n)), "idc_last_timing")
         return float(ms.value), int(n.value)
+
+
+class Batch:
+    """Independent problems (SweepContexts on one GPU) swept in one persistent launch per DG degree."""
+
+    def __init__(self):
+        self._lib = load_library()
+        h = C.c_void_p()
+        _check(self._lib.idc_batch_create(C.byref(h)), "idc_batch_create")
+        self._h = h
+        self._members = []
+
+    def add(self, ctx: "SweepContext"):
+        _check(self._lib.idc_batch_add(self._h, ctx._h), "idc_batch_add")
+        self._members.append(ctx)
+
+    def _arr(self, ptrs):
+        n = len(self._members)
+        if ptrs is None:
+            return None
+        assert len(ptrs) == n
+        return (C.c_void_p * n)(*[None if p is None else C.c_void_p(int(p)) for p in ptrs])
+
+    def sweep(self, src_ptrs, out_ptrs, phi_ptrs=None, dt=np.inf, precision=PREC_FP64):
+        _check(self._lib.idc_batch_sweep(self._h, self._arr(src_ptrs), self._arr(out_ptrs), self._arr(phi_ptrs),
+                                         float(dt), int(precision)), "idc_batch_sweep")
+
+    def autotune(self, src_ptrs, out_ptrs, dt=np.inf, precision=PREC_FP64):
+        _check(self._lib.idc_batch_autotune(self._h, self._arr(src_ptrs), self._arr(out_ptrs), float(dt),
+                                            int(precision)), "idc_batch_autotune")
+
+    def last_ms(self) -> float:
+        ms = C.c_double()
+        _check(self._lib.idc_batch_last_timing(self._h, C.byref(ms)), "idc_batch_last_timing")
+        return float(ms.value)
+
+    def close(self):
+        if self._h:
+            self._lib.idc_batch_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 def sweep_noalloc(nx, ny, p, ax, bx, ay, by, xi_ptr, eta_ptr, w_ptr, nq, quad_bounds, sigma_t_ptr, source_ptr,

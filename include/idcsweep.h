@@ -197,6 +197,30 @@ int idc_idc_integrate(idc_ctx *ctx, double *psi_inout, const double *source, dou
 int idc_sweep_fused(idc_ctx *ctx, const double *source, double *result, double dt, const double *phi_scatter,
                     double scatter_scale, double *phi_out, int precision, int loc);
 
+/* ---- tile shapes and batches ------------------------------------------------------------------------- */
+
+/* Tile shape of the sweep kernel: ordinates per row segment (seg: 4, 8, 16 or 32) and compute warps per
+ * thread block (1..7); 0, 0 restores the default heuristic.  Results do not depend on it. */
+int idc_set_tile_shape(idc_ctx *ctx, int32_t seg, int32_t warps);
+
+/* Autotuner: times every tile shape on this context's problem with `source` (device psi array) and keeps
+ * the fastest (reported in *seg, *warps). */
+int idc_autotune(idc_ctx *ctx, const double *source, double dt, int precision, int32_t *seg, int32_t *warps);
+
+/* A batch of independent problems (contexts on one GPU) swept together: one persistent launch per DG
+ * degree whose work queue interleaves every problem's row blocks.  idc_batch_sweep takes host arrays of
+ * device pointers, one entry per added context in order (entries may be NULL: no source / not stored /
+ * no moments); FP64 or FP32_REFINED.  idc_batch_autotune picks the tile shape of each degree by timing
+ * the batched sweep on the given inputs.  No counterpart in the reference (it sweeps one problem). */
+typedef struct idc_batch idc_batch;
+int idc_batch_create(idc_batch **out);
+int idc_batch_add(idc_batch *b, idc_ctx *ctx);
+int idc_batch_sweep(idc_batch *b, const double *const *sources, double *const *results, double *const *phi_out,
+                    double dt, int precision);
+int idc_batch_autotune(idc_batch *b, const double *const *sources, double *const *results, double dt, int precision);
+int idc_batch_last_timing(idc_batch *b, double *ms);
+int idc_batch_destroy(idc_batch *b);
+
 /* ---- discrete adjoint --------------------------------------------------------------------------------- */
 
 /* Transposed sweep: result = L^{-T} source on interior cells, where L^{-1} is the sweep of idc_sweep_out

@@ -1,0 +1,74 @@
+"""Batched sweeps (several problems in one launch per DG degree) and the autotuner: psi is bitwise the
+per-problem sweep's (cell arithmetic does not depend on the tiling), phi agrees to rounding."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_err
+from idcsweep import abi
+from idcsweep.problems import lognormal, random_problem
+
+pytestmark = pytest.mark.gpu
+
+
+def _ctx(P):
+    c = abi.SweepContext(P.nx, P.ny, P.p, P.ax, P.bx, P.ay, P.by)
+    c.set_ordinates(P.xi, P.eta, P.w, P.quad)
+    c.set_sigma(P.sigma_t, P.sigma_s)
+    return c
+
+
+def _problems():
+    return [random_problem(9, 7, 1, 4, seed=1), random_problem(16, 20, 2, 8, seed=2), lognormal(24, 1, 12, seed=3),
+            random_problem(5, 13, 2, 4, seed=4, dt=0.2), lognormal(12, 2, 16, seed=5), random_problem(1, 6, 1, 8, seed=6)]
+
+
+@pytest.mark.parametrize("prec", [abi.PREC_FP64, abi.PREC_FP32_REFINED])
+def test_batched_sweep_matches_individual_sweeps(prec):
+    probs = _problems()
+    dts = {P.dt for P in probs}
+    ctxs = [_ctx(P) for P in probs]
+    try:
+        for dt in dts:
+            sel = [k for k, P in enumerate(probs) if P.dt == dt]
+            srcs = [torch.from_numpy(probs[k].source).cuda() for k in sel]
+            outs = [torch.zeros_like(s) for s in srcs]
+            phis = [torch.zeros(probs[k].phi_shape(), dtype=torch.float64, device="cuda") for k in sel]
+            with abi.Batch() as b:
+                for k in sel:
+                    b.add(ctxs[k])
+                b.sweep([s.data_ptr() for s in srcs], [o.data_ptr() for o in outs], [f.data_ptr() for f in phis], dt,
+                        prec)
+                b.sweep([s.data_ptr() for s in srcs], [o.data_ptr() for o in outs], [f.data_ptr() for f in phis], dt,
+                        prec)   # reuse (re-armed traces)
+            for j, k in enumerate(sel):
+                want = torch.zeros_like(srcs[j])
+                wphi = torch.zeros_like(phis[j])
+                ctxs[k].sweep_out(srcs[j].data_ptr(), want.data_ptr(), dt, wphi.data_ptr(), prec, loc=abi.LOC_DEVICE)
+                assert torch.equal(outs[j][1:-1, 1:-1], want[1:-1, 1:-1])
+                assert rel_err(phis[j].cpu().numpy(), wphi.cpu().numpy()) < 1e-14
+    finally:
+        for c in ctxs:
+            c.close()
+
+
+def test_autotuners_keep_results():
+    probs = _problems()[:3]
+    ctxs = [_ctx(P) for P in probs]
+    try:
+        srcs = [torch.from_numpy(P.source).cuda() for P in probs]
+        outs = [torch.zeros_like(s) for s in srcs]
+        with abi.Batch() as b:
+            for c in ctxs:
+                b.add(c)
+            b.autotune([s.data_ptr() for s in srcs], [o.data_ptr() for o in outs], np.inf)
+            b.sweep([s.data_ptr() for s in srcs], [o.data_ptr() for o in outs], None, np.inf)
+        for j, c in enumerate(ctxs):
+            seg, wn = c.autotune(srcs[j].data_ptr(), np.inf)
+            assert seg in (4, 8, 16, 32) and 1 <= wn <= 7
+            want = torch.zeros_like(srcs[j])
+            c.sweep_out(srcs[j].data_ptr(), want.data_ptr(), np.inf, None, loc=abi.LOC_DEVICE)
+            assert torch.equal(outs[j][1:-1, 1:-1], want[1:-1, 1:-1])
+    finally:
+        for c in ctxs:
+            c.close()
