@@ -180,6 +180,141 @@ def run_reference_arm(args):
 
 
 # ----------------------------------------------------------------------------------------------------
+# the other configurations, measured beside the headline (rank 0, one GPU)
+# ----------------------------------------------------------------------------------------------------
+
+def _ctx_for(abi, P, dev):
+    c = abi.SweepContext(P.nx, P.ny, P.p, P.ax, P.bx, P.ay, P.by, device=dev)
+    c.set_ordinates(P.xi, P.eta, P.w, P.quad)
+    c.set_sigma(P.sigma_t, P.sigma_s)
+    return c
+
+
+def extra_gmres_dsa(abi, torch, dev):
+    """256x256 Q2 S16 log-normal steady problem, GMRES(30) + DSA to 1e-10 (FP64 and refined sweeps)."""
+    P = problem(0)
+    out = {"workload": "256x256 Q2 S16 log-normal steady, GMRES(30)+DSA(30 CG steps), abs tol 1e-10"}
+    for name, prec in (("fp64", abi.PREC_FP64), ("fp32_refined", abi.PREC_FP32_REFINED)):
+        with _ctx_for(abi, P, dev) as c:
+            c.set_preconditioner(abi.PRECOND_DSA, 30)
+            d = torch.from_numpy(P.source).to(f"cuda:{dev}")
+            c.gmres_solve(d.data_ptr(), P.dt, abs_tol=1e-10, restart=30, max_its=3000, precision=prec,
+                          loc=abi.LOC_DEVICE)   # warm-up (schedules, buffers)
+            d = torch.from_numpy(P.source).to(f"cuda:{dev}")
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            its, res = c.gmres_solve(d.data_ptr(), P.dt, abs_tol=1e-10, restart=30, max_its=3000, precision=prec,
+                                     loc=abi.LOC_DEVICE)
+            torch.cuda.synchronize()
+            out[name] = {"iterations": its, "residual": res, "ms": (time.perf_counter() - t0) * 1e3}
+    return out
+
+
+def extra_idc(abi, torch, dev, steps=10):
+    """512x512 Q1 S12 lattice, IMEX-IDC (4 Gauss-Lobatto nodes, 3 corrections), dt = 0.005, one CUDA graph
+    per step; `steps` of the configuration's 100 steps are timed."""
+    from idcsweep.problems import lattice
+    P = lattice(512, 1, 12, dt=0.005)
+    out = {"workload": f"512x512 Q1 S12 lattice, IMEX-IDC 4 nodes 3 corrections, dt 0.005, {steps} steps timed"}
+    with _ctx_for(abi, P, dev) as c:
+        psi = torch.zeros(P.psi_shape(), dtype=torch.float64, device=f"cuda:{dev}")
+        src = torch.from_numpy(P.source).to(f"cuda:{dev}")
+        for name, prec in (("fp64", abi.PREC_FP64), ("fp32_refined", abi.PREC_FP32_REFINED)):
+            c.idc_integrate(psi.data_ptr(), src.data_ptr(), P.dt, 2, 4, 3, abi.SCATTER_EXPLICIT, prec, use_graph=True,
+                            loc=abi.LOC_DEVICE)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            sw = c.idc_integrate(psi.data_ptr(), src.data_ptr(), P.dt, steps, 4, 3, abi.SCATTER_EXPLICIT, prec,
+                                 use_graph=True, loc=abi.LOC_DEVICE)
+            torch.cuda.synchronize()
+            sec = time.perf_counter() - t0
+            out[name] = {"ms_per_step": sec * 1e3 / steps, "sweeps": sw,
+                         "sweep_unknowns_per_s": sw * P.unknowns_per_sweep / sec}
+    return out
+
+
+def extra_adjoint(abi, torch, dev):
+    """128x128 Q1 S8, log-normal sigma_t (median 2, log-sd 0.7), c = 0.9, Gaussian source at the left third,
+    detector = scalar flux over a 16x16 window at the right third: gradients of all 3 nx ny per-cell
+    parameters (sigma_t, sigma_s, source) from one adjoint solve."""
+    from idcsweep.problems import detector_window, lognormal
+    P = lognormal(128, 1, 8, seed=0, median=2.0, log_sd=0.7, c_fixed=0.9, source="gaussian")
+    c_det = torch.from_numpy(detector_window(P, cells=16)).to(f"cuda:{dev}")
+    out = {"workload": "128x128 Q1 S8 log-normal (median 2, log-sd 0.7), c = 0.9, Gaussian source, 16x16 detector",
+           "gradient_entries": 3 * P.nx * P.ny}
+    with _ctx_for(abi, P, dev) as c:
+        psi = torch.from_numpy(P.source).to(f"cuda:{dev}")
+        c.gmres_solve(psi.data_ptr(), P.dt, abs_tol=1e-12, restart=30, max_its=3000, loc=abi.LOC_DEVICE)
+        g_t = torch.zeros((P.nx + 2) * (P.ny + 2), dtype=torch.float64, device=f"cuda:{dev}")
+        g_s = torch.zeros_like(g_t)
+        g_q = torch.zeros(P.phi_shape(), dtype=torch.float64, device=f"cuda:{dev}")
+        for name, prec in (("fp64", abi.PREC_FP64), ("fp32_refined", abi.PREC_FP32_REFINED)):
+            args = (psi.data_ptr(), c_det.data_ptr(), g_t.data_ptr(), g_s.data_ptr(), g_q.data_ptr())
+            c.adjoint_grad(*args, dt=P.dt, abs_tol=1e-12, precision=prec, loc=abi.LOC_DEVICE)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            its, res = c.adjoint_grad(*args, dt=P.dt, abs_tol=1e-12, precision=prec, loc=abi.LOC_DEVICE)
+            torch.cuda.synchronize()
+            sec = time.perf_counter() - t0
+            out[name] = {"grads_per_s": 3 * P.nx * P.ny / sec, "ms": sec * 1e3, "adjoint_iterations": its}
+    return out
+
+
+def extra_batched(abi, torch, dev, n_problems=64):
+    """64 independent steady problems: side U{32,...,384}, S4/S8/S12/S16, Q1/Q2, log-normal sigma_t (median 1,
+    log-sd 1), c U[0.3, 0.99] (seeded); one sweep of every problem, batched (one launch per DG degree,
+    autotuned tile shapes) against one problem at a time with the default FP64 sweep."""
+    from idcsweep.quadrature import level_symmetric_2d
+    rng = np.random.default_rng(2024)
+    ctxs, srcs, outs, phis, unknowns = [], [], [], [], 0
+    try:
+        for _ in range(n_problems):
+            n = int(rng.choice(np.arange(32, 385, 32)))
+            sn = int(rng.choice([4, 8, 12, 16]))
+            p = int(rng.choice([1, 2]))
+            st = np.zeros((n + 2, n + 2))
+            st[1:-1, 1:-1] = np.exp(rng.standard_normal((n, n)))
+            ss = np.zeros_like(st)
+            ss[1:-1, 1:-1] = rng.uniform(0.3, 0.99, (n, n)) * st[1:-1, 1:-1]
+            xi, eta, w, q = level_symmetric_2d(sn)
+            c = abi.SweepContext(n, n, p, 0.0, 7.0, 0.0, 7.0, device=dev)
+            c.set_ordinates(xi, eta, w, q)
+            c.set_sigma(st.ravel().copy(), ss.ravel().copy())
+            s_ = torch.zeros((n + 2, n + 2, xi.size, p + 1, p + 1), dtype=torch.float64, device=f"cuda:{dev}")
+            s_[1:-1, 1:-1, :, 0, 0] = 1.0 / (4 * math.pi)
+            ctxs.append(c)
+            srcs.append(s_)
+            outs.append(torch.zeros_like(s_))
+            phis.append(torch.zeros((n + 2, n + 2, p + 1, p + 1), dtype=torch.float64, device=f"cuda:{dev}"))
+            unknowns += n * n * xi.size * (p + 1) ** 2
+        for _ in range(2):
+            one = 0.0
+            for k, c in enumerate(ctxs):
+                c.sweep_out(srcs[k].data_ptr(), outs[k].data_ptr(), math.inf, phis[k].data_ptr(), abi.PREC_FP64,
+                            loc=abi.LOC_DEVICE)
+                one += c.last_timing()[0]
+        with abi.Batch() as b:
+            for c in ctxs:
+                b.add(c)
+            S, O, F = [x.data_ptr() for x in srcs], [x.data_ptr() for x in outs], [x.data_ptr() for x in phis]
+            b.autotune(S, O, math.inf, abi.PREC_FP64)
+            res = {}
+            for name, prec in (("fp64", abi.PREC_FP64), ("fp32_refined", abi.PREC_FP32_REFINED)):
+                for _ in range(2):
+                    b.sweep(S, O, F, math.inf, prec)
+                best = min((b.sweep(S, O, F, math.inf, prec), b.last_ms())[1] for _ in range(3))
+                res[name] = {"device_ms": best, "unknowns_per_s": unknowns / (best * 1e-3),
+                             "hbm_frac_of_measured": 16.0 * unknowns / (best * 1e-3) / 1e9 / hbm_peak()[0]}
+        return {"workload": f"{n_problems} independent steady problems, sides 32..384, S4..S16, Q1/Q2",
+                "unknowns_per_sweep": unknowns, "one_at_a_time_fp64": {"device_ms": one,
+                                                                      "unknowns_per_s": unknowns / (one * 1e-3)},
+                "batched_autotuned": res, "speedup_fp64": one / res["fp64"]["device_ms"]}
+    finally:
+        for c in ctxs:
+            c.close()
+
+
+# ----------------------------------------------------------------------------------------------------
 # our arm
 # ----------------------------------------------------------------------------------------------------
 
@@ -315,6 +450,14 @@ def run_ours(args):
         "clocks": clocks,
     }
 
+    if not args.no_extras and world == 1:
+        for key, fn in (("gmres_dsa", extra_gmres_dsa), ("idc", extra_idc), ("adjoint", extra_adjoint),
+                        ("batched", extra_batched)):
+            try:
+                line[key] = fn(abi, torch, dev)
+            except Exception as e:   # reported, never fatal for the headline line
+                line[key] = {"error": str(e)[:200]}
+
     if not args.no_cpu_baseline and world == 1:
         try:
             sec, threads, phi_ref = time_reference_cpu(P, reps=2)
@@ -343,6 +486,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg (profiling runs)")
     ap.add_argument("--nx", type=int, default=NX, help="grid side (default: the benchmark's 256; smaller for ncu)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the other configurations (GMRES+DSA, IDC, adjoint, batched) measured beside the headline")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)

@@ -434,6 +434,23 @@ int idc_batch_autotune(idc_batch *b, const double *const *sources, double *const
     ABI_GUARD_END
 }
 
+int idc_batch_set_shape(idc_batch *b, int dg_degree, int precision, int32_t seg, int32_t warps) {
+    ABI_GUARD_BEGIN
+    if (!b) return fail(IDC_ERR_ARG, "null batch");
+    ABI_TRY(b->impl.set_shape((int)dg_degree + 1, precision, seg, warps));
+    return IDC_OK;
+    ABI_GUARD_END
+}
+
+int idc_batch_get_shape(idc_batch *b, int dg_degree, int precision, int32_t *seg, int32_t *warps) {
+    if (!b || !seg || !warps) return fail(IDC_ERR_ARG, "idc_batch_get_shape: null argument");
+    int s = 0, w = 0;
+    b->impl.get_shape((int)dg_degree + 1, precision, &s, &w);
+    *seg = s;
+    *warps = w;
+    return IDC_OK;
+}
+
 int idc_batch_last_timing(idc_batch *b, double *ms) {
     if (!b) return fail(IDC_ERR_ARG, "null batch");
     if (ms) *ms = b->impl.last_ms;

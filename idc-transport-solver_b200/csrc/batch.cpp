@@ -264,6 +264,36 @@ Status Batch::sweep(const double *const *srcs, double *const *outs, const double
     return Status::ok();
 }
 
+Status Batch::set_shape(int P, int precision, int seg, int wn) {
+    const auto key = std::make_pair(P, precision);
+    if (seg == 0 && wn == 0) {
+        tuned.erase(key);
+    } else {
+        if ((seg != 4 && seg != 8 && seg != 16 && seg != 32) || wn < 1 || wn > 7)
+            return bad(IDC_ERR_ARG, "batch tile shape: seg must be 4, 8, 16 or 32 and wn in 1..7");
+        tuned[key] = {seg, wn};
+    }
+    release();
+    return Status::ok();
+}
+
+void Batch::get_shape(int P, int precision, int *seg, int *wn) const {
+    const auto it = tuned.find(std::make_pair(P, precision));
+    if (it != tuned.end()) {
+        *seg = it->second.first;
+        *wn = it->second.second;
+        return;
+    }
+    int qmax = 0;
+    for (auto *c : members)
+        if (c->P == P) qmax = std::max(qmax, qmax_of(*c));
+    if (qmax == 0) {
+        *seg = *wn = 0;
+        return;
+    }
+    default_shape(qmax, seg, wn);
+}
+
 Status Batch::autotune(const double *const *srcs, double *const *outs, double dt, int precision) {
     if (members.empty()) return bad(IDC_ERR_STATE, "empty batch");
     for (int P : {1, 2, 3}) {

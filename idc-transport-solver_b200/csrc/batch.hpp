@@ -19,6 +19,9 @@ public:
                  double *const *phis, double dt, int precision);
     // times the candidate tile shapes per degree on the given inputs and keeps the fastest
     Status autotune(const double *const *srcs, double *const *outs, double dt, int precision);
+    // the tile shape used for degree P at `precision` (set: seg in {4,8,16,32}, wn in 1..7; 0, 0 = default)
+    Status set_shape(int P, int precision, int seg, int wn);
+    void get_shape(int P, int precision, int *seg, int *wn) const;
 
     std::vector<Context *> members;
     std::map<std::pair<int, int>, std::pair<int, int>> tuned;   // (P, precision) -> (seg, wn)

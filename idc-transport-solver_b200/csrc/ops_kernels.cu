@@ -18,6 +18,8 @@ inline int blocks_for(size_t n, int threads = kThreads) {
 }
 
 // phi(i,j,k) <- beta*phi + alpha * sum_q w_q psi(q,i,j,k): TransportOperator::Pmv, :140-158.
+// In this file a zero beta means the output's old values are not read (BLAS convention), so an
+// uninitialised output array never leaks NaN through 0 * NaN.
 // One thread per (interior cell, dof).
 __global__ void pmv_kernel(GridDims g, double alpha, double beta, const double *__restrict__ w,
                            const double *__restrict__ psi, double *__restrict__ phi) {
@@ -29,7 +31,7 @@ __global__ void pmv_kernel(GridDims g, double alpha, double beta, const double *
         const int i = 1 + (int)(cell / g.ny), j = 1 + (int)(cell % g.ny);
         const size_t cidx = (size_t)i * (g.ny + 2) + j;
         const double *ps = psi + cidx * (size_t)g.nq * N + k;
-        double acc = phi[cidx * N + k] * beta;
+        double acc = beta == 0.0 ? 0.0 : phi[cidx * N + k] * beta;   // beta = 0: phi is not read
         for (int q = 0; q < g.nq; ++q) acc += alpha * w[q] * ps[(size_t)q * N];
         phi[cidx * N + k] = acc;
     }
@@ -49,7 +51,7 @@ __global__ void smv_kernel(GridDims g, double alpha, double beta, const double *
         const size_t cidx = (size_t)i * (g.ny + 2) + j;
         const double v = (sigma_s[cidx] * phi[cidx * N + k] / (4.0 * M_PI)) * alpha;
         const size_t idx = cidx * per_cell + within;
-        psi[idx] = beta * psi[idx] + v;
+        psi[idx] = beta == 0.0 ? v : beta * psi[idx] + v;   // beta = 0: psi is not read
     }
 }
 
@@ -119,7 +121,7 @@ __global__ void lmv_kernel(GridDims g, double alpha, double beta, const double *
                 for (int b = e - 1; b >= 0; b -= 2) x3[e + P * d] -= double(2 * (2 * e + 1)) * cv * x0[b + P * d];
         double *Y = y + base;
 #pragma unroll
-        for (int k = 0; k < N; ++k) Y[k] = beta * Y[k] + alpha * x3[k];
+        for (int k = 0; k < N; ++k) Y[k] = beta == 0.0 ? alpha * x3[k] : beta * Y[k] + alpha * x3[k];
     }
 }
 
@@ -226,7 +228,8 @@ __global__ void multiaxpy_kernel(double *__restrict__ w, const double *__restric
 // y = a*x + b*y
 __global__ void axpby_kernel(double a, const double *__restrict__ x, double b, double *__restrict__ y, size_t n) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        y[i] = a * x[i] + b * y[i];
+        // BLAS convention: a zero coefficient means the operand is not read (so 0 * NaN never leaks in)
+        y[i] = b == 0.0 ? a * x[i] : (a == 0.0 ? b * y[i] : a * x[i] + b * y[i]);
 }
 
 // out[0] += sum x*y

@@ -401,6 +401,30 @@ __device__ void modal_helper(const SweepArgs &a, const SweepItem &item, const La
                 ++n;
         n = __shfl_sync(kFullMask, n, 0);
 
+        // the item above: wait until the first value of column `fetch` is written before loading the
+        // columns (one load per poll, with a bounded back-off, so that many waiting items do not flood L2)
+        if (has_dep) {
+            int ok = 1;
+            if (lane == 0) {
+                unsigned ns = 0;
+                for (long long poll = 0;; ++poll) {
+                    if (!is_sentinel(ld_relaxed_f64(trace + (size_t)fetch * col_stride))) break;
+                    if ((poll & 63) == 63 && ld_relaxed(a.error) != kDevOk) {
+                        ok = 0;
+                        break;
+                    }
+                    if (poll > a.spin_limit) {
+                        atomicCAS(a.error, kDevOk, kDevTimeout);
+                        ok = 0;
+                        break;
+                    }
+                    if (ns) __nanosleep(ns);
+                    ns = ns ? min(ns * 2, 1024u) : 32u;
+                }
+            }
+            if (!__shfl_sync(kFullMask, ok, 0)) break;
+        }
+
         double v[kS][kV];
         unsigned col_ok = (1u << n) - 1u;   // bit t: column fetch + t complete in this lane
 #pragma unroll

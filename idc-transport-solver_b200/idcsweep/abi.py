@@ -43,6 +43,7 @@ EXPORTED_SYMBOLS = (
     "idc_adjoint_grad", "idc_set_preconditioner", "idc_idc_integrate", "idc_write_sd2", "idc_read_sd2",
     "idc_write_af2", "idc_read_af2", "idc_sweep_fused", "idc_set_tile_shape", "idc_autotune", "idc_batch_create",
     "idc_batch_add", "idc_batch_sweep", "idc_batch_autotune", "idc_batch_last_timing", "idc_batch_destroy",
+    "idc_batch_set_shape", "idc_batch_get_shape",
 )
 
 
@@ -99,6 +100,8 @@ def load_library(path: str = LIB_PATH):
     lib.idc_batch_autotune.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), C.c_double, C.c_int]
     lib.idc_batch_last_timing.argtypes = [vp, _dp]
     lib.idc_batch_destroy.argtypes = [vp]
+    lib.idc_batch_set_shape.argtypes = [vp, C.c_int, C.c_int, C.c_int32, C.c_int32]
+    lib.idc_batch_get_shape.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
     lib.idc_idc_integrate.argtypes = [vp, vp, vp, C.c_double, C.c_int64, C.c_int32, C.c_int32, C.c_int, C.c_int,
                                       C.c_double, C.c_int32, C.c_int64, C.c_int, C.c_int, C.POINTER(C.c_int64)]
     lib.idc_adjoint_grad.argtypes = [vp, vp, vp, C.c_double, C.c_double, C.c_int32, C.c_int64, C.c_int, vp, vp, vp,
@@ -312,6 +315,16 @@ class Batch:
     def autotune(self, src_ptrs, out_ptrs, dt=np.inf, precision=PREC_FP64):
         _check(self._lib.idc_batch_autotune(self._h, self._arr(src_ptrs), self._arr(out_ptrs), float(dt),
                                             int(precision)), "idc_batch_autotune")
+
+    def set_shape(self, dg_degree: int, precision: int, seg: int, warps: int):
+        _check(self._lib.idc_batch_set_shape(self._h, int(dg_degree), int(precision), int(seg), int(warps)),
+               "idc_batch_set_shape")
+
+    def get_shape(self, dg_degree: int, precision: int):
+        sg, wp = C.c_int32(), C.c_int32()
+        _check(self._lib.idc_batch_get_shape(self._h, int(dg_degree), int(precision), C.byref(sg), C.byref(wp)),
+               "idc_batch_get_shape")
+        return int(sg.value), int(wp.value)
 
     def last_ms(self) -> float:
         ms = C.c_double()

@@ -219,6 +219,10 @@ int idc_batch_sweep(idc_batch *b, const double *const *sources, double *const *r
                     double dt, int precision);
 int idc_batch_autotune(idc_batch *b, const double *const *sources, double *const *results, double dt, int precision);
 int idc_batch_last_timing(idc_batch *b, double *ms);
+/* The tile shape a batch uses for its problems of DG degree dg_degree at `precision` (what the autotuner
+ * picked, the default, or what was set; set 0, 0 to return to the default). */
+int idc_batch_set_shape(idc_batch *b, int dg_degree, int precision, int32_t seg, int32_t warps);
+int idc_batch_get_shape(idc_batch *b, int dg_degree, int precision, int32_t *seg, int32_t *warps);
 int idc_batch_destroy(idc_batch *b);
 
 /* ---- discrete adjoint --------------------------------------------------------------------------------- */
