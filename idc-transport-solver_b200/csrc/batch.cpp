@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 
 namespace idc {
 
@@ -65,6 +66,8 @@ void Batch::release() {
         cudaFree(g.d_items);
         cudaFree(g.d_sync);
         cudaFree(g.d_table);
+        cudaFreeHost(g.h_table);
+        if (g.upload_done) cudaEventDestroy(g.upload_done);
         for (double *p : g.trace) cudaFree(p);
         for (double *p : g.phi_part) cudaFree(p);
         for (double *p : g.inflow) cudaFree(p);
@@ -127,6 +130,9 @@ Status Batch::build_group(Group &g, int precision) {
     IDC_TRY_CUDA(cudaMalloc(&g.d_sync, sizeof(int) * 2));
     IDC_TRY_CUDA(cudaMemset(g.d_sync, 0, sizeof(int) * 2));
     IDC_TRY_CUDA(cudaMalloc(&g.d_table, sizeof(SweepArgs) * g.members.size()));
+    IDC_TRY_CUDA(cudaMallocHost(&g.h_table, sizeof(SweepArgs) * g.members.size()));
+    IDC_TRY_CUDA(cudaEventCreateWithFlags(&g.upload_done, cudaEventDisableTiming));
+    g.uploaded.clear();
     g.trace.assign(g.members.size(), nullptr);
     g.trace_len.assign(g.members.size(), 0);
     g.phi_part.assign(g.members.size(), nullptr);
@@ -136,7 +142,7 @@ Status Batch::build_group(Group &g, int precision) {
         const size_t tl = per[m].size() * (size_t)c.nx * g.G * c.P;   // one trace row per item of the member
         IDC_TRY_CUDA(cudaMalloc(&g.trace[m], sizeof(double) * tl));
         g.trace_len[m] = tl;
-        IDC_TRY_CUDA(launch_fill_u64(reinterpret_cast<unsigned long long *>(g.trace[m]), tl, kTraceSentinel, c0.stream));
+        IDC_TRY_CUDA(launch_fill_u64(reinterpret_cast<unsigned long long *>(g.trace[m]), tl, kTraceSentinel, stream()));
         IDC_TRY_CUDA(cudaMalloc(&g.phi_part[m], sizeof(double) * (size_t)ipr[m] * c.phi_len()));
         IDC_TRY_CUDA(cudaMalloc(&g.inflow[m], sizeof(double) * (size_t)(c.nx + c.ny) * c.nq * c.P));
     }
@@ -146,14 +152,14 @@ Status Batch::build_group(Group &g, int precision) {
     if (per_sm < 1) return bad(IDC_ERR_UNSUPPORTED, "batched sweep kernel does not fit on an SM");
     g.grid = std::min(g.n_items, per_sm * c0.num_sms);
     g.precision = precision;
-    IDC_TRY_CUDA(cudaStreamSynchronize(c0.stream));
+    IDC_TRY_CUDA(cudaStreamSynchronize(stream()));
     return Status::ok();
 }
 
 Status Batch::launch_group(Group &g, const double *const *srcs, double *const *outs, const double *const *phi_sc,
                            double scale, double *const *phis, double dt) {
     Context &c0 = *members[g.members[0]];
-    cudaStream_t st = c0.stream;
+    cudaStream_t st = stream();
     std::vector<SweepArgs> table(g.members.size());
     for (size_t m = 0; m < g.members.size(); ++m) {
         const int p = g.members[m];
@@ -191,24 +197,33 @@ Status Batch::launch_group(Group &g, const double *const *srcs, double *const *o
             a.phi_part = g.phi_part[m];
             a.phi_slots = g.items_per_rb[m];
             a.phi_slot_stride = c.phi_len();
+            a.phi = phis[p];   // the batched reduction's output (the sweep kernel writes the slots)
         }
-        if (a.src) {
-            IDC_TRY_CUDA(launch_inflow_traces(c.P, g.precision != IDC_PREC_FP32_REFINED, a.src, c.d_xi, c.d_eta, (int)c.nx,
-                                              (int)c.ny, (int)c.nq, g.inflow[m], st));
-            a.inflow = g.inflow[m];
-        }
+        if (a.src) a.inflow = g.inflow[m];
+    }
+    bool any_src = false, any_phi = false;
+    for (const auto &a : table) {
+        any_src |= a.src != nullptr;
+        any_phi |= a.phi != nullptr;
+    }
+    // upload the table only when it changed (pinned source: no stream synchronisation)
+    const size_t bytes = sizeof(SweepArgs) * table.size();
+    if (g.uploaded.size() != table.size() || std::memcmp(g.uploaded.data(), table.data(), bytes) != 0) {
+        IDC_TRY_CUDA(cudaEventSynchronize(g.upload_done));   // the previous upload no longer reads h_table
+        std::memcpy(g.h_table, table.data(), bytes);
+        IDC_TRY_CUDA(cudaMemcpyAsync(g.d_table, g.h_table, bytes, cudaMemcpyHostToDevice, st));
+        IDC_TRY_CUDA(cudaEventRecord(g.upload_done, st));
+        g.uploaded = table;
     }
     SweepArgs launch = table[0];   // the launch-wide fields (items, queue, error, tile shape) are common
-    IDC_TRY_CUDA(cudaMemcpyAsync(g.d_table, table.data(), sizeof(SweepArgs) * table.size(), cudaMemcpyHostToDevice, st));
+    // three launches per degree, whatever the number of problems: inflow traces, the sweep, the moments
+    if (any_src)
+        IDC_TRY_CUDA(launch_batched_helpers(c0.P, g.precision != IDC_PREC_FP32_REFINED, g.d_table, (int)table.size(),
+                                            true, false, st));
     IDC_TRY_CUDA(cudaMemsetAsync(g.d_sync, 0, sizeof(int), st));
     IDC_TRY_CUDA(launch_sweep_modal_batched(c0.P, g.precision, launch, g.d_table, g.grid, g.smem, st));
-    for (size_t m = 0; m < g.members.size(); ++m) {
-        const int p = g.members[m];
-        if (phis && phis[p]) {
-            Context &c = *members[p];
-            IDC_TRY_CUDA(launch_reduce_phi_partials(c.dims(), g.phi_part[m], g.items_per_rb[m], c.phi_len(), phis[p], st));
-        }
-    }
+    if (any_phi)
+        IDC_TRY_CUDA(launch_batched_helpers(c0.P, false, g.d_table, (int)table.size(), false, true, st));
     return Status::ok();
 }
 

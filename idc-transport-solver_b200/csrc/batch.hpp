@@ -35,6 +35,9 @@ private:
         SweepItem *d_items = nullptr;
         int *d_sync = nullptr;
         SweepArgs *d_table = nullptr;
+        SweepArgs *h_table = nullptr;            // pinned: uploads do not synchronise the stream
+        std::vector<SweepArgs> uploaded;         // the table on the device (re-uploaded only on change)
+        cudaEvent_t upload_done = nullptr;       // the last upload has read h_table
         std::vector<double *> trace, phi_part, inflow;
         std::vector<size_t> trace_len;
     };
@@ -42,6 +45,9 @@ private:
     Status launch_group(Group &g, const double *const *srcs, double *const *outs, const double *const *phi_sc,
                         double scale, double *const *phis, double dt);
     void release();
+    // every group launches on the first member's stream, so that one synchronisation and one event pair
+    // cover the whole batched sweep
+    cudaStream_t stream() const { return members[0]->stream; }
     std::vector<Group> groups;
 };
 

@@ -91,6 +91,11 @@ cudaError_t launch_sweep_modal(int P, int precision, const SweepArgs &args, int 
 // FP64 or refined precision.
 cudaError_t launch_sweep_modal_batched(int P, int precision, const SweepArgs &launch, const SweepArgs *table, int grid,
                                        size_t smem, cudaStream_t stream);
+// The batched launch's helpers, one launch each for all `members` problems of the table: inflow traces
+// (into each problem's `inflow` from its `src`, packed modal if modal_inflow) and the moment reduction
+// (each problem's `phi_part` slots into its `phi`).
+cudaError_t launch_batched_helpers(int P, bool modal_inflow, const SweepArgs *table, int members, bool inflow,
+                                   bool reduce, cudaStream_t stream);
 cudaError_t sweep_modal_occupancy(int P, int precision, int seg, int threads, size_t smem, int *blocks_per_sm);
 size_t sweep_modal_smem_bytes(int P, int wn, int G, int seg);
 // Inflow traces of the ghost cells of `src` for the modal kernel: out[(k * nq + q) * P + m], k < nx the

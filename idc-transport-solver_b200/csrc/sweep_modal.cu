@@ -67,6 +67,71 @@ __global__ void inflow_traces_kernel(const double *src, const double *xi, const 
     }
 }
 
+// Batched forms of the inflow-trace kernel and of the moment reduction: one launch for every problem of
+// a batched sweep (blockIdx.y = problem), reading the problems' arrays from the launch's SweepArgs table.
+template <int P, bool MODAL>
+__global__ void inflow_traces_batched_kernel(const SweepArgs *__restrict__ table) {
+    const SweepArgs &a = table[blockIdx.y];
+    if (!a.src || !a.inflow) return;
+    constexpr int N = P * P;
+    const int nx = a.nx, ny = a.ny, nq = a.nq;
+    for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < (size_t)(nx + ny) * nq;
+         idx += (size_t)gridDim.x * blockDim.x) {
+        const int k = (int)(idx / nq), q = (int)(idx % nq);
+        const bool xneg = a.xi[q] < 0, yneg = a.eta[q] < 0;
+        int i, j;
+        if (k < nx) {
+            i = xneg ? nx - k : 1 + k;
+            j = yneg ? ny + 1 : 0;
+        } else {
+            i = xneg ? nx + 1 : 0;
+            j = yneg ? ny - (k - nx) : 1 + (k - nx);
+        }
+        const double *v = a.src + (((size_t)i * (ny + 2) + j) * nq + q) * N;
+        double h[P];
+#pragma unroll
+        for (int m = 0; m < P; ++m) h[m] = 0.0;
+#pragma unroll
+        for (int d = 0; d < P; ++d)
+#pragma unroll
+            for (int e = 0; e < P; ++e) {
+                const double sgn = ((xneg && (d & 1)) != (yneg && (e & 1))) ? -1.0 : 1.0;
+                const double val = sgn * v[e + P * d];
+                if (k < nx)
+                    h[d] += val;
+                else
+                    h[e] += val;
+            }
+        double *o = const_cast<double *>(a.inflow) + idx * P;   // the batch owns these trace buffers
+#pragma unroll
+        for (int m = 0; m < P; ++m) {
+            if (MODAL) {
+                double acc = 0.0;
+#pragma unroll
+                for (int n = 0; n < P; ++n) acc = fma(ModalTable<P>::W(m, n), h[n], acc);
+                o[m] = acc;
+            } else {
+                o[m] = h[m];
+            }
+        }
+    }
+}
+
+// phi = sum of the problem's partial-moment slots (fixed order), ghost cells zero; phi is the table's `phi`.
+__global__ void reduce_partials_batched_kernel(const SweepArgs *__restrict__ table, int N) {
+    const SweepArgs &a = table[blockIdx.y];
+    if (!a.phi || !a.phi_part) return;
+    const size_t total = (size_t)(a.nx + 2) * (a.ny + 2) * N;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const size_t cell = t / N;
+        const int i = (int)(cell / (a.ny + 2)), j = (int)(cell % (a.ny + 2));
+        double acc = 0.0;
+        if (i >= 1 && i <= a.nx && j >= 1 && j <= a.ny)
+            for (int sl = 0; sl < a.phi_slots; ++sl) acc += a.phi_part[(size_t)sl * a.phi_slot_stride + t];
+        a.phi[t] = acc;
+    }
+}
+
 template <int P, int MODE, bool ADJ>
 cudaError_t launch_dir(const SweepArgs &args, int grid, size_t smem, cudaStream_t stream) {
     switch (args.seg) {
@@ -165,6 +230,25 @@ cudaError_t launch_sweep_modal_batched(int P, int precision, const SweepArgs &la
                                       : launch_batched_t<3, 1>(launch, table, grid, smem, stream);
         default: return cudaErrorInvalidValue;
     }
+}
+
+cudaError_t launch_batched_helpers(int P, bool modal_inflow, const SweepArgs *table, int members, bool inflow,
+                                   bool reduce, cudaStream_t stream) {
+    if (members < 1 || members > 65535) return cudaErrorInvalidValue;
+    const dim3 grid(148, (unsigned)members), block(128);
+    if (inflow) {
+        switch (P) {
+            case 1: modal_inflow ? inflow_traces_batched_kernel<1, true><<<grid, block, 0, stream>>>(table)
+                                 : inflow_traces_batched_kernel<1, false><<<grid, block, 0, stream>>>(table); break;
+            case 2: modal_inflow ? inflow_traces_batched_kernel<2, true><<<grid, block, 0, stream>>>(table)
+                                 : inflow_traces_batched_kernel<2, false><<<grid, block, 0, stream>>>(table); break;
+            case 3: modal_inflow ? inflow_traces_batched_kernel<3, true><<<grid, block, 0, stream>>>(table)
+                                 : inflow_traces_batched_kernel<3, false><<<grid, block, 0, stream>>>(table); break;
+            default: return cudaErrorInvalidValue;
+        }
+    }
+    if (reduce) reduce_partials_batched_kernel<<<dim3(148, (unsigned)members), 256, 0, stream>>>(table, P * P);
+    return cudaGetLastError();
 }
 
 cudaError_t sweep_modal_occupancy(int P, int precision, int seg, int threads, size_t smem, int *blocks_per_sm) {
