@@ -36,19 +36,18 @@ Status bad(int code, const std::string &m) {
     return s;
 }
 
-// Default shape: the widest segment whose lane use is within 10 points of the best (fewer chunks and
-// items), 7 compute warps.
-void default_shape(int qmax, int *seg, int *wn) {
+// Default shape: the narrowest segment with the best lane use, the single problem's default warps.
+void default_shape(int P, int qmax, int *seg, int *wn) {
     double best = -1.0;
-    for (int cand : {32, 16, 8, 4}) {
+    for (int cand : {4, 8, 16, 32}) {
         const int nch = (qmax + cand - 1) / cand;
         const double eff = (double)qmax / (nch * cand);
-        if (eff > best + 0.1) {
+        if (eff > best + 1e-9) {
             best = eff;
             *seg = cand;
         }
     }
-    *wn = 7;
+    *wn = sweep_modal_default_wn(P);
 }
 
 int qmax_of(const Context &c) {
@@ -87,8 +86,9 @@ Status Batch::add(Context *c) {
 
 Status Batch::build_group(Group &g, int precision) {
     Context &c0 = *members[g.members[0]];
+    g.G = g.seg;
+    g.wn = sweep_modal_fit_wn(c0.P, precision, g.wn, g.G, g.seg);
     const int seg = g.seg, wn = g.wn, rw = 32 / seg, rows_cta = wn * rw;
-    g.G = seg;
     std::vector<std::vector<SweepItem>> per(g.members.size());
     std::vector<int> nrb(g.members.size()), ipr(g.members.size());
     for (size_t m = 0; m < g.members.size(); ++m) {
@@ -147,8 +147,8 @@ Status Batch::build_group(Group &g, int precision) {
         IDC_TRY_CUDA(cudaMalloc(&g.inflow[m], sizeof(double) * (size_t)(c.nx + c.ny) * c.nq * c.P));
     }
     int per_sm = 0;
-    g.smem = sweep_modal_smem_bytes(c0.P, wn, g.G, seg);
-    IDC_TRY_CUDA(sweep_modal_occupancy(c0.P, precision, seg, (wn + 1) * 32, g.smem, &per_sm));
+    g.smem = sweep_modal_smem_bytes(c0.P, precision, wn, g.G, seg);
+    IDC_TRY_CUDA(sweep_modal_occupancy(c0.P, precision, seg, sweep_modal_threads(c0.P, wn), g.smem, &per_sm));
     if (per_sm < 1) return bad(IDC_ERR_UNSUPPORTED, "batched sweep kernel does not fit on an SM");
     g.grid = std::min(g.n_items, per_sm * c0.num_sms);
     g.precision = precision;
@@ -248,9 +248,9 @@ Status Batch::sweep(const double *const *srcs, double *const *outs, const double
             const auto key = std::make_pair(P, precision);
             if (tuned.count(key)) {
                 g.seg = tuned[key].first;
-                g.wn = tuned[key].second;
+                g.wn = std::min(tuned[key].second, sweep_modal_max_wn(P));
             } else {
-                default_shape(qmax, &g.seg, &g.wn);
+                default_shape(P, qmax, &g.seg, &g.wn);
             }
             g.precision = precision;
             groups.push_back(g);
@@ -306,7 +306,7 @@ void Batch::get_shape(int P, int precision, int *seg, int *wn) const {
         *seg = *wn = 0;
         return;
     }
-    default_shape(qmax, seg, wn);
+    default_shape(P, qmax, seg, wn);
 }
 
 Status Batch::autotune(const double *const *srcs, double *const *outs, double dt, int precision) {
@@ -318,7 +318,7 @@ Status Batch::autotune(const double *const *srcs, double *const *outs, double dt
         float best = 1e30f;
         std::pair<int, int> bsh{0, 0};
         for (int cs : {4, 8, 16, 32})
-            for (int cw : {3, 5, 7}) {
+            for (int cw = std::max(1, sweep_modal_max_wn(P) - 3); cw <= sweep_modal_max_wn(P); ++cw) {
                 tuned[std::make_pair(P, precision)] = {cs, cw};
                 release();
                 for (int rep = 0; rep < 2; ++rep) IDC_TRY(sweep(srcs, outs, nullptr, 1.0, nullptr, dt, precision));

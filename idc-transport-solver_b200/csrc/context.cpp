@@ -170,8 +170,9 @@ Status Context::autotune(const double *src, double dt, int precision, int *seg_o
     IDC_TRY(ensure_phi_buffers(1));
     float best = 1e30f;
     int bs = 0, bw = 0;
+    const int mw = sweep_modal_max_wn(P);
     for (int cs : {4, 8, 16, 32})
-        for (int cw : {3, 5, 7}) {
+        for (int cw = std::max(1, mw - 3); cw <= mw; ++cw) {
             IDC_TRY(set_tile_shape(cs, cw));
             float ms = 0.f;
             for (int rep = 0; rep < 2; ++rep) {
@@ -214,9 +215,12 @@ Status Context::ensure_phi_buffers(int count) {
 
 // Tile shape of the warp and modal kernels: ordinates of a quadrant are split into nch chunks of at most
 // G ordinates, each chunk on a row segment of `seg` lanes (a power of two, at least 4); a warp holds
-// 32/seg rows and a CTA wn compute warps (at most 7, plus the helper warp).
-static void choose_warp_tiling(int qmax, int user_G, int user_rows, int max_wn, int *G_out, int *seg_out,
-                               int *wn_out) {
+// 32/seg rows and a CTA wn compute warps (at most max_wn, default default_wn; the modal kernel adds a
+// helper warp and its aux warps, the warp kernel the helper warp).  The warp kernel prefers wide
+// segments; the modal kernel the narrowest segment with the best lane use (4 lanes, 8 rows per warp:
+// measured fastest on B200 at S4..S16).
+static void choose_warp_tiling(int qmax, int user_G, int user_rows, int max_wn, int default_wn, bool narrow,
+                               int *G_out, int *seg_out, int *wn_out) {
     int seg = 16, G = 0;
     if (user_G > 0) {
         G = std::min(user_G, 32);
@@ -226,11 +230,12 @@ static void choose_warp_tiling(int qmax, int user_G, int user_rows, int max_wn, 
         // from wide to narrow: a narrower segment must use its lanes clearly better (> 10 points) to win,
         // since every extra chunk adds moment atomics and work items
         double best = -1.0;
-        for (int cand : {32, 16, 8, 4}) {
+        for (int k = 0; k < 4; ++k) {
+            const int cand = narrow ? (4 << k) : (32 >> k);
             const int nch = (qmax + cand - 1) / cand;
             const int g = (qmax + nch - 1) / nch;
             const double eff = (double)qmax / (nch * cand);
-            if (eff > best + 0.1) {
+            if (eff > best + (narrow ? 1e-9 : 0.1)) {
                 best = eff;
                 seg = cand;
                 G = g;
@@ -238,7 +243,7 @@ static void choose_warp_tiling(int qmax, int user_G, int user_rows, int max_wn, 
         }
     }
     const int rw = 32 / seg;
-    int wn = user_rows > 0 ? std::max(1, user_rows / rw) : 7;
+    int wn = user_rows > 0 ? std::max(1, user_rows / rw) : default_wn;
     wn = std::min(wn, max_wn);
     *G_out = G;
     *seg_out = seg;
@@ -252,14 +257,18 @@ Status Context::build_schedule(int precision) {
     for (int k = 0; k < 4; ++k) qmax = std::max<int>(qmax, (int)(quad[k + 1] - quad[k]));
     if (qmax == 0) return bad(IDC_ERR_ARG, "no ordinates");
     int G = 0, R = 0;
+    const int max_wn = kernel == kModal ? sweep_modal_max_wn(P) : 7;
     if (use_warp_kernel && tune_seg > 0) {
         seg = tune_seg;
-        wn = tune_wn;
+        wn = std::min(tune_wn, max_wn);
         const int nch = (qmax + seg - 1) / seg;
         G = (qmax + nch - 1) / nch;
+        if (kernel == kModal) wn = sweep_modal_fit_wn(P, precision, wn, G, seg);
         R = wn * (32 / seg);
     } else if (use_warp_kernel) {
-        choose_warp_tiling(qmax, user_G, user_R, 7, &G, &seg, &wn);
+        choose_warp_tiling(qmax, user_G, user_R, max_wn, kernel == kModal ? sweep_modal_default_wn(P) : 7,
+                           kernel == kModal, &G, &seg, &wn);
+        if (kernel == kModal) wn = sweep_modal_fit_wn(P, precision, wn, G, seg);
         R = wn * (32 / seg);
     } else {
         const int max_threads = 320;
@@ -330,8 +339,8 @@ Status Context::build_schedule(int precision) {
 
     int per_sm = 0;
     if (kernel == kModal) {
-        block = (wn + 1) * 32;
-        smem = sweep_modal_smem_bytes(P, wn, G, seg);
+        block = sweep_modal_threads(P, wn);
+        smem = sweep_modal_smem_bytes(P, precision, wn, G, seg);
         IDC_TRY_CUDA(sweep_modal_occupancy(P, precision, seg, block, smem, &per_sm));
     } else if (kernel == kWarp) {
         block = (wn + 1) * 32;

@@ -69,6 +69,7 @@ __device__ __forceinline__ void cp_wait() {
 // Bounded, warp-uniform wait on an mbarrier phase.  Returns false if the wait gave up or another warp
 // has recorded an error; in both cases the device error word is non-zero afterwards.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *error, long long limit) {
+    if (mbar_test(bar, parity)) return true;   // a completed phase: the non-blocking test is cheaper
     for (long long n = 0;; ++n) {
         if (mbar_try(bar, parity)) return true;
         if ((n & 63) == 63 && ld_relaxed(error) != kDevOk) return false;

@@ -81,6 +81,7 @@ cudaError_t launch_sweep_warp(int P, int precision, const SweepArgs &args, int g
 cudaError_t sweep_warp_occupancy(int P, int precision, int threads, size_t smem, int *blocks_per_sm);
 size_t sweep_warp_smem_bytes(int P, int wn, int G, int seg);
 constexpr int kWarpRingSlots = 8;
+constexpr int kModalSolutionSlots = 4;   // modal kernel: step results in flight per compute warp
 
 // Modal sweep kernel (sweep_modal.cu): same arguments as the warp kernel plus `inflow`, traces of P values.
 cudaError_t launch_sweep_modal(int P, int precision, const SweepArgs &args, int grid, size_t smem, cudaStream_t stream);
@@ -97,7 +98,14 @@ cudaError_t launch_sweep_modal_batched(int P, int precision, const SweepArgs &la
 cudaError_t launch_batched_helpers(int P, bool modal_inflow, const SweepArgs *table, int members, bool inflow,
                                    bool reduce, cudaStream_t stream);
 cudaError_t sweep_modal_occupancy(int P, int precision, int seg, int threads, size_t smem, int *blocks_per_sm);
-size_t sweep_modal_smem_bytes(int P, int wn, int G, int seg);
+size_t sweep_modal_smem_bytes(int P, int precision, int wn, int G, int seg);
+// Modal kernel CTA shape: wn compute warps, one helper warp and one or two aux warps per compute warp;
+// at most sweep_modal_max_wn(P) compute warps (the register file holds one CTA).  fit_wn: the largest
+// wn <= the given one whose shared memory fits the device.
+int sweep_modal_max_wn(int P);
+int sweep_modal_default_wn(int P);   // the most compute warps with two aux warps each
+int sweep_modal_threads(int P, int wn);
+int sweep_modal_fit_wn(int P, int precision, int wn, int G, int seg);
 // Inflow traces of the ghost cells of `src` for the modal kernel: out[(k * nq + q) * P + m], k < nx the
 // ghost row below column k, k >= nx the ghost column left of row k - nx (sweep order); packed modal
 // coefficients if `modal`, else sign-flipped physical traces.

@@ -2,6 +2,8 @@
 // memory size, and the inflow-trace kernel.  The kernels are in sweep_modal_impl.cuh.
 #include "sweep_modal_impl.cuh"
 
+#include <algorithm>
+
 IDC_MODAL_LAUNCHERS(extern, 0, false)
 IDC_MODAL_LAUNCHERS(extern, 0, true)
 IDC_MODAL_LAUNCHERS(extern, 1, false)
@@ -15,7 +17,6 @@ namespace idc {
 namespace {
 
 using modal::kS;
-using modal::kMaxWarps;
 using modal::prefetch_depth;
 
 // Inflow traces of the ghost cells, one thread per (boundary position k, ordinate q):
@@ -186,13 +187,39 @@ cudaError_t launch_batched_t(const SweepArgs &launch, const SweepArgs *table, in
 
 }  // namespace
 
-size_t sweep_modal_smem_bytes(int P, int wn, int G, int seg) {
-    const int N = P * P;
-    return sizeof(uint64_t) * 2 * (wn + 1) * kS +
-           sizeof(double) * ((size_t)(wn + 1) * kS * G * P + (size_t)wn * prefetch_depth(P) * 32 * N +
-                             (size_t)wn * prefetch_depth(P) * (32 / seg) * (N + 2) + (size_t)((G + 1) & ~1) +
-                             (size_t)2 * wn * 32 * N);
+template <int P>
+size_t smem_p(int precision, int wn, int G, int seg) {
+    const int na = modal::aux_per_compute(P, wn), D = prefetch_depth(P), rw = 32 / seg;
+    switch (precision) {
+        case 0: return modal::layout_bytes(wn, na, G, P, D, rw, modal::cellin_words<P, 0>());
+        case 1: return modal::layout_bytes(wn, na, G, P, D, rw, modal::cellin_words<P, 1>());
+        default: return modal::layout_bytes(wn, na, G, P, D, rw, modal::cellin_words<P, 2>());
+    }
 }
+
+size_t sweep_modal_smem_bytes(int P, int precision, int wn, int G, int seg) {
+    switch (P) {
+        case 1: return smem_p<1>(precision, wn, G, seg);
+        case 2: return smem_p<2>(precision, wn, G, seg);
+        default: return smem_p<3>(precision, wn, G, seg);
+    }
+}
+
+int sweep_modal_threads(int P, int wn) { return modal::cta_warps(P, wn) * 32; }
+
+int sweep_modal_default_wn(int P) { return (modal::max_warps(P) - 1) / 3; }
+
+int sweep_modal_fit_wn(int P, int precision, int wn, int G, int seg) {
+    int dev = 0, limit = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&limit, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+        limit = 227 * 1024;
+    wn = std::min(wn, modal::max_compute_warps(P));
+    while (wn > 1 && sweep_modal_smem_bytes(P, precision, wn, G, seg) > (size_t)limit) --wn;
+    return wn;
+}
+
+int sweep_modal_max_wn(int P) { return modal::max_compute_warps(P); }
 
 #define IDC_MDISPATCH(P_, FN, ...)             \
     switch (precision) {                       \
@@ -204,7 +231,7 @@ size_t sweep_modal_smem_bytes(int P, int wn, int G, int seg) {
 
 cudaError_t launch_sweep_modal(int P, int precision, const SweepArgs &args, int grid, size_t smem,
                                cudaStream_t stream) {
-    if (args.wn < 1 || args.wn + 1 > kMaxWarps || !args.trace || args.seg < 4 || args.seg > 32 ||
+    if (args.wn < 1 || args.wn > sweep_modal_max_wn(P) || !args.trace || args.seg < 4 || args.seg > 32 ||
         (args.seg & (args.seg - 1)) || args.G > args.seg)
         return cudaErrorInvalidValue;
     switch (P) {
@@ -217,7 +244,7 @@ cudaError_t launch_sweep_modal(int P, int precision, const SweepArgs &args, int 
 
 cudaError_t launch_sweep_modal_batched(int P, int precision, const SweepArgs &launch, const SweepArgs *table, int grid,
                                        size_t smem, cudaStream_t stream) {
-    if (launch.wn < 1 || launch.wn + 1 > kMaxWarps || launch.seg < 4 || launch.seg > 32 || (launch.seg & (launch.seg - 1)) ||
+    if (launch.wn < 1 || launch.wn > sweep_modal_max_wn(P) || launch.seg < 4 || launch.seg > 32 || (launch.seg & (launch.seg - 1)) ||
         launch.G > launch.seg || !table || launch.adjoint)
         return cudaErrorInvalidValue;
     if (precision != 0 && precision != 1) return cudaErrorInvalidValue;

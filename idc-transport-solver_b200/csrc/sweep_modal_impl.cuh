@@ -16,9 +16,12 @@
 //     themselves (a slot holds a NaN-payload sentinel that arithmetic never produces; 8-byte accesses
 //     are single-copy atomic), copies ready columns into ring 0 and re-arms the slots.  The first row
 //     block's helper copies the inflow traces of the ghost row (inflow_traces_kernel) instead.
-//   * each lane prefetches its next cells' source with cp.async (lane o == 0 of a row also sigma_t and
-//     the fused scattering source), prefetch_depth(P) cells ahead, into a per-warp stage ring.
 //   * the loop over columns is instantiated per quadrant, so the quadrant's sign flips are constants.
+//   * each compute warp has one or two aux warps and a ring of kModalSolutionSlots step slots: an aux
+//     warp loads a step's source (cp.async), prepares its inputs (modal source, reciprocals) into the
+//     slot, and after the compute warp has left the step result there, transforms it back to the cell
+//     dofs, stores psi and forms the moments.  A compute warp's step is thus only the inputs' wait,
+//     receive, cell step and send: the cell-to-cell dependency chain and little else.
 //   * the fused moments phi = sum_q w_q psi_q: a row segment's weighted values meet in shared memory and
 //     one partial moment per (cell, dof, ordinate chunk) is stored; reduce_phi_partials (ops_kernels.cu)
 //     adds the chunks in a fixed order, so phi is bitwise reproducible.
@@ -52,36 +55,22 @@ namespace idc {
 namespace modal {
 
 constexpr int kS = kWarpRingSlots;
-constexpr int kMaxWarps = 8;   // up to 7 compute warps + 1 helper
+constexpr int kZ = kModalSolutionSlots;
+
+// Warps per CTA: Wn compute warps, the helper warp and nA aux warps per compute warp, bounded so that
+// the register file holds one CTA (the degree sets the registers a thread needs; warps are allocated in
+// groups of four, so 11 warps get the registers of 12).  Two aux warps per compute warp when they fit.
+__host__ __device__ constexpr int max_warps(int P) { return P == 3 ? 11 : 15; }
+__host__ __device__ constexpr int max_compute_warps(int P) { return (max_warps(P) - 1) / 2; }
+__host__ __device__ constexpr int aux_per_compute(int P, int wn) { return 3 * wn + 1 <= max_warps(P) ? 2 : 1; }
+__host__ __device__ constexpr int cta_warps(int P, int wn) { return wn * (1 + aux_per_compute(P, wn)) + 1; }
 
 __device__ __forceinline__ int T_steps(int nx, int Rw) { return nx + Rw - 1; }
 
-// Source prefetch depth (cells ahead per lane) within the shared-memory budget.
-__host__ __device__ constexpr int prefetch_depth(int P) { return P == 3 ? 4 : 8; }
+// Source prefetch depth of an aux warp (cells ahead per lane, in its own steps).
+__host__ __device__ constexpr int prefetch_depth(int) { return 4; }
 
-struct Layout {
-    uint64_t *full, *empty;   // [Wn+1][kS]
-    double *ring;             // [Wn+1][kS][G][P]: y traces
-    double *src;              // [Wn][D][32][N]: each lane's cell source dofs
-    double *cellst;           // [Wn][D][32/seg][N+2]: per row: sigma_t, sigma_s, phi_scatter[N]
-    double *w;                // [G]
-    double *red;              // [2][Wn][32][N]: per-lane weighted values for the moment reduction
-};
-
-__device__ __forceinline__ Layout carve(unsigned char *raw, int wn, int G, int P, int D, int rw) {
-    const int N = P * P;
-    Layout L;
-    L.full = reinterpret_cast<uint64_t *>(raw);
-    L.empty = L.full + (wn + 1) * kS;
-    L.ring = reinterpret_cast<double *>(L.empty + (wn + 1) * kS);
-    L.src = L.ring + (size_t)(wn + 1) * kS * G * P;
-    L.cellst = L.src + (size_t)wn * D * 32 * N;
-    L.w = L.cellst + (size_t)wn * D * rw * (N + 2);
-    L.red = L.w + ((G + 1) & ~1);
-    return L;
-}
-
-// Inputs of one cell step prepared ahead of the step.  MODE 0 / 2: packed modal source and reciprocal
+// Inputs of one cell step, prepared by an aux warp.  MODE 0 / 2: packed modal source and reciprocal
 // denominators.  MODE 1: the sign-flipped physical source, FP32 reciprocals and s = sigma_t + 1/dt.
 template <int P, int MODE>
 struct CellIn {
@@ -90,6 +79,45 @@ struct CellIn {
     ModalRecip<P, TS> r;
     double s;
 };
+template <int P, int MODE>
+__host__ __device__ constexpr int cellin_words() {
+    static_assert(sizeof(CellIn<P, MODE>) % 8 == 0, "CellIn is a whole number of 8-byte words");
+    return (int)(sizeof(CellIn<P, MODE>) / 8);
+}
+
+struct Layout {
+    uint64_t *full, *empty;      // [Wn+1][kS]: y-trace rings
+    uint64_t *in_full, *z_full;  // [Wn][kZ]: step slots (inputs ready / result ready)
+    double *ring;                // [Wn+1][kS][G][P]: y traces
+    double *slot;                // [Wn][kZ][CW + N][32]: a step's inputs (CW 8-byte words) and result
+    double *src;                 // [Wn*nA][D][32][N]: an aux warp's prefetched cell source dofs
+    double *cellst;              // [Wn*nA][D][32/seg][N+2]: per row: sigma_t, sigma_s, phi_scatter[N]
+    double *w;                   // [G]
+    double *red;                 // [Wn*nA][32][N]: an aux warp's weighted values for the moment reduction
+};
+
+__host__ __device__ constexpr size_t layout_bytes(int wn, int na, int G, int P, int D, int rw, int cw) {
+    return sizeof(uint64_t) * (size_t)(2 * (wn + 1) * kS + 2 * wn * kZ) +
+           sizeof(double) * ((size_t)(wn + 1) * kS * G * P + (size_t)wn * kZ * (cw + P * P) * 32 +
+                             (size_t)wn * na * D * 32 * P * P + (size_t)wn * na * D * rw * (P * P + 2) +
+                             (size_t)((G + 1) & ~1) + (size_t)wn * na * 32 * P * P);
+}
+
+__device__ __forceinline__ Layout carve(unsigned char *raw, int wn, int na, int G, int P, int D, int rw, int cw) {
+    const int N = P * P;
+    Layout L;
+    L.full = reinterpret_cast<uint64_t *>(raw);
+    L.empty = L.full + (wn + 1) * kS;
+    L.in_full = L.empty + (wn + 1) * kS;
+    L.z_full = L.in_full + wn * kZ;
+    L.ring = reinterpret_cast<double *>(L.z_full + wn * kZ);
+    L.slot = L.ring + (size_t)(wn + 1) * kS * G * P;
+    L.src = L.slot + (size_t)wn * kZ * (cw + N) * 32;
+    L.cellst = L.src + (size_t)wn * na * D * 32 * N;
+    L.w = L.cellst + (size_t)wn * na * D * rw * (N + 2);
+    L.red = L.w + ((G + 1) & ~1);
+    return L;
+}
 
 template <int P, int MODE, bool XN, bool YN, bool ADJ>
 __device__ __forceinline__ void prep_cell(CellIn<P, MODE> &in, const double *sp, const double *cp, const SweepArgs &a,
@@ -171,40 +199,33 @@ __device__ __forceinline__ void refined_step(double (&xp)[P * P], const CellIn<P
     }
 }
 
-// Compute warp.  Per column step s the loop runs: receive the y trace, the cell step (the only part on
-// the cell-to-cell dependency chain), send the outgoing y trace, then prepare the next cell (modal
-// source, reciprocals) and finish this one (cell dofs, psi store, moments), whose instructions fill the
-// step's latency.  Lanes without a cell this step compute on stale stage data and store nothing.
+// Compute warp.  Per column step s the loop runs: wait for the step's prepared inputs (slot s % kZ),
+// receive the y trace, the cell step (the only part on the cell-to-cell dependency chain), send the
+// outgoing y trace and leave the step result in the slot for the aux warp.  Lanes without a cell this
+// step compute on stale inputs; nothing is stored for them.
 template <int P, int MODE, int SEG, bool XN, bool YN, bool ADJ>
 __device__ __forceinline__ void modal_rows(const SweepArgs &a, const SweepItem &item, const Layout &L, int w,
                                            int lane, bool has_consumer, int it_index) {
     constexpr int N = P * P;
+    constexpr int CW = cellin_words<P, MODE>();
     using TS = std::conditional_t<MODE == 0, double, float>;   // modal solve type
     using TR = std::conditional_t<MODE == 2, float, double>;   // trace type
     using TZ = std::conditional_t<MODE == 1, double, TS>;      // step result (modal Z, or MODE 1 dofs)
     constexpr int seg = SEG, Rw = 32 / SEG;
     const int G = a.G, rows_cta = a.wn * Rw;
     const int rr = lane / seg, o = lane - rr * seg;
-    const int row_w = item.row_block * rows_cta + w * Rw;   // the warp's first row in sweep order
-    const int row = row_w + rr;
-    const bool row_valid = row < a.ny;
-    const bool act = (o < item.q_count) && row_valid;
+    const int row = item.row_block * rows_cta + w * Rw + rr;
+    const bool act = (o < item.q_count) && row < a.ny;
     const int q = item.q_begin + (act ? o : 0);
-    // traversal direction: the quadrant's own, reversed for the transposed sweep
-    constexpr bool TX = XN != ADJ, TY = YN != ADJ;
-    const int j = TY ? (a.ny - row) : (1 + row);
-    const size_t plane = (size_t)a.nq * N;
-    const size_t istride = (size_t)(a.ny + 2) * plane;
     const bool last_warp = w == a.wn - 1;
 
-    double axd = 0.0, ayd = 0.0, wq = 0.0;
+    double axd = 0.0, ayd = 0.0;
     TR f[P];   // x trace (modal, or physical in MODE 1) entering the next cell of this row
 #pragma unroll
     for (int m = 0; m < P; ++m) f[m] = TR(0);
     if (act) {
         axd = fabs(a.xi[q]) / a.dx;
         ayd = fabs(a.eta[q]) / a.dy;
-        wq = L.w[o];
         if (a.inflow) {
             const double *in = a.inflow + ((size_t)(a.nx + row) * a.nq + q) * P;
 #pragma unroll
@@ -215,52 +236,25 @@ __device__ __forceinline__ void modal_rows(const SweepArgs &a, const SweepItem &
     TR gprev[P];   // this lane's outgoing y trace of the previous step
 #pragma unroll
     for (int m = 0; m < P; ++m) gprev[m] = TR(0);
-
-    constexpr int D = prefetch_depth(P);
-    constexpr int NC = N + 2;
-    const int phi_slot = a.phi_slots > 0 ? it_index % a.phi_slots : 0;
-    double *my_src = L.src + ((size_t)w * D * 32 + lane) * N;     // stage b at + b*32*N
-    double *my_cell = L.cellst + ((size_t)w * D * Rw + rr) * NC;  // stage b at + b*Rw*NC
-
-    // One cp.async group per step (possibly empty), D - 1 steps in flight ahead of the current one.
-    auto prefetch = [&](int s) {
-        const int c = s - rr;
-        if (s < T_steps(a.nx, Rw) && row_valid && c >= 0 && c < a.nx) {
-            const int i = TX ? a.nx - c : 1 + c;
-            if (act && a.src) {
-                const double *g = a.src + (size_t)i * istride + (size_t)j * plane + (size_t)q * N;
-                double *d = my_src + (size_t)(s % D) * 32 * N;
-#pragma unroll
-                for (int k = 0; k < N; ++k) cp_async8(d + k, g + k);
-            }
-            if (o == 0) {
-                const size_t cidx = (size_t)i * (a.ny + 2) + j;
-                double *d = my_cell + (size_t)(s % D) * Rw * NC;
-                cp_async8(d, a.sigma_t + cidx);
-                if (a.phi_scatter) {
-                    cp_async8(d + 1, a.sigma_s + cidx);
-#pragma unroll
-                    for (int k = 0; k < N; ++k) cp_async8(d + 2 + k, a.phi_scatter + cidx * N + k);
-                }
-            }
-        }
-        cp_commit();
-    };
+    const unsigned long long *slots = reinterpret_cast<const unsigned long long *>(L.slot) +
+                                      (size_t)w * kZ * (CW + N) * 32 + lane;
 
     const int T = T_steps(a.nx, Rw);
-#pragma unroll
-    for (int s = 0; s < D - 1; ++s) prefetch(s);
-    CellIn<P, MODE> cur;
-    cp_wait<D - 2>();
-    __syncwarp();
-    prep_cell<P, MODE, XN, YN, ADJ>(cur, my_src, my_cell, a, od, wq);
-
     for (int s = 0; s < T; ++s) {
-        prefetch(s + D - 1);
-        cp_wait<D - 2>();   // stage s + 1 has landed
-        __syncwarp();       // lane o == 0's cell-data copies are visible to its row segment
         const int c = s - rr;
         const bool valid = act && c >= 0 && c < a.nx;
+        const int zs = s % kZ;
+
+        // the step's inputs, prepared by the aux warp (word-major in the slot: conflict-free)
+        if (!mbar_wait(L.in_full + w * kZ + zs, (uint32_t)((s / kZ) & 1), a.error, a.spin_limit)) break;
+        CellIn<P, MODE> cur;
+        {
+            unsigned long long wv[CW];
+            const unsigned long long *sp = slots + (size_t)zs * (CW + N) * 32;
+#pragma unroll
+            for (int k = 0; k < CW; ++k) wv[k] = sp[k * 32];
+            memcpy(&cur, wv, sizeof(cur));
+        }
 
         // y trace: rows rr > 0 from the lane seg below in the warp (previous step), row 0 from the ring
         TR g[P];
@@ -316,11 +310,118 @@ __device__ __forceinline__ void modal_rows(const SweepArgs &a, const SweepItem &
             mbar_arrive(L.full + (w + 1) * kS + slot);
         }
 
-        // next cell's inputs (stage s + 1; stale for lanes without a next cell, never stored)
-        prep_cell<P, MODE, XN, YN, ADJ>(cur, my_src + (size_t)((s + 1) % D) * 32 * N,
-                                        my_cell + (size_t)((s + 1) % D) * Rw * NC, a, od, wq);
+        // the step result into the slot (the aux warp reuses the slot for step s + kZ after reading it)
+        TZ *zp = reinterpret_cast<TZ *>(L.slot + ((size_t)(w * kZ + zs) * (CW + N) + CW) * 32) + lane;
+#pragma unroll
+        for (int k = 0; k < N; ++k) zp[k * 32] = Z[k];
+        mbar_arrive(L.z_full + w * kZ + zs);
+    }
+}
 
-        // this cell's dofs, psi and moments
+// Aux warp k of compute warp w (of na): owns the steps s = k (mod na), so the slots s % kZ with the same
+// residue (kZ is a multiple of na).  It prepares the inputs of its first steps, then per owned step s:
+// waits for the result, finishes the cell (cell dofs from the backward modal transform or the MODE 1
+// sign flips, the psi store, the moments) and prepares step s + kZ in the freed slot.  The source is
+// prefetched with cp.async, prefetch_depth() of the warp's own steps ahead, into a per-warp stage ring
+// (lane o == 0 of a row also loads sigma_t and the fused scattering source).  A row segment's weighted
+// values meet in shared memory; the warp's Rw x N (row, dof) sums over each segment's ordinates are
+// spread over the lanes, each a fixed pairwise tree, and stored into this chunk's partial moments.
+template <int P, int MODE, int SEG, bool XN, bool YN, bool ADJ>
+__device__ __forceinline__ void modal_aux(const SweepArgs &a, const SweepItem &item, const Layout &L, int w,
+                                          int k0, int na, int lane, int it_index) {
+    constexpr int N = P * P;
+    constexpr int CW = cellin_words<P, MODE>();
+    using TS = std::conditional_t<MODE == 0, double, float>;
+    using TZ = std::conditional_t<MODE == 1, double, TS>;
+    constexpr int seg = SEG, Rw = 32 / SEG;
+    constexpr int D = prefetch_depth(P);
+    constexpr int NC = N + 2;
+    const int rr = lane / seg, o = lane - rr * seg;
+    const int row_w = item.row_block * a.wn * Rw + w * Rw;
+    const int row = row_w + rr;
+    const bool row_valid = row < a.ny;
+    const bool act = (o < item.q_count) && row_valid;
+    const int q = item.q_begin + (act ? o : 0);
+    constexpr bool TX = XN != ADJ, TY = YN != ADJ;
+    const int j = TY ? (a.ny - row) : (1 + row);
+    const size_t plane = (size_t)a.nq * N;
+    const size_t istride = (size_t)(a.ny + 2) * plane;
+    double axd = 0.0, ayd = 0.0, wq = 0.0;
+    if (act) {
+        axd = fabs(a.xi[q]) / a.dx;
+        ayd = fabs(a.eta[q]) / a.dy;
+        wq = L.w[o];
+    }
+    const ModalOrdinate<P, TS> od = modal_ordinate<P, TS, ADJ>(axd, ayd);
+    const int phi_slot = a.phi_slots > 0 ? it_index % a.phi_slots : 0;
+    const int ai = w * na + k0;   // this aux warp among the CTA's
+    double *red = L.red + (size_t)ai * 32 * N;
+    double *my_src = L.src + ((size_t)ai * D * 32 + lane) * N;     // stage b at + b*32*N
+    double *my_cell = L.cellst + ((size_t)ai * D * Rw + rr) * NC;  // stage b at + b*Rw*NC
+    const int T = T_steps(a.nx, Rw);
+
+    // the warp's own steps in order: target i is step k0 + i na; one cp.async group per target
+    auto prefetch = [&](int i) {
+        const int s = k0 + i * na;
+        const int c = s - rr;
+        if (s < T && row_valid && c >= 0 && c < a.nx) {
+            const int ci = TX ? a.nx - c : 1 + c;
+            if (act && a.src) {
+                const double *g = a.src + (size_t)ci * istride + (size_t)j * plane + (size_t)q * N;
+                double *d = my_src + (size_t)(i % D) * 32 * N;
+#pragma unroll
+                for (int k = 0; k < N; ++k) cp_async8(d + k, g + k);
+            }
+            if (o == 0) {
+                const size_t cidx = (size_t)ci * (a.ny + 2) + j;
+                double *d = my_cell + (size_t)(i % D) * Rw * NC;
+                cp_async8(d, a.sigma_t + cidx);
+                if (a.phi_scatter) {
+                    cp_async8(d + 1, a.sigma_s + cidx);
+#pragma unroll
+                    for (int k = 0; k < N; ++k) cp_async8(d + 2 + k, a.phi_scatter + cidx * N + k);
+                }
+            }
+        }
+        cp_commit();
+    };
+    // prepare target i into its slot and release the slot to the compute warp
+    auto prepare = [&](int i) {
+        prefetch(i + D - 1);
+        cp_wait<D - 2>();   // target i has landed
+        __syncwarp();       // lane o == 0's cell-data copies are visible to its row segment
+        const int s = k0 + i * na;
+        CellIn<P, MODE> cur;
+        prep_cell<P, MODE, XN, YN, ADJ>(cur, my_src + (size_t)(i % D) * 32 * N, my_cell + (size_t)(i % D) * Rw * NC,
+                                        a, od, wq);
+        unsigned long long wv[CW];
+        memcpy(wv, &cur, sizeof(cur));
+        unsigned long long *sp = reinterpret_cast<unsigned long long *>(L.slot) +
+                                 ((size_t)(w * kZ + s % kZ) * (CW + N)) * 32 + lane;
+#pragma unroll
+        for (int k = 0; k < CW; ++k) sp[k * 32] = wv[k];
+        mbar_arrive(L.in_full + w * kZ + s % kZ);
+    };
+
+#pragma unroll
+    for (int i = 0; i < D - 1; ++i) prefetch(i);
+    const int ahead = kZ / na;   // targets in flight: the slots this warp owns
+    for (int i = 0; i < ahead && k0 + i * na < T; ++i) prepare(i);
+
+    for (int i = 0; k0 + i * na < T; ++i) {
+        const int s = k0 + i * na;
+        const int zs = s % kZ;
+        if (!mbar_wait(L.z_full + w * kZ + zs, (uint32_t)((s / kZ) & 1), a.error, a.spin_limit)) break;
+        TZ Z[N];
+        const TZ *zp = reinterpret_cast<const TZ *>(L.slot + ((size_t)(w * kZ + zs) * (CW + N) + CW) * 32) + lane;
+#pragma unroll
+        for (int k = 0; k < N; ++k) Z[k] = zp[k * 32];
+        // the slot's next step (its inputs overwrite nothing the compute warp still reads; the result
+        // was read above)
+        if (k0 + (i + ahead) * na < T) prepare(i + ahead);
+
+        const int c = s - rr;
+        const bool valid = act && c >= 0 && c < a.nx;
         double x[N];
         if constexpr (MODE != 1) {
             TS xv[N];
@@ -333,18 +434,13 @@ __device__ __forceinline__ void modal_rows(const SweepArgs &a, const SweepItem &
 #pragma unroll
                 for (int e = 0; e < P; ++e) x[e + P * d] = flip_sign<XN>(d) * flip_sign<YN>(e) * Z[e + P * d];
         }
-        const size_t cell = (size_t)(TX ? a.nx - c : 1 + c) * istride + (size_t)j * plane + (size_t)q * N;
         if (a.out && valid) {
-            double *op = a.out + cell;
+            double *op = a.out + (size_t)(TX ? a.nx - c : 1 + c) * istride + (size_t)j * plane + (size_t)q * N;
 #pragma unroll
             for (int k = 0; k < N; ++k) op[k] = x[k];
         }
-        // moments: the warp's weighted values meet in shared memory (two buffers by step parity, so one
-        // __syncwarp per step orders the writes against the previous step's reads); the warp's Rw x N
-        // (row, dof) sums over each row segment's ordinates are spread over the lanes, each a fixed
-        // pairwise tree, and stored into this chunk's partial moments
         if (a.phi_part) {
-            double *red = L.red + ((size_t)(s & 1) * a.wn + w) * 32 * N;
+            __syncwarp();   // the previous step's reads of the stage are done
 #pragma unroll
             for (int k = 0; k < N; ++k) red[lane * N + k] = valid ? (ADJ ? x[k] : wq * x[k]) : 0.0;
             __syncwarp();
@@ -473,13 +569,14 @@ __device__ void modal_helper(const SweepArgs &a, const SweepItem &item, const La
 }
 
 template <int P, int MODE, int SEG, bool ADJ, bool BATCHED>
-__global__ void __launch_bounds__(kMaxWarps * 32, 1) sweep_modal_kernel(const SweepArgs a0,
-                                                                        const SweepArgs *__restrict__ table) {
+__global__ void __launch_bounds__(max_warps(P) * 32, 1) sweep_modal_kernel(const SweepArgs a0,
+                                                                           const SweepArgs *__restrict__ table) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_item;
     __shared__ int s_stop;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const Layout L = carve(smem_raw, a0.wn, a0.G, P, prefetch_depth(P), 32 / SEG);
+    const int na = aux_per_compute(P, a0.wn);
+    const Layout L = carve(smem_raw, a0.wn, na, a0.G, P, prefetch_depth(P), 32 / SEG, cellin_words<P, MODE>());
     const int rows_cta = a0.wn * (32 / SEG);
     __shared__ __align__(16) SweepArgs s_args;   // batched: the current item's problem descriptor
 
@@ -488,11 +585,16 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 1) sweep_modal_kernel(const Sw
             const int it = atomicAdd(a0.next_item, 1);
             s_item = it;
             s_stop = (it >= a0.n_items) || (ld_relaxed(a0.error) != kDevOk);
-            if (!s_stop)
+            if (!s_stop) {
                 for (int b = 0; b < (a0.wn + 1) * kS; ++b) {
                     mbar_init(L.full + b, 32);
                     mbar_init(L.empty + b, 32);
                 }
+                for (int b = 0; b < a0.wn * kZ; ++b) {
+                    mbar_init(L.in_full + b, 32);
+                    mbar_init(L.z_full + b, 32);
+                }
+            }
         }
         __syncthreads();
         const int it = s_item;
@@ -517,8 +619,16 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 1) sweep_modal_kernel(const Sw
                 case 2: modal_rows<P, MODE, SEG, true, false, ADJ>(a, item, L, warp, lane, has_consumer, local); break;
                 default: modal_rows<P, MODE, SEG, true, true, ADJ>(a, item, L, warp, lane, has_consumer, local); break;
             }
-        } else {
+        } else if (warp == a0.wn) {
             modal_helper<P>(a, item, L, lane);
+        } else {
+            const int ax = warp - a0.wn - 1, w = ax / na, k0 = ax - w * na;   // aux warp k0 of compute warp w
+            switch (item.quadrant) {
+                case 0: modal_aux<P, MODE, SEG, false, false, ADJ>(a, item, L, w, k0, na, lane, local); break;
+                case 1: modal_aux<P, MODE, SEG, false, true, ADJ>(a, item, L, w, k0, na, lane, local); break;
+                case 2: modal_aux<P, MODE, SEG, true, false, ADJ>(a, item, L, w, k0, na, lane, local); break;
+                default: modal_aux<P, MODE, SEG, true, true, ADJ>(a, item, L, w, k0, na, lane, local); break;
+            }
         }
         __syncthreads();
     }
@@ -529,7 +639,7 @@ cudaError_t launch_seg(const SweepArgs &args, int grid, size_t smem, cudaStream_
     auto kern = sweep_modal_kernel<P, MODE, SEG, ADJ, false>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    kern<<<grid, (args.wn + 1) * 32, smem, stream>>>(args, nullptr);
+    kern<<<grid, cta_warps(P, args.wn) * 32, smem, stream>>>(args, nullptr);
     return cudaGetLastError();
 }
 
@@ -539,7 +649,7 @@ cudaError_t launch_seg_batched(const SweepArgs &launch, const SweepArgs *table, 
     auto kern = sweep_modal_kernel<P, MODE, SEG, false, true>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    kern<<<grid, (launch.wn + 1) * 32, smem, stream>>>(launch, table);
+    kern<<<grid, cta_warps(P, launch.wn) * 32, smem, stream>>>(launch, table);
     return cudaGetLastError();
 }
 

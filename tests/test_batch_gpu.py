@@ -72,3 +72,34 @@ def test_autotuners_keep_results():
     finally:
         for c in ctxs:
             c.close()
+
+
+def test_batched_sweep_complete_on_return():
+    """Every degree group has finished when the batched sweep returns: the results are read at once on
+    another stream, with the largest problem in the last group to launch (the highest degree)."""
+    probs = [random_problem(24, 24, 1, 4, seed=11), lognormal(160, 2, 16, seed=12)]
+    ctxs = [_ctx(P) for P in probs]
+    try:
+        srcs = [torch.from_numpy(P.source).cuda() for P in probs]
+        outs = [torch.zeros_like(s) for s in srcs]
+        phis = [torch.zeros(P.phi_shape(), dtype=torch.float64, device="cuda") for P in probs]
+        want = []
+        for j, c in enumerate(ctxs):
+            w = torch.zeros_like(srcs[j])
+            c.sweep_out(srcs[j].data_ptr(), w.data_ptr(), np.inf, None, loc=abi.LOC_DEVICE)
+            want.append(w.cpu())
+        with abi.Batch() as b:
+            for c in ctxs:
+                b.add(c)
+            for _ in range(3):
+                for o in outs:
+                    o.zero_()
+                torch.cuda.synchronize()
+                b.sweep([s.data_ptr() for s in srcs], [o.data_ptr() for o in outs], [f.data_ptr() for f in phis],
+                        np.inf)
+                got = [o.cpu() for o in outs]   # torch's stream: ordered after the sweep only by its return
+                for j in range(len(probs)):
+                    assert torch.equal(got[j][1:-1, 1:-1], want[j][1:-1, 1:-1])
+    finally:
+        for c in ctxs:
+            c.close()
