@@ -200,7 +200,8 @@ int idc_sweep_fused(idc_ctx *ctx, const double *source, double *result, double d
 /* ---- tile shapes and batches ------------------------------------------------------------------------- */
 
 /* Tile shape of the sweep kernel: ordinates per row segment (seg: 4, 8, 16 or 32) and compute warps per
- * thread block (1..7); 0, 0 restores the default heuristic.  Results do not depend on it. */
+ * thread block (1..7; the modal kernel uses at most 5 at DG degree 2 and 7 below, and fewer if the shape's
+ * shared memory would not fit); 0, 0 restores the default heuristic.  Results do not depend on it. */
 int idc_set_tile_shape(idc_ctx *ctx, int32_t seg, int32_t warps);
 
 /* Autotuner: times every tile shape on this context's problem with `source` (device psi array) and keeps
