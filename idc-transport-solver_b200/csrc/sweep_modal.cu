@@ -191,9 +191,9 @@ template <int P>
 size_t smem_p(int precision, int wn, int G, int seg) {
     const int na = modal::aux_per_compute(P, wn), D = prefetch_depth(P), rw = 32 / seg;
     switch (precision) {
-        case 0: return modal::layout_bytes(wn, na, G, P, D, rw, modal::cellin_words<P, 0>());
-        case 1: return modal::layout_bytes(wn, na, G, P, D, rw, modal::cellin_words<P, 1>());
-        default: return modal::layout_bytes(wn, na, G, P, D, rw, modal::cellin_words<P, 2>());
+        case 0: return modal::layout_bytes(wn, na, G, P, D, rw, modal::slot_words<P, 0>());
+        case 1: return modal::layout_bytes(wn, na, G, P, D, rw, modal::slot_words<P, 1>());
+        default: return modal::layout_bytes(wn, na, G, P, D, rw, modal::slot_words<P, 2>());
     }
 }
 

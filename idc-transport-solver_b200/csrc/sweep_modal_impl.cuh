@@ -70,8 +70,8 @@ __device__ __forceinline__ int T_steps(int nx, int Rw) { return nx + Rw - 1; }
 // Source prefetch depth of an aux warp (cells ahead per lane, in its own steps).
 __host__ __device__ constexpr int prefetch_depth(int) { return 4; }
 
-// Inputs of one cell step, prepared by an aux warp.  MODE 0 / 2: packed modal source and reciprocal
-// denominators.  MODE 1: the sign-flipped physical source, FP32 reciprocals and s = sigma_t + 1/dt.
+// Inputs of one cell step.  MODE 0 / 2: packed modal source and reciprocal denominators.  MODE 1: the
+// sign-flipped physical source, FP32 reciprocals and s = sigma_t + 1/dt.
 template <int P, int MODE>
 struct CellIn {
     using TS = std::conditional_t<MODE == 0, double, float>;
@@ -79,10 +79,18 @@ struct CellIn {
     ModalRecip<P, TS> r;
     double s;
 };
+// What an aux warp hands the compute warp per step: the source part and s.  The compute warp forms the
+// reciprocals itself (it has slack; the aux warps pace the pipeline), which halves the slot traffic.
 template <int P, int MODE>
-__host__ __device__ constexpr int cellin_words() {
-    static_assert(sizeof(CellIn<P, MODE>) % 8 == 0, "CellIn is a whole number of 8-byte words");
-    return (int)(sizeof(CellIn<P, MODE>) / 8);
+struct CellSrc {
+    using TS = std::conditional_t<MODE == 0, double, float>;
+    std::conditional_t<MODE == 1, double, TS> v[P * P];
+    double s;
+};
+template <int P, int MODE>
+__host__ __device__ constexpr int slot_words() {
+    static_assert(sizeof(CellSrc<P, MODE>) % 8 == 0, "CellSrc is a whole number of 8-byte words");
+    return (int)(sizeof(CellSrc<P, MODE>) / 8);
 }
 
 struct Layout {
@@ -119,7 +127,7 @@ __device__ __forceinline__ Layout carve(unsigned char *raw, int wn, int na, int 
     return L;
 }
 
-template <int P, int MODE, bool XN, bool YN, bool ADJ>
+template <int P, int MODE, bool XN, bool YN, bool ADJ, bool RECIP = true>
 __device__ __forceinline__ void prep_cell(CellIn<P, MODE> &in, const double *sp, const double *cp, const SweepArgs &a,
                                           const ModalOrdinate<P, typename CellIn<P, MODE>::TS> &od, double wq) {
     constexpr int N = P * P;
@@ -138,7 +146,7 @@ __device__ __forceinline__ void prep_cell(CellIn<P, MODE> &in, const double *sp,
         }
     }
     in.s = cp[0] + a.inv_dt;
-    in.r = modal_recip<P, TS>(od, TS(in.s));
+    if constexpr (RECIP) in.r = modal_recip<P, TS>(od, TS(in.s));
     if constexpr (MODE != 1) {
         TS v[N];
 #pragma unroll
@@ -207,7 +215,7 @@ template <int P, int MODE, int SEG, bool XN, bool YN, bool ADJ>
 __device__ __forceinline__ void modal_rows(const SweepArgs &a, const SweepItem &item, const Layout &L, int w,
                                            int lane, bool has_consumer, int it_index) {
     constexpr int N = P * P;
-    constexpr int CW = cellin_words<P, MODE>();
+    constexpr int CW = slot_words<P, MODE>();
     using TS = std::conditional_t<MODE == 0, double, float>;   // modal solve type
     using TR = std::conditional_t<MODE == 2, float, double>;   // trace type
     using TZ = std::conditional_t<MODE == 1, double, TS>;      // step result (modal Z, or MODE 1 dofs)
@@ -253,7 +261,12 @@ __device__ __forceinline__ void modal_rows(const SweepArgs &a, const SweepItem &
             const unsigned long long *sp = slots + (size_t)zs * (CW + N) * 32;
 #pragma unroll
             for (int k = 0; k < CW; ++k) wv[k] = sp[k * 32];
-            memcpy(&cur, wv, sizeof(cur));
+            CellSrc<P, MODE> cs;
+            memcpy(&cs, wv, sizeof(cs));
+#pragma unroll
+            for (int k = 0; k < N; ++k) cur.v[k] = cs.v[k];
+            cur.s = cs.s;
+            cur.r = modal_recip<P, TS>(od, TS(cs.s));
         }
 
         // y trace: rows rr > 0 from the lane seg below in the warp (previous step), row 0 from the ring
@@ -330,7 +343,7 @@ template <int P, int MODE, int SEG, bool XN, bool YN, bool ADJ>
 __device__ __forceinline__ void modal_aux(const SweepArgs &a, const SweepItem &item, const Layout &L, int w,
                                           int k0, int na, int lane, int it_index) {
     constexpr int N = P * P;
-    constexpr int CW = cellin_words<P, MODE>();
+    constexpr int CW = slot_words<P, MODE>();
     using TS = std::conditional_t<MODE == 0, double, float>;
     using TZ = std::conditional_t<MODE == 1, double, TS>;
     constexpr int seg = SEG, Rw = 32 / SEG;
@@ -392,10 +405,14 @@ __device__ __forceinline__ void modal_aux(const SweepArgs &a, const SweepItem &i
         __syncwarp();       // lane o == 0's cell-data copies are visible to its row segment
         const int s = k0 + i * na;
         CellIn<P, MODE> cur;
-        prep_cell<P, MODE, XN, YN, ADJ>(cur, my_src + (size_t)(i % D) * 32 * N, my_cell + (size_t)(i % D) * Rw * NC,
-                                        a, od, wq);
+        prep_cell<P, MODE, XN, YN, ADJ, false>(cur, my_src + (size_t)(i % D) * 32 * N,
+                                               my_cell + (size_t)(i % D) * Rw * NC, a, od, wq);
+        CellSrc<P, MODE> cs;
+#pragma unroll
+        for (int k = 0; k < N; ++k) cs.v[k] = cur.v[k];
+        cs.s = cur.s;
         unsigned long long wv[CW];
-        memcpy(wv, &cur, sizeof(cur));
+        memcpy(wv, &cs, sizeof(cs));
         unsigned long long *sp = reinterpret_cast<unsigned long long *>(L.slot) +
                                  ((size_t)(w * kZ + s % kZ) * (CW + N)) * 32 + lane;
 #pragma unroll
@@ -576,7 +593,7 @@ __global__ void __launch_bounds__(max_warps(P) * 32, 1) sweep_modal_kernel(const
     __shared__ int s_stop;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int na = aux_per_compute(P, a0.wn);
-    const Layout L = carve(smem_raw, a0.wn, na, a0.G, P, prefetch_depth(P), 32 / SEG, cellin_words<P, MODE>());
+    const Layout L = carve(smem_raw, a0.wn, na, a0.G, P, prefetch_depth(P), 32 / SEG, slot_words<P, MODE>());
     const int rows_cta = a0.wn * (32 / SEG);
     __shared__ __align__(16) SweepArgs s_args;   // batched: the current item's problem descriptor
 
