@@ -57,6 +57,7 @@ Context::~Context() {
     cudaFree(d_krylov);
     cudaFree(d_small);
     cudaFree(d_dsa_ws);
+    if (dsa_exec) cudaGraphExecDestroy(dsa_exec);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);

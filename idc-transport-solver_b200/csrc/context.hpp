@@ -132,6 +132,12 @@ public:
     int dsa_steps = 30;            // Jacobi-PCG steps per DSA application
     double *d_dsa_ws = nullptr;    // DSA workspace
     size_t dsa_ws_len = 0;
+    // the DSA Jacobi-PCG steps as one CUDA graph (workspace pointers only; rebuilt when the workspace or
+    // the step count changes)
+    cudaGraphExec_t dsa_exec = nullptr;
+    const double *dsa_exec_ws = nullptr;
+    int dsa_exec_steps = -1;
+    Status dsa_cg_graphed();
     size_t krylov_len = 0;
     double *d_small = nullptr;     // GMRES Hessenberg column / coefficients (device)
 

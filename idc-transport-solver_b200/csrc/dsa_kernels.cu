@@ -189,30 +189,57 @@ cudaError_t dsa_setup(const GridDims &g, const double *sigma_t, const double *si
 
 // out = v + e_00 with C e = sigma_s v_00 approximated by cg_steps Jacobi-PCG steps from e = 0 (out may
 // alias v).  5 kernels per step; returns the number of launches in *launches.
+namespace {
+struct DsaWs {
+    double *Dc, *sa, *dinv, *x, *r, *z, *p, *q, *part, *sc;
+    DsaWs(double *ws, int n) {
+        Dc = ws, sa = ws + n, dinv = ws + 2 * (size_t)n, x = ws + 3 * (size_t)n, r = ws + 4 * (size_t)n;
+        z = ws + 5 * (size_t)n, p = ws + 6 * (size_t)n, q = ws + 7 * (size_t)n;
+        part = ws + 8 * (size_t)n, sc = part + 148 * 4;
+    }
+};
+}  // namespace
+
+cudaError_t dsa_rhs(const GridDims &g, const double *sigma_s, const double *v, double *ws, cudaStream_t s) {
+    const int n = g.nx * g.ny;
+    const DsaWs w(ws, n);
+    dsa_rhs_kernel<<<blocks_for(n), kThreads, 0, s>>>(g.nx, g.ny, g.P * g.P, sigma_s, v, w.dinv, w.x, w.r, w.z, w.p,
+                                                      w.part);
+    return cudaGetLastError();
+}
+
+cudaError_t dsa_cg(const GridDims &g, int cg_steps, double *ws, cudaStream_t s) {
+    const int n = g.nx * g.ny;
+    const DsaWs w(ws, n);
+    const int nb = blocks_for(n);
+    cg_scalar_kernel<<<1, kThreads, 0, s>>>(nb, w.part, w.sc, 0);
+    for (int it = 0; it < cg_steps; ++it) {
+        dsa_apply_kernel<<<nb, kThreads, 0, s>>>(g.nx, g.ny, g.dx, g.dy, w.Dc, w.sa, w.p, w.q, w.part);
+        cg_scalar_kernel<<<1, kThreads, 0, s>>>(nb, w.part, w.sc, 1);
+        cg_update_kernel<<<nb, kThreads, 0, s>>>(n, w.sc, w.p, w.q, w.dinv, w.x, w.r, w.z, w.part);
+        cg_scalar_kernel<<<1, kThreads, 0, s>>>(nb, w.part, w.sc, 2);
+        cg_dir_kernel<<<nb, kThreads, 0, s>>>(n, w.sc, w.z, w.p);
+    }
+    return cudaGetLastError();
+}
+
+int dsa_cg_launches(int cg_steps) { return 1 + 5 * cg_steps; }
+
+cudaError_t dsa_correct(const GridDims &g, const double *v, double *ws, double *out, cudaStream_t s) {
+    const int n = g.nx * g.ny;
+    const DsaWs w(ws, n);
+    const size_t tot = (size_t)(g.nx + 2) * (g.ny + 2) * g.P * g.P;
+    dsa_correct_kernel<<<blocks_for(tot), kThreads, 0, s>>>(g.nx, g.ny, g.P * g.P, v, w.x, out);
+    return cudaGetLastError();
+}
+
 cudaError_t dsa_apply(const GridDims &g, const double *sigma_s, const double *v, double *out, int cg_steps, double *ws,
                       cudaStream_t s, int *launches) {
-    const int n = g.nx * g.ny;
-    const int N = g.P * g.P;
-    double *Dc = ws, *sa = ws + n, *dinv = ws + 2 * (size_t)n, *x = ws + 3 * (size_t)n, *r = ws + 4 * (size_t)n,
-           *z = ws + 5 * (size_t)n, *p = ws + 6 * (size_t)n, *q = ws + 7 * (size_t)n;
-    double *part = ws + 8 * (size_t)n, *sc = part + 148 * 4;
-    const int nb = blocks_for(n);
-    dsa_rhs_kernel<<<nb, kThreads, 0, s>>>(g.nx, g.ny, N, sigma_s, v, dinv, x, r, z, p, part);
-    cg_scalar_kernel<<<1, kThreads, 0, s>>>(nb, part, sc, 0);
-    int L = 2;
-    for (int it = 0; it < cg_steps; ++it) {
-        dsa_apply_kernel<<<nb, kThreads, 0, s>>>(g.nx, g.ny, g.dx, g.dy, Dc, sa, p, q, part);
-        cg_scalar_kernel<<<1, kThreads, 0, s>>>(nb, part, sc, 1);
-        cg_update_kernel<<<nb, kThreads, 0, s>>>(n, sc, p, q, dinv, x, r, z, part);
-        cg_scalar_kernel<<<1, kThreads, 0, s>>>(nb, part, sc, 2);
-        cg_dir_kernel<<<nb, kThreads, 0, s>>>(n, sc, z, p);
-        L += 5;
-    }
-    const size_t tot = (size_t)(g.nx + 2) * (g.ny + 2) * N;
-    dsa_correct_kernel<<<blocks_for(tot), kThreads, 0, s>>>(g.nx, g.ny, N, v, x, out);
-    L += 1;
-    if (launches) *launches = L;
-    return cudaGetLastError();
+    cudaError_t e = dsa_rhs(g, sigma_s, v, ws, s);
+    if (e == cudaSuccess) e = dsa_cg(g, cg_steps, ws, s);
+    if (e == cudaSuccess) e = dsa_correct(g, v, ws, out, s);
+    if (launches) *launches = 2 + dsa_cg_launches(cg_steps);
+    return e;
 }
 
 }  // namespace idc

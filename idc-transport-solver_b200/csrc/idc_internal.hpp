@@ -158,6 +158,12 @@ size_t dsa_workspace_doubles(int nx, int ny);
 cudaError_t dsa_setup(const GridDims &g, const double *sigma_t, const double *sigma_s, double *ws, cudaStream_t s);
 cudaError_t dsa_apply(const GridDims &g, const double *sigma_s, const double *v, double *out, int cg_steps, double *ws,
                       cudaStream_t s, int *launches);
+// dsa_apply in three parts: the right-hand side from v, the Jacobi-PCG steps (workspace only, so one
+// CUDA graph of them serves every call on the same workspace), the correction out = v + x
+cudaError_t dsa_rhs(const GridDims &g, const double *sigma_s, const double *v, double *ws, cudaStream_t s);
+cudaError_t dsa_cg(const GridDims &g, int cg_steps, double *ws, cudaStream_t s);
+int dsa_cg_launches(int cg_steps);
+cudaError_t dsa_correct(const GridDims &g, const double *v, double *ws, double *out, cudaStream_t s);
 // sum over interior cells of (a - b)^2 into *out (device double, pre-zeroed by the launcher)
 cudaError_t launch_l2dist2(const GridDims &g, const double *a, const double *b, double *out, cudaStream_t s);
 

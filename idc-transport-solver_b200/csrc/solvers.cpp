@@ -107,8 +107,10 @@ Status Context::gmres(Op apply, const double *b, double *x, double abs_tol, int 
         for (int j = 0; j < m && its < max_its; ++j) {
             if (dsa) {
                 int nl = 0;
-                IDC_TRY_CUDA(dsa_apply(dims(), d_sigma_s, Vc(j), Zc(j), dsa_steps, d_dsa_ws, stream, &nl));
-                launches += nl;
+                IDC_TRY_CUDA(dsa_rhs(dims(), d_sigma_s, Vc(j), d_dsa_ws, stream));
+                IDC_TRY(dsa_cg_graphed());
+                IDC_TRY_CUDA(dsa_correct(dims(), Vc(j), d_dsa_ws, Zc(j), stream));
+                launches += 2 + dsa_cg_launches(dsa_steps);
                 IDC_TRY(apply(Zc(j), Vc(j + 1)));
             } else {
                 IDC_TRY(apply(Vc(j), Vc(j + 1)));
@@ -200,6 +202,28 @@ Status Context::gmres_peierls(const double *src, double *psi_out, double dt, dou
     if (!converged)
         return bad(IDC_ERR_NOT_CONVERGED, "GMRES transport solve failed to converge (max_its reached, residual " +
                                               std::to_string(resid) + ")");
+    return Status::ok();
+}
+
+// The DSA steps (dsa_cg) captured once into a CUDA graph and replayed: one launch instead of 1 + 5 per
+// step (150 at 30 steps), whose launch gaps exceed the kernels' run times at these sizes.
+Status Context::dsa_cg_graphed() {
+    if (!dsa_exec || dsa_exec_ws != d_dsa_ws || dsa_exec_steps != dsa_steps) {
+        if (dsa_exec) cudaGraphExecDestroy(dsa_exec);
+        dsa_exec = nullptr;
+        IDC_TRY_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        const cudaError_t e = dsa_cg(dims(), dsa_steps, d_dsa_ws, stream);
+        cudaGraph_t graph = nullptr;
+        const cudaError_t e2 = cudaStreamEndCapture(stream, &graph);
+        IDC_TRY_CUDA(e);
+        IDC_TRY_CUDA(e2);
+        const cudaError_t e3 = cudaGraphInstantiate(&dsa_exec, graph, 0);
+        cudaGraphDestroy(graph);
+        IDC_TRY_CUDA(e3);
+        dsa_exec_ws = d_dsa_ws;
+        dsa_exec_steps = dsa_steps;
+    }
+    IDC_TRY_CUDA(cudaGraphLaunch(dsa_exec, stream));
     return Status::ok();
 }
 
