@@ -103,7 +103,7 @@ size_t sweep_modal_smem_bytes(int P, int precision, int wn, int G, int seg);
 // at most sweep_modal_max_wn(P) compute warps (the register file holds one CTA).  fit_wn: the largest
 // wn <= the given one whose shared memory fits the device.
 int sweep_modal_max_wn(int P);
-int sweep_modal_default_wn(int P);   // the most compute warps with two aux warps each
+int sweep_modal_default_wn(int P);
 int sweep_modal_threads(int P, int wn);
 int sweep_modal_fit_wn(int P, int precision, int wn, int G, int seg);
 // Inflow traces of the ghost cells of `src` for the modal kernel: out[(k * nq + q) * P + m], k < nx the

@@ -207,7 +207,8 @@ size_t sweep_modal_smem_bytes(int P, int precision, int wn, int G, int seg) {
 
 int sweep_modal_threads(int P, int wn) { return modal::cta_warps(P, wn) * 32; }
 
-int sweep_modal_default_wn(int P) { return (modal::max_warps(P) - 1) / 3; }
+// 4 compute warps with 2 aux warps each (13 warps): measured fastest on B200 at Q1 and Q2, S4..S16
+int sweep_modal_default_wn(int) { return 4; }
 
 int sweep_modal_fit_wn(int P, int precision, int wn, int G, int seg) {
     int dev = 0, limit = 0;

@@ -57,18 +57,20 @@ namespace modal {
 constexpr int kS = kWarpRingSlots;
 constexpr int kZ = kModalSolutionSlots;
 
-// Warps per CTA: Wn compute warps, the helper warp and nA aux warps per compute warp, bounded so that
-// the register file holds one CTA (the degree sets the registers a thread needs; warps are allocated in
-// groups of four, so 11 warps get the registers of 12).  Two aux warps per compute warp when they fit.
-__host__ __device__ constexpr int max_warps(int P) { return P == 3 ? 11 : 15; }
+// Warps per CTA: Wn compute warps, the helper warp and nA aux warps per compute warp (the most of 4, 2, 1
+// that fit; kZ is a multiple of each), at most 16 warps: one CTA per SM, 128 registers a thread.
+__host__ __device__ constexpr int max_warps(int) { return 16; }
 __host__ __device__ constexpr int max_compute_warps(int P) { return (max_warps(P) - 1) / 2; }
-__host__ __device__ constexpr int aux_per_compute(int P, int wn) { return 3 * wn + 1 <= max_warps(P) ? 2 : 1; }
+__host__ __device__ constexpr int aux_per_compute(int P, int wn) {
+    return 5 * wn + 1 <= max_warps(P) ? 4 : (3 * wn + 1 <= max_warps(P) ? 2 : 1);
+}
 __host__ __device__ constexpr int cta_warps(int P, int wn) { return wn * (1 + aux_per_compute(P, wn)) + 1; }
 
 __device__ __forceinline__ int T_steps(int nx, int Rw) { return nx + Rw - 1; }
 
-// Source prefetch depth of an aux warp (cells ahead per lane, in its own steps).
-__host__ __device__ constexpr int prefetch_depth(int) { return 4; }
+// Source prefetch depth of an aux warp (cells ahead per lane, in its own steps, which are nA steps apart;
+// the loads are issued two of its steps ahead, well beyond the HBM latency at every nA).
+__host__ __device__ constexpr int prefetch_depth(int) { return 3; }
 
 // Inputs of one cell step.  MODE 0 / 2: packed modal source and reciprocal denominators.  MODE 1: the
 // sign-flipped physical source, FP32 reciprocals and s = sigma_t + 1/dt.
