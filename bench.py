@@ -9,8 +9,9 @@ The headline `value` is the fastest sweep that meets the 1e-8 relative accuracy 
 sweep (FP32 cell solves with FP64 refinement, timed beside it as `fp32_refined`, is slower on B200:
 the refinement lengthens the cell-to-cell chain of a latency-bound wavefront).  Each precision runs
 with the tile shape the library's autotuner picks for this problem (idc_autotune), chosen before the
-timed region.  `e2e` times the same step through the C ABI with pinned HOST buffers (host -> device
-copy of the source and device -> host copy of psi and phi inside the timed region).
+timed region.  `e2e` times K such steps through the C ABI on pinned HOST buffers
+(idc_sweep_out_many: every step uploads its source and downloads psi and phi inside the timed region;
+the copies of neighbouring steps overlap the sweeps on separate streams).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -404,12 +405,11 @@ def run_ours(args):
     hs, ho, hp = h_src.numpy(), h_out.numpy(), h_phi.numpy()
     e2e_s, e2e_phi_err = float("nan"), None
     if not args.no_e2e:
-        e2e_steps = max(1, min(args.steps, 10))
-        ctx.sweep_out(hs, ho, P.dt, hp, abi.PREC_FP64, loc=abi.LOC_HOST)
+        e2e_steps = max(2, min(args.steps, 10))
+        ctx.sweep_out_many([hs] * 2, [ho] * 2, [hp] * 2, P.dt, abi.PREC_FP64)   # buffers and streams
         barrier()
         t0 = time.perf_counter()
-        for _ in range(e2e_steps):
-            ctx.sweep_out(hs, ho, P.dt, hp, abi.PREC_FP64, loc=abi.LOC_HOST)
+        ctx.sweep_out_many([hs] * e2e_steps, [ho] * e2e_steps, [hp] * e2e_steps, P.dt, abi.PREC_FP64)
         e2e_s = (time.perf_counter() - t0) / e2e_steps
         if dist is not None:
             t = torch.tensor([e2e_s], device=f"cuda:{dev}")

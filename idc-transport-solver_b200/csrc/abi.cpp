@@ -182,18 +182,35 @@ int idc_sweep_out(idc_ctx *ctx, const double *source, double *result, double dt,
         ABI_TRY_CUDA(cudaMemcpyAsync(d_src, source, sizeof(double) * c.psi_len(), cudaMemcpyHostToDevice, c.stream));
         ABI_TRY(c.sweep(d_src, d_res, dt, d_phi, precision));
         // interior cells only; the caller's ghost cells of result stay as they were
-        const size_t cell = (size_t)c.nq * c.N;
-        for (int64_t i = 1; i <= c.nx; ++i) {
-            const size_t off = ((size_t)i * (c.ny + 2) + 1) * cell;
-            ABI_TRY_CUDA(cudaMemcpyAsync(result + off, d_res + off, sizeof(double) * cell * c.ny,
-                                         cudaMemcpyDeviceToHost, c.stream));
-        }
+        ABI_TRY_CUDA(c.copy_interior_d2h(result, d_res, c.stream));
         if (phi_out)
             ABI_TRY_CUDA(cudaMemcpyAsync(phi_out, d_phi, sizeof(double) * c.phi_len(), cudaMemcpyDeviceToHost, c.stream));
         ABI_TRY(c.check_device_error());
     }
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, c.ev0, c.ev1) == cudaSuccess) c.last_sweep_ms = ms;
+    return IDC_OK;
+    ABI_GUARD_END
+}
+
+int idc_sweep_out_many(idc_ctx *ctx, int64_t count, const double *const *sources, double *const *results,
+                       double *const *phi_out, double dt, int precision, int loc) {
+    ABI_GUARD_BEGIN
+    if (!ctx || count < 0 || (count > 0 && (!sources || !results))) return fail(IDC_ERR_ARG, "idc_sweep_out_many: null argument");
+    if (!valid_loc(loc)) return fail(IDC_ERR_ARG, "bad loc");
+    for (int64_t k = 0; k < count; ++k)
+        if (!sources[k] || !results[k]) return fail(IDC_ERR_ARG, "idc_sweep_out_many: null source or result");
+    idc::Context &c = ctx->impl;
+    if (!c.have_ordinates) return fail(IDC_ERR_STATE, "idc_sweep_out_many before idc_set_ordinates");
+    if (!c.have_sigma) return fail(IDC_ERR_STATE, "idc_sweep_out_many before idc_set_sigma");
+    ABI_TRY_CUDA(cudaSetDevice(c.device));
+    c.launches = 0;
+    if (loc == IDC_LOC_DEVICE) {
+        for (int64_t k = 0; k < count; ++k) ABI_TRY(c.sweep(sources[k], results[k], dt, phi_out ? phi_out[k] : nullptr, precision));
+        ABI_TRY(c.check_device_error());
+    } else {
+        ABI_TRY(c.sweep_host_many(count, sources, results, phi_out, dt, precision));
+    }
     return IDC_OK;
     ABI_GUARD_END
 }
@@ -481,12 +498,7 @@ int idc_sweep_adjoint(idc_ctx *ctx, const double *source, double *result, double
         double *d_mom = moments_out ? c.phi_buf(2) : nullptr;
         ABI_TRY_CUDA(cudaMemcpyAsync(d_src, source, sizeof(double) * c.psi_len(), cudaMemcpyHostToDevice, c.stream));
         ABI_TRY(c.sweep(d_src, d_res, dt, d_mom, precision, nullptr, 1.0, true));
-        const size_t cell = (size_t)c.nq * c.N;
-        for (int64_t i = 1; i <= c.nx; ++i) {
-            const size_t off = ((size_t)i * (c.ny + 2) + 1) * cell;
-            ABI_TRY_CUDA(cudaMemcpyAsync(result + off, d_res + off, sizeof(double) * cell * c.ny,
-                                         cudaMemcpyDeviceToHost, c.stream));
-        }
+        ABI_TRY_CUDA(c.copy_interior_d2h(result, d_res, c.stream));
         if (moments_out)
             ABI_TRY_CUDA(cudaMemcpyAsync(moments_out, d_mom, sizeof(double) * c.phi_len(), cudaMemcpyDeviceToHost,
                                          c.stream));

@@ -58,6 +58,13 @@ Context::~Context() {
     cudaFree(d_small);
     cudaFree(d_dsa_ws);
     if (dsa_exec) cudaGraphExecDestroy(dsa_exec);
+    for (int b = 0; b < 2; ++b) {
+        if (ev_in[b]) cudaEventDestroy(ev_in[b]);
+        if (ev_done[b]) cudaEventDestroy(ev_done[b]);
+        if (ev_out[b]) cudaEventDestroy(ev_out[b]);
+    }
+    if (copy_in) cudaStreamDestroy(copy_in);
+    if (copy_out) cudaStreamDestroy(copy_out);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);
@@ -356,6 +363,55 @@ Status Context::build_schedule(int precision) {
     grid = std::min(n_items, per_sm * num_sms);
     occupancy_precision = precision;
     return Status::ok();
+}
+
+// The interior cells of a psi array, device -> host, as one strided copy: nx runs of ny cells (the
+// interior j range of one column i), (ny + 2) cells apart in both arrays.
+cudaError_t Context::copy_interior_d2h(double *host, const double *dev, cudaStream_t s) const {
+    const size_t cell = (size_t)nq * N * sizeof(double);
+    const size_t off = ((size_t)1 * (ny + 2) + 1) * (size_t)nq * N;
+    return cudaMemcpy2DAsync(host + off, (ny + 2) * cell, dev + off, (ny + 2) * cell, ny * cell, (size_t)nx,
+                             cudaMemcpyDeviceToHost, s);
+}
+
+Status Context::sweep_host_many(int64_t count, const double *const *srcs, double *const *outs,
+                                double *const *phis, double dt, int precision) {
+    if (count < 1) return Status::ok();
+    IDC_TRY_CUDA(cudaSetDevice(device));
+    IDC_TRY(ensure_psi_buffers(4));   // sources in 0, 1; results in 2, 3
+    IDC_TRY(ensure_phi_buffers(5));   // moments in 3, 4
+    if (!copy_in) {
+        IDC_TRY_CUDA(cudaStreamCreateWithFlags(&copy_in, cudaStreamNonBlocking));
+        IDC_TRY_CUDA(cudaStreamCreateWithFlags(&copy_out, cudaStreamNonBlocking));
+        for (int b = 0; b < 2; ++b) {
+            IDC_TRY_CUDA(cudaEventCreateWithFlags(&ev_in[b], cudaEventDisableTiming));
+            IDC_TRY_CUDA(cudaEventCreateWithFlags(&ev_done[b], cudaEventDisableTiming));
+            IDC_TRY_CUDA(cudaEventCreateWithFlags(&ev_out[b], cudaEventDisableTiming));
+        }
+    }
+    const size_t cell = (size_t)nq * N;
+    for (int64_t k = 0; k < count; ++k) {
+        const int b = (int)(k & 1);
+        double *d_src = psi_buf(b), *d_res = psi_buf(2 + b), *d_phi = phis ? phi_buf(3 + b) : nullptr;
+        // upload, once the sweep two steps back has read this source buffer
+        if (k >= 2) IDC_TRY_CUDA(cudaStreamWaitEvent(copy_in, ev_done[b], 0));
+        IDC_TRY_CUDA(cudaMemcpyAsync(d_src, srcs[k], sizeof(double) * psi_len(), cudaMemcpyHostToDevice, copy_in));
+        IDC_TRY_CUDA(cudaEventRecord(ev_in[b], copy_in));
+        // sweep, once the source is in and the download two steps back has read this result buffer
+        IDC_TRY_CUDA(cudaStreamWaitEvent(stream, ev_in[b], 0));
+        if (k >= 2) IDC_TRY_CUDA(cudaStreamWaitEvent(stream, ev_out[b], 0));
+        IDC_TRY(sweep(d_src, d_res, dt, d_phi, precision));
+        IDC_TRY_CUDA(cudaEventRecord(ev_done[b], stream));
+        // download the interior cells (the caller's ghost cells stay as they were) and the moments
+        IDC_TRY_CUDA(cudaStreamWaitEvent(copy_out, ev_done[b], 0));
+        IDC_TRY_CUDA(copy_interior_d2h(outs[k], d_res, copy_out));
+        if (phis && phis[k])
+            IDC_TRY_CUDA(cudaMemcpyAsync(phis[k], d_phi, sizeof(double) * phi_len(), cudaMemcpyDeviceToHost, copy_out));
+        IDC_TRY_CUDA(cudaEventRecord(ev_out[b], copy_out));
+    }
+    IDC_TRY_CUDA(cudaStreamSynchronize(copy_out));
+    IDC_TRY_CUDA(cudaStreamSynchronize(copy_in));
+    return check_device_error();
 }
 
 Status Context::check_device_error() {

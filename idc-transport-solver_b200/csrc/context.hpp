@@ -41,6 +41,12 @@ public:
     // Sweep: out <- L^{-1} (src [+ scale * S phi_scatter]); phi (nullable) <- P out.  src may equal out.
     Status sweep(const double *src, double *out, double dt, double *phi, int precision,
                  const double *phi_scatter = nullptr, double scatter_scale = 1.0, bool adjoint = false);
+    // count out-of-place sweeps of HOST arrays (srcs[k] -> outs[k] interior cells, phis[k] if phis), the
+    // upload of step k+1, the sweep of step k and the download of step k-1 overlapped on three streams
+    // with double-buffered device arrays
+    Status sweep_host_many(int64_t count, const double *const *srcs, double *const *outs, double *const *phis,
+                           double dt, int precision);
+    cudaError_t copy_interior_d2h(double *host, const double *dev, cudaStream_t s) const;
     Status pmv(double alpha, double beta, const double *psi, double *phi);
     Status smv(double alpha, double beta, const double *phi, double *psi);
     Status lmv(double alpha, double beta, const double *x, double *y);
@@ -135,6 +141,8 @@ public:
     // the DSA Jacobi-PCG steps as one CUDA graph (workspace pointers only; rebuilt when the workspace or
     // the step count changes)
     cudaGraphExec_t dsa_exec = nullptr;
+    cudaStream_t copy_in = nullptr, copy_out = nullptr;   // sweep_host_many's copy streams
+    cudaEvent_t ev_in[2] = {}, ev_done[2] = {}, ev_out[2] = {};
     const double *dsa_exec_ws = nullptr;
     int dsa_exec_steps = -1;
     Status dsa_cg_graphed();

@@ -43,7 +43,7 @@ EXPORTED_SYMBOLS = (
     "idc_adjoint_grad", "idc_set_preconditioner", "idc_idc_integrate", "idc_write_sd2", "idc_read_sd2",
     "idc_write_af2", "idc_read_af2", "idc_sweep_fused", "idc_set_tile_shape", "idc_autotune", "idc_batch_create",
     "idc_batch_add", "idc_batch_sweep", "idc_batch_autotune", "idc_batch_last_timing", "idc_batch_destroy",
-    "idc_batch_set_shape", "idc_batch_get_shape",
+    "idc_batch_set_shape", "idc_batch_get_shape", "idc_sweep_out_many",
 )
 
 
@@ -89,6 +89,8 @@ def load_library(path: str = LIB_PATH):
     lib.idc_last_timing.argtypes = [vp, _dp, C.POINTER(C.c_int64)]
     lib.idc_set_tiling.argtypes = [vp, C.c_int32, C.c_int32]
     lib.idc_sweep_out.argtypes = [vp, vp, vp, C.c_double, vp, C.c_int, C.c_int]
+    lib.idc_sweep_out_many.argtypes = [vp, C.c_int64, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.c_double,
+                                       C.c_int, C.c_int]
     lib.idc_sweep_adjoint.argtypes = [vp, vp, vp, C.c_double, vp, C.c_int, C.c_int]
     lib.idc_set_preconditioner.argtypes = [vp, C.c_int, C.c_int32]
     lib.idc_sweep_fused.argtypes = [vp, vp, vp, C.c_double, vp, C.c_double, vp, C.c_int, C.c_int]
@@ -203,6 +205,15 @@ class SweepContext:
         """result <- L^{-1} source (interior cells); phi (if given) <- P result."""
         _check(self._lib.idc_sweep_out(self._h, _ptr(source, loc), _ptr(result, loc), float(dt), _ptr(phi, loc),
                                        int(precision), loc), "idc_sweep_out")
+
+    def sweep_out_many(self, sources, results, phis=None, dt=np.inf, precision=PREC_FP64, loc=LOC_HOST):
+        """results[k] <- L^{-1} sources[k] (interior cells), phis[k] <- P results[k]; on host arrays the
+        copies of neighbouring steps overlap the sweeps."""
+        n = len(sources)
+        arr = lambda xs: (C.c_void_p * n)(*[_ptr(x, loc) for x in xs])
+        _check(self._lib.idc_sweep_out_many(self._h, n, arr(sources), arr(results),
+                                            None if phis is None else arr(phis), float(dt), int(precision), loc),
+               "idc_sweep_out_many")
 
     def pmv(self, alpha, beta, psi, phi, loc=LOC_HOST):
         _check(self._lib.idc_pmv(self._h, alpha, beta, _ptr(psi, loc), _ptr(phi, loc), loc), "idc_pmv")

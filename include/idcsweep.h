@@ -104,6 +104,14 @@ int idc_sweep(idc_ctx *ctx, double *psi_inout, double dt, double *phi_out, int p
 int idc_sweep_out(idc_ctx *ctx, const double *source, double *result, double dt, double *phi_out, int precision,
                   int loc);
 
+/* `count` out-of-place sweeps (sources[k] -> results[k], phi_out[k] if phi_out is not NULL), each as
+ * idc_sweep_out.  With loc = IDC_LOC_HOST the upload of step k+1, the sweep of step k and the download of
+ * step k-1 overlap (three streams, double-buffered device arrays), so a sequence of host-resident steps
+ * costs about the slower copy direction per step instead of both; host arrays should be pinned.  A
+ * batch-of-right-hand-sides form of SweepPattern::Sweep with no counterpart in the reference. */
+int idc_sweep_out_many(idc_ctx *ctx, int64_t count, const double *const *sources, double *const *results,
+                       double *const *phi_out, double dt, int precision, int loc);
+
 /* ---- transport operators (operators/RKDG/TransportOperator.hpp:25-43), interior cells ------------ */
 
 /* phi <- beta*phi + alpha * sum_q w_q psi_q.              TransportOperator::Pmv, TransportOperator.cpp:140-158 */
