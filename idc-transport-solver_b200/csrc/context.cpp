@@ -171,7 +171,7 @@ Status Context::set_tile_shape(int s, int w) {
     return Status::ok();
 }
 
-// Candidate tile shapes, timed with CUDA events on this problem (second of two sweeps each).
+// Candidate tile shapes, timed with CUDA events on this problem (best of three sweeps after a warm-up).
 Status Context::autotune(const double *src, double dt, int precision, int *seg_out, int *wn_out) {
     if (kernel != kModal) return bad(IDC_ERR_UNSUPPORTED, "the autotuner tunes the modal kernel");
     IDC_TRY(ensure_psi_buffers(1));
@@ -182,11 +182,13 @@ Status Context::autotune(const double *src, double dt, int precision, int *seg_o
     for (int cs : {4, 8, 16, 32})
         for (int cw = std::max(1, mw - 3); cw <= mw; ++cw) {
             IDC_TRY(set_tile_shape(cs, cw));
-            float ms = 0.f;
-            for (int rep = 0; rep < 2; ++rep) {
+            float ms = 1e30f;
+            for (int rep = 0; rep < 4; ++rep) {   // one warm-up, then the best of three
                 IDC_TRY(sweep(src, psi_buf(0), dt, phi_buf(0), precision));
                 IDC_TRY(check_device_error());
-                IDC_TRY_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+                float t = 0.f;
+                IDC_TRY_CUDA(cudaEventElapsedTime(&t, ev0, ev1));
+                if (rep > 0) ms = std::min(ms, t);
             }
             if (ms < best) {
                 best = ms;

@@ -400,15 +400,17 @@ __device__ __forceinline__ void modal_aux(const SweepArgs &a, const SweepItem &i
         }
         cp_commit();
     };
-    // prepare target i into its slot and release the slot to the compute warp
-    auto prepare = [&](int i) {
+    // target i's inputs: wait for its stage (one cp.async group per target, in order), form them
+    auto stage_in = [&](int i, CellIn<P, MODE> &cur) {
         prefetch(i + D - 1);
         cp_wait<D - 2>();   // target i has landed
         __syncwarp();       // lane o == 0's cell-data copies are visible to its row segment
-        const int s = k0 + i * na;
-        CellIn<P, MODE> cur;
         prep_cell<P, MODE, XN, YN, ADJ, false>(cur, my_src + (size_t)(i % D) * 32 * N,
                                                my_cell + (size_t)(i % D) * Rw * NC, a, od, wq);
+    };
+    // ...into its slot, released to the compute warp
+    auto publish = [&](int i, const CellIn<P, MODE> &cur) {
+        const int s = k0 + i * na;
         CellSrc<P, MODE> cs;
 #pragma unroll
         for (int k = 0; k < N; ++k) cs.v[k] = cur.v[k];
@@ -425,7 +427,11 @@ __device__ __forceinline__ void modal_aux(const SweepArgs &a, const SweepItem &i
 #pragma unroll
     for (int i = 0; i < D - 1; ++i) prefetch(i);
     const int ahead = kZ / na;   // targets in flight: the slots this warp owns
-    for (int i = 0; i < ahead && k0 + i * na < T; ++i) prepare(i);
+    for (int i = 0; i < ahead; ++i) {
+        CellIn<P, MODE> cur;
+        stage_in(i, cur);
+        if (k0 + i * na < T) publish(i, cur);
+    }
 
     for (int i = 0; k0 + i * na < T; ++i) {
         const int s = k0 + i * na;
@@ -435,10 +441,10 @@ __device__ __forceinline__ void modal_aux(const SweepArgs &a, const SweepItem &i
         const TZ *zp = reinterpret_cast<const TZ *>(L.slot + ((size_t)(w * kZ + zs) * (CW + N) + CW) * 32) + lane;
 #pragma unroll
         for (int k = 0; k < N; ++k) Z[k] = zp[k * 32];
-        // the slot's next step (its inputs overwrite nothing the compute warp still reads; the result
-        // was read above)
-        if (k0 + (i + ahead) * na < T) prepare(i + ahead);
-
+        // the slot's next step (target i + ahead; a dummy past the last step) and this step's cell dofs:
+        // two independent transforms with no barrier between them, so their instructions interleave
+        CellIn<P, MODE> nxt;
+        stage_in(i + ahead, nxt);
         const int c = s - rr;
         const bool valid = act && c >= 0 && c < a.nx;
         double x[N];
@@ -453,6 +459,8 @@ __device__ __forceinline__ void modal_aux(const SweepArgs &a, const SweepItem &i
 #pragma unroll
                 for (int e = 0; e < P; ++e) x[e + P * d] = flip_sign<XN>(d) * flip_sign<YN>(e) * Z[e + P * d];
         }
+        // its inputs overwrite nothing the compute warp still reads; the result was read above
+        if (k0 + (i + ahead) * na < T) publish(i + ahead, nxt);
         if (a.out && valid) {
             double *op = a.out + (size_t)(TX ? a.nx - c : 1 + c) * istride + (size_t)j * plane + (size_t)q * N;
 #pragma unroll
