@@ -243,15 +243,18 @@ def extra_idc(abi, torch, dev, steps=10):
 def extra_adjoint(abi, torch, dev):
     """128x128 Q1 S8, log-normal sigma_t (median 2, log-sd 0.7), c = 0.9, Gaussian source at the left third,
     detector = scalar flux over a 16x16 window at the right third: gradients of all 3 nx ny per-cell
-    parameters (sigma_t, sigma_s, source) from one adjoint solve."""
+    parameters (sigma_t, sigma_s, source) from one adjoint solve (GMRES with the transposed DSA)."""
     from idcsweep.problems import detector_window, lognormal
     P = lognormal(128, 1, 8, seed=0, median=2.0, log_sd=0.7, c_fixed=0.9, source="gaussian")
     c_det = torch.from_numpy(detector_window(P, cells=16)).to(f"cuda:{dev}")
-    out = {"workload": "128x128 Q1 S8 log-normal (median 2, log-sd 0.7), c = 0.9, Gaussian source, 16x16 detector",
+    out = {"workload": "128x128 Q1 S8 log-normal (median 2, log-sd 0.7), c = 0.9, Gaussian source, 16x16 detector; "
+                       "adjoint GMRES(30) + transposed DSA (20 CG steps), abs tol 1e-12",
            "gradient_entries": 3 * P.nx * P.ny}
     with _ctx_for(abi, P, dev) as c:
         psi = torch.from_numpy(P.source).to(f"cuda:{dev}")
+        c.set_preconditioner(abi.PRECOND_DSA, 30)   # forward DSA; the adjoint uses its transpose
         c.gmres_solve(psi.data_ptr(), P.dt, abs_tol=1e-12, restart=30, max_its=3000, loc=abi.LOC_DEVICE)
+        c.set_preconditioner(abi.PRECOND_DSA, 20)   # 20 inner CG steps: the fastest adjoint solve here
         g_t = torch.zeros((P.nx + 2) * (P.ny + 2), dtype=torch.float64, device=f"cuda:{dev}")
         g_s = torch.zeros_like(g_t)
         g_q = torch.zeros(P.phi_shape(), dtype=torch.float64, device=f"cuda:{dev}")

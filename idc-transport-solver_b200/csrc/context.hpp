@@ -60,7 +60,7 @@ public:
     // whether the residual reached abs_tol (the caller decides whether that is an error)
     template <typename Op>
     Status gmres(Op apply, const double *b, double *x, double abs_tol, int restart, int64_t max_its, int64_t *iters,
-                 double *resid, bool *converged, bool dsa = false);
+                 double *resid, bool *converged, int dsa_mode = 0);   // 0 none, 1 DSA, 2 transposed DSA
     Status set_preconditioner(int kind, int inner_steps);   // 0 none, 1 DSA
     // IDC time integration (idc.cpp): psi (device, in/out) advanced `steps` steps of size dt with M
     // Gauss-Lobatto nodes and K corrections; scattering 0 = explicit (IMEX, one sweep per substep, CUDA

@@ -137,7 +137,8 @@ __global__ void cg_dir_kernel(int n, const double *__restrict__ sc, const double
 }
 
 // Initial state for x = 0: r = f = sigma_s * v_00 (interior), z = p = dinv r, x = 0; part <- block sums of r . z.
-__global__ void dsa_rhs_kernel(int nx, int ny, int N, const double *__restrict__ ss, const double *__restrict__ v,
+// rhs f = sigma_s v_00 (forward), or v_00 (transposed: sigma_s is applied to the solution instead)
+__global__ void dsa_rhs_kernel(int nx, int ny, int N, const double *__restrict__ ss, int scale, const double *__restrict__ v,
                                const double *__restrict__ dinv, double *__restrict__ x, double *__restrict__ r,
                                double *__restrict__ z, double *__restrict__ p, double *__restrict__ part) {
     const int n = nx * ny;
@@ -145,7 +146,7 @@ __global__ void dsa_rhs_kernel(int nx, int ny, int N, const double *__restrict__
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
         const int i = t / ny, j = t - (t / ny) * ny;
         const size_t c = (size_t)(i + 1) * (ny + 2) + (j + 1);
-        const double f = ss[c] * v[c * N];
+        const double f = scale ? ss[c] * v[c * N] : v[c * N];
         const double zt = dinv[t] * f;
         x[t] = 0.0;
         r[t] = f;
@@ -156,15 +157,19 @@ __global__ void dsa_rhs_kernel(int nx, int ny, int N, const double *__restrict__
     block_sum(dot, part);
 }
 
-// out = v, out_00 += x on interior cells (phi layout).
-__global__ void dsa_correct_kernel(int nx, int ny, int N, const double *v, const double *__restrict__ x, double *out) {
+// out = v, out_00 += x (forward) or sigma_s x (transposed, ss non-null) on interior cells (phi layout).
+__global__ void dsa_correct_kernel(int nx, int ny, int N, const double *v, const double *__restrict__ x,
+                                   const double *__restrict__ ss, double *out) {
     const size_t total = (size_t)(nx + 2) * (ny + 2) * N;
     for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
         const size_t c = t / N;
         const int k = (int)(t - c * N);
         const int i = (int)(c / (ny + 2)), j = (int)(c % (ny + 2));
         double val = v[t];
-        if (k == 0 && i >= 1 && i <= nx && j >= 1 && j <= ny) val += x[(size_t)(i - 1) * ny + (j - 1)];
+        if (k == 0 && i >= 1 && i <= nx && j >= 1 && j <= ny) {
+            const double xc = x[(size_t)(i - 1) * ny + (j - 1)];
+            val += ss ? ss[c] * xc : xc;
+        }
         out[t] = val;
     }
 }
@@ -200,11 +205,12 @@ struct DsaWs {
 };
 }  // namespace
 
-cudaError_t dsa_rhs(const GridDims &g, const double *sigma_s, const double *v, double *ws, cudaStream_t s) {
+cudaError_t dsa_rhs(const GridDims &g, const double *sigma_s, const double *v, double *ws, cudaStream_t s,
+                    bool transpose) {
     const int n = g.nx * g.ny;
     const DsaWs w(ws, n);
-    dsa_rhs_kernel<<<blocks_for(n), kThreads, 0, s>>>(g.nx, g.ny, g.P * g.P, sigma_s, v, w.dinv, w.x, w.r, w.z, w.p,
-                                                      w.part);
+    dsa_rhs_kernel<<<blocks_for(n), kThreads, 0, s>>>(g.nx, g.ny, g.P * g.P, sigma_s, transpose ? 0 : 1, v, w.dinv,
+                                                      w.x, w.r, w.z, w.p, w.part);
     return cudaGetLastError();
 }
 
@@ -225,19 +231,20 @@ cudaError_t dsa_cg(const GridDims &g, int cg_steps, double *ws, cudaStream_t s) 
 
 int dsa_cg_launches(int cg_steps) { return 1 + 5 * cg_steps; }
 
-cudaError_t dsa_correct(const GridDims &g, const double *v, double *ws, double *out, cudaStream_t s) {
+cudaError_t dsa_correct(const GridDims &g, const double *v, double *ws, double *out, cudaStream_t s,
+                        const double *sigma_s_after) {
     const int n = g.nx * g.ny;
     const DsaWs w(ws, n);
     const size_t tot = (size_t)(g.nx + 2) * (g.ny + 2) * g.P * g.P;
-    dsa_correct_kernel<<<blocks_for(tot), kThreads, 0, s>>>(g.nx, g.ny, g.P * g.P, v, w.x, out);
+    dsa_correct_kernel<<<blocks_for(tot), kThreads, 0, s>>>(g.nx, g.ny, g.P * g.P, v, w.x, sigma_s_after, out);
     return cudaGetLastError();
 }
 
 cudaError_t dsa_apply(const GridDims &g, const double *sigma_s, const double *v, double *out, int cg_steps, double *ws,
                       cudaStream_t s, int *launches) {
-    cudaError_t e = dsa_rhs(g, sigma_s, v, ws, s);
+    cudaError_t e = dsa_rhs(g, sigma_s, v, ws, s, false);
     if (e == cudaSuccess) e = dsa_cg(g, cg_steps, ws, s);
-    if (e == cudaSuccess) e = dsa_correct(g, v, ws, out, s);
+    if (e == cudaSuccess) e = dsa_correct(g, v, ws, out, s, nullptr);
     if (launches) *launches = 2 + dsa_cg_launches(cg_steps);
     return e;
 }

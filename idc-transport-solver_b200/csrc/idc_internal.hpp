@@ -159,11 +159,15 @@ cudaError_t dsa_setup(const GridDims &g, const double *sigma_t, const double *si
 cudaError_t dsa_apply(const GridDims &g, const double *sigma_s, const double *v, double *out, int cg_steps, double *ws,
                       cudaStream_t s, int *launches);
 // dsa_apply in three parts: the right-hand side from v, the Jacobi-PCG steps (workspace only, so one
-// CUDA graph of them serves every call on the same workspace), the correction out = v + x
-cudaError_t dsa_rhs(const GridDims &g, const double *sigma_s, const double *v, double *ws, cudaStream_t s);
+// CUDA graph of them serves every call on the same workspace), the correction out = v + x.  The
+// transposed preconditioner (for the adjoint operator) takes rhs = v_00 and corrects by sigma_s x:
+// out = v + E sigma_s C^{-1} R v, the transpose of v + E C^{-1} sigma_s R v (C symmetric).
+cudaError_t dsa_rhs(const GridDims &g, const double *sigma_s, const double *v, double *ws, cudaStream_t s,
+                    bool transpose);
 cudaError_t dsa_cg(const GridDims &g, int cg_steps, double *ws, cudaStream_t s);
 int dsa_cg_launches(int cg_steps);
-cudaError_t dsa_correct(const GridDims &g, const double *v, double *ws, double *out, cudaStream_t s);
+cudaError_t dsa_correct(const GridDims &g, const double *v, double *ws, double *out, cudaStream_t s,
+                        const double *sigma_s_after);
 // sum over interior cells of (a - b)^2 into *out (device double, pre-zeroed by the launcher)
 cudaError_t launch_l2dist2(const GridDims &g, const double *a, const double *b, double *out, cudaStream_t s);
 

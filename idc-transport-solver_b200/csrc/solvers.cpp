@@ -59,7 +59,8 @@ Status Context::apply_peierls(const double *x, double *y, double *tmp_phi, doubl
 // linear) and x = Z y.
 template <typename Op>
 Status Context::gmres(Op apply, const double *b, double *x, double abs_tol, int restart, int64_t max_its,
-                      int64_t *iters_out, double *resid_out, bool *converged_out, bool dsa) {
+                      int64_t *iters_out, double *resid_out, bool *converged_out, int dsa_mode) {
+    const bool dsa = dsa_mode != 0;
     if (restart < 1 || restart > 60) return bad(IDC_ERR_ARG, "gmres restart must be in 1..60");
     const size_t n = phi_len();
     const int m = restart;
@@ -107,9 +108,10 @@ Status Context::gmres(Op apply, const double *b, double *x, double abs_tol, int 
         for (int j = 0; j < m && its < max_its; ++j) {
             if (dsa) {
                 int nl = 0;
-                IDC_TRY_CUDA(dsa_rhs(dims(), d_sigma_s, Vc(j), d_dsa_ws, stream));
+                const bool tr = dsa_mode == 2;
+                IDC_TRY_CUDA(dsa_rhs(dims(), d_sigma_s, Vc(j), d_dsa_ws, stream, tr));
                 IDC_TRY(dsa_cg_graphed());
-                IDC_TRY_CUDA(dsa_correct(dims(), Vc(j), d_dsa_ws, Zc(j), stream));
+                IDC_TRY_CUDA(dsa_correct(dims(), Vc(j), d_dsa_ws, Zc(j), stream, tr ? d_sigma_s : nullptr));
                 launches += 2 + dsa_cg_launches(dsa_steps);
                 IDC_TRY(apply(Zc(j), Vc(j + 1)));
             } else {
@@ -194,7 +196,7 @@ Status Context::gmres_peierls(const double *src, double *psi_out, double dt, dou
     bool converged = false;
     double resid = 0.0;
     auto op = [&](const double *in, double *out) { return apply_peierls(in, out, tmp, dt, precision); };
-    IDC_TRY(gmres(op, b, x, abs_tol, restart, max_its, iters_out, &resid, &converged, precond_kind == 1));
+    IDC_TRY(gmres(op, b, x, abs_tol, restart, max_its, iters_out, &resid, &converged, precond_kind == 1 ? 1 : 0));
     // psi = L^{-1} (S phi + Q)  (PETScPeierlsSolver.cpp:504-505)
     IDC_TRY(sweep(src, psi_out, dt, nullptr, precision, x, 1.0));
     IDC_TRY(check_device_error());
@@ -256,7 +258,8 @@ Status Context::adjoint_solve(const double *detector, double *lam_out, double *L
     bool converged = false;
     double resid = 0.0;
     auto op = [&](const double *in, double *out) { return apply_peierls_adjoint(in, out, tmp, dt, precision); };
-    IDC_TRY(gmres(op, detector, mu, abs_tol, restart, max_its, iters, &resid, &converged));
+    // the transposed DSA preconditions the adjoint operator (the same spectrum as the forward one)
+    IDC_TRY(gmres(op, detector, mu, abs_tol, restart, max_its, iters, &resid, &converged, precond_kind == 1 ? 2 : 0));
     IDC_TRY(sweep(nullptr, lam_out, dt, Lam_out, precision, mu, 1.0, true));
     IDC_TRY(check_device_error());
     if (resid_out) *resid_out = resid;

@@ -271,7 +271,8 @@ class SweepContext:
         return int(sg.value), int(wp.value)
 
     def set_preconditioner(self, kind: int, inner_steps: int = 30):
-        """Right preconditioner of gmres_solve: PRECOND_NONE or PRECOND_DSA (inner_steps CG steps)."""
+        """Right preconditioner of gmres_solve (and, transposed, of adjoint_grad): PRECOND_NONE or PRECOND_DSA
+        (inner_steps CG steps)."""
         _check(self._lib.idc_set_preconditioner(self._h, int(kind), int(inner_steps)), "idc_set_preconditioner")
 
     def sweep_adjoint(self, source, result, dt=np.inf, moments=None, precision=PREC_FP64, loc=LOC_HOST):

@@ -174,7 +174,8 @@ int idc_gmres_solve(idc_ctx *ctx, double *source_inout, double dt, double abs_to
  * sigma_s r_00 with Marshak vacuum boundaries, by inner_steps Jacobi-preconditioned CG steps; GMRES then
  * runs in its flexible form.  The reference has DSA only in 1-D (SIP-DG inside its PETSc Peierls solver,
  * linear_solvers/RKDG/ImplicitSolver/PETScPeierlsSolver.cpp:27-376); the converged solution does not
- * depend on the preconditioner. */
+ * depend on the preconditioner.  The adjoint solve of idc_adjoint_grad uses its transpose (rhs r_00,
+ * correction sigma_s e), which gives the adjoint operator the preconditioned spectrum of the forward. */
 int idc_set_preconditioner(idc_ctx *ctx, int kind, int32_t inner_steps);
 
 /* ---- time integration ------------------------------------------------------------------------------- */
