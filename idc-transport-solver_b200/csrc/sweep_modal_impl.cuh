@@ -402,6 +402,7 @@ __device__ __forceinline__ void modal_aux(const SweepArgs &a, const SweepItem &i
     };
     // target i's inputs: wait for its stage (one cp.async group per target, in order), form them
     auto stage_in = [&](int i, CellIn<P, MODE> &cur) {
+        __syncwarp();   // the row segment's reads of the cell-data stage that lane o == 0 refills are done
         prefetch(i + D - 1);
         cp_wait<D - 2>();   // target i has landed
         __syncwarp();       // lane o == 0's cell-data copies are visible to its row segment
