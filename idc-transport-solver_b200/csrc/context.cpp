@@ -552,6 +552,13 @@ Status Context::lmv(double alpha, double beta, const double *x, double *y) {
     return Status::ok();
 }
 
+// res = (L - S P) psi given phi = P psi: Lmv(1, 0) then Smv(-1, 1) in one pass over psi, rounded alike
+Status Context::transport_residual(const double *psi, const double *phi, double *res) {
+    IDC_TRY_CUDA(launch_lmv(dims(), 1.0, 0.0, d_sigma_t, d_xi, d_eta, psi, res, stream, -1.0, d_sigma_s, phi));
+    launches += 1;
+    return Status::ok();
+}
+
 Status Context::l2dist(const double *a, const double *b, double *out_host) {
     IDC_TRY_CUDA(launch_l2dist2(dims(), a, b, d_scalar_, stream));
     launches += 1;

@@ -50,6 +50,7 @@ public:
     Status pmv(double alpha, double beta, const double *psi, double *phi);
     Status smv(double alpha, double beta, const double *phi, double *psi);
     Status lmv(double alpha, double beta, const double *x, double *y);
+    Status transport_residual(const double *psi, const double *phi, double *res);   // (L - S P) psi, phi = P psi
     Status l2dist(const double *a, const double *b, double *out_host);
     Status source_iteration(const double *src, double *psi_out, double dt, double abs_tol, int64_t max_its,
                             int precision, int64_t *iters, double *err);

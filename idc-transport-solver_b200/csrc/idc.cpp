@@ -169,8 +169,7 @@ Status Context::idc_integrate(double *psi, const double *Q, double dt, int64_t s
 
     auto residual = [&](int l) -> Status {   // res_l = (L - S P) psi_l  (ComputeResiduals, idc.cpp:1657-1667)
         IDC_TRY(pmv(1.0, 0.0, stage(l), phi(l)));
-        IDC_TRY(lmv(1.0, 0.0, stage(l), res(l)));
-        IDC_TRY(smv(-1.0, 1.0, phi(l), res(l)));
+        IDC_TRY(transport_residual(stage(l), phi(l), res(l)));
         return Status::ok();
     };
     auto source = [&](int n, bool correction, bool imex) -> Status {
@@ -202,8 +201,7 @@ Status Context::idc_integrate(double *psi, const double *Q, double dt, int64_t s
         }
         for (int p = 0; p < K; ++p) {
             for (int l = 0; l < M; ++l) {
-                IDC_TRY(lmv(1.0, 0.0, stage(l), res(l)));
-                IDC_TRY(smv(-1.0, 1.0, phi(l), res(l)));
+                IDC_TRY(transport_residual(stage(l), phi(l), res(l)));
                 IDC_TRY_CUDA(cudaMemcpyAsync(phi_old(l), phi(l), sizeof(double) * nm, cudaMemcpyDeviceToDevice, stream));
             }
             for (int n = 1; n < M; ++n) {

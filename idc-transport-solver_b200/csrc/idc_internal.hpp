@@ -125,8 +125,10 @@ cudaError_t launch_pmv(const GridDims &g, double alpha, double beta, const doubl
                        double *phi, cudaStream_t s);
 cudaError_t launch_smv(const GridDims &g, double alpha, double beta, const double *sigma_s, const double *phi,
                        double *psi, cudaStream_t s);
+// y = beta y + alpha L x (+ gamma sigma_s phi_sc / (4 pi) when phi_sc is given: Lmv and Smv in one pass)
 cudaError_t launch_lmv(const GridDims &g, double alpha, double beta, const double *sigma_t, const double *xi,
-                       const double *eta, const double *x, double *y, cudaStream_t s);
+                       const double *eta, const double *x, double *y, cudaStream_t s, double gamma = 0.0,
+                       const double *sigma_s = nullptr, const double *phi_sc = nullptr);
 cudaError_t launch_zero_ghost_phi(const GridDims &g, double *phi, cudaStream_t s);
 // phi = sum over `slots` partial-moment arrays (interior cells, fixed order); ghost cells of phi zeroed
 cudaError_t launch_reduce_phi_partials(const GridDims &g, const double *part, int slots, size_t stride, double *phi,

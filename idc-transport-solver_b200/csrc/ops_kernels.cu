@@ -38,37 +38,44 @@ __global__ void pmv_kernel(GridDims g, double alpha, double beta, const double *
 }
 
 // psi(q,i,j,k) <- beta*psi + alpha*sigma_s(i,j)*phi(i,j,k)/(4 pi): TransportOperator::Smv, :317-400.
+// One thread per (interior cell, ordinate): the cell's sigma_s phi / (4 pi) is formed once and written to
+// the ordinate's N dofs.  IDX is the index type (32-bit whenever nx ny nq fits).
+template <typename IDX>
 __global__ void smv_kernel(GridDims g, double alpha, double beta, const double *__restrict__ sigma_s,
                            const double *__restrict__ phi, double *__restrict__ psi) {
     const int N = g.P * g.P;
-    const size_t per_cell = (size_t)g.nq * N;
-    const size_t total = (size_t)g.nx * g.ny * per_cell;
-    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
-        const size_t cell = t / per_cell;
-        const size_t within = t - cell * per_cell;
-        const int k = (int)(within % N);
-        const int i = 1 + (int)(cell / g.ny), j = 1 + (int)(cell % g.ny);
+    const IDX total = (IDX)g.nx * g.ny * g.nq;
+    for (IDX t = blockIdx.x * (IDX)blockDim.x + threadIdx.x; t < total; t += (IDX)gridDim.x * blockDim.x) {
+        const IDX cell = t / (IDX)g.nq;
+        const int q = (int)(t - cell * (IDX)g.nq);
+        const int i = 1 + (int)(cell / (IDX)g.ny), j = 1 + (int)(cell - (cell / (IDX)g.ny) * (IDX)g.ny);
         const size_t cidx = (size_t)i * (g.ny + 2) + j;
-        const double v = (sigma_s[cidx] * phi[cidx * N + k] / (4.0 * M_PI)) * alpha;
-        const size_t idx = cidx * per_cell + within;
-        psi[idx] = beta == 0.0 ? v : beta * psi[idx] + v;   // beta = 0: psi is not read
+        const double ss = sigma_s[cidx];
+        double *out = psi + (cidx * g.nq + q) * N;
+        for (int k = 0; k < N; ++k) {
+            const double v = (ss * phi[cidx * N + k] / (4.0 * M_PI)) * alpha;
+            out[k] = beta == 0.0 ? v : beta * out[k] + v;   // beta = 0: psi is not read
+        }
     }
 }
 
 // y <- beta*y + alpha*(Omega.grad + sigma_t) x: TransportOperator::Lmv, :1215-1480 (piecewise-constant
-// sigma).  One thread per (interior cell, ordinate).
-template <int P>
+// sigma).  One thread per (interior cell, ordinate).  With phi_sc, the scattering term of Smv is added in
+// the same pass, y += (sigma_s phi_sc / (4 pi)) gamma, rounded as Lmv followed by Smv(gamma, 1) would
+// round it (the IDC residual (L - S P) psi in one pass over psi).
+template <int P, typename IDX>
 __global__ void lmv_kernel(GridDims g, double alpha, double beta, const double *__restrict__ sigma_t,
                            const double *__restrict__ xi_a, const double *__restrict__ eta_a,
-                           const double *__restrict__ x, double *__restrict__ y) {
+                           const double *__restrict__ x, double *__restrict__ y, double gamma,
+                           const double *__restrict__ sigma_s, const double *__restrict__ phi_sc) {
     constexpr int N = P * P;
     const size_t plane = (size_t)g.nq * N;
     const size_t istride = (size_t)(g.ny + 2) * plane;
-    const size_t total = (size_t)g.nx * g.ny * g.nq;
-    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
-        const int q = (int)(t % g.nq);
-        const size_t cell = t / g.nq;
-        const int i = 1 + (int)(cell / g.ny), j = 1 + (int)(cell % g.ny);
+    const IDX total = (IDX)g.nx * g.ny * g.nq;
+    for (IDX t = blockIdx.x * (IDX)blockDim.x + threadIdx.x; t < total; t += (IDX)gridDim.x * blockDim.x) {
+        const IDX cell = t / (IDX)g.nq;
+        const int q = (int)(t - cell * (IDX)g.nq);
+        const int i = 1 + (int)(cell / (IDX)g.ny), j = 1 + (int)(cell - (cell / (IDX)g.ny) * (IDX)g.ny);
         const double xi = xi_a[q], eta = eta_a[q];
         const bool xneg = xi <= 0.0, yneg = eta <= 0.0;
         const size_t base = (size_t)i * istride + (size_t)j * plane + (size_t)q * N;
@@ -120,8 +127,18 @@ __global__ void lmv_kernel(GridDims g, double alpha, double beta, const double *
 #pragma unroll
                 for (int b = e - 1; b >= 0; b -= 2) x3[e + P * d] -= double(2 * (2 * e + 1)) * cv * x0[b + P * d];
         double *Y = y + base;
+        if (!phi_sc) {
 #pragma unroll
-        for (int k = 0; k < N; ++k) Y[k] = beta == 0.0 ? alpha * x3[k] : beta * Y[k] + alpha * x3[k];
+            for (int k = 0; k < N; ++k) Y[k] = beta == 0.0 ? alpha * x3[k] : beta * Y[k] + alpha * x3[k];
+        } else {
+            const size_t cidx = (size_t)i * (g.ny + 2) + j;
+            const double ss = sigma_s[cidx];
+#pragma unroll
+            for (int k = 0; k < N; ++k) {
+                const double lv = beta == 0.0 ? __dmul_rn(alpha, x3[k]) : beta * Y[k] + alpha * x3[k];
+                Y[k] = __dadd_rn(lv, (ss * phi_sc[cidx * N + k] / (4.0 * M_PI)) * gamma);
+            }
+        }
     }
 }
 
@@ -362,18 +379,34 @@ cudaError_t launch_pmv(const GridDims &g, double alpha, double beta, const doubl
 
 cudaError_t launch_smv(const GridDims &g, double alpha, double beta, const double *sigma_s, const double *phi,
                        double *psi, cudaStream_t s) {
-    const size_t n = (size_t)g.nx * g.ny * g.nq * g.P * g.P;
-    smv_kernel<<<blocks_for(n), kThreads, 0, s>>>(g, alpha, beta, sigma_s, phi, psi);
+    const size_t n = (size_t)g.nx * g.ny * g.nq;
+    if (n < (size_t)INT32_MAX)
+        smv_kernel<int32_t><<<blocks_for(n), kThreads, 0, s>>>(g, alpha, beta, sigma_s, phi, psi);
+    else
+        smv_kernel<size_t><<<blocks_for(n), kThreads, 0, s>>>(g, alpha, beta, sigma_s, phi, psi);
     return cudaGetLastError();
 }
 
+template <int P>
+static void lmv_p(const GridDims &g, size_t n, double alpha, double beta, const double *sigma_t, const double *xi,
+                  const double *eta, const double *x, double *y, double gamma, const double *sigma_s,
+                  const double *phi_sc, cudaStream_t s) {
+    if (n < (size_t)INT32_MAX)
+        lmv_kernel<P, int32_t><<<blocks_for(n), kThreads, 0, s>>>(g, alpha, beta, sigma_t, xi, eta, x, y, gamma, sigma_s,
+                                                                   phi_sc);
+    else
+        lmv_kernel<P, size_t><<<blocks_for(n), kThreads, 0, s>>>(g, alpha, beta, sigma_t, xi, eta, x, y, gamma, sigma_s,
+                                                                  phi_sc);
+}
+
 cudaError_t launch_lmv(const GridDims &g, double alpha, double beta, const double *sigma_t, const double *xi,
-                       const double *eta, const double *x, double *y, cudaStream_t s) {
+                       const double *eta, const double *x, double *y, cudaStream_t s, double gamma,
+                       const double *sigma_s, const double *phi_sc) {
     const size_t n = (size_t)g.nx * g.ny * g.nq;
     switch (g.P) {
-        case 1: lmv_kernel<1><<<blocks_for(n), kThreads, 0, s>>>(g, alpha, beta, sigma_t, xi, eta, x, y); break;
-        case 2: lmv_kernel<2><<<blocks_for(n), kThreads, 0, s>>>(g, alpha, beta, sigma_t, xi, eta, x, y); break;
-        case 3: lmv_kernel<3><<<blocks_for(n), kThreads, 0, s>>>(g, alpha, beta, sigma_t, xi, eta, x, y); break;
+        case 1: lmv_p<1>(g, n, alpha, beta, sigma_t, xi, eta, x, y, gamma, sigma_s, phi_sc, s); break;
+        case 2: lmv_p<2>(g, n, alpha, beta, sigma_t, xi, eta, x, y, gamma, sigma_s, phi_sc, s); break;
+        case 3: lmv_p<3>(g, n, alpha, beta, sigma_t, xi, eta, x, y, gamma, sigma_s, phi_sc, s); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
