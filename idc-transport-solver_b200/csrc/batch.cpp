@@ -169,7 +169,7 @@ Status Batch::launch_group(Group &g, const double *const *srcs, double *const *o
         a.src = srcs ? srcs[p] : nullptr;
         a.out = outs ? outs[p] : nullptr;
         a.sigma_t = c.d_sigma_t;
-        a.sigma_s = c.d_sigma_s;
+        a.sigma_s = nullptr;   // the modal kernel's fused source takes ready scattering moments
         a.phi_scatter = phi_sc ? phi_sc[p] : nullptr;
         a.scatter_scale = scale;
         a.xi = c.d_xi;

@@ -14,7 +14,8 @@ public:
     ~Batch();
     Status add(Context *c);
     // per problem p (arrays indexed like `members`, entries nullable): outs[p] <- L^{-1}(srcs[p] +
-    // scale S phi_sc[p]), phis[p] <- P outs[p]; device pointers
+    // scale phi_sc[p]), phis[p] <- P outs[p]; device pointers.  phi_sc[p] holds the scattering moments
+    // sigma_s phi / (4 pi) per cell (launch_scatter_moments), S phi without the ordinate broadcast
     Status sweep(const double *const *srcs, double *const *outs, const double *const *phi_sc, double scale,
                  double *const *phis, double dt, int precision);
     // times the candidate tile shapes per degree on the given inputs and keeps the fastest

@@ -54,10 +54,10 @@ Context::~Context() {
     cudaFree(d_phi_part);
     cudaFree(d_trace);
     cudaFree(d_inflow);
+    cudaFree(d_scat);
     cudaFree(d_krylov);
     cudaFree(d_small);
     cudaFree(d_dsa_ws);
-    if (dsa_exec) cudaGraphExecDestroy(dsa_exec);
     for (int b = 0; b < 2; ++b) {
         if (ev_in[b]) cudaEventDestroy(ev_in[b]);
         if (ev_done[b]) cudaEventDestroy(ev_done[b]);
@@ -510,6 +510,20 @@ Status Context::sweep(const double *src, double *out, double dt, double *phi, in
                                               (int)ny, (int)nq, d_inflow, stream));
             launches += 1;
             a.inflow = d_inflow;
+        }
+        if (phi_scatter && !adjoint) {   // the scattering source's moments, once per cell instead of per ordinate
+            if (scat_len < phi_len()) {
+                if (capturing) return bad(IDC_ERR_STATE, "scattering buffer allocation inside a stream capture");
+                cudaFree(d_scat);
+                d_scat = nullptr;
+                scat_len = 0;
+                IDC_TRY_CUDA(cudaMalloc(&d_scat, sizeof(double) * phi_len()));
+                scat_len = phi_len();
+            }
+            IDC_TRY_CUDA(launch_scatter_moments(dims(), d_sigma_s, phi_scatter, d_scat, stream));
+            launches += 1;
+            a.phi_scatter = d_scat;
+            a.sigma_s = nullptr;
         }
         if (!capturing) IDC_TRY_CUDA(cudaEventRecord(ev0, stream));   // the timing covers the sweep kernel alone
         IDC_TRY_CUDA(launch_sweep_modal(P, precision, a, grid, smem, stream));

@@ -121,6 +121,8 @@ public:
     double *d_trace = nullptr;     // warp / modal kernel: per-item last-row traces (sentinel-armed)
     double *d_inflow = nullptr;    // modal kernel: inflow traces of the ghost cells
     size_t inflow_len = 0;
+    double *d_scat = nullptr;      // modal kernel: the fused scattering source's moments sigma_s phi / (4 pi)
+    size_t scat_len = 0;
     size_t trace_len = 0;
     int items_per_rb = 0;          // work items per row block (= ordinate chunks over all quadrants)
     double *d_phi_part = nullptr;  // warp kernel: per-chunk partial moments
@@ -139,14 +141,8 @@ public:
     int dsa_steps = 30;            // Jacobi-PCG steps per DSA application
     double *d_dsa_ws = nullptr;    // DSA workspace
     size_t dsa_ws_len = 0;
-    // the DSA Jacobi-PCG steps as one CUDA graph (workspace pointers only; rebuilt when the workspace or
-    // the step count changes)
-    cudaGraphExec_t dsa_exec = nullptr;
     cudaStream_t copy_in = nullptr, copy_out = nullptr;   // sweep_host_many's copy streams
     cudaEvent_t ev_in[2] = {}, ev_done[2] = {}, ev_out[2] = {};
-    const double *dsa_exec_ws = nullptr;
-    int dsa_exec_steps = -1;
-    Status dsa_cg_graphed();
     size_t krylov_len = 0;
     double *d_small = nullptr;     // GMRES Hessenberg column / coefficients (device)
 

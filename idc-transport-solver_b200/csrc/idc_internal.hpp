@@ -36,8 +36,10 @@ struct SweepArgs {
     const double *inflow;      // modal kernel: inflow traces of the ghost cells [nx + ny][nq][P], or null
     double *out;               // psi (written); may equal src (in-place sweep).  Warp kernel: null = not stored
     const double *sigma_t;     // (nx+2)(ny+2), piecewise constant
-    const double *sigma_s;     // (nx+2)(ny+2) or null: fused isotropic scattering source
-    const double *phi_scatter; // phi used by the fused scattering source, or null
+    const double *sigma_s;     // (nx+2)(ny+2) or null: fused isotropic scattering source (elimination kernels)
+    const double *phi_scatter; // fused scattering source, or null.  Elimination kernels: phi (scaled by sigma_s
+                               // / (4 pi) in the kernel).  Modal forward sweep: the per-cell moments
+                               // sigma_s phi / (4 pi) of launch_scatter_moments.  Transposed modal sweep: mu
     double *phi;               // fused moment output (atomically accumulated, pre-zeroed), or null
     double *phi_part;          // warp kernel: per-chunk partial moments [phi_slots][stride], or null
     int phi_slots;             // warp kernel: ordinate chunks per row block (items per row block)
@@ -130,11 +132,18 @@ cudaError_t launch_lmv(const GridDims &g, double alpha, double beta, const doubl
                        const double *eta, const double *x, double *y, cudaStream_t s, double gamma = 0.0,
                        const double *sigma_s = nullptr, const double *phi_sc = nullptr);
 cudaError_t launch_zero_ghost_phi(const GridDims &g, double *phi, cudaStream_t s);
+// out = sigma_s phi / (4 pi) per interior cell and moment (the isotropic scattering source of Smv, formed once
+// per cell for the modal sweep's fused source; ghost cells of out are not written)
+cudaError_t launch_scatter_moments(const GridDims &g, const double *sigma_s, const double *phi, double *out,
+                                   cudaStream_t s);
 // phi = sum over `slots` partial-moment arrays (interior cells, fixed order); ghost cells of phi zeroed
 cudaError_t launch_reduce_phi_partials(const GridDims &g, const double *part, int slots, size_t stride, double *phi,
                                        cudaStream_t s);
 // Krylov helpers on flat FP64 vectors of length n (device pointers; `out` arrays are device memory)
-cudaError_t launch_multidot(const double *V, int nv, size_t ld, const double *w, size_t n, double *out, cudaStream_t s);
+// out[k] = V_k . w for k < nv (<= 64), in a fixed order; scratch holds multidot_scratch_doubles() doubles
+size_t multidot_scratch_doubles();
+cudaError_t launch_multidot(const double *V, int nv, size_t ld, const double *w, size_t n, double *out, double *scratch,
+                            cudaStream_t s);
 cudaError_t launch_multiaxpy(double *w, const double *V, int nv, size_t ld, const double *c, size_t n, cudaStream_t s);
 cudaError_t launch_axpby(double a, const double *x, double b, double *y, size_t n, cudaStream_t s);
 cudaError_t launch_dot(const double *x, const double *y, size_t n, double *out, cudaStream_t s);
@@ -155,21 +164,16 @@ struct IdcTerms {
 cudaError_t launch_idc_source(const GridDims &g, const IdcTerms &t, const double *Q, double *out, cudaStream_t s);
 cudaError_t launch_phi_combine(size_t n, const double *a, const double *b, const double *c, double *out, cudaStream_t s);
 // DSA preconditioner (dsa_kernels.cu): workspace size, coefficient setup from the cross sections, and
-// out = v + C^{-1}(sigma_s v_00) on the (0,0) moment by cg_steps Jacobi-PCG steps (out may alias v)
+// out = v + C^{-1}(sigma_s v_00) on the (0,0) moment by cg_steps Jacobi-PCG steps (out may alias v): one
+// cooperative kernel (right-hand side and steps) and the correction kernel.  The transposed preconditioner
+// (for the adjoint operator) takes rhs = v_00 and corrects by sigma_s x: out = v + E sigma_s C^{-1} R v, the
+// transpose of v + E C^{-1} sigma_s R v (C symmetric).  A grid barrier that gives up sets *error.
 size_t dsa_workspace_doubles(int nx, int ny);
 cudaError_t dsa_setup(const GridDims &g, const double *sigma_t, const double *sigma_s, double *ws, cudaStream_t s);
-cudaError_t dsa_apply(const GridDims &g, const double *sigma_s, const double *v, double *out, int cg_steps, double *ws,
-                      cudaStream_t s, int *launches);
-// dsa_apply in three parts: the right-hand side from v, the Jacobi-PCG steps (workspace only, so one
-// CUDA graph of them serves every call on the same workspace), the correction out = v + x.  The
-// transposed preconditioner (for the adjoint operator) takes rhs = v_00 and corrects by sigma_s x:
-// out = v + E sigma_s C^{-1} R v, the transpose of v + E C^{-1} sigma_s R v (C symmetric).
-cudaError_t dsa_rhs(const GridDims &g, const double *sigma_s, const double *v, double *ws, cudaStream_t s,
-                    bool transpose);
-cudaError_t dsa_cg(const GridDims &g, int cg_steps, double *ws, cudaStream_t s);
-int dsa_cg_launches(int cg_steps);
-cudaError_t dsa_correct(const GridDims &g, const double *v, double *ws, double *out, cudaStream_t s,
-                        const double *sigma_s_after);
+cudaError_t dsa_precondition(const GridDims &g, const double *sigma_s, const double *v, double *out, int cg_steps,
+                             double *ws, bool transpose, int num_sms, int *error, long long spin_limit,
+                             cudaStream_t s);
+constexpr int kDsaLaunches = 2;
 // sum over interior cells of (a - b)^2 into *out (device double, pre-zeroed by the launcher)
 cudaError_t launch_l2dist2(const GridDims &g, const double *a, const double *b, double *out, cudaStream_t s);
 

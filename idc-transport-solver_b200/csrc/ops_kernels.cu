@@ -142,6 +142,20 @@ __global__ void lmv_kernel(GridDims g, double alpha, double beta, const double *
     }
 }
 
+// out = sigma_s phi / (4 pi) on interior cells, rounded as TransportOperator::Smv rounds its scattering term
+// (operators/RKDG/TransportOperator.cpp:317-400): the modal sweep adds scale * out to its source.
+__global__ void scatter_moments_kernel(GridDims g, const double *__restrict__ sigma_s, const double *__restrict__ phi,
+                                       double *__restrict__ out) {
+    const int N = g.P * g.P;
+    const size_t total = (size_t)g.nx * g.ny * N;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const size_t cell = t / N;
+        const int k = (int)(t - cell * N);
+        const size_t cidx = (size_t)(1 + cell / g.ny) * (g.ny + 2) + 1 + cell % g.ny;
+        out[cidx * N + k] = sigma_s[cidx] * phi[cidx * N + k] / (4.0 * M_PI);
+    }
+}
+
 __global__ void zero_ghost_phi_kernel(GridDims g, double *phi) {
     const int N = g.P * g.P;
     const int nxg = g.nx + 2, nyg = g.ny + 2;
@@ -203,33 +217,43 @@ __global__ void l2dist2_kernel(GridDims g, const double *__restrict__ a, const d
     }
 }
 
-// out[k] += sum_i V[k*ld + i] * w[i], k < nv (nv <= kMaxKrylov + 1); out pre-zeroed by the launcher.
+// Partial dot products V_k . w for the vectors k = 4 blockIdx.y .. +3 (< nv) over this block's share of i
+// (grid-stride in x), each a fixed-order block sum, into part[k * gridDim.x + blockIdx.x].  w is read once
+// per four vectors.
 constexpr int kMaxDots = 64;
-__global__ void multidot_kernel(const double *__restrict__ V, int nv, size_t ld, const double *__restrict__ w, size_t n,
-                                double *__restrict__ out) {
-    __shared__ double red[kMaxDots][kThreads / 32];
-    double acc[kMaxDots];
-#pragma unroll
-    for (int k = 0; k < kMaxDots; ++k) acc[k] = 0.0;
+constexpr int kDotBlocks = 2 * 148;
+__global__ void multidot_partial_kernel(const double *__restrict__ V, int nv, size_t ld, const double *__restrict__ w,
+                                        size_t n, double *__restrict__ part) {
+    __shared__ double red[4][kThreads / 32];
+    const int k0 = 4 * blockIdx.y;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         const double wi = w[i];
 #pragma unroll
-        for (int k = 0; k < kMaxDots; ++k)
-            if (k < nv) acc[k] += V[(size_t)k * ld + i] * wi;
+        for (int m = 0; m < 4; ++m)
+            if (k0 + m < nv) acc[m] = fma(V[(size_t)(k0 + m) * ld + i], wi, acc[m]);
     }
 #pragma unroll
-    for (int k = 0; k < kMaxDots; ++k) {
-        if (k >= nv) break;
-        double v = acc[k];
+    for (int m = 0; m < 4; ++m) {
+        double v = acc[m];
         for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-        if ((threadIdx.x & 31) == 0) red[k][threadIdx.x >> 5] = v;
+        if ((threadIdx.x & 31) == 0) red[m][threadIdx.x >> 5] = v;
     }
     __syncthreads();
-    for (int k = threadIdx.x; k < nv; k += blockDim.x) {
-        double v = 0.0;
-        for (int t = 0; t < (int)(blockDim.x >> 5); ++t) v += red[k][t];
-        atomicAdd(out + k, v);
+    if (threadIdx.x < 4 && k0 + (int)threadIdx.x < nv) {
+        double v = red[threadIdx.x][0];
+        for (int t = 1; t < (int)(blockDim.x >> 5); ++t) v += red[threadIdx.x][t];
+        part[(size_t)(k0 + threadIdx.x) * gridDim.x + blockIdx.x] = v;
     }
+}
+
+// out[k] = sum over the nb partial sums of vector k (one warp per k, fixed order).
+__global__ void multidot_final_kernel(const double *__restrict__ part, int nb, double *__restrict__ out) {
+    const int k = blockIdx.x;
+    double v = 0.0;
+    for (int b = threadIdx.x; b < nb; b += 32) v += part[(size_t)k * nb + b];
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    if (threadIdx.x == 0) out[k] = v;
 }
 
 // w[i] -= sum_k c[k] V[k*ld + i]
@@ -340,17 +364,17 @@ __global__ void adjoint_gradient_kernel(GridDims g, const double *__restrict__ p
 
 }  // namespace
 
-cudaError_t launch_multidot(const double *V, int nv, size_t ld, const double *w, size_t n, double *out,
+size_t multidot_scratch_doubles() { return (size_t)kMaxDots * kDotBlocks; }
+
+cudaError_t launch_multidot(const double *V, int nv, size_t ld, const double *w, size_t n, double *out, double *scratch,
                             cudaStream_t s) {
-    if (nv > kMaxDots) return cudaErrorInvalidValue;
-    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(double) * nv, s);
-    if (e != cudaSuccess) return e;
-    int blocks = blocks_for(n);
-    if (blocks > 148 * 2) blocks = 148 * 2;
-    multidot_kernel<<<blocks, kThreads, 0, s>>>(V, nv, ld, w, n, out);
+    if (nv < 1 || nv > kMaxDots) return cudaErrorInvalidValue;
+    int bx = blocks_for(n);
+    if (bx > kDotBlocks) bx = kDotBlocks;
+    multidot_partial_kernel<<<dim3(bx, (nv + 3) / 4), kThreads, 0, s>>>(V, nv, ld, w, n, scratch);
+    multidot_final_kernel<<<nv, 32, 0, s>>>(scratch, bx, out);
     return cudaGetLastError();
 }
-
 cudaError_t launch_multiaxpy(double *w, const double *V, int nv, size_t ld, const double *c, size_t n, cudaStream_t s) {
     multiaxpy_kernel<<<blocks_for(n), kThreads, 0, s>>>(w, V, nv, ld, c, n);
     return cudaGetLastError();
@@ -409,6 +433,13 @@ cudaError_t launch_lmv(const GridDims &g, double alpha, double beta, const doubl
         case 3: lmv_p<3>(g, n, alpha, beta, sigma_t, xi, eta, x, y, gamma, sigma_s, phi_sc, s); break;
         default: return cudaErrorInvalidValue;
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scatter_moments(const GridDims &g, const double *sigma_s, const double *phi, double *out,
+                                   cudaStream_t s) {
+    const size_t total = (size_t)g.nx * g.ny * g.P * g.P;
+    scatter_moments_kernel<<<blocks_for(total), kThreads, 0, s>>>(g, sigma_s, phi, out);
     return cudaGetLastError();
 }
 

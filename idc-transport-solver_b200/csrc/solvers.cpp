@@ -72,7 +72,8 @@ Status Context::gmres(Op apply, const double *b, double *x, double abs_tol, int 
         IDC_TRY_CUDA(cudaMalloc(&d_krylov, sizeof(double) * need));
         krylov_len = need;
     }
-    if (!d_small) IDC_TRY_CUDA(cudaMalloc(&d_small, sizeof(double) * 128));
+    if (!d_small) IDC_TRY_CUDA(cudaMalloc(&d_small, sizeof(double) * (128 + multidot_scratch_doubles())));
+    double *dot_scratch = d_small + 128;
     double *V = d_krylov;
     auto Vc = [&](int k) { return V + (size_t)k * n; };
     auto Zc = [&](int k) { return V + (size_t)(m + 1 + k) * n; };
@@ -107,25 +108,22 @@ Status Context::gmres(Op apply, const double *b, double *x, double abs_tol, int 
         int k = 0;   // columns built in this cycle
         for (int j = 0; j < m && its < max_its; ++j) {
             if (dsa) {
-                int nl = 0;
-                const bool tr = dsa_mode == 2;
-                IDC_TRY_CUDA(dsa_rhs(dims(), d_sigma_s, Vc(j), d_dsa_ws, stream, tr));
-                IDC_TRY(dsa_cg_graphed());
-                IDC_TRY_CUDA(dsa_correct(dims(), Vc(j), d_dsa_ws, Zc(j), stream, tr ? d_sigma_s : nullptr));
-                launches += 2 + dsa_cg_launches(dsa_steps);
+                IDC_TRY_CUDA(dsa_precondition(dims(), d_sigma_s, Vc(j), Zc(j), dsa_steps, d_dsa_ws, dsa_mode == 2,
+                                              num_sms, d_sync + 1, spin_limit, stream));
+                launches += kDsaLaunches;
                 IDC_TRY(apply(Zc(j), Vc(j + 1)));
             } else {
                 IDC_TRY(apply(Vc(j), Vc(j + 1)));
             }
             // CGS2: h = V^T w, w -= V h, twice
-            IDC_TRY_CUDA(launch_multidot(V, j + 1, n, Vc(j + 1), n, d_small, stream));
+            IDC_TRY_CUDA(launch_multidot(V, j + 1, n, Vc(j + 1), n, d_small, dot_scratch, stream));
             IDC_TRY_CUDA(cudaMemcpyAsync(h.data(), d_small, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost, stream));
             IDC_TRY_CUDA(launch_multiaxpy(Vc(j + 1), V, j + 1, n, d_small, n, stream));
-            IDC_TRY_CUDA(launch_multidot(V, j + 1, n, Vc(j + 1), n, d_small + 64, stream));
+            IDC_TRY_CUDA(launch_multidot(V, j + 1, n, Vc(j + 1), n, d_small + 64, dot_scratch, stream));
             IDC_TRY_CUDA(cudaMemcpyAsync(h2.data(), d_small + 64, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost,
                                          stream));
             IDC_TRY_CUDA(launch_multiaxpy(Vc(j + 1), V, j + 1, n, d_small + 64, n, stream));
-            launches += 4;
+            launches += 6;
             double hn = 0.0;
             IDC_TRY(dot_host(Vc(j + 1), Vc(j + 1), n, &hn));   // synchronises: h, h2 are on the host now
             hn = std::sqrt(hn);
@@ -204,28 +202,6 @@ Status Context::gmres_peierls(const double *src, double *psi_out, double dt, dou
     if (!converged)
         return bad(IDC_ERR_NOT_CONVERGED, "GMRES transport solve failed to converge (max_its reached, residual " +
                                               std::to_string(resid) + ")");
-    return Status::ok();
-}
-
-// The DSA steps (dsa_cg) captured once into a CUDA graph and replayed: one launch instead of 1 + 5 per
-// step (150 at 30 steps), whose launch gaps exceed the kernels' run times at these sizes.
-Status Context::dsa_cg_graphed() {
-    if (!dsa_exec || dsa_exec_ws != d_dsa_ws || dsa_exec_steps != dsa_steps) {
-        if (dsa_exec) cudaGraphExecDestroy(dsa_exec);
-        dsa_exec = nullptr;
-        IDC_TRY_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-        const cudaError_t e = dsa_cg(dims(), dsa_steps, d_dsa_ws, stream);
-        cudaGraph_t graph = nullptr;
-        const cudaError_t e2 = cudaStreamEndCapture(stream, &graph);
-        IDC_TRY_CUDA(e);
-        IDC_TRY_CUDA(e2);
-        const cudaError_t e3 = cudaGraphInstantiate(&dsa_exec, graph, 0);
-        cudaGraphDestroy(graph);
-        IDC_TRY_CUDA(e3);
-        dsa_exec_ws = d_dsa_ws;
-        dsa_exec_steps = dsa_steps;
-    }
-    IDC_TRY_CUDA(cudaGraphLaunch(dsa_exec, stream));
     return Status::ok();
 }
 

@@ -101,7 +101,7 @@ struct Layout {
     double *ring;                // [Wn+1][kS][G][P]: y traces
     double *slot;                // [Wn][kZ][CW + N][32]: a step's inputs (CW 8-byte words) and result
     double *src;                 // [Wn*nA][D][32][N]: an aux warp's prefetched cell source dofs
-    double *cellst;              // [Wn*nA][D][32/seg][N+2]: per row: sigma_t, sigma_s, phi_scatter[N]
+    double *cellst;              // [Wn*nA][D][32/seg][N+1]: per row: sigma_t, then the fused source's moments[N]
     double *w;                   // [G]
     double *red;                 // [Wn*nA][32][N]: an aux warp's weighted values for the moment reduction
 };
@@ -109,7 +109,7 @@ struct Layout {
 __host__ __device__ constexpr size_t layout_bytes(int wn, int na, int G, int P, int D, int rw, int cw) {
     return sizeof(uint64_t) * (size_t)(2 * (wn + 1) * kS + 2 * wn * kZ) +
            sizeof(double) * ((size_t)(wn + 1) * kS * G * P + (size_t)wn * kZ * (cw + P * P) * 32 +
-                             (size_t)wn * na * D * 32 * P * P + (size_t)wn * na * D * rw * (P * P + 2) +
+                             (size_t)wn * na * D * 32 * P * P + (size_t)wn * na * D * rw * (P * P + 1) +
                              (size_t)((G + 1) & ~1) + (size_t)wn * na * 32 * P * P);
 }
 
@@ -124,7 +124,7 @@ __device__ __forceinline__ Layout carve(unsigned char *raw, int wn, int na, int 
     L.slot = L.ring + (size_t)(wn + 1) * kS * G * P;
     L.src = L.slot + (size_t)wn * kZ * (cw + N) * 32;
     L.cellst = L.src + (size_t)wn * na * D * 32 * N;
-    L.w = L.cellst + (size_t)wn * na * D * rw * (N + 2);
+    L.w = L.cellst + (size_t)wn * na * D * rw * (N + 1);
     L.red = L.w + ((G + 1) & ~1);
     return L;
 }
@@ -138,13 +138,13 @@ __device__ __forceinline__ void prep_cell(CellIn<P, MODE> &in, const double *sp,
 #pragma unroll
     for (int k = 0; k < N; ++k) src[k] = a.src ? sp[k] : 0.0;
     if (a.phi_scatter) {
-        if constexpr (!ADJ) {   // fused TransportOperator::Smv(scale, 1, sigma_s, phi -> src)
-            const double sv = cp[1];
+        if constexpr (!ADJ) {   // fused TransportOperator::Smv(scale, 1, sigma_s, phi -> src); the moments
+                                // sigma_s phi / (4 pi) come from launch_scatter_moments (no division here)
 #pragma unroll
-            for (int k = 0; k < N; ++k) src[k] += a.scatter_scale * (sv * cp[2 + k] / (4.0 * M_PI));
+            for (int k = 0; k < N; ++k) src[k] += a.scatter_scale * cp[1 + k];
         } else {                // adjoint: the transpose of Pmv, w_q * mu
 #pragma unroll
-            for (int k = 0; k < N; ++k) src[k] = fma(wq, cp[2 + k], src[k]);
+            for (int k = 0; k < N; ++k) src[k] = fma(wq, cp[1 + k], src[k]);
         }
     }
     in.s = cp[0] + a.inv_dt;
@@ -338,7 +338,7 @@ __device__ __forceinline__ void modal_rows(const SweepArgs &a, const SweepItem &
 // waits for the result, finishes the cell (cell dofs from the backward modal transform or the MODE 1
 // sign flips, the psi store, the moments) and prepares step s + kZ in the freed slot.  The source is
 // prefetched with cp.async, prefetch_depth() of the warp's own steps ahead, into a per-warp stage ring
-// (lane o == 0 of a row also loads sigma_t and the fused scattering source).  A row segment's weighted
+// (lane o == 0 of a row also loads sigma_t and the fused source's moments).  A row segment's weighted
 // values meet in shared memory; the warp's Rw x N (row, dof) sums over each segment's ordinates are
 // spread over the lanes, each a fixed pairwise tree, and stored into this chunk's partial moments.
 template <int P, int MODE, int SEG, bool XN, bool YN, bool ADJ>
@@ -350,7 +350,7 @@ __device__ __forceinline__ void modal_aux(const SweepArgs &a, const SweepItem &i
     using TZ = std::conditional_t<MODE == 1, double, TS>;
     constexpr int seg = SEG, Rw = 32 / SEG;
     constexpr int D = prefetch_depth(P);
-    constexpr int NC = N + 2;
+    constexpr int NC = N + 1;
     const int rr = lane / seg, o = lane - rr * seg;
     const int row_w = item.row_block * a.wn * Rw + w * Rw;
     const int row = row_w + rr;
@@ -392,9 +392,8 @@ __device__ __forceinline__ void modal_aux(const SweepArgs &a, const SweepItem &i
                 double *d = my_cell + (size_t)(i % D) * Rw * NC;
                 cp_async8(d, a.sigma_t + cidx);
                 if (a.phi_scatter) {
-                    cp_async8(d + 1, a.sigma_s + cidx);
 #pragma unroll
-                    for (int k = 0; k < N; ++k) cp_async8(d + 2 + k, a.phi_scatter + cidx * N + k);
+                    for (int k = 0; k < N; ++k) cp_async8(d + 1 + k, a.phi_scatter + cidx * N + k);
                 }
             }
         }
