@@ -43,6 +43,7 @@ Context::~Context() {
     for (double *p : phi_bufs_) cudaFree(p);
     for (double *p : idc_psi_) cudaFree(p);
     for (double *p : idc_phi_) cudaFree(p);
+    for (double *p : transient_bufs_) cudaFree(p);
     cudaFree(d_scalar_);
     cudaFree(d_xi);
     cudaFree(d_eta);
@@ -83,7 +84,7 @@ Status Context::init() {
     IDC_TRY_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     IDC_TRY_CUDA(cudaEventCreate(&ev0));
     IDC_TRY_CUDA(cudaEventCreate(&ev1));
-    IDC_TRY_CUDA(cudaMalloc(&d_scalar_, sizeof(double) * 4));
+    IDC_TRY_CUDA(cudaMalloc(&d_scalar_, sizeof(double) * (4 + multidot_scratch_doubles())));   // + dot scratch
     // IDC_SWEEP_KERNEL=warp|rowsync selects one of the elimination kernels instead of the modal one
     if (const char *k = std::getenv("IDC_SWEEP_KERNEL")) {
         const std::string v(k);

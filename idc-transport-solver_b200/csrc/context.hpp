@@ -76,6 +76,15 @@ public:
     Status adjoint_gradient(const double *psi, const double *detector, double dt, double abs_tol, int restart,
                             int64_t max_its, int precision, double *dsig_t, double *dsig_s, double *dq,
                             int64_t *iters, double *resid);
+    // (L' - S P)^T lam = b for a psi-sized b (interior cells): with nu = S^T lam, (I - S^T L'^{-T} P^T) nu =
+    // S^T L'^{-T} b by GMRES, then lam = L'^{-T} (b + P^T nu); Lam_out = sum_q lam_q
+    Status adjoint_solve_psi(const double *b, double *lam_out, double *Lam_out, double dt, double abs_tol, int restart,
+                             int64_t max_its, int precision, int64_t *iters);
+    // gradients of J = c . P psi^steps for implicit-Euler steps (1/dt + L - S P) psi^{n+1} = psi^n / dt + Q
+    // (device arrays), states kept every `checkpoint_every` steps and recomputed segment by segment
+    Status adjoint_transient(const double *psi0, const double *Q, double dt, int64_t steps, const double *detector,
+                             int64_t checkpoint_every, double abs_tol, int restart, int64_t max_its, int precision,
+                             double *dsig_t, double *dsig_s, double *dq, double *dpsi0, double *J, int64_t *solves);
     Status dot_host(const double *x, const double *y, size_t n, double *out);
 
     // ---- buffers ----
@@ -149,6 +158,7 @@ public:
 private:
     Status build_schedule(int precision);
     std::vector<double *> psi_bufs_, phi_bufs_;
+    std::vector<double *> transient_bufs_;   // adjoint_transient: checkpoints, segment states, lam, b, source
     std::vector<double *> idc_psi_, idc_phi_;
     double *d_scalar_ = nullptr;
 };

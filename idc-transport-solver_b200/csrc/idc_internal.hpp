@@ -146,14 +146,15 @@ cudaError_t launch_multidot(const double *V, int nv, size_t ld, const double *w,
                             cudaStream_t s);
 cudaError_t launch_multiaxpy(double *w, const double *V, int nv, size_t ld, const double *c, size_t n, cudaStream_t s);
 cudaError_t launch_axpby(double a, const double *x, double b, double *y, size_t n, cudaStream_t s);
-cudaError_t launch_dot(const double *x, const double *y, size_t n, double *out, cudaStream_t s);
+cudaError_t launch_dot(const double *x, const double *y, size_t n, double *out, double *scratch, cudaStream_t s);
 // adjoint Peierls operator: y = x - sigma_s/(4 pi) lam on interior cells, y = x on ghost cells
 cudaError_t launch_adjoint_scatter(const GridDims &g, const double *sigma_s, const double *x, const double *lam,
                                    double *y, cudaStream_t s);
 // per-cell gradients of J = c . phi from the forward psi, phi and the adjoint lam, Lam = sum_q lam_q
 // (outputs on the halo layouts, interior cells written, any of them nullable)
 cudaError_t launch_adjoint_gradient(const GridDims &g, const double *psi, const double *lam, const double *phi,
-                                    const double *Lam, double *dsig_t, double *dsig_s, double *dq, cudaStream_t s);
+                                    const double *Lam, double *dsig_t, double *dsig_s, double *dq, cudaStream_t s,
+                                    bool accumulate = false);
 // IDC (ops_kernels.cu): out = sum_k c_k A_k + Q on interior cells, Q on ghost cells (Q nullable = 0)
 struct IdcTerms {
     static constexpr int kMax = 10;

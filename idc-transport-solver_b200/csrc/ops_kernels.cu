@@ -274,20 +274,6 @@ __global__ void axpby_kernel(double a, const double *__restrict__ x, double b, d
 }
 
 // out[0] += sum x*y
-__global__ void dot_kernel(const double *__restrict__ x, const double *__restrict__ y, size_t n, double *__restrict__ out) {
-    double acc = 0.0;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        acc += x[i] * y[i];
-    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
-    __shared__ double ws[kThreads / 32];
-    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = acc;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        acc = threadIdx.x < (blockDim.x >> 5) ? ws[threadIdx.x] : 0.0;
-        for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
-        if (threadIdx.x == 0) atomicAdd(out, acc);
-    }
-}
 
 
 
@@ -334,9 +320,11 @@ __global__ void adjoint_scatter_kernel(GridDims g, const double *__restrict__ si
 // Gradients of J = c . phi per interior cell (one warp per cell; the cell's nq*N values are contiguous):
 // dJ/dsigma_t = -sum_{q,k} lam psi, dJ/dsigma_s = sum_k Lam_k phi_k / (4 pi), dJ/dq_k = Lam_k / (4 pi),
 // with Lam = sum_q lam_q and q the isotropic source moments (angular source q / (4 pi)).
+// With `accumulate` the contributions are added to the outputs (sums over time steps).
 __global__ void adjoint_gradient_kernel(GridDims g, const double *__restrict__ psi, const double *__restrict__ lam,
                                         const double *__restrict__ phi, const double *__restrict__ Lam,
-                                        double *__restrict__ dsig_t, double *__restrict__ dsig_s, double *__restrict__ dq) {
+                                        double *__restrict__ dsig_t, double *__restrict__ dsig_s, double *__restrict__ dq,
+                                        int accumulate) {
     const int N = g.P * g.P;
     const int lane = threadIdx.x & 31;
     const size_t warps = (size_t)gridDim.x * (blockDim.x / 32);
@@ -352,12 +340,12 @@ __global__ void adjoint_gradient_kernel(GridDims g, const double *__restrict__ p
         if (lane < N) {
             const double L = Lam[cidx * N + lane];
             accs = L * phi[cidx * N + lane];
-            if (dq) dq[cidx * N + lane] = L / (4.0 * M_PI);
+            if (dq) dq[cidx * N + lane] = (accumulate ? dq[cidx * N + lane] : 0.0) + L / (4.0 * M_PI);
         }
         for (int off = 16; off > 0; off >>= 1) accs += __shfl_xor_sync(0xffffffffu, accs, off);
         if (lane == 0) {
-            if (dsig_t) dsig_t[cidx] = -acc;
-            if (dsig_s) dsig_s[cidx] = accs / (4.0 * M_PI);
+            if (dsig_t) dsig_t[cidx] = (accumulate ? dsig_t[cidx] : 0.0) - acc;
+            if (dsig_s) dsig_s[cidx] = (accumulate ? dsig_s[cidx] : 0.0) + accs / (4.0 * M_PI);
         }
     }
 }
@@ -385,13 +373,8 @@ cudaError_t launch_axpby(double a, const double *x, double b, double *y, size_t 
     return cudaGetLastError();
 }
 
-cudaError_t launch_dot(const double *x, const double *y, size_t n, double *out, cudaStream_t s) {
-    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(double), s);
-    if (e != cudaSuccess) return e;
-    int blocks = blocks_for(n);
-    if (blocks > 148 * 4) blocks = 148 * 4;
-    dot_kernel<<<blocks, kThreads, 0, s>>>(x, y, n, out);
-    return cudaGetLastError();
+cudaError_t launch_dot(const double *x, const double *y, size_t n, double *out, double *scratch, cudaStream_t s) {
+    return launch_multidot(x, 1, n, y, n, out, scratch, s);   // fixed order: bitwise reproducible
 }
 
 cudaError_t launch_pmv(const GridDims &g, double alpha, double beta, const double *w, const double *psi, double *phi,
@@ -479,9 +462,11 @@ cudaError_t launch_adjoint_scatter(const GridDims &g, const double *sigma_s, con
 }
 
 cudaError_t launch_adjoint_gradient(const GridDims &g, const double *psi, const double *lam, const double *phi,
-                                    const double *Lam, double *dsig_t, double *dsig_s, double *dq, cudaStream_t s) {
+                                    const double *Lam, double *dsig_t, double *dsig_s, double *dq, cudaStream_t s,
+                                    bool accumulate) {
     const size_t warps = (size_t)g.nx * g.ny;
-    adjoint_gradient_kernel<<<blocks_for(warps * 32), kThreads, 0, s>>>(g, psi, lam, phi, Lam, dsig_t, dsig_s, dq);
+    adjoint_gradient_kernel<<<blocks_for(warps * 32), kThreads, 0, s>>>(g, psi, lam, phi, Lam, dsig_t, dsig_s, dq,
+                                                                        accumulate ? 1 : 0);
     return cudaGetLastError();
 }
 

@@ -33,8 +33,8 @@ Status bad(int code, const std::string &m) {
 }  // namespace
 
 Status Context::dot_host(const double *x, const double *y, size_t n, double *out) {
-    IDC_TRY_CUDA(launch_dot(x, y, n, d_scalar_, stream));
-    launches += 1;
+    IDC_TRY_CUDA(launch_dot(x, y, n, d_scalar_, d_scalar_ + 4, stream));
+    launches += 2;
     IDC_TRY_CUDA(cudaMemcpyAsync(out, d_scalar_, sizeof(double), cudaMemcpyDeviceToHost, stream));
     IDC_TRY_CUDA(cudaStreamSynchronize(stream));
     return Status::ok();
@@ -258,6 +258,130 @@ Status Context::adjoint_gradient(const double *psi, const double *detector, doub
     if (dq) IDC_TRY_CUDA(cudaMemsetAsync(dq, 0, sizeof(double) * phi_len(), stream));
     IDC_TRY_CUDA(launch_adjoint_gradient(dims(), psi, lam, phi, Lam, dsig_t, dsig_s, dq, stream));
     launches += 1;
+    return Status::ok();
+}
+
+Status Context::adjoint_solve_psi(const double *b, double *lam_out, double *Lam_out, double dt, double abs_tol,
+                                  int restart, int64_t max_its, int precision, int64_t *iters) {
+    if (kernel != kModal) return bad(IDC_ERR_UNSUPPORTED, "the adjoint needs the modal sweep kernel");
+    IDC_TRY(ensure_phi_buffers(9));
+    double *nu = phi_buf(6), *tmp = phi_buf(7), *rhs = phi_buf(8);
+    // rhs = S^T L'^{-T} b: the transposed sweep's moment sums, scaled by sigma_s / (4 pi); ghost cells zero
+    IDC_TRY(sweep(b, nullptr, dt, tmp, precision, nullptr, 1.0, true));
+    IDC_TRY_CUDA(cudaMemsetAsync(rhs, 0, sizeof(double) * phi_len(), stream));
+    IDC_TRY_CUDA(launch_scatter_moments(dims(), d_sigma_s, tmp, rhs, stream));
+    launches += 1;
+    bool converged = false;
+    double resid = 0.0;
+    auto op = [&](const double *in, double *out) { return apply_peierls_adjoint(in, out, tmp, dt, precision); };
+    IDC_TRY(gmres(op, rhs, nu, abs_tol, restart, max_its, iters, &resid, &converged, precond_kind == 1 ? 2 : 0));
+    IDC_TRY(sweep(b, lam_out, dt, Lam_out, precision, nu, 1.0, true));   // lam = L'^{-T} (b + P^T nu)
+    IDC_TRY(check_device_error());
+    if (!converged)
+        return bad(IDC_ERR_NOT_CONVERGED, "adjoint GMRES failed to converge (max_its reached, residual " +
+                                              std::to_string(resid) + ")");
+    return Status::ok();
+}
+
+// Discrete adjoint of implicit-Euler time stepping (the reference's `dirk` integrator with the `euler`
+// table, time_integrators/RKDG/dirk.cpp; equally IDC's prediction sweeps, time_integrators/RKDG/idc.cpp:
+// 846-955): A psi^{n+1} = psi^n / dt + Q with A = 1/dt + L - S P, each step solved by the Peierls GMRES, and
+// J = c . P psi^N.  The adjoint runs backwards: A^T lam^N = P^T c, A^T lam^n = lam^{n+1} / dt, and
+//     dJ/dsigma_t = -sum_n sum_{q,k} lam^n psi^n,   dJ/dsigma_s = sum_n sum_k Lam^n_k phi^n_k / (4 pi),
+//     dJ/dq_k = sum_n Lam^n_k / (4 pi),             dJ/dpsi^0 = lam^1 / dt
+// per cell (Q = q / (4 pi) on every ordinate, constant in time).  Checkpointing: the forward pass keeps
+// psi^{mK} (K = checkpoint_every); the backward pass recomputes each segment's states from its checkpoint
+// (the same deterministic solves, so the states are bitwise those of the forward pass) and runs the
+// segment's adjoint steps, so memory holds N/K + K states instead of N.  Inflow (ghost cells of Q) is data,
+// not differentiated.
+Status Context::adjoint_transient(const double *psi0, const double *Q, double dt, int64_t steps,
+                                  const double *detector, int64_t checkpoint_every, double abs_tol, int restart,
+                                  int64_t max_its, int precision, double *dsig_t, double *dsig_s, double *dq,
+                                  double *dpsi0, double *J, int64_t *solves) {
+    if (!have_ordinates || !have_sigma) return bad(IDC_ERR_STATE, "transient adjoint before ordinates and sigma");
+    if (kernel != kModal) return bad(IDC_ERR_UNSUPPORTED, "the adjoint needs the modal sweep kernel");
+    if (steps < 1) return bad(IDC_ERR_ARG, "transient adjoint needs at least one step");
+    if (!(dt > 0) || !std::isfinite(dt)) return bad(IDC_ERR_ARG, "transient adjoint needs a finite positive dt");
+    const int64_t K = checkpoint_every > 0 ? std::min(checkpoint_every, steps)
+                                           : std::max<int64_t>(1, (int64_t)std::ceil(std::sqrt((double)steps)));
+    const int64_t M = (steps + K - 1) / K;   // segments; checkpoints psi^{mK}, m = 0..M-1
+    const size_t np = psi_len(), nm = phi_len();
+    const int need = (int)(M + K + 3);
+    IDC_TRY_CUDA(cudaSetDevice(device));
+    while ((int)transient_bufs_.size() < need) {   // zeroed once: the sweeps write interior cells only, so the
+        double *p = nullptr;                        // ghost cells of every state stay zero
+        IDC_TRY_CUDA(cudaMalloc(&p, sizeof(double) * np));
+        IDC_TRY_CUDA(cudaMemsetAsync(p, 0, sizeof(double) * np, stream));
+        transient_bufs_.push_back(p);
+    }
+    auto ckpt = [&](int64_t m) { return transient_bufs_[(size_t)m]; };
+    auto seg = [&](int64_t k) { return transient_bufs_[(size_t)(M + k - 1)]; };   // k = 1..K
+    double *lam = transient_bufs_[(size_t)(M + K)], *b = transient_bufs_[(size_t)(M + K + 1)];
+    double *src = transient_bufs_[(size_t)(M + K + 2)];
+    IDC_TRY(ensure_phi_buffers(11));
+    double *Lam = phi_buf(9), *phi = phi_buf(10);
+    int64_t nsolve = 0;
+
+    // one step: out = A^{-1} (in / dt + Q)
+    auto step = [&](const double *in, double *out) -> Status {
+        IdcTerms tm{};
+        tm.n = 1;
+        tm.a[0] = in;
+        tm.c[0] = 1.0 / dt;
+        IDC_TRY_CUDA(launch_idc_source(dims(), tm, Q, src, stream));
+        launches += 1;
+        int64_t its = 0;
+        double r = 0.0;
+        IDC_TRY(gmres_peierls(src, out, dt, abs_tol, restart, max_its, precision, &its, &r));
+        ++nsolve;
+        return Status::ok();
+    };
+
+    // forward pass: checkpoints, and psi^N in the last segment slot for J
+    IDC_TRY_CUDA(cudaMemcpyAsync(ckpt(0), psi0, sizeof(double) * np, cudaMemcpyDeviceToDevice, stream));
+    const double *cur = ckpt(0);
+    for (int64_t n = 1; n <= steps; ++n) {
+        double *out = (n % K == 0 && n / K < M) ? ckpt(n / K) : seg(1);
+        IDC_TRY(step(cur, out));
+        cur = out;
+    }
+    IDC_TRY(pmv(1.0, 0.0, cur, phi));
+    if (J) IDC_TRY(dot_host(phi, detector, nm, J));
+
+    if (dsig_t) IDC_TRY_CUDA(cudaMemsetAsync(dsig_t, 0, sizeof(double) * sig_len(), stream));
+    if (dsig_s) IDC_TRY_CUDA(cudaMemsetAsync(dsig_s, 0, sizeof(double) * sig_len(), stream));
+    if (dq) IDC_TRY_CUDA(cudaMemsetAsync(dq, 0, sizeof(double) * nm, stream));
+    // backward pass, one segment (m K, min((m+1) K, N)] at a time
+    for (int64_t m = M - 1; m >= 0; --m) {
+        const int64_t n0 = m * K, n1 = std::min(steps, n0 + K);
+        for (int64_t k = 1; k <= n1 - n0; ++k) IDC_TRY(step(k == 1 ? ckpt(m) : seg(k - 1), seg(k)));
+        for (int64_t n = n1; n > n0; --n) {
+            int64_t its = 0;
+            if (n == steps) {   // A^T lam^N = P^T c
+                double resid = 0.0;
+                IDC_TRY(adjoint_solve(detector, lam, Lam, dt, abs_tol, restart, max_its, precision, &its, &resid));
+            } else {            // A^T lam^n = lam^{n+1} / dt
+                IDC_TRY_CUDA(launch_axpby(1.0 / dt, lam, 0.0, b, np, stream));
+                launches += 1;
+                IDC_TRY(adjoint_solve_psi(b, lam, Lam, dt, abs_tol, restart, max_its, precision, &its));
+            }
+            ++nsolve;
+            const double *psin = seg(n - n0);
+            IDC_TRY(pmv(1.0, 0.0, psin, phi));
+            IDC_TRY_CUDA(launch_adjoint_gradient(dims(), psin, lam, phi, Lam, dsig_t, dsig_s, dq, stream, true));
+            launches += 1;
+        }
+    }
+    if (dpsi0) {   // lam^1 / dt on interior cells, zero ghost cells
+        IdcTerms tm{};
+        tm.n = 1;
+        tm.a[0] = lam;
+        tm.c[0] = 1.0 / dt;
+        IDC_TRY_CUDA(launch_idc_source(dims(), tm, nullptr, dpsi0, stream));
+        launches += 1;
+    }
+    IDC_TRY(check_device_error());
+    if (solves) *solves = nsolve;
     return Status::ok();
 }
 

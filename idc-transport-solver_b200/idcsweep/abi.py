@@ -43,7 +43,7 @@ EXPORTED_SYMBOLS = (
     "idc_adjoint_grad", "idc_set_preconditioner", "idc_idc_integrate", "idc_write_sd2", "idc_read_sd2",
     "idc_write_af2", "idc_read_af2", "idc_sweep_fused", "idc_set_tile_shape", "idc_autotune", "idc_batch_create",
     "idc_batch_add", "idc_batch_sweep", "idc_batch_autotune", "idc_batch_last_timing", "idc_batch_destroy",
-    "idc_batch_set_shape", "idc_batch_get_shape", "idc_sweep_out_many",
+    "idc_batch_set_shape", "idc_batch_get_shape", "idc_sweep_out_many", "idc_adjoint_transient",
 )
 
 
@@ -108,6 +108,8 @@ def load_library(path: str = LIB_PATH):
                                       C.c_double, C.c_int32, C.c_int64, C.c_int, C.c_int, C.POINTER(C.c_int64)]
     lib.idc_adjoint_grad.argtypes = [vp, vp, vp, C.c_double, C.c_double, C.c_int32, C.c_int64, C.c_int, vp, vp, vp,
                                      C.c_int, C.POINTER(C.c_int64), _dp]
+    lib.idc_adjoint_transient.argtypes = [vp, vp, vp, C.c_double, C.c_int64, vp, C.c_int64, C.c_double, C.c_int32,
+                                          C.c_int64, C.c_int, vp, vp, vp, vp, _dp, C.c_int, C.POINTER(C.c_int64)]
     lib.idc_gmres_solve.argtypes = [vp, vp, C.c_double, C.c_double, C.c_int32, C.c_int64, C.c_int, C.c_int,
                                     C.POINTER(C.c_int64), _dp]
     lib.idc_sweep_noalloc.argtypes = [C.POINTER(ProblemDesc), C.c_int64, vp, vp, vp, vp, vp, vp, vp, C.c_double, vp,
@@ -291,6 +293,21 @@ class SweepContext:
                                           _ptr(dsigma_s, loc), _ptr(dsource, loc), loc, C.byref(its), C.byref(res)),
                "idc_adjoint_grad")
         return int(its.value), float(res.value)
+
+    def adjoint_transient(self, psi0, source, detector, dt, steps, checkpoint_every=0, dsigma_t=None, dsigma_s=None,
+                          dsource=None, dpsi0=None, abs_tol=1e-12, restart=30, max_its=3000, precision=PREC_FP64,
+                          loc=LOC_HOST):
+        """Gradients of J = detector . phi(psi^steps) after `steps` implicit-Euler steps from psi0 with the
+        constant source, written into the given arrays (sigma_t, sigma_s: halo cell layout; dsource: phi
+        layout; dpsi0: psi layout).  Returns (J, number of forward and adjoint GMRES solves)."""
+        jv = C.c_double()
+        ns = C.c_int64()
+        _check(self._lib.idc_adjoint_transient(self._h, _ptr(psi0, loc), _ptr(source, loc), float(dt), int(steps),
+                                               _ptr(detector, loc), int(checkpoint_every), float(abs_tol),
+                                               int(restart), int(max_its), int(precision), _ptr(dsigma_t, loc),
+                                               _ptr(dsigma_s, loc), _ptr(dsource, loc), _ptr(dpsi0, loc),
+                                               C.byref(jv), loc, C.byref(ns)), "idc_adjoint_transient")
+        return float(jv.value), int(ns.value)
 
     def last_timing(self):
         ms = C.c_double()

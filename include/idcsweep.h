@@ -259,6 +259,24 @@ int idc_adjoint_grad(idc_ctx *ctx, const double *psi, const double *detector, do
                      int32_t restart, int64_t max_its, int precision, double *dsigma_t, double *dsigma_s,
                      double *dsource, int loc, int64_t *iters, double *final_resid);
 
+/* Gradients of J = sum detector * phi(psi^steps) after `steps` implicit-Euler steps
+ * (1/dt + L - S P) psi^{n+1} = psi^n / dt + source, psi^0 = psi0 (each step the Peierls GMRES solve of
+ * idc_gmres_solve), with respect to the per-cell sigma_t, sigma_s (halo layout), the isotropic source
+ * moments dsource (phi layout; source = moment / (4 pi) on every ordinate, constant in time) and the
+ * initial angular flux dpsi0 (psi layout, ghost cells zero).  The adjoint steps run backwards,
+ * A^T lam^N = P^T detector and A^T lam^n = lam^{n+1} / dt, and the gradients sum the per-step terms of
+ * idc_adjoint_grad over n.  The forward states are checkpointed every `checkpoint_every` steps (<= 0: about
+ * sqrt(steps)) and recomputed segment by segment in the backward pass, so device memory holds about
+ * steps / checkpoint_every + checkpoint_every angular fluxes.  J (nullable) receives the functional;
+ * *solves (nullable) the number of forward and adjoint GMRES solves.  Ghost cells of source are the fixed
+ * inflow (not differentiated).  Outputs are nullable.  No counterpart in the reference: it is the transpose
+ * of the implicit-Euler (DIRK 1) time step of time_integrators/RKDG/dirk.cpp, which is also IDC's
+ * prediction step (time_integrators/RKDG/idc.cpp:846-955). */
+int idc_adjoint_transient(idc_ctx *ctx, const double *psi0, const double *source, double dt, int64_t steps,
+                          const double *detector, int64_t checkpoint_every, double abs_tol, int32_t restart,
+                          int64_t max_its, int precision, double *dsigma_t, double *dsigma_s, double *dsource,
+                          double *dpsi0, double *J, int loc, int64_t *solves);
+
 /* ---- binary files ------------------------------------------------------------------------------------ */
 
 /* The reference's serial 2-D binary formats, on the halo layouts of this ABI (no GPU involved).

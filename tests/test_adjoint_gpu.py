@@ -149,3 +149,47 @@ def test_adjoint_rejects_unrefined_fp32():
         with pytest.raises(abi.IdcError) as e:
             ctx.sweep_adjoint(P.source, np.zeros(P.psi_shape()), P.dt, precision=abi.PREC_FP32)
         assert e.value.code == abi.IDC_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("p,sn", [(1, 4), (2, 8)])
+@pytest.mark.parametrize("prec,tol", [(abi.PREC_FP64, 1e-9), (abi.PREC_FP32_REFINED, 1e-8)])
+def test_transient_adjoint_matches_cpu_adjoint(restatement, p, sn, prec, tol):
+    """Implicit-Euler steps: the GPU's checkpointed backward adjoint (idc_adjoint_transient) against the CPU
+    FP64 transient adjoint on the restatement (tests/adjoint_ref.py), J included."""
+    from adjoint_ref import transient_gradient
+    P = lognormal(10, p, sn, seed=21 + p, median=2.0, log_sd=0.7, c_fixed=0.8, source="gaussian")
+    OP = to_oracle(P)
+    c = detector_window(P, cells=3)
+    rng = np.random.default_rng(6)
+    psi0 = np.zeros(P.psi_shape())
+    psi0[1:-1, 1:-1] = rng.uniform(0.0, 1.0, psi0[1:-1, 1:-1].shape)
+    dt, steps = 0.2, 4
+    J_ref, gt_ref, gs_ref, gq_ref, gp_ref = transient_gradient(restatement, OP, psi0, P.source.copy(), c, dt, steps)
+    gt, gs = np.zeros(P.sigma_t.shape), np.zeros(P.sigma_s.shape)
+    gq, gp = np.zeros(P.phi_shape()), np.zeros(P.psi_shape())
+    with context_for(P) as ctx:
+        J, solves = ctx.adjoint_transient(psi0, P.source, c, dt, steps, checkpoint_every=2, dsigma_t=gt,
+                                          dsigma_s=gs, dsource=gq, dpsi0=gp, abs_tol=1e-13, precision=prec)
+    assert solves == 3 * steps   # forward, recomputation (two segments of two), adjoint
+    assert abs(J - J_ref) <= tol * abs(J_ref)
+    gt, gs = gt.reshape(P.nx + 2, P.ny + 2), gs.reshape(P.nx + 2, P.ny + 2)
+    for got, want in ((gt, gt_ref), (gs, gs_ref), (gq, gq_ref), (gp, gp_ref)):
+        assert rel_err(got[1:-1, 1:-1], want[1:-1, 1:-1]) < tol
+
+
+def test_transient_adjoint_checkpoint_interval_is_bitwise_neutral():
+    """Recomputing the states from checkpoints reproduces the forward pass exactly, so every checkpoint
+    interval gives bitwise the same gradients."""
+    P = lognormal(24, 1, 8, seed=9, median=2.0, log_sd=0.7, c_fixed=0.9, source="gaussian")
+    c = detector_window(P, cells=4)
+    psi0 = np.zeros(P.psi_shape())
+    outs = []
+    with context_for(P) as ctx:
+        ctx.set_preconditioner(abi.PRECOND_DSA, 20)
+        for K in (1, 3, 7, 0):
+            gt, gq = np.zeros(P.sigma_t.shape), np.zeros(P.phi_shape())
+            J, _ = ctx.adjoint_transient(psi0, P.source, c, 0.1, 7, checkpoint_every=K, dsigma_t=gt, dsource=gq)
+            outs.append((J, gt, gq))
+    for J, gt, gq in outs[1:]:
+        assert J == outs[0][0]
+        assert np.array_equal(gt, outs[0][1]) and np.array_equal(gq, outs[0][2])

@@ -70,3 +70,52 @@ def test_oracle_adjoint_gradient_matches_central_differences(restatement):
             vals.append(functional(restatement, OP, forward(restatement, OP, s2, P.dt), c))
         fd = (vals[0] - vals[1]) / (2 * h)
         assert abs(fd - g_q[i, j, 0, 0]) <= 1e-6 * abs(g_q).max()
+
+
+def test_oracle_transient_adjoint_matches_central_differences(restatement):
+    """Implicit-Euler steps on the restatement: the backward adjoint gradients against central differences
+    of the forward time stepping (sigma_t, sigma_s, source moment, initial flux)."""
+    from adjoint_ref import forward_transient, transient_gradient
+    P = lognormal(6, 1, 4, seed=8, median=2.0, log_sd=0.7, c_fixed=0.8, source="gaussian")
+    OP = to_oracle(P)
+    c = detector_window(P, cells=2)
+    Q = P.source.reshape(OP.psi_shape()).copy()
+    rng = np.random.default_rng(4)
+    psi0 = np.zeros(OP.psi_shape())
+    psi0[1:-1, 1:-1] = rng.uniform(0.0, 1.0, psi0[1:-1, 1:-1].shape)
+    dt, steps = 0.2, 3
+    J, g_t, g_s, g_q, g_p = transient_gradient(restatement, OP, psi0, Q, c, dt, steps)
+
+    def J_of(psi0_, Q_):
+        return functional(restatement, OP, forward_transient(restatement, OP, psi0_, Q_, dt, steps)[-1], c)
+
+    assert abs(J_of(psi0, Q) - J) <= 1e-13 * abs(J)
+    st0, ss0 = OP.sigma_t.copy(), OP.sigma_s.copy()
+    for i, j in ((2, 3), (5, 1), (4, 6)):
+        k = i * (P.ny + 2) + j
+        for arr, g in ((st0, g_t), (ss0, g_s)):
+            h = 1e-4 * arr[k]
+            vals = []
+            for sgn in (1, -1):
+                pert = arr.copy()
+                pert[k] += sgn * h
+                if arr is st0:
+                    OP.sigma_t = pert
+                else:
+                    OP.sigma_s = pert
+                vals.append(J_of(psi0, Q))
+            OP.sigma_t, OP.sigma_s = st0.copy(), ss0.copy()
+            assert abs((vals[0] - vals[1]) / (2 * h) - g[i, j]) <= 1e-6 * abs(g).max()
+        h = 1e-3
+        vals = []
+        for sgn in (1, -1):
+            Q2 = Q.copy()
+            Q2[i, j, :, 0, 0] += sgn * h / (4 * np.pi)
+            vals.append(J_of(psi0, Q2))
+        assert abs((vals[0] - vals[1]) / (2 * h) - g_q[i, j, 0, 0]) <= 1e-6 * abs(g_q).max()
+        vals = []
+        for sgn in (1, -1):
+            p2 = psi0.copy()
+            p2[i, j, 3, 1, 0] += sgn * h
+            vals.append(J_of(p2, Q))
+        assert abs((vals[0] - vals[1]) / (2 * h) - g_p[i, j, 3, 1, 0]) <= 1e-6 * abs(g_p).max()
