@@ -270,6 +270,40 @@ def extra_adjoint(abi, torch, dev):
     return out
 
 
+def extra_adjoint_transient(abi, torch, dev, steps=10, dt=0.5, every=0):
+    """The same 128x128 Q1 S8 problem, time dependent: gradients of the detector response after 10
+    implicit-Euler steps of dt = 0.5 from zero flux with respect to all per-cell sigma_t, sigma_s, source
+    moments (and the initial angular flux), by the checkpointed backward adjoint (states every ~sqrt(10)
+    steps, recomputed per segment).  grads_per_s counts the 3 nx ny per-cell parameters, as the steady line."""
+    from idcsweep.problems import detector_window, lognormal
+    P = lognormal(128, 1, 8, seed=0, median=2.0, log_sd=0.7, c_fixed=0.9, source="gaussian")
+    d = f"cuda:{dev}"
+    c_det = torch.from_numpy(detector_window(P, cells=16)).to(d)
+    src = torch.from_numpy(P.source).to(d)
+    psi0 = torch.zeros_like(src)
+    out = {"workload": f"128x128 Q1 S8 as the adjoint line, {steps} implicit-Euler steps of dt {dt} from zero "
+                       "flux; GMRES(30) + DSA (20 CG steps) forward and adjoint, abs tol 1e-12",
+           "gradient_entries": 3 * P.nx * P.ny, "initial_flux_entries": int(np.prod(P.psi_shape()))}
+    with _ctx_for(abi, P, dev) as c:
+        c.set_preconditioner(abi.PRECOND_DSA, 20)
+        g_t = torch.zeros((P.nx + 2) * (P.ny + 2), dtype=torch.float64, device=d)
+        g_s = torch.zeros_like(g_t)
+        g_q = torch.zeros(P.phi_shape(), dtype=torch.float64, device=d)
+        g_p = torch.zeros_like(src)
+        args = (psi0.data_ptr(), src.data_ptr(), c_det.data_ptr(), dt, steps)
+        kw = dict(checkpoint_every=every, dsigma_t=g_t.data_ptr(), dsigma_s=g_s.data_ptr(), dsource=g_q.data_ptr(),
+                  dpsi0=g_p.data_ptr(), abs_tol=1e-12, loc=abi.LOC_DEVICE)
+        c.adjoint_transient(*args, **kw)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        J, solves = c.adjoint_transient(*args, **kw)
+        torch.cuda.synchronize()
+        sec = time.perf_counter() - t0
+        out["fp64"] = {"grads_per_s": out["gradient_entries"] / sec, "ms": sec * 1e3, "gmres_solves": solves,
+                       "J": J}
+    return out
+
+
 def extra_batched(abi, torch, dev, n_problems=64):
     """64 independent steady problems: side U{32,...,384}, S4/S8/S12/S16, Q1/Q2, log-normal sigma_t (median 1,
     log-sd 1), c U[0.3, 0.99] (seeded); one sweep of every problem, batched (one launch per DG degree,
@@ -467,8 +501,7 @@ def run_ours(args):
     }
 
     if not args.no_extras and world == 1:
-        for key, fn in (("gmres_dsa", extra_gmres_dsa), ("idc", extra_idc), ("adjoint", extra_adjoint),
-                        ("batched", extra_batched)):
+        for key, fn in EXTRAS.items():
             try:
                 line[key] = fn(abi, torch, dev)
             except Exception as e:   # reported, never fatal for the headline line
@@ -493,6 +526,19 @@ def run_ours(args):
     return 0
 
 
+EXTRAS = {"gmres_dsa": extra_gmres_dsa, "idc": extra_idc, "adjoint": extra_adjoint,
+          "adjoint_transient": extra_adjoint_transient, "batched": extra_batched}
+
+
+def run_only_extra(name):
+    """One of the other configurations alone (profiling runs: its launch list without the headline's)."""
+    import torch
+    from idcsweep import abi
+    abi.load_library()
+    print(json.dumps({name: EXTRAS[name](abi, torch, 0)}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -506,7 +552,11 @@ def main():
                     help="default tile shapes, no tuning launches (profiling runs)")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the other configurations (GMRES+DSA, IDC, adjoint, batched) measured beside the headline")
+    ap.add_argument("--only-extra", choices=tuple(EXTRAS), default=None,
+                    help="run one of the other configurations alone and print its JSON (profiling runs)")
     args = ap.parse_args()
+    if args.only_extra:
+        return run_only_extra(args.only_extra)
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_ours(args)
