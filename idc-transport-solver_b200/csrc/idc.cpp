@@ -146,7 +146,7 @@ Status Context::idc_integrate(double *psi, const double *Q, double dt, int64_t s
     // buffers: M stages, M residuals, one source (psi-sized); M moments, M previous-level moments, one
     // scattering combination (moment-sized)
     const size_t np = psi_len(), nm = phi_len();
-    const int need_psi = 2 * M + 1, need_phi = 2 * M + 1;
+    const int need_psi = 2 * M + 1, need_phi = 3 * M + 1;
     IDC_TRY_CUDA(cudaSetDevice(device));
     while ((int)idc_psi_.size() < need_psi) {
         double *p = nullptr;
@@ -165,6 +165,7 @@ Status Context::idc_integrate(double *psi, const double *Q, double dt, int64_t s
     auto phi = [&](int l) { return idc_phi_[l]; };
     auto phi_old = [&](int l) { return idc_phi_[M + l]; };
     double *phi_s = idc_phi_[2 * M];
+    auto scat = [&](int l) { return idc_phi_[2 * M + 1 + l]; };   // sigma_s phi_l / (4 pi)
     int64_t sweeps = 0;
 
     auto residual = [&](int l) -> Status {   // res_l = (L - S P) psi_l  (ComputeResiduals, idc.cpp:1657-1667)
@@ -199,14 +200,41 @@ Status Context::idc_integrate(double *psi, const double *Q, double dt, int64_t s
             IDC_TRY(sweep(src, stage(n), h * dt, phi(n), precision, phi(n - 1), 1.0));
             ++sweeps;
         }
+        const bool fused = M <= kIdcFusedMaxNodes;
         for (int p = 0; p < K; ++p) {
+            if (fused) {   // every substep's residual terms in one pass over the stages (into res(1 .. M-1))
+                IdcCorr cr{};
+                for (int l = 0; l < M; ++l) {
+                    IDC_TRY_CUDA(launch_scatter_moments(dims(), d_sigma_s, phi(l), scat(l), stream));
+                    cr.stage[l] = stage(l);
+                    cr.scat[l] = scat(l);
+                }
+                for (int n = 1; n < M; ++n) {
+                    cr.out[n] = res(n);
+                    const double h = t[n] - t[n - 1];
+                    for (int l = 0; l < M; ++l) cr.c[n][l] = (n == l ? 1.0 : 0.0) - W[(size_t)n * M + l] / h;
+                }
+                IDC_TRY_CUDA(launch_idc_corrections(dims(), M, cr, d_sigma_t, d_xi, d_eta, stream));
+                launches += M + 1;
+            }
             for (int l = 0; l < M; ++l) {
-                IDC_TRY(transport_residual(stage(l), phi(l), res(l)));
+                if (!fused) IDC_TRY(transport_residual(stage(l), phi(l), res(l)));
                 IDC_TRY_CUDA(cudaMemcpyAsync(phi_old(l), phi(l), sizeof(double) * nm, cudaMemcpyDeviceToDevice, stream));
             }
             for (int n = 1; n < M; ++n) {
                 const double h = t[n] - t[n - 1];
-                IDC_TRY(source(n, true, true));
+                if (fused) {   // src_n = psi_{n-1} / (h dt) + Q + (the residual terms)
+                    IdcTerms tm{};
+                    tm.n = 2;
+                    tm.a[0] = stage(n - 1);
+                    tm.c[0] = 1.0 / (h * dt);
+                    tm.a[1] = res(n);
+                    tm.c[1] = 1.0;
+                    IDC_TRY_CUDA(launch_idc_source(dims(), tm, Q, src, stream));
+                    launches += 1;
+                } else {
+                    IDC_TRY(source(n, true, true));
+                }
                 IDC_TRY_CUDA(launch_phi_combine(nm, phi(n - 1), phi_old(n - 1), phi_old(n), phi_s, stream));
                 launches += 1;
                 IDC_TRY(sweep(src, stage(n), h * dt, phi(n), precision, phi_s, 1.0));

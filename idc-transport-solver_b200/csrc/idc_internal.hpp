@@ -163,6 +163,18 @@ struct IdcTerms {
     double c[kMax];
 };
 cudaError_t launch_idc_source(const GridDims &g, const IdcTerms &t, const double *Q, double *out, cudaStream_t s);
+// The residual terms of one IDC correction level's sources: out[n] = sum_l c[n][l] (L - S P) stage[l] on
+// interior cells, n = 1 .. M-1, for M nodes (2 .. kIdcFusedMaxNodes); scat[l] = sigma_s P stage[l] / (4 pi)
+// per cell (launch_scatter_moments)
+constexpr int kIdcFusedMaxNodes = 5;
+struct IdcCorr {
+    const double *stage[kIdcFusedMaxNodes];
+    const double *scat[kIdcFusedMaxNodes];
+    double *out[kIdcFusedMaxNodes];
+    double c[kIdcFusedMaxNodes][kIdcFusedMaxNodes];
+};
+cudaError_t launch_idc_corrections(const GridDims &g, int M, const IdcCorr &t, const double *sigma_t, const double *xi,
+                                   const double *eta, cudaStream_t s);
 cudaError_t launch_phi_combine(size_t n, const double *a, const double *b, const double *c, double *out, cudaStream_t s);
 // DSA preconditioner (dsa_kernels.cu): workspace size, coefficient setup from the cross sections, and
 // out = v + C^{-1}(sigma_s v_00) on the (0,0) moment by cg_steps Jacobi-PCG steps (out may alias v): one

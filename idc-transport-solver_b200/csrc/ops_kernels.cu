@@ -63,6 +63,61 @@ __global__ void smv_kernel(GridDims g, double alpha, double beta, const double *
 // sigma).  One thread per (interior cell, ordinate).  With phi_sc, the scattering term of Smv is added in
 // the same pass, y += (sigma_s phi_sc / (4 pi)) gamma, rounded as Lmv followed by Smv(gamma, 1) would
 // round it (the IDC residual (L - S P) psi in one pass over psi).
+// (Omega.grad + sigma_t) x at one interior (cell, ordinate): TransportOperator::Lmv, :1215-1480 (piecewise
+// constant sigma), with x's dofs of the cell at x + base and its upwind neighbours' at +-istride, +-plane.
+template <int P>
+__device__ __forceinline__ void lmv_point(const GridDims &g, const double *__restrict__ x, size_t base, size_t istride,
+                                          size_t plane, double xi, double eta, double s, double (&x3)[P * P]) {
+    constexpr int N = P * P;
+    const bool xneg = xi <= 0.0, yneg = eta <= 0.0;
+    const double *X0 = x + base;
+    const double *X1 = x + base + (xneg ? (ptrdiff_t)istride : -(ptrdiff_t)istride);
+    const double *X2 = x + base + (yneg ? (ptrdiff_t)plane : -(ptrdiff_t)plane);
+    double x0[N], x1[N], x2[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        x0[k] = X0[k];
+        x1[k] = X1[k];
+        x2[k] = X2[k];
+    }
+#pragma unroll
+    for (int k = 0; k < N; ++k) x3[k] = s * x0[k];
+    double cv = xi / g.dx;
+#pragma unroll
+    for (int d = 0; d < P; ++d)
+#pragma unroll
+        for (int a = 0; a < P; ++a)
+#pragma unroll
+            for (int e = 0; e < P; ++e) {
+                const double f = xneg ? (neg1pow(a) * x1[e + P * a] + neg1pow(d + a + 1) * x0[e + P * a])
+                                      : (x0[e + P * a] + neg1pow(d + 1) * x1[e + P * a]);
+                x3[e + P * d] += cv * double(2 * d + 1) * f;
+            }
+#pragma unroll
+    for (int d = 0; d < P; ++d)
+#pragma unroll
+        for (int a = d - 1; a >= 0; a -= 2)
+#pragma unroll
+            for (int e = 0; e < P; ++e) x3[e + P * d] -= double(2 * (2 * d + 1)) * cv * x0[e + P * a];
+    cv = eta / g.dy;
+#pragma unroll
+    for (int d = 0; d < P; ++d)
+#pragma unroll
+        for (int e = 0; e < P; ++e)
+#pragma unroll
+            for (int b = 0; b < P; ++b) {
+                const double f = yneg ? (neg1pow(b) * x2[b + P * d] + neg1pow(e + b + 1) * x0[b + P * d])
+                                      : (x0[b + P * d] + neg1pow(e + 1) * x2[b + P * d]);
+                x3[e + P * d] += cv * double(2 * e + 1) * f;
+            }
+#pragma unroll
+    for (int d = 0; d < P; ++d)
+#pragma unroll
+        for (int e = 0; e < P; ++e)
+#pragma unroll
+            for (int b = e - 1; b >= 0; b -= 2) x3[e + P * d] -= double(2 * (2 * e + 1)) * cv * x0[b + P * d];
+}
+
 template <int P, typename IDX>
 __global__ void lmv_kernel(GridDims g, double alpha, double beta, const double *__restrict__ sigma_t,
                            const double *__restrict__ xi_a, const double *__restrict__ eta_a,
@@ -77,55 +132,9 @@ __global__ void lmv_kernel(GridDims g, double alpha, double beta, const double *
         const int q = (int)(t - cell * (IDX)g.nq);
         const int i = 1 + (int)(cell / (IDX)g.ny), j = 1 + (int)(cell - (cell / (IDX)g.ny) * (IDX)g.ny);
         const double xi = xi_a[q], eta = eta_a[q];
-        const bool xneg = xi <= 0.0, yneg = eta <= 0.0;
         const size_t base = (size_t)i * istride + (size_t)j * plane + (size_t)q * N;
-        const double *X0 = x + base;
-        const double *X1 = x + base + (xneg ? (ptrdiff_t)istride : -(ptrdiff_t)istride);
-        const double *X2 = x + base + (yneg ? (ptrdiff_t)plane : -(ptrdiff_t)plane);
-        double x0[N], x1[N], x2[N], x3[N];
-#pragma unroll
-        for (int k = 0; k < N; ++k) {
-            x0[k] = X0[k];
-            x1[k] = X1[k];
-            x2[k] = X2[k];
-        }
-        const double s = sigma_t[(size_t)i * (g.ny + 2) + j];
-#pragma unroll
-        for (int k = 0; k < N; ++k) x3[k] = s * x0[k];
-        double cv = xi / g.dx;
-#pragma unroll
-        for (int d = 0; d < P; ++d)
-#pragma unroll
-            for (int a = 0; a < P; ++a)
-#pragma unroll
-                for (int e = 0; e < P; ++e) {
-                    const double f = xneg ? (neg1pow(a) * x1[e + P * a] + neg1pow(d + a + 1) * x0[e + P * a])
-                                          : (x0[e + P * a] + neg1pow(d + 1) * x1[e + P * a]);
-                    x3[e + P * d] += cv * double(2 * d + 1) * f;
-                }
-#pragma unroll
-        for (int d = 0; d < P; ++d)
-#pragma unroll
-            for (int a = d - 1; a >= 0; a -= 2)
-#pragma unroll
-                for (int e = 0; e < P; ++e) x3[e + P * d] -= double(2 * (2 * d + 1)) * cv * x0[e + P * a];
-        cv = eta / g.dy;
-#pragma unroll
-        for (int d = 0; d < P; ++d)
-#pragma unroll
-            for (int e = 0; e < P; ++e)
-#pragma unroll
-                for (int b = 0; b < P; ++b) {
-                    const double f = yneg ? (neg1pow(b) * x2[b + P * d] + neg1pow(e + b + 1) * x0[b + P * d])
-                                          : (x0[b + P * d] + neg1pow(e + 1) * x2[b + P * d]);
-                    x3[e + P * d] += cv * double(2 * e + 1) * f;
-                }
-#pragma unroll
-        for (int d = 0; d < P; ++d)
-#pragma unroll
-            for (int e = 0; e < P; ++e)
-#pragma unroll
-                for (int b = e - 1; b >= 0; b -= 2) x3[e + P * d] -= double(2 * (2 * e + 1)) * cv * x0[b + P * d];
+        double x3[N];
+        lmv_point<P>(g, x, base, istride, plane, xi, eta, sigma_t[(size_t)i * (g.ny + 2) + j], x3);
         double *Y = y + base;
         if (!phi_sc) {
 #pragma unroll
@@ -140,6 +149,54 @@ __global__ void lmv_kernel(GridDims g, double alpha, double beta, const double *
             }
         }
     }
+}
+
+// The residual part of every IDC correction source of one correction level, in one pass over the stages:
+//     out_n = sum_l c[n][l] res_l,   res_l = (L - S P) psi_l = Lmv(psi_l) - scat_l,
+// scat_l = sigma_s phi_l / (4 pi) per cell (scatter_moments_kernel), n = 1 .. M-1, l = 0 .. M-1
+// (IDCIntegrator::ComputeResiduals / ComputeSource, time_integrators/RKDG/idc.cpp:1657-1740), each res_l
+// rounded as Lmv followed by Smv rounds it.  The residuals are never stored: a level reads its M stages once
+// (neighbours from L2) and writes M-1 arrays, where stored residuals cost M reads and M writes, then M reads
+// per source.  Interior cells only.  (At most 128 registers for P <= 2, two blocks per SM: the loads of a
+// stage wait on the previous stage's arithmetic, so bandwidth comes from resident warps.)
+template <int P, int M, typename IDX>
+__global__ void __launch_bounds__(kThreads, P <= 2 ? 2 : 1)
+    idc_corr_kernel(GridDims g, IdcCorr t, const double *__restrict__ sigma_t, const double *__restrict__ xi_a,
+                    const double *__restrict__ eta_a) {
+    constexpr int N = P * P;
+    const size_t plane = (size_t)g.nq * N;
+    const size_t istride = (size_t)(g.ny + 2) * plane;
+    const IDX total = (IDX)g.nx * g.ny * g.nq;
+    const IDX e = blockIdx.x * (IDX)blockDim.x + threadIdx.x;
+    if (e >= total) return;
+    const IDX cell = e / (IDX)g.nq;
+    const int q = (int)(e - cell * (IDX)g.nq);
+    const int i = 1 + (int)(cell / (IDX)g.ny), j = 1 + (int)(cell - (cell / (IDX)g.ny) * (IDX)g.ny);
+    const double xi = xi_a[q], eta = eta_a[q];
+    const size_t cidx = (size_t)i * (g.ny + 2) + j;
+    const size_t base = (size_t)i * istride + (size_t)j * plane + (size_t)q * N;
+    const double st = sigma_t[cidx];
+    double acc[M - 1][N];
+#pragma unroll
+    for (int n = 0; n < M - 1; ++n)
+#pragma unroll
+        for (int k = 0; k < N; ++k) acc[n][k] = 0.0;
+#pragma unroll
+    for (int l = 0; l < M; ++l) {
+        double x3[N];
+        lmv_point<P>(g, t.stage[l], base, istride, plane, xi, eta, st, x3);
+        const double *sm = t.scat[l] + cidx * N;
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            const double r = __dadd_rn(__dmul_rn(1.0, x3[k]), sm[k] * -1.0);
+#pragma unroll
+            for (int n = 0; n < M - 1; ++n) acc[n][k] = fma(t.c[n + 1][l], r, acc[n][k]);
+        }
+    }
+#pragma unroll
+    for (int n = 0; n < M - 1; ++n)
+#pragma unroll
+        for (int k = 0; k < N; ++k) t.out[n + 1][base + k] = acc[n][k];
 }
 
 // out = sigma_s phi / (4 pi) on interior cells, rounded as TransportOperator::Smv rounds its scattering term
@@ -468,6 +525,42 @@ cudaError_t launch_adjoint_gradient(const GridDims &g, const double *psi, const 
     adjoint_gradient_kernel<<<blocks_for(warps * 32), kThreads, 0, s>>>(g, psi, lam, phi, Lam, dsig_t, dsig_s, dq,
                                                                         accumulate ? 1 : 0);
     return cudaGetLastError();
+}
+
+template <int P, int M>
+static void idc_corr_pm(const GridDims &g, const IdcCorr &t, const double *sigma_t, const double *xi, const double *eta,
+                        cudaStream_t s) {
+    // one thread per element and no grid stride: blocks run in index order, so the resident ones cover a
+    // contiguous front of cell rows and an x-neighbour row is still in L2 when it is read again
+    const size_t n = (size_t)g.nx * g.ny * g.nq;
+    const size_t blocks = (n + kThreads - 1) / kThreads;
+    if (n < (size_t)INT32_MAX)
+        idc_corr_kernel<P, M, int32_t><<<(unsigned)blocks, kThreads, 0, s>>>(g, t, sigma_t, xi, eta);
+    else
+        idc_corr_kernel<P, M, size_t><<<(unsigned)blocks, kThreads, 0, s>>>(g, t, sigma_t, xi, eta);
+}
+
+template <int P>
+static cudaError_t idc_corr_p(const GridDims &g, int M, const IdcCorr &t, const double *sigma_t, const double *xi,
+                              const double *eta, cudaStream_t s) {
+    switch (M) {
+        case 2: idc_corr_pm<P, 2>(g, t, sigma_t, xi, eta, s); break;
+        case 3: idc_corr_pm<P, 3>(g, t, sigma_t, xi, eta, s); break;
+        case 4: idc_corr_pm<P, 4>(g, t, sigma_t, xi, eta, s); break;
+        case 5: idc_corr_pm<P, 5>(g, t, sigma_t, xi, eta, s); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_idc_corrections(const GridDims &g, int M, const IdcCorr &t, const double *sigma_t, const double *xi,
+                                   const double *eta, cudaStream_t s) {
+    switch (g.P) {
+        case 1: return idc_corr_p<1>(g, M, t, sigma_t, xi, eta, s);
+        case 2: return idc_corr_p<2>(g, M, t, sigma_t, xi, eta, s);
+        case 3: return idc_corr_p<3>(g, M, t, sigma_t, xi, eta, s);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 cudaError_t launch_idc_source(const GridDims &g, const IdcTerms &t, const double *Q, double *out, cudaStream_t s) {
