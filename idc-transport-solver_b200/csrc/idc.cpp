@@ -204,6 +204,7 @@ Status Context::idc_integrate(double *psi, const double *Q, double dt, int64_t s
         for (int p = 0; p < K; ++p) {
             if (fused) {   // every substep's residual terms in one pass over the stages (into res(1 .. M-1))
                 IdcCorr cr{};
+                cr.Q = Q;
                 for (int l = 0; l < M; ++l) {
                     IDC_TRY_CUDA(launch_scatter_moments(dims(), d_sigma_s, phi(l), scat(l), stream));
                     cr.stage[l] = stage(l);
@@ -223,14 +224,12 @@ Status Context::idc_integrate(double *psi, const double *Q, double dt, int64_t s
             }
             for (int n = 1; n < M; ++n) {
                 const double h = t[n] - t[n - 1];
-                if (fused) {   // src_n = psi_{n-1} / (h dt) + Q + (the residual terms)
+                if (fused) {   // src_n = (Q + the residual terms, with Q's ghost cells) + psi_{n-1} / (h dt)
                     IdcTerms tm{};
-                    tm.n = 2;
+                    tm.n = 1;
                     tm.a[0] = stage(n - 1);
                     tm.c[0] = 1.0 / (h * dt);
-                    tm.a[1] = res(n);
-                    tm.c[1] = 1.0;
-                    IDC_TRY_CUDA(launch_idc_source(dims(), tm, Q, src, stream));
+                    IDC_TRY_CUDA(launch_idc_source(dims(), tm, res(n), src, stream));
                     launches += 1;
                 } else {
                     IDC_TRY(source(n, true, true));
@@ -250,6 +249,11 @@ Status Context::idc_integrate(double *psi, const double *Q, double dt, int64_t s
     IDC_TRY_CUDA(cudaMemcpyAsync(stage(0), psi, sizeof(double) * np, cudaMemcpyDeviceToDevice, stream));
     for (int l = 1; l < M; ++l)
         IDC_TRY_CUDA(cudaMemcpyAsync(stage(l), Q, sizeof(double) * np, cudaMemcpyDeviceToDevice, stream));
+    // the fused IMEX corrections write interior cells of res(1 .. M-1) only: their ghost cells hold Q's (the
+    // inflow), which the substep sources copy
+    if (scattering == 0 && M <= kIdcFusedMaxNodes)
+        for (int l = 1; l < M; ++l)
+            IDC_TRY_CUDA(cudaMemcpyAsync(res(l), Q, sizeof(double) * np, cudaMemcpyDeviceToDevice, stream));
     if (scattering == 0) {
         if (use_graph && steps > 0) {
             // first step uncaptured (builds the sweep schedule, allocates nothing inside the capture), then

@@ -163,11 +163,12 @@ struct IdcTerms {
     double c[kMax];
 };
 cudaError_t launch_idc_source(const GridDims &g, const IdcTerms &t, const double *Q, double *out, cudaStream_t s);
-// The residual terms of one IDC correction level's sources: out[n] = sum_l c[n][l] (L - S P) stage[l] on
-// interior cells, n = 1 .. M-1, for M nodes (2 .. kIdcFusedMaxNodes); scat[l] = sigma_s P stage[l] / (4 pi)
-// per cell (launch_scatter_moments)
+// One IDC correction level's sources but their psi_{n-1} / (h dt) terms: out[n] = Q + sum_l c[n][l] (L - S P)
+// stage[l] on interior cells, n = 1 .. M-1, for M nodes (2 .. kIdcFusedMaxNodes); scat[l] =
+// sigma_s P stage[l] / (4 pi) per cell (launch_scatter_moments)
 constexpr int kIdcFusedMaxNodes = 5;
 struct IdcCorr {
+    const double *Q;
     const double *stage[kIdcFusedMaxNodes];
     const double *scat[kIdcFusedMaxNodes];
     double *out[kIdcFusedMaxNodes];

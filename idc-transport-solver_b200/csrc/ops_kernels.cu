@@ -151,8 +151,9 @@ __global__ void lmv_kernel(GridDims g, double alpha, double beta, const double *
     }
 }
 
-// The residual part of every IDC correction source of one correction level, in one pass over the stages:
-//     out_n = sum_l c[n][l] res_l,   res_l = (L - S P) psi_l = Lmv(psi_l) - scat_l,
+// Every IDC correction source of one correction level but its psi_{n-1} / (h dt) term, in one pass over the
+// stages:
+//     out_n = Q + sum_l c[n][l] res_l,   res_l = (L - S P) psi_l = Lmv(psi_l) - scat_l,
 // scat_l = sigma_s phi_l / (4 pi) per cell (scatter_moments_kernel), n = 1 .. M-1, l = 0 .. M-1
 // (IDCIntegrator::ComputeResiduals / ComputeSource, time_integrators/RKDG/idc.cpp:1657-1740), each res_l
 // rounded as Lmv followed by Smv rounds it.  The residuals are never stored: a level reads its M stages once
@@ -177,10 +178,13 @@ __global__ void __launch_bounds__(kThreads, P <= 2 ? 2 : 1)
     const size_t base = (size_t)i * istride + (size_t)j * plane + (size_t)q * N;
     const double st = sigma_t[cidx];
     double acc[M - 1][N];
+    double q0[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) q0[k] = t.Q[base + k];
 #pragma unroll
     for (int n = 0; n < M - 1; ++n)
 #pragma unroll
-        for (int k = 0; k < N; ++k) acc[n][k] = 0.0;
+        for (int k = 0; k < N; ++k) acc[n][k] = q0[k];
 #pragma unroll
     for (int l = 0; l < M; ++l) {
         double x3[N];
