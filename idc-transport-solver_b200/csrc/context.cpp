@@ -56,6 +56,7 @@ Context::~Context() {
     cudaFree(d_trace);
     cudaFree(d_inflow);
     cudaFree(d_scat);
+    cudaFree(d_src2mix);
     cudaFree(d_krylov);
     cudaFree(d_small);
     cudaFree(d_dsa_ws);
@@ -432,7 +433,8 @@ Status Context::check_device_error() {
 }
 
 Status Context::sweep(const double *src, double *out, double dt, double *phi, int precision,
-                      const double *phi_scatter, double scatter_scale, bool adjoint) {
+                      const double *phi_scatter, double scatter_scale, bool adjoint, const double *src2,
+                      double src2_scale) {
     if (!have_ordinates) return bad(IDC_ERR_STATE, "sweep before idc_set_ordinates");
     if (!have_sigma) return bad(IDC_ERR_STATE, "sweep before idc_set_sigma");
     if (precision < 0 || precision > 2) return bad(IDC_ERR_ARG, "unknown precision");
@@ -441,11 +443,41 @@ Status Context::sweep(const double *src, double *out, double dt, double *phi, in
         return bad(IDC_ERR_UNSUPPORTED, "a sweep without source or output array needs the warp-pipelined kernel");
     if (adjoint && (kernel != kModal || precision == IDC_PREC_FP32))
         return bad(IDC_ERR_UNSUPPORTED, "the transposed sweep needs the modal kernel in FP64 or refined precision");
+    if (src2 && (adjoint || kernel != kModal || !src))
+        return bad(IDC_ERR_UNSUPPORTED, "a second source needs a forward modal sweep with a first source");
     IDC_TRY(build_schedule(precision));
     IDC_TRY_CUDA(cudaSetDevice(device));
 
+    size_t launch_smem = smem;
+    if (src2) {
+        int limit = 0;
+        IDC_TRY_CUDA(cudaDeviceGetAttribute(&limit, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+        if (precision != IDC_PREC_FP32 && smem + sweep_modal_src2_bytes(P, wn) <= (size_t)limit) {
+            launch_smem = smem + sweep_modal_src2_bytes(P, wn);
+        } else {   // no in-sweep variant for this precision, or its stages do not fit: combine first
+            if (src2mix_len < psi_len()) {
+                if (capturing) return bad(IDC_ERR_STATE, "source buffer allocation inside a stream capture");
+                cudaFree(d_src2mix);
+                d_src2mix = nullptr;
+                src2mix_len = 0;
+                IDC_TRY_CUDA(cudaMalloc(&d_src2mix, sizeof(double) * psi_len()));
+                src2mix_len = psi_len();
+            }
+            IdcTerms tm{};
+            tm.n = 1;
+            tm.a[0] = src2;
+            tm.c[0] = src2_scale;
+            IDC_TRY_CUDA(launch_idc_source(dims(), tm, src, d_src2mix, stream));
+            launches += 1;
+            src = d_src2mix;
+            src2 = nullptr;
+        }
+    }
+
     SweepArgs a{};
     a.src = src;
+    a.src2 = src2;
+    a.src2_scale = src2_scale;
     a.out = out;
     a.sigma_t = d_sigma_t;
     a.sigma_s = d_sigma_s;
@@ -527,7 +559,7 @@ Status Context::sweep(const double *src, double *out, double dt, double *phi, in
             a.sigma_s = nullptr;
         }
         if (!capturing) IDC_TRY_CUDA(cudaEventRecord(ev0, stream));   // the timing covers the sweep kernel alone
-        IDC_TRY_CUDA(launch_sweep_modal(P, precision, a, grid, smem, stream));
+        IDC_TRY_CUDA(launch_sweep_modal(P, precision, a, grid, launch_smem, stream));
     } else if (kernel == kWarp)
         IDC_TRY_CUDA(launch_sweep_warp(P, precision, a, grid, smem, stream));
     else

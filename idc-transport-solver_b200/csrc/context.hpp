@@ -39,8 +39,11 @@ public:
 
     // ---- operators on device pointers ----
     // Sweep: out <- L^{-1} (src [+ scale * S phi_scatter]); phi (nullable) <- P out.  src may equal out.
+    // src2 (modal kernel, forward): the source is src + src2_scale * src2 on interior cells, combined by the
+    // sweep's aux warps (or, when its stages do not fit in shared memory, by a kernel into a scratch array)
     Status sweep(const double *src, double *out, double dt, double *phi, int precision,
-                 const double *phi_scatter = nullptr, double scatter_scale = 1.0, bool adjoint = false);
+                 const double *phi_scatter = nullptr, double scatter_scale = 1.0, bool adjoint = false,
+                 const double *src2 = nullptr, double src2_scale = 0.0);
     // count out-of-place sweeps of HOST arrays (srcs[k] -> outs[k] interior cells, phis[k] if phis), the
     // upload of step k+1, the sweep of step k and the download of step k-1 overlapped on three streams
     // with double-buffered device arrays
@@ -132,6 +135,8 @@ public:
     size_t inflow_len = 0;
     double *d_scat = nullptr;      // modal kernel: the fused scattering source's moments sigma_s phi / (4 pi)
     size_t scat_len = 0;
+    double *d_src2mix = nullptr;   // src + scale src2 when the second source's stages do not fit
+    size_t src2mix_len = 0;
     size_t trace_len = 0;
     int items_per_rb = 0;          // work items per row block (= ordinate chunks over all quadrants)
     double *d_phi_part = nullptr;  // warp kernel: per-chunk partial moments

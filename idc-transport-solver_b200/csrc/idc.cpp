@@ -194,10 +194,9 @@ Status Context::idc_integrate(double *psi, const double *Q, double dt, int64_t s
     // one IMEX step: only stream work, so it can be captured
     auto imex_step = [&]() -> Status {
         IDC_TRY(pmv(1.0, 0.0, stage(0), phi(0)));
-        for (int n = 1; n < M; ++n) {   // prediction: IMEX Euler
+        for (int n = 1; n < M; ++n) {   // prediction: IMEX Euler, source Q + psi_{n-1} / (h dt) formed in the sweep
             const double h = t[n] - t[n - 1];
-            IDC_TRY(source(n, false, true));
-            IDC_TRY(sweep(src, stage(n), h * dt, phi(n), precision, phi(n - 1), 1.0));
+            IDC_TRY(sweep(Q, stage(n), h * dt, phi(n), precision, phi(n - 1), 1.0, false, stage(n - 1), 1.0 / (h * dt)));
             ++sweeps;
         }
         const bool fused = M <= kIdcFusedMaxNodes;
@@ -224,19 +223,14 @@ Status Context::idc_integrate(double *psi, const double *Q, double dt, int64_t s
             }
             for (int n = 1; n < M; ++n) {
                 const double h = t[n] - t[n - 1];
-                if (fused) {   // src_n = (Q + the residual terms, with Q's ghost cells) + psi_{n-1} / (h dt)
-                    IdcTerms tm{};
-                    tm.n = 1;
-                    tm.a[0] = stage(n - 1);
-                    tm.c[0] = 1.0 / (h * dt);
-                    IDC_TRY_CUDA(launch_idc_source(dims(), tm, res(n), src, stream));
-                    launches += 1;
-                } else {
-                    IDC_TRY(source(n, true, true));
-                }
+                if (!fused) IDC_TRY(source(n, true, true));
                 IDC_TRY_CUDA(launch_phi_combine(nm, phi(n - 1), phi_old(n - 1), phi_old(n), phi_s, stream));
                 launches += 1;
-                IDC_TRY(sweep(src, stage(n), h * dt, phi(n), precision, phi_s, 1.0));
+                if (fused)   // src_n = (Q + the residual terms, with Q's ghost cells) + psi_{n-1} / (h dt)
+                    IDC_TRY(sweep(res(n), stage(n), h * dt, phi(n), precision, phi_s, 1.0, false, stage(n - 1),
+                                  1.0 / (h * dt)));
+                else
+                    IDC_TRY(sweep(src, stage(n), h * dt, phi(n), precision, phi_s, 1.0));
                 ++sweeps;
             }
         }

@@ -33,6 +33,8 @@ struct SweepItem {
 struct SweepArgs {
     const double *src;         // angular source (read); ghost cells carry the inflow values.  Warp and modal
                                // kernels: null means zero source and vacuum inflow
+    const double *src2;        // modal forward sweep: a second angular source added to src as
+    double src2_scale;         // fma(src2_scale, src2, src) on interior cells (null: none)
     const double *inflow;      // modal kernel: inflow traces of the ghost cells [nx + ny][nq][P], or null
     double *out;               // psi (written); may equal src (in-place sweep).  Warp kernel: null = not stored
     const double *sigma_t;     // (nx+2)(ny+2), piecewise constant
@@ -101,6 +103,8 @@ cudaError_t launch_batched_helpers(int P, bool modal_inflow, const SweepArgs *ta
                                    bool reduce, cudaStream_t stream);
 cudaError_t sweep_modal_occupancy(int P, int precision, int seg, int threads, size_t smem, int *blocks_per_sm);
 size_t sweep_modal_smem_bytes(int P, int precision, int wn, int G, int seg);
+// shared memory a launch with a second source (SweepArgs::src2) adds to sweep_modal_smem_bytes
+size_t sweep_modal_src2_bytes(int P, int wn);
 // Modal kernel CTA shape: wn compute warps, one helper warp and one or two aux warps per compute warp;
 // at most sweep_modal_max_wn(P) compute warps (the register file holds one CTA).  fit_wn: the largest
 // wn <= the given one whose shared memory fits the device.

@@ -197,6 +197,14 @@ size_t smem_p(int precision, int wn, int G, int seg) {
     }
 }
 
+size_t sweep_modal_src2_bytes(int P, int wn) {
+    switch (P) {
+        case 1: return modal::src2_layout_bytes(wn, modal::aux_per_compute(1, wn), 1, prefetch_depth(1));
+        case 2: return modal::src2_layout_bytes(wn, modal::aux_per_compute(2, wn), 2, prefetch_depth(2));
+        default: return modal::src2_layout_bytes(wn, modal::aux_per_compute(3, wn), 3, prefetch_depth(3));
+    }
+}
+
 size_t sweep_modal_smem_bytes(int P, int precision, int wn, int G, int seg) {
     switch (P) {
         case 1: return smem_p<1>(precision, wn, G, seg);

@@ -104,6 +104,8 @@ struct Layout {
     double *cellst;              // [Wn*nA][D][32/seg][N+1]: per row: sigma_t, then the fused source's moments[N]
     double *w;                   // [G]
     double *red;                 // [Wn*nA][32][N]: an aux warp's weighted values for the moment reduction
+    double *src2;                // [Wn*nA][D][32][N]: the second source's stages (launches with src2 only; the
+                                 // launch adds src2_layout_bytes to the shared memory)
 };
 
 __host__ __device__ constexpr size_t layout_bytes(int wn, int na, int G, int P, int D, int rw, int cw) {
@@ -111,6 +113,11 @@ __host__ __device__ constexpr size_t layout_bytes(int wn, int na, int G, int P, 
            sizeof(double) * ((size_t)(wn + 1) * kS * G * P + (size_t)wn * kZ * (cw + P * P) * 32 +
                              (size_t)wn * na * D * 32 * P * P + (size_t)wn * na * D * rw * (P * P + 1) +
                              (size_t)((G + 1) & ~1) + (size_t)wn * na * 32 * P * P);
+}
+
+// Shared memory of the second source's stages (after the rest of the layout).
+__host__ __device__ constexpr size_t src2_layout_bytes(int wn, int na, int P, int D) {
+    return sizeof(double) * (size_t)wn * na * D * 32 * P * P;
 }
 
 __device__ __forceinline__ Layout carve(unsigned char *raw, int wn, int na, int G, int P, int D, int rw, int cw) {
@@ -126,17 +133,23 @@ __device__ __forceinline__ Layout carve(unsigned char *raw, int wn, int na, int 
     L.cellst = L.src + (size_t)wn * na * D * 32 * N;
     L.w = L.cellst + (size_t)wn * na * D * rw * (N + 1);
     L.red = L.w + ((G + 1) & ~1);
+    L.src2 = L.red + (size_t)wn * na * 32 * N;
     return L;
 }
 
-template <int P, int MODE, bool XN, bool YN, bool ADJ, bool RECIP = true>
-__device__ __forceinline__ void prep_cell(CellIn<P, MODE> &in, const double *sp, const double *cp, const SweepArgs &a,
+template <int P, int MODE, bool XN, bool YN, bool ADJ, bool RECIP = true, bool SRC2 = false>
+__device__ __forceinline__ void prep_cell(CellIn<P, MODE> &in, const double *sp, const double *sp2, const double *cp,
+                                          const SweepArgs &a,
                                           const ModalOrdinate<P, typename CellIn<P, MODE>::TS> &od, double wq) {
     constexpr int N = P * P;
     using TS = typename CellIn<P, MODE>::TS;
     double src[N];
 #pragma unroll
     for (int k = 0; k < N; ++k) src[k] = a.src ? sp[k] : 0.0;
+    if constexpr (SRC2) {   // the second source, as the IDC source kernel combines it
+#pragma unroll
+        for (int k = 0; k < N; ++k) src[k] = fma(a.src2_scale, sp2[k], src[k]);
+    }
     if (a.phi_scatter) {
         if constexpr (!ADJ) {   // fused TransportOperator::Smv(scale, 1, sigma_s, phi -> src); the moments
                                 // sigma_s phi / (4 pi) come from launch_scatter_moments (no division here)
@@ -341,7 +354,7 @@ __device__ __forceinline__ void modal_rows(const SweepArgs &a, const SweepItem &
 // (lane o == 0 of a row also loads sigma_t and the fused source's moments).  A row segment's weighted
 // values meet in shared memory; the warp's Rw x N (row, dof) sums over each segment's ordinates are
 // spread over the lanes, each a fixed pairwise tree, and stored into this chunk's partial moments.
-template <int P, int MODE, int SEG, bool XN, bool YN, bool ADJ>
+template <int P, int MODE, int SEG, bool XN, bool YN, bool ADJ, bool SRC2 = false>
 __device__ __forceinline__ void modal_aux(const SweepArgs &a, const SweepItem &item, const Layout &L, int w,
                                           int k0, int na, int lane, int it_index) {
     constexpr int N = P * P;
@@ -372,6 +385,7 @@ __device__ __forceinline__ void modal_aux(const SweepArgs &a, const SweepItem &i
     const int ai = w * na + k0;   // this aux warp among the CTA's
     double *red = L.red + (size_t)ai * 32 * N;
     double *my_src = L.src + ((size_t)ai * D * 32 + lane) * N;     // stage b at + b*32*N
+    double *my_src2 = L.src2 + ((size_t)ai * D * 32 + lane) * N;   // (launches with src2)
     double *my_cell = L.cellst + ((size_t)ai * D * Rw + rr) * NC;  // stage b at + b*Rw*NC
     const int T = T_steps(a.nx, Rw);
 
@@ -384,6 +398,12 @@ __device__ __forceinline__ void modal_aux(const SweepArgs &a, const SweepItem &i
             if (act && a.src) {
                 const double *g = a.src + (size_t)ci * istride + (size_t)j * plane + (size_t)q * N;
                 double *d = my_src + (size_t)(i % D) * 32 * N;
+#pragma unroll
+                for (int k = 0; k < N; ++k) cp_async8(d + k, g + k);
+            }
+            if (SRC2 && act) {
+                const double *g = a.src2 + (size_t)ci * istride + (size_t)j * plane + (size_t)q * N;
+                double *d = my_src2 + (size_t)(i % D) * 32 * N;
 #pragma unroll
                 for (int k = 0; k < N; ++k) cp_async8(d + k, g + k);
             }
@@ -405,7 +425,7 @@ __device__ __forceinline__ void modal_aux(const SweepArgs &a, const SweepItem &i
         prefetch(i + D - 1);
         cp_wait<D - 2>();   // target i has landed
         __syncwarp();       // lane o == 0's cell-data copies are visible to its row segment
-        prep_cell<P, MODE, XN, YN, ADJ, false>(cur, my_src + (size_t)(i % D) * 32 * N,
+        prep_cell<P, MODE, XN, YN, ADJ, false, SRC2>(cur, my_src + (size_t)(i % D) * 32 * N, my_src2 + (size_t)(i % D) * 32 * N,
                                                my_cell + (size_t)(i % D) * Rw * NC, a, od, wq);
     };
     // ...into its slot, released to the compute warp
@@ -595,7 +615,7 @@ __device__ void modal_helper(const SweepArgs &a, const SweepItem &item, const La
     }
 }
 
-template <int P, int MODE, int SEG, bool ADJ, bool BATCHED>
+template <int P, int MODE, int SEG, bool ADJ, bool BATCHED, bool SRC2 = false>
 __global__ void __launch_bounds__(max_warps(P) * 32, 1) sweep_modal_kernel(const SweepArgs a0,
                                                                            const SweepArgs *__restrict__ table) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -651,10 +671,10 @@ __global__ void __launch_bounds__(max_warps(P) * 32, 1) sweep_modal_kernel(const
         } else {
             const int ax = warp - a0.wn - 1, w = ax / na, k0 = ax - w * na;   // aux warp k0 of compute warp w
             switch (item.quadrant) {
-                case 0: modal_aux<P, MODE, SEG, false, false, ADJ>(a, item, L, w, k0, na, lane, local); break;
-                case 1: modal_aux<P, MODE, SEG, false, true, ADJ>(a, item, L, w, k0, na, lane, local); break;
-                case 2: modal_aux<P, MODE, SEG, true, false, ADJ>(a, item, L, w, k0, na, lane, local); break;
-                default: modal_aux<P, MODE, SEG, true, true, ADJ>(a, item, L, w, k0, na, lane, local); break;
+                case 0: modal_aux<P, MODE, SEG, false, false, ADJ, SRC2>(a, item, L, w, k0, na, lane, local); break;
+                case 1: modal_aux<P, MODE, SEG, false, true, ADJ, SRC2>(a, item, L, w, k0, na, lane, local); break;
+                case 2: modal_aux<P, MODE, SEG, true, false, ADJ, SRC2>(a, item, L, w, k0, na, lane, local); break;
+                default: modal_aux<P, MODE, SEG, true, true, ADJ, SRC2>(a, item, L, w, k0, na, lane, local); break;
             }
         }
         __syncthreads();
@@ -663,7 +683,14 @@ __global__ void __launch_bounds__(max_warps(P) * 32, 1) sweep_modal_kernel(const
 
 template <int P, int MODE, int SEG, bool ADJ>
 cudaError_t launch_seg(const SweepArgs &args, int grid, size_t smem, cudaStream_t stream) {
+    // the second source has its own instantiation (forward, FP64 and refined precision), so the other
+    // launches run the kernel without it
     auto kern = sweep_modal_kernel<P, MODE, SEG, ADJ, false>;
+    if constexpr (!ADJ && MODE != 2) {
+        if (args.src2) kern = sweep_modal_kernel<P, MODE, SEG, false, false, true>;
+    } else {
+        if (args.src2) return cudaErrorInvalidValue;
+    }
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     kern<<<grid, cta_warps(P, args.wn) * 32, smem, stream>>>(args, nullptr);
