@@ -227,6 +227,7 @@ def extra_idc(abi, torch, dev, steps=10):
         psi = torch.zeros(P.psi_shape(), dtype=torch.float64, device=f"cuda:{dev}")
         src = torch.from_numpy(P.source).to(f"cuda:{dev}")
         for name, prec in (("fp64", abi.PREC_FP64), ("fp32_refined", abi.PREC_FP32_REFINED)):
+            out.setdefault("tile_shape", {})[name] = c.autotune(src.data_ptr(), P.dt, prec)
             c.idc_integrate(psi.data_ptr(), src.data_ptr(), P.dt, 2, 4, 3, abi.SCATTER_EXPLICIT, prec, use_graph=True,
                             loc=abi.LOC_DEVICE)
             torch.cuda.synchronize()
