@@ -607,8 +607,8 @@ Status Context::transport_residual(const double *psi, const double *phi, double 
 }
 
 Status Context::l2dist(const double *a, const double *b, double *out_host) {
-    IDC_TRY_CUDA(launch_l2dist2(dims(), a, b, d_scalar_, stream));
-    launches += 1;
+    IDC_TRY_CUDA(launch_l2dist2(dims(), a, b, d_scalar_, d_scalar_ + 4, stream));
+    launches += 2;
     double v = 0;
     IDC_TRY_CUDA(cudaMemcpyAsync(&v, d_scalar_, sizeof(double), cudaMemcpyDeviceToHost, stream));
     IDC_TRY_CUDA(cudaStreamSynchronize(stream));

@@ -192,7 +192,9 @@ cudaError_t dsa_precondition(const GridDims &g, const double *sigma_s, const dou
                              double *ws, bool transpose, int num_sms, int *error, long long spin_limit,
                              cudaStream_t s);
 constexpr int kDsaLaunches = 2;
-// sum over interior cells of (a - b)^2 into *out (device double, pre-zeroed by the launcher)
-cudaError_t launch_l2dist2(const GridDims &g, const double *a, const double *b, double *out, cudaStream_t s);
+// sum over interior cells of (a - b)^2 into *out (device double), in a fixed order; scratch holds
+// multidot_scratch_doubles() doubles
+cudaError_t launch_l2dist2(const GridDims &g, const double *a, const double *b, double *out, double *scratch,
+                           cudaStream_t s);
 
 }  // namespace idc

@@ -274,7 +274,7 @@ __global__ void l2dist2_kernel(GridDims g, const double *__restrict__ a, const d
     if (threadIdx.x < 32) {
         acc = threadIdx.x < (blockDim.x >> 5) ? warp_sums[threadIdx.x] : 0.0;
         for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
-        if (threadIdx.x == 0) atomicAdd(out, acc);
+        if (threadIdx.x == 0) out[blockIdx.x] = acc;   // per-block partial, added in a fixed order afterwards
     }
 }
 
@@ -505,13 +505,13 @@ cudaError_t launch_fill_u64(unsigned long long *p, size_t n, unsigned long long 
     return cudaGetLastError();
 }
 
-cudaError_t launch_l2dist2(const GridDims &g, const double *a, const double *b, double *out, cudaStream_t s) {
-    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(double), s);
-    if (e != cudaSuccess) return e;
-    const size_t n = (size_t)g.nx * g.ny * g.P * g.P;
-    int blocks = blocks_for(n);
-    if (blocks > 148 * 4) blocks = 148 * 4;
-    l2dist2_kernel<<<blocks, kThreads, 0, s>>>(g, a, b, out);
+cudaError_t launch_l2dist2(const GridDims &g, const double *a, const double *b, double *out, double *scratch,
+                           cudaStream_t s) {
+    const size_t total = (size_t)g.nx * g.ny * g.P * g.P;
+    int blocks = blocks_for(total);
+    if (blocks > kDotBlocks) blocks = kDotBlocks;
+    l2dist2_kernel<<<blocks, kThreads, 0, s>>>(g, a, b, scratch);
+    multidot_final_kernel<<<1, 32, 0, s>>>(scratch, blocks, out);   // fixed order: bitwise reproducible
     return cudaGetLastError();
 }
 

@@ -115,3 +115,23 @@ def test_set_preconditioner_rejects_bad_arguments():
             ctx.set_preconditioner(7, 30)
         with pytest.raises(abi.IdcError):
             ctx.set_preconditioner(abi.PRECOND_DSA, 0)
+
+
+@pytest.mark.parametrize("dsa", [False, True])
+def test_solves_are_bitwise_reproducible(dsa):
+    """Every reduction of the solvers (dot products, Krylov norms, the SI distance, the DSA inner products)
+    adds its partial sums in a fixed order, so repeating a solve gives bitwise the same result."""
+    P = lognormal(40, 1, 8, seed=12, c_range=(0.5, 0.99))
+    with context_for(P) as ctx:
+        if dsa:
+            ctx.set_preconditioner(abi.PRECOND_DSA, 20)
+        outs = []
+        for _ in range(2):
+            a = P.source.copy()
+            its_g, res_g = ctx.gmres_solve(a, P.dt, abs_tol=1e-10)
+            b = P.source.copy()
+            its_s, err_s = ctx.source_iteration(b, P.dt, abs_tol=1e-8, max_its=2000)
+            outs.append((a, b, its_g, res_g, its_s, err_s))
+    (a0, b0, *r0), (a1, b1, *r1) = outs
+    assert np.array_equal(a0, a1) and np.array_equal(b0, b1)
+    assert r0 == r1
