@@ -393,7 +393,6 @@ Status Context::sweep_host_many(int64_t count, const double *const *srcs, double
             IDC_TRY_CUDA(cudaEventCreateWithFlags(&ev_out[b], cudaEventDisableTiming));
         }
     }
-    const size_t cell = (size_t)nq * N;
     for (int64_t k = 0; k < count; ++k) {
         const int b = (int)(k & 1);
         double *d_src = psi_buf(b), *d_res = psi_buf(2 + b), *d_phi = phis ? phi_buf(3 + b) : nullptr;
