@@ -83,3 +83,22 @@ def test_idc_rejects_bad_arguments():
             args.update(kw)
             with pytest.raises(abi.IdcError):
                 ctx.idc_integrate(psi0.copy(), P.source, args["dt"], 1, args["num_nodes"], 3, args["scattering"])
+
+
+@pytest.mark.parametrize("p,M,prec,tol", [
+    (2, 4, abi.PREC_FP64, 1e-12),     # Q2
+    (1, 2, abi.PREC_FP64, 1e-12), (1, 3, abi.PREC_FP64, 1e-12), (1, 5, abi.PREC_FP64, 1e-12),
+    (1, 6, abi.PREC_FP64, 1e-12),     # more nodes than the fused correction kernel takes
+    (1, 4, abi.PREC_FP32, 5e-3),      # unrefined FP32 sweeps: sources combined into a scratch array first
+])
+def test_imex_idc_degrees_nodes_precisions(restatement, p, M, prec, tol):
+    """IMEX-IDC against the restated reference for every way a substep's source is formed: in the sweep
+    (fused correction sources plus psi_{n-1} / (h dt)), combined into a scratch array first, or by the
+    separate residual and source kernels."""
+    P, psi0 = _problem(n=9, p=p)
+    want = idc_steps(restatement, to_oracle(P), psi0, P.source, P.dt, 2, M=M, K=2, scattering="explicit")
+    with context_for(P) as ctx:
+        psi = psi0.copy()
+        sweeps = ctx.idc_integrate(psi, P.source, P.dt, 2, M, 2, abi.SCATTER_EXPLICIT, prec, use_graph=True)
+    assert sweeps == 2 * 3 * (M - 1)
+    assert rel_err(psi[1:-1, 1:-1], want[1:-1, 1:-1]) < tol
