@@ -59,6 +59,7 @@ Context::~Context() {
     cudaFree(d_src2mix);
     cudaFree(d_krylov);
     cudaFree(d_small);
+    cudaFreeHost(h_small);
     cudaFree(d_dsa_ws);
     for (int b = 0; b < 2; ++b) {
         if (ev_in[b]) cudaEventDestroy(ev_in[b]);

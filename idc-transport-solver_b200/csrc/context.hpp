@@ -159,6 +159,8 @@ public:
     cudaEvent_t ev_in[2] = {}, ev_done[2] = {}, ev_out[2] = {};
     size_t krylov_len = 0;
     double *d_small = nullptr;     // GMRES Hessenberg column / coefficients (device)
+    double *h_small = nullptr;     // GMRES: pinned host copy of the column, the new vector's norm and the error
+                                   // word (one copy and one synchronisation per Arnoldi step)
 
 private:
     Status build_schedule(int precision);

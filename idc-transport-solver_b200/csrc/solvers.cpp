@@ -4,6 +4,7 @@
 #include "context.hpp"
 
 #include <algorithm>
+#include <cstring>
 #include <cmath>
 #include <vector>
 
@@ -73,6 +74,7 @@ Status Context::gmres(Op apply, const double *b, double *x, double abs_tol, int 
         krylov_len = need;
     }
     if (!d_small) IDC_TRY_CUDA(cudaMalloc(&d_small, sizeof(double) * (128 + multidot_scratch_doubles())));
+    if (!h_small) IDC_TRY_CUDA(cudaMallocHost(&h_small, sizeof(double) * 129));
     double *dot_scratch = d_small + 128;
     double *V = d_krylov;
     auto Vc = [&](int k) { return V + (size_t)k * n; };
@@ -97,7 +99,7 @@ Status Context::gmres(Op apply, const double *b, double *x, double abs_tol, int 
     IDC_TRY(dot_host(Vc(0), Vc(0), n, &beta));
     beta = std::sqrt(beta);
 
-    std::vector<double> H((size_t)(m + 1) * m, 0.0), cs(m), sn(m), g(m + 1), h(m + 1), h2(m + 1), yv(m);
+    std::vector<double> H((size_t)(m + 1) * m, 0.0), cs(m), sn(m), g(m + 1), yv(m);
     int64_t its = 0;
     double resid = beta;
     bool converged = resid <= abs_tol;
@@ -115,19 +117,23 @@ Status Context::gmres(Op apply, const double *b, double *x, double abs_tol, int 
             } else {
                 IDC_TRY(apply(Vc(j), Vc(j + 1)));
             }
-            // CGS2: h = V^T w, w -= V h, twice
+            // CGS2: h = V^T w, w -= V h, twice; then |w|^2.  The two coefficient columns (d_small[0..], [64..]),
+            // the squared norm (d_small[127]) and the device error word reach the host in one pinned copy
+            // with one synchronisation.
             IDC_TRY_CUDA(launch_multidot(V, j + 1, n, Vc(j + 1), n, d_small, dot_scratch, stream));
-            IDC_TRY_CUDA(cudaMemcpyAsync(h.data(), d_small, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost, stream));
             IDC_TRY_CUDA(launch_multiaxpy(Vc(j + 1), V, j + 1, n, d_small, n, stream));
             IDC_TRY_CUDA(launch_multidot(V, j + 1, n, Vc(j + 1), n, d_small + 64, dot_scratch, stream));
-            IDC_TRY_CUDA(cudaMemcpyAsync(h2.data(), d_small + 64, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost,
-                                         stream));
             IDC_TRY_CUDA(launch_multiaxpy(Vc(j + 1), V, j + 1, n, d_small + 64, n, stream));
-            launches += 6;
-            double hn = 0.0;
-            IDC_TRY(dot_host(Vc(j + 1), Vc(j + 1), n, &hn));   // synchronises: h, h2 are on the host now
-            hn = std::sqrt(hn);
-            for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = h[i] + h2[i];
+            IDC_TRY_CUDA(launch_dot(Vc(j + 1), Vc(j + 1), n, d_small + 127, dot_scratch, stream));
+            launches += 8;
+            IDC_TRY_CUDA(cudaMemcpyAsync(h_small, d_small, sizeof(double) * 128, cudaMemcpyDeviceToHost, stream));
+            IDC_TRY_CUDA(cudaMemcpyAsync(h_small + 128, d_sync + 1, sizeof(int), cudaMemcpyDeviceToHost, stream));
+            IDC_TRY_CUDA(cudaStreamSynchronize(stream));
+            int dev_err = 0;
+            std::memcpy(&dev_err, h_small + 128, sizeof(int));
+            if (dev_err != kDevOk) IDC_TRY(check_device_error());   // re-arms the sweep state, returns the error
+            double hn = std::sqrt(h_small[127]);
+            for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = h_small[i] + h_small[64 + i];
             H[(size_t)(j + 1) * m + j] = hn;
             if (hn > 0.0) {
                 IDC_TRY_CUDA(launch_axpby(0.0, Vc(j + 1), 1.0 / hn, Vc(j + 1), n, stream));
@@ -150,7 +156,6 @@ Status Context::gmres(Op apply, const double *b, double *x, double abs_tol, int 
             resid = std::fabs(g[j + 1]);
             ++its;
             k = j + 1;
-            IDC_TRY(check_device_error());
             if (resid <= abs_tol || hn == 0.0) break;
         }
         // y = H^{-1} g, x += V y
