@@ -60,3 +60,16 @@ def test_no_device_is_a_status_not_a_crash():
     ok = abi.ProblemDesc(4, 4, 0.0, 1.0, 0.0, 1.0, 1, 0, 0, 0)
     assert lib.idc_ctx_create(C.byref(ok), C.byref(h)) == abi.IDC_ERR_CUDA
     assert not h.value
+
+
+def test_solver_entry_points_reject_null_arguments():
+    """The solver and adjoint entry points answer a null context or array with IDC_ERR_ARG before they touch
+    a device, like the reference's argument checks (no GPU needed)."""
+    lib = abi.load_library()
+    its, res, jv, ns = C.c_int64(), C.c_double(), C.c_double(), C.c_int64()
+    assert lib.idc_gmres_solve(None, None, 1.0, 1e-8, 30, 10, 0, 0, C.byref(its), C.byref(res)) == abi.IDC_ERR_ARG
+    assert lib.idc_adjoint_grad(None, None, None, 1.0, 1e-8, 30, 10, 0, None, None, None, 0, C.byref(its),
+                                C.byref(res)) == abi.IDC_ERR_ARG
+    assert lib.idc_adjoint_transient(None, None, None, 0.1, 3, None, 0, 1e-8, 30, 10, 0, None, None, None, None,
+                                     C.byref(jv), 0, C.byref(ns)) == abi.IDC_ERR_ARG
+    assert b"null" in lib.idc_last_error_message()
