@@ -161,6 +161,41 @@ def time_reference_cpu(P, reps: int):
     return sec / reps, int(os.environ.get("OMP_NUM_THREADS", threads)), phi
 
 
+def config0_against_reference(abi, torch, dev):
+    """The reference's own CPU-runnable case: 64x64 lattice on [0,7]^2, Q1, S8, one implicit-Euler step of
+    dt = 0.01 from zero flux, source iteration to 1e-10 (absolute l2 of phi changes, SISolver's rule).  The
+    GPU's idc_source_iteration against the reference's SISolver::Solve (oracle/_ref) on all host cores,
+    same inputs; phi compared."""
+    from idcsweep.problems import lattice
+    from oracle.bindings import Problem as OP, Reference
+    P = lattice(64, 1, 8, dt=0.01)
+    out = {"workload": "64x64 Q1 S8 lattice, one implicit-Euler step dt 0.01, source iteration to 1e-10"}
+    with _ctx_for(abi, P, dev) as c:
+        for rep in range(2):   # the first builds the schedule
+            psi = torch.from_numpy(P.source).to(f"cuda:{dev}")
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            its, change = c.source_iteration(psi.data_ptr(), P.dt, abs_tol=1e-10, max_its=5000, loc=abi.LOC_DEVICE)
+            torch.cuda.synchronize()
+            sec = time.perf_counter() - t0
+        phi = torch.zeros(P.phi_shape(), dtype=torch.float64, device=f"cuda:{dev}")
+        c.pmv(1.0, 0.0, psi.data_ptr(), phi.data_ptr(), loc=abi.LOC_DEVICE)
+        gphi = phi.cpu().numpy()
+    out["gpu"] = {"ms": sec * 1e3, "iterations": its, "last_change": change}
+    threads = os.cpu_count() or 1
+    o = OP(P.nx, P.ny, P.p, P.xi, P.eta, P.w, P.quad, P.sigma_t, P.sigma_s, P.ax, P.bx, P.ay, P.by)
+    with Reference().open(o, P.dt, abs_tol=1e-10, max_its=5000) as h:
+        h.source_iteration(P.source, P.dt)   # warm-up
+        t0 = time.perf_counter()
+        rpsi = h.source_iteration(P.source, P.dt)
+        rsec = time.perf_counter() - t0
+        rphi = h.pmv(rpsi)
+    out["reference_cpu"] = {"ms": rsec * 1e3, "threads": int(os.environ.get("OMP_NUM_THREADS", threads))}
+    out["speedup"] = rsec / sec
+    out["phi_rel_diff"] = float(np.abs(gphi - rphi).max() / np.abs(rphi).max())
+    return out
+
+
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -520,6 +555,10 @@ def run_ours(args):
         except Exception as e:  # the reference library may be absent where it was never built
             line["cpu_baseline"] = None
             line["cpu_baseline_error"] = str(e)[:200]
+        try:   # the reference's own small case, solved by both sides
+            line["config0_source_iteration"] = config0_against_reference(abi, torch, dev)
+        except Exception as e:
+            line["config0_source_iteration"] = {"error": str(e)[:200]}
     emit(line)
     ctx.close()
     if dist is not None:
