@@ -141,13 +141,22 @@ def emit(d):
     print(json.dumps(d), flush=True)
 
 
+def bench_config(P, world: int) -> dict:
+    """The workload description both arms print (the same keys and values for the same problem)."""
+    return {"workload": WORKLOAD if P.nx == NX else WORKLOAD.replace("256x256", f"{P.nx}x{P.nx}"),
+            "nx": P.nx, "ny": P.ny, "p": P_DEG, "nq": P.nq, "unknowns_per_step": P.unknowns_per_sweep,
+            "parallelism": f"replicas{world}" if world > 1 else "single",
+            "l2": "inputs larger than L2 (source 690 MB, psi 690 MB per step); no flush"}
+
+
 # ----------------------------------------------------------------------------------------------------
 # reference arm: the reference's own CPU sweep
 # ----------------------------------------------------------------------------------------------------
 
-def time_reference_cpu(P, reps: int):
-    """SweepOperator::Apply of the reference (oracle/_ref), OpenMP on all host cores.  Returns
-    (seconds per sweep, threads, psi of the last sweep)."""
+def time_reference_cpu(P, reps: int, warmup: int = 1):
+    """SweepOperator::Apply of the reference (oracle/_ref), OpenMP on all host cores: `warmup` untimed
+    sweeps (the first gives the oracle result), then `reps` timed ones.  Returns (seconds per sweep,
+    threads, phi of the oracle result)."""
     from oracle.bindings import Problem as OP, Reference
     threads = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
@@ -155,7 +164,9 @@ def time_reference_cpu(P, reps: int):
     ref = Reference()
     o = OP(P.nx, P.ny, P.p, P.xi, P.eta, P.w, P.quad, P.sigma_t, P.sigma_s, P.ax, P.bx, P.ay, P.by)
     with ref.open(o, P.dt) as h:
-        psi = h.sweep(P.source, P.dt)            # warm-up, and the oracle result
+        psi = h.sweep(P.source, P.dt)
+        for _ in range(max(0, warmup - 1)):
+            h.sweep(P.source, P.dt)
         sec = h.time_sweeps(P.source, P.dt, reps)
         phi = h.pmv(psi)
     return sec / reps, int(os.environ.get("OMP_NUM_THREADS", threads)), phi
@@ -200,20 +211,21 @@ def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    P = problem(0)
+    P = problem(0, args.nx)
     steps = max(1, args.steps)
-    reps = max(1, min(steps, 3))
+    warm = max(1, args.warmup)
     t0 = time.time()
-    sec, threads, _ = time_reference_cpu(P, reps)
+    sec, threads, _ = time_reference_cpu(P, steps, warm)
     value = P.unknowns_per_sweep / sec
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
-        "steps": reps, "warmup": 1, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+        "steps": steps, "warmup": warm, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "256x256 Q2 S16 log-normal steady sweep (reference CPU, FP64 GE)",
-                   "nx": NX, "ny": NX, "p": P_DEG, "nq": P.nq, "unknowns_per_step": P.unknowns_per_sweep},
+        "config": bench_config(P, args.gpus),
+        "reference_path": "SweepOperator::Apply (wavefront pattern, Gaussian-elimination cell solves), FP64, "
+                          "OpenMP on all host cores",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
-                         "sample": f"{reps} full sweeps of the workload after 1 warm-up sweep"},
+                         "sample": f"{steps} full sweeps of the workload after {warm} warm-up sweep(s)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "wall_s": time.time() - t0,
     }
@@ -515,12 +527,8 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD if P.nx == NX else WORKLOAD.replace("256x256", f"{P.nx}x{P.nx}"),
-                   "nx": P.nx, "ny": P.ny, "p": P_DEG, "nq": P.nq,
-                   "unknowns_per_step": unknowns, "parallelism": f"replicas{world}" if world > 1 else "single",
-                   "l2": "inputs larger than L2 (source 690 MB, psi 690 MB per step); no flush",
-                   "tile_shape": {"fp64": list(shapes[abi.PREC_FP64]),
-                                  "fp32_refined": list(shapes[abi.PREC_FP32_REFINED])}},
+        "config": bench_config(P, world),
+        "tile_shape": {"fp64": list(shapes[abi.PREC_FP64]), "fp32_refined": list(shapes[abi.PREC_FP32_REFINED])},
         "roofline": {"bound": "hbm", "achieved": alg / (k64 * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                      "frac": alg / (k64 * 1e-3) / 1e9 / peak, "traffic": traffic,
                      "algorithmic_bytes": alg, "kernel_ms": k64, "peak_kind": peak_kind},
@@ -545,9 +553,10 @@ def run_ours(args):
 
     if not args.no_cpu_baseline and world == 1:
         try:
-            sec, threads, phi_ref = time_reference_cpu(P, reps=2)
+            sec, threads, phi_ref = time_reference_cpu(P, args.steps, warm)
             line["cpu_baseline"] = {"value": unknowns / sec, "unit": UNIT, "cores": threads, "kind": "reference",
-                                    "sample": "2 full sweeps of the workload after 1 warm-up sweep"}
+                                    "sample": f"{args.steps} full sweeps of the workload after {warm} warm-up "
+                                              "sweep(s)"}
             scale = np.abs(phi_ref).max()
             line["err_phi_vs_oracle"] = {
                 "fp64": float(np.abs(phi64.cpu().numpy() - phi_ref).max() / scale),

@@ -22,6 +22,14 @@ namespace {
 
 thread_local std::string g_last_error;
 
+}  // namespace
+
+namespace idc {
+void set_last_error(const std::string &msg) { g_last_error = msg; }
+}  // namespace idc
+
+namespace {
+
 int fail(const idc::Status &s) {
     g_last_error = s.msg;
     return s.code;
@@ -605,6 +613,14 @@ int idc_adjoint_transient(idc_ctx *ctx, const double *psi0, const double *source
             ABI_TRY_CUDA(cudaMemcpyAsync(dpsi0, d_p0, sizeof(double) * c.psi_len(), cudaMemcpyDeviceToHost, c.stream));
     }
     ABI_TRY_CUDA(cudaStreamSynchronize(c.stream));
+    return IDC_OK;
+    ABI_GUARD_END
+}
+
+int idc_set_spin_limit(idc_ctx *ctx, int64_t polls) {
+    ABI_GUARD_BEGIN
+    if (!ctx) return fail(IDC_ERR_ARG, "null context");
+    ctx->impl.spin_limit = polls > 0 ? (long long)polls : idc::Context::kDefaultSpinLimit;
     return IDC_OK;
     ABI_GUARD_END
 }

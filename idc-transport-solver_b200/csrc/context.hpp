@@ -148,7 +148,8 @@ public:
     float last_sweep_ms = 0.f;
     bool capturing = false;   // a CUDA graph capture is open on `stream`: no timing events, no host syncs
     int64_t launches = 0;
-    long long spin_limit = 1ll << 22;
+    static constexpr long long kDefaultSpinLimit = 1ll << 22;
+    long long spin_limit = kDefaultSpinLimit;   // polls before a device-side wait gives up (idc_set_spin_limit)
 
     double *d_krylov = nullptr;    // GMRES basis, (restart + 1) phi-sized vectors (+ restart for flexible GMRES)
     int precond_kind = 0;          // 0 none, 1 DSA (right preconditioner of the forward Peierls GMRES)

@@ -10,6 +10,10 @@
 
 namespace idc {
 
+// Text returned by idc_last_error_message() on the calling thread (abi.cpp), for entry points that
+// report errors outside the context-based ABI layer.
+void set_last_error(const std::string &msg);
+
 // Device-side error codes written to the context's error word.
 enum DeviceError : int {
     kDevOk = 0,

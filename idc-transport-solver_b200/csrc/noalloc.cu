@@ -10,6 +10,11 @@
 // The array is a static __device__ object: every GPU that loads this library holds it (about 96 KiB)
 // until the process exits.  Its host-side name is only a stand-in, so its device address is looked up
 // once per device with cudaGetSymbolAddress, with that device current, on the first call on that device.
+//
+// The sweep runs without fused moments; phi_out is formed afterwards by the moment kernel of idc_pmv,
+// which adds the ordinates of each (cell, dof) in index order, so phi_out repeats bitwise from call to
+// call (the row-synchronous kernel's fused moments would add across thread blocks with atomics).  The
+// call reads the ordinates back to the host and synchronises `stream` before it returns.
 #include "idc_internal.hpp"
 #include "idcsweep.h"
 
@@ -35,11 +40,9 @@ int *g_scratch_addr[kMaxDevices] = {};    // device address of g_sweep_scratch, 
 idc::SweepItem g_items_host[kMaxItems];   // staging for the item list (host, static)
 double g_xi_host[kMaxOrdinates], g_eta_host[kMaxOrdinates];
 
-// Status codes are the whole error report of this entry point; the text is kept for debuggers.
-thread_local std::string g_msg;
-
+// The status code is returned; its text goes to idc_last_error_message() as for every other entry point.
 int fail(int code, const std::string &m) {
-    g_msg = m;
+    idc::set_last_error(m);
     return code;
 }
 
@@ -73,7 +76,7 @@ extern "C" int idc_sweep_noalloc(const idc_problem_desc *desc, int64_t nq, const
     for (int k = 0; k < 4; ++k)
         if (quad_bounds[k + 1] < quad_bounds[k]) return fail(IDC_ERR_ARG, "idc_sweep_noalloc: bad quad_bounds");
 
-    const int P = (int)desc->dg_degree + 1, N = P * P;
+    const int P = (int)desc->dg_degree + 1;
     const int64_t nx = desc->nx, ny = desc->ny;
 
     // tile shape: the same automatic choice as the context-based entry points
@@ -154,8 +157,6 @@ extern "C" int idc_sweep_noalloc(const idc_problem_desc *desc, int64_t nq, const
     // the array keeps the last call's contents: clear head, error word and progress flags
     e = cudaMemcpyAsync(items, g_items_host, sizeof(idc::SweepItem) * n, cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(scratch, 0, sizeof(int) * (2 + (size_t)n), stream);
-    if (e == cudaSuccess && phi_out)
-        e = cudaMemsetAsync(phi_out, 0, sizeof(double) * (size_t)(nx + 2) * (ny + 2) * N, stream);
     if (e != cudaSuccess) return fail(IDC_ERR_CUDA, std::string("idc_sweep_noalloc: staging: ") + cudaGetErrorString(e));
 
     idc::SweepArgs a{};
@@ -165,7 +166,7 @@ extern "C" int idc_sweep_noalloc(const idc_problem_desc *desc, int64_t nq, const
     a.sigma_s = nullptr;
     a.phi_scatter = nullptr;
     a.scatter_scale = 1.0;
-    a.phi = phi_out;
+    a.phi = nullptr;   // phi_out is formed after the sweep, in a fixed order
     a.xi = xi;
     a.eta = eta;
     a.w = w;
@@ -185,11 +186,21 @@ extern "C" int idc_sweep_noalloc(const idc_problem_desc *desc, int64_t nq, const
     a.progress = progress;
     a.spin_limit = 1ll << 22;
     e = idc::launch_sweep(P, precision, a, std::min(n, per_sm * sms), block, smem, stream);
+    if (e != cudaSuccess) return fail(IDC_ERR_CUDA, std::string("idc_sweep_noalloc: sweep: ") + cudaGetErrorString(e));
+    if (phi_out) {   // phi = sum_q w_q psi_q on interior cells in index order (TransportOperator::Pmv), ghosts 0
+        const idc::GridDims g{(int)nx, (int)ny, (int)nq, P, a.dx, a.dy};
+        e = idc::launch_zero_ghost_phi(g, phi_out, stream);
+        if (e == cudaSuccess) e = idc::launch_pmv(g, 1.0, 0.0, w, result, phi_out, stream);
+        if (e != cudaSuccess)
+            return fail(IDC_ERR_CUDA, std::string("idc_sweep_noalloc: moments: ") + cudaGetErrorString(e));
+    }
+    // the error word comes back on the caller's stream, behind the sweep (a legacy-stream copy would also
+    // wait for the caller's other blocking streams)
+    int dev_err = 0;
+    e = cudaMemcpyAsync(&dev_err, err_word, sizeof(int), cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) return fail(IDC_ERR_CUDA, std::string("idc_sweep_noalloc: sweep: ") + cudaGetErrorString(e));
-    int dev_err = 0;
-    e = cudaMemcpy(&dev_err, err_word, sizeof(int), cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) return fail(IDC_ERR_CUDA, std::string("idc_sweep_noalloc: error word: ") + cudaGetErrorString(e));
-    if (dev_err != idc::kDevOk) return fail(IDC_ERR_TIMEOUT, "idc_sweep_noalloc: a device-side wait gave up");
+    if (dev_err != idc::kDevOk)
+        return fail(IDC_ERR_TIMEOUT, "idc_sweep_noalloc: a device-side wait gave up; the result is not valid");
     return IDC_OK;
 }

@@ -35,6 +35,9 @@ PREC_FP64 = 0
 PREC_FP32_REFINED = 1
 PREC_FP32 = 2
 
+IDC_NOALLOC_MAX_ITEMS = 4096        # include/idcsweep.h
+IDC_NOALLOC_MAX_ORDINATES = 1024
+
 # Every symbol include/idcsweep.h declares (checked by tests/test_abi_symbols.py).
 EXPORTED_SYMBOLS = (
     "idc_ctx_create", "idc_ctx_destroy", "idc_set_ordinates", "idc_set_sigma", "idc_sweep", "idc_pmv",
@@ -44,6 +47,7 @@ EXPORTED_SYMBOLS = (
     "idc_write_af2", "idc_read_af2", "idc_sweep_fused", "idc_set_tile_shape", "idc_autotune", "idc_batch_create",
     "idc_batch_add", "idc_batch_sweep", "idc_batch_autotune", "idc_batch_last_timing", "idc_batch_destroy",
     "idc_batch_set_shape", "idc_batch_get_shape", "idc_sweep_out_many", "idc_adjoint_transient",
+    "idc_set_spin_limit",
 )
 
 
@@ -88,6 +92,7 @@ def load_library(path: str = LIB_PATH):
     lib.idc_last_error_message.restype = C.c_char_p
     lib.idc_last_timing.argtypes = [vp, _dp, C.POINTER(C.c_int64)]
     lib.idc_set_tiling.argtypes = [vp, C.c_int32, C.c_int32]
+    lib.idc_set_spin_limit.argtypes = [vp, C.c_int64]
     lib.idc_sweep_out.argtypes = [vp, vp, vp, C.c_double, vp, C.c_int, C.c_int]
     lib.idc_sweep_out_many.argtypes = [vp, C.c_int64, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.c_double,
                                        C.c_int, C.c_int]
@@ -308,6 +313,10 @@ class SweepContext:
                                                _ptr(dsigma_s, loc), _ptr(dsource, loc), _ptr(dpsi0, loc),
                                                C.byref(jv), loc, C.byref(ns)), "idc_adjoint_transient")
         return float(jv.value), int(ns.value)
+
+    def set_spin_limit(self, polls: int = 0):
+        """Polls before a device-side wait gives up (0: the default)."""
+        _check(self._lib.idc_set_spin_limit(self._h, int(polls)), "idc_set_spin_limit")
 
     def last_timing(self):
         ms = C.c_double()

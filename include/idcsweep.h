@@ -145,7 +145,11 @@ int idc_source_iteration(idc_ctx *ctx, double *source_inout, double dt, double a
  *
  * Everything is passed in: xi, eta, w (nq each), sigma_t, source, result and phi_out (nullable) are DEVICE
  * pointers on desc->device; quad_bounds is a host array.  The call makes no cudaMalloc/cudaFree and uses
- * no context.  The sweep's own scratch (work-queue head, error word, progress flags, work-item list) is
+ * no context.  As in idc_sweep_out, the inflow values are read from the ghost cells of `source` and only
+ * the interior cells of `result` are written (its ghost cells keep what the caller put there).  phi_out
+ * receives sum_q w_q result_q on the interior cells, added in ordinate order (bitwise the same on every
+ * call), and zero on its ghost cells.  The call reads xi and eta back to check their quadrant signs and
+ * synchronises `stream` before it returns; on failure idc_last_error_message() has the reason.  The sweep's own scratch (work-queue head, error word, progress flags, work-item list) is
  * one fixed file-scope device array of about 96 KiB that every GPU loading the library keeps until the
  * process exits; problems needing more than IDC_NOALLOC_MAX_ITEMS work items, or more than
  * IDC_NOALLOC_MAX_ORDINATES ordinates, are rejected with IDC_ERR_ARG (use idc_sweep_out for those).
@@ -303,6 +307,15 @@ const char *idc_strerror(int status);
 
 /* Text of the most recent error on this thread (static per-thread storage). */
 const char *idc_last_error_message(void);
+
+/* Bound of every device-side wait of the context's kernels (a wait on another warp's or thread block's
+ * progress, polled or blocking in the barrier unit): after `polls` polls the wait gives up, the kernel
+ * records the failure in the context's device error word, every warp leaves, and the call returns
+ * IDC_ERR_TIMEOUT after re-arming the context's trace buffers, so the next call starts clean.  polls <= 0
+ * restores the default (2^22 polls, seconds of waiting; a sweep's waits normally end within microseconds).
+ * Meant for failure-detection tests and for callers that want a hung peer reported sooner.  The
+ * reference has no counterpart (its OpenMP barriers wait without bound). */
+int idc_set_spin_limit(idc_ctx *ctx, int64_t polls);
 
 /* Device time in milliseconds of the last sweep kernel launched by the context (CUDA events on the
  * launching stream), and the number of kernels the last idc_* call launched. */

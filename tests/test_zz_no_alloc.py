@@ -32,7 +32,8 @@ def _context_result(P):
 def _noalloc_result(P):
     d = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float64)).cuda()
     xi, eta, w, st, src = d(P.xi), d(P.eta), d(P.w), d(P.sigma_t), d(P.source)
-    out = src.clone()                                   # ghost cells: the inflow values, as in psi_inout
+    # NaN everywhere: every interior value must be written by the call, the ghost cells left alone
+    out = torch.full_like(src, float("nan"))
     phi = torch.full(P.phi_shape(), float("nan"), dtype=torch.float64, device="cuda")   # must be cleared by the call
     torch.cuda.synchronize()
     rc = abi.sweep_noalloc(P.nx, P.ny, P.p, P.ax, P.bx, P.ay, P.by, xi.data_ptr(), eta.data_ptr(), w.data_ptr(),
@@ -40,7 +41,12 @@ def _noalloc_result(P):
                            abi.PREC_FP64, device=0, stream=None)
     assert rc == abi.IDC_OK, rc
     assert torch.equal(src, d(P.source))                # the source is not modified
-    return out.cpu().numpy(), phi.cpu().numpy()
+    out = out.cpu().numpy()
+    interior = np.zeros(out.shape[:2], bool)
+    interior[1:-1, 1:-1] = True
+    assert np.isnan(out[~interior]).all()               # ghost cells of the result are not written
+    out[~interior] = P.source[~interior]                # ... and take the inflow values for the comparison
+    return out, phi.cpu().numpy()
 
 
 def test_noalloc_matches_sweep_on_two_calls_in_a_row():
@@ -49,8 +55,18 @@ def test_noalloc_matches_sweep_on_two_calls_in_a_row():
     for P in (first, second):
         ref_psi, ref_phi = _context_result(P)
         psi, phi = _noalloc_result(P)
+        assert not np.isnan(psi).any() and not np.isnan(phi).any()
         assert rel_err(psi, ref_psi) < TOL64
         assert rel_err(phi, ref_phi) < TOL64
+
+
+def test_noalloc_phi_repeats_bitwise():
+    """phi_out is summed over the ordinates in a fixed order, so two calls give the same bits."""
+    P = random_problem(40, 33, 2, 12, seed=406)
+    psi1, phi1 = _noalloc_result(P)
+    psi2, phi2 = _noalloc_result(P)
+    assert np.array_equal(phi1, phi2)
+    assert np.array_equal(psi1, psi2)
 
 
 def test_noalloc_rejects_oversized_problems():
@@ -62,3 +78,5 @@ def test_noalloc_rejects_oversized_problems():
     rc = abi.sweep_noalloc(2, 70000, 0.0, 1.0, 0.0, 1.0, 0, xi.data_ptr(), eta.data_ptr(), w.data_ptr(), P.nq,
                            P.quad, dummy.data_ptr(), dummy.data_ptr(), dummy.data_ptr())
     assert rc == abi.IDC_ERR_ARG
+    msg = abi.load_library().idc_last_error_message().decode()
+    assert "work items" in msg and str(abi.IDC_NOALLOC_MAX_ITEMS) in msg, msg
