@@ -4,6 +4,8 @@
 * ``Reference``   -> oracle/_ref/libidcref.so, the reference solver compiled from its own sources
   by oracle/Makefile.ref with the driver oracle/ref_driver.cpp.  Present only where the reference
   tree was available at build time (it travels with the repository snapshot once built).
+  ``Reference(REFERENCE_GPU_SO)`` is the same reference with the GPU sweep pattern plugged in
+  (oracle/sweep_pattern_gpu.cpp, pattern "gpu-wavefront"), linked against libidcsweep.so.
 
 Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg import this module.
 """
@@ -18,6 +20,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 RESTATEMENT_SO = os.path.join(HERE, "_build", "liboracle.so")
 REFERENCE_SO = os.path.join(HERE, "_ref", "libidcref.so")
+REFERENCE_GPU_SO = os.path.join(HERE, "_ref", "libidcref_gpu.so")
 
 _dp = C.POINTER(C.c_double)
 
@@ -158,8 +161,10 @@ class Reference:
         lib.ref_si_solve.argtypes = [C.c_void_p, _dp, C.c_double, C.POINTER(C.c_int64), _dp]
         lib.ref_write_sd.argtypes = [C.c_void_p, _dp, C.c_char_p]
         lib.ref_write_af.argtypes = [C.c_void_p, _dp, C.c_char_p]
+        lib.ref_idc_steps.argtypes = [C.c_void_p, _dp, _dp, C.c_double, C.c_int64, C.c_int64, C.c_int64, C.c_double,
+                                      C.c_int64]
         for f in ("ref_apply", "ref_apply_timed", "ref_pmv", "ref_smv", "ref_lmv", "ref_si_solve", "ref_write_sd",
-                  "ref_write_af"):
+                  "ref_write_af", "ref_idc_steps"):
             getattr(lib, f).restype = C.c_int
         self.lib = lib
 
@@ -221,6 +226,16 @@ class _RefHandle:
     def write_af(self, psi, path: str):
         """The reference's OrdinateFlux::WriteToDisk of psi (halo layout)."""
         assert self.lib.ref_write_af(self.h, _p(np.ascontiguousarray(psi, np.float64)), path.encode()) == 0
+
+    def idc_steps(self, psi0, source, dt, steps, num_nodes=4, num_corrections=3, si_abs_tol=1e-14,
+                  si_max_its=100000):
+        """psi after `steps` steps of the reference's IDCIntegrator (non-hybrid update form, Gauss-Lobatto
+        nodes, source-iteration substeps to si_abs_tol); ghost cells of the result are zero."""
+        psi = np.ascontiguousarray(psi0, np.float64).copy()
+        src = np.ascontiguousarray(source, np.float64)
+        assert self.lib.ref_idc_steps(self.h, _p(psi), _p(src), float(dt), int(steps), int(num_nodes),
+                                      int(num_corrections), float(si_abs_tol), int(si_max_its)) == 0
+        return psi
 
     def source_iteration(self, source, dt=np.inf):
         psi = np.ascontiguousarray(source, np.float64).copy()

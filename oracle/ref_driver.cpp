@@ -9,6 +9,7 @@
 //   * SweepOperator<RKDG::OrdinateFlux>::Apply   linear_solvers/Abstract/SweepOperator.cpp:118-135
 //   * TransportOperator::Pmv / Smv / Lmv         operators/RKDG/TransportOperator.cpp:37, 203, 1215
 //   * SISolver<RKDG::OrdinateFlux>::Solve        linear_solvers/Abstract/ImplicitSolver/SISolver.cpp:190
+//   * IDCIntegrator::Step (non-hybrid)           time_integrators/RKDG/idc.cpp:521, 846-955
 //
 // Ordinate injection.  The reference has no level-symmetric set (utils/Quadrule/OrdinateSet.cpp:37-59),
 // so the driver places the caller's (xi, eta, w) into OrdinateSet's static cache under a private order
@@ -32,6 +33,7 @@
 # include "objects/RKDG/DensityFunction.hpp"
 # include "objects/RKDG/OrdinateFlux.hpp"
 # include "operators/RKDG/TransportOperator.hpp"
+# include "time_integrators/RKDG/idc.hpp"
 # include "utils/ParameterList.hpp"
 # include "utils/Quadrule/OrdinateSet.hpp"
 # include "utils/global.hpp"
@@ -253,6 +255,47 @@ int ref_si_solve ( void * h, double * source_inout, double dt, int64_t * iters, 
         if ( iters ) *iters = -1;
         return 0;
     } catch ( std::exception & e ) { std::fprintf( stderr, "ref_si_solve: %s\n", e.what() ); return 1; }
+}
+
+// `steps` time steps of size dt with the reference's own IDC integrator: IDCIntegrator::Create
+// (time_integrators/RKDG/idc.cpp:94-102) in the non-hybrid update form (idc_type "update") on
+// num_nodes Gauss-Lobatto nodes (SetNodes reads them from Global::input_list, :2305-2381) with
+// num_corr corrections; every substep is SISolver::Solve to si_abs_tol (solve_type "source-iteration",
+// started from the integrator's initial guess), each step IDCIntegrator::Step (:521-560 ->
+// Step_Nonhybrid :846-955).  psi_inout holds psi^0 on entry and psi^steps on return (halo layout; the
+// integrator returns the last stage with its ghost cells zeroed); source is q, constant in time, its ghost
+// cells the inflow values.
+int ref_idc_steps ( void * h, double * psi_inout, const double * source, double dt, int64_t steps,
+                    int64_t num_nodes, int64_t num_corr, double si_abs_tol, int64_t si_max_its ) {
+    auto * P = static_cast<RefProblem *>(h);
+    try {
+        ParameterList pl = P->plist;
+        char buf[64];
+        pl.SetValue( "cfl", "1" );   // read by TimeIntegrator's constructor; Step takes the step size itself
+        pl.SetValue( "ang_order", std::to_string( P->order_key ) );
+        pl.SetValue( "ordinate_type", "spherical-triangle" );   // the type the injected set is cached under
+        pl.SetValue( "ordinate_sym_reduce", "true" );
+        pl.SetValue( "idc_type", "update" );
+        pl.SetValue( "idc_num_corr", std::to_string( num_corr ) );
+        pl.SetValue( "hybrid_method", "none" );
+        pl.SetValue( "solve_type", "source-iteration" );
+        std::snprintf( buf, sizeof buf, "%.17g", si_abs_tol ); pl.SetValue( "abs_tol", buf );
+        pl.SetValue( "max_its", std::to_string( si_max_its ) );
+        Global::input_list.SetValue( "idc_nodes_type", "gauss-lobatto" );
+        Global::input_list.SetValue( "idc_num_nodes", std::to_string( num_nodes ) );
+
+        std::unique_ptr<IDCIntegrator> idc( IDCIntegrator::Create( pl ) );
+        OrdinateSet oset( P->order_key, true, OrdinateSet::OrdinateType::SphericalTriangle );
+        RKDG::OrdinateFlux psi, src;
+        psi.Reconfigure( *P->dd, oset, P->p );
+        src.Reconfigure( *P->dd, oset, P->p );
+        CopyIn( psi, psi_inout, P->psi_len() );
+        CopyIn( src, source, P->psi_len() );
+        for ( int64_t n = 0; n < steps; ++n )
+            idc->Step( psi, src, *P->sigma_t, *P->sigma_s, dt );
+        CopyOut( psi, psi_inout, P->psi_len() );
+        return 0;
+    } catch ( std::exception & e ) { std::fprintf( stderr, "ref_idc_steps: %s\n", e.what() ); return 1; }
 }
 
 // DensityFunction::WriteToDisk (objects/RKDG/DensityFunction.cpp:2228-2400) of a scalar flux given on the

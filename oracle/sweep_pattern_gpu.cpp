@@ -1,0 +1,121 @@
+//------------------------------------------------------------------------------------------------------------
+// SweepPatternGPU: the reference-side binding of the B200 sweep, as a maintainer of the reference adds it.
+//
+// A new sweep pattern, registered under the deck key `sweep_pattern gpu-wavefront` through the reference's
+// own factory (SweepPatternDerivedFactory, linear_solvers/Abstract/SweepPattern/SweepPattern.cpp:274-306),
+// whose Sweep (the virtual of SweepPattern.hpp:117-122) hands the reference's arrays to the C ABI of
+// libidcsweep.so (include/idcsweep.h).  SweepOperator::Apply (SweepOperator.cpp:118-135) and everything
+// above it -- SISolver, the Peierls solvers, the DIRK and IDC integrators -- call it unchanged.
+//
+// It needs three one-line additions to the reference's headers, which oracle/plugin_headers.py makes in
+// copies under oracle/_ref/plugin_include (the reference tree is not touched):
+//   * `class SweepPatternGPU;` among the nested pattern declarations of SweepOperator
+//     (linear_solvers/Abstract/SweepOperator.hpp:44-46), as every pattern is a nested class;
+//   * `double GetDt() const` in SweepCellSolveBase (Abstract/SweepCellSolve/SweepCellSolveBase.hpp:118)
+//     and in SweepCellSolveManager (Abstract/SweepCellSolve/SweepCellSolveManager.hpp:97): Apply hands dt
+//     to the cell solvers (SetDt), not to the pattern, and the GPU sweep needs it.
+//
+// Built by oracle/Makefile.ref into oracle/_ref/libidcref_gpu.so (the reference objects, the test driver
+// oracle/ref_driver.cpp and this file, linked against libidcsweep.so).  Test infrastructure: the tests run
+// the reference's own solvers through it and compare with the reference's CPU patterns.
+//------------------------------------------------------------------------------------------------------------
+
+# include <cstring>
+# include <stdexcept>
+# include <string>
+# include <vector>
+
+# include "idcsweep.h"
+# include "linear_solvers/Abstract/SweepOperator.hpp"
+# include "linear_solvers/Abstract/SweepPattern/SweepPattern.hpp"
+# include "linear_solvers/Abstract/SweepPattern/SweepPatternDerivedFactory.hpp"
+# include "linear_solvers/Abstract/SweepPattern/SweepPatternUniCart.hpp"
+# include "linear_solvers/Abstract/SweepCellSolve/SweepCellSolveManager.hpp"
+# include "objects/RKDG/CrossSection.hpp"
+# include "objects/RKDG/OrdinateFlux.hpp"
+# include "utils/global.hpp"
+
+namespace {
+
+// The reference reports errors as exceptions; the ABI returns status codes.
+void idc_check ( int rc, const char * what ) {
+    if ( rc != IDC_OK )
+        throw std::runtime_error( std::string( "gpu-wavefront: " ) + what + ": " + idc_strerror( rc ) + ": "
+                                  + idc_last_error_message() );
+}
+
+} // namespace
+
+
+template< class OrdinateFlux >
+class SweepOperator<OrdinateFlux>::SweepPatternGPU : public SweepOperator<OrdinateFlux>::SweepPatternUniCart {
+
+    friend typename SweepPattern::template SweepPatternDerivedFactory<SweepPatternGPU>;
+
+protected:
+
+    // The context is created once per SweepOperator: the grid and the ordinate set are fixed for its life.
+    SweepPatternGPU ( const SweepOperator<OrdinateFlux> & op, const ParameterList & input_list )
+        : SweepPatternUniCart( op, input_list ) {
+
+        idc_problem_desc d {};
+        d.nx = op.nx(0);
+        d.ny = op.nx(1);
+        d.ax = op.ax(0);
+        d.bx = op.bx(0);
+        d.ay = op.ax(1);
+        d.by = op.bx(1);
+        d.dg_degree = Global::DG_degree;
+        d.sigma_degree = 0;
+        d.device = 0;
+        d.flags = 0;
+        idc_check( idc_ctx_create( &d, &this->ctx ), "idc_ctx_create" );
+
+        const int64_t nq = op.nq();
+        std::vector<double> xi( nq ), eta( nq ), w( nq );
+        for ( int64_t q = 0; q < nq; ++q ) {
+            xi[q] = op.xi(q);
+            eta[q] = op.eta(q);
+            w[q] = op.w(q);
+        }
+        const int64_t qb[5] = { op.Quadrants(0), op.Quadrants(1), op.Quadrants(2), op.Quadrants(3),
+                                op.Quadrants(4) };
+        idc_check( idc_set_ordinates( this->ctx, nq, xi.data(), eta.data(), w.data(), qb ), "idc_set_ordinates" );
+    }
+
+public:
+
+    ~SweepPatternGPU ( void ) override {  idc_ctx_destroy( this->ctx );  }
+
+    static const std::string Descriptor ( void ) {  return "gpu-wavefront";  }
+    const std::string GetDescriptor ( void ) const override {  return Descriptor();  }
+
+    // SweepPattern::Sweep: result <- L^{-1} source with the inflow values in the ghost cells of `source`.
+    void Sweep ( const OrdinateFlux & source, OrdinateFlux & result, const RKDG::CrossSection & sigma,
+                 const RKDG::OrdinateFlux * const /* initial_condition: not used by a direct sweep */ ) const override {
+
+        if ( this->sweep_octants_in_sequence )   // reflecting boundaries (SweepPatternUniCart.cpp:46-88)
+            throw std::runtime_error( "gpu-wavefront: reflecting boundaries are not supported" );
+
+        idc_check( idc_set_sigma( this->ctx, sigma.PointerAtCell( 0, 0 ), nullptr, IDC_LOC_HOST ), "idc_set_sigma" );
+        const double dt = this->sw_op.sweep_cell_solve->GetDt();   // set by SweepOperator::Apply
+        if ( &source == &result ) {
+            idc_check( idc_sweep( this->ctx, result.PointerAtCell( 0, 0 ), dt, nullptr, IDC_PREC_FP64, IDC_LOC_HOST ),
+                       "idc_sweep" );
+        } else {
+            idc_check( idc_sweep_out( this->ctx, source.PointerAtCell( 0, 0 ), result.PointerAtCell( 0, 0 ), dt,
+                                      nullptr, IDC_PREC_FP64, IDC_LOC_HOST ), "idc_sweep_out" );
+        }
+    }
+
+private:
+
+    idc_ctx * ctx = nullptr;
+};
+
+
+// Registration under "gpu-wavefront", as the reference's own patterns register (SweepPatternUniCartWavefront.cpp,
+// end of file).
+template class SweepOperator<RKDG::OrdinateFlux>::SweepPatternGPU;
+template class SweepOperator<RKDG::OrdinateFlux>::SweepPattern::SweepPatternDerivedFactory<
+    SweepOperator<RKDG::OrdinateFlux>::SweepPatternGPU >;

@@ -4,11 +4,13 @@ oracle/ref_driver.cpp) on small seeded problems.
 
     python tests/golden/make_golden.py
 
-Each fixture holds the problem inputs (grid, ordinates, cross sections, angular source, dt) and the
-reference's outputs: the in-place sweep (SweepOperator::Apply), phi = Pmv(psi), Lmv(source), Smv and
+Each fixture in this folder holds the problem inputs (grid, ordinates, cross sections, angular source,
+dt) and the reference's outputs: the in-place sweep (SweepOperator::Apply), phi = Pmv(psi), Lmv(source), Smv and
 the source-iteration solution (SISolver::Solve).  The reference publishes no test vectors of its own,
 so these are the pins for the CPU restatement (tests/test_oracle_golden.py) and the CUDA path
-(tests/test_sweep_gpu.py).
+(tests/test_sweep_gpu.py).  config/ holds the reference's results on full-size benchmark problems
+(config/config0_lattice64_q1_s8.npz: its own 64x64 lattice case solved by SISolver::Solve), for the GPU
+tests at those sizes.
 """
 import os
 import sys
@@ -36,8 +38,29 @@ CASES = [
 ]
 
 
+def config0(ref):
+    """The reference's own CPU-runnable case at full size: 64x64 lattice on [0,7]^2, Q1, S8, one implicit-Euler
+    step of dt = 0.01 from zero flux, source iteration to 1e-10 (absolute l2 change of phi, SISolver::Solve).
+    The fixture keeps the inputs' cross sections, the source's checksum, the reference's phi and its psi on
+    64 seeded cells (the whole psi would be 5.6 MB)."""
+    P = lattice(64, 1, 8, dt=0.01)
+    o = OP(P.nx, P.ny, P.p, P.xi, P.eta, P.w, P.quad, P.sigma_t, P.sigma_s, P.ax, P.bx, P.ay, P.by)
+    with ref.open(o, P.dt, abs_tol=1e-10, max_its=5000) as h:
+        psi = h.source_iteration(P.source, P.dt)
+        phi = h.pmv(psi)
+    rng = np.random.default_rng(64)
+    cells = np.stack([rng.integers(1, P.nx + 1, 64), rng.integers(1, P.ny + 1, 64)], axis=1)
+    np.savez_compressed(
+        os.path.join(HERE, "config", "config0_lattice64_q1_s8.npz"), nx=P.nx, ny=P.ny, p=P.p, dt=P.dt,
+        sigma_t=P.sigma_t, sigma_s=P.sigma_s, source_sum=P.source.sum(), source_abs_sum=np.abs(P.source).sum(),
+        si_tol=1e-10, phi=phi, cells=cells, psi_cells=psi[cells[:, 0], cells[:, 1]])
+    print("wrote config0_lattice64_q1_s8", phi.shape)
+
+
 def main():
     ref = Reference()
+    os.makedirs(os.path.join(HERE, "config"), exist_ok=True)
+    config0(ref)
     for name, build in CASES:
         P = build()
         o = OP(P.nx, P.ny, P.p, P.xi, P.eta, P.w, P.quad, P.sigma_t, P.sigma_s, P.ax, P.bx, P.ay, P.by)

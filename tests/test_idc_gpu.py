@@ -102,3 +102,42 @@ def test_imex_idc_degrees_nodes_precisions(restatement, p, M, prec, tol):
         sweeps = ctx.idc_integrate(psi, P.source, P.dt, 2, M, 2, abi.SCATTER_EXPLICIT, prec, use_graph=True)
     assert sweeps == 2 * 3 * (M - 1)
     assert rel_err(psi[1:-1, 1:-1], want[1:-1, 1:-1]) < tol
+
+
+@pytest.mark.parametrize("case", [
+    dict(kind="lattice", n=10, p=1, sn=4, M=4, K=3, steps=3),
+    dict(kind="random", n=7, p=2, sn=8, M=4, K=3, steps=2),
+    dict(kind="random", n=6, p=1, sn=12, M=3, K=2, steps=2),
+])
+def test_implicit_idc_matches_reference_integrator(reference, case):
+    """The GPU's implicit IDC (GMRES substeps to 1e-14) against the reference's own IDCIntegrator (oracle/_ref:
+    IDCIntegrator::Step, update form, Gauss-Lobatto nodes, SISolver substeps to 1e-14), vacuum boundaries."""
+    if case["kind"] == "lattice":
+        P = lattice(case["n"], case["p"], case["sn"], dt=0.01)
+    else:
+        P = random_problem(case["n"], case["n"] + 1, case["p"], case["sn"], seed=31, dt=0.05, inflow=False,
+                           sigma_range=(0.5, 4.0))
+    psi0 = np.zeros(P.psi_shape())
+    psi0[1:-1, 1:-1] = 0.05
+    with reference.open(to_oracle(P), P.dt, abs_tol=1e-14, max_its=100000) as h:
+        want = h.idc_steps(psi0, P.source, P.dt, case["steps"], case["M"], case["K"], si_abs_tol=1e-14)
+    with context_for(P) as ctx:
+        psi = psi0.copy()
+        ctx.idc_integrate(psi, P.source, P.dt, case["steps"], case["M"], case["K"], abi.SCATTER_IMPLICIT,
+                          abi.PREC_FP64, abs_tol=1e-14)
+    assert rel_err(psi[1:-1, 1:-1], want[1:-1, 1:-1]) < 1e-10
+
+
+def test_implicit_idc_with_inflow_stepwise_matches_reference_integrator(reference):
+    """With inflow data the reference zeroes the ghost cells of each step's result; one GPU step per call
+    with the ghost cells zeroed in between reproduces its multi-step result."""
+    P = random_problem(6, 5, 1, 8, seed=3, dt=0.05, inflow=True, sigma_range=(0.5, 4.0))
+    psi0 = np.zeros(P.psi_shape())
+    with reference.open(to_oracle(P), P.dt, abs_tol=1e-14, max_its=100000) as h:
+        want = h.idc_steps(psi0, P.source, P.dt, 3, 4, 3, si_abs_tol=1e-14)
+    psi = psi0.copy()
+    with context_for(P) as ctx:
+        for _ in range(3):
+            ctx.idc_integrate(psi, P.source, P.dt, 1, 4, 3, abi.SCATTER_IMPLICIT, abi.PREC_FP64, abs_tol=1e-14)
+            psi[0], psi[-1], psi[:, 0], psi[:, -1] = 0.0, 0.0, 0.0, 0.0
+    assert rel_err(psi, want) < 1e-10

@@ -1,0 +1,69 @@
+"""The drop-in boundary seen from the reference's side: the reference solver, compiled from its own
+sources, with the GPU sweep pattern plugged into its factory (oracle/sweep_pattern_gpu.cpp, deck key
+`sweep_pattern gpu-wavefront`, oracle/_ref/libidcref_gpu.so).  The reference's own SweepOperator::Apply,
+SISolver::Solve and IDCIntegrator::Step run unchanged on top of it; their results must match the same
+reference code with its CPU wavefront pattern."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import gpu_available, rel_err, to_oracle
+from idcsweep.problems import lattice, random_problem
+from oracle.bindings import REFERENCE_GPU_SO, Reference
+
+pytestmark = pytest.mark.skipif(not os.path.exists(REFERENCE_GPU_SO),
+                                reason="oracle/_ref/libidcref_gpu.so not built (needs the reference sources)")
+
+
+@pytest.fixture(scope="module")
+def plugged():
+    return Reference(REFERENCE_GPU_SO)
+
+
+@pytest.mark.skipif(gpu_available(), reason="checks the failure without a GPU")
+def test_plugin_fails_loudly_without_a_gpu(plugged):
+    """No CUDA device: creating the pattern throws (the reference's error style) and the driver reports it;
+    nothing falls back to a CPU sweep."""
+    P = random_problem(4, 3, 1, 4, seed=1)
+    with pytest.raises(RuntimeError):
+        plugged.open(to_oracle(P), P.dt, pattern="gpu-wavefront")
+    with plugged.open(to_oracle(P), P.dt, pattern="wavefront") as h:   # the CPU patterns still work
+        assert np.isfinite(h.sweep(P.source, P.dt)).all()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("p,sn,dt", [(0, 4, 0.5), (1, 8, np.inf), (2, 12, 0.05)])
+def test_reference_apply_through_plugin(plugged, p, sn, dt):
+    P = random_problem(13, 9, p, sn, seed=50 + p, dt=dt)
+    with plugged.open(to_oracle(P), P.dt, pattern="wavefront") as h:
+        want = h.sweep(P.source, P.dt)
+    with plugged.open(to_oracle(P), P.dt, pattern="gpu-wavefront") as h:
+        got = h.sweep(P.source, P.dt)
+    assert rel_err(got, want) < 1e-12
+
+
+@pytest.mark.gpu
+def test_reference_source_iteration_through_plugin(plugged):
+    """SISolver::Solve (SISolver.cpp:190-254) on the reference's 64x64 lattice case, gpu-wavefront against
+    wavefront."""
+    P = lattice(64, 1, 8, dt=0.01)
+    out = {}
+    for pattern in ("wavefront", "gpu-wavefront"):
+        with plugged.open(to_oracle(P), P.dt, pattern=pattern, abs_tol=1e-10, max_its=5000) as h:
+            psi = h.source_iteration(P.source, P.dt)
+            out[pattern] = h.pmv(psi)
+    assert rel_err(out["gpu-wavefront"], out["wavefront"]) < 1e-12
+
+
+@pytest.mark.gpu
+def test_reference_idc_integrator_through_plugin(plugged):
+    """IDCIntegrator::Step (idc.cpp:521, 846-955) with SISolver substeps, sweeping on the GPU."""
+    P = random_problem(12, 10, 1, 8, seed=61, dt=0.05, inflow=False, sigma_range=(0.5, 4.0))
+    psi0 = np.zeros(P.psi_shape())
+    psi0[1:-1, 1:-1] = 0.05
+    out = {}
+    for pattern in ("wavefront", "gpu-wavefront"):
+        with plugged.open(to_oracle(P), P.dt, pattern=pattern, abs_tol=1e-13, max_its=100000) as h:
+            out[pattern] = h.idc_steps(psi0, P.source, P.dt, 2, 4, 3, si_abs_tol=1e-13)
+    assert rel_err(out["gpu-wavefront"], out["wavefront"]) < 1e-11

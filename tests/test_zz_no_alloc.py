@@ -75,7 +75,7 @@ def test_noalloc_rejects_oversized_problems():
     xi, eta, w = d(P.xi), d(P.eta), d(P.w)
     dummy = torch.zeros(16, dtype=torch.float64, device="cuda")
     # S2 has one ordinate per quadrant: 16 rows per item, so 4 * 70000/16 items exceed the fixed scratch
-    rc = abi.sweep_noalloc(2, 70000, 0.0, 1.0, 0.0, 1.0, 0, xi.data_ptr(), eta.data_ptr(), w.data_ptr(), P.nq,
+    rc = abi.sweep_noalloc(2, 70000, 0, 0.0, 1.0, 0.0, 1.0, xi.data_ptr(), eta.data_ptr(), w.data_ptr(), P.nq,
                            P.quad, dummy.data_ptr(), dummy.data_ptr(), dummy.data_ptr())
     assert rc == abi.IDC_ERR_ARG
     msg = abi.load_library().idc_last_error_message().decode()
