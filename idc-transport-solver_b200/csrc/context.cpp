@@ -87,10 +87,10 @@ Status Context::init() {
     IDC_TRY_CUDA(cudaEventCreate(&ev0));
     IDC_TRY_CUDA(cudaEventCreate(&ev1));
     IDC_TRY_CUDA(cudaMalloc(&d_scalar_, sizeof(double) * (4 + multidot_scratch_doubles())));   // + dot scratch
-    // IDC_SWEEP_KERNEL=warp|rowsync selects one of the elimination kernels instead of the modal one
+    // IDC_SWEEP_KERNEL=modal|warp|rowsync selects another sweep kernel than the lane-pipelined one
     if (const char *k = std::getenv("IDC_SWEEP_KERNEL")) {
         const std::string v(k);
-        kernel = v == "rowsync" ? kRowSync : v == "warp" ? kWarp : kModal;
+        kernel = v == "rowsync" ? kRowSync : v == "warp" ? kWarp : v == "modal" ? kModal : kLane;
     }
     use_warp_kernel = kernel != kRowSync;
     return Status::ok();
@@ -160,6 +160,12 @@ Status Context::set_tiling(int G, int R) {
     return Status::ok();
 }
 
+// The lane kernel sweeps in FP64; the FP32 modes run on the modal kernel.
+int Context::kernel_for(int precision) const {
+    if (kernel == kLane && !sweep_lane_supports(P, precision, 4)) return kModal;
+    return kernel;
+}
+
 Status Context::set_tile_shape(int s, int w) {
     if (s == 0 && w == 0) {
         tune_seg = tune_wn = 0;
@@ -176,14 +182,16 @@ Status Context::set_tile_shape(int s, int w) {
 
 // Candidate tile shapes, timed with CUDA events on this problem (best of three sweeps after a warm-up).
 Status Context::autotune(const double *src, double dt, int precision, int *seg_out, int *wn_out) {
-    if (kernel != kModal) return bad(IDC_ERR_UNSUPPORTED, "the autotuner tunes the modal kernel");
+    if (!modal_family()) return bad(IDC_ERR_UNSUPPORTED, "the autotuner tunes the lane and modal kernels");
     IDC_TRY(ensure_psi_buffers(1));
     IDC_TRY(ensure_phi_buffers(1));
     float best = 1e30f;
     int bs = 0, bw = 0;
-    const int mw = sweep_modal_max_wn(P);
+    const bool lane = kernel_for(precision) == kLane;   // lane kernel: segment widths only, one warp per item
+    const int mw = lane ? 1 : sweep_modal_max_wn(P);
     for (int cs : {4, 8, 16, 32})
         for (int cw = std::max(1, mw - 3); cw <= mw; ++cw) {
+            if (lane && !sweep_lane_supports(P, precision, cs)) continue;
             IDC_TRY(set_tile_shape(cs, cw));
             float ms = 1e30f;
             for (int rep = 0; rep < 4; ++rep) {   // one warm-up, then the best of three
@@ -270,18 +278,26 @@ Status Context::build_schedule(int precision) {
     for (int k = 0; k < 4; ++k) qmax = std::max<int>(qmax, (int)(quad[k + 1] - quad[k]));
     if (qmax == 0) return bad(IDC_ERR_ARG, "no ordinates");
     int G = 0, R = 0;
-    const int max_wn = kernel == kModal ? sweep_modal_max_wn(P) : 7;
+    active = kernel_for(precision);
+    const int max_wn = active == kModal ? sweep_modal_max_wn(P) : active == kLane ? 1 : 7;
+    const bool modal_like = active == kModal || active == kLane;
     if (use_warp_kernel && tune_seg > 0) {
         seg = tune_seg;
+        if (active == kLane && !sweep_lane_supports(P, precision, seg)) seg = 16;
         wn = std::min(tune_wn, max_wn);
         const int nch = (qmax + seg - 1) / seg;
         G = (qmax + nch - 1) / nch;
-        if (kernel == kModal) wn = sweep_modal_fit_wn(P, precision, wn, G, seg);
+        if (active == kModal) wn = sweep_modal_fit_wn(P, precision, wn, G, seg);
         R = wn * (32 / seg);
     } else if (use_warp_kernel) {
-        choose_warp_tiling(qmax, user_G, user_R, max_wn, kernel == kModal ? sweep_modal_default_wn(P) : 7,
-                           kernel == kModal, &G, &seg, &wn);
-        if (kernel == kModal) wn = sweep_modal_fit_wn(P, precision, wn, G, seg);
+        choose_warp_tiling(qmax, user_G, user_R, max_wn, active == kModal ? sweep_modal_default_wn(P) : max_wn,
+                           modal_like, &G, &seg, &wn);
+        if (active == kLane && !sweep_lane_supports(P, precision, seg)) {   // 32 lanes: 16 and two chunks
+            seg = 16;
+            const int nch = (qmax + seg - 1) / seg;
+            G = (qmax + nch - 1) / nch;
+        }
+        if (active == kModal) wn = sweep_modal_fit_wn(P, precision, wn, G, seg);
         R = wn * (32 / seg);
     } else {
         const int max_threads = 320;
@@ -343,7 +359,7 @@ Status Context::build_schedule(int precision) {
     if (use_warp_kernel) {
         cudaFree(d_trace);
         d_trace = nullptr;
-        const size_t tl = (size_t)n_items * nx * G * (kernel == kModal ? P : N);
+        const size_t tl = (size_t)n_items * nx * G * (modal_like ? P : N);
         IDC_TRY_CUDA(cudaMalloc(&d_trace, sizeof(double) * tl));
         trace_len = tl;
         IDC_TRY_CUDA(launch_fill_u64(reinterpret_cast<unsigned long long *>(d_trace), tl, kTraceSentinel, stream));
@@ -351,11 +367,15 @@ Status Context::build_schedule(int precision) {
     }
 
     int per_sm = 0;
-    if (kernel == kModal) {
+    if (active == kLane) {
+        block = sweep_lane_warps() * 32;
+        smem = 0;   // fixed per kernel instance (set by the launcher)
+        IDC_TRY_CUDA(sweep_lane_occupancy(P, seg, false, &per_sm));
+    } else if (active == kModal) {
         block = sweep_modal_threads(P, wn);
         smem = sweep_modal_smem_bytes(P, precision, wn, G, seg);
         IDC_TRY_CUDA(sweep_modal_occupancy(P, precision, seg, block, smem, &per_sm));
-    } else if (kernel == kWarp) {
+    } else if (active == kWarp) {
         block = (wn + 1) * 32;
         smem = sweep_warp_smem_bytes(P, wn, G, seg);
         IDC_TRY_CUDA(sweep_warp_occupancy(P, precision, block, smem, &per_sm));
@@ -365,7 +385,10 @@ Status Context::build_schedule(int precision) {
         IDC_TRY_CUDA(sweep_occupancy(P, precision, block, smem, &per_sm));
     }
     if (per_sm < 1) return bad(IDC_ERR_UNSUPPORTED, "sweep kernel does not fit on an SM with this tiling");
-    grid = std::min(n_items, per_sm * num_sms);
+    if (active == kLane)   // one item per warp at a time
+        grid = std::min((n_items + sweep_lane_warps() - 1) / sweep_lane_warps(), per_sm * num_sms);
+    else
+        grid = std::min(n_items, per_sm * num_sms);
     occupancy_precision = precision;
     return Status::ok();
 }
@@ -441,15 +464,17 @@ Status Context::sweep(const double *src, double *out, double dt, double *phi, in
     if (!(dt > 0)) return bad(IDC_ERR_ARG, "dt must be positive (+inf for steady state)");
     if ((!src || !out) && !use_warp_kernel)
         return bad(IDC_ERR_UNSUPPORTED, "a sweep without source or output array needs the warp-pipelined kernel");
-    if (adjoint && (kernel != kModal || precision == IDC_PREC_FP32))
+    if (adjoint && (!modal_family() || precision == IDC_PREC_FP32))
         return bad(IDC_ERR_UNSUPPORTED, "the transposed sweep needs the modal kernel in FP64 or refined precision");
-    if (src2 && (adjoint || kernel != kModal || !src))
+    if (src2 && (adjoint || !modal_family() || !src))
         return bad(IDC_ERR_UNSUPPORTED, "a second source needs a forward modal sweep with a first source");
     IDC_TRY(build_schedule(precision));
     IDC_TRY_CUDA(cudaSetDevice(device));
 
     size_t launch_smem = smem;
-    if (src2) {
+    if (src2 && active == kLane) {
+        // the lane kernel has its own instance with the second source's stages
+    } else if (src2) {
         int limit = 0;
         IDC_TRY_CUDA(cudaDeviceGetAttribute(&limit, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
         if (precision != IDC_PREC_FP32 && smem + sweep_modal_src2_bytes(P, wn) <= (size_t)limit) {
@@ -501,7 +526,7 @@ Status Context::sweep(const double *src, double *out, double dt, double *phi, in
     a.seg = seg;
     a.wn = wn;
     a.trace = d_trace;
-    a.trace_stride = (size_t)nx * tiling.G * (kernel == kModal ? P : N);
+    a.trace_stride = (size_t)nx * tiling.G * ((active == kModal || active == kLane) ? P : N);
     a.next_item = d_sync;
     a.error = d_sync + 1;
     a.progress = d_sync + 2;
@@ -528,8 +553,8 @@ Status Context::sweep(const double *src, double *out, double dt, double *phi, in
     IDC_TRY_CUDA(cudaMemsetAsync(d_sync, 0, sizeof(int), stream));
     IDC_TRY_CUDA(cudaMemsetAsync(d_sync + 2, 0, sizeof(int) * n_items, stream));
     if (a.phi) IDC_TRY_CUDA(cudaMemsetAsync(phi, 0, sizeof(double) * phi_len(), stream));
-    if (kernel != kModal && !capturing) IDC_TRY_CUDA(cudaEventRecord(ev0, stream));
-    if (kernel == kModal) {
+    if (active != kModal && active != kLane && !capturing) IDC_TRY_CUDA(cudaEventRecord(ev0, stream));
+    if (active == kModal || active == kLane) {
         if (src && !adjoint) {   // inflow traces of the ghost cells (packed modal, or physical for the refined mode)
             const size_t need = (size_t)(nx + ny) * nq * P;
             if (inflow_len < need) {
@@ -559,8 +584,11 @@ Status Context::sweep(const double *src, double *out, double dt, double *phi, in
             a.sigma_s = nullptr;
         }
         if (!capturing) IDC_TRY_CUDA(cudaEventRecord(ev0, stream));   // the timing covers the sweep kernel alone
-        IDC_TRY_CUDA(launch_sweep_modal(P, precision, a, grid, launch_smem, stream));
-    } else if (kernel == kWarp)
+        if (active == kLane)
+            IDC_TRY_CUDA(launch_sweep_lane(P, a, grid, stream));
+        else
+            IDC_TRY_CUDA(launch_sweep_modal(P, precision, a, grid, launch_smem, stream));
+    } else if (active == kWarp)
         IDC_TRY_CUDA(launch_sweep_warp(P, precision, a, grid, smem, stream));
     else
         IDC_TRY_CUDA(launch_sweep(P, precision, a, grid, block, smem, stream));

@@ -124,11 +124,16 @@ public:
     SweepItem *d_items = nullptr;
     int n_items = 0;
     int *d_sync = nullptr;        // [0] queue head, [1] error word, [2..] progress per item
-    // sweep kernel: modal (sweep_modal.cu, default), warp-pipelined with elimination (sweep_warp.cu) or
-    // row-synchronous (sweep_kernels.cu)
-    enum Kernel { kRowSync = 0, kWarp = 1, kModal = 2 };
-    int kernel = kModal;
-    bool use_warp_kernel = true;   // kernel is kWarp or kModal (same schedule and trace protocol)
+    // sweep kernel: lane-pipelined (sweep_lane.cu, default; FP64 sweeps), modal (sweep_modal.cu; every
+    // precision, and the FP32 modes when kLane is selected), warp-pipelined with elimination (sweep_warp.cu)
+    // or row-synchronous (sweep_kernels.cu)
+    enum Kernel { kRowSync = 0, kWarp = 1, kModal = 2, kLane = 3 };
+    int kernel = kLane;
+    int active = kLane;            // the kernel the current schedule was built for (kernel_for(precision))
+    bool use_warp_kernel = true;   // kernel is kWarp, kModal or kLane (same trace protocol)
+    // the modal cell arithmetic (modal or lane kernel): the transposed sweep, IDC, batches
+    bool modal_family() const { return kernel == kModal || kernel == kLane; }
+    int kernel_for(int precision) const;
     int seg = 0, wn = 0;           // warp kernel tiling
     double *d_trace = nullptr;     // warp / modal kernel: per-item last-row traces (sentinel-armed)
     double *d_inflow = nullptr;    // modal kernel: inflow traces of the ghost cells

@@ -139,7 +139,7 @@ Status Context::idc_integrate(double *psi, const double *Q, double dt, int64_t s
     if (!(dt > 0) || !std::isfinite(dt)) return bad(IDC_ERR_ARG, "IDC needs a finite positive dt");
     if (steps < 0) return bad(IDC_ERR_ARG, "negative step count");
     if (scattering != 0 && scattering != 1) return bad(IDC_ERR_ARG, "scattering must be 0 (explicit) or 1 (implicit)");
-    if (kernel != kModal) return bad(IDC_ERR_UNSUPPORTED, "IDC needs the modal sweep kernel");
+    if (!modal_family()) return bad(IDC_ERR_UNSUPPORTED, "IDC needs the modal sweep kernel");
     std::vector<double> t, W;
     idc_nodes_and_weights(M, t, W);
 

@@ -233,7 +233,7 @@ Status Context::apply_peierls_adjoint(const double *x, double *y, double *tmp_ph
 // lam_out (psi-sized, nullable) and Lam_out = sum_q lam_q (moment-sized) are device arrays.
 Status Context::adjoint_solve(const double *detector, double *lam_out, double *Lam_out, double dt, double abs_tol,
                               int restart, int64_t max_its, int precision, int64_t *iters, double *resid_out) {
-    if (kernel != kModal) return bad(IDC_ERR_UNSUPPORTED, "the adjoint needs the modal sweep kernel");
+    if (!modal_family()) return bad(IDC_ERR_UNSUPPORTED, "the adjoint needs the modal sweep kernel");
     IDC_TRY(ensure_phi_buffers(8));
     double *mu = phi_buf(6), *tmp = phi_buf(7);
     bool converged = false;
@@ -268,7 +268,7 @@ Status Context::adjoint_gradient(const double *psi, const double *detector, doub
 
 Status Context::adjoint_solve_psi(const double *b, double *lam_out, double *Lam_out, double dt, double abs_tol,
                                   int restart, int64_t max_its, int precision, int64_t *iters) {
-    if (kernel != kModal) return bad(IDC_ERR_UNSUPPORTED, "the adjoint needs the modal sweep kernel");
+    if (!modal_family()) return bad(IDC_ERR_UNSUPPORTED, "the adjoint needs the modal sweep kernel");
     IDC_TRY(ensure_phi_buffers(9));
     double *nu = phi_buf(6), *tmp = phi_buf(7), *rhs = phi_buf(8);
     // rhs = S^T L'^{-T} b: the transposed sweep's moment sums, scaled by sigma_s / (4 pi); ghost cells zero
@@ -304,7 +304,7 @@ Status Context::adjoint_transient(const double *psi0, const double *Q, double dt
                                   int64_t max_its, int precision, double *dsig_t, double *dsig_s, double *dq,
                                   double *dpsi0, double *J, int64_t *solves) {
     if (!have_ordinates || !have_sigma) return bad(IDC_ERR_STATE, "transient adjoint before ordinates and sigma");
-    if (kernel != kModal) return bad(IDC_ERR_UNSUPPORTED, "the adjoint needs the modal sweep kernel");
+    if (!modal_family()) return bad(IDC_ERR_UNSUPPORTED, "the adjoint needs the modal sweep kernel");
     if (steps < 1) return bad(IDC_ERR_ARG, "transient adjoint needs at least one step");
     if (!(dt > 0) || !std::isfinite(dt)) return bad(IDC_ERR_ARG, "transient adjoint needs a finite positive dt");
     const int64_t K = checkpoint_every > 0 ? std::min(checkpoint_every, steps)
