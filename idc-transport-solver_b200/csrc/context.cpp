@@ -160,18 +160,22 @@ Status Context::set_tiling(int G, int R) {
     return Status::ok();
 }
 
-// The lane kernel sweeps in FP64; the FP32 modes run on the modal kernel.
+// The kernel of a sweep at `precision`: with the default (kLane) the one the tile shape names (warps = 0:
+// the lane kernel, else the modal kernel), and without a tile shape the lane kernel; the lane kernel
+// sweeps in FP64 only, the FP32 modes run on the modal kernel.  IDC_SWEEP_KERNEL fixes another kernel.
 int Context::kernel_for(int precision) const {
-    if (kernel == kLane && !sweep_lane_supports(P, precision, 4)) return kModal;
-    return kernel;
+    if (kernel != kLane) return kernel;
+    if (tune_seg > 0 && tune_wn > 0) return kModal;
+    return sweep_lane_supports(P, precision, tune_seg > 0 ? tune_seg : 4) ? kLane : kModal;
 }
 
 Status Context::set_tile_shape(int s, int w) {
     if (s == 0 && w == 0) {
         tune_seg = tune_wn = 0;
     } else {
-        if ((s != 4 && s != 8 && s != 16 && s != 32) || w < 1 || w > 7)
-            return bad(IDC_ERR_ARG, "tile shape: seg must be 4, 8, 16 or 32 and wn in 1..7");
+        if ((s != 4 && s != 8 && s != 16 && s != 32) || w < 0 || w > 7 || (w == 0 && s == 32))
+            return bad(IDC_ERR_ARG, "tile shape: seg must be 4, 8, 16 or 32 and wn in 0..7 (0: the lane kernel, "
+                                    "seg 4, 8 or 16)");
         tune_seg = s;
         tune_wn = w;
     }
@@ -187,11 +191,13 @@ Status Context::autotune(const double *src, double dt, int precision, int *seg_o
     IDC_TRY(ensure_phi_buffers(1));
     float best = 1e30f;
     int bs = 0, bw = 0;
-    const bool lane = kernel_for(precision) == kLane;   // lane kernel: segment widths only, one warp per item
-    const int mw = lane ? 1 : sweep_modal_max_wn(P);
+    // candidates: the lane kernel's segment widths (warps = 0; FP64 and the default kernel choice only), then
+    // the modal kernel's segment widths and compute-warp counts
+    const bool lane = kernel == kLane && sweep_lane_supports(P, precision, 4);
+    const int mw = sweep_modal_max_wn(P);
     for (int cs : {4, 8, 16, 32})
-        for (int cw = std::max(1, mw - 3); cw <= mw; ++cw) {
-            if (lane && !sweep_lane_supports(P, precision, cs)) continue;
+        for (int cw = lane ? 0 : std::max(1, mw - 3); cw <= mw; cw = cw == 0 ? std::max(1, mw - 3) : cw + 1) {
+            if (cw == 0 && !sweep_lane_supports(P, precision, cs)) continue;
             IDC_TRY(set_tile_shape(cs, cw));
             float ms = 1e30f;
             for (int rep = 0; rep < 4; ++rep) {   // one warm-up, then the best of three
@@ -284,7 +290,7 @@ Status Context::build_schedule(int precision) {
     if (use_warp_kernel && tune_seg > 0) {
         seg = tune_seg;
         if (active == kLane && !sweep_lane_supports(P, precision, seg)) seg = 16;
-        wn = std::min(tune_wn, max_wn);
+        wn = tune_wn > 0 ? std::min(tune_wn, max_wn) : (active == kModal ? sweep_modal_default_wn(P) : 1);
         const int nch = (qmax + seg - 1) / seg;
         G = (qmax + nch - 1) / nch;
         if (active == kModal) wn = sweep_modal_fit_wn(P, precision, wn, G, seg);

@@ -8,28 +8,33 @@
 // Every warp is an independent worker with its own work item: Rw = 32/SEG consecutive rows (in sweep
 // order) of one quadrant for one chunk of <= SEG ordinates, swept across all columns.  Lane (rr, o) =
 // (lane / SEG, lane % SEG) owns ordinate q_begin + o on row rr; row rr runs one column behind row rr-1 and
-// takes its y trace by __shfl_up, the x trace stays in the lane.  A step of the warp does, for every lane,
-// everything that cell needs, so there is no hand-off between warps inside a thread block at all:
-//   * the chain: the y trace in, the modal cell step, the traces out (the only cell-to-cell dependency);
-//   * the inputs of the next step: its source dofs (staged in shared memory by cp.async, kStages steps
-//     ahead), sigma_t, the fused scattering moments and second source, the forward modal transform and
-//     the reciprocal denominators -- independent of the chain, so the compiler interleaves them with it;
-//   * the finish of this step: the backward transform, the psi store and the row segment's moment sums
-//     (one partial per ordinate chunk, added in a fixed order by reduce_phi_partials: bitwise
-//     reproducible).
-// A warp has few neighbours on its SM sub-partition (four warps per thread block, one per sub-partition,
-// one or two blocks per SM), so it may hold up to 255 registers and its step is one long stretch of
-// independent instructions around a short dependency chain.
+// takes its y trace by __shfl_up, the x trace stays in the lane.  Iteration s of a warp does, for every
+// lane, all the work of three cells, with no barrier between them, so the compiler can interleave their
+// instructions and each hides the others' latencies:
+//   * the chain of step s: the y trace in, the modal cell step, the traces out (the only dependency from
+//     cell to cell, so the only part whose latency sits on the wavefront's critical path);
+//   * the finish of step s - 1: the backward transform, the psi store, and the row segment's moment sums
+//     by a butterfly of shuffles (one partial per ordinate chunk, each sum a fixed tree, added in a fixed
+//     order by reduce_phi_partials: bitwise reproducible);
+//   * the inputs of step s + 1: its source dofs and sigma_t (and the second source), copied into shared
+//     memory by cp.async kStages - 1 steps ahead, each lane its own (lane o == 0 of a row copies the fused
+//     scattering moments and hands them to its row by shuffles), the forward modal transform and the
+//     reciprocal denominators.
+// The loop body is one iteration for every quadrant (the quadrant's sign flips are applied to the cell
+// values at run time as sign-bit flips, exact), so the hot loop stays small for the instruction caches.
+// Four warps per thread block, one per SM sub-partition; a warp may hold up to 255 registers.  Measured on
+// B200: one warp with enough independent work issues FP64 at the sub-partition's full rate.
 //
 // Between row blocks: the warp's last row writes its outgoing y traces, column by column, into the item's
-// trace buffer with relaxed 8-byte stores; the warp of the item below loads them kTraceAhead steps before
-// it needs them (the loop is unrolled by that depth so that the values stay in registers), finds a slot
-// still holding the NaN-payload sentinel only if it caught up with its producer (then it polls that
-// column, bounded), and writes the sentinel back after use.  The first row block reads the ghost row's
-// inflow traces (inflow_traces_kernel) instead.  Items are dequeued per warp in row-block order from an
-// atomic counter, so an item's producer is always held by a running warp: no deadlock, and no thread
-// block needs any other to be resident.  Every wait is bounded (spin_limit); on expiry the warp records
-// kDevTimeout in the device error word and leaves, and every other warp leaves when it sees the word.
+// trace buffer with relaxed 8-byte stores; row 0 of the item below loads column s + 1 with relaxed loads
+// at iteration s (a whole iteration, longer than an L2 round trip, before use).  A value still holding the
+// NaN-payload sentinel means the consumer has caught up with its producer: it then polls (bounded) until
+// the producer is two columns further, which gives it slack for the next loads.  The consumer writes the
+// sentinel back after use.  The first row block reads the ghost row's inflow traces (inflow_traces_kernel)
+// the same way.  Items are dequeued per warp in row-block order from an atomic counter, so an item's
+// producer is always held by a running warp: no deadlock, and no thread block needs any other to be
+// resident.  Every wait is bounded (spin_limit); on expiry the warp records kDevTimeout in the device
+// error word and leaves, and every other warp leaves when it sees the word.
 //
 // Transposed sweep (ADJ): reverse traversal order per quadrant, the transposed cell operator and coupling
 // of modal_cell.cuh, zero inflow, the fused source w_q * mu and unweighted moment sums (the transposes of
@@ -46,26 +51,87 @@
 namespace idc {
 namespace lane {
 
-constexpr int kWarps = 4;        // warps per thread block: one per SM sub-partition
-constexpr int kStages = 6;       // source stages in shared memory: a step's inputs are loaded this many steps ahead
-constexpr int kTraceAhead = 4;   // row 0's y traces are loaded this many steps before use
+constexpr int kWarps = 4;    // warps per thread block: one per SM sub-partition
+constexpr int kStages = 6;   // stages in shared memory: a step's inputs are copied this many steps minus one ahead
 
-// Shared memory of one warp, in doubles: source stages [kStages][32][N] (lane-major, conflict-free),
-// the second source's stages (launches with one), cell-data stages [kStages][Rw][1 + N] (sigma_t and the
-// fused scattering moments, loaded by lane o == 0 of each row) and the moment reduction buffer [32][N].
+// Doubles per (column, ordinate) slot of the trace buffer.
+__host__ __device__ constexpr int trace_slot(int P) { return P; }
+
+// Shared memory of one warp, in doubles: source stages [kStages][32][N] (lane-major, conflict-free), the
+// second source's stages (launches with one), sigma_t stages [kStages][32] (each lane its own copy) and the
+// fused scattering moments' stages [kStages][Rw][N] (copied by lane o == 0 of each row).
 __host__ __device__ constexpr size_t warp_doubles(int P, int seg, bool src2) {
-    return (size_t)kStages * 32 * P * P * (src2 ? 2 : 1) + (size_t)kStages * (32 / seg) * (P * P + 1) +
-           (size_t)32 * P * P;
+    return (size_t)kStages * 32 * P * P * (src2 ? 2 : 1) + (size_t)kStages * 32 + (size_t)kStages * (32 / seg) * P * P;
 }
 __host__ __device__ constexpr size_t block_smem_bytes(int P, int seg, bool src2) {
     return sizeof(double) * warp_doubles(P, seg, src2) * kWarps;
 }
 
-template <int P, int SEG, bool XN, bool YN, bool ADJ, bool SRC2>
+// x with its sign bit flipped where `mask` has it (mask: 0 or 0x80000000 in the high word).
+__device__ __forceinline__ double flip_by(double x, unsigned mask) {
+    return __hiloint2double(__double2hiint(x) ^ (int)mask, __double2loint(x));
+}
+
+// Sums of v[0 .. N) over the SEG lanes of a row segment (o = lane % SEG) by recursive halving: at the
+// stage of distance h a lane keeps the lower half of its current range if bit h of o is clear, the upper
+// half otherwise, and adds its partner's copy of it (the halves always sit in slots 0 .. len-1).  After
+// log2(SEG) stages lane o holds the sums of k in [*lo, *hi) in slots 0 .. *hi - *lo.  Every sum is a fixed
+// tree over the segment's lanes.
+template <int N, int SEG, int LEN = N, int H = SEG / 2>
+__device__ __forceinline__ void segment_sums(double (&v)[N], int o, int *lo, int *hi) {
+    if constexpr (H >= 1) {
+        constexpr int HALF = (LEN + 1) / 2;
+        const bool upper = (o & H) != 0;
+#pragma unroll
+        for (int i = 0; i < HALF; ++i) {
+            const double keep = upper ? (i + HALF < LEN ? v[i + HALF] : 0.0) : v[i];
+            const double give = upper ? v[i] : (i + HALF < LEN ? v[i + HALF] : 0.0);
+            v[i] = keep + __shfl_xor_sync(kFullMask, give, H);
+        }
+        const int mid = *lo + HALF;
+        if (upper)
+            *lo = mid < *hi ? mid : *hi;
+        else
+            *hi = mid < *hi ? mid : *hi;
+        segment_sums<N, SEG, HALF, H / 2>(v, o, lo, hi);
+    }
+}
+
+// The consumer caught up with its producer (a value of column s still held the sentinel): wait until the
+// producer has written column `last` and all of column s, bounded.  Returns false if the wait gave up or
+// another warp has failed (the error word is then set).  Out of line: the hot loop stays small.
+template <int P>
+__device__ __noinline__ bool wait_for_producer(const double *dep_trace, int s, int last, bool reader, int G,
+                                               int *error, long long spin_limit, long long *polls, int lane) {
+    const size_t col = (size_t)G * P;
+    for (int want = last;;) {
+        bool still = false;
+        if (reader) {
+#pragma unroll
+            for (int m = 0; m < P; ++m) still |= is_sentinel(ld_relaxed_f64(dep_trace + (size_t)want * col + m));
+        }
+        if (!__any_sync(kFullMask, still)) {
+            if (want == s) return true;
+            want = s;
+            continue;
+        }
+        ++*polls;
+        if ((*polls & 63) == 63 && ld_relaxed(error) != kDevOk) return false;
+        if (*polls > spin_limit) {
+            if (lane == 0) atomicCAS(error, kDevOk, kDevTimeout);
+            return false;
+        }
+        __nanosleep(64);
+    }
+}
+
+template <int P, int SEG, bool ADJ, bool SRC2>
 __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &item, int it_index, double *wsm,
                                          int lane) {
-    constexpr int N = P * P, Rw = 32 / SEG, D = kStages, K = kTraceAhead, NC = N + 1;
-    constexpr bool TX = XN != ADJ, TY = YN != ADJ;
+    constexpr int N = P * P, Rw = 32 / SEG, D = kStages;
+    // quadrant signs: flips of the cell values (exact), traversal directions (reversed for the transpose)
+    const bool XN = item.quadrant >= 2, YN = (item.quadrant & 1) != 0;
+    const bool TX = XN != ADJ, TY = YN != ADJ;
     const int rr = lane / SEG, o = lane - rr * SEG;
     const int row_w = item.row_block * Rw;
     const int row = row_w + rr;
@@ -73,17 +139,21 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
     const bool act = (o < item.q_count) && row_valid;
     const int q = item.q_begin + (act ? o : 0);
     const int j = TY ? (a.ny - row) : (1 + row);
-    const int nx = a.nx, G = a.G;
+    const int nx = a.nx;
     const size_t plane = (size_t)a.nq * N;
     const size_t istride = (size_t)(a.ny + 2) * plane;
     const bool has_dep = item.dep >= 0;
     const bool has_consumer = row_w + Rw < a.ny;
     const int T = nx + Rw - 1;
+    const size_t tcol = (size_t)a.G * P;   // doubles per trace column
+    const int xi0 = TX ? nx : 1, xis = TX ? -1 : 1;   // array x index of sweep column c: xi0 + xis * c
+    const unsigned xm = XN ? 0x80000000u : 0u, ym = YN ? 0x80000000u : 0u;
+    auto fmask = [&](int k) { return ((k / P) & 1 ? xm : 0u) ^ ((k % P) & 1 ? ym : 0u); };   // k = e + P d
 
-    double *stage = wsm + (size_t)lane * N;                           // step t at + (t % D) * 32 * N
-    double *stage2 = wsm + (size_t)D * 32 * N + (size_t)lane * N;     // (SRC2 launches only)
-    double *cell = wsm + (size_t)D * 32 * N * (SRC2 ? 2 : 1) + (size_t)rr * NC;   // + (t % D) * Rw * NC
-    double *red = cell - (size_t)rr * NC + (size_t)D * Rw * NC;      // [32][N]
+    double *stage = wsm + (size_t)lane * N;                            // step t at + (t % D) * 32 * N
+    double *stage2 = wsm + (size_t)D * 32 * N + (size_t)lane * N;      // (SRC2 launches only)
+    double *sig = wsm + (size_t)D * 32 * N * (SRC2 ? 2 : 1) + lane;    // + (t % D) * 32
+    double *mom = wsm + (size_t)D * 32 * N * (SRC2 ? 2 : 1) + (size_t)D * 32 + (size_t)rr * N;   // + (t % D) * Rw * N
 
     double axd = 0.0, ayd = 0.0, wq = 0.0;
     if (act) {
@@ -103,32 +173,31 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
         for (int m = 0; m < P; ++m) f[m] = in[m];
     }
 
-    // where row 0 of this item reads its y traces: the item above (sentinel-armed) or the ghost row's inflow
+    // row 0 reads its y traces from the item above (sentinel-armed) or the ghost row's inflow
     const bool reader = rr == 0 && o < item.q_count && row_valid;
     double *dep_trace = has_dep ? a.trace + (size_t)item.dep * a.trace_stride + (size_t)o * P : nullptr;
     const double *inflow_y = (!has_dep && a.inflow && !ADJ) ? a.inflow + (size_t)q * P : nullptr;
+    double *out_trace = a.trace + (size_t)it_index * a.trace_stride + (size_t)o * P;
+    const bool writer = has_consumer && rr == Rw - 1 && o < item.q_count;
     auto load_trace = [&](int c, double (&v)[P]) {
 #pragma unroll
         for (int m = 0; m < P; ++m) v[m] = 0.0;
         if (reader && c < nx) {
             if (has_dep) {
 #pragma unroll
-                for (int m = 0; m < P; ++m) v[m] = ld_relaxed_f64(dep_trace + (size_t)c * G * P + m);
+                for (int m = 0; m < P; ++m) v[m] = ld_relaxed_f64(dep_trace + (size_t)c * tcol + m);
             } else if (inflow_y) {
 #pragma unroll
                 for (int m = 0; m < P; ++m) v[m] = inflow_y[(size_t)c * a.nq * P + m];
             }
         }
     };
-    double *out_trace = a.trace + (size_t)it_index * a.trace_stride + (size_t)o * P;
-    const bool writer = has_consumer && rr == Rw - 1 && o < item.q_count;
 
-    // step t's inputs into stage t % D: the source dofs (every active lane its own), sigma_t and the fused
-    // scattering moments (lane o == 0 of the row); one cp.async group per step, empty past the last
+    // step t's inputs into stage t % D, one cp.async group per step (empty past the last step)
     auto prefetch = [&](int t) {
         const int c = t - rr;
         if (t < T && row_valid && c >= 0 && c < nx) {
-            const int ci = TX ? nx - c : 1 + c;
+            const int ci = xi0 + xis * c;
             const size_t base = (size_t)ci * istride + (size_t)j * plane + (size_t)q * N;
             if (act && a.src) {
                 double *d = stage + (size_t)(t % D) * 32 * N;
@@ -140,23 +209,20 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
 #pragma unroll
                 for (int k = 0; k < N; ++k) cp_async8(d + k, a.src2 + base + k);
             }
-            if (o == 0) {
-                const size_t cidx = (size_t)ci * (a.ny + 2) + j;
-                double *d = cell + (size_t)(t % D) * Rw * NC;
-                cp_async8(d, a.sigma_t + cidx);
-                if (a.phi_scatter) {
+            const size_t cidx = (size_t)ci * (a.ny + 2) + j;
+            cp_async8(sig + (size_t)(t % D) * 32, a.sigma_t + cidx);
+            if (o == 0 && a.phi_scatter) {
+                double *d = mom + (size_t)(t % D) * Rw * N;
 #pragma unroll
-                    for (int k = 0; k < N; ++k) cp_async8(d + 1 + k, a.phi_scatter + cidx * N + k);
-                }
+                for (int k = 0; k < N; ++k) cp_async8(d + k, a.phi_scatter + cidx * N + k);
             }
         }
         cp_commit();
     };
 
-    // step t's modal source and reciprocals from its landed stage
+    // step t's modal source and reciprocals from its landed stage (the caller has waited for its group)
     auto prepare = [&](int t, double (&S)[N], ModalRecip<P, double> &r) {
         const double *sp = stage + (size_t)(t % D) * 32 * N;
-        const double *cp = cell + (size_t)(t % D) * Rw * NC;
         double src[N];
 #pragma unroll
         for (int k = 0; k < N; ++k) src[k] = a.src ? sp[k] : 0.0;
@@ -165,153 +231,125 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
 #pragma unroll
             for (int k = 0; k < N; ++k) src[k] = fma(a.src2_scale, sp2[k], src[k]);
         }
-        if (a.phi_scatter) {
-            if constexpr (!ADJ) {   // fused TransportOperator::Smv(scale, 1, sigma_s, phi -> src)
+        if (a.phi_scatter) {   // lane o == 0's copy of the cell's moments, handed to its row segment
+            const double *mp = mom + (size_t)(t % D) * Rw * N;
 #pragma unroll
-                for (int k = 0; k < N; ++k) src[k] += a.scatter_scale * cp[1 + k];
-            } else {                // the transpose of Pmv: w_q * mu
-#pragma unroll
-                for (int k = 0; k < N; ++k) src[k] = fma(wq, cp[1 + k], src[k]);
+            for (int k = 0; k < N; ++k) {
+                const double mk = __shfl_sync(kFullMask, o == 0 ? mp[k] : 0.0, rr * SEG);
+                if constexpr (!ADJ)   // fused TransportOperator::Smv(scale, 1, sigma_s, phi -> src)
+                    src[k] += a.scatter_scale * mk;
+                else                  // the transpose of Pmv: w_q * mu
+                    src[k] = fma(wq, mk, src[k]);
             }
         }
-        r = modal_recip<P, double>(od, cp[0] + a.inv_dt);
-        modal_forward<P, XN, YN, double, ADJ>(S, src);
+        r = modal_recip<P, double>(od, sig[(size_t)(t % D) * 32] + a.inv_dt);
+#pragma unroll
+        for (int k = 0; k < N; ++k) src[k] = flip_by(src[k], fmask(k));
+        modal_forward<P, false, false, double, ADJ>(S, src);
     };
 
     const int phi_slot = a.phi_slots > 0 ? it_index % a.phi_slots : 0;
     long long polls = 0;
-    bool failed = false;
 
-    // prologue: stages 0 .. D-2 in flight, step 0 prepared, row 0's traces of columns 0 .. K-1 loaded
+    // prologue: stages 0 .. D-2 in flight, step 0 prepared, row 0's trace of column 0 loaded
 #pragma unroll
     for (int t = 0; t < D - 1; ++t) prefetch(t);
     cp_wait<D - 2>();
-    __syncwarp();
     double S[N];
     ModalRecip<P, double> r;
     prepare(0, S, r);
-    double tr[K][P];
-#pragma unroll
-    for (int u = 0; u < K; ++u) load_trace(u, tr[u]);
-    double gprev[P];
+    double tnext[P];
+    load_trace(0, tnext);
+    double gprev[P], Zp[N];
 #pragma unroll
     for (int m = 0; m < P; ++m) gprev[m] = 0.0;
-
-    for (int s0 = 0; s0 < T && !failed; s0 += K) {
 #pragma unroll
-        for (int u = 0; u < K; ++u) {
-            const int s = s0 + u;
-            if (s >= T || failed) break;   // warp-uniform
-            const int c = s - rr;
-            const bool valid = act && c >= 0 && c < nx;
+    for (int k = 0; k < N; ++k) Zp[k] = 0.0;
 
-            // ---- the y trace in: from the lane seg below (previous step), row 0 from the item above ----
-            double g[P];
+    // iteration s: chain of step s (s < T), finish of step s - 1 (s >= 1), inputs of step s + 1
+    for (int s = 0; s <= T; ++s) {
+        const int c = s - rr;
+        const bool valid = act && c >= 0 && c < nx;
+
+        // ---- the y trace in: from the row below (previous step); row 0 from the item above ----
+        double g[P];
 #pragma unroll
-            for (int m = 0; m < P; ++m) g[m] = __shfl_up_sync(kFullMask, gprev[m], SEG);
-            if (has_dep && s < nx) {   // row 0 consumes column s of the item above
+        for (int m = 0; m < P; ++m) g[m] = __shfl_up_sync(kFullMask, gprev[m], SEG);
+        if (s < nx) {   // row 0 consumes column s (loaded an iteration ago)
+            if (has_dep) {
                 bool bad = false;
 #pragma unroll
-                for (int m = 0; m < P; ++m) bad |= reader && is_sentinel(tr[u][m]);
-                if (__any_sync(kFullMask, bad)) {   // caught up with the producer: poll this column, bounded
-                    unsigned ns = 32;
-                    for (;;) {
-                        bool still = false;
-                        if (reader) {
+                for (int m = 0; m < P; ++m) bad |= reader && is_sentinel(tnext[m]);
+                if (__any_sync(kFullMask, bad)) {   // caught up with the producer: wait for two columns of slack
+                    if (!wait_for_producer<P>(dep_trace, s, min(s + 2, nx - 1), reader, a.G, a.error, a.spin_limit,
+                                              &polls, lane))
+                        break;
+                    load_trace(s, tnext);
+                }
+                if (reader) {   // re-arm the consumed column for the next sweep
 #pragma unroll
-                            for (int m = 0; m < P; ++m) {
-                                if (is_sentinel(tr[u][m])) tr[u][m] = ld_relaxed_f64(dep_trace + (size_t)s * G * P + m);
-                                still |= is_sentinel(tr[u][m]);
-                            }
-                        }
-                        if (!__any_sync(kFullMask, still)) break;
-                        ++polls;
-                        if ((polls & 63) == 63 && ld_relaxed(a.error) != kDevOk) {
-                            failed = true;
-                            break;
-                        }
-                        if (polls > a.spin_limit) {
-                            if (lane == 0) atomicCAS(a.error, kDevOk, kDevTimeout);
-                            failed = true;
-                            break;
-                        }
-                        __nanosleep(ns);
-                        ns = ns < 1024 ? ns * 2 : 1024;
-                    }
-                    if (failed) break;
+                    for (int m = 0; m < P; ++m) st_relaxed_f64(dep_trace + (size_t)s * tcol + m, sentinel_value());
                 }
             }
             if (rr == 0) {
 #pragma unroll
-                for (int m = 0; m < P; ++m) g[m] = tr[u][m];
+                for (int m = 0; m < P; ++m) g[m] = tnext[m];
             }
+        }
+        load_trace(s + 1, tnext);
 
-            // ---- the cell step: the chain from cell to cell ----
-            double Z[N], fn[P], gout[P];
+        // ---- the chain of step s ----
+        double Z[N], fn[P], gout[P];
 #pragma unroll
-            for (int m = 0; m < P; ++m) fn[m] = f[m];
-            modal_step<P, double, ADJ>(Z, S, fn, g, gout, od, r);
+        for (int m = 0; m < P; ++m) fn[m] = f[m];
+        modal_step<P, double, ADJ>(Z, S, fn, g, gout, od, r);
 #pragma unroll
-            for (int m = 0; m < P; ++m) {
-                f[m] = valid ? fn[m] : f[m];
-                gprev[m] = valid ? gout[m] : 0.0;
-            }
+        for (int m = 0; m < P; ++m) {
+            f[m] = valid ? fn[m] : f[m];
+            gprev[m] = valid ? gout[m] : 0.0;
+        }
+        const int cout = s - (Rw - 1);   // traces out: relaxed stores, each value its own flag
+        if (writer && cout >= 0 && cout < nx) {
+#pragma unroll
+            for (int m = 0; m < P; ++m) st_relaxed_f64(out_trace + (size_t)cout * tcol + m, gout[m]);
+        }
 
-            // ---- traces out (relaxed stores: each value is its own flag) and row 0's trace bookkeeping ----
-            const int cout = s - (Rw - 1);
-            if (writer && cout >= 0 && cout < nx) {
-#pragma unroll
-                for (int m = 0; m < P; ++m) st_relaxed_f64(out_trace + (size_t)cout * G * P + m, gout[m]);
-            }
-            if (reader && has_dep && s < nx) {   // re-arm the consumed column for the next sweep
-#pragma unroll
-                for (int m = 0; m < P; ++m) st_relaxed_f64(dep_trace + (size_t)s * G * P + m, sentinel_value());
-            }
-            load_trace(s + K, tr[u]);
-
-            // ---- the next step's inputs (independent of the chain) ----
-            prefetch(s + D - 1);   // into the stage step s - 1 used (read while preparing it, a step ago)
-            cp_wait<D - 2>();      // step s + 1's group has landed
-            __syncwarp();   // lane o == 0's cell data of step s + 1 is visible to its row
-            prepare(s + 1, S, r);
-
-            // ---- this step's finish: cell dofs, psi, moments ----
+        // ---- the finish of step s - 1: cell dofs, psi, moments ----
+        if (s >= 1) {   // warp-uniform
+            const int cp = c - 1;
+            const bool vp = act && cp >= 0 && cp < nx;
             double x[N];
-            modal_backward<P, XN, YN, double, ADJ>(x, Z);
-            if (a.out && valid) {
-                double *op = a.out + (size_t)(TX ? nx - c : 1 + c) * istride + (size_t)j * plane + (size_t)q * N;
+            modal_backward<P, false, false, double, ADJ>(x, Zp);
+#pragma unroll
+            for (int k = 0; k < N; ++k) x[k] = flip_by(x[k], fmask(k));
+            if (a.out && vp) {
+                double *op = a.out + (size_t)(xi0 + xis * cp) * istride + (size_t)j * plane + (size_t)q * N;
 #pragma unroll
                 for (int k = 0; k < N; ++k) op[k] = x[k];
             }
             if (a.phi_part) {
 #pragma unroll
-                for (int k = 0; k < N; ++k) red[lane * N + k] = valid ? (ADJ ? x[k] : wq * x[k]) : 0.0;
-                __syncwarp();
-                constexpr int kSums = Rw * N;
+                for (int k = 0; k < N; ++k) x[k] = vp ? (ADJ ? x[k] : wq * x[k]) : 0.0;
+                int lo = 0, hi = N;
+                segment_sums<N, SEG>(x, o, &lo, &hi);
+                if (row_valid && cp >= 0 && cp < nx) {
+                    double *pp = a.phi_part + (size_t)phi_slot * a.phi_slot_stride +
+                                 ((size_t)(xi0 + xis * cp) * (a.ny + 2) + j) * N;
 #pragma unroll
-                for (int mm = 0; mm < (kSums + 31) / 32; ++mm) {
-                    const int t = lane + 32 * mm;
-                    const int r2 = t / N, k = t - (t / N) * N;
-                    const int c2 = s - r2, row2 = row_w + r2;
-                    if (t < kSums && row2 < a.ny && c2 >= 0 && c2 < nx) {
-                        const double *sr = red + (size_t)r2 * SEG * N + k;
-                        double v[SEG];
-#pragma unroll
-                        for (int oo = 0; oo < SEG; ++oo) v[oo] = sr[oo * N];
-#pragma unroll
-                        for (int h = 1; h < SEG; h <<= 1)
-#pragma unroll
-                            for (int oo = 0; oo < SEG; oo += 2 * h) v[oo] += v[oo + h];
-                        const int i2 = TX ? nx - c2 : 1 + c2, j2 = TY ? (a.ny - row2) : (1 + row2);
-                        a.phi_part[(size_t)phi_slot * a.phi_slot_stride + ((size_t)i2 * (a.ny + 2) + j2) * N + k] = v[0];
-                    }
+                    for (int i = 0; i < (N + SEG - 1) / SEG; ++i)
+                        if (lo + i < hi) pp[lo + i] = x[i];
                 }
-                __syncwarp();   // the sums are read before the next step overwrites the buffer
             }
         }
+#pragma unroll
+        for (int k = 0; k < N; ++k) Zp[k] = Z[k];
+
+        // ---- the inputs of step s + 1 ----
+        prefetch(s + D - 1);   // into the stage of step s - 1 (read an iteration ago)
+        cp_wait<D - 2>();      // step s + 1's group has landed
+        prepare(s + 1, S, r);
     }
     cp_wait<0>();
-    __syncwarp();
 }
 
 template <int P, int SEG, bool ADJ, bool SRC2>
@@ -327,13 +365,7 @@ __global__ void __launch_bounds__(kWarps * 32, 1) sweep_lane_kernel(const SweepA
         }
         it = __shfl_sync(kFullMask, it, 0);
         if (it >= a.n_items) return;
-        const SweepItem item = a.items[it];
-        switch (item.quadrant) {
-            case 0: run_item<P, SEG, false, false, ADJ, SRC2>(a, item, it, wsm, lane); break;
-            case 1: run_item<P, SEG, false, true, ADJ, SRC2>(a, item, it, wsm, lane); break;
-            case 2: run_item<P, SEG, true, false, ADJ, SRC2>(a, item, it, wsm, lane); break;
-            default: run_item<P, SEG, true, true, ADJ, SRC2>(a, item, it, wsm, lane); break;
-        }
+        run_item<P, SEG, ADJ, SRC2>(a, a.items[it], it, wsm, lane);
     }
 }
 

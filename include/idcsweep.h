@@ -213,12 +213,15 @@ int idc_sweep_fused(idc_ctx *ctx, const double *source, double *result, double d
 /* ---- tile shapes and batches ------------------------------------------------------------------------- */
 
 /* Tile shape of the sweep kernel: ordinates per row segment (seg: 4, 8, 16 or 32) and compute warps per
- * thread block (1..7; the modal kernel uses at most 5 at DG degree 2 and 7 below, and fewer if the shape's
- * shared memory would not fit); 0, 0 restores the default heuristic.  Results do not depend on it. */
+ * thread block.  warps = 0 selects the lane-pipelined kernel (every warp sweeps its own row block of 32/seg
+ * rows; seg 4, 8 or 16; FP64 sweeps); warps 1..7 the modal kernel with that many compute warps stacked per
+ * thread block (at most 5 at DG degree 2 and 7 below, fewer if the shape's shared memory would not fit).
+ * 0, 0 restores the default (the lane kernel for FP64, the modal kernel for the FP32 modes).  Results do
+ * not depend on it beyond the last bits of the moments. */
 int idc_set_tile_shape(idc_ctx *ctx, int32_t seg, int32_t warps);
 
-/* Autotuner: times every tile shape on this context's problem with `source` (device psi array) and keeps
- * the fastest (reported in *seg, *warps). */
+/* Autotuner: times every tile shape of both kernels on this context's problem with `source` (device psi
+ * array) and keeps the fastest (reported in *seg, *warps; warps = 0: the lane kernel). */
 int idc_autotune(idc_ctx *ctx, const double *source, double dt, int precision, int32_t *seg, int32_t *warps);
 
 /* A batch of independent problems (contexts on one GPU) swept together: one persistent launch per DG

@@ -131,6 +131,27 @@ def test_tiling_does_not_change_psi():
         assert np.array_equal(o, out[0])
 
 
+@pytest.mark.parametrize("p,sn,dt", [(2, 16, np.inf), (1, 12, 0.05), (0, 4, 1.0)])
+def test_lane_and_modal_kernels_agree_on_every_tile_shape(restatement, p, sn, dt):
+    """The lane-pipelined kernel (warps = 0) and the modal kernel (warps >= 1) do the same cell arithmetic:
+    psi is bitwise the same for every tile shape of either; phi differs only in the order of its sums."""
+    P = random_problem(37, 45, p, sn, seed=70 + p, dt=dt)
+    ref = restatement.sweep(to_oracle(P), P.source, P.dt)
+    shapes = [(4, 0), (8, 0), (16, 0), (4, 4), (8, 3), (16, 2), (32, 1), (0, 0)]
+    outs = []
+    with context_for(P) as ctx:
+        for shape in shapes:
+            ctx.set_tile_shape(*shape)
+            psi = P.source.copy()
+            phi = np.zeros(P.phi_shape())
+            ctx.sweep(psi, P.dt, phi, abi.PREC_FP64)
+            outs.append((psi, phi))
+    assert rel_err(outs[0][0], ref) < 1e-12
+    for psi, phi in outs[1:]:
+        assert np.array_equal(psi, outs[0][0])
+        assert rel_err(phi, outs[0][1]) < 1e-14
+
+
 def test_bad_ordinates_rejected():
     P = random_problem(4, 4, 1, 4, seed=1)
     with abi.SweepContext(4, 4, 1) as ctx:
