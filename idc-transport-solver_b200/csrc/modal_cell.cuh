@@ -96,9 +96,10 @@ __device__ __forceinline__ ModalOrdinate<P, T> modal_ordinate(double axd, double
         o.pp_im_m = T((axd + ayd) * Tab::nu(0));
     }
     if constexpr (Tab::kPairs > 0 && Tab::kHasReal) {
-        o.pr_re = T(axd * Tab::mu(0) + ayd * Tab::lam_real());
+        // explicit fused multiply-adds: every kernel that inlines this rounds these sums the same way
+        o.pr_re = T(fma(axd, Tab::mu(0), ayd * Tab::lam_real()));
         o.pr_im = T(axd * Tab::nu(0));
-        o.rp_re = T(axd * Tab::lam_real() + ayd * Tab::mu(0));
+        o.rp_re = T(fma(axd, Tab::lam_real(), ayd * Tab::mu(0)));
         o.rp_im = T(ayd * Tab::nu(0));
     }
     if constexpr (Tab::kHasReal) o.rr_re = T((axd + ayd) * Tab::lam_real());

@@ -237,7 +237,7 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
             for (int k = 0; k < N; ++k) {
                 const double mk = __shfl_sync(kFullMask, o == 0 ? mp[k] : 0.0, rr * SEG);
                 if constexpr (!ADJ)   // fused TransportOperator::Smv(scale, 1, sigma_s, phi -> src)
-                    src[k] += a.scatter_scale * mk;
+                    src[k] = fma(a.scatter_scale, mk, src[k]);
                 else                  // the transpose of Pmv: w_q * mu
                     src[k] = fma(wq, mk, src[k]);
             }

@@ -154,7 +154,7 @@ __device__ __forceinline__ void prep_cell(CellIn<P, MODE> &in, const double *sp,
         if constexpr (!ADJ) {   // fused TransportOperator::Smv(scale, 1, sigma_s, phi -> src); the moments
                                 // sigma_s phi / (4 pi) come from launch_scatter_moments (no division here)
 #pragma unroll
-            for (int k = 0; k < N; ++k) src[k] += a.scatter_scale * cp[1 + k];
+            for (int k = 0; k < N; ++k) src[k] = fma(a.scatter_scale, cp[1 + k], src[k]);
         } else {                // adjoint: the transpose of Pmv, w_q * mu
 #pragma unroll
             for (int k = 0; k < N; ++k) src[k] = fma(wq, cp[1 + k], src[k]);
