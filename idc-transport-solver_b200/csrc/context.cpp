@@ -57,6 +57,7 @@ Context::~Context() {
     cudaFree(d_inflow);
     cudaFree(d_scat);
     cudaFree(d_src2mix);
+    cudaFree(d_msrc);
     cudaFree(d_krylov);
     cudaFree(d_small);
     cudaFreeHost(h_small);
@@ -93,6 +94,8 @@ Status Context::init() {
         kernel = v == "rowsync" ? kRowSync : v == "warp" ? kWarp : v == "modal" ? kModal : kLane;
     }
     use_warp_kernel = kernel != kRowSync;
+    // IDC_MOMENTS_FAST_PATH=0 sweeps the Krylov iterations through the per-ordinate transforms as well
+    if (const char *f = std::getenv("IDC_MOMENTS_FAST_PATH")) moments_fast_path = std::string(f) != "0";
     return Status::ok();
 }
 
@@ -331,6 +334,8 @@ Status Context::build_schedule(int precision) {
             beg += sz;
         }
     }
+    quad_slots[0] = 0;   // the partial-moment slots (items of a row block) of each quadrant
+    for (int k = 0; k < 4; ++k) quad_slots[k + 1] = quad_slots[k] + (int)chunks[k].size();
     std::vector<int> prev_index;   // index of the same (quadrant, chunk) in the previous row block
     for (int rb = 0; rb < nrb; ++rb) {
         std::vector<int> cur_index;
@@ -555,6 +560,10 @@ Status Context::sweep(const double *src, double *out, double dt, double *phi, in
         a.phi_slot_stride = phi_len();
     }
 
+    // moments-only forward sweeps (the Krylov iterations) on the lane kernel: no per-ordinate transforms
+    const bool phi_only = active == kLane && !src && !out && phi && !adjoint && !src2 && precision == IDC_PREC_FP64 &&
+                          a.phi_part && moments_fast_path;
+
     // queue head and progress flags start at zero; the error word is kept until checked
     IDC_TRY_CUDA(cudaMemsetAsync(d_sync, 0, sizeof(int), stream));
     IDC_TRY_CUDA(cudaMemsetAsync(d_sync + 2, 0, sizeof(int) * n_items, stream));
@@ -589,6 +598,21 @@ Status Context::sweep(const double *src, double *out, double dt, double *phi, in
             a.phi_scatter = d_scat;
             a.sigma_s = nullptr;
         }
+        if (phi_only) {   // the scattering source in the packed modal basis, once per (cell, quadrant)
+            const size_t need = sig_len() * 4 * N;
+            if (msrc_len < need) {
+                if (capturing) return bad(IDC_ERR_STATE, "modal source buffer allocation inside a stream capture");
+                cudaFree(d_msrc);
+                d_msrc = nullptr;
+                msrc_len = 0;
+                IDC_TRY_CUDA(cudaMalloc(&d_msrc, sizeof(double) * need));
+                msrc_len = need;
+            }
+            IDC_TRY_CUDA(launch_modal_sources(dims(), a.phi_scatter, scatter_scale, d_msrc, stream));
+            launches += 1;
+            a.modal_src = d_msrc;
+            a.phi_scatter = nullptr;
+        }
         if (!capturing) IDC_TRY_CUDA(cudaEventRecord(ev0, stream));   // the timing covers the sweep kernel alone
         if (active == kLane)
             IDC_TRY_CUDA(launch_sweep_lane(P, a, grid, stream));
@@ -600,7 +624,10 @@ Status Context::sweep(const double *src, double *out, double dt, double *phi, in
         IDC_TRY_CUDA(launch_sweep(P, precision, a, grid, block, smem, stream));
     if (!capturing) IDC_TRY_CUDA(cudaEventRecord(ev1, stream));
     launches += 1;
-    if (a.phi_part) {
+    if (a.phi_part && phi_only) {
+        IDC_TRY_CUDA(launch_reduce_modal_partials(dims(), d_phi_part, quad_slots, phi_len(), phi, stream));
+        launches += 1;
+    } else if (a.phi_part) {
         IDC_TRY_CUDA(launch_reduce_phi_partials(dims(), d_phi_part, items_per_rb, phi_len(), phi, stream));
         launches += 1;
     }

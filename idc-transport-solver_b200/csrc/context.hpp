@@ -141,6 +141,10 @@ public:
     double *d_scat = nullptr;      // modal kernel: the fused scattering source's moments sigma_s phi / (4 pi)
     size_t scat_len = 0;
     double *d_src2mix = nullptr;   // src + scale src2 when the second source's stages do not fit
+    double *d_msrc = nullptr;      // lane kernel, moments-only sweeps: packed modal sources [(nx+2)(ny+2)][4][N]
+    size_t msrc_len = 0;
+    bool moments_fast_path = true;
+    int quad_slots[5] = {0, 0, 0, 0, 0};   // partial-moment slots of each quadrant within a row block
     size_t src2mix_len = 0;
     size_t trace_len = 0;
     int items_per_rb = 0;          // work items per row block (= ordinate chunks over all quadrants)

@@ -70,6 +70,9 @@ struct SweepArgs {
     long long spin_limit;      // polls before a wait gives up
     int adjoint;               // modal kernel: 1 = transposed sweep (reverse order; phi_scatter is mu and the
                                // fused source is w_q mu; the moments are unweighted sums over ordinates)
+    const double *modal_src;   // lane kernel, moments-only forward sweeps: the packed modal source of every
+                               // (cell, quadrant), [(nx+2)(ny+2)][4][N] (launch_modal_sources), or null; the
+                               // partial moments are then packed modal sums (launch_reduce_modal_partials)
 };
 
 // Launch geometry picked by the host (autotuner or defaults).
@@ -139,6 +142,16 @@ struct GridDims {
     int nx, ny, nq, P;
     double dx, dy;
 };
+// Moments-only forward sweeps (no source array, psi not stored) on the lane kernel: the source of a cell is
+// the isotropic scattering source, the same for every ordinate of a quadrant, so its packed modal transform
+// is formed once per (cell, quadrant): out[(cell * 4 + k) * N + m] = W flip_k(scale * moments) W^T (moments
+// = sigma_s phi / (4 pi) of launch_scatter_moments, null for none).  The sweep then sums w_q Z in the packed
+// basis per ordinate chunk, and the reduction transforms each quadrant's sum back once per cell:
+// phi = sum_k flip_k(V (sum_{slots of k} part) V^T), slots [slot_begin[k], slot_begin[k+1]) of quadrant k,
+// interior cells in a fixed order, ghost cells zero.
+cudaError_t launch_modal_sources(const GridDims &g, const double *moments, double scale, double *out, cudaStream_t s);
+cudaError_t launch_reduce_modal_partials(const GridDims &g, const double *part, const int slot_begin[5], size_t stride,
+                                         double *phi, cudaStream_t s);
 cudaError_t launch_pmv(const GridDims &g, double alpha, double beta, const double *w, const double *psi,
                        double *phi, cudaStream_t s);
 cudaError_t launch_smv(const GridDims &g, double alpha, double beta, const double *sigma_s, const double *phi,

@@ -39,7 +39,11 @@
 // Transposed sweep (ADJ): reverse traversal order per quadrant, the transposed cell operator and coupling
 // of modal_cell.cuh, zero inflow, the fused source w_q * mu and unweighted moment sums (the transposes of
 // Smv's broadcast and of Pmv).  SRC2 adds a second source, fma(src2_scale, src2, src), as the IDC source
-// kernel combines them.  FP64 arithmetic (the reference's).
+// kernel combines them.  PHI: the moments-only forward sweep of the Krylov iterations (no source array,
+// psi not stored): the cell's source is its isotropic scattering source, the same for every ordinate of a
+// quadrant, read already in the packed modal basis (launch_modal_sources, once per cell and quadrant), and
+// the moments are summed in the packed basis (launch_reduce_modal_partials transforms each quadrant's sum
+// back once per cell), so neither modal transform is done per ordinate.  FP64 arithmetic (the reference's).
 #pragma once
 
 #include "device_sync.cuh"
@@ -52,7 +56,7 @@ namespace idc {
 namespace lane {
 
 constexpr int kWarps = 4;    // warps per thread block: one per SM sub-partition
-constexpr int kStages = 6;   // stages in shared memory: a step's inputs are copied this many steps minus one ahead
+constexpr int kStages = 8;   // stages in shared memory (a power of two): a step's inputs are copied this many steps minus one ahead
 
 // Doubles per (column, ordinate) slot of the trace buffer.
 __host__ __device__ constexpr int trace_slot(int P) { return P; }
@@ -125,7 +129,7 @@ __device__ __noinline__ bool wait_for_producer(const double *dep_trace, int s, i
     }
 }
 
-template <int P, int SEG, bool ADJ, bool SRC2>
+template <int P, int SEG, bool ADJ, bool SRC2, bool PHI>
 __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &item, int it_index, double *wsm,
                                          int lane) {
     constexpr int N = P * P, Rw = 32 / SEG, D = kStages;
@@ -199,7 +203,14 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
         if (t < T && row_valid && c >= 0 && c < nx) {
             const int ci = xi0 + xis * c;
             const size_t base = (size_t)ci * istride + (size_t)j * plane + (size_t)q * N;
-            if (act && a.src) {
+            const size_t cidx = (size_t)ci * (a.ny + 2) + j;
+            if (PHI && act) {   // the cell's packed modal source of this quadrant (the same for the row segment)
+                double *d = stage + (size_t)(t % D) * 32 * N;
+                const double *g = a.modal_src + (cidx * 4 + item.quadrant) * N;
+#pragma unroll
+                for (int k = 0; k < N; ++k) cp_async8(d + k, g + k);
+            }
+            if (!PHI && act && a.src) {
                 double *d = stage + (size_t)(t % D) * 32 * N;
 #pragma unroll
                 for (int k = 0; k < N; ++k) cp_async8(d + k, a.src + base + k);
@@ -209,9 +220,8 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
 #pragma unroll
                 for (int k = 0; k < N; ++k) cp_async8(d + k, a.src2 + base + k);
             }
-            const size_t cidx = (size_t)ci * (a.ny + 2) + j;
             cp_async8(sig + (size_t)(t % D) * 32, a.sigma_t + cidx);
-            if (o == 0 && a.phi_scatter) {
+            if (!PHI && o == 0 && a.phi_scatter) {
                 double *d = mom + (size_t)(t % D) * Rw * N;
 #pragma unroll
                 for (int k = 0; k < N; ++k) cp_async8(d + k, a.phi_scatter + cidx * N + k);
@@ -223,6 +233,12 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
     // step t's modal source and reciprocals from its landed stage (the caller has waited for its group)
     auto prepare = [&](int t, double (&S)[N], ModalRecip<P, double> &r) {
         const double *sp = stage + (size_t)(t % D) * 32 * N;
+        if constexpr (PHI) {
+#pragma unroll
+            for (int k = 0; k < N; ++k) S[k] = sp[k];
+            r = modal_recip<P, double>(od, sig[(size_t)(t % D) * 32] + a.inv_dt);
+            return;
+        }
         double src[N];
 #pragma unroll
         for (int k = 0; k < N; ++k) src[k] = a.src ? sp[k] : 0.0;
@@ -231,7 +247,7 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
 #pragma unroll
             for (int k = 0; k < N; ++k) src[k] = fma(a.src2_scale, sp2[k], src[k]);
         }
-        if (a.phi_scatter) {   // lane o == 0's copy of the cell's moments, handed to its row segment
+        if (!PHI && a.phi_scatter) {   // lane o == 0's copy of the cell's moments, handed to its row segment
             const double *mp = mom + (size_t)(t % D) * Rw * N;
 #pragma unroll
             for (int k = 0; k < N; ++k) {
@@ -314,15 +330,20 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
             for (int m = 0; m < P; ++m) st_relaxed_f64(out_trace + (size_t)cout * tcol + m, gout[m]);
         }
 
-        // ---- the finish of step s - 1: cell dofs, psi, moments ----
-        if (s >= 1) {   // warp-uniform
+        // ---- the finish of step s - 1: cell dofs, psi, moments (PHI: the packed modal moments) ----
+        {   // (at s = 0 nothing is valid: Zp is zero and no store is made)
             const int cp = c - 1;
             const bool vp = act && cp >= 0 && cp < nx;
             double x[N];
-            modal_backward<P, false, false, double, ADJ>(x, Zp);
+            if constexpr (PHI) {
 #pragma unroll
-            for (int k = 0; k < N; ++k) x[k] = flip_by(x[k], fmask(k));
-            if (a.out && vp) {
+                for (int k = 0; k < N; ++k) x[k] = Zp[k];
+            } else {
+                modal_backward<P, false, false, double, ADJ>(x, Zp);
+#pragma unroll
+                for (int k = 0; k < N; ++k) x[k] = flip_by(x[k], fmask(k));
+            }
+            if (!PHI && a.out && vp) {
                 double *op = a.out + (size_t)(xi0 + xis * cp) * istride + (size_t)j * plane + (size_t)q * N;
 #pragma unroll
                 for (int k = 0; k < N; ++k) op[k] = x[k];
@@ -352,7 +373,7 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
     cp_wait<0>();
 }
 
-template <int P, int SEG, bool ADJ, bool SRC2>
+template <int P, int SEG, bool ADJ, bool SRC2, bool PHI>
 __global__ void __launch_bounds__(kWarps * 32, 1) sweep_lane_kernel(const SweepArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -365,13 +386,13 @@ __global__ void __launch_bounds__(kWarps * 32, 1) sweep_lane_kernel(const SweepA
         }
         it = __shfl_sync(kFullMask, it, 0);
         if (it >= a.n_items) return;
-        run_item<P, SEG, ADJ, SRC2>(a, a.items[it], it, wsm, lane);
+        run_item<P, SEG, ADJ, SRC2, PHI>(a, a.items[it], it, wsm, lane);
     }
 }
 
-template <int P, int SEG, bool ADJ, bool SRC2>
+template <int P, int SEG, bool ADJ, bool SRC2, bool PHI = false>
 cudaError_t launch(const SweepArgs &args, int grid, cudaStream_t stream) {
-    auto kern = sweep_lane_kernel<P, SEG, ADJ, SRC2>;
+    auto kern = sweep_lane_kernel<P, SEG, ADJ, SRC2, PHI>;
     const size_t smem = block_smem_bytes(P, SEG, SRC2);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -381,7 +402,7 @@ cudaError_t launch(const SweepArgs &args, int grid, cudaStream_t stream) {
 
 template <int P, int SEG, bool ADJ, bool SRC2>
 cudaError_t occupancy(int *blocks_per_sm) {
-    auto kern = sweep_lane_kernel<P, SEG, ADJ, SRC2>;
+    auto kern = sweep_lane_kernel<P, SEG, ADJ, SRC2, false>;
     const size_t smem = block_smem_bytes(P, SEG, SRC2);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;

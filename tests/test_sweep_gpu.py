@@ -152,6 +152,33 @@ def test_lane_and_modal_kernels_agree_on_every_tile_shape(restatement, p, sn, dt
         assert rel_err(phi, outs[0][1]) < 1e-14
 
 
+@pytest.mark.parametrize("p,sn,dt", [(2, 16, np.inf), (1, 8, 0.2), (0, 4, np.inf)])
+def test_moments_only_sweep_matches_per_ordinate_sweep(restatement, p, sn, dt):
+    """The Krylov iterations' sweep (no source array, psi not stored, moments of the fused scattering source
+    out) runs on the lane kernel without per-ordinate transforms (modal sources per cell and quadrant, moments
+    summed in the packed basis); its moments must match the per-ordinate path (modal kernel) and P L^-1 S
+    of the restatement."""
+    torch = pytest.importorskip("torch")
+    P = random_problem(33, 29, p, sn, seed=90 + p, dt=dt, inflow=False)
+    rng = np.random.default_rng(3)
+    x = np.zeros(P.phi_shape())
+    x[1:-1, 1:-1] = rng.uniform(0.1, 1.0, x[1:-1, 1:-1].shape)
+    xd = torch.from_numpy(x).cuda()
+    outs = []
+    for shape in ((4, 0), (8, 0), (16, 0), (4, 4)):   # lane kernel (moments-only path) and modal kernel
+        with context_for(P) as ctx:
+            ctx.set_tile_shape(*shape)
+            phi = torch.zeros(P.phi_shape(), dtype=torch.float64, device="cuda")
+            ctx.sweep_fused(None, None, P.dt, xd.data_ptr(), 1.0, phi.data_ptr())
+            outs.append(phi.cpu().numpy())
+    OP = to_oracle(P)
+    src = restatement.smv(OP, x, np.zeros(P.psi_shape()), 1.0, 0.0)   # S x on interior cells
+    want = restatement.pmv(OP, restatement.sweep(OP, src, P.dt))
+    for phi in outs:
+        assert rel_err(phi, want) < 1e-12
+        assert rel_err(phi, outs[-1]) < 1e-13
+
+
 def test_bad_ordinates_rejected():
     P = random_problem(4, 4, 1, 4, seed=1)
     with abi.SweepContext(4, 4, 1) as ctx:
