@@ -483,7 +483,7 @@ Status Context::sweep(const double *src, double *out, double dt, double *phi, in
     IDC_TRY_CUDA(cudaSetDevice(device));
 
     size_t launch_smem = smem;
-    if (src2 && active == kLane) {
+    if (src2 && active == kLane && precision == IDC_PREC_FP64) {
         // the lane kernel has its own instance with the second source's stages
     } else if (src2) {
         int limit = 0;
@@ -561,8 +561,7 @@ Status Context::sweep(const double *src, double *out, double dt, double *phi, in
     }
 
     // moments-only forward sweeps (the Krylov iterations) on the lane kernel: no per-ordinate transforms
-    const bool phi_only = active == kLane && !src && !out && phi && !adjoint && !src2 && precision == IDC_PREC_FP64 &&
-                          a.phi_part && moments_fast_path;
+    const bool phi_only = active == kLane && !src && !out && phi && !adjoint && !src2 && a.phi_part && moments_fast_path;
 
     // queue head and progress flags start at zero; the error word is kept until checked
     IDC_TRY_CUDA(cudaMemsetAsync(d_sync, 0, sizeof(int), stream));
@@ -615,7 +614,7 @@ Status Context::sweep(const double *src, double *out, double dt, double *phi, in
         }
         if (!capturing) IDC_TRY_CUDA(cudaEventRecord(ev0, stream));   // the timing covers the sweep kernel alone
         if (active == kLane)
-            IDC_TRY_CUDA(launch_sweep_lane(P, a, grid, stream));
+            IDC_TRY_CUDA(launch_sweep_lane(P, precision, a, grid, stream));
         else
             IDC_TRY_CUDA(launch_sweep_modal(P, precision, a, grid, launch_smem, stream));
     } else if (active == kWarp)

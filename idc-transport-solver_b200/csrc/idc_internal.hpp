@@ -95,11 +95,12 @@ constexpr int kWarpRingSlots = 8;
 constexpr int kModalSolutionSlots = 4;   // modal kernel: step results in flight per compute warp
 
 // Lane-pipelined sweep kernel (sweep_lane.cu): every warp an independent worker on one item of 32/seg rows
-// (R = 32/seg, G <= seg), FP64, forward (optionally with src2) or transposed; `grid` thread blocks of
+// (R = 32/seg, G <= seg); FP64 forward (optionally with src2), transposed or moments-only, and FP32
+// (IDC_PREC_FP32) forward or moments-only sweeps; `grid` thread blocks of
 // sweep_lane_warps() warps.  Same arguments and trace protocol as the modal kernel.
 bool sweep_lane_supports(int P, int precision, int seg);
 int sweep_lane_warps();
-cudaError_t launch_sweep_lane(int P, const SweepArgs &args, int grid, cudaStream_t stream);
+cudaError_t launch_sweep_lane(int P, int precision, const SweepArgs &args, int grid, cudaStream_t stream);
 cudaError_t sweep_lane_occupancy(int P, int seg, bool src2, int *blocks_per_sm);
 
 // Modal sweep kernel (sweep_modal.cu): same arguments as the warp kernel plus `inflow`, traces of P values.

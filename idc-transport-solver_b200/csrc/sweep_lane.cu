@@ -6,18 +6,26 @@ namespace idc {
 
 namespace {
 
-template <int P, bool ADJ, bool SRC2, bool PHI = false>
+template <int P, bool ADJ, bool SRC2, bool PHI = false, typename TC = double>
 cudaError_t launch_p(const SweepArgs &args, int grid, cudaStream_t stream) {
     switch (args.seg) {
-        case 4: return lane::launch<P, 4, ADJ, SRC2, PHI>(args, grid, stream);
-        case 8: return lane::launch<P, 8, ADJ, SRC2, PHI>(args, grid, stream);
-        case 16: return lane::launch<P, 16, ADJ, SRC2, PHI>(args, grid, stream);
+        case 4: return lane::launch<P, 4, ADJ, SRC2, PHI, TC>(args, grid, stream);
+        case 8: return lane::launch<P, 8, ADJ, SRC2, PHI, TC>(args, grid, stream);
+        case 16: return lane::launch<P, 16, ADJ, SRC2, PHI, TC>(args, grid, stream);
         default: return cudaErrorInvalidValue;
     }
 }
 
 template <int P>
-cudaError_t launch_dir(const SweepArgs &args, int grid, cudaStream_t stream) {
+cudaError_t launch_dir(const SweepArgs &args, int grid, cudaStream_t stream, bool fp32) {
+    if (fp32) {   // FP32 arithmetic: forward sweeps, with or without psi
+        if (args.adjoint || args.src2) return cudaErrorInvalidValue;
+        if (args.modal_src) {
+            if (args.src || args.out || !args.phi_part) return cudaErrorInvalidValue;
+            return launch_p<P, false, false, true, float>(args, grid, stream);
+        }
+        return launch_p<P, false, false, false, float>(args, grid, stream);
+    }
     if (args.modal_src) {   // moments-only forward sweep
         if (args.adjoint || args.src2 || args.src || args.out || !args.phi_part) return cudaErrorInvalidValue;
         return launch_p<P, false, false, true>(args, grid, stream);
@@ -109,17 +117,19 @@ cudaError_t occ_p(int seg, bool src2, int *n) {
 }  // namespace
 
 bool sweep_lane_supports(int P, int precision, int seg) {
-    return P >= 1 && P <= 3 && precision == 0 && (seg == 4 || seg == 8 || seg == 16);
+    return P >= 1 && P <= 3 && (precision == 0 || precision == 2) && (seg == 4 || seg == 8 || seg == 16);
 }
 
 int sweep_lane_warps() { return lane::kWarps; }
 
-cudaError_t launch_sweep_lane(int P, const SweepArgs &args, int grid, cudaStream_t stream) {
+cudaError_t launch_sweep_lane(int P, int precision, const SweepArgs &args, int grid, cudaStream_t stream) {
     if (!args.trace || args.G > args.seg || args.R != 32 / args.seg) return cudaErrorInvalidValue;
+    if (precision != 0 && precision != 2) return cudaErrorInvalidValue;
+    const bool fp32 = precision == 2;
     switch (P) {
-        case 1: return launch_dir<1>(args, grid, stream);
-        case 2: return launch_dir<2>(args, grid, stream);
-        case 3: return launch_dir<3>(args, grid, stream);
+        case 1: return launch_dir<1>(args, grid, stream, fp32);
+        case 2: return launch_dir<2>(args, grid, stream, fp32);
+        case 3: return launch_dir<3>(args, grid, stream, fp32);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -43,7 +43,9 @@
 // psi not stored): the cell's source is its isotropic scattering source, the same for every ordinate of a
 // quadrant, read already in the packed modal basis (launch_modal_sources, once per cell and quadrant), and
 // the moments are summed in the packed basis (launch_reduce_modal_partials transforms each quadrant's sum
-// back once per cell), so neither modal transform is done per ordinate.  FP64 arithmetic (the reference's).
+// back once per cell), so neither modal transform is done per ordinate.  TC is the arithmetic: double (the
+// reference's FP64) or float (the unrefined FP32 sweep of IDC_PREC_FP32: FP32 cell arithmetic and moment
+// sums, FP64 arrays and traces), forward sweeps only.
 #pragma once
 
 #include "device_sync.cuh"
@@ -71,25 +73,27 @@ __host__ __device__ constexpr size_t block_smem_bytes(int P, int seg, bool src2)
     return sizeof(double) * warp_doubles(P, seg, src2) * kWarps;
 }
 
-// x with its sign bit flipped where `mask` has it (mask: 0 or 0x80000000 in the high word).
+// x with its sign bit flipped where `mask` has it (mask: 0 or 0x80000000, the sign bit of a float or of a
+// double's high word).
 __device__ __forceinline__ double flip_by(double x, unsigned mask) {
     return __hiloint2double(__double2hiint(x) ^ (int)mask, __double2loint(x));
 }
+__device__ __forceinline__ float flip_by(float x, unsigned mask) { return __int_as_float(__float_as_int(x) ^ (int)mask); }
 
 // Sums of v[0 .. N) over the SEG lanes of a row segment (o = lane % SEG) by recursive halving: at the
 // stage of distance h a lane keeps the lower half of its current range if bit h of o is clear, the upper
 // half otherwise, and adds its partner's copy of it (the halves always sit in slots 0 .. len-1).  After
 // log2(SEG) stages lane o holds the sums of k in [*lo, *hi) in slots 0 .. *hi - *lo.  Every sum is a fixed
 // tree over the segment's lanes.
-template <int N, int SEG, int LEN = N, int H = SEG / 2>
-__device__ __forceinline__ void segment_sums(double (&v)[N], int o, int *lo, int *hi) {
+template <int N, int SEG, int LEN = N, int H = SEG / 2, typename T>
+__device__ __forceinline__ void segment_sums(T (&v)[N], int o, int *lo, int *hi) {
     if constexpr (H >= 1) {
         constexpr int HALF = (LEN + 1) / 2;
         const bool upper = (o & H) != 0;
 #pragma unroll
         for (int i = 0; i < HALF; ++i) {
-            const double keep = upper ? (i + HALF < LEN ? v[i + HALF] : 0.0) : v[i];
-            const double give = upper ? v[i] : (i + HALF < LEN ? v[i + HALF] : 0.0);
+            const T keep = upper ? (i + HALF < LEN ? v[i + HALF] : T(0)) : v[i];
+            const T give = upper ? v[i] : (i + HALF < LEN ? v[i + HALF] : T(0));
             v[i] = keep + __shfl_xor_sync(kFullMask, give, H);
         }
         const int mid = *lo + HALF;
@@ -97,7 +101,7 @@ __device__ __forceinline__ void segment_sums(double (&v)[N], int o, int *lo, int
             *lo = mid < *hi ? mid : *hi;
         else
             *hi = mid < *hi ? mid : *hi;
-        segment_sums<N, SEG, HALF, H / 2>(v, o, lo, hi);
+        segment_sums<N, SEG, HALF, H / 2, T>(v, o, lo, hi);
     }
 }
 
@@ -129,7 +133,7 @@ __device__ __noinline__ bool wait_for_producer(const double *dep_trace, int s, i
     }
 }
 
-template <int P, int SEG, bool ADJ, bool SRC2, bool PHI>
+template <int P, int SEG, bool ADJ, bool SRC2, bool PHI, typename TC>
 __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &item, int it_index, double *wsm,
                                          int lane) {
     constexpr int N = P * P, Rw = 32 / SEG, D = kStages;
@@ -165,16 +169,16 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
         ayd = fabs(a.eta[q]) / a.dy;
         wq = a.w[q];
     }
-    const ModalOrdinate<P, double> od = modal_ordinate<P, double, ADJ>(axd, ayd);
+    const ModalOrdinate<P, TC> od = modal_ordinate<P, TC, ADJ>(axd, ayd);
 
     // the row's x trace entering its first column (ghost-column inflow; zero for the transposed sweep)
-    double f[P];
+    TC f[P];
 #pragma unroll
-    for (int m = 0; m < P; ++m) f[m] = 0.0;
+    for (int m = 0; m < P; ++m) f[m] = TC(0);
     if (act && a.inflow && !ADJ) {
         const double *in = a.inflow + ((size_t)(nx + row) * a.nq + q) * P;
 #pragma unroll
-        for (int m = 0; m < P; ++m) f[m] = in[m];
+        for (int m = 0; m < P; ++m) f[m] = TC(in[m]);
     }
 
     // row 0 reads its y traces from the item above (sentinel-armed) or the ghost row's inflow
@@ -231,12 +235,12 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
     };
 
     // step t's modal source and reciprocals from its landed stage (the caller has waited for its group)
-    auto prepare = [&](int t, double (&S)[N], ModalRecip<P, double> &r) {
+    auto prepare = [&](int t, TC (&S)[N], ModalRecip<P, TC> &r) {
         const double *sp = stage + (size_t)(t % D) * 32 * N;
         if constexpr (PHI) {
 #pragma unroll
-            for (int k = 0; k < N; ++k) S[k] = sp[k];
-            r = modal_recip<P, double>(od, sig[(size_t)(t % D) * 32] + a.inv_dt);
+            for (int k = 0; k < N; ++k) S[k] = TC(sp[k]);
+            r = modal_recip<P, TC>(od, TC(sig[(size_t)(t % D) * 32] + a.inv_dt));
             return;
         }
         double src[N];
@@ -258,10 +262,11 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
                     src[k] = fma(wq, mk, src[k]);
             }
         }
-        r = modal_recip<P, double>(od, sig[(size_t)(t % D) * 32] + a.inv_dt);
+        r = modal_recip<P, TC>(od, TC(sig[(size_t)(t % D) * 32] + a.inv_dt));
+        TC sv[N];
 #pragma unroll
-        for (int k = 0; k < N; ++k) src[k] = flip_by(src[k], fmask(k));
-        modal_forward<P, false, false, double, ADJ>(S, src);
+        for (int k = 0; k < N; ++k) sv[k] = flip_by(TC(src[k]), fmask(k));
+        modal_forward<P, false, false, TC, ADJ>(S, sv);
     };
 
     const int phi_slot = a.phi_slots > 0 ? it_index % a.phi_slots : 0;
@@ -271,16 +276,16 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
 #pragma unroll
     for (int t = 0; t < D - 1; ++t) prefetch(t);
     cp_wait<D - 2>();
-    double S[N];
-    ModalRecip<P, double> r;
+    TC S[N];
+    ModalRecip<P, TC> r;
     prepare(0, S, r);
     double tnext[P];
     load_trace(0, tnext);
-    double gprev[P], Zp[N];
+    TC gprev[P], Zp[N];
 #pragma unroll
-    for (int m = 0; m < P; ++m) gprev[m] = 0.0;
+    for (int m = 0; m < P; ++m) gprev[m] = TC(0);
 #pragma unroll
-    for (int k = 0; k < N; ++k) Zp[k] = 0.0;
+    for (int k = 0; k < N; ++k) Zp[k] = TC(0);
 
     // iteration s: chain of step s (s < T), finish of step s - 1 (s >= 1), inputs of step s + 1
     for (int s = 0; s <= T; ++s) {
@@ -288,7 +293,7 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
         const bool valid = act && c >= 0 && c < nx;
 
         // ---- the y trace in: from the row below (previous step); row 0 from the item above ----
-        double g[P];
+        TC g[P];
 #pragma unroll
         for (int m = 0; m < P; ++m) g[m] = __shfl_up_sync(kFullMask, gprev[m], SEG);
         if (s < nx) {   // row 0 consumes column s (loaded an iteration ago)
@@ -309,48 +314,48 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
             }
             if (rr == 0) {
 #pragma unroll
-                for (int m = 0; m < P; ++m) g[m] = tnext[m];
+                for (int m = 0; m < P; ++m) g[m] = TC(tnext[m]);
             }
         }
         load_trace(s + 1, tnext);
 
         // ---- the chain of step s ----
-        double Z[N], fn[P], gout[P];
+        TC Z[N], fn[P], gout[P];
 #pragma unroll
         for (int m = 0; m < P; ++m) fn[m] = f[m];
-        modal_step<P, double, ADJ>(Z, S, fn, g, gout, od, r);
+        modal_step<P, TC, ADJ>(Z, S, fn, g, gout, od, r);
 #pragma unroll
         for (int m = 0; m < P; ++m) {
             f[m] = valid ? fn[m] : f[m];
-            gprev[m] = valid ? gout[m] : 0.0;
+            gprev[m] = valid ? gout[m] : TC(0);
         }
         const int cout = s - (Rw - 1);   // traces out: relaxed stores, each value its own flag
         if (writer && cout >= 0 && cout < nx) {
 #pragma unroll
-            for (int m = 0; m < P; ++m) st_relaxed_f64(out_trace + (size_t)cout * tcol + m, gout[m]);
+            for (int m = 0; m < P; ++m) st_relaxed_f64(out_trace + (size_t)cout * tcol + m, double(gout[m]));
         }
 
         // ---- the finish of step s - 1: cell dofs, psi, moments (PHI: the packed modal moments) ----
         {   // (at s = 0 nothing is valid: Zp is zero and no store is made)
             const int cp = c - 1;
             const bool vp = act && cp >= 0 && cp < nx;
-            double x[N];
+            TC x[N];
             if constexpr (PHI) {
 #pragma unroll
                 for (int k = 0; k < N; ++k) x[k] = Zp[k];
             } else {
-                modal_backward<P, false, false, double, ADJ>(x, Zp);
+                modal_backward<P, false, false, TC, ADJ>(x, Zp);
 #pragma unroll
                 for (int k = 0; k < N; ++k) x[k] = flip_by(x[k], fmask(k));
             }
             if (!PHI && a.out && vp) {
                 double *op = a.out + (size_t)(xi0 + xis * cp) * istride + (size_t)j * plane + (size_t)q * N;
 #pragma unroll
-                for (int k = 0; k < N; ++k) op[k] = x[k];
+                for (int k = 0; k < N; ++k) op[k] = double(x[k]);
             }
             if (a.phi_part) {
 #pragma unroll
-                for (int k = 0; k < N; ++k) x[k] = vp ? (ADJ ? x[k] : wq * x[k]) : 0.0;
+                for (int k = 0; k < N; ++k) x[k] = vp ? (ADJ ? x[k] : TC(wq) * x[k]) : TC(0);
                 int lo = 0, hi = N;
                 segment_sums<N, SEG>(x, o, &lo, &hi);
                 if (row_valid && cp >= 0 && cp < nx) {
@@ -358,7 +363,7 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
                                  ((size_t)(xi0 + xis * cp) * (a.ny + 2) + j) * N;
 #pragma unroll
                     for (int i = 0; i < (N + SEG - 1) / SEG; ++i)
-                        if (lo + i < hi) pp[lo + i] = x[i];
+                        if (lo + i < hi) pp[lo + i] = double(x[i]);
                 }
             }
         }
@@ -373,7 +378,7 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
     cp_wait<0>();
 }
 
-template <int P, int SEG, bool ADJ, bool SRC2, bool PHI>
+template <int P, int SEG, bool ADJ, bool SRC2, bool PHI, typename TC>
 __global__ void __launch_bounds__(kWarps * 32, 1) sweep_lane_kernel(const SweepArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -386,13 +391,13 @@ __global__ void __launch_bounds__(kWarps * 32, 1) sweep_lane_kernel(const SweepA
         }
         it = __shfl_sync(kFullMask, it, 0);
         if (it >= a.n_items) return;
-        run_item<P, SEG, ADJ, SRC2, PHI>(a, a.items[it], it, wsm, lane);
+        run_item<P, SEG, ADJ, SRC2, PHI, TC>(a, a.items[it], it, wsm, lane);
     }
 }
 
-template <int P, int SEG, bool ADJ, bool SRC2, bool PHI = false>
+template <int P, int SEG, bool ADJ, bool SRC2, bool PHI = false, typename TC = double>
 cudaError_t launch(const SweepArgs &args, int grid, cudaStream_t stream) {
-    auto kern = sweep_lane_kernel<P, SEG, ADJ, SRC2, PHI>;
+    auto kern = sweep_lane_kernel<P, SEG, ADJ, SRC2, PHI, TC>;
     const size_t smem = block_smem_bytes(P, SEG, SRC2);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -402,7 +407,7 @@ cudaError_t launch(const SweepArgs &args, int grid, cudaStream_t stream) {
 
 template <int P, int SEG, bool ADJ, bool SRC2>
 cudaError_t occupancy(int *blocks_per_sm) {
-    auto kern = sweep_lane_kernel<P, SEG, ADJ, SRC2, false>;
+    auto kern = sweep_lane_kernel<P, SEG, ADJ, SRC2, false, double>;
     const size_t smem = block_smem_bytes(P, SEG, SRC2);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
