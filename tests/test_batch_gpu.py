@@ -65,7 +65,7 @@ def test_autotuners_keep_results():
             b.sweep([s.data_ptr() for s in srcs], [o.data_ptr() for o in outs], None, np.inf)
         for j, c in enumerate(ctxs):
             seg, wn = c.autotune(srcs[j].data_ptr(), np.inf)
-            assert seg in (4, 8, 16, 32) and 1 <= wn <= 7
+            assert seg in (4, 8, 16, 32) and 0 <= wn <= 7   # wn = 0: the lane kernel
             want = torch.zeros_like(srcs[j])
             c.sweep_out(srcs[j].data_ptr(), want.data_ptr(), np.inf, None, loc=abi.LOC_DEVICE)
             assert torch.equal(outs[j][1:-1, 1:-1], want[1:-1, 1:-1])
