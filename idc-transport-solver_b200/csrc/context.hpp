@@ -60,6 +60,10 @@ public:
     Status gmres_peierls(const double *src, double *psi_out, double dt, double abs_tol, int restart, int64_t max_its,
                          int precision, int64_t *iters, double *resid);
     Status apply_peierls(const double *x, double *y, double *tmp_phi, double dt, int precision);
+    // precision IDC_PREC_FP32_IR of gmres_peierls: FP32 Krylov solves inside FP64 iterative refinement
+    Status gmres_peierls_ir(const double *src, double *psi_out, double dt, double abs_tol, int restart,
+                            int64_t max_its, int64_t *iters, double *resid);
+    int ir_corrections = 0;   // corrections (FP64 residual sweeps) of the last refined solve
     // GMRES(restart) from x = 0 on A x = b for an operator on moment-sized vectors; *converged reports
     // whether the residual reached abs_tol (the caller decides whether that is an error)
     template <typename Op>

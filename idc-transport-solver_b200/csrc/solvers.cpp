@@ -192,6 +192,8 @@ Status Context::gmres(Op apply, const double *b, double *x, double abs_tol, int 
 Status Context::gmres_peierls(const double *src, double *psi_out, double dt, double abs_tol, int restart,
                               int64_t max_its, int precision, int64_t *iters_out, double *resid_out) {
     if (!use_warp_kernel) return bad(IDC_ERR_UNSUPPORTED, "GMRES needs the warp-pipelined sweep kernel");
+    if (precision == IDC_PREC_FP32_IR) return gmres_peierls_ir(src, psi_out, dt, abs_tol, restart, max_its, iters_out,
+                                                               resid_out);
     IDC_TRY(ensure_phi_buffers(6));
     double *b = phi_buf(3), *x = phi_buf(4), *tmp = phi_buf(5);
     // right-hand side b = P L^{-1} Q (PETScPeierlsSolver.cpp:461-466)
@@ -206,6 +208,59 @@ Status Context::gmres_peierls(const double *src, double *psi_out, double dt, dou
     if (resid_out) *resid_out = resid;
     if (!converged)
         return bad(IDC_ERR_NOT_CONVERGED, "GMRES transport solve failed to converge (max_its reached, residual " +
+                                              std::to_string(resid) + ")");
+    return Status::ok();
+}
+
+// FP64 iterative refinement of the Peierls system A phi = b (A = I - P L^{-1} S, b = P L^{-1} Q) around FP32
+// Krylov solves: b, every residual r = b - A phi and the final psi = L^{-1}(S phi + Q) come from FP64 sweeps;
+// each correction A d = r is solved by GMRES (with the DSA preconditioner if set) whose sweeps run in FP32
+// arithmetic, to kIrInnerReduction of |r| (the FP32 operator is accurate to about 1e-7 relative), and
+// phi += d.  Stops when |r| <= abs_tol (the same absolute criterion as the FP64 solve).  *iters_out counts the
+// FP32 Krylov iterations, the FP64 residual sweeps come on top (one per correction).
+Status Context::gmres_peierls_ir(const double *src, double *psi_out, double dt, double abs_tol, int restart,
+                                 int64_t max_its, int64_t *iters_out, double *resid_out) {
+    constexpr double kIrInnerReduction = 1e-5;
+    constexpr int kIrMaxCorrections = 20;
+    IDC_TRY(ensure_phi_buffers(9));
+    double *b = phi_buf(3), *x = phi_buf(4), *tmp = phi_buf(5), *r = phi_buf(6), *d = phi_buf(7), *ax = phi_buf(8);
+    const size_t n = phi_len();
+    IDC_TRY(sweep(src, nullptr, dt, b, IDC_PREC_FP64));
+    IDC_TRY_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, stream));
+    IDC_TRY_CUDA(cudaMemcpyAsync(r, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream));
+    auto op32 = [&](const double *in, double *out) { return apply_peierls(in, out, tmp, dt, IDC_PREC_FP32); };
+    int64_t total = 0;
+    double resid = 0.0;
+    bool converged = false;
+    ir_corrections = 0;
+    for (int k = 0;; ++k) {
+        double rr = 0.0;
+        IDC_TRY(dot_host(r, r, n, &rr));
+        resid = std::sqrt(rr);
+        if (resid <= abs_tol) {
+            converged = true;
+            break;
+        }
+        if (k >= kIrMaxCorrections || total >= max_its) break;
+        int64_t its = 0;
+        double ires = 0.0;
+        bool iconv = false;
+        IDC_TRY(gmres(op32, r, d, std::max(abs_tol, kIrInnerReduction * resid), restart, max_its - total, &its, &ires,
+                      &iconv, precond_kind == 1 ? 1 : 0));
+        total += its;
+        ++ir_corrections;
+        IDC_TRY_CUDA(launch_axpby(1.0, d, 1.0, x, n, stream));            // phi += d
+        IDC_TRY(apply_peierls(x, ax, tmp, dt, IDC_PREC_FP64));             // r = b - A phi in FP64
+        IDC_TRY_CUDA(cudaMemcpyAsync(r, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream));
+        IDC_TRY_CUDA(launch_axpby(-1.0, ax, 1.0, r, n, stream));
+        launches += 3;
+    }
+    IDC_TRY(sweep(src, psi_out, dt, nullptr, IDC_PREC_FP64, x, 1.0));
+    IDC_TRY(check_device_error());
+    if (iters_out) *iters_out = total;
+    if (resid_out) *resid_out = resid;
+    if (!converged)
+        return bad(IDC_ERR_NOT_CONVERGED, "GMRES iterative refinement failed to converge (residual " +
                                               std::to_string(resid) + ")");
     return Status::ok();
 }

@@ -34,6 +34,7 @@ LOC_DEVICE = 1
 PREC_FP64 = 0
 PREC_FP32_REFINED = 1
 PREC_FP32 = 2
+PREC_FP32_IR = 3          # idc_gmres_solve: FP32 Krylov sweeps inside FP64 iterative refinement
 
 IDC_NOALLOC_MAX_ITEMS = 4096        # include/idcsweep.h
 IDC_NOALLOC_MAX_ORDINATES = 1024

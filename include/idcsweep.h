@@ -45,8 +45,11 @@ enum { IDC_LOC_HOST = 0, IDC_LOC_DEVICE = 1 };
 /* Arithmetic of a sweep.  IDC_PREC_FP64 restates the reference's FP64 Gaussian elimination.
  * IDC_PREC_FP32_REFINED factors and solves each cell system in FP32 and refines the solution with
  * FP64 residuals of the same cell system (all inputs, outputs and inter-cell traces stay FP64).
- * IDC_PREC_FP32 is the unrefined FP32 solve (for error studies). */
-enum { IDC_PREC_FP64 = 0, IDC_PREC_FP32_REFINED = 1, IDC_PREC_FP32 = 2 };
+ * IDC_PREC_FP32 is the unrefined FP32 solve (FP32 cell arithmetic and moment sums; about 1e-7 relative).
+ * IDC_PREC_FP32_IR (idc_gmres_solve only) runs the Krylov iterations with FP32 sweeps inside an FP64
+ * iterative refinement of the solve: the right-hand side, every residual and the final psi come from FP64
+ * sweeps, so the solution meets the FP64 tolerance. */
+enum { IDC_PREC_FP64 = 0, IDC_PREC_FP32_REFINED = 1, IDC_PREC_FP32 = 2, IDC_PREC_FP32_IR = 3 };
 
 typedef struct idc_ctx idc_ctx;
 
@@ -166,7 +169,9 @@ int idc_sweep_noalloc(const idc_problem_desc *desc, int64_t nq, const double *xi
 /* GMRES(restart) on the scalar flux, the Peierls form (I - P L^{-1} S) phi = P L^{-1} Q, from a zero
  * initial guess; stops when the residual 2-norm is <= abs_tol (absolute, the reference's default criterion),
  * then psi = L^{-1}(S phi + Q) is returned in source_inout (Q on entry).  Arnoldi (CGS2), Hessenberg least
- * squares and all vectors are FP64; `precision` selects the sweep arithmetic.  Replaces
+ * squares and all vectors are FP64; `precision` selects the sweep arithmetic, or IDC_PREC_FP32_IR: FP64
+ * iterative refinement whose corrections are GMRES solves with FP32 sweeps (*iters then counts their
+ * iterations; each correction adds one FP64 residual sweep).  Replaces
  * PETScPeierlsSolver::Solve with IPLS (linear_solvers/Abstract/ImplicitSolver/PETScPeierlsSolver.cpp:423-572);
  * PETSc's LGMRES augmentation is not reproduced (same fixed point, different iteration counts).  Returns
  * IDC_ERR_NOT_CONVERGED after max_its iterations, as the reference throws. */

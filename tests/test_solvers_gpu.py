@@ -26,7 +26,7 @@ def context_for(P):
 
 
 @pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
-@pytest.mark.parametrize("prec", [abi.PREC_FP64, abi.PREC_FP32_REFINED])
+@pytest.mark.parametrize("prec", [abi.PREC_FP64, abi.PREC_FP32_REFINED, abi.PREC_FP32_IR])
 def test_gmres_reaches_reference_si_fixed_point(path, prec):
     z = np.load(path)
     P = lambda: None
@@ -38,6 +38,28 @@ def test_gmres_reaches_reference_si_fixed_point(path, prec):
         its, res = ctx.gmres_solve(psi, float(z["dt"]), abs_tol=1e-13, restart=30, max_its=500, precision=prec)
         assert res <= 1e-13
         assert rel_err(psi, z["si_psi"]) < 1e-10
+
+
+@pytest.mark.parametrize("dsa", [False, True])
+def test_fp32_krylov_with_fp64_refinement_meets_the_fp64_tolerance(dsa):
+    """IDC_PREC_FP32_IR: FP32 sweeps in the Krylov iterations, FP64 residuals and solution: the same
+    solution as the FP64 solve to the tolerance, although an FP32 sweep alone is accurate to ~1e-7 only."""
+    P = lognormal(64, 2, 8, seed=4, c_range=(0.5, 0.99))
+    out = {}
+    with context_for(P) as ctx:
+        if dsa:
+            ctx.set_preconditioner(abi.PRECOND_DSA, 20)
+        for prec in (abi.PREC_FP64, abi.PREC_FP32_IR):
+            psi = P.source.copy()
+            its, res = ctx.gmres_solve(psi, P.dt, abs_tol=1e-10, restart=30, max_its=2000, precision=prec)
+            assert res <= 1e-10
+            out[prec] = psi
+        one = P.source.copy()
+        ctx.sweep(one, P.dt, None, abi.PREC_FP32)
+        two = P.source.copy()
+        ctx.sweep(two, P.dt, None, abi.PREC_FP64)
+    assert rel_err(out[abi.PREC_FP32_IR], out[abi.PREC_FP64]) < 1e-9
+    assert 1e-9 < rel_err(one, two) < 1e-5   # a single FP32 sweep is FP32-accurate
 
 
 def test_gmres_matches_restatement_si_on_lattice(restatement):
