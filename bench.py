@@ -245,10 +245,14 @@ def _ctx_for(abi, P, dev):
 
 
 def extra_gmres_dsa(abi, torch, dev):
-    """256x256 Q2 S16 log-normal steady problem, GMRES(30) + DSA to 1e-10 (FP64 and refined sweeps)."""
+    """256x256 Q2 S16 log-normal steady problem, GMRES(30) + DSA to 1e-10: FP64 sweeps, per-cell refined FP32
+    sweeps, and FP32 Krylov sweeps inside FP64 iterative refinement of the solve (error against the FP64 solve
+    stated); then the Krylov iterations' moments-only sweep alone in FP64 and FP32."""
     P = problem(0)
     out = {"workload": "256x256 Q2 S16 log-normal steady, GMRES(30)+DSA(30 CG steps), abs tol 1e-10"}
-    for name, prec in (("fp64", abi.PREC_FP64), ("fp32_refined", abi.PREC_FP32_REFINED)):
+    sols = {}
+    for name, prec in (("fp64", abi.PREC_FP64), ("fp32_refined", abi.PREC_FP32_REFINED),
+                       ("fp32_krylov_fp64_refinement", abi.PREC_FP32_IR)):
         with _ctx_for(abi, P, dev) as c:
             c.set_preconditioner(abi.PRECOND_DSA, 30)
             d = torch.from_numpy(P.source).to(f"cuda:{dev}")
@@ -261,6 +265,26 @@ def extra_gmres_dsa(abi, torch, dev):
                                      loc=abi.LOC_DEVICE)
             torch.cuda.synchronize()
             out[name] = {"iterations": its, "residual": res, "ms": (time.perf_counter() - t0) * 1e3}
+            sols[name] = d.cpu().numpy()
+    for name in ("fp32_refined", "fp32_krylov_fp64_refinement"):
+        out[name]["psi_rel_diff_vs_fp64"] = float(np.abs(sols[name] - sols["fp64"]).max() / np.abs(sols["fp64"]).max())
+    out["speedup_fp32_krylov_fp64_refinement_vs_fp64"] = out["fp64"]["ms"] / out["fp32_krylov_fp64_refinement"]["ms"]
+    # the Krylov iterations' moments-only sweep alone (no source, psi not stored), FP64 against FP32
+    with _ctx_for(abi, P, dev) as c:
+        x = torch.from_numpy(np.random.default_rng(1).uniform(0.1, 1.0, P.phi_shape())).to(f"cuda:{dev}")
+        ph = torch.zeros_like(x)
+        sweeps = {}
+        for name, prec in (("fp64", abi.PREC_FP64), ("fp32", abi.PREC_FP32)):
+            ms = []
+            for rep in range(8):
+                c.sweep_fused(None, None, P.dt, x.data_ptr(), 1.0, ph.data_ptr(), prec)
+                ms.append(c.last_timing()[0])
+            sweeps[name] = {"kernel_ms": min(ms[3:]), "phi": ph.clone()}
+        out["moments_only_sweep"] = {
+            "fp64_kernel_ms": sweeps["fp64"]["kernel_ms"], "fp32_kernel_ms": sweeps["fp32"]["kernel_ms"],
+            "speedup_fp32_vs_fp64": sweeps["fp64"]["kernel_ms"] / sweeps["fp32"]["kernel_ms"],
+            "err_phi_fp32_vs_fp64": float(((sweeps["fp32"]["phi"] - sweeps["fp64"]["phi"]).abs().max() /
+                                           sweeps["fp64"]["phi"].abs().max()).item())}
     return out
 
 
@@ -480,6 +504,8 @@ def run_ours(args):
     warm = max(3, args.warmup)
     ms32, k32, _, _ = timed(abi.PREC_FP32_REFINED, args.steps, warm)
     phi32 = phi.clone()
+    msf, kf, _, _ = timed(abi.PREC_FP32, args.steps, warm)   # unrefined FP32 arithmetic (about 1e-7)
+    phif = phi.clone()
     ms64, k64, launches, clocks = timed(abi.PREC_FP64, args.steps, warm, sampler=(rank == 0))
     phi64 = phi.clone()
 
@@ -528,7 +554,8 @@ def run_ours(args):
         "dtype": "f64",
         "data": "synthetic",
         "config": bench_config(P, world),
-        "tile_shape": {"fp64": list(shapes[abi.PREC_FP64]), "fp32_refined": list(shapes[abi.PREC_FP32_REFINED])},
+        "tile_shape": {"fp64": list(shapes[abi.PREC_FP64]), "fp32_refined": list(shapes[abi.PREC_FP32_REFINED]),
+                   "fp32": list(shapes[abi.PREC_FP32])},
         "roofline": {"bound": "hbm", "achieved": alg / (k64 * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                      "frac": alg / (k64 * 1e-3) / 1e9 / peak, "traffic": traffic,
                      "algorithmic_bytes": alg, "kernel_ms": k64, "peak_kind": peak_kind},
@@ -536,6 +563,9 @@ def run_ours(args):
                          "roofline_frac": alg / (k32 * 1e-3) / 1e9 / peak},
         "speedup_fp32_refined_vs_fp64": ms64 / ms32,
         "err_phi_fp32_refined_vs_fp64_gpu": err_fp32_vs_fp64,
+        "fp32": {"value": world * unknowns / (msf * 1e-3), "ms_per_step": msf, "kernel_ms": kf,
+                 "speedup_vs_fp64": ms64 / msf,
+                 "err_phi_vs_fp64_gpu": float(((phif - phi64).abs().max() / phi64.abs().max()).item())},
         "e2e": None if args.no_e2e else {
             "value": world * unknowns / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(hs.nbytes),
             "d2h_bytes_per_step": int(P.nx * P.ny * P.nq * P.N * 8 + hp.nbytes), "ms_per_step": e2e_s * 1e3,
@@ -560,7 +590,8 @@ def run_ours(args):
             scale = np.abs(phi_ref).max()
             line["err_phi_vs_oracle"] = {
                 "fp64": float(np.abs(phi64.cpu().numpy() - phi_ref).max() / scale),
-                "fp32_refined": float(np.abs(phi32.cpu().numpy() - phi_ref).max() / scale)}
+                "fp32_refined": float(np.abs(phi32.cpu().numpy() - phi_ref).max() / scale),
+                "fp32": float(np.abs(phif.cpu().numpy() - phi_ref).max() / scale)}
         except Exception as e:  # the reference library may be absent where it was never built
             line["cpu_baseline"] = None
             line["cpu_baseline_error"] = str(e)[:200]
