@@ -17,8 +17,10 @@ the copies of neighbouring steps overlap the sweeps on separate streams).
 
 --impl reference times the reference solver's own CPU sweep (SweepOperator::Apply, compiled from the
 reference's sources into oracle/_ref/libidcref.so) on all host cores, same workload and metric.
-Under torchrun (N > 1) every rank sweeps its own independent problem (seed = rank; no collective on
-the data path, weak scaling); rank 0 prints the line.
+Under torchrun (N > 1) the ranks split the one problem by ordinates (each sweeps a slice of every
+quadrant's ordinates; one NCCL all-reduce of the moments per step; strong scaling), or with --mode replicas
+every rank sweeps its own independent problem (seed = rank; no collective, weak scaling); rank 0 prints the
+line.
 """
 from __future__ import annotations
 
@@ -434,6 +436,112 @@ def extra_batched(abi, torch, dev, n_problems=64):
 # our arm
 # ----------------------------------------------------------------------------------------------------
 
+def run_partitioned(args):
+    """One problem (the workload) split by ordinates over the ranks: every rank sweeps a balanced slice of each
+    quadrant's ordinates of the whole grid (its own context, source slice and psi slice resident on its GPU)
+    and one all-reduce (sum, NCCL) of the partial moments per step completes phi -- the path's only exchange.
+    `value` = the whole problem's unknowns / the slowest rank's time per step (strong scaling).  `e2e` adds,
+    on every rank, the upload of its source slice and the download of its psi slice and of phi."""
+    import datetime
+    import torch
+    import torch.distributed as tdist
+    from idcsweep import abi
+    from idcsweep.distributed import local_quadrature, partition_ordinates
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    P = problem(0, args.nx)
+    idx = partition_ordinates(P.quad, world, rank)
+    xi, eta, w, q = local_quadrature(P.xi, P.eta, P.w, P.quad, idx)
+    ctx = abi.SweepContext(P.nx, P.ny, P.p, P.ax, P.bx, P.ay, P.by, device=dev)
+    ctx.set_ordinates(xi, eta, w, q)
+    ctx.set_sigma(P.sigma_t, P.sigma_s)
+    h_src = np.ascontiguousarray(P.source[:, :, idx])
+    src = torch.from_numpy(h_src).to(f"cuda:{dev}")
+    out = torch.empty_like(src)
+    phi = torch.zeros(P.phi_shape(), dtype=torch.float64, device=f"cuda:{dev}")
+    shape = (0, 0) if args.no_autotune else ctx.autotune(src.data_ptr(), P.dt, abi.PREC_FP64)
+    ctx.set_tile_shape(*shape)
+
+    counted = [0]
+
+    def step():
+        ctx.sweep_out(src.data_ptr(), out.data_ptr(), P.dt, phi.data_ptr(), abi.PREC_FP64, loc=abi.LOC_DEVICE)
+        counted[0] += ctx.last_timing()[1]
+        tdist.all_reduce(phi)   # on torch's current stream, after the (synchronous) sweep returned
+
+    def time_steps(fn, steps):
+        torch.cuda.synchronize()
+        tdist.barrier()
+        torch.cuda.synchronize()
+        stream = torch.cuda.current_stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        tdist.barrier()
+        torch.cuda.synchronize()
+        t = torch.tensor([e0.elapsed_time(e1) / steps], device=f"cuda:{dev}")
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        return float(t.item())
+
+    warm = max(3, args.warmup)
+    for _ in range(warm):
+        step()
+    clocks = ClockSampler(dev) if rank == 0 else None
+    if clocks:
+        clocks.__enter__()
+    counted[0] = 0
+    ms = time_steps(step, args.steps)
+    launches = counted[0]
+    if clocks:
+        clocks.__exit__()
+    kernel_ms = ctx.last_timing()[0]
+
+    # end to end: this rank's host slice in, its psi slice and phi out, every step
+    hs = torch.from_numpy(h_src).pin_memory()
+    ho = torch.empty_like(hs).pin_memory()
+    hp = torch.zeros(P.phi_shape(), dtype=torch.float64).pin_memory()
+
+    def e2e_step():
+        src.copy_(hs, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        step()
+        ho.copy_(out, non_blocking=True)
+        hp.copy_(phi, non_blocking=True)
+
+    e2e_step()
+    e2e_ms = None if args.no_e2e else time_steps(e2e_step, max(2, args.steps))
+    phi_host = phi.cpu().numpy()
+    tdist.barrier()
+    ctx.close()
+    if rank == 0:
+        unknowns = P.unknowns_per_sweep
+        alg = algorithmic_bytes(P)
+        peak, peak_kind = hbm_peak()
+        cfg = bench_config(P, world)
+        cfg["parallelism"] = f"ordinates{world}"
+        emit({
+            "metric": METRIC, "value": unknowns / (ms * 1e-3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": warm, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "config": cfg, "tile_shape": {"fp64": list(shape)},
+            "roofline": {"bound": "hbm", "achieved": alg / world / (kernel_ms * 1e-3) / 1e9, "peak": peak,
+                         "unit": "GB/s", "frac": alg / world / (kernel_ms * 1e-3) / 1e9 / peak, "traffic": None,
+                         "algorithmic_bytes_per_rank": alg / world, "kernel_ms": kernel_ms, "peak_kind": peak_kind},
+            "e2e": None if e2e_ms is None else {
+                "value": unknowns / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(h_src.nbytes) * world,
+                "d2h_bytes_per_step": int(h_src.nbytes + phi_host.nbytes) * world, "ms_per_step": e2e_ms},
+            "gpu_launches": launches, "clocks": clocks.summary() if clocks else None,
+            "exchange": "one NCCL all-reduce (sum) of phi per step, %d bytes" % phi_host.nbytes})
+    tdist.destroy_process_group()
+    return 0
+
+
 def run_ours(args):
     import torch
     from idcsweep import abi
@@ -622,6 +730,10 @@ def run_only_extra(name):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--mode", choices=("partitioned", "replicas"), default="partitioned",
+                    help="more than one GPU (torchrun): one problem split by ordinates with an all-reduce of the "
+                         "moments per step (strong scaling, the default), or one independent problem per GPU "
+                         "(weak scaling)")
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
@@ -639,6 +751,11 @@ def main():
         return run_only_extra(args.only_extra)
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.mode == "partitioned" and "WORLD_SIZE" in os.environ and int(os.environ["WORLD_SIZE"]) > 1:
+        return run_partitioned(args)
+    if args.mode == "partitioned" and "WORLD_SIZE" in os.environ and args.gpus == 1 and os.environ.get(
+            "IDC_BENCH_PARTITIONED_ONE"):   # the partitioned path on one rank (its code path, checked on one GPU)
+        return run_partitioned(args)
     return run_ours(args)
 
 
