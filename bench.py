@@ -423,10 +423,51 @@ def extra_batched(abi, torch, dev, n_problems=64):
                 best = min((b.sweep(S, O, F, math.inf, prec), b.last_ms())[1] for _ in range(3))
                 res[name] = {"device_ms": best, "unknowns_per_s": unknowns / (best * 1e-3),
                              "hbm_frac_of_measured": 16.0 * unknowns / (best * 1e-3) / 1e9 / hbm_peak()[0]}
+            # GMRES + DSA (20 CG steps) to 1e-8 on every problem: one at a time, then batched (one batched sweep per
+            # Krylov step for all unconverged problems)
+            for c in ctxs:
+                c.set_preconditioner(abi.PRECOND_DSA, 20)
+            sizes = [int(np.prod(s_.shape)) // (s_.shape[0] * s_.shape[1]) * (s_.shape[0] - 2) * (s_.shape[1] - 2)
+                     for s_ in srcs]
+            work = [x.clone() for x in srcs]
+            for k, c in enumerate(ctxs):   # warm-up (buffers, schedules)
+                c.gmres_solve(work[k].data_ptr(), math.inf, abs_tol=1e-8, restart=30, max_its=3000,
+                              loc=abi.LOC_DEVICE)
+            work = [x.clone() for x in srcs]
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            single_its = []
+            for k, c in enumerate(ctxs):
+                single_its.append(c.gmres_solve(work[k].data_ptr(), math.inf, abs_tol=1e-8, restart=30, max_its=3000,
+                                                loc=abi.LOC_DEVICE)[0])
+            torch.cuda.synchronize()
+            single_s = time.perf_counter() - t0
+            single_psi = work
+            work = [x.clone() for x in srcs]
+            b.gmres_solve([x.data_ptr() for x in work], math.inf, abs_tol=1e-8, restart=30, max_its=3000)   # warm-up
+            work = [x.clone() for x in srcs]
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            batch_its, batch_res = b.gmres_solve([x.data_ptr() for x in work], math.inf, abs_tol=1e-8, restart=30,
+                                                 max_its=3000)
+            torch.cuda.synchronize()
+            batch_s = time.perf_counter() - t0
+            diff = max(float(((work[k] - single_psi[k]).abs().max() / single_psi[k].abs().max()).item())
+                       for k in range(len(ctxs)))
+            sweeps_single = sum((i + 2) * u for i, u in zip(single_its, sizes))
+            sweeps_batch = sum((i + 2) * u for i, u in zip(batch_its, sizes))
+            solves = {"workload": "GMRES(30) + DSA (20 CG steps) to 1e-8 on every problem, FP64",
+                      "one_at_a_time": {"ms": single_s * 1e3, "krylov_iterations": int(sum(single_its)),
+                                        "sweep_unknowns_per_s": sweeps_single / single_s},
+                      "batched": {"ms": batch_s * 1e3, "krylov_iterations": int(sum(batch_its)),
+                                  "max_iterations": int(max(batch_its)),
+                                  "sweep_unknowns_per_s": sweeps_batch / batch_s},
+                      "speedup": single_s / batch_s, "psi_rel_diff_batched_vs_single": diff}
         return {"workload": f"{n_problems} independent steady problems, sides 32..384, S4..S16, Q1/Q2",
                 "unknowns_per_sweep": unknowns, "one_at_a_time_fp64": {"device_ms": one,
                                                                       "unknowns_per_s": unknowns / (one * 1e-3)},
-                "batched_autotuned": res, "speedup_fp64": one / res["fp64"]["device_ms"]}
+                "batched_autotuned": res, "speedup_fp64": one / res["fp64"]["device_ms"],
+                "gmres_dsa_solves": solves}
     finally:
         for c in ctxs:
             c.close()

@@ -482,6 +482,16 @@ int idc_batch_last_timing(idc_batch *b, double *ms) {
     return IDC_OK;
 }
 
+int idc_batch_gmres_solve(idc_batch *b, double *const *psi_inout, double dt, double abs_tol, int32_t restart,
+                          int64_t max_its, int precision, int64_t *iters, double *final_resids) {
+    ABI_GUARD_BEGIN
+    if (!b || !psi_inout) return fail(IDC_ERR_ARG, "idc_batch_gmres_solve: null argument");
+    if (max_its < 0 || !(abs_tol >= 0)) return fail(IDC_ERR_ARG, "idc_batch_gmres_solve: bad tolerance");
+    ABI_TRY(b->impl.gmres_solve(psi_inout, dt, abs_tol, restart, max_its, precision, iters, final_resids));
+    return IDC_OK;
+    ABI_GUARD_END
+}
+
 int idc_batch_destroy(idc_batch *b) {
     delete b;
     return IDC_OK;

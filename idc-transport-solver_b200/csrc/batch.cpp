@@ -157,7 +157,7 @@ Status Batch::build_group(Group &g, int precision) {
 }
 
 Status Batch::launch_group(Group &g, const double *const *srcs, double *const *outs, const double *const *phi_sc,
-                           double scale, double *const *phis, double dt) {
+                           double scale, double *const *phis, double dt, const std::vector<char> *active) {
     Context &c0 = *members[g.members[0]];
     cudaStream_t st = stream();
     std::vector<SweepArgs> table(g.members.size());
@@ -200,6 +200,15 @@ Status Batch::launch_group(Group &g, const double *const *srcs, double *const *o
             a.phi = phis[p];   // the batched reduction's output (the sweep kernel writes the slots)
         }
         if (a.src) a.inflow = g.inflow[m];
+        if (active && !(*active)[p]) {   // left out: its items return at once, the helpers see no arrays
+            a.skip = 1;
+            a.src = nullptr;
+            a.out = nullptr;
+            a.phi_scatter = nullptr;
+            a.phi = nullptr;
+            a.phi_part = nullptr;
+            a.inflow = nullptr;
+        }
     }
     bool any_src = false, any_phi = false;
     for (const auto &a : table) {
@@ -228,7 +237,7 @@ Status Batch::launch_group(Group &g, const double *const *srcs, double *const *o
 }
 
 Status Batch::sweep(const double *const *srcs, double *const *outs, const double *const *phi_sc, double scale,
-                    double *const *phis, double dt, int precision) {
+                    double *const *phis, double dt, int precision, const std::vector<char> *active) {
     if (members.empty()) return bad(IDC_ERR_STATE, "empty batch");
     if (precision != IDC_PREC_FP64 && precision != IDC_PREC_FP32_REFINED)
         return bad(IDC_ERR_UNSUPPORTED, "batched sweeps run in FP64 or refined precision");
@@ -258,7 +267,7 @@ Status Batch::sweep(const double *const *srcs, double *const *outs, const double
         for (auto &g : groups) IDC_TRY(build_group(g, precision));
     }
     IDC_TRY_CUDA(cudaEventRecord(c0.ev0, c0.stream));
-    for (auto &g : groups) IDC_TRY(launch_group(g, srcs, outs, phi_sc, scale, phis, dt));
+    for (auto &g : groups) IDC_TRY(launch_group(g, srcs, outs, phi_sc, scale, phis, dt, active));
     IDC_TRY_CUDA(cudaEventRecord(c0.ev1, c0.stream));
     IDC_TRY_CUDA(cudaStreamSynchronize(c0.stream));
     for (auto &g : groups) {
@@ -276,6 +285,245 @@ Status Batch::sweep(const double *const *srcs, double *const *outs, const double
     float ms = 0.f;
     IDC_TRY_CUDA(cudaEventElapsedTime(&ms, c0.ev0, c0.ev1));
     last_ms = ms;
+    return Status::ok();
+}
+
+// Batched GMRES: Context::gmres_peierls's algorithm (CGS2 Arnoldi, Givens rotations on the host, restarts
+// from the true residual, flexible GMRES with the member's DSA preconditioner) run on every member in lock
+// step.  A step applies the Peierls operator of every unconverged member, A v = v - P L^{-1} S v, through
+// ONE batched sweep (members that have converged are skipped inside the launch), then queues each member's
+// orthogonalisation on the device and brings every member's Hessenberg column back with one
+// synchronisation.  A member whose cycle ends restarts from its true residual in the next step's sweep.
+Status Batch::gmres_solve(double *const *psi_inout, double dt, double abs_tol, int restart, int64_t max_its,
+                          int precision, int64_t *iters_out, double *resids_out) {
+    if (members.empty()) return bad(IDC_ERR_STATE, "empty batch");
+    if (restart < 1 || restart > 60) return bad(IDC_ERR_ARG, "gmres restart must be in 1..60");
+    if (!psi_inout) return bad(IDC_ERR_ARG, "null psi arrays");
+    const size_t M = members.size();
+    for (size_t p = 0; p < M; ++p)
+        if (!psi_inout[p]) return bad(IDC_ERR_ARG, "null psi array of a batch member");
+    Context &c0 = *members[0];
+    IDC_TRY_CUDA(cudaSetDevice(c0.device));
+    cudaStream_t st = stream();
+    const int m = restart;
+
+    struct State {
+        Context *c;
+        size_t n;
+        int m;
+        bool dsa;
+        double *V, *b, *x, *tmp, *scat;
+        std::vector<double> H, cs, sn, g, yv;
+        double beta = 0, resid = 0;
+        int j = 0;
+        int64_t its = 0;
+        bool done = false, converged = false, restart_pending = false;
+        double *in = nullptr, *out = nullptr;
+        double *Vc(int k) const { return V + (size_t)k * n; }
+        double *Zc(int k) const { return V + (size_t)(m + 1 + k) * n; }   // flexible GMRES: Z after V_0 .. V_m
+    };
+    int *d_err = nullptr;   // one device error word per member for its DSA grid barriers
+    IDC_TRY_CUDA(cudaMalloc(&d_err, sizeof(int) * M));
+    struct Free {
+        int *p;
+        ~Free() { cudaFree(p); }
+    } free_err{d_err};
+    IDC_TRY_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int) * M, st));
+    std::vector<State> S(M);
+    for (size_t p = 0; p < M; ++p) {
+        Context &c = *members[p];
+        State &z = S[p];
+        z.c = &c;
+        z.n = c.phi_len();
+        z.m = m;
+        z.dsa = c.precond_kind == 1;
+        const size_t need = (size_t)(z.dsa ? 2 * m + 1 : m + 1) * z.n;
+        if (c.krylov_len < need) {
+            cudaFree(c.d_krylov);
+            c.d_krylov = nullptr;
+            c.krylov_len = 0;
+            IDC_TRY_CUDA(cudaMalloc(&c.d_krylov, sizeof(double) * need));
+            c.krylov_len = need;
+        }
+        if (!c.d_small) IDC_TRY_CUDA(cudaMalloc(&c.d_small, sizeof(double) * (128 + multidot_scratch_doubles())));
+        if (!c.h_small) IDC_TRY_CUDA(cudaMallocHost(&c.h_small, sizeof(double) * 129));
+        IDC_TRY(c.ensure_phi_buffers(7));
+        z.V = c.d_krylov;
+        z.b = c.phi_buf(3);
+        z.x = c.phi_buf(4);
+        z.tmp = c.phi_buf(5);
+        z.scat = c.phi_buf(6);
+        z.H.assign((size_t)(m + 1) * m, 0.0);
+        z.cs.assign(m, 0.0);
+        z.sn.assign(m, 0.0);
+        z.g.assign(m + 1, 0.0);
+        z.yv.assign(m, 0.0);
+        if (z.dsa) {
+            const size_t wl = dsa_workspace_doubles((int)c.nx, (int)c.ny);
+            if (c.dsa_ws_len < wl) {
+                cudaFree(c.d_dsa_ws);
+                c.d_dsa_ws = nullptr;
+                c.dsa_ws_len = 0;
+                IDC_TRY_CUDA(cudaMalloc(&c.d_dsa_ws, sizeof(double) * wl));
+                c.dsa_ws_len = wl;
+            }
+            IDC_TRY_CUDA(dsa_setup(c.dims(), c.d_sigma_t, c.d_sigma_s, c.d_dsa_ws, st));
+        }
+        IDC_TRY_CUDA(cudaMemsetAsync(z.x, 0, sizeof(double) * z.n, st));
+    }
+    std::vector<const double *> srcs(M), scats(M);
+    std::vector<double *> outs(M, nullptr), bs(M), tmps(M);
+    for (size_t p = 0; p < M; ++p) {
+        srcs[p] = psi_inout[p];
+        bs[p] = S[p].b;
+        tmps[p] = S[p].tmp;
+        scats[p] = S[p].scat;
+    }
+    // right-hand sides b = P L^{-1} Q of every member in one batched sweep, then r = b, beta = |b|
+    IDC_TRY(sweep(srcs.data(), nullptr, nullptr, 1.0, bs.data(), dt, precision));
+    for (auto &z : S) {
+        IDC_TRY_CUDA(cudaMemcpyAsync(z.Vc(0), z.b, sizeof(double) * z.n, cudaMemcpyDeviceToDevice, st));
+        IDC_TRY_CUDA(launch_dot(z.Vc(0), z.Vc(0), z.n, z.c->d_small + 127, z.c->d_small + 128, st));
+        IDC_TRY_CUDA(cudaMemcpyAsync(z.c->h_small + 127, z.c->d_small + 127, sizeof(double), cudaMemcpyDeviceToHost, st));
+    }
+    IDC_TRY_CUDA(cudaStreamSynchronize(st));
+    auto start_cycle = [&](State &z) -> Status {
+        IDC_TRY_CUDA(launch_axpby(0.0, z.Vc(0), 1.0 / z.beta, z.Vc(0), z.n, st));
+        std::fill(z.g.begin(), z.g.end(), 0.0);
+        z.g[0] = z.beta;
+        z.j = 0;
+        return Status::ok();
+    };
+    for (auto &z : S) {
+        z.beta = std::sqrt(z.c->h_small[127]);
+        z.resid = z.beta;
+        z.converged = z.resid <= abs_tol;
+        z.done = z.converged || z.beta == 0.0 || max_its == 0;
+        if (!z.done) IDC_TRY(start_cycle(z));
+    }
+    std::vector<char> active(M);
+    for (;;) {
+        bool any = false;
+        for (size_t p = 0; p < M; ++p) {
+            active[p] = !S[p].done;
+            any |= !S[p].done;
+        }
+        if (!any) break;
+        // the vectors to apply A to: x (a restart's true residual) or the next basis (preconditioned) vector
+        for (size_t p = 0; p < M; ++p) {
+            State &z = S[p];
+            if (z.done) continue;
+            Context &c = *z.c;
+            if (z.restart_pending) {
+                z.in = z.x;
+                z.out = z.Vc(0);
+            } else {
+                if (z.dsa) {
+                    IDC_TRY_CUDA(dsa_precondition(c.dims(), c.d_sigma_s, z.Vc(z.j), z.Zc(z.j), c.dsa_steps, c.d_dsa_ws,
+                                                  false, c.num_sms, d_err + p, c.spin_limit, st));
+                    z.in = z.Zc(z.j);
+                } else {
+                    z.in = z.Vc(z.j);
+                }
+                z.out = z.Vc(z.j + 1);
+            }
+            IDC_TRY_CUDA(launch_scatter_moments(c.dims(), c.d_sigma_s, z.in, z.scat, st));
+        }
+        IDC_TRY(sweep(nullptr, nullptr, scats.data(), 1.0, tmps.data(), dt, precision, &active));
+        for (size_t p = 0; p < M; ++p) {
+            State &z = S[p];
+            if (z.done) continue;
+            Context &c = *z.c;
+            const size_t n = z.n;
+            IDC_TRY_CUDA(launch_axpby(1.0, z.in, 0.0, z.out, n, st));     // A in = in - P L^{-1} S in
+            IDC_TRY_CUDA(launch_axpby(-1.0, z.tmp, 1.0, z.out, n, st));
+            double *ds = c.d_small, *scratch = c.d_small + 128;
+            if (z.restart_pending) {   // r = b - A x
+                IDC_TRY_CUDA(launch_axpby(1.0, z.b, -1.0, z.Vc(0), n, st));
+                IDC_TRY_CUDA(launch_dot(z.Vc(0), z.Vc(0), n, ds + 127, scratch, st));
+            } else {                   // CGS2 against V_0 .. V_j, then |w|^2
+                const int j = z.j;
+                IDC_TRY_CUDA(launch_multidot(z.V, j + 1, n, z.Vc(j + 1), n, ds, scratch, st));
+                IDC_TRY_CUDA(launch_multiaxpy(z.Vc(j + 1), z.V, j + 1, n, ds, n, st));
+                IDC_TRY_CUDA(launch_multidot(z.V, j + 1, n, z.Vc(j + 1), n, ds + 64, scratch, st));
+                IDC_TRY_CUDA(launch_multiaxpy(z.Vc(j + 1), z.V, j + 1, n, ds + 64, n, st));
+                IDC_TRY_CUDA(launch_dot(z.Vc(j + 1), z.Vc(j + 1), n, ds + 127, scratch, st));
+            }
+            IDC_TRY_CUDA(cudaMemcpyAsync(c.h_small, ds, sizeof(double) * 128, cudaMemcpyDeviceToHost, st));
+            IDC_TRY_CUDA(cudaMemcpyAsync(c.h_small + 128, d_err + p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        }
+        IDC_TRY_CUDA(cudaStreamSynchronize(st));
+        for (size_t p = 0; p < M; ++p) {
+            State &z = S[p];
+            if (z.done) continue;
+            const double *h = z.c->h_small;
+            int dev_err = 0;
+            std::memcpy(&dev_err, h + 128, sizeof(int));
+            if (dev_err != kDevOk)
+                return bad(IDC_ERR_TIMEOUT, "a DSA grid barrier gave up in a batched GMRES solve");
+            if (z.restart_pending) {
+                z.restart_pending = false;
+                z.beta = std::sqrt(h[127]);
+                z.resid = z.beta;
+                z.converged = z.resid <= abs_tol;
+                z.done = z.converged || z.beta == 0.0 || z.its >= max_its;
+                if (!z.done) IDC_TRY(start_cycle(z));
+                continue;
+            }
+            const int j = z.j;
+            const double hn = std::sqrt(h[127]);
+            for (int i = 0; i <= j; ++i) z.H[(size_t)i * m + j] = h[i] + h[64 + i];
+            z.H[(size_t)(j + 1) * m + j] = hn;
+            if (hn > 0.0) IDC_TRY_CUDA(launch_axpby(0.0, z.Vc(j + 1), 1.0 / hn, z.Vc(j + 1), z.n, st));
+            for (int i = 0; i < j; ++i) {
+                const double a = z.H[(size_t)i * m + j], c = z.H[(size_t)(i + 1) * m + j];
+                z.H[(size_t)i * m + j] = z.cs[i] * a + z.sn[i] * c;
+                z.H[(size_t)(i + 1) * m + j] = -z.sn[i] * a + z.cs[i] * c;
+            }
+            const double a = z.H[(size_t)j * m + j], c = z.H[(size_t)(j + 1) * m + j];
+            const double r = std::hypot(a, c);
+            z.cs[j] = r > 0.0 ? a / r : 1.0;
+            z.sn[j] = r > 0.0 ? c / r : 0.0;
+            z.H[(size_t)j * m + j] = r;
+            z.H[(size_t)(j + 1) * m + j] = 0.0;
+            z.g[j + 1] = -z.sn[j] * z.g[j];
+            z.g[j] = z.cs[j] * z.g[j];
+            z.resid = std::fabs(z.g[j + 1]);
+            ++z.its;
+            const bool cycle_end = z.resid <= abs_tol || hn == 0.0 || j + 1 == m || z.its >= max_its;
+            if (!cycle_end) {
+                z.j = j + 1;
+                continue;
+            }
+            // y = H^{-1} g, x += Z y (or V y)
+            const int k = j + 1;
+            for (int i = k - 1; i >= 0; --i) {
+                double sum = z.g[i];
+                for (int l = i + 1; l < k; ++l) sum -= z.H[(size_t)i * m + l] * z.yv[l];
+                z.yv[i] = -(sum / z.H[(size_t)i * m + i]);   // negated: multiaxpy subtracts
+            }
+            IDC_TRY_CUDA(cudaMemcpyAsync(z.c->d_small, z.yv.data(), sizeof(double) * k, cudaMemcpyHostToDevice, st));
+            IDC_TRY_CUDA(launch_multiaxpy(z.x, z.dsa ? z.Zc(0) : z.V, k, z.n, z.c->d_small, z.n, st));
+            if (z.resid <= abs_tol) {
+                z.converged = true;
+                z.done = true;
+            } else if (z.its >= max_its || hn == 0.0) {
+                z.done = true;
+            } else {
+                z.restart_pending = true;
+            }
+        }
+    }
+    // psi = L^{-1}(S phi + Q) of every member in one batched sweep (in place: Q in, psi out)
+    for (auto &z : S) IDC_TRY_CUDA(launch_scatter_moments(z.c->dims(), z.c->d_sigma_s, z.x, z.scat, st));
+    IDC_TRY(sweep(srcs.data(), psi_inout, scats.data(), 1.0, nullptr, dt, precision));
+    bool all = true;
+    for (size_t p = 0; p < M; ++p) {
+        if (iters_out) iters_out[p] = S[p].its;
+        if (resids_out) resids_out[p] = S[p].resid;
+        all &= S[p].converged;
+    }
+    if (!all) return bad(IDC_ERR_NOT_CONVERGED, "a batched GMRES solve stopped at its iteration limit");
     return Status::ok();
 }
 

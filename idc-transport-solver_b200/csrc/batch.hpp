@@ -17,7 +17,13 @@ public:
     // scale phi_sc[p]), phis[p] <- P outs[p]; device pointers.  phi_sc[p] holds the scattering moments
     // sigma_s phi / (4 pi) per cell (launch_scatter_moments), S phi without the ordinate broadcast
     Status sweep(const double *const *srcs, double *const *outs, const double *const *phi_sc, double scale,
-                 double *const *phis, double dt, int precision);
+                 double *const *phis, double dt, int precision, const std::vector<char> *active = nullptr);
+    // GMRES(restart) on every member's Peierls system at once (the algorithm of Context::gmres_peierls, with
+    // each member's preconditioner): every Krylov step sweeps all unconverged members in one batched sweep,
+    // their Arnoldi steps and DSA applications run on the device per member, with one host synchronisation
+    // per step for all.  psi_inout[p]: Q on entry, psi on return (device).  iters / resids: per member.
+    Status gmres_solve(double *const *psi_inout, double dt, double abs_tol, int restart, int64_t max_its,
+                       int precision, int64_t *iters, double *resids);
     // times the candidate tile shapes per degree on the given inputs and keeps the fastest
     Status autotune(const double *const *srcs, double *const *outs, double dt, int precision);
     // the tile shape used for degree P at `precision` (set: seg in {4,8,16,32}, wn in 1..7; 0, 0 = default)
@@ -44,7 +50,7 @@ private:
     };
     Status build_group(Group &g, int precision);
     Status launch_group(Group &g, const double *const *srcs, double *const *outs, const double *const *phi_sc,
-                        double scale, double *const *phis, double dt);
+                        double scale, double *const *phis, double dt, const std::vector<char> *active);
     void release();
     // every group launches on the first member's stream, so that one synchronisation and one event pair
     // cover the whole batched sweep

@@ -70,6 +70,8 @@ struct SweepArgs {
     long long spin_limit;      // polls before a wait gives up
     int adjoint;               // modal kernel: 1 = transposed sweep (reverse order; phi_scatter is mu and the
                                // fused source is w_q mu; the moments are unweighted sums over ordinates)
+    int skip;                  // batched modal launch: 1 = this problem is not swept this time (its items return
+                               // at once; nothing of it is read or written)
     const double *modal_src;   // lane kernel, moments-only forward sweeps: the packed modal source of every
                                // (cell, quadrant), [(nx+2)(ny+2)][4][N] (launch_modal_sources), or null; the
                                // partial moments are then packed modal sums (launch_reduce_modal_partials)

@@ -652,6 +652,10 @@ __global__ void __launch_bounds__(max_warps(P) * 32, 1) sweep_modal_kernel(const
             unsigned long long *dw = reinterpret_cast<unsigned long long *>(&s_args);
             for (int k = threadIdx.x; k < (int)(sizeof(SweepArgs) / 8); k += blockDim.x) dw[k] = sw[k];
             __syncthreads();
+            if (s_args.skip) {   // a problem left out of this sweep (block-uniform): take the next item
+                __syncthreads();
+                continue;
+            }
         }
         const SweepArgs &a = BATCHED ? s_args : a0;
         // the item's index within its problem (its trace buffer and partial-moment slot)

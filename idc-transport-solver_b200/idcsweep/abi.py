@@ -48,7 +48,7 @@ EXPORTED_SYMBOLS = (
     "idc_write_af2", "idc_read_af2", "idc_sweep_fused", "idc_set_tile_shape", "idc_autotune", "idc_batch_create",
     "idc_batch_add", "idc_batch_sweep", "idc_batch_autotune", "idc_batch_last_timing", "idc_batch_destroy",
     "idc_batch_set_shape", "idc_batch_get_shape", "idc_sweep_out_many", "idc_adjoint_transient",
-    "idc_set_spin_limit",
+    "idc_set_spin_limit", "idc_batch_gmres_solve",
 )
 
 
@@ -108,6 +108,8 @@ def load_library(path: str = LIB_PATH):
     lib.idc_batch_autotune.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), C.c_double, C.c_int]
     lib.idc_batch_last_timing.argtypes = [vp, _dp]
     lib.idc_batch_destroy.argtypes = [vp]
+    lib.idc_batch_gmres_solve.argtypes = [vp, C.POINTER(vp), C.c_double, C.c_double, C.c_int32, C.c_int64, C.c_int,
+                                          C.POINTER(C.c_int64), _dp]
     lib.idc_batch_set_shape.argtypes = [vp, C.c_int, C.c_int, C.c_int32, C.c_int32]
     lib.idc_batch_get_shape.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
     lib.idc_idc_integrate.argtypes = [vp, vp, vp, C.c_double, C.c_int64, C.c_int32, C.c_int32, C.c_int, C.c_int,
@@ -350,6 +352,15 @@ class Batch:
     def sweep(self, src_ptrs, out_ptrs, phi_ptrs=None, dt=np.inf, precision=PREC_FP64):
         _check(self._lib.idc_batch_sweep(self._h, self._arr(src_ptrs), self._arr(out_ptrs), self._arr(phi_ptrs),
                                          float(dt), int(precision)), "idc_batch_sweep")
+
+    def gmres_solve(self, psi_ptrs, dt=np.inf, abs_tol=1e-8, restart=30, max_its=3000, precision=PREC_FP64):
+        """In place on every member (device pointers, Q in, psi out).  Returns (iterations, residuals) lists."""
+        n = len(psi_ptrs)
+        its = (C.c_int64 * n)()
+        res = (C.c_double * n)()
+        _check(self._lib.idc_batch_gmres_solve(self._h, self._arr(psi_ptrs), float(dt), float(abs_tol), int(restart),
+                                               int(max_its), int(precision), its, res), "idc_batch_gmres_solve")
+        return list(its), list(res)
 
     def autotune(self, src_ptrs, out_ptrs, dt=np.inf, precision=PREC_FP64):
         _check(self._lib.idc_batch_autotune(self._h, self._arr(src_ptrs), self._arr(out_ptrs), float(dt),

@@ -245,6 +245,16 @@ int idc_batch_last_timing(idc_batch *b, double *ms);
  * picked, the default, or what was set; set 0, 0 to return to the default). */
 int idc_batch_set_shape(idc_batch *b, int dg_degree, int precision, int32_t seg, int32_t warps);
 int idc_batch_get_shape(idc_batch *b, int dg_degree, int precision, int32_t *seg, int32_t *warps);
+/* GMRES(restart) to abs_tol on every member's Peierls system at once (each member's problem as
+ * idc_gmres_solve solves it, with the preconditioner set on its context): every Krylov step applies the
+ * operators of all unconverged members through one batched sweep and brings their Arnoldi columns back with
+ * one synchronisation; converged members drop out of the launches.  psi_inout: host array of device
+ * pointers, one per member in order (Q on entry, psi on return); iters and final_resids (nullable): host
+ * arrays with one entry per member.  FP64 or FP32_REFINED sweeps.  IDC_ERR_NOT_CONVERGED if a member
+ * stopped at max_its.  The batched form of PETScPeierlsSolver::Solve (linear_solvers/Abstract/
+ * ImplicitSolver/PETScPeierlsSolver.cpp:423-572) for many independent problems; the reference solves one. */
+int idc_batch_gmres_solve(idc_batch *b, double *const *psi_inout, double dt, double abs_tol, int32_t restart,
+                          int64_t max_its, int precision, int64_t *iters, double *final_resids);
 int idc_batch_destroy(idc_batch *b);
 
 /* ---- discrete adjoint --------------------------------------------------------------------------------- */

@@ -103,3 +103,35 @@ def test_batched_sweep_complete_on_return():
     finally:
         for c in ctxs:
             c.close()
+
+
+@pytest.mark.parametrize("dsa", [False, True])
+def test_batched_gmres_matches_single_solves(dsa):
+    """Every member's Peierls GMRES (+ DSA) solved together, one batched sweep per Krylov step with converged
+    members skipped: the same solutions as the members' own solves to the tolerance."""
+    probs = [random_problem(12, 9, 1, 4, seed=21), lognormal(40, 2, 8, seed=22, c_range=(0.3, 0.99)),
+             lognormal(24, 1, 12, seed=23, c_range=(0.5, 0.95)), random_problem(7, 16, 2, 4, seed=24, inflow=False)]
+    tol = 1e-10
+    ctxs = [_ctx(P) for P in probs]
+    try:
+        for c in ctxs:
+            if dsa:
+                c.set_preconditioner(abi.PRECOND_DSA, 20)
+        want, want_its = [], []
+        for P, c in zip(probs, ctxs):
+            psi = P.source.copy()
+            its, res = c.gmres_solve(psi, P.dt, abs_tol=tol, restart=10, max_its=2000)
+            want.append(psi)
+            want_its.append(its)
+        psis = [torch.from_numpy(P.source).cuda() for P in probs]
+        with abi.Batch() as b:
+            for c in ctxs:
+                b.add(c)
+            its, res = b.gmres_solve([x.data_ptr() for x in psis], np.inf, abs_tol=tol, restart=10, max_its=2000)
+        for k, P in enumerate(probs):
+            assert res[k] <= tol
+            assert abs(its[k] - want_its[k]) <= 1
+            assert rel_err(psis[k].cpu().numpy(), want[k]) < 1e-8
+    finally:
+        for c in ctxs:
+            c.close()
