@@ -500,8 +500,9 @@ Status Batch::gmres_solve(double *const *psi_inout, double dt, double abs_tol, i
             for (int i = k - 1; i >= 0; --i) {
                 double sum = z.g[i];
                 for (int l = i + 1; l < k; ++l) sum -= z.H[(size_t)i * m + l] * z.yv[l];
-                z.yv[i] = -(sum / z.H[(size_t)i * m + i]);   // negated: multiaxpy subtracts
+                z.yv[i] = sum / z.H[(size_t)i * m + i];
             }
+            for (int i = 0; i < k; ++i) z.yv[i] = -z.yv[i];   // multiaxpy subtracts
             IDC_TRY_CUDA(cudaMemcpyAsync(z.c->d_small, z.yv.data(), sizeof(double) * k, cudaMemcpyHostToDevice, st));
             IDC_TRY_CUDA(launch_multiaxpy(z.x, z.dsa ? z.Zc(0) : z.V, k, z.n, z.c->d_small, z.n, st));
             if (z.resid <= abs_tol) {
