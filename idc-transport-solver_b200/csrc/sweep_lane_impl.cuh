@@ -58,16 +58,21 @@ namespace idc {
 namespace lane {
 
 constexpr int kWarps = 4;    // warps per thread block: one per SM sub-partition
-constexpr int kStages = 8;   // stages in shared memory (a power of two): a step's inputs are copied this many steps minus one ahead
+constexpr int kStages = 6;   // stages in shared memory: a step's inputs are copied this many steps minus one ahead
+constexpr int kOutBufs = 2;  // psi leaves through a ring of this many per-warp buffers
+
 
 // Doubles per (column, ordinate) slot of the trace buffer.
 __host__ __device__ constexpr int trace_slot(int P) { return P; }
 
 // Shared memory of one warp, in doubles: source stages [kStages][32][N] (lane-major, conflict-free), the
-// second source's stages (launches with one), sigma_t stages [kStages][32] (each lane its own copy) and the
-// fused scattering moments' stages [kStages][Rw][N] (copied by lane o == 0 of each row).
+// second source's stages (launches with one), sigma_t stages [kStages][32] (each lane its own copy), the
+// fused scattering moments' stages [kStages][Rw][N] (copied by lane o == 0 of each row) and the psi out
+// buffers [kOutBufs][32][N] (lane-major: row rr's SEG ordinates are the reference's contiguous row segment).
+// Every part is an even number of doubles, so each starts on a 16-byte boundary.
 __host__ __device__ constexpr size_t warp_doubles(int P, int seg, bool src2) {
-    return (size_t)kStages * 32 * P * P * (src2 ? 2 : 1) + (size_t)kStages * 32 + (size_t)kStages * (32 / seg) * P * P;
+    return (size_t)kStages * 32 * P * P * (src2 ? 2 : 1) + (size_t)kStages * 32 + (size_t)kStages * (32 / seg) * P * P +
+           (size_t)kOutBufs * 32 * P * P;
 }
 __host__ __device__ constexpr size_t block_smem_bytes(int P, int seg, bool src2) {
     return sizeof(double) * warp_doubles(P, seg, src2) * kWarps;
@@ -105,29 +110,76 @@ __device__ __forceinline__ void segment_sums(T (&v)[N], int o, int *lo, int *hi)
     }
 }
 
-// The consumer caught up with its producer (a value of column s still held the sentinel): wait until the
-// producer has written column `last` and all of column s, bounded.  Returns false if the wait gave up or
-// another warp has failed (the error word is then set).  Out of line: the hot loop stays small.
+// Global accesses under a predicate instead of a branch, so that the loop body stays one basic block and
+// the scheduler can interleave the three cells' work.  An access whose predicate is false is not made.
+__device__ __forceinline__ void st_f64_if(double *p, double v, bool pred) {
+    asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %2, 0;\n\t@q st.global.f64 [%0], %1;\n\t}" ::"l"(p), "d"(v),
+                 "r"((int)pred));
+}
+__device__ __forceinline__ void st_relaxed_f64_if(double *p, double v, bool pred) {
+    asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %2, 0;\n\t@q st.relaxed.gpu.global.f64 [%0], %1;\n\t}" ::"l"(p),
+                 "d"(v), "r"((int)pred));
+}
+// 0.0 where the predicate is false
+__device__ __forceinline__ double ld_relaxed_f64_if(const double *p, bool pred) {
+    double v;
+    asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %2, 0;\n\tmov.f64 %0, 0d0000000000000000;\n\t"
+                 "@q ld.relaxed.gpu.global.f64 %0, [%1];\n\t}"
+                 : "=d"(v)
+                 : "l"(p), "r"((int)pred));
+    return v;
+}
+// 8-byte cp.async that writes zeros into dst where the predicate is false (source size 0: nothing is read;
+// callers still pass a source inside a valid allocation)
+__device__ __forceinline__ void cp_async8_zfill(void *dst, const void *src, bool pred) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(saddr(dst)), "l"(src), "r"(pred ? 8 : 0));
+}
+__device__ __forceinline__ void cp_async8_if(void *dst, const void *src, bool pred) {
+    asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %2, 0;\n\t@q cp.async.ca.shared.global [%0], [%1], 8;\n\t}" ::"r"(
+                     saddr(dst)),
+                 "l"(src), "r"((int)pred));
+}
+
+// Bulk copies shared -> global (the copy engine reads the buffer after the issuing thread moves on): one
+// per row segment of psi.  The writes into the buffer are made visible to the copy engine by the proxy fence.
+__device__ __forceinline__ void bulk_store_if(double *dst, const double *src, unsigned bytes, bool pred) {
+    asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %3, 0;\n\t@q cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n\t}" ::"l"(dst),
+                 "r"(saddr(src)), "r"(bytes), "r"((int)pred)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+template <int n>
+__device__ __forceinline__ void bulk_wait_read() {
+    asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(n) : "memory");
+}
+template <int n>
+__device__ __forceinline__ void bulk_wait() {
+    asm volatile("cp.async.bulk.wait_group %0;" ::"n"(n) : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// The consumer caught up with its producer (a value of column s still held the sentinel): wait, bounded,
+// until the producer has written column s.  Waiting for no more than that keeps the lag between row blocks
+// at its minimum (measured on B200: waiting for two more columns of slack, to wait less often, made the
+// 256x256 Q2 S16 sweep 10-20% slower).  Returns the poll count so far, or -1 if the wait gave up or another
+// warp has failed (the error word is then set).  Out of line: the hot loop stays small; every argument is a
+// register.
 template <int P>
-__device__ __noinline__ bool wait_for_producer(const double *dep_trace, int s, int last, bool reader, int G,
-                                               int *error, long long spin_limit, long long *polls, int lane) {
-    const size_t col = (size_t)G * P;
-    for (int want = last;;) {
+__device__ __noinline__ long long wait_for_producer(const double *dep_trace, int s, bool reader, int G, int *error,
+                                                    long long spin_limit, long long polls, int lane) {
+    const double *col = dep_trace + (size_t)s * G * P;
+    for (;;) {
         bool still = false;
         if (reader) {
 #pragma unroll
-            for (int m = 0; m < P; ++m) still |= is_sentinel(ld_relaxed_f64(dep_trace + (size_t)want * col + m));
+            for (int m = 0; m < P; ++m) still |= is_sentinel(ld_relaxed_f64(col + m));
         }
-        if (!__any_sync(kFullMask, still)) {
-            if (want == s) return true;
-            want = s;
-            continue;
-        }
-        ++*polls;
-        if ((*polls & 63) == 63 && ld_relaxed(error) != kDevOk) return false;
-        if (*polls > spin_limit) {
+        if (!__any_sync(kFullMask, still)) return polls;
+        ++polls;
+        if ((polls & 63) == 63 && ld_relaxed(error) != kDevOk) return -1;
+        if (polls > spin_limit) {
             if (lane == 0) atomicCAS(error, kDevOk, kDevTimeout);
-            return false;
+            return -1;
         }
         __nanosleep(64);
     }
@@ -140,28 +192,36 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
     // quadrant signs: flips of the cell values (exact), traversal directions (reversed for the transpose)
     const bool XN = item.quadrant >= 2, YN = (item.quadrant & 1) != 0;
     const bool TX = XN != ADJ, TY = YN != ADJ;
+    const int quadrant = item.quadrant;
     const int rr = lane / SEG, o = lane - rr * SEG;
     const int row_w = item.row_block * Rw;
     const int row = row_w + rr;
     const bool row_valid = row < a.ny;
     const bool act = (o < item.q_count) && row_valid;
     const int q = item.q_begin + (act ? o : 0);
-    const int j = TY ? (a.ny - row) : (1 + row);
+    const int j = row_valid ? (TY ? (a.ny - row) : (1 + row)) : 1;
     const int nx = a.nx;
     const size_t plane = (size_t)a.nq * N;
     const size_t istride = (size_t)(a.ny + 2) * plane;
+    const size_t cstride = (size_t)(a.ny + 2);
     const bool has_dep = item.dep >= 0;
     const bool has_consumer = row_w + Rw < a.ny;
+    const bool has_scatter = !PHI && a.phi_scatter != nullptr;
     const int T = nx + Rw - 1;
     const size_t tcol = (size_t)a.G * P;   // doubles per trace column
     const int xi0 = TX ? nx : 1, xis = TX ? -1 : 1;   // array x index of sweep column c: xi0 + xis * c
     const unsigned xm = XN ? 0x80000000u : 0u, ym = YN ? 0x80000000u : 0u;
     auto fmask = [&](int k) { return ((k / P) & 1 ? xm : 0u) ^ ((k % P) & 1 ? ym : 0u); };   // k = e + P d
+    const double *valid_addr = a.sigma_t;   // a source address for accesses that are not made
 
     double *stage = wsm + (size_t)lane * N;                            // step t at + (t % D) * 32 * N
     double *stage2 = wsm + (size_t)D * 32 * N + (size_t)lane * N;      // (SRC2 launches only)
     double *sig = wsm + (size_t)D * 32 * N * (SRC2 ? 2 : 1) + lane;    // + (t % D) * 32
     double *mom = wsm + (size_t)D * 32 * N * (SRC2 ? 2 : 1) + (size_t)D * 32 + (size_t)rr * N;   // + (t % D) * Rw * N
+    double *obuf = wsm + (size_t)D * 32 * N * (SRC2 ? 2 : 1) + (size_t)D * 32 + (size_t)D * Rw * N;   // + b * 32 * N
+    // psi rows leave by bulk copies when every row segment starts and ends on a 16-byte boundary
+    const bool bulk_out = a.out != nullptr && ((size_t)a.out & 15) == 0 && ((size_t)a.nq * N) % 2 == 0 &&
+                          ((size_t)item.q_begin * N) % 2 == 0 && ((size_t)item.q_count * N) % 2 == 0;
 
     double axd = 0.0, ayd = 0.0, wq = 0.0;
     if (act) {
@@ -181,77 +241,67 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
         for (int m = 0; m < P; ++m) f[m] = TC(in[m]);
     }
 
-    // row 0 reads its y traces from the item above (sentinel-armed) or the ghost row's inflow
+    // row 0 reads its y traces from the item above (sentinel-armed) or the ghost row's inflow, the same way
     const bool reader = rr == 0 && o < item.q_count && row_valid;
     double *dep_trace = has_dep ? a.trace + (size_t)item.dep * a.trace_stride + (size_t)o * P : nullptr;
-    const double *inflow_y = (!has_dep && a.inflow && !ADJ) ? a.inflow + (size_t)q * P : nullptr;
+    const double *tin = has_dep ? dep_trace : ((a.inflow && !ADJ) ? a.inflow + (size_t)q * P : nullptr);
+    const size_t tin_col = has_dep ? tcol : (size_t)a.nq * P;
+    const bool tin_ok = reader && tin != nullptr;
     double *out_trace = a.trace + (size_t)it_index * a.trace_stride + (size_t)o * P;
     const bool writer = has_consumer && rr == Rw - 1 && o < item.q_count;
     auto load_trace = [&](int c, double (&v)[P]) {
+        const bool p = tin_ok && c < nx;
+        const double *ptr = p ? tin + (size_t)c * tin_col : valid_addr;
 #pragma unroll
-        for (int m = 0; m < P; ++m) v[m] = 0.0;
-        if (reader && c < nx) {
-            if (has_dep) {
-#pragma unroll
-                for (int m = 0; m < P; ++m) v[m] = ld_relaxed_f64(dep_trace + (size_t)c * tcol + m);
-            } else if (inflow_y) {
-#pragma unroll
-                for (int m = 0; m < P; ++m) v[m] = inflow_y[(size_t)c * a.nq * P + m];
-            }
-        }
+        for (int m = 0; m < P; ++m) v[m] = ld_relaxed_f64_if(ptr + m, p);
     };
 
-    // step t's inputs into stage t % D, one cp.async group per step (empty past the last step)
+    // step t's inputs into stage t % D, one cp.async group per step; a cell outside the row gets zeros
     auto prefetch = [&](int t) {
         const int c = t - rr;
-        if (t < T && row_valid && c >= 0 && c < nx) {
-            const int ci = xi0 + xis * c;
-            const size_t base = (size_t)ci * istride + (size_t)j * plane + (size_t)q * N;
-            const size_t cidx = (size_t)ci * (a.ny + 2) + j;
-            if (PHI && act) {   // the cell's packed modal source of this quadrant (the same for the row segment)
-                double *d = stage + (size_t)(t % D) * 32 * N;
-                const double *g = a.modal_src + (cidx * 4 + item.quadrant) * N;
+        const bool in = row_valid && c >= 0 && c < nx;
+        const size_t cidx = in ? (size_t)(xi0 + xis * c) * cstride + j : 0;
+        double *d = stage + (size_t)(t % D) * 32 * N;
+        if constexpr (PHI) {   // the cell's packed modal source of this quadrant (the same for the row segment)
+            const double *g = a.modal_src + (cidx * 4 + quadrant) * N;
 #pragma unroll
-                for (int k = 0; k < N; ++k) cp_async8(d + k, g + k);
-            }
-            if (!PHI && act && a.src) {
-                double *d = stage + (size_t)(t % D) * 32 * N;
+            for (int k = 0; k < N; ++k) cp_async8_zfill(d + k, g + k, in && act);
+        } else {
+            const bool ps = in && act && a.src != nullptr;
+            const double *g = ps ? a.src + cidx * plane + (size_t)q * N : valid_addr;
 #pragma unroll
-                for (int k = 0; k < N; ++k) cp_async8(d + k, a.src + base + k);
-            }
-            if (SRC2 && act) {
-                double *d = stage2 + (size_t)(t % D) * 32 * N;
+            for (int k = 0; k < N; ++k) cp_async8_zfill(d + k, g + k, ps);
+        }
+        if constexpr (SRC2) {
+            double *d2 = stage2 + (size_t)(t % D) * 32 * N;
+            const double *g2 = (in && act) ? a.src2 + cidx * plane + (size_t)q * N : valid_addr;
 #pragma unroll
-                for (int k = 0; k < N; ++k) cp_async8(d + k, a.src2 + base + k);
-            }
-            cp_async8(sig + (size_t)(t % D) * 32, a.sigma_t + cidx);
-            if (!PHI && o == 0 && a.phi_scatter) {
-                double *d = mom + (size_t)(t % D) * Rw * N;
+            for (int k = 0; k < N; ++k) cp_async8_zfill(d2 + k, g2 + k, in && act);
+        }
+        cp_async8_zfill(sig + (size_t)(t % D) * 32, a.sigma_t + cidx, in);
+        if (!PHI) {   // lane o == 0 of a row copies the cell's fused scattering moments (one copy per row)
+            const bool pm = in && o == 0 && has_scatter;
+            const double *gm = pm ? a.phi_scatter + cidx * N : valid_addr;
+            double *dm = mom + (size_t)(t % D) * Rw * N;
 #pragma unroll
-                for (int k = 0; k < N; ++k) cp_async8(d + k, a.phi_scatter + cidx * N + k);
-            }
+            for (int k = 0; k < N; ++k) cp_async8_if(dm + k, gm + k, pm);
         }
         cp_commit();
     };
 
-    // step t's modal source and reciprocals from its landed stage (the caller has waited for its group)
-    auto prepare = [&](int t, TC (&S)[N], ModalRecip<P, TC> &r) {
+    // step t's raw inputs from its landed stage: the source (with the second source and the fused scattering
+    // source) and sigma_t + 1/dt
+    auto load_inputs = [&](int t, double (&src)[N], double &st) {
         const double *sp = stage + (size_t)(t % D) * 32 * N;
-        if constexpr (PHI) {
 #pragma unroll
-            for (int k = 0; k < N; ++k) S[k] = TC(sp[k]);
-            r = modal_recip<P, TC>(od, TC(sig[(size_t)(t % D) * 32] + a.inv_dt));
-            return;
-        }
-        double src[N];
-#pragma unroll
-        for (int k = 0; k < N; ++k) src[k] = a.src ? sp[k] : 0.0;
+        for (int k = 0; k < N; ++k) src[k] = sp[k];
         if constexpr (SRC2) {
             const double *sp2 = stage2 + (size_t)(t % D) * 32 * N;
 #pragma unroll
             for (int k = 0; k < N; ++k) src[k] = fma(a.src2_scale, sp2[k], src[k]);
         }
-        if (!PHI && a.phi_scatter) {   // lane o == 0's copy of the cell's moments, handed to its row segment
+        st = sig[(size_t)(t % D) * 32] + a.inv_dt;
+        if (has_scatter) {   // lane o == 0's copy of the cell's moments, handed to its row segment
             const double *mp = mom + (size_t)(t % D) * Rw * N;
 #pragma unroll
             for (int k = 0; k < N; ++k) {
@@ -262,14 +312,23 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
                     src[k] = fma(wq, mk, src[k]);
             }
         }
-        r = modal_recip<P, TC>(od, TC(sig[(size_t)(t % D) * 32] + a.inv_dt));
-        TC sv[N];
+    };
+    // the modal source and the reciprocal denominators of the raw inputs
+    auto transform = [&](const double (&src)[N], double st, TC (&S)[N], ModalRecip<P, TC> &r) {
+        r = modal_recip<P, TC>(od, TC(st));
+        if constexpr (PHI) {
 #pragma unroll
-        for (int k = 0; k < N; ++k) sv[k] = flip_by(TC(src[k]), fmask(k));
-        modal_forward<P, false, false, TC, ADJ>(S, sv);
+            for (int k = 0; k < N; ++k) S[k] = TC(src[k]);
+        } else {
+            TC sv[N];
+#pragma unroll
+            for (int k = 0; k < N; ++k) sv[k] = flip_by(TC(src[k]), fmask(k));
+            modal_forward<P, false, false, TC, ADJ>(S, sv);
+        }
     };
 
     const int phi_slot = a.phi_slots > 0 ? it_index % a.phi_slots : 0;
+    double *phi_base = a.phi_part ? a.phi_part + (size_t)phi_slot * a.phi_slot_stride : nullptr;
     long long polls = 0;
 
     // prologue: stages 0 .. D-2 in flight, step 0 prepared, row 0's trace of column 0 loaded
@@ -278,7 +337,11 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
     cp_wait<D - 2>();
     TC S[N];
     ModalRecip<P, TC> r;
-    prepare(0, S, r);
+    {
+        double src0[N], st0;
+        load_inputs(0, src0, st0);
+        transform(src0, st0, S, r);
+    }
     double tnext[P];
     load_trace(0, tnext);
     TC gprev[P], Zp[N];
@@ -287,36 +350,40 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
 #pragma unroll
     for (int k = 0; k < N; ++k) Zp[k] = TC(0);
 
-    // iteration s: chain of step s (s < T), finish of step s - 1 (s >= 1), inputs of step s + 1
+    // Iteration s: chain of step s (s < T), finish of step s - 1 (s >= 1), inputs of step s + 1.  After the
+    // loads at its top (and the wait for a producer, rarely taken) the iteration is one basic block.
     for (int s = 0; s <= T; ++s) {
         const int c = s - rr;
         const bool valid = act && c >= 0 && c < nx;
+
+        // ---- step s + 1's raw inputs (its group was committed D - 2 iterations ago) ----
+        cp_wait<D - 3>();
+        double srcn[N], stn;
+        load_inputs(s + 1, srcn, stn);
 
         // ---- the y trace in: from the row below (previous step); row 0 from the item above ----
         TC g[P];
 #pragma unroll
         for (int m = 0; m < P; ++m) g[m] = __shfl_up_sync(kFullMask, gprev[m], SEG);
-        if (s < nx) {   // row 0 consumes column s (loaded an iteration ago)
-            if (has_dep) {
-                bool bad = false;
+        if (has_dep) {
+            bool bad = false;
 #pragma unroll
-                for (int m = 0; m < P; ++m) bad |= reader && is_sentinel(tnext[m]);
-                if (__any_sync(kFullMask, bad)) {   // caught up with the producer: wait for two columns of slack
-                    if (!wait_for_producer<P>(dep_trace, s, min(s + 2, nx - 1), reader, a.G, a.error, a.spin_limit,
-                                              &polls, lane))
-                        break;
-                    load_trace(s, tnext);
-                }
-                if (reader) {   // re-arm the consumed column for the next sweep
-#pragma unroll
-                    for (int m = 0; m < P; ++m) st_relaxed_f64(dep_trace + (size_t)s * tcol + m, sentinel_value());
-                }
-            }
-            if (rr == 0) {
-#pragma unroll
-                for (int m = 0; m < P; ++m) g[m] = TC(tnext[m]);
+            for (int m = 0; m < P; ++m) bad |= reader && s < nx && is_sentinel(tnext[m]);
+            if (__any_sync(kFullMask, bad)) {   // caught up with the producer: wait for two columns of slack
+                polls = wait_for_producer<P>(dep_trace, s, reader, a.G, a.error, a.spin_limit,
+                                             polls, lane);
+                if (polls < 0) break;
+                load_trace(s, tnext);
             }
         }
+        {   // re-arm the consumed column for the next sweep
+            const bool p = has_dep && reader && s < nx;
+            double *ptr = p ? dep_trace + (size_t)s * tcol : out_trace;
+#pragma unroll
+            for (int m = 0; m < P; ++m) st_relaxed_f64_if(ptr + m, sentinel_value(), p);
+        }
+#pragma unroll
+        for (int m = 0; m < P; ++m) g[m] = (rr == 0) ? TC(tnext[m]) : g[m];
         load_trace(s + 1, tnext);
 
         // ---- the chain of step s ----
@@ -329,16 +396,20 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
             f[m] = valid ? fn[m] : f[m];
             gprev[m] = valid ? gout[m] : TC(0);
         }
-        const int cout = s - (Rw - 1);   // traces out: relaxed stores, each value its own flag
-        if (writer && cout >= 0 && cout < nx) {
+        {   // traces out: relaxed stores, each value its own flag
+            const int cout = s - (Rw - 1);
+            const bool p = writer && cout >= 0 && cout < nx;
+            double *ptr = p ? out_trace + (size_t)cout * tcol : out_trace;
 #pragma unroll
-            for (int m = 0; m < P; ++m) st_relaxed_f64(out_trace + (size_t)cout * tcol + m, double(gout[m]));
+            for (int m = 0; m < P; ++m) st_relaxed_f64_if(ptr + m, double(gout[m]), p);
         }
 
         // ---- the finish of step s - 1: cell dofs, psi, moments (PHI: the packed modal moments) ----
         {   // (at s = 0 nothing is valid: Zp is zero and no store is made)
             const int cp = c - 1;
-            const bool vp = act && cp >= 0 && cp < nx;
+            const bool inrow = row_valid && cp >= 0 && cp < nx;
+            const bool vp = act && inrow;
+            const size_t cidx = inrow ? (size_t)(xi0 + xis * cp) * cstride + j : 0;
             TC x[N];
             if constexpr (PHI) {
 #pragma unroll
@@ -347,35 +418,44 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
                 modal_backward<P, false, false, TC, ADJ>(x, Zp);
 #pragma unroll
                 for (int k = 0; k < N; ++k) x[k] = flip_by(x[k], fmask(k));
-            }
-            if (!PHI && a.out && vp) {
-                double *op = a.out + (size_t)(xi0 + xis * cp) * istride + (size_t)j * plane + (size_t)q * N;
+                double *ob = obuf + (size_t)(s & (kOutBufs - 1)) * 32 * N;
+                bulk_wait_read<kOutBufs - 1>();   // the copy that read this buffer kOutBufs steps ago is done
+                __syncwarp();
 #pragma unroll
-                for (int k = 0; k < N; ++k) op[k] = double(x[k]);
-            }
-            if (a.phi_part) {
+                for (int k = 0; k < N; ++k) ob[(size_t)lane * N + k] = double(x[k]);
+                fence_proxy_async_smem();
+                __syncwarp();
+                {
+                    const bool pb = bulk_out && o == 0 && inrow;
+                    double *dst = pb ? a.out + cidx * plane + (size_t)item.q_begin * N : out_trace;
+                    bulk_store_if(dst, ob + (size_t)rr * SEG * N, (unsigned)(item.q_count * N * sizeof(double)), pb);
+                    bulk_commit();
+                }
+                {   // rows whose segments are not 16-byte aligned: per-lane stores
+                    const bool ps = vp && a.out != nullptr && !bulk_out;
+                    double *op = ps ? a.out + cidx * plane + (size_t)q * N : out_trace;
 #pragma unroll
-                for (int k = 0; k < N; ++k) x[k] = vp ? (ADJ ? x[k] : TC(wq) * x[k]) : TC(0);
-                int lo = 0, hi = N;
-                segment_sums<N, SEG>(x, o, &lo, &hi);
-                if (row_valid && cp >= 0 && cp < nx) {
-                    double *pp = a.phi_part + (size_t)phi_slot * a.phi_slot_stride +
-                                 ((size_t)(xi0 + xis * cp) * (a.ny + 2) + j) * N;
-#pragma unroll
-                    for (int i = 0; i < (N + SEG - 1) / SEG; ++i)
-                        if (lo + i < hi) pp[lo + i] = double(x[i]);
+                    for (int k = 0; k < N; ++k) st_f64_if(op + k, double(x[k]), ps);
                 }
             }
+#pragma unroll
+            for (int k = 0; k < N; ++k) x[k] = vp ? (ADJ ? x[k] : TC(wq) * x[k]) : TC(0);
+            int lo = 0, hi = N;
+            segment_sums<N, SEG>(x, o, &lo, &hi);
+            const bool pp = inrow && phi_base != nullptr;
+            double *pt = pp ? phi_base + cidx * N : out_trace;
+#pragma unroll
+            for (int i = 0; i < (N + SEG - 1) / SEG; ++i) st_f64_if(pt + lo + i, double(x[i]), pp && lo + i < hi);
         }
 #pragma unroll
         for (int k = 0; k < N; ++k) Zp[k] = Z[k];
 
-        // ---- the inputs of step s + 1 ----
-        prefetch(s + D - 1);   // into the stage of step s - 1 (read an iteration ago)
-        cp_wait<D - 2>();      // step s + 1's group has landed
-        prepare(s + 1, S, r);
+        // ---- the inputs of step s + 1, and the copies of step s + D - 1 ----
+        transform(srcn, stn, S, r);
+        prefetch(s + D - 1);   // into the stage of step s - 1 (read two iterations ago)
     }
     cp_wait<0>();
+    bulk_wait<0>();
 }
 
 template <int P, int SEG, bool ADJ, bool SRC2, bool PHI, typename TC>
