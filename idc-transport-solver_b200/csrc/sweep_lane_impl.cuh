@@ -60,6 +60,7 @@ namespace lane {
 constexpr int kWarps = 4;    // warps per thread block: one per SM sub-partition
 constexpr int kStages = 6;   // stages in shared memory: a step's inputs are copied this many steps minus one ahead
 constexpr int kOutBufs = 2;  // psi leaves through a ring of this many per-warp buffers
+constexpr int kMomStride = 34;   // doubles per moment index k in the moment buffer (32 lanes + 2: conflict-free sums)
 
 
 // Doubles per (column, ordinate) slot of the trace buffer.
@@ -68,11 +69,13 @@ __host__ __device__ constexpr int trace_slot(int P) { return P; }
 // Shared memory of one warp, in doubles: source stages [kStages][32][N] (lane-major, conflict-free), the
 // second source's stages (launches with one), sigma_t stages [kStages][32] (each lane its own copy), the
 // fused scattering moments' stages [kStages][Rw][N] (copied by lane o == 0 of each row) and the psi out
-// buffers [kOutBufs][32][N] (lane-major: row rr's SEG ordinates are the reference's contiguous row segment).
+// buffers [kOutBufs][32][N] (lane-major: row rr's SEG ordinates are the reference's contiguous row segment)
+// and, for 16-wide segments, the weighted moment values [N][kMomStride] (k-major: a row segment's SEG values
+// of one k are adjacent).
 // Every part is an even number of doubles, so each starts on a 16-byte boundary.
 __host__ __device__ constexpr size_t warp_doubles(int P, int seg, bool src2) {
     return (size_t)kStages * 32 * P * P * (src2 ? 2 : 1) + (size_t)kStages * 32 + (size_t)kStages * (32 / seg) * P * P +
-           (size_t)kOutBufs * 32 * P * P;
+           (size_t)kOutBufs * 32 * P * P + (seg >= 16 ? (size_t)P * P * kMomStride : 0);
 }
 __host__ __device__ constexpr size_t block_smem_bytes(int P, int seg, bool src2) {
     return sizeof(double) * warp_doubles(P, seg, src2) * kWarps;
@@ -219,17 +222,21 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
     double *sig = wsm + (size_t)D * 32 * N * (SRC2 ? 2 : 1) + lane;    // + (t % D) * 32
     double *mom = wsm + (size_t)D * 32 * N * (SRC2 ? 2 : 1) + (size_t)D * 32 + (size_t)rr * N;   // + (t % D) * Rw * N
     double *obuf = wsm + (size_t)D * 32 * N * (SRC2 ? 2 : 1) + (size_t)D * 32 + (size_t)D * Rw * N;   // + b * 32 * N
+    double *mbuf = obuf + (size_t)kOutBufs * 32 * N;   // [N][kMomStride]
     // psi rows leave by bulk copies when every row segment starts and ends on a 16-byte boundary
     const bool bulk_out = a.out != nullptr && ((size_t)a.out & 15) == 0 && ((size_t)a.nq * N) % 2 == 0 &&
                           ((size_t)item.q_begin * N) % 2 == 0 && ((size_t)item.q_count * N) % 2 == 0;
 
-    double axd = 0.0, ayd = 0.0, wq = 0.0;
+    // an inactive lane runs the cell step of a unit ordinate (finite values) with moment weight zero, so that
+    // the moment sums need no selects
+    double axd = 1.0, ayd = 1.0, wq = 0.0;
     if (act) {
         axd = fabs(a.xi[q]) / a.dx;
         ayd = fabs(a.eta[q]) / a.dy;
         wq = a.w[q];
     }
     const ModalOrdinate<P, TC> od = modal_ordinate<P, TC, ADJ>(axd, ayd);
+    const TC wv = act ? (ADJ ? TC(1) : TC(wq)) : TC(0);   // moment weight (the transpose sums unweighted)
 
     // the row's x trace entering its first column (ghost-column inflow; zero for the transposed sweep)
     TC f[P];
@@ -279,8 +286,8 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
             for (int k = 0; k < N; ++k) cp_async8_zfill(d2 + k, g2 + k, in && act);
         }
         cp_async8_zfill(sig + (size_t)(t % D) * 32, a.sigma_t + cidx, in);
-        if (!PHI) {   // lane o == 0 of a row copies the cell's fused scattering moments (one copy per row)
-            const bool pm = in && o == 0 && has_scatter;
+        if (has_scatter) {   // lane o == 0 of a row copies the cell's fused scattering moments (one copy per row)
+            const bool pm = in && o == 0;
             const double *gm = pm ? a.phi_scatter + cidx * N : valid_addr;
             double *dm = mom + (size_t)(t % D) * Rw * N;
 #pragma unroll
@@ -327,11 +334,24 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
         }
     };
 
+    // psi of step t from its out buffer (filled at iteration t + 1) with per-lane stores (row segments that are
+    // not 16-byte aligned)
+    auto store_psi_lanes = [&](int t) {
+        const int ct = t - rr;
+        const bool ps = act && ct >= 0 && ct < nx;
+        const double *ob = obuf + (size_t)((t + 1) & (kOutBufs - 1)) * 32 * N + (size_t)lane * N;
+        double *op = ps ? a.out + ((size_t)(xi0 + xis * ct) * cstride + j) * plane + (size_t)q * N : out_trace;
+#pragma unroll
+        for (int k = 0; k < N; ++k) st_f64_if(op + k, ob[k], ps);
+    };
+    const bool lane_out = !PHI && a.out != nullptr && !bulk_out;
+
     const int phi_slot = a.phi_slots > 0 ? it_index % a.phi_slots : 0;
     double *phi_base = a.phi_part ? a.phi_part + (size_t)phi_slot * a.phi_slot_stride : nullptr;
     long long polls = 0;
 
-    // prologue: stages 0 .. D-2 in flight, step 0 prepared, row 0's trace of column 0 loaded
+    // prologue: stages 0 .. D-1 in flight, step 0 prepared, step 1's raw inputs loaded, row 0's trace of
+    // column 0 loaded
 #pragma unroll
     for (int t = 0; t < D - 1; ++t) prefetch(t);
     cp_wait<D - 2>();
@@ -342,6 +362,10 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
         load_inputs(0, src0, st0);
         transform(src0, st0, S, r);
     }
+    double srcn[N], stn;
+    cp_wait<D - 3>();
+    load_inputs(1, srcn, stn);
+    prefetch(D - 1);
     double tnext[P];
     load_trace(0, tnext);
     TC gprev[P], Zp[N];
@@ -350,16 +374,12 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
 #pragma unroll
     for (int k = 0; k < N; ++k) Zp[k] = TC(0);
 
-    // Iteration s: chain of step s (s < T), finish of step s - 1 (s >= 1), inputs of step s + 1.  After the
-    // loads at its top (and the wait for a producer, rarely taken) the iteration is one basic block.
+    // Iteration s: the y trace in (and the wait for a producer, rarely taken); then one basic block with the
+    // chain of step s (s < T) first, as it is the wavefront's critical path, the finish of step s - 1 and the
+    // transform of step s + 1's inputs; then the loads and copies for later steps.
     for (int s = 0; s <= T; ++s) {
         const int c = s - rr;
         const bool valid = act && c >= 0 && c < nx;
-
-        // ---- step s + 1's raw inputs (its group was committed D - 2 iterations ago) ----
-        cp_wait<D - 3>();
-        double srcn[N], stn;
-        load_inputs(s + 1, srcn, stn);
 
         // ---- the y trace in: from the row below (previous step); row 0 from the item above ----
         TC g[P];
@@ -408,7 +428,6 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
         {   // (at s = 0 nothing is valid: Zp is zero and no store is made)
             const int cp = c - 1;
             const bool inrow = row_valid && cp >= 0 && cp < nx;
-            const bool vp = act && inrow;
             const size_t cidx = inrow ? (size_t)(xi0 + xis * cp) * cstride + j : 0;
             TC x[N];
             if constexpr (PHI) {
@@ -418,41 +437,64 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
                 modal_backward<P, false, false, TC, ADJ>(x, Zp);
 #pragma unroll
                 for (int k = 0; k < N; ++k) x[k] = flip_by(x[k], fmask(k));
-                double *ob = obuf + (size_t)(s & (kOutBufs - 1)) * 32 * N;
-                bulk_wait_read<kOutBufs - 1>();   // the copy that read this buffer kOutBufs steps ago is done
-                __syncwarp();
+            }
+            double *ob = obuf + (size_t)(s & (kOutBufs - 1)) * 32 * N;
+            if constexpr (!PHI) bulk_wait_read<kOutBufs - 1>();   // the copy that read this buffer is done
+            __syncwarp();   // and every lane's reads of the buffers in the previous iterations
+            if constexpr (!PHI) {
 #pragma unroll
                 for (int k = 0; k < N; ++k) ob[(size_t)lane * N + k] = double(x[k]);
-                fence_proxy_async_smem();
-                __syncwarp();
-                {
-                    const bool pb = bulk_out && o == 0 && inrow;
-                    double *dst = pb ? a.out + cidx * plane + (size_t)item.q_begin * N : out_trace;
-                    bulk_store_if(dst, ob + (size_t)rr * SEG * N, (unsigned)(item.q_count * N * sizeof(double)), pb);
-                    bulk_commit();
-                }
-                {   // rows whose segments are not 16-byte aligned: per-lane stores
-                    const bool ps = vp && a.out != nullptr && !bulk_out;
-                    double *op = ps ? a.out + cidx * plane + (size_t)q * N : out_trace;
-#pragma unroll
-                    for (int k = 0; k < N; ++k) st_f64_if(op + k, double(x[k]), ps);
-                }
             }
+            if constexpr (SEG >= 16) {
 #pragma unroll
-            for (int k = 0; k < N; ++k) x[k] = vp ? (ADJ ? x[k] : TC(wq) * x[k]) : TC(0);
-            int lo = 0, hi = N;
-            segment_sums<N, SEG>(x, o, &lo, &hi);
+                for (int k = 0; k < N; ++k) mbuf[k * kMomStride + lane] = double(wv * x[k]);
+            }
+            if constexpr (!PHI) fence_proxy_async_smem();
+            __syncwarp();
+            if constexpr (!PHI) {   // row rr's segment: one bulk copy by lane o == 0
+                const bool pb = bulk_out && o == 0 && inrow;
+                double *dst = pb ? a.out + cidx * plane + (size_t)item.q_begin * N : out_trace;
+                bulk_store_if(dst, ob + (size_t)rr * SEG * N, (unsigned)(item.q_count * N * sizeof(double)), pb);
+                bulk_commit();
+            }
+            // the moments of row rr: sums of the SEG weighted values in fixed trees, one partial per ordinate
+            // chunk (added in a fixed order by the reduction kernel: bitwise reproducible).  16-wide segments
+            // sum moment k = o in ordinate order from the shared buffer; narrower ones by a shuffle butterfly
+            // (measured on B200: each is the faster one at its width).
             const bool pp = inrow && phi_base != nullptr;
             double *pt = pp ? phi_base + cidx * N : out_trace;
+            if constexpr (SEG >= 16) {
+                const int k = o < N ? o : N - 1;
+                const double2 *mv = reinterpret_cast<const double2 *>(mbuf + k * kMomStride + rr * SEG);
+                double2 v = mv[0];
+                double sum = v.x + v.y;
 #pragma unroll
-            for (int i = 0; i < (N + SEG - 1) / SEG; ++i) st_f64_if(pt + lo + i, double(x[i]), pp && lo + i < hi);
+                for (int h = 1; h < SEG / 2; ++h) {
+                    v = mv[h];
+                    sum += v.x;
+                    sum += v.y;
+                }
+                st_f64_if(pt + k, sum, pp && o < N);
+            } else {
+#pragma unroll
+                for (int k = 0; k < N; ++k) x[k] = wv * x[k];
+                int lo = 0, hi = N;
+                segment_sums<N, SEG>(x, o, &lo, &hi);
+#pragma unroll
+                for (int i = 0; i < (N + SEG - 1) / SEG; ++i) st_f64_if(pt + lo + i, double(x[i]), pp && lo + i < hi);
+            }
         }
 #pragma unroll
         for (int k = 0; k < N; ++k) Zp[k] = Z[k];
 
-        // ---- the inputs of step s + 1, and the copies of step s + D - 1 ----
+        // ---- the inputs of step s + 1 ----
         transform(srcn, stn, S, r);
-        prefetch(s + D - 1);   // into the stage of step s - 1 (read two iterations ago)
+
+        // ---- step s + 2's raw inputs (copied D - 2 iterations ago), the copies of step s + D ----
+        if (lane_out) store_psi_lanes(s - 1);
+        cp_wait<D - 3>();
+        load_inputs(s + 2, srcn, stn);
+        prefetch(s + D);   // into the stage of step s (read two iterations ago)
     }
     cp_wait<0>();
     bulk_wait<0>();
