@@ -9,32 +9,38 @@
 // order) of one quadrant for one chunk of <= SEG ordinates, swept across all columns.  Lane (rr, o) =
 // (lane / SEG, lane % SEG) owns ordinate q_begin + o on row rr; row rr runs one column behind row rr-1 and
 // takes its y trace by __shfl_up, the x trace stays in the lane.  Iteration s of a warp does, for every
-// lane, all the work of three cells, with no barrier between them, so the compiler can interleave their
-// instructions and each hides the others' latencies:
+// lane, the work of three cells:
 //   * the chain of step s: the y trace in, the modal cell step, the traces out (the only dependency from
 //     cell to cell, so the only part whose latency sits on the wavefront's critical path);
-//   * the finish of step s - 1: the backward transform, the psi store, and the row segment's moment sums
-//     by a butterfly of shuffles (one partial per ordinate chunk, each sum a fixed tree, added in a fixed
-//     order by reduce_phi_partials: bitwise reproducible);
-//   * the inputs of step s + 1: its source dofs and sigma_t (and the second source), copied into shared
-//     memory by cp.async kStages - 1 steps ahead, each lane its own (lane o == 0 of a row copies the fused
-//     scattering moments and hands them to its row by shuffles), the forward modal transform and the
-//     reciprocal denominators.
-// The loop body is one iteration for every quadrant (the quadrant's sign flips are applied to the cell
-// values at run time as sign-bit flips, exact), so the hot loop stays small for the instruction caches.
-// Four warps per thread block, one per SM sub-partition; a warp may hold up to 255 registers.  Measured on
-// B200: one warp with enough independent work issues FP64 at the sub-partition's full rate.
+//   * the finish of step s - 1: the backward transform; psi through a per-warp shared buffer whose rows are
+//     the reference's contiguous row segments, one bulk copy (cp.async.bulk) per row segment; the row
+//     segment's moment sums (a shuffle butterfly for 4- and 8-wide segments, sums over a k-major shared
+//     buffer for 16-wide ones), one partial per ordinate chunk, each a fixed tree, added in a fixed order by
+//     reduce_phi_partials: bitwise reproducible;
+//   * the inputs of step s + 1: the forward modal transform and the reciprocal denominators of its source
+//     dofs and sigma_t (and second source, and fused scattering moments), which were copied into shared
+//     memory by cp.async kStages - 2 iterations earlier.
+// After the y trace's arrival (and, rarely, a wait for the producer) the chain, the finish and the transform
+// are one basic block with the chain first: every global access in it is predicated instead of branched
+// around, so the scheduler interleaves the three cells' instructions.  The loads and copies for later steps
+// and the work behind uniform branches (scattering moments, psi rows that are not 16-byte aligned) follow in
+// a tail section.  Measured on B200 at 256x256 Q2 S16 (FP64): the branchy form of the same work ran its
+// phases one after another (the per-phase times summed to the iteration time) and scattered 8-byte psi
+// stores, 32 sectors per instruction, were a third of the kernel's time.  The loop body is one iteration for
+// every quadrant (the quadrant's sign flips are applied to the cell values at run time as sign-bit flips,
+// exact), so the hot loop stays small for the instruction caches.  Four warps per thread block, one per SM
+// sub-partition.
 //
 // Between row blocks: the warp's last row writes its outgoing y traces, column by column, into the item's
-// trace buffer with relaxed 8-byte stores; row 0 of the item below loads column s + 1 with relaxed loads
-// at iteration s (a whole iteration, longer than an L2 round trip, before use).  A value still holding the
-// NaN-payload sentinel means the consumer has caught up with its producer: it then polls (bounded) until
-// the producer is two columns further, which gives it slack for the next loads.  The consumer writes the
-// sentinel back after use.  The first row block reads the ghost row's inflow traces (inflow_traces_kernel)
-// the same way.  Items are dequeued per warp in row-block order from an atomic counter, so an item's
-// producer is always held by a running warp: no deadlock, and no thread block needs any other to be
-// resident.  Every wait is bounded (spin_limit); on expiry the warp records kDevTimeout in the device
-// error word and leaves, and every other warp leaves when it sees the word.
+// trace buffer with relaxed 8-byte stores; row 0 of the item below loads column s + 1 with relaxed loads at
+// iteration s.  A value still holding the NaN-payload sentinel means the consumer has caught up with its
+// producer: it then polls (bounded) until the producer has written that column, and no further, which
+// keeps the lag between row blocks at its minimum.  The consumer writes the sentinel back after use.  The
+// first row block reads the ghost row's inflow traces (inflow_traces_kernel) the same way.  Items are
+// dequeued per warp in row-block order from an atomic counter, so an item's producer is always held by a
+// running warp: no deadlock, and no thread block needs any other to be resident.  Every wait is bounded
+// (spin_limit); on expiry the warp records kDevTimeout in the device error word and leaves, and every other
+// warp leaves when it sees the word.
 //
 // Transposed sweep (ADJ): reverse traversal order per quadrant, the transposed cell operator and coupling
 // of modal_cell.cuh, zero inflow, the fused source w_q * mu and unweighted moment sums (the transposes of
@@ -61,7 +67,6 @@ constexpr int kWarps = 4;    // warps per thread block: one per SM sub-partition
 constexpr int kStages = 6;   // stages in shared memory: a step's inputs are copied this many steps minus one ahead
 constexpr int kOutBufs = 2;  // psi leaves through a ring of this many per-warp buffers
 constexpr int kMomStride = 34;   // doubles per moment index k in the moment buffer (32 lanes + 2: conflict-free sums)
-
 
 // Doubles per (column, ordinate) slot of the trace buffer.
 __host__ __device__ constexpr int trace_slot(int P) { return P; }
