@@ -616,7 +616,8 @@ def run_ours(args):
 
     def timed(prec, steps, warmup, sampler=False):
         if prec not in shapes:   # the library's autotuner: a tile shape per precision, outside the timing
-            shapes[prec] = (0, 0) if args.no_autotune else ctx.autotune(src.data_ptr(), P.dt, prec)
+            shapes[prec] = (tuple(args.tile) if args.tile else (0, 0) if args.no_autotune else
+                            ctx.autotune(src.data_ptr(), P.dt, prec))
         ctx.set_tile_shape(*shapes[prec])
         for _ in range(warmup):
             ctx.sweep_out(src.data_ptr(), out.data_ptr(), P.dt, phi.data_ptr(), prec, loc=abi.LOC_DEVICE)
@@ -651,10 +652,12 @@ def run_ours(args):
         return total_ms / steps, statistics.mean(kernel_ms), launches, (clocks.summary() if clocks else None)
 
     warm = max(3, args.warmup)
-    ms32, k32, _, _ = timed(abi.PREC_FP32_REFINED, args.steps, warm)
-    phi32 = phi.clone()
-    msf, kf, _, _ = timed(abi.PREC_FP32, args.steps, warm)   # unrefined FP32 arithmetic (about 1e-7)
-    phif = phi.clone()
+    ms32 = k32 = msf = kf = phi32 = phif = None
+    if not args.fp64_only:
+        ms32, k32, _, _ = timed(abi.PREC_FP32_REFINED, args.steps, warm)
+        phi32 = phi.clone()
+        msf, kf, _, _ = timed(abi.PREC_FP32, args.steps, warm)   # unrefined FP32 arithmetic (about 1e-7)
+        phif = phi.clone()
     ms64, k64, launches, clocks = timed(abi.PREC_FP64, args.steps, warm, sampler=(rank == 0))
     phi64 = phi.clone()
 
@@ -681,7 +684,7 @@ def run_ours(args):
     alg = algorithmic_bytes(P)
     peak, peak_kind = hbm_peak()
     traffic = measured_traffic(P.nx)
-    err_fp32_vs_fp64 = float(((phi32 - phi64).abs().max() / phi64.abs().max()).item())
+    err_fp32_vs_fp64 = None if phi32 is None else float(((phi32 - phi64).abs().max() / phi64.abs().max()).item())
 
     if rank != 0:
         ctx.close()
@@ -703,18 +706,21 @@ def run_ours(args):
         "dtype": "f64",
         "data": "synthetic",
         "config": bench_config(P, world),
-        "tile_shape": {"fp64": list(shapes[abi.PREC_FP64]), "fp32_refined": list(shapes[abi.PREC_FP32_REFINED]),
-                   "fp32": list(shapes[abi.PREC_FP32])},
+        "tile_shape": {name: list(shapes[p]) for name, p in (("fp64", abi.PREC_FP64),
+                                                             ("fp32_refined", abi.PREC_FP32_REFINED),
+                                                             ("fp32", abi.PREC_FP32)) if p in shapes},
         "roofline": {"bound": "hbm", "achieved": alg / (k64 * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                      "frac": alg / (k64 * 1e-3) / 1e9 / peak, "traffic": traffic,
                      "algorithmic_bytes": alg, "kernel_ms": k64, "peak_kind": peak_kind},
-        "fp32_refined": {"value": world * unknowns / (ms32 * 1e-3), "ms_per_step": ms32, "kernel_ms": k32,
-                         "roofline_frac": alg / (k32 * 1e-3) / 1e9 / peak},
-        "speedup_fp32_refined_vs_fp64": ms64 / ms32,
+        "fp32_refined": None if ms32 is None else {
+            "value": world * unknowns / (ms32 * 1e-3), "ms_per_step": ms32, "kernel_ms": k32,
+            "roofline_frac": alg / (k32 * 1e-3) / 1e9 / peak},
+        "speedup_fp32_refined_vs_fp64": None if ms32 is None else ms64 / ms32,
         "err_phi_fp32_refined_vs_fp64_gpu": err_fp32_vs_fp64,
-        "fp32": {"value": world * unknowns / (msf * 1e-3), "ms_per_step": msf, "kernel_ms": kf,
-                 "speedup_vs_fp64": ms64 / msf,
-                 "err_phi_vs_fp64_gpu": float(((phif - phi64).abs().max() / phi64.abs().max()).item())},
+        "fp32": None if msf is None else {
+            "value": world * unknowns / (msf * 1e-3), "ms_per_step": msf, "kernel_ms": kf,
+            "speedup_vs_fp64": ms64 / msf,
+            "err_phi_vs_fp64_gpu": float(((phif - phi64).abs().max() / phi64.abs().max()).item())},
         "e2e": None if args.no_e2e else {
             "value": world * unknowns / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(hs.nbytes),
             "d2h_bytes_per_step": int(P.nx * P.ny * P.nq * P.N * 8 + hp.nbytes), "ms_per_step": e2e_s * 1e3,
@@ -738,9 +744,8 @@ def run_ours(args):
                                               "sweep(s)"}
             scale = np.abs(phi_ref).max()
             line["err_phi_vs_oracle"] = {
-                "fp64": float(np.abs(phi64.cpu().numpy() - phi_ref).max() / scale),
-                "fp32_refined": float(np.abs(phi32.cpu().numpy() - phi_ref).max() / scale),
-                "fp32": float(np.abs(phif.cpu().numpy() - phi_ref).max() / scale)}
+                name: float(np.abs(f.cpu().numpy() - phi_ref).max() / scale)
+                for name, f in (("fp64", phi64), ("fp32_refined", phi32), ("fp32", phif)) if f is not None}
         except Exception as e:  # the reference library may be absent where it was never built
             line["cpu_baseline"] = None
             line["cpu_baseline_error"] = str(e)[:200]
@@ -783,6 +788,11 @@ def main():
     ap.add_argument("--nx", type=int, default=NX, help="grid side (default: the benchmark's 256; smaller for ncu)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="default tile shapes, no tuning launches (profiling runs)")
+    ap.add_argument("--tile", type=lambda v: [int(x) for x in v.split(",")], default=None, metavar="SEG,WARPS",
+                    help="one fixed tile shape for every precision, no tuning launches (profiling runs; "
+                         "WARPS 0 = the lane kernel)")
+    ap.add_argument("--fp64-only", action="store_true",
+                    help="time the FP64 sweep alone, without the FP32 legs (profiling runs)")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the other configurations (GMRES+DSA, IDC, adjoint, batched) measured beside the headline")
     ap.add_argument("--only-extra", choices=tuple(EXTRAS), default=None,
