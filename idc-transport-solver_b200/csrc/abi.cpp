@@ -635,6 +635,15 @@ int idc_set_spin_limit(idc_ctx *ctx, int64_t polls) {
     ABI_GUARD_END
 }
 
+int idc_set_allreduce(idc_ctx *ctx, idc_allreduce_fn fn, void *user) {
+    ABI_GUARD_BEGIN
+    if (!ctx) return fail(IDC_ERR_ARG, "null context");
+    ctx->impl.allreduce_fn = fn;
+    ctx->impl.allreduce_user = fn ? user : nullptr;
+    return IDC_OK;
+    ABI_GUARD_END
+}
+
 int idc_last_timing(idc_ctx *ctx, double *sweep_kernel_ms, int64_t *kernels_launched) {
     if (!ctx) return fail(IDC_ERR_ARG, "null context");
     if (sweep_kernel_ms) *sweep_kernel_ms = ctx->impl.last_sweep_ms;

@@ -630,6 +630,12 @@ Status Context::sweep(const double *src, double *out, double dt, double *phi, in
         IDC_TRY_CUDA(launch_reduce_phi_partials(dims(), d_phi_part, items_per_rb, phi_len(), phi, stream));
         launches += 1;
     }
+    if (phi && allreduce_fn) {   // this rank's ordinates gave partial moments: complete them over the ranks
+        if (capturing) return bad(IDC_ERR_STATE, "an all-reduce hook cannot run inside a stream capture");
+        IDC_TRY_CUDA(cudaStreamSynchronize(stream));
+        const int rc = allreduce_fn(phi, (int64_t)phi_len(), allreduce_user);
+        if (rc != 0) return bad(IDC_ERR_STATE, "the all-reduce hook failed (returned " + std::to_string(rc) + ")");
+    }
     return Status::ok();
 }
 

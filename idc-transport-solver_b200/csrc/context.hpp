@@ -163,6 +163,10 @@ public:
     int64_t launches = 0;
     static constexpr long long kDefaultSpinLimit = 1ll << 22;
     long long spin_limit = kDefaultSpinLimit;   // polls before a device-side wait gives up (idc_set_spin_limit)
+    // ordinate-partitioned solves: sums every moment output of a sweep over the ranks, in place (device memory);
+    // 0 on success (idc_set_allreduce)
+    int (*allreduce_fn)(double *data, int64_t n, void *user) = nullptr;
+    void *allreduce_user = nullptr;
 
     double *d_krylov = nullptr;    // GMRES basis, (restart + 1) phi-sized vectors (+ restart for flexible GMRES)
     int precond_kind = 0;          // 0 none, 1 DSA (right preconditioner of the forward Peierls GMRES)

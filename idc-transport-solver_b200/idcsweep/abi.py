@@ -48,7 +48,7 @@ EXPORTED_SYMBOLS = (
     "idc_write_af2", "idc_read_af2", "idc_sweep_fused", "idc_set_tile_shape", "idc_autotune", "idc_batch_create",
     "idc_batch_add", "idc_batch_sweep", "idc_batch_autotune", "idc_batch_last_timing", "idc_batch_destroy",
     "idc_batch_set_shape", "idc_batch_get_shape", "idc_sweep_out_many", "idc_adjoint_transient",
-    "idc_set_spin_limit", "idc_batch_gmres_solve",
+    "idc_set_spin_limit", "idc_batch_gmres_solve", "idc_set_allreduce",
 )
 
 
@@ -66,6 +66,10 @@ class ProblemDesc(C.Structure):
 
 _dp = C.POINTER(C.c_double)
 _lib = None
+
+
+# int (*)(double *data, int64_t n, void *user): the all-reduce hook of idc_set_allreduce
+ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int64, C.c_void_p)
 
 
 def load_library(path: str = LIB_PATH):
@@ -94,6 +98,7 @@ def load_library(path: str = LIB_PATH):
     lib.idc_last_timing.argtypes = [vp, _dp, C.POINTER(C.c_int64)]
     lib.idc_set_tiling.argtypes = [vp, C.c_int32, C.c_int32]
     lib.idc_set_spin_limit.argtypes = [vp, C.c_int64]
+    lib.idc_set_allreduce.argtypes = [vp, ALLREDUCE_FN, vp]
     lib.idc_sweep_out.argtypes = [vp, vp, vp, C.c_double, vp, C.c_int, C.c_int]
     lib.idc_sweep_out_many.argtypes = [vp, C.c_int64, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.c_double,
                                        C.c_int, C.c_int]
@@ -320,6 +325,23 @@ class SweepContext:
     def set_spin_limit(self, polls: int = 0):
         """Polls before a device-side wait gives up (0: the default)."""
         _check(self._lib.idc_set_spin_limit(self._h, int(polls)), "idc_set_spin_limit")
+
+    def set_allreduce(self, fn=None):
+        """fn(ptr, n) -> int sums the n doubles at device address ptr over the ranks in place (0 on success);
+        None turns the hook off.  The wrapper is kept alive with the context."""
+        if fn is None:
+            self._allreduce = None
+            _check(self._lib.idc_set_allreduce(self._h, ALLREDUCE_FN(), None), "idc_set_allreduce")
+            return
+
+        def tramp(ptr, n, user):
+            try:
+                return int(fn(int(ptr), int(n)))
+            except Exception:   # never let an exception cross the C boundary
+                return 1
+
+        self._allreduce = ALLREDUCE_FN(tramp)
+        _check(self._lib.idc_set_allreduce(self._h, self._allreduce, None), "idc_set_allreduce")
 
     def last_timing(self):
         ms = C.c_double()

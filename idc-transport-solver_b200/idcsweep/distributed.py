@@ -43,6 +43,28 @@ def local_quadrature(xi, eta, w, quad, idx):
     return xi_l, eta_l, w_l, q
 
 
+class _DeviceVector:
+    """A float64 vector of n entries at a raw device address, for torch.as_tensor without a copy."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, False), "version": 3,
+                                         "strides": None}
+
+
+def torch_allreduce_hook(device, group=None):
+    """The all-reduce hook of idc_set_allreduce over torch.distributed (NCCL): sums the moment array in place on
+    every rank and returns once the sums are there."""
+    dev = torch.device(device)
+
+    def fn(ptr: int, n: int) -> int:
+        t = torch.as_tensor(_DeviceVector(ptr, n), device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+        torch.cuda.current_stream(dev).synchronize()
+        return 0
+
+    return fn
+
+
 class GpuBackend:
     """Sweeps of this rank's ordinates on its GPU through libidcsweep (device tensors)."""
 
@@ -158,3 +180,25 @@ class DistributedTransport:
         phi = x.reshape(shape)
         _, psi = self.b.sweep(src, phi, dt, precision, want_psi=True)
         return phi, psi, its, resid
+
+    def gmres_device(self, src, dt, abs_tol=1e-10, restart=30, max_its=3000, precision=0, hook=None):
+        """The same solve by the library's GMRES on this rank's context (GpuBackend only): the partial moments
+        of every sweep are completed by an all-reduce hook (idc_set_allreduce), so the Arnoldi process, the
+        DSA preconditioner if the context has one, and the stopping test run on the device, identically on
+        every rank, with one host synchronisation per Krylov step.  `hook` defaults to torch.distributed's
+        all-reduce.  Returns (phi, local psi, iterations, residual)."""
+        ctx = self.b.ctx
+        ctx.set_allreduce(hook if hook is not None else torch_allreduce_hook(self.b.device, self.group))
+        try:
+            psi = src.clone()
+            its, res = ctx.gmres_solve(psi.data_ptr(), dt, abs_tol=abs_tol, restart=restart, max_its=max_its,
+                                       precision=precision, loc=1)
+        finally:
+            ctx.set_allreduce(None)
+        phi = self.b.zeros_phi()
+        ctx.pmv(1.0, 0.0, psi.data_ptr(), phi.data_ptr(), loc=1)
+        if hook is None:
+            self._reduce(phi)
+        else:
+            hook(phi.data_ptr(), phi.numel())
+        return phi, psi, its, res

@@ -335,6 +335,21 @@ const char *idc_last_error_message(void);
  * reference has no counterpart (its OpenMP barriers wait without bound). */
 int idc_set_spin_limit(idc_ctx *ctx, int64_t polls);
 
+/* Ordinate-partitioned solves over several processes (one rank per GPU; each rank's context holds its slice
+ * of every quadrant's ordinates, e.g. contiguous near-equal chunks): `fn` sums a moment-sized array of the
+ * context's GPU over the ranks, in place, and must give every rank bitwise the same sums (an NCCL or MPI
+ * all-reduce does).  Once set, every moment output of the context's sweeps is completed by one call of `fn`
+ * before it is used or returned, so idc_source_iteration, idc_gmres_solve (with DSA, and IDC_PREC_FP32_IR)
+ * and idc_sweep's phi run the whole quadrature's algorithm: the moment-sized vectors (Krylov basis, DSA
+ * state) are replicated and every rank computes the same Arnoldi steps and stopping decisions; psi stays
+ * the rank's own ordinates.  The context synchronises its stream before each call; `fn` returns 0 once
+ * the sums are in `data`, anything else fails the call with IDC_ERR_STATE.  fn = NULL turns it off.  Not
+ * inside CUDA graph captures (idc_idc_integrate with use_graph: IDC_ERR_STATE).  The reference spreads
+ * its solves over MPI ranks by space instead (KBA sweeps, linear_solvers/Abstract/SweepPattern/
+ * SweepPatternUniCartKBA.cpp, with MPI_Allreduce of the norms, objects/RKDG/DensityFunction.cpp:1154). */
+typedef int (*idc_allreduce_fn)(double *data, int64_t n, void *user);
+int idc_set_allreduce(idc_ctx *ctx, idc_allreduce_fn fn, void *user);
+
 /* Device time in milliseconds of the last sweep kernel launched by the context (CUDA events on the
  * launching stream), and the number of kernels the last idc_* call launched. */
 int idc_last_timing(idc_ctx *ctx, double *sweep_kernel_ms, int64_t *kernels_launched);
