@@ -193,6 +193,47 @@ __device__ __noinline__ long long wait_for_producer(const double *dep_trace, int
     }
 }
 
+// The backward transform of one cell, x = Vb Z Vb^T, and the forward transform of another, S = Wb v Wb^T
+// (modal_backward and modal_forward of modal_cell.cuh with no flips: the same operations in the same order,
+// so the results are bitwise theirs), emitted statement by statement side by side: the two independent FMA
+// chains are adjacent in the instruction stream, and each FMA of one can issue while the other's previous
+// result is still in the pipe.
+template <int P, typename T, bool ADJ>
+__device__ __forceinline__ void modal_backward_forward(T (&x)[P * P], const T (&Z)[P * P], T (&S)[P * P],
+                                                       const T (&v)[P * P]) {
+    T tb[P * P], tf[P * P];
+#pragma unroll
+    for (int i = 0; i < P; ++i)
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+            // backward: tb(d = i, b = k) = sum_a Vb(d,a) Z(a,b); forward: tf(a = i, e = k) = sum_d Wb(a,d) v(d,e)
+            T ab = Z[k] * T(basis_v<P, ADJ>(i, 0));
+            T af = v[k] * T(basis_w<P, ADJ>(i, 0));
+#pragma unroll
+            for (int m = 1; m < P; ++m) {
+                ab = fma(T(basis_v<P, ADJ>(i, m)), Z[k + P * m], ab);
+                af = fma(T(basis_w<P, ADJ>(i, m)), v[k + P * m], af);
+            }
+            tb[k + P * i] = ab;
+            tf[k + P * i] = af;
+        }
+#pragma unroll
+    for (int i = 0; i < P; ++i)
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+            // backward: x(d = i, e = k) = sum_b Vb(e,b) tb(d,b); forward: S(a = i, b = k) = sum_e Wb(b,e) tf(a,e)
+            T ab = tb[P * i] * T(basis_v<P, ADJ>(k, 0));
+            T af = tf[P * i] * T(basis_w<P, ADJ>(k, 0));
+#pragma unroll
+            for (int m = 1; m < P; ++m) {
+                ab = fma(T(basis_v<P, ADJ>(k, m)), tb[m + P * i], ab);
+                af = fma(T(basis_w<P, ADJ>(k, m)), tf[m + P * i], af);
+            }
+            x[k + P * i] = ab;
+            S[k + P * i] = af;
+        }
+}
+
 template <int P, int SEG, bool ADJ, bool SRC2, bool PHI, typename TC>
 __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &item, int it_index, double *wsm,
                                          int lane) {
@@ -325,7 +366,8 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
             }
         }
     };
-    // the modal source and the reciprocal denominators of the raw inputs
+    // the modal source and the reciprocal denominators of the raw inputs (the prologue's step; in the loop the
+    // forward transform runs beside the previous step's backward transform)
     auto transform = [&](const double (&src)[N], double st, TC (&S)[N], ModalRecip<P, TC> &r) {
         r = modal_recip<P, TC>(od, TC(st));
         if constexpr (PHI) {
@@ -438,11 +480,17 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
             if constexpr (PHI) {
 #pragma unroll
                 for (int k = 0; k < N; ++k) x[k] = Zp[k];
-            } else {
-                modal_backward<P, false, false, TC, ADJ>(x, Zp);
+#pragma unroll
+                for (int k = 0; k < N; ++k) S[k] = TC(srcn[k]);
+            } else {   // this step's backward transform beside step s + 1's forward transform
+                TC sv[N];
+#pragma unroll
+                for (int k = 0; k < N; ++k) sv[k] = flip_by(TC(srcn[k]), fmask(k));
+                modal_backward_forward<P, TC, ADJ>(x, Zp, S, sv);
 #pragma unroll
                 for (int k = 0; k < N; ++k) x[k] = flip_by(x[k], fmask(k));
             }
+            r = modal_recip<P, TC>(od, TC(stn));
             double *ob = obuf + (size_t)(s & (kOutBufs - 1)) * 32 * N;
             if constexpr (!PHI) bulk_wait_read<kOutBufs - 1>();   // the copy that read this buffer is done
             __syncwarp();   // and every lane's reads of the buffers in the previous iterations
@@ -492,8 +540,6 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
 #pragma unroll
         for (int k = 0; k < N; ++k) Zp[k] = Z[k];
 
-        // ---- the inputs of step s + 1 ----
-        transform(srcn, stn, S, r);
 
         // ---- step s + 2's raw inputs (copied D - 2 iterations ago), the copies of step s + D ----
         if (lane_out) store_psi_lanes(s - 1);
