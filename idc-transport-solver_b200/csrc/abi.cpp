@@ -58,6 +58,62 @@ bool valid_loc(int loc) { return loc == IDC_LOC_HOST || loc == IDC_LOC_DEVICE; }
 
 }  // namespace
 
+namespace {
+
+// The staging shared by the time-dependent adjoints: inputs to the device, the solve, gradients back.
+template <typename Run>
+int adjoint_time_abi(const char *name, idc_ctx *ctx, const double *psi0, const double *source, const double *detector,
+                     double abs_tol, int64_t max_its, double *dsigma_t, double *dsigma_s, double *dsource,
+                     double *dpsi0, double *J, int loc, int64_t *solves, Run run) {
+    ABI_GUARD_BEGIN
+    if (!ctx || !psi0 || !source || !detector) return fail(IDC_ERR_ARG, (std::string(name) + ": null argument").c_str());
+    if (!valid_loc(loc)) return fail(IDC_ERR_ARG, "bad loc");
+    if (max_its < 0 || !(abs_tol >= 0)) return fail(IDC_ERR_ARG, (std::string(name) + ": bad tolerance").c_str());
+    idc::Context &c = ctx->impl;
+    if (!c.have_ordinates || !c.have_sigma) return fail(IDC_ERR_STATE, (std::string(name) + " before ordinates and sigma").c_str());
+    ABI_TRY_CUDA(cudaSetDevice(c.device));
+    c.launches = 0;
+    ABI_TRY(c.ensure_psi_buffers(3));
+    ABI_TRY(c.ensure_phi_buffers(15));
+    const double *d_psi0 = psi0, *d_src = source;
+    double *d_det = c.phi_buf(11);
+    double *d_gt = dsigma_t, *d_gs = dsigma_s, *d_gq = dsource, *d_p0 = dpsi0;
+    const cudaMemcpyKind in = loc == IDC_LOC_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    if (loc == IDC_LOC_HOST) {
+        ABI_TRY_CUDA(cudaMemcpyAsync(c.psi_buf(0), psi0, sizeof(double) * c.psi_len(), in, c.stream));
+        ABI_TRY_CUDA(cudaMemcpyAsync(c.psi_buf(1), source, sizeof(double) * c.psi_len(), in, c.stream));
+        d_psi0 = c.psi_buf(0);
+        d_src = c.psi_buf(1);
+        d_gt = dsigma_t ? c.phi_buf(12) : nullptr;   // sigma-sized results fit a moment-sized buffer
+        d_gs = dsigma_s ? c.phi_buf(13) : nullptr;
+        d_gq = dsource ? c.phi_buf(14) : nullptr;
+        d_p0 = dpsi0 ? c.psi_buf(2) : nullptr;
+    }
+    ABI_TRY_CUDA(cudaMemcpyAsync(d_det, detector, sizeof(double) * c.phi_len(), in, c.stream));
+    ABI_TRY_CUDA(idc::launch_zero_ghost_phi(c.dims(), d_det, c.stream));
+    double jv = 0.0;
+    int64_t ns = 0;
+    idc::Status st = run(c, d_psi0, d_src, d_det, d_gt, d_gs, d_gq, d_p0, &jv, &ns);
+    if (solves) *solves = ns;
+    if (!st.good()) return fail(st);
+    if (J) *J = jv;
+    if (loc == IDC_LOC_HOST) {
+        if (dsigma_t)
+            ABI_TRY_CUDA(cudaMemcpyAsync(dsigma_t, d_gt, sizeof(double) * c.sig_len(), cudaMemcpyDeviceToHost, c.stream));
+        if (dsigma_s)
+            ABI_TRY_CUDA(cudaMemcpyAsync(dsigma_s, d_gs, sizeof(double) * c.sig_len(), cudaMemcpyDeviceToHost, c.stream));
+        if (dsource)
+            ABI_TRY_CUDA(cudaMemcpyAsync(dsource, d_gq, sizeof(double) * c.phi_len(), cudaMemcpyDeviceToHost, c.stream));
+        if (dpsi0)
+            ABI_TRY_CUDA(cudaMemcpyAsync(dpsi0, d_p0, sizeof(double) * c.psi_len(), cudaMemcpyDeviceToHost, c.stream));
+    }
+    ABI_TRY_CUDA(cudaStreamSynchronize(c.stream));
+    return IDC_OK;
+    ABI_GUARD_END
+}
+
+}  // namespace
+
 extern "C" {
 
 const char *idc_strerror(int status) {
@@ -574,54 +630,42 @@ int idc_adjoint_grad(idc_ctx *ctx, const double *psi, const double *detector, do
     ABI_GUARD_END
 }
 
+
 int idc_adjoint_transient(idc_ctx *ctx, const double *psi0, const double *source, double dt, int64_t steps,
                           const double *detector, int64_t checkpoint_every, double abs_tol, int32_t restart,
                           int64_t max_its, int precision, double *dsigma_t, double *dsigma_s, double *dsource,
                           double *dpsi0, double *J, int loc, int64_t *solves) {
+    return adjoint_time_abi(
+        "idc_adjoint_transient", ctx, psi0, source, detector, abs_tol, max_its, dsigma_t, dsigma_s, dsource, dpsi0, J,
+        loc, solves,
+        [&](idc::Context &c, const double *p0, const double *q, const double *det, double *gt, double *gs, double *gq,
+            double *gp, double *jv, int64_t *ns) {
+            return c.adjoint_transient(p0, q, dt, steps, det, checkpoint_every, abs_tol, restart, max_its, precision,
+                                       gt, gs, gq, gp, jv, ns);
+        });
+}
+
+int idc_adjoint_idc(idc_ctx *ctx, const double *psi0, const double *source, double dt, int64_t steps,
+                    int32_t num_nodes, int32_t num_corrections, const double *detector, int64_t checkpoint_every,
+                    double abs_tol, int32_t restart, int64_t max_its, int precision, double *dsigma_t,
+                    double *dsigma_s, double *dsource, double *dpsi0, double *J, int loc, int64_t *solves) {
+    return adjoint_time_abi(
+        "idc_adjoint_idc", ctx, psi0, source, detector, abs_tol, max_its, dsigma_t, dsigma_s, dsource, dpsi0, J, loc,
+        solves,
+        [&](idc::Context &c, const double *p0, const double *q, const double *det, double *gt, double *gs, double *gq,
+            double *gp, double *jv, int64_t *ns) {
+            return c.adjoint_idc(p0, q, dt, steps, num_nodes, num_corrections, det, checkpoint_every, abs_tol, restart,
+                                 max_its, precision, gt, gs, gq, gp, jv, ns);
+        });
+}
+
+int idc_lmv_transpose(idc_ctx *ctx, double alpha, double beta, const double *x, double *y, int loc) {
     ABI_GUARD_BEGIN
-    if (!ctx || !psi0 || !source || !detector) return fail(IDC_ERR_ARG, "idc_adjoint_transient: null argument");
-    if (!valid_loc(loc)) return fail(IDC_ERR_ARG, "bad loc");
-    if (max_its < 0 || !(abs_tol >= 0)) return fail(IDC_ERR_ARG, "idc_adjoint_transient: bad tolerance");
+    if (!ctx || !x || !y) return fail(IDC_ERR_ARG, "idc_lmv_transpose: null argument");
+    if (loc != IDC_LOC_DEVICE) return fail(IDC_ERR_ARG, "idc_lmv_transpose: device arrays only");
     idc::Context &c = ctx->impl;
-    if (!c.have_ordinates || !c.have_sigma)
-        return fail(IDC_ERR_STATE, "idc_adjoint_transient before ordinates and sigma");
-    ABI_TRY_CUDA(cudaSetDevice(c.device));
-    c.launches = 0;
-    ABI_TRY(c.ensure_psi_buffers(3));
-    ABI_TRY(c.ensure_phi_buffers(15));
-    const double *d_psi0 = psi0, *d_src = source;
-    double *d_det = c.phi_buf(11);
-    double *d_gt = dsigma_t, *d_gs = dsigma_s, *d_gq = dsource, *d_p0 = dpsi0;
-    const cudaMemcpyKind in = loc == IDC_LOC_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
-    if (loc == IDC_LOC_HOST) {
-        ABI_TRY_CUDA(cudaMemcpyAsync(c.psi_buf(0), psi0, sizeof(double) * c.psi_len(), in, c.stream));
-        ABI_TRY_CUDA(cudaMemcpyAsync(c.psi_buf(1), source, sizeof(double) * c.psi_len(), in, c.stream));
-        d_psi0 = c.psi_buf(0);
-        d_src = c.psi_buf(1);
-        d_gt = dsigma_t ? c.phi_buf(12) : nullptr;   // sigma-sized results fit a moment-sized buffer
-        d_gs = dsigma_s ? c.phi_buf(13) : nullptr;
-        d_gq = dsource ? c.phi_buf(14) : nullptr;
-        d_p0 = dpsi0 ? c.psi_buf(2) : nullptr;
-    }
-    ABI_TRY_CUDA(cudaMemcpyAsync(d_det, detector, sizeof(double) * c.phi_len(), in, c.stream));
-    ABI_TRY_CUDA(idc::launch_zero_ghost_phi(c.dims(), d_det, c.stream));
-    double jv = 0.0;
-    int64_t ns = 0;
-    idc::Status st = c.adjoint_transient(d_psi0, d_src, dt, steps, d_det, checkpoint_every, abs_tol, restart, max_its,
-                                         precision, d_gt, d_gs, d_gq, d_p0, &jv, &ns);
-    if (solves) *solves = ns;
-    if (!st.good()) return fail(st);
-    if (J) *J = jv;
-    if (loc == IDC_LOC_HOST) {
-        if (dsigma_t)
-            ABI_TRY_CUDA(cudaMemcpyAsync(dsigma_t, d_gt, sizeof(double) * c.sig_len(), cudaMemcpyDeviceToHost, c.stream));
-        if (dsigma_s)
-            ABI_TRY_CUDA(cudaMemcpyAsync(dsigma_s, d_gs, sizeof(double) * c.sig_len(), cudaMemcpyDeviceToHost, c.stream));
-        if (dsource)
-            ABI_TRY_CUDA(cudaMemcpyAsync(dsource, d_gq, sizeof(double) * c.phi_len(), cudaMemcpyDeviceToHost, c.stream));
-        if (dpsi0)
-            ABI_TRY_CUDA(cudaMemcpyAsync(dpsi0, d_p0, sizeof(double) * c.psi_len(), cudaMemcpyDeviceToHost, c.stream));
-    }
+    if (!c.have_ordinates || !c.have_sigma) return fail(IDC_ERR_STATE, "idc_lmv_transpose before ordinates and sigma");
+    ABI_TRY(c.lmv_transpose(alpha, beta, x, y));
     ABI_TRY_CUDA(cudaStreamSynchronize(c.stream));
     return IDC_OK;
     ABI_GUARD_END

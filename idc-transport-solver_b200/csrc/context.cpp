@@ -44,6 +44,8 @@ Context::~Context() {
     for (double *p : idc_psi_) cudaFree(p);
     for (double *p : idc_phi_) cudaFree(p);
     for (double *p : transient_bufs_) cudaFree(p);
+    for (double *p : adj_idc_bufs_) cudaFree(p);
+    cudaFree(d_ones_);
     cudaFree(d_scalar_);
     cudaFree(d_xi);
     cudaFree(d_eta);
@@ -127,9 +129,13 @@ Status Context::set_ordinates(int64_t nq_in, const double *xi, const double *eta
     IDC_TRY_CUDA(cudaMemcpy(d_eta, eta, sizeof(double) * nq_in, cudaMemcpyHostToDevice));
     IDC_TRY_CUDA(cudaMemcpy(d_w, w, sizeof(double) * nq_in, cudaMemcpyHostToDevice));
     if (nq_in != nq) {
-        // psi-sized buffers depend on nq
-        for (double *p : psi_bufs_) cudaFree(p);
-        psi_bufs_.clear();
+        // psi-sized buffers (and the unweighted-sum weights) depend on nq
+        for (auto *v : {&psi_bufs_, &idc_psi_, &transient_bufs_, &adj_idc_bufs_}) {
+            for (double *p : *v) cudaFree(p);
+            v->clear();
+        }
+        cudaFree(d_ones_);
+        d_ones_ = nullptr;
     }
     nq = nq_in;
     for (int k = 0; k < 5; ++k) quad[k] = qb[k];
@@ -669,6 +675,26 @@ Status Context::lmv(double alpha, double beta, const double *x, double *y) {
 Status Context::transport_residual(const double *psi, const double *phi, double *res) {
     IDC_TRY_CUDA(launch_lmv(dims(), 1.0, 0.0, d_sigma_t, d_xi, d_eta, psi, res, stream, -1.0, d_sigma_s, phi));
     launches += 1;
+    return Status::ok();
+}
+
+Status Context::lmv_transpose(double alpha, double beta, const double *x, double *y) {
+    IDC_TRY_CUDA(cudaSetDevice(device));
+    IDC_TRY_CUDA(launch_lmv_transpose(dims(), alpha, beta, d_sigma_t, d_xi, d_eta, d_w, x, y, stream));
+    launches += 1;
+    return Status::ok();
+}
+
+Status Context::transport_residual_transpose(const double *z, double *y, double *zsum) {
+    if (!d_ones_) {
+        std::vector<double> ones((size_t)nq, 1.0);
+        IDC_TRY_CUDA(cudaMalloc(&d_ones_, sizeof(double) * nq));
+        IDC_TRY_CUDA(cudaMemcpy(d_ones_, ones.data(), sizeof(double) * nq, cudaMemcpyHostToDevice));
+    }
+    IDC_TRY_CUDA(launch_pmv(dims(), 1.0, 0.0, d_ones_, z, zsum, stream));   // sum_q z_q
+    IDC_TRY_CUDA(launch_lmv_transpose(dims(), 1.0, 0.0, d_sigma_t, d_xi, d_eta, d_w, z, y, stream, -1.0, d_sigma_s,
+                                      zsum));
+    launches += 2;
     return Status::ok();
 }
 

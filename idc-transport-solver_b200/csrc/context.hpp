@@ -92,6 +92,15 @@ public:
     Status adjoint_transient(const double *psi0, const double *Q, double dt, int64_t steps, const double *detector,
                              int64_t checkpoint_every, double abs_tol, int restart, int64_t max_its, int precision,
                              double *dsig_t, double *dsig_s, double *dq, double *dpsi0, double *J, int64_t *solves);
+    // gradients of J = c . P psi^steps for implicit-scattering IDC steps (idc_integrate with scattering 1: M
+    // Gauss-Lobatto nodes, K corrections, update form), the same checkpointing
+    Status adjoint_idc(const double *psi0, const double *Q, double dt, int64_t steps, int M, int K,
+                       const double *detector, int64_t checkpoint_every, double abs_tol, int restart, int64_t max_its,
+                       int precision, double *dsig_t, double *dsig_s, double *dq, double *dpsi0, double *J,
+                       int64_t *solves);
+    // y = (L - S P)^T z on interior cells (the transpose of transport_residual); zsum: a moment-sized scratch
+    Status transport_residual_transpose(const double *z, double *y, double *zsum);
+    Status lmv_transpose(double alpha, double beta, const double *x, double *y);   // y = beta y + alpha L^T x
     Status dot_host(const double *x, const double *y, size_t n, double *out);
 
     // ---- buffers ----
@@ -184,6 +193,8 @@ private:
     Status build_schedule(int precision);
     std::vector<double *> psi_bufs_, phi_bufs_;
     std::vector<double *> transient_bufs_;   // adjoint_transient: checkpoints, segment states, lam, b, source
+    std::vector<double *> adj_idc_bufs_;    // adjoint_idc: checkpoints, step inputs, stages, adjoint states
+    double *d_ones_ = nullptr;              // nq ones: unweighted moment sums through the Pmv kernel
     std::vector<double *> idc_psi_, idc_phi_;
     double *d_scalar_ = nullptr;
 };

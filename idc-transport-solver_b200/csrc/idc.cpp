@@ -322,3 +322,190 @@ Status Context::idc_integrate(double *psi, const double *Q, double dt, int64_t s
 }
 
 }  // namespace idc
+
+namespace idc {
+
+// Discrete adjoint of implicit-scattering IDC time stepping (idc_integrate with scattering = 1, the reference's
+// IDCIntegrator::Step_Nonhybrid in update form, time_integrators/RKDG/idc.cpp:846-955, 1657-1740).  One step
+// from psi_in, with A_n = 1/(h_n dt) + T, T = L - S P (transport_residual) and c_nl = delta_nl - W(n,l)/h_n:
+//     level 0:  A_n u^0_n = u^0_{n-1} / (h_n dt) + Q                                (n = 1..M-1, u^p_0 = psi_in)
+//     level p:  A_n u^p_n = u^p_{n-1} / (h_n dt) + sum_l c_nl T u^{p-1}_l + Q       (p = 1..K)
+//     psi_out = u^K_{M-1}.
+// Backwards through a step, ubar being the adjoint of the stages and rbar that of the residuals T u^{p-1}_l:
+//     for p = K..0, n = M-1..1:  A_n^T lam = ubar_n (adjoint_solve_psi);  ubar_{n-1} += lam / (h_n dt);
+//                                 rbar_l += c_nl lam;  the solve's gradient terms (-lam^T dA u, lam^T dQ);
+//     then ubar^{p-1}_l = T^T rbar_l (lmvt_kernel; l = 0 feeds psi_in's adjoint) and the residuals' gradient
+//     terms +rbar^T dT u^{p-1}_l (the solve's form with the opposite sign and no source term).
+// psi_in's adjoint (every level's first substep and its l = 0 residual) becomes the previous step's psi_out
+// adjoint; J = c . P psi^N starts the last step with P^T c.  Checkpointing as in adjoint_transient: psi at
+// every CK-th step boundary; the backward pass recomputes a segment's step inputs, then each step's stages
+// (bitwise those of the forward pass: every solve is reproducible).  Inflow (Q's ghost cells) is data.
+Status Context::adjoint_idc(const double *psi0, const double *Q, double dt, int64_t steps, int M, int K,
+                            const double *detector, int64_t checkpoint_every, double abs_tol, int restart,
+                            int64_t max_its, int precision, double *dsig_t, double *dsig_s, double *dq, double *dpsi0,
+                            double *J, int64_t *solves) {
+    if (!have_ordinates || !have_sigma) return bad(IDC_ERR_STATE, "IDC adjoint before ordinates and sigma");
+    if (!modal_family()) return bad(IDC_ERR_UNSUPPORTED, "the adjoint needs the modal sweep kernel");
+    if (steps < 1) return bad(IDC_ERR_ARG, "IDC adjoint needs at least one step");
+    if (!(dt > 0) || !std::isfinite(dt)) return bad(IDC_ERR_ARG, "IDC adjoint needs a finite positive dt");
+    if (M < 2 || M > 8) return bad(IDC_ERR_ARG, "IDC nodes must be in 2..8");
+    if (K < 0 || K > 16) return bad(IDC_ERR_ARG, "IDC corrections must be in 0..16");
+    std::vector<double> t, W;
+    idc_nodes_and_weights(M, t, W);
+    const int64_t CK = checkpoint_every > 0 ? std::min(checkpoint_every, steps)
+                                            : std::max<int64_t>(1, (int64_t)std::ceil(std::sqrt((double)steps)));
+    const int64_t NS = (steps + CK - 1) / CK;
+    const size_t np = psi_len(), nm = phi_len();
+    const int64_t n_stage = (int64_t)(K + 1) * M;
+    const int64_t need = NS + CK + n_stage + 3 * (int64_t)M + 6;
+    IDC_TRY_CUDA(cudaSetDevice(device));
+    while ((int64_t)adj_idc_bufs_.size() < need) {   // zeroed once: the kernels below write interior cells only
+        double *p = nullptr;
+        IDC_TRY_CUDA(cudaMalloc(&p, sizeof(double) * np));
+        IDC_TRY_CUDA(cudaMemsetAsync(p, 0, sizeof(double) * np, stream));
+        adj_idc_bufs_.push_back(p);
+    }
+    auto ckpt = [&](int64_t m) { return adj_idc_bufs_[(size_t)m]; };
+    auto inp = [&](int64_t k) { return adj_idc_bufs_[(size_t)(NS + k)]; };   // k = 0..CK-1
+    auto stage = [&](int p, int n) { return adj_idc_bufs_[(size_t)(NS + CK + (int64_t)p * M + n)]; };
+    const size_t b0 = (size_t)(NS + CK + n_stage);
+    auto res = [&](int l) { return adj_idc_bufs_[b0 + l]; };
+    auto ubar = [&](int l) { return adj_idc_bufs_[b0 + M + l]; };
+    auto rbar = [&](int l) { return adj_idc_bufs_[b0 + 2 * M + l]; };
+    double *lam = adj_idc_bufs_[b0 + 3 * M], *tmp = adj_idc_bufs_[b0 + 3 * M + 1];
+    double *src = adj_idc_bufs_[b0 + 3 * M + 2], *pbar = adj_idc_bufs_[b0 + 3 * M + 3];
+    double *inbar = adj_idc_bufs_[b0 + 3 * M + 4], *zsum = adj_idc_bufs_[b0 + 3 * M + 5];   // zsum: moment-sized use
+    IDC_TRY(ensure_phi_buffers(11));
+    double *Lam = phi_buf(9), *phi = phi_buf(10);
+    int64_t nsolve = 0;
+    // stage ghost cells hold the inflow (Q's ghost cells), as in idc_integrate; the solves write interiors only
+    for (int p = 0; p <= K; ++p)
+        for (int n = 1; n < M; ++n)
+            IDC_TRY_CUDA(cudaMemcpyAsync(stage(p, n), Q, sizeof(double) * np, cudaMemcpyDeviceToDevice, stream));
+
+    auto solve = [&](int p, int n) -> Status {   // A_n u^p_n = u^p_{n-1}/(h dt) [+ sum_l c_nl res_l] + Q
+        const double h = t[n] - t[n - 1];
+        IdcTerms tm{};
+        tm.n = 0;
+        tm.a[tm.n] = stage(p, n - 1);
+        tm.c[tm.n++] = 1.0 / (h * dt);
+        if (p > 0)
+            for (int l = 0; l < M; ++l) {
+                tm.a[tm.n] = res(l);
+                tm.c[tm.n++] = (n == l ? 1.0 : 0.0) - W[(size_t)n * M + l] / h;
+            }
+        IDC_TRY_CUDA(launch_idc_source(dims(), tm, Q, src, stream));
+        launches += 1;
+        int64_t its = 0;
+        double r = 0.0;
+        IDC_TRY(gmres_peierls(src, stage(p, n), h * dt, abs_tol, restart, max_its, precision, &its, &r));
+        ++nsolve;
+        return Status::ok();
+    };
+    // one forward step from `in`, every level's stages kept; the result is stage(K, M - 1)
+    auto step_store = [&](const double *in) -> Status {
+        for (int p = 0; p <= K; ++p)
+            IDC_TRY_CUDA(cudaMemcpyAsync(stage(p, 0), in, sizeof(double) * np, cudaMemcpyDeviceToDevice, stream));
+        for (int n = 1; n < M; ++n) IDC_TRY(solve(0, n));
+        for (int p = 1; p <= K; ++p) {
+            for (int l = 0; l < M; ++l) {   // res_l = (L - S P) u^{p-1}_l
+                IDC_TRY(pmv(1.0, 0.0, stage(p - 1, l), phi));
+                IDC_TRY(transport_residual(stage(p - 1, l), phi, res(l)));
+            }
+            for (int n = 1; n < M; ++n) IDC_TRY(solve(p, n));
+        }
+        return Status::ok();
+    };
+    auto axpy = [&](double a, const double *x, double *y) -> Status {
+        IDC_TRY_CUDA(launch_axpby(a, x, 1.0, y, np, stream));
+        launches += 1;
+        return Status::ok();
+    };
+
+    // forward pass: checkpoints at the segment boundaries, J from psi^N
+    IDC_TRY_CUDA(cudaMemcpyAsync(ckpt(0), psi0, sizeof(double) * np, cudaMemcpyDeviceToDevice, stream));
+    const double *cur = ckpt(0);
+    for (int64_t s = 1; s <= steps; ++s) {
+        IDC_TRY(step_store(cur));
+        cur = stage(K, M - 1);
+        if (s % CK == 0 && s / CK < NS) {
+            IDC_TRY_CUDA(cudaMemcpyAsync(ckpt(s / CK), cur, sizeof(double) * np, cudaMemcpyDeviceToDevice, stream));
+            cur = ckpt(s / CK);
+        }
+    }
+    IDC_TRY(pmv(1.0, 0.0, cur, phi));
+    if (J) IDC_TRY(dot_host(phi, detector, nm, J));
+
+    if (dsig_t) IDC_TRY_CUDA(cudaMemsetAsync(dsig_t, 0, sizeof(double) * sig_len(), stream));
+    if (dsig_s) IDC_TRY_CUDA(cudaMemsetAsync(dsig_s, 0, sizeof(double) * sig_len(), stream));
+    if (dq) IDC_TRY_CUDA(cudaMemsetAsync(dq, 0, sizeof(double) * nm, stream));
+    IDC_TRY_CUDA(launch_weighted_broadcast(dims(), d_w, detector, pbar, stream));   // P^T c
+    launches += 1;
+
+    // the adjoint of one step: pbar (psi_out's adjoint) -> pbar (psi_in's adjoint), stages of the step in place
+    auto adjoint_step = [&]() -> Status {
+        for (int l = 0; l < M; ++l) IDC_TRY_CUDA(cudaMemsetAsync(ubar(l), 0, sizeof(double) * np, stream));
+        IDC_TRY_CUDA(cudaMemcpyAsync(ubar(M - 1), pbar, sizeof(double) * np, cudaMemcpyDeviceToDevice, stream));
+        IDC_TRY_CUDA(cudaMemsetAsync(inbar, 0, sizeof(double) * np, stream));
+        for (int p = K; p >= 0; --p) {
+            if (p > 0)
+                for (int l = 0; l < M; ++l) IDC_TRY_CUDA(cudaMemsetAsync(rbar(l), 0, sizeof(double) * np, stream));
+            for (int n = M - 1; n >= 1; --n) {
+                const double h = t[n] - t[n - 1];
+                int64_t its = 0;
+                IDC_TRY(adjoint_solve_psi(ubar(n), lam, Lam, h * dt, abs_tol, restart, max_its, precision, &its));
+                ++nsolve;
+                IDC_TRY(pmv(1.0, 0.0, stage(p, n), phi));
+                IDC_TRY_CUDA(launch_adjoint_gradient(dims(), stage(p, n), lam, phi, Lam, dsig_t, dsig_s, dq, stream,
+                                                     true, 1.0));
+                launches += 1;
+                IDC_TRY(axpy(1.0 / (h * dt), lam, n == 1 ? inbar : ubar(n - 1)));
+                if (p > 0)
+                    for (int l = 0; l < M; ++l) {
+                        const double c = (n == l ? 1.0 : 0.0) - W[(size_t)n * M + l] / h;
+                        if (c != 0.0) IDC_TRY(axpy(c, lam, rbar(l)));
+                    }
+            }
+            if (p > 0)
+                for (int l = 0; l < M; ++l) {   // res_l = T u^{p-1}_l: the adjoint of level p-1's stage l
+                    double *y = l == 0 ? tmp : ubar(l);
+                    IDC_TRY(transport_residual_transpose(rbar(l), y, zsum));
+                    if (l == 0) IDC_TRY(axpy(1.0, tmp, inbar));
+                    IDC_TRY(pmv(1.0, 0.0, stage(p - 1, l), phi));
+                    IDC_TRY_CUDA(launch_adjoint_gradient(dims(), stage(p - 1, l), rbar(l), phi, zsum, dsig_t, dsig_s,
+                                                         nullptr, stream, true, -1.0));
+                    launches += 1;
+                }
+        }
+        IDC_TRY_CUDA(cudaMemcpyAsync(pbar, inbar, sizeof(double) * np, cudaMemcpyDeviceToDevice, stream));
+        return Status::ok();
+    };
+
+    // backward pass, one segment (m CK, min((m+1) CK, steps)] at a time
+    for (int64_t m = NS - 1; m >= 0; --m) {
+        const int64_t n0 = m * CK, n1 = std::min(steps, n0 + CK);
+        IDC_TRY_CUDA(cudaMemcpyAsync(inp(0), ckpt(m), sizeof(double) * np, cudaMemcpyDeviceToDevice, stream));
+        for (int64_t k = 1; k < n1 - n0; ++k) {   // the segment's step inputs
+            IDC_TRY(step_store(inp(k - 1)));
+            IDC_TRY_CUDA(cudaMemcpyAsync(inp(k), stage(K, M - 1), sizeof(double) * np, cudaMemcpyDeviceToDevice,
+                                         stream));
+        }
+        for (int64_t s = n1; s > n0; --s) {
+            IDC_TRY(step_store(inp(s - n0 - 1)));
+            IDC_TRY(adjoint_step());
+        }
+    }
+    if (dpsi0) {   // interior cells; zero ghost cells
+        IdcTerms tm{};
+        tm.n = 1;
+        tm.a[0] = pbar;
+        tm.c[0] = 1.0;
+        IDC_TRY_CUDA(launch_idc_source(dims(), tm, nullptr, dpsi0, stream));
+        launches += 1;
+    }
+    IDC_TRY(check_device_error());
+    if (solves) *solves = nsolve;
+    return Status::ok();
+}
+
+}  // namespace idc

@@ -163,6 +163,14 @@ cudaError_t launch_smv(const GridDims &g, double alpha, double beta, const doubl
 cudaError_t launch_lmv(const GridDims &g, double alpha, double beta, const double *sigma_t, const double *xi,
                        const double *eta, const double *x, double *y, cudaStream_t s, double gamma = 0.0,
                        const double *sigma_s = nullptr, const double *phi_sc = nullptr);
+// y = beta y + alpha L^T x on interior cells (+ gamma w_q sigma_s zsum / (4 pi) when zsum = sum_q x_q is given:
+// gamma = -1 gives (L - S P)^T x); ghost cells of x are not read as unknowns, ghost cells of y not written
+cudaError_t launch_lmv_transpose(const GridDims &g, double alpha, double beta, const double *sigma_t, const double *xi,
+                                 const double *eta, const double *w, const double *x, double *y, cudaStream_t s,
+                                 double gamma = 0.0, const double *sigma_s = nullptr, const double *zsum = nullptr);
+// out = w_q m on interior cells (P^T of a moment array as an angular array); ghost cells of out not written
+cudaError_t launch_weighted_broadcast(const GridDims &g, const double *w, const double *m, double *out,
+                                     cudaStream_t s);
 cudaError_t launch_zero_ghost_phi(const GridDims &g, double *phi, cudaStream_t s);
 // out = sigma_s phi / (4 pi) per interior cell and moment (the isotropic scattering source of Smv, formed once
 // per cell for the modal sweep's fused source; ghost cells of out are not written)
@@ -184,9 +192,11 @@ cudaError_t launch_adjoint_scatter(const GridDims &g, const double *sigma_s, con
                                    double *y, cudaStream_t s);
 // per-cell gradients of J = c . phi from the forward psi, phi and the adjoint lam, Lam = sum_q lam_q
 // (outputs on the halo layouts, interior cells written, any of them nullable)
+// (scale multiplies every contribution: -1 for the gradient terms of an explicitly applied operator, e.g.
+// the IDC residuals, whose sensitivity enters with the opposite sign of a solve's)
 cudaError_t launch_adjoint_gradient(const GridDims &g, const double *psi, const double *lam, const double *phi,
                                     const double *Lam, double *dsig_t, double *dsig_s, double *dq, cudaStream_t s,
-                                    bool accumulate = false);
+                                    bool accumulate = false, double scale = 1.0);
 // IDC (ops_kernels.cu): out = sum_k c_k A_k + Q on interior cells, Q on ghost cells (Q nullable = 0)
 struct IdcTerms {
     static constexpr int kMax = 10;

@@ -118,6 +118,116 @@ __device__ __forceinline__ void lmv_point(const GridDims &g, const double *__res
             for (int b = e - 1; b >= 0; b -= 2) x3[e + P * d] -= double(2 * (2 * e + 1)) * cv * x0[b + P * d];
 }
 
+// (Omega.grad + sigma_t)^T x at one interior (cell, ordinate): the transpose of lmv_point's stencil.  Cell c's
+// row of L couples c with its upwind neighbours, so c's row of L^T gathers c's own value through the transposed
+// cell matrix and the values of the cells downwind of c (whose upwind neighbour c is) through the transposed
+// face matrices; a downwind neighbour outside the interior contributes nothing (`dn_x`, `dn_y` false): the
+// ghost cells hold boundary data, not unknowns.
+template <int P>
+__device__ __forceinline__ void lmvt_point(const GridDims &g, const double *__restrict__ x, size_t base, size_t istride,
+                                           size_t plane, double xi, double eta, double s, bool dn_x, bool dn_y,
+                                           double (&y)[P * P]) {
+    constexpr int N = P * P;
+    const bool xneg = xi <= 0.0, yneg = eta <= 0.0;
+    const double *X0 = x + base;
+    const double *XD = x + base + (xneg ? -(ptrdiff_t)istride : (ptrdiff_t)istride);   // downwind in x
+    const double *YD = x + base + (yneg ? -(ptrdiff_t)plane : (ptrdiff_t)plane);       // downwind in y
+    double x0[N], xd[N], yd[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        x0[k] = X0[k];
+        xd[k] = dn_x ? XD[k] : 0.0;
+        yd[k] = dn_y ? YD[k] : 0.0;
+    }
+#pragma unroll
+    for (int k = 0; k < N; ++k) y[k] = s * x0[k];
+    double cv = xi / g.dx;
+    // lmv_point: row (d,e) += cv (2d+1) [own(d,a) x0(a,e) + up(d,a) x_up(a,e)], and -2(2d+1) cv x0(a,e) for
+    // a = d-1, d-3, ...; the transpose moves each coefficient to row (a,e), column (d,e)
+#pragma unroll
+    for (int d = 0; d < P; ++d)
+#pragma unroll
+        for (int a = 0; a < P; ++a) {
+            const double own = cv * double(2 * d + 1) * (xneg ? neg1pow(d + a + 1) : 1.0);
+            const double up = cv * double(2 * d + 1) * (xneg ? neg1pow(a) : neg1pow(d + 1));
+#pragma unroll
+            for (int e = 0; e < P; ++e) y[e + P * a] += own * x0[e + P * d] + up * xd[e + P * d];
+        }
+#pragma unroll
+    for (int d = 0; d < P; ++d)
+#pragma unroll
+        for (int a = d - 1; a >= 0; a -= 2)
+#pragma unroll
+            for (int e = 0; e < P; ++e) y[e + P * a] -= double(2 * (2 * d + 1)) * cv * x0[e + P * d];
+    cv = eta / g.dy;
+#pragma unroll
+    for (int e = 0; e < P; ++e)
+#pragma unroll
+        for (int b = 0; b < P; ++b) {
+            const double own = cv * double(2 * e + 1) * (yneg ? neg1pow(e + b + 1) : 1.0);
+            const double up = cv * double(2 * e + 1) * (yneg ? neg1pow(b) : neg1pow(e + 1));
+#pragma unroll
+            for (int d = 0; d < P; ++d) y[b + P * d] += own * x0[e + P * d] + up * yd[e + P * d];
+        }
+#pragma unroll
+    for (int e = 0; e < P; ++e)
+#pragma unroll
+        for (int b = e - 1; b >= 0; b -= 2)
+#pragma unroll
+            for (int d = 0; d < P; ++d) y[b + P * d] -= double(2 * (2 * e + 1)) * cv * x0[e + P * d];
+}
+
+// y <- beta*y + alpha*L^T x on interior cells, plus gamma * w_q sigma_s zsum / (4 pi) when zsum (the
+// unweighted moment sums of x, sum_q x_q) is given: with gamma = -1 that is (L - S P)^T x, the transpose of
+// the IDC residual operator (S P x puts sigma_s sum_q w_q x_q / (4 pi) on every ordinate; its transpose puts
+// w_q sigma_s sum_q' x_q' / (4 pi) on ordinate q).  Ghost cells of y are not written.
+template <int P, typename IDX>
+__global__ void lmvt_kernel(GridDims g, double alpha, double beta, const double *__restrict__ sigma_t,
+                            const double *__restrict__ xi_a, const double *__restrict__ eta_a,
+                            const double *__restrict__ w_a, const double *__restrict__ x, double *__restrict__ y,
+                            double gamma, const double *__restrict__ sigma_s, const double *__restrict__ zsum) {
+    constexpr int N = P * P;
+    const size_t plane = (size_t)g.nq * N;
+    const size_t istride = (size_t)(g.ny + 2) * plane;
+    const IDX total = (IDX)g.nx * g.ny * g.nq;
+    for (IDX t = blockIdx.x * (IDX)blockDim.x + threadIdx.x; t < total; t += (IDX)gridDim.x * blockDim.x) {
+        const IDX cell = t / (IDX)g.nq;
+        const int q = (int)(t - cell * (IDX)g.nq);
+        const int i = 1 + (int)(cell / (IDX)g.ny), j = 1 + (int)(cell - (cell / (IDX)g.ny) * (IDX)g.ny);
+        const double xi = xi_a[q], eta = eta_a[q];
+        const int id = i + (xi <= 0.0 ? -1 : 1), jd = j + (eta <= 0.0 ? -1 : 1);
+        const size_t base = (size_t)i * istride + (size_t)j * plane + (size_t)q * N;
+        const size_t cidx = (size_t)i * (g.ny + 2) + j;
+        double y3[N];
+        lmvt_point<P>(g, x, base, istride, plane, xi, eta, sigma_t[cidx], id >= 1 && id <= g.nx, jd >= 1 && jd <= g.ny,
+                      y3);
+        if (zsum) {
+            const double c = gamma * w_a[q] * sigma_s[cidx] / (4.0 * M_PI);
+#pragma unroll
+            for (int k = 0; k < N; ++k) y3[k] = fma(c, zsum[cidx * N + k], y3[k]);
+        }
+        double *Y = y + base;
+#pragma unroll
+        for (int k = 0; k < N; ++k) Y[k] = beta == 0.0 ? alpha * y3[k] : beta * Y[k] + alpha * y3[k];
+    }
+}
+
+// out(q, cell, k) = w_q m(cell, k) on interior cells: P^T m, the adjoint of the moment functional m . P psi as
+// an angular array.  Ghost cells of out are not written.
+__global__ void weighted_broadcast_kernel(GridDims g, const double *__restrict__ w, const double *__restrict__ m,
+                                          double *__restrict__ out) {
+    const int N = g.P * g.P;
+    const size_t total = (size_t)g.nx * g.ny * g.nq * N;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const size_t cell = t / ((size_t)g.nq * N);
+        const size_t rest = t - cell * ((size_t)g.nq * N);
+        const int q = (int)(rest / N), k = (int)(rest - (size_t)q * N);
+        const int i = 1 + (int)(cell / g.ny), j = 1 + (int)(cell % g.ny);
+        const size_t cidx = (size_t)i * (g.ny + 2) + j;
+        out[(cidx * g.nq + q) * N + k] = w[q] * m[cidx * N + k];
+    }
+}
+
 template <int P, typename IDX>
 __global__ void lmv_kernel(GridDims g, double alpha, double beta, const double *__restrict__ sigma_t,
                            const double *__restrict__ xi_a, const double *__restrict__ eta_a,
@@ -385,7 +495,7 @@ __global__ void adjoint_scatter_kernel(GridDims g, const double *__restrict__ si
 __global__ void adjoint_gradient_kernel(GridDims g, const double *__restrict__ psi, const double *__restrict__ lam,
                                         const double *__restrict__ phi, const double *__restrict__ Lam,
                                         double *__restrict__ dsig_t, double *__restrict__ dsig_s, double *__restrict__ dq,
-                                        int accumulate) {
+                                        int accumulate, double scale) {
     const int N = g.P * g.P;
     const int lane = threadIdx.x & 31;
     const size_t warps = (size_t)gridDim.x * (blockDim.x / 32);
@@ -401,12 +511,12 @@ __global__ void adjoint_gradient_kernel(GridDims g, const double *__restrict__ p
         if (lane < N) {
             const double L = Lam[cidx * N + lane];
             accs = L * phi[cidx * N + lane];
-            if (dq) dq[cidx * N + lane] = (accumulate ? dq[cidx * N + lane] : 0.0) + L / (4.0 * M_PI);
+            if (dq) dq[cidx * N + lane] = (accumulate ? dq[cidx * N + lane] : 0.0) + scale * (L / (4.0 * M_PI));
         }
         for (int off = 16; off > 0; off >>= 1) accs += __shfl_xor_sync(0xffffffffu, accs, off);
         if (lane == 0) {
-            if (dsig_t) dsig_t[cidx] = (accumulate ? dsig_t[cidx] : 0.0) - acc;
-            if (dsig_s) dsig_s[cidx] = (accumulate ? dsig_s[cidx] : 0.0) + accs / (4.0 * M_PI);
+            if (dsig_t) dsig_t[cidx] = (accumulate ? dsig_t[cidx] : 0.0) - scale * acc;
+            if (dsig_s) dsig_s[cidx] = (accumulate ? dsig_s[cidx] : 0.0) + scale * (accs / (4.0 * M_PI));
         }
     }
 }
@@ -467,6 +577,37 @@ static void lmv_p(const GridDims &g, size_t n, double alpha, double beta, const 
                                                                   phi_sc);
 }
 
+template <int P>
+static void lmvt_p(const GridDims &g, size_t n, double alpha, double beta, const double *sigma_t, const double *xi,
+                   const double *eta, const double *w, const double *x, double *y, double gamma,
+                   const double *sigma_s, const double *zsum, cudaStream_t s) {
+    if (n < (size_t)INT32_MAX)
+        lmvt_kernel<P, int32_t><<<blocks_for(n), kThreads, 0, s>>>(g, alpha, beta, sigma_t, xi, eta, w, x, y, gamma,
+                                                                    sigma_s, zsum);
+    else
+        lmvt_kernel<P, size_t><<<blocks_for(n), kThreads, 0, s>>>(g, alpha, beta, sigma_t, xi, eta, w, x, y, gamma,
+                                                                   sigma_s, zsum);
+}
+
+cudaError_t launch_lmv_transpose(const GridDims &g, double alpha, double beta, const double *sigma_t, const double *xi,
+                                 const double *eta, const double *w, const double *x, double *y, cudaStream_t s,
+                                 double gamma, const double *sigma_s, const double *zsum) {
+    const size_t n = (size_t)g.nx * g.ny * g.nq;
+    switch (g.P) {
+        case 1: lmvt_p<1>(g, n, alpha, beta, sigma_t, xi, eta, w, x, y, gamma, sigma_s, zsum, s); break;
+        case 2: lmvt_p<2>(g, n, alpha, beta, sigma_t, xi, eta, w, x, y, gamma, sigma_s, zsum, s); break;
+        case 3: lmvt_p<3>(g, n, alpha, beta, sigma_t, xi, eta, w, x, y, gamma, sigma_s, zsum, s); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_weighted_broadcast(const GridDims &g, const double *w, const double *m, double *out,
+                                     cudaStream_t s) {
+    weighted_broadcast_kernel<<<blocks_for((size_t)g.nx * g.ny * g.nq * g.P * g.P), kThreads, 0, s>>>(g, w, m, out);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_lmv(const GridDims &g, double alpha, double beta, const double *sigma_t, const double *xi,
                        const double *eta, const double *x, double *y, cudaStream_t s, double gamma,
                        const double *sigma_s, const double *phi_sc) {
@@ -524,10 +665,10 @@ cudaError_t launch_adjoint_scatter(const GridDims &g, const double *sigma_s, con
 
 cudaError_t launch_adjoint_gradient(const GridDims &g, const double *psi, const double *lam, const double *phi,
                                     const double *Lam, double *dsig_t, double *dsig_s, double *dq, cudaStream_t s,
-                                    bool accumulate) {
+                                    bool accumulate, double scale) {
     const size_t warps = (size_t)g.nx * g.ny;
     adjoint_gradient_kernel<<<blocks_for(warps * 32), kThreads, 0, s>>>(g, psi, lam, phi, Lam, dsig_t, dsig_s, dq,
-                                                                        accumulate ? 1 : 0);
+                                                                        accumulate ? 1 : 0, scale);
     return cudaGetLastError();
 }
 

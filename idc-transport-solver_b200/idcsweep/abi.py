@@ -48,7 +48,7 @@ EXPORTED_SYMBOLS = (
     "idc_write_af2", "idc_read_af2", "idc_sweep_fused", "idc_set_tile_shape", "idc_autotune", "idc_batch_create",
     "idc_batch_add", "idc_batch_sweep", "idc_batch_autotune", "idc_batch_last_timing", "idc_batch_destroy",
     "idc_batch_set_shape", "idc_batch_get_shape", "idc_sweep_out_many", "idc_adjoint_transient",
-    "idc_set_spin_limit", "idc_batch_gmres_solve", "idc_set_allreduce",
+    "idc_set_spin_limit", "idc_batch_gmres_solve", "idc_set_allreduce", "idc_adjoint_idc", "idc_lmv_transpose",
 )
 
 
@@ -99,6 +99,9 @@ def load_library(path: str = LIB_PATH):
     lib.idc_set_tiling.argtypes = [vp, C.c_int32, C.c_int32]
     lib.idc_set_spin_limit.argtypes = [vp, C.c_int64]
     lib.idc_set_allreduce.argtypes = [vp, ALLREDUCE_FN, vp]
+    lib.idc_adjoint_idc.argtypes = [vp, vp, vp, C.c_double, C.c_int64, C.c_int32, C.c_int32, vp, C.c_int64, C.c_double,
+                                    C.c_int32, C.c_int64, C.c_int, vp, vp, vp, vp, _dp, C.c_int, C.POINTER(C.c_int64)]
+    lib.idc_lmv_transpose.argtypes = [vp, C.c_double, C.c_double, vp, vp, C.c_int]
     lib.idc_sweep_out.argtypes = [vp, vp, vp, C.c_double, vp, C.c_int, C.c_int]
     lib.idc_sweep_out_many.argtypes = [vp, C.c_int64, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.c_double,
                                        C.c_int, C.c_int]
@@ -321,6 +324,27 @@ class SweepContext:
                                                _ptr(dsigma_s, loc), _ptr(dsource, loc), _ptr(dpsi0, loc),
                                                C.byref(jv), loc, C.byref(ns)), "idc_adjoint_transient")
         return float(jv.value), int(ns.value)
+
+    def adjoint_idc(self, psi0, source, detector, dt, steps, num_nodes=4, num_corrections=3, checkpoint_every=0,
+                    dsigma_t=None, dsigma_s=None, dsource=None, dpsi0=None, abs_tol=1e-12, restart=30, max_its=3000,
+                    precision=PREC_FP64, loc=LOC_HOST):
+        """Gradients of J = detector . phi(psi^steps) after `steps` implicit-scattering IDC steps (num_nodes
+        Gauss-Lobatto nodes, num_corrections corrections) from psi0 with the constant source, written into the
+        given arrays.  Returns (J, number of forward and adjoint GMRES solves)."""
+        jv = C.c_double()
+        ns = C.c_int64()
+        _check(self._lib.idc_adjoint_idc(self._h, _ptr(psi0, loc), _ptr(source, loc), float(dt), int(steps),
+                                         int(num_nodes), int(num_corrections), _ptr(detector, loc),
+                                         int(checkpoint_every), float(abs_tol), int(restart), int(max_its),
+                                         int(precision), _ptr(dsigma_t, loc), _ptr(dsigma_s, loc),
+                                         _ptr(dsource, loc), _ptr(dpsi0, loc), C.byref(jv), loc, C.byref(ns)),
+               "idc_adjoint_idc")
+        return float(jv.value), int(ns.value)
+
+    def lmv_transpose(self, alpha, beta, x_ptr, y_ptr):
+        """Device pointers: y <- beta y + alpha L^T x (interior cells)."""
+        _check(self._lib.idc_lmv_transpose(self._h, float(alpha), float(beta), C.c_void_p(int(x_ptr)),
+                                           C.c_void_p(int(y_ptr)), LOC_DEVICE), "idc_lmv_transpose")
 
     def set_spin_limit(self, polls: int = 0):
         """Polls before a device-side wait gives up (0: the default)."""

@@ -299,6 +299,30 @@ int idc_adjoint_transient(idc_ctx *ctx, const double *psi0, const double *source
                           int64_t max_its, int precision, double *dsigma_t, double *dsigma_s, double *dsource,
                           double *dpsi0, double *J, int loc, int64_t *solves);
 
+/* The same gradients for IDC time stepping with implicit scattering (idc_idc_integrate with
+ * IDC_SCATTER_IMPLICIT: num_nodes Gauss-Lobatto nodes, num_corrections correction sweeps, update form, every
+ * substep (1/(h dt) + L - S P) psi_n = src_n solved by the Peierls GMRES), J = sum detector * phi(psi^steps).
+ * The adjoint runs backwards through every step's correction levels: for each substep the transposed
+ * solve A_n^T lam = (the stage's adjoint), which feeds the previous substep's adjoint (lam / (h dt)) and the
+ * adjoints of the previous level's residuals (the quadrature weights times lam); those become the previous
+ * level's stage adjoints through the transpose of the residual operator, (L - S P)^T (the transposed Lmv).
+ * The gradient terms are the solves' (as idc_adjoint_transient) and the residuals' (the same form, opposite
+ * sign, no source term).  Checkpointing as idc_adjoint_transient (each step's stages are recomputed from its
+ * input in the backward pass); device memory holds about steps / checkpoint_every + checkpoint_every +
+ * (num_corrections + 1) num_nodes + 3 num_nodes angular fluxes.  No counterpart in the reference: it is the
+ * transpose of IDCIntegrator::Step_Nonhybrid with ComputeResiduals / ComputeSource (update form),
+ * time_integrators/RKDG/idc.cpp:846-955, 1657-1740. */
+int idc_adjoint_idc(idc_ctx *ctx, const double *psi0, const double *source, double dt, int64_t steps,
+                    int32_t num_nodes, int32_t num_corrections, const double *detector, int64_t checkpoint_every,
+                    double abs_tol, int32_t restart, int64_t max_its, int precision, double *dsigma_t,
+                    double *dsigma_s, double *dsource, double *dpsi0, double *J, int loc, int64_t *solves);
+
+/* y = beta y + alpha L^T x on interior cells (device arrays, psi layout): the transpose of idc_lmv with x's
+ * ghost cells taken as zero (boundary data, not unknowns); y's ghost cells are not written.  The transpose of
+ * TransportOperator::Lmv (operators/RKDG/TransportOperator.cpp:1215-1689), which the reference has no use for;
+ * the IDC adjoint applies it to the residuals' adjoints. */
+int idc_lmv_transpose(idc_ctx *ctx, double alpha, double beta, const double *x, double *y, int loc);
+
 /* ---- binary files ------------------------------------------------------------------------------------ */
 
 /* The reference's serial 2-D binary formats, on the halo layouts of this ABI (no GPU involved).
