@@ -378,6 +378,40 @@ def extra_adjoint_transient(abi, torch, dev, steps=10, dt=0.5, every=0):
     return out
 
 
+def extra_adjoint_idc(abi, torch, dev, steps=4, dt=0.5, nodes=4, corrections=3, every=0):
+    """The same 128x128 Q1 S8 problem with IDC time stepping (4 Gauss-Lobatto nodes, 3 corrections, implicit
+    scattering: every substep a GMRES + DSA solve): gradients of the detector response after 4 steps of
+    dt = 0.5 from zero flux through the correction sweeps (idc_adjoint_idc), checkpointed."""
+    from idcsweep.problems import detector_window, lognormal
+    P = lognormal(128, 1, 8, seed=0, median=2.0, log_sd=0.7, c_fixed=0.9, source="gaussian")
+    d = f"cuda:{dev}"
+    c_det = torch.from_numpy(detector_window(P, cells=16)).to(d)
+    src = torch.from_numpy(P.source).to(d)
+    psi0 = torch.zeros_like(src)
+    out = {"workload": f"128x128 Q1 S8 as the adjoint line, {steps} IDC steps ({nodes} Gauss-Lobatto nodes, "
+                       f"{corrections} corrections, implicit scattering) of dt {dt} from zero flux; GMRES(30) + DSA "
+                       "(20 CG steps) forward and adjoint, abs tol 1e-12",
+           "gradient_entries": 3 * P.nx * P.ny}
+    with _ctx_for(abi, P, dev) as c:
+        c.set_preconditioner(abi.PRECOND_DSA, 20)
+        g_t = torch.zeros((P.nx + 2) * (P.ny + 2), dtype=torch.float64, device=d)
+        g_s = torch.zeros_like(g_t)
+        g_q = torch.zeros(P.phi_shape(), dtype=torch.float64, device=d)
+        g_p = torch.zeros_like(src)
+        args = (psi0.data_ptr(), src.data_ptr(), c_det.data_ptr(), dt, steps, nodes, corrections)
+        kw = dict(checkpoint_every=every, dsigma_t=g_t.data_ptr(), dsigma_s=g_s.data_ptr(), dsource=g_q.data_ptr(),
+                  dpsi0=g_p.data_ptr(), abs_tol=1e-12, loc=abi.LOC_DEVICE)
+        c.adjoint_idc(*args, **kw)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        J, solves = c.adjoint_idc(*args, **kw)
+        torch.cuda.synchronize()
+        sec = time.perf_counter() - t0
+        out["fp64"] = {"grads_per_s": out["gradient_entries"] / sec, "ms": sec * 1e3, "gmres_solves": solves,
+                       "J": J}
+    return out
+
+
 def extra_batched(abi, torch, dev, n_problems=64):
     """64 independent steady problems: side U{32,...,384}, S4/S8/S12/S16, Q1/Q2, log-normal sigma_t (median 1,
     log-sd 1), c U[0.3, 0.99] (seeded); one sweep of every problem, batched (one launch per DG degree,
@@ -761,7 +795,7 @@ def run_ours(args):
 
 
 EXTRAS = {"gmres_dsa": extra_gmres_dsa, "idc": extra_idc, "adjoint": extra_adjoint,
-          "adjoint_transient": extra_adjoint_transient, "batched": extra_batched}
+          "adjoint_transient": extra_adjoint_transient, "adjoint_idc": extra_adjoint_idc, "batched": extra_batched}
 
 
 def run_only_extra(name):
