@@ -679,6 +679,14 @@ int idc_set_spin_limit(idc_ctx *ctx, int64_t polls) {
     ABI_GUARD_END
 }
 
+int idc_set_reflecting(idc_ctx *ctx, int32_t edges) {
+    ABI_GUARD_BEGIN
+    if (!ctx) return fail(IDC_ERR_ARG, "null context");
+    ABI_TRY(ctx->impl.set_reflecting((int)edges));
+    return IDC_OK;
+    ABI_GUARD_END
+}
+
 int idc_set_allreduce(idc_ctx *ctx, idc_allreduce_fn fn, void *user) {
     ABI_GUARD_BEGIN
     if (!ctx) return fail(IDC_ERR_ARG, "null context");

@@ -46,6 +46,10 @@ Context::~Context() {
     for (double *p : transient_bufs_) cudaFree(p);
     for (double *p : adj_idc_bufs_) cudaFree(p);
     cudaFree(d_ones_);
+    cudaFree(d_rmap);
+    cudaFree(d_reflect_);
+    cudaFree(d_reflect_g_);
+    cudaFree(d_reflect_vec_);
     cudaFree(d_scalar_);
     cudaFree(d_xi);
     cudaFree(d_eta);
@@ -136,12 +140,172 @@ Status Context::set_ordinates(int64_t nq_in, const double *xi, const double *eta
         }
         cudaFree(d_ones_);
         d_ones_ = nullptr;
+        cudaFree(d_reflect_);
+        d_reflect_ = nullptr;
+        cudaFree(d_reflect_g_);   // sized by nq and the reflecting edges
+        d_reflect_g_ = nullptr;
+        reflect_g_len_ = 0;
+        cudaFree(d_reflect_vec_);
+        d_reflect_vec_ = nullptr;
+        reflect_vec_len_ = 0;
     }
     nq = nq_in;
     for (int k = 0; k < 5; ++k) quad[k] = qb[k];
     have_ordinates = true;
     n_items = 0;   // schedule rebuilt lazily
     occupancy_precision = -1;
+    if (reflect_mask) return update_reflect_map();
+    return Status::ok();
+}
+
+// The reflection partner of every ordinate in x (-xi, eta) and in y (xi, -eta), found as the reference's
+// OrdinateData::ComputeReflectMap finds it (utils/Quadrule/OrdinateSet.cpp:1093-1140: coordinates equal
+// within 1e-14).
+Status Context::update_reflect_map() {
+    std::vector<double> xi(nq), eta(nq);
+    IDC_TRY_CUDA(cudaMemcpy(xi.data(), d_xi, sizeof(double) * nq, cudaMemcpyDeviceToHost));
+    IDC_TRY_CUDA(cudaMemcpy(eta.data(), d_eta, sizeof(double) * nq, cudaMemcpyDeviceToHost));
+    std::vector<int> map(2 * (size_t)nq, -1);
+    for (int dim = 0; dim < 2; ++dim)
+        for (int64_t q = 0; q < nq; ++q) {
+            for (int64_t k = 0; k < nq; ++k) {
+                const double dx_ = dim == 0 ? xi[q] + xi[k] : xi[q] - xi[k];
+                const double dy_ = dim == 1 ? eta[q] + eta[k] : eta[q] - eta[k];
+                if (std::fabs(dx_) < 1e-14 && std::fabs(dy_) < 1e-14) {
+                    map[(size_t)dim * nq + q] = (int)k;
+                    break;
+                }
+            }
+            if (map[(size_t)dim * nq + q] < 0)
+                return bad(IDC_ERR_ARG, "reflecting boundaries: ordinate " + std::to_string(q) +
+                                            " has no reflection partner in dimension " + std::to_string(dim));
+        }
+    cudaFree(d_rmap);
+    d_rmap = nullptr;
+    IDC_TRY_CUDA(cudaMalloc(&d_rmap, sizeof(int) * map.size()));
+    IDC_TRY_CUDA(cudaMemcpy(d_rmap, map.data(), sizeof(int) * map.size(), cudaMemcpyHostToDevice));
+    return Status::ok();
+}
+
+Status Context::set_reflecting(int mask) {
+    if (mask < 0 || mask > 15) return bad(IDC_ERR_ARG, "reflecting edges: bits 1 x-min, 2 x-max, 4 y-min, 8 y-max");
+    IDC_TRY_CUDA(cudaSetDevice(device));
+    const int old = reflect_mask;
+    reflect_mask = mask;
+    if (mask && have_ordinates) {
+        Status st = update_reflect_map();
+        if (!st.good()) {
+            reflect_mask = old;
+            return st;
+        }
+    }
+    return Status::ok();
+}
+
+// A sweep with reflecting boundaries, as the reference's SweepPatternUniCartWavefront::Sweep makes it
+// (linear_solvers/Abstract/SweepPattern/SweepPatternUniCartWavefront.cpp:186-251): the quadrants one after
+// another in its default order 3, 2, 1, 0 (SweepPatternUniCart.cpp:33-36), in place, and after each the
+// reflecting edges' ghost cells refilled from the current interior values (OrdinateFlux::ReflectBoundaries).
+// The array starts as the reference's in-place array does: the source, with the fused scattering term
+// materialised (the reference applies Smv into the array before Apply), so a quadrant swept before its
+// reflection partner reads the ghost values the array came with.
+Status Context::sweep_reflecting(const double *src, double *out, double dt, double *phi, int precision,
+                                 const double *phi_scatter, double scatter_scale, bool adjoint, const double *src2) {
+    if (adjoint || src2)
+        return bad(IDC_ERR_UNSUPPORTED, "reflecting boundaries: forward sweeps with one source only");
+    if (kernel_for(precision) != kLane)
+        return bad(IDC_ERR_UNSUPPORTED,
+                   "reflecting boundaries need the lane kernel: FP64 or FP32 sweeps at a lane tile shape");
+    if (allreduce_fn)
+        return bad(IDC_ERR_UNSUPPORTED, "reflecting boundaries with ordinates partitioned over ranks");
+    double *w = out;
+    if (!w) {
+        if (!d_reflect_) {
+            if (capturing) return bad(IDC_ERR_STATE, "reflecting-sweep buffer allocation inside a stream capture");
+            IDC_TRY_CUDA(cudaMalloc(&d_reflect_, sizeof(double) * psi_len()));
+        }
+        w = d_reflect_;
+    }
+    if (src) {
+        if (w != src)
+            IDC_TRY_CUDA(cudaMemcpyAsync(w, src, sizeof(double) * psi_len(), cudaMemcpyDeviceToDevice, stream));
+    } else {
+        IDC_TRY_CUDA(cudaMemsetAsync(w, 0, sizeof(double) * psi_len(), stream));
+    }
+    if (phi_scatter) {   // TransportOperator::Smv(scale, 1, sigma_s, phi -> w)
+        IDC_TRY_CUDA(launch_smv(dims(), scatter_scale, 1.0, d_sigma_s, phi_scatter, w, stream));
+        launches += 1;
+    }
+    return reflect_quadrants(w, dt, phi, precision);
+}
+
+// The sequential-quadrant sweep proper, in place on a prepared array w; phi (optional) gets the moments of
+// all four quadrants.
+Status Context::reflect_quadrants(double *w, double dt, double *phi, int precision) {
+    in_reflect_ = true;
+    Status st = Status::ok();
+    for (int quad : {3, 2, 1, 0}) {
+        quad_mask_ = 1 << quad;
+        skip_reduce_ = quad != 0;   // the chunk partials of every quadrant are summed after the last
+        st = sweep(w, w, dt, phi, precision);
+        if (!st.good()) break;
+        cudaError_t e = launch_reflect_boundaries(dims(), reflect_mask, d_xi, d_eta, d_rmap, w, stream);
+        if (e != cudaSuccess) {
+            st = cuda_status(e, "launch_reflect_boundaries");
+            break;
+        }
+        launches += 1;
+    }
+    in_reflect_ = false;
+    quad_mask_ = 0;
+    skip_reduce_ = false;
+    return st;
+}
+
+Status Context::reflect_ghosts(double *psi, double *packed, bool to_packed) {
+    IDC_TRY_CUDA(launch_reflect_ghosts(dims(), reflect_mask, d_xi, d_eta, psi, packed, to_packed, stream));
+    launches += 1;
+    return Status::ok();
+}
+
+// SISolver::Solve (linear_solvers/Abstract/ImplicitSolver/SISolver.cpp:190-254) with reflecting edges.  psi
+// starts at zero (SetInitialGuess(nullptr)), and each iteration copies the source with OpDomain::Interior |
+// OpDomain::Boundary, which leaves out the reflecting edges' ghost cells (DomainDecomposition::DetermineOffsets,
+// objects/DomainDecomposition.cpp:271-330): the reflections left by one sweep are the inflow that the next
+// sweep's quadrants read before their partners are swept.  The fixed point is the reflecting problem's solution.
+Status Context::source_iteration_reflecting(const double *src, double *psi_out, double dt, double abs_tol,
+                                            int64_t max_its, int precision, int64_t *iters, double *err) {
+    if (src == psi_out) return bad(IDC_ERR_ARG, "source iteration: source and psi must be different arrays");
+    const size_t ng = reflect_ghost_len(dims(), reflect_mask);
+    if (reflect_g_len_ < ng) {
+        if (capturing) return bad(IDC_ERR_STATE, "reflecting-sweep buffer allocation inside a stream capture");
+        cudaFree(d_reflect_g_);
+        d_reflect_g_ = nullptr;
+        reflect_g_len_ = 0;
+        IDC_TRY_CUDA(cudaMalloc(&d_reflect_g_, sizeof(double) * ng));
+        reflect_g_len_ = ng;
+    }
+    IDC_TRY(ensure_phi_buffers(2));
+    double *phi_cur = phi_buf(0), *phi_last = phi_buf(1);
+    IDC_TRY_CUDA(cudaMemsetAsync(phi_cur, 0, sizeof(double) * phi_len(), stream));
+    IDC_TRY_CUDA(cudaMemsetAsync(phi_last, 0, sizeof(double) * phi_len(), stream));
+    IDC_TRY_CUDA(cudaMemsetAsync(psi_out, 0, sizeof(double) * psi_len(), stream));
+    int64_t it = 0;
+    double e = INFINITY;
+    while (it < max_its && e > abs_tol) {
+        ++it;
+        std::swap(phi_cur, phi_last);
+        IDC_TRY(reflect_ghosts(psi_out, d_reflect_g_, true));    // keep the reflections of the last sweep
+        IDC_TRY_CUDA(cudaMemcpyAsync(psi_out, src, sizeof(double) * psi_len(), cudaMemcpyDeviceToDevice, stream));
+        IDC_TRY(reflect_ghosts(psi_out, d_reflect_g_, false));
+        IDC_TRY_CUDA(launch_smv(dims(), 1.0, 1.0, d_sigma_s, phi_last, psi_out, stream));
+        launches += 1;
+        IDC_TRY(reflect_quadrants(psi_out, dt, phi_cur, precision));
+        IDC_TRY(l2dist(phi_cur, phi_last, &e));
+        IDC_TRY(check_device_error());
+    }
+    if (iters) *iters = it;
+    if (err) *err = e;
     return Status::ok();
 }
 
@@ -485,6 +649,8 @@ Status Context::sweep(const double *src, double *out, double dt, double *phi, in
         return bad(IDC_ERR_UNSUPPORTED, "the transposed sweep needs the modal kernel in FP64 or refined precision");
     if (src2 && (adjoint || !modal_family() || !src))
         return bad(IDC_ERR_UNSUPPORTED, "a second source needs a forward modal sweep with a first source");
+    if (reflect_mask && !in_reflect_)
+        return sweep_reflecting(src, out, dt, phi, precision, phi_scatter, scatter_scale, adjoint, src2);
     IDC_TRY(build_schedule(precision));
     IDC_TRY_CUDA(cudaSetDevice(device));
 
@@ -539,6 +705,7 @@ Status Context::sweep(const double *src, double *out, double dt, double *phi, in
     a.n_items = n_items;
     a.R = tiling.R;
     a.G = tiling.G;
+    a.quad_mask = quad_mask_;
     a.n_refine = 1;
     a.seg = seg;
     a.wn = wn;
@@ -632,7 +799,7 @@ Status Context::sweep(const double *src, double *out, double dt, double *phi, in
     if (a.phi_part && phi_only) {
         IDC_TRY_CUDA(launch_reduce_modal_partials(dims(), d_phi_part, quad_slots, phi_len(), phi, stream));
         launches += 1;
-    } else if (a.phi_part) {
+    } else if (a.phi_part && !skip_reduce_) {
         IDC_TRY_CUDA(launch_reduce_phi_partials(dims(), d_phi_part, items_per_rb, phi_len(), phi, stream));
         launches += 1;
     }
@@ -713,6 +880,7 @@ Status Context::l2dist(const double *a, const double *b, double *out_host) {
 // fused into the sweep (source read + scattering term on the fly, moments in the epilogue).
 Status Context::source_iteration(const double *src, double *psi_out, double dt, double abs_tol, int64_t max_its,
                                  int precision, int64_t *iters, double *err) {
+    if (reflect_mask) return source_iteration_reflecting(src, psi_out, dt, abs_tol, max_its, precision, iters, err);
     IDC_TRY(ensure_phi_buffers(2));
     double *phi_cur = phi_buf(0), *phi_last = phi_buf(1);
     IDC_TRY_CUDA(cudaMemsetAsync(phi_cur, 0, sizeof(double) * phi_len(), stream));

@@ -66,9 +66,12 @@ public:
     int ir_corrections = 0;   // corrections (FP64 residual sweeps) of the last refined solve
     // GMRES(restart) from x = 0 on A x = b for an operator on moment-sized vectors; *converged reports
     // whether the residual reached abs_tol (the caller decides whether that is an error)
+    // whether the residual reached abs_tol (the caller decides whether that is an error).  n_extra unknowns
+    // follow the moments in every vector (the reflecting edges' ghost values); the preconditioner leaves them.
     template <typename Op>
     Status gmres(Op apply, const double *b, double *x, double abs_tol, int restart, int64_t max_its, int64_t *iters,
-                 double *resid, bool *converged, int dsa_mode = 0);   // 0 none, 1 DSA, 2 transposed DSA
+                 double *resid, bool *converged, int dsa_mode = 0,   // 0 none, 1 DSA, 2 transposed DSA
+                 size_t n_extra = 0);
     Status set_preconditioner(int kind, int inner_steps);   // 0 none, 1 DSA
     // IDC time integration (idc.cpp): psi (device, in/out) advanced `steps` steps of size dt with M
     // Gauss-Lobatto nodes and K corrections; scattering 0 = explicit (IMEX, one sweep per substep, CUDA
@@ -176,6 +179,28 @@ public:
     // 0 on success (idc_set_allreduce)
     int (*allreduce_fn)(double *data, int64_t n, void *user) = nullptr;
     void *allreduce_user = nullptr;
+    // reflecting boundaries (idc_set_reflecting): the reference's BoundaryEdge bits, the reflection partners
+    // [2][nq] on the device, and the state of a sequential-quadrant sweep in progress
+    int reflect_mask = 0;
+    int *d_rmap = nullptr;
+    int quad_mask_ = 0;
+    bool skip_reduce_ = false, in_reflect_ = false;
+    double *d_reflect_ = nullptr;   // psi-sized work array of reflecting sweeps that return no psi
+    double *d_reflect_g_ = nullptr;  // the reflecting edges' ghost values, packed (source iteration)
+    size_t reflect_g_len_ = 0;
+    double *d_reflect_vec_ = nullptr;   // GMRES vectors [moments; packed ghost values]: b, x, work
+    size_t reflect_vec_len_ = 0;
+    Status set_reflecting(int mask);
+    Status update_reflect_map();
+    Status sweep_reflecting(const double *src, double *out, double dt, double *phi, int precision,
+                            const double *phi_scatter, double scatter_scale, bool adjoint, const double *src2);
+    Status reflect_quadrants(double *w, double dt, double *phi, int precision);
+    Status reflect_ghosts(double *psi, double *packed, bool to_packed);
+    Status source_iteration_reflecting(const double *src, double *psi_out, double dt, double abs_tol,
+                                       int64_t max_its, int precision, int64_t *iters, double *err);
+    Status apply_peierls_reflecting(const double *x, double *y, double *tmp, double dt, int precision);
+    Status gmres_peierls_reflecting(const double *src, double *psi_out, double dt, double abs_tol, int restart,
+                                    int64_t max_its, int precision, int64_t *iters, double *resid);
 
     double *d_krylov = nullptr;    // GMRES basis, (restart + 1) phi-sized vectors (+ restart for flexible GMRES)
     int precond_kind = 0;          // 0 none, 1 DSA (right preconditioner of the forward Peierls GMRES)

@@ -72,6 +72,8 @@ struct SweepArgs {
                                // fused source is w_q mu; the moments are unweighted sums over ordinates)
     int skip;                  // batched modal launch: 1 = this problem is not swept this time (its items return
                                // at once; nothing of it is read or written)
+    int quad_mask;             // lane kernel: quadrants swept by this launch (bit k = quadrant k), 0 = all; items of
+                               // the others return at once (reflecting boundaries sweep the quadrants in sequence)
     const double *modal_src;   // lane kernel, moments-only forward sweeps: the packed modal source of every
                                // (cell, quadrant), [(nx+2)(ny+2)][4][N] (launch_modal_sources), or null; the
                                // partial moments are then packed modal sums (launch_reduce_modal_partials)
@@ -171,6 +173,19 @@ cudaError_t launch_lmv_transpose(const GridDims &g, double alpha, double beta, c
 // out = w_q m on interior cells (P^T of a moment array as an angular array); ghost cells of out not written
 cudaError_t launch_weighted_broadcast(const GridDims &g, const double *w, const double *m, double *out,
                                      cudaStream_t s);
+// Reflecting boundaries (OrdinateFlux::ReflectBoundaries, objects/RKDG/OrdinateFlux.cpp:1181-1415): for each
+// reflecting edge in `mask` (1 x-min, 2 x-max, 4 y-min, 8 y-max), the ghost cells of the ordinates entering
+// through it (at y-max, of every ordinate, as the reference's loop) take the first interior cell's values of
+// their reflected ordinate (rmap[q] for x, rmap[nq + q] for y) with the mirrored Legendre modes' signs, (-1)^d
+// (x) or (-1)^e (y)
+cudaError_t launch_reflect_boundaries(const GridDims &g, int mask, const double *xi, const double *eta,
+                                      const int *rmap, double *psi, cudaStream_t s);
+// The ghost values of the reflecting edges' entering ordinates, packed edge after edge (x-min, x-max, y-min, y-max
+// of `mask`), each edge [cell][q][dof]; the entries of ordinates leaving through an edge are 0 in the pack.
+// to_packed: packed <- ghosts; else ghosts <- packed (0 for leaving ordinates, and for all when packed is null).
+size_t reflect_ghost_len(const GridDims &g, int mask);
+cudaError_t launch_reflect_ghosts(const GridDims &g, int mask, const double *xi, const double *eta, double *psi,
+                                  double *packed, bool to_packed, cudaStream_t s);
 cudaError_t launch_zero_ghost_phi(const GridDims &g, double *phi, cudaStream_t s);
 // out = sigma_s phi / (4 pi) per interior cell and moment (the isotropic scattering source of Smv, formed once
 // per cell for the modal sweep's fused source; ghost cells of out are not written)

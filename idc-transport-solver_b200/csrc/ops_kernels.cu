@@ -228,6 +228,78 @@ __global__ void weighted_broadcast_kernel(GridDims g, const double *__restrict__
     }
 }
 
+// One thread per (edge cell, ordinate, dof) of the reflecting edges: see launch_reflect_boundaries.
+__global__ void reflect_kernel(GridDims g, int mask, const double *__restrict__ xi, const double *__restrict__ eta,
+                               const int *__restrict__ rmap, double *__restrict__ psi) {
+    const int N = g.P * g.P;
+    const size_t nxe = (size_t)g.ny * g.nq * N, nye = (size_t)g.nx * g.nq * N;   // per x edge, per y edge
+    const size_t total = 2 * nxe + 2 * nye;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const int edge = t < nxe ? 0 : t < 2 * nxe ? 1 : t < 2 * nxe + nye ? 2 : 3;   // x-min, x-max, y-min, y-max
+        if (!((mask >> edge) & 1)) continue;
+        size_t r = edge < 2 ? t - edge * nxe : t - 2 * nxe - (edge - 2) * nye;
+        const int k = (int)(r % N);
+        r /= N;
+        const int q = (int)(r % g.nq);
+        const int cell = (int)(r / g.nq);   // j - 1 (x edges) or i - 1 (y edges)
+        // ordinates entering through the edge: xi > 0 at x-min, xi < 0 at x-max, eta > 0 at y-min; at y-max the
+        // reference's loop takes every quadrant (OrdinateFlux.cpp:1399), so the ghost values of the ordinates
+        // leaving there, which no sweep reads, are written as well
+        const bool in = edge == 0 ? xi[q] > 0.0 : edge == 1 ? xi[q] < 0.0 : edge == 2 ? eta[q] > 0.0 : true;
+        if (!in) continue;
+        const int d = k / g.P, e = k - (k / g.P) * g.P;
+        int ig, jg, ii, jj, qr;
+        double sgn;
+        if (edge < 2) {
+            jg = jj = cell + 1;
+            ig = edge == 0 ? 0 : g.nx + 1;
+            ii = edge == 0 ? 1 : g.nx;
+            qr = rmap[q];
+            sgn = (d & 1) ? -1.0 : 1.0;
+        } else {
+            ig = ii = cell + 1;
+            jg = edge == 2 ? 0 : g.ny + 1;
+            jj = edge == 2 ? 1 : g.ny;
+            qr = rmap[g.nq + q];
+            sgn = (e & 1) ? -1.0 : 1.0;
+        }
+        const size_t src = (((size_t)ii * (g.ny + 2) + jj) * g.nq + qr) * N + k;
+        const size_t dst = (((size_t)ig * (g.ny + 2) + jg) * g.nq + q) * N + k;
+        psi[dst] = sgn * psi[src];
+    }
+}
+
+// One thread per (edge cell, ordinate, dof) of the reflecting edges, packed edge after edge (x-min, x-max, y-min,
+// y-max; absent edges take no room): see launch_reflect_ghosts.
+__global__ void reflect_ghosts_kernel(GridDims g, int mask, const double *__restrict__ xi,
+                                      const double *__restrict__ eta, double *__restrict__ psi,
+                                      double *__restrict__ packed, int to_packed) {
+    const int N = g.P * g.P;
+    const size_t nxe = (size_t)g.ny * g.nq * N, nye = (size_t)g.nx * g.nq * N;
+    size_t len[4], total = 0;
+    for (int e = 0; e < 4; ++e) {
+        len[e] = ((mask >> e) & 1) ? (e < 2 ? nxe : nye) : 0;
+        total += len[e];
+    }
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        int edge = 0;
+        size_t r = t;
+        while (r >= len[edge]) r -= len[edge++];
+        const int k = (int)(r % N);
+        r /= N;
+        const int q = (int)(r % g.nq);
+        const int cell = (int)(r / g.nq);
+        const bool in = edge == 0 ? xi[q] > 0.0 : edge == 1 ? xi[q] < 0.0 : edge == 2 ? eta[q] > 0.0 : eta[q] < 0.0;
+        const int ig = edge < 2 ? (edge == 0 ? 0 : g.nx + 1) : cell + 1;
+        const int jg = edge < 2 ? cell + 1 : (edge == 2 ? 0 : g.ny + 1);
+        const size_t gi = (((size_t)ig * (g.ny + 2) + jg) * g.nq + q) * N + k;
+        if (to_packed)
+            packed[t] = in ? psi[gi] : 0.0;
+        else
+            psi[gi] = (in && packed) ? packed[t] : 0.0;
+    }
+}
+
 template <int P, typename IDX>
 __global__ void lmv_kernel(GridDims g, double alpha, double beta, const double *__restrict__ sigma_t,
                            const double *__restrict__ xi_a, const double *__restrict__ eta_a,
@@ -605,6 +677,26 @@ cudaError_t launch_lmv_transpose(const GridDims &g, double alpha, double beta, c
 cudaError_t launch_weighted_broadcast(const GridDims &g, const double *w, const double *m, double *out,
                                      cudaStream_t s) {
     weighted_broadcast_kernel<<<blocks_for((size_t)g.nx * g.ny * g.nq * g.P * g.P), kThreads, 0, s>>>(g, w, m, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reflect_boundaries(const GridDims &g, int mask, const double *xi, const double *eta,
+                                      const int *rmap, double *psi, cudaStream_t s) {
+    const size_t total = 2 * (size_t)(g.nx + g.ny) * g.nq * g.P * g.P;
+    reflect_kernel<<<blocks_for(total), kThreads, 0, s>>>(g, mask, xi, eta, rmap, psi);
+    return cudaGetLastError();
+}
+
+size_t reflect_ghost_len(const GridDims &g, int mask) {
+    const size_t per = (size_t)g.nq * g.P * g.P;
+    return per * ((mask & 1 ? g.ny : 0) + (mask & 2 ? g.ny : 0) + (mask & 4 ? g.nx : 0) + (mask & 8 ? g.nx : 0));
+}
+
+cudaError_t launch_reflect_ghosts(const GridDims &g, int mask, const double *xi, const double *eta, double *psi,
+                                  double *packed, bool to_packed, cudaStream_t s) {
+    const size_t total = reflect_ghost_len(g, mask);
+    if (total == 0) return cudaSuccess;
+    reflect_ghosts_kernel<<<blocks_for(total), kThreads, 0, s>>>(g, mask, xi, eta, psi, packed, to_packed ? 1 : 0);
     return cudaGetLastError();
 }
 

@@ -60,10 +60,10 @@ Status Context::apply_peierls(const double *x, double *y, double *tmp_phi, doubl
 // linear) and x = Z y.
 template <typename Op>
 Status Context::gmres(Op apply, const double *b, double *x, double abs_tol, int restart, int64_t max_its,
-                      int64_t *iters_out, double *resid_out, bool *converged_out, int dsa_mode) {
+                      int64_t *iters_out, double *resid_out, bool *converged_out, int dsa_mode, size_t n_extra) {
     const bool dsa = dsa_mode != 0;
     if (restart < 1 || restart > 60) return bad(IDC_ERR_ARG, "gmres restart must be in 1..60");
-    const size_t n = phi_len();
+    const size_t n = phi_len() + n_extra;
     const int m = restart;
     const size_t need = (size_t)(dsa ? 2 * m + 1 : m + 1) * n;
     if (krylov_len < need) {
@@ -113,6 +113,9 @@ Status Context::gmres(Op apply, const double *b, double *x, double abs_tol, int 
                 IDC_TRY_CUDA(dsa_precondition(dims(), d_sigma_s, Vc(j), Zc(j), dsa_steps, d_dsa_ws, dsa_mode == 2,
                                               num_sms, d_sync + 1, spin_limit, stream));
                 launches += kDsaLaunches;
+                if (n_extra)
+                    IDC_TRY_CUDA(cudaMemcpyAsync(Zc(j) + phi_len(), Vc(j) + phi_len(), sizeof(double) * n_extra,
+                                                 cudaMemcpyDeviceToDevice, stream));
                 IDC_TRY(apply(Zc(j), Vc(j + 1)));
             } else {
                 IDC_TRY(apply(Vc(j), Vc(j + 1)));
@@ -188,10 +191,81 @@ Status Context::gmres(Op apply, const double *b, double *x, double abs_tol, int 
     return Status::ok();
 }
 
+// The Peierls operator with reflecting edges, on x = [phi; g], g the reflecting edges' ghost values at the start
+// of a sweep (packed as launch_reflect_ghosts packs them): the sequential-quadrant sweep of the scattering
+// source S phi with vacuum inflow on the other edges and g on the reflecting ones, y = x - [P psi; g(psi)], g(psi)
+// the ghost values that the sweep leaves.  Source iteration with reflecting edges is the fixed-point iteration
+// of exactly this map (the reflections of one sweep are the next sweep's inflow), so GMRES on it reaches the
+// source-iteration fixed point for every set of reflecting edges.  The reference's Peierls operator
+// (PETScPeierlsSolver.cpp:529-572) starts every sweep from zero ghost cells instead (Smv over OpDomain::All of
+// a scalar flux unpacked with zero halos): the same solution where the quadrant order reaches every reflection
+// partner before it is read (x-min and y-min edges), a different one elsewhere.
+Status Context::apply_peierls_reflecting(const double *x, double *y, double *tmp, double dt, int precision) {
+    const size_t np = phi_len(), n = np + reflect_ghost_len(dims(), reflect_mask);
+    double *w = d_reflect_;
+    IDC_TRY_CUDA(cudaMemsetAsync(w, 0, sizeof(double) * psi_len(), stream));
+    IDC_TRY(reflect_ghosts(w, const_cast<double *>(x) + np, false));
+    IDC_TRY_CUDA(launch_smv(dims(), 1.0, 1.0, d_sigma_s, x, w, stream));
+    IDC_TRY(reflect_quadrants(w, dt, tmp, precision));
+    IDC_TRY(reflect_ghosts(w, tmp + np, true));
+    IDC_TRY_CUDA(launch_axpby(1.0, x, 0.0, y, n, stream));
+    IDC_TRY_CUDA(launch_axpby(-1.0, tmp, 1.0, y, n, stream));
+    launches += 3;
+    return Status::ok();
+}
+
+// GMRES on (I - K) [phi; g] = b with K the map above and b the sweep of Q (its own inflow on the other edges,
+// zero reflecting ghost values); then psi is the sweep of Q + S phi with g in the reflecting ghost cells.
+Status Context::gmres_peierls_reflecting(const double *src, double *psi_out, double dt, double abs_tol, int restart,
+                                         int64_t max_its, int precision, int64_t *iters_out, double *resid_out) {
+    if (precision == IDC_PREC_FP32_IR)
+        return bad(IDC_ERR_UNSUPPORTED, "reflecting boundaries: GMRES with FP64 or FP32 sweeps");
+    if (kernel_for(precision) != kLane)
+        return bad(IDC_ERR_UNSUPPORTED,
+                   "reflecting boundaries need the lane kernel: FP64 or FP32 sweeps at a lane tile shape");
+    if (allreduce_fn)
+        return bad(IDC_ERR_UNSUPPORTED, "reflecting boundaries with ordinates partitioned over ranks");
+    const size_t np = phi_len(), ng = reflect_ghost_len(dims(), reflect_mask), n = np + ng;
+    if (capturing && (!d_reflect_ || reflect_vec_len_ < 3 * n))
+        return bad(IDC_ERR_STATE, "reflecting-solve buffer allocation inside a stream capture");
+    if (!d_reflect_) IDC_TRY_CUDA(cudaMalloc(&d_reflect_, sizeof(double) * psi_len()));
+    if (reflect_vec_len_ < 3 * n) {
+        cudaFree(d_reflect_vec_);
+        d_reflect_vec_ = nullptr;
+        reflect_vec_len_ = 0;
+        IDC_TRY_CUDA(cudaMalloc(&d_reflect_vec_, sizeof(double) * 3 * n));
+        reflect_vec_len_ = 3 * n;
+    }
+    double *b = d_reflect_vec_, *x = b + n, *tmp = x + n;
+    double *w = d_reflect_;
+    IDC_TRY_CUDA(cudaMemcpyAsync(w, src, sizeof(double) * psi_len(), cudaMemcpyDeviceToDevice, stream));
+    IDC_TRY(reflect_ghosts(w, nullptr, false));
+    IDC_TRY(reflect_quadrants(w, dt, b, precision));
+    IDC_TRY(reflect_ghosts(w, b + np, true));
+    bool converged = false;
+    double resid = 0.0;
+    auto op = [&](const double *in, double *out) { return apply_peierls_reflecting(in, out, tmp, dt, precision); };
+    IDC_TRY(gmres(op, b, x, abs_tol, restart, max_its, iters_out, &resid, &converged, precond_kind == 1 ? 1 : 0,
+                  ng));
+    IDC_TRY_CUDA(cudaMemcpyAsync(psi_out, src, sizeof(double) * psi_len(), cudaMemcpyDeviceToDevice, stream));
+    IDC_TRY(reflect_ghosts(psi_out, x + np, false));
+    IDC_TRY_CUDA(launch_smv(dims(), 1.0, 1.0, d_sigma_s, x, psi_out, stream));
+    launches += 1;
+    IDC_TRY(reflect_quadrants(psi_out, dt, nullptr, precision));
+    IDC_TRY(check_device_error());
+    if (resid_out) *resid_out = resid;
+    if (!converged)
+        return bad(IDC_ERR_NOT_CONVERGED, "GMRES transport solve failed to converge (max_its reached, residual " +
+                                              std::to_string(resid) + ")");
+    return Status::ok();
+}
+
 // (I - P L^{-1} S) phi = P L^{-1} Q (PETScPeierlsSolver.cpp:423-572), then psi = L^{-1}(S phi + Q).
 Status Context::gmres_peierls(const double *src, double *psi_out, double dt, double abs_tol, int restart,
                               int64_t max_its, int precision, int64_t *iters_out, double *resid_out) {
     if (!use_warp_kernel) return bad(IDC_ERR_UNSUPPORTED, "GMRES needs the warp-pipelined sweep kernel");
+    if (reflect_mask)
+        return gmres_peierls_reflecting(src, psi_out, dt, abs_tol, restart, max_its, precision, iters_out, resid_out);
     if (precision == IDC_PREC_FP32_IR) return gmres_peierls_ir(src, psi_out, dt, abs_tol, restart, max_its, iters_out,
                                                                resid_out);
     IDC_TRY(ensure_phi_buffers(6));

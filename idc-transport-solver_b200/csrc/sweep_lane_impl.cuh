@@ -238,6 +238,7 @@ template <int P, int SEG, bool ADJ, bool SRC2, bool PHI, typename TC>
 __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &item, int it_index, double *wsm,
                                          int lane) {
     constexpr int N = P * P, Rw = 32 / SEG, D = kStages;
+    if (a.quad_mask != 0 && ((a.quad_mask >> item.quadrant) & 1) == 0) return;   // another quadrant's launch
     // quadrant signs: flips of the cell values (exact), traversal directions (reversed for the transpose)
     const bool XN = item.quadrant >= 2, YN = (item.quadrant & 1) != 0;
     const bool TX = XN != ADJ, TY = YN != ADJ;

@@ -20,6 +20,7 @@ LIB_PATH = os.path.join(os.path.dirname(HERE), "build", "libidcsweep.so")
 IDC_OK = 0
 PRECOND_NONE, PRECOND_DSA = 0, 1
 SCATTER_EXPLICIT, SCATTER_IMPLICIT = 0, 1
+EDGE_X_MIN, EDGE_X_MAX, EDGE_Y_MIN, EDGE_Y_MAX = 1, 2, 4, 8
 IDC_ERR_ARG = 1
 IDC_ERR_UNSUPPORTED = 2
 IDC_ERR_CUDA = 3
@@ -49,6 +50,7 @@ EXPORTED_SYMBOLS = (
     "idc_batch_add", "idc_batch_sweep", "idc_batch_autotune", "idc_batch_last_timing", "idc_batch_destroy",
     "idc_batch_set_shape", "idc_batch_get_shape", "idc_sweep_out_many", "idc_adjoint_transient",
     "idc_set_spin_limit", "idc_batch_gmres_solve", "idc_set_allreduce", "idc_adjoint_idc", "idc_lmv_transpose",
+    "idc_set_reflecting",
 )
 
 
@@ -102,6 +104,7 @@ def load_library(path: str = LIB_PATH):
     lib.idc_adjoint_idc.argtypes = [vp, vp, vp, C.c_double, C.c_int64, C.c_int32, C.c_int32, vp, C.c_int64, C.c_double,
                                     C.c_int32, C.c_int64, C.c_int, vp, vp, vp, vp, _dp, C.c_int, C.POINTER(C.c_int64)]
     lib.idc_lmv_transpose.argtypes = [vp, C.c_double, C.c_double, vp, vp, C.c_int]
+    lib.idc_set_reflecting.argtypes = [vp, C.c_int32]
     lib.idc_sweep_out.argtypes = [vp, vp, vp, C.c_double, vp, C.c_int, C.c_int]
     lib.idc_sweep_out_many.argtypes = [vp, C.c_int64, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.c_double,
                                        C.c_int, C.c_int]
@@ -345,6 +348,10 @@ class SweepContext:
         """Device pointers: y <- beta y + alpha L^T x (interior cells)."""
         _check(self._lib.idc_lmv_transpose(self._h, float(alpha), float(beta), C.c_void_p(int(x_ptr)),
                                            C.c_void_p(int(y_ptr)), LOC_DEVICE), "idc_lmv_transpose")
+
+    def set_reflecting(self, edges: int = 0):
+        """Reflecting edges: EDGE_X_MIN | EDGE_X_MAX | EDGE_Y_MIN | EDGE_Y_MAX (0: none)."""
+        _check(self._lib.idc_set_reflecting(self._h, int(edges)), "idc_set_reflecting")
 
     def set_spin_limit(self, polls: int = 0):
         """Polls before a device-side wait gives up (0: the default)."""

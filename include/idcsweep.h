@@ -359,6 +359,28 @@ const char *idc_last_error_message(void);
  * reference has no counterpart (its OpenMP barriers wait without bound). */
 int idc_set_spin_limit(idc_ctx *ctx, int64_t polls);
 
+/* Reflecting boundaries: `edges` as the reference's BoundaryEdge bits (IDC_EDGE_X_MIN 1, IDC_EDGE_X_MAX 2,
+ * IDC_EDGE_Y_MIN 4, IDC_EDGE_Y_MAX 8; 0 = none, the default).  With any, every sweep of the context (idc_sweep,
+ * idc_source_iteration, idc_gmres_solve) runs the quadrants one after another in the reference's order
+ * 3, 2, 1, 0, in place, and after each quadrant refills the reflecting edges' ghost cells of the ordinates
+ * entering through them with the first interior cell's values of the reflected ordinate, the mirrored
+ * Legendre modes negated (SweepPatternUniCartWavefront::Sweep with sweep_octants_in_sequence,
+ * linear_solvers/Abstract/SweepPattern/SweepPatternUniCartWavefront.cpp:186-251, and
+ * OrdinateFlux::ReflectBoundaries, objects/RKDG/OrdinateFlux.cpp:1181-1360).  Every ordinate needs its
+ * reflection partner in the set (IDC_ERR_ARG otherwise, as the reference's ComputeReflectMap).  The
+ * source's ghost cells on the other edges are the inflow; the result's ghost cells on reflecting edges hold
+ * the last reflection.  idc_source_iteration follows SISolver::Solve: psi starts at zero and the reflecting
+ * edges' ghost cells are not copied from the source, so each sweep reads the reflections of the last.
+ * idc_gmres_solve adds the reflecting edges' incoming ghost values to its unknowns and reaches the same fixed
+ * point for every edge set.  FP64 and FP32 sweeps (the lane kernel); IDC_PREC_FP32_IR, transposed sweeps,
+ * IDC time stepping, batches and ordinate-partitioned solves with reflecting boundaries return
+ * IDC_ERR_UNSUPPORTED. */
+#define IDC_EDGE_X_MIN 1
+#define IDC_EDGE_X_MAX 2
+#define IDC_EDGE_Y_MIN 4
+#define IDC_EDGE_Y_MAX 8
+int idc_set_reflecting(idc_ctx *ctx, int32_t edges);
+
 /* Ordinate-partitioned solves over several processes (one rank per GPU; each rank's context holds its slice
  * of every quadrant's ordinates, e.g. contiguous near-equal chunks): `fn` sums a moment-sized array of the
  * context's GPU over the ranks, in place, and must give every rank bitwise the same sums (an NCCL or MPI

@@ -45,6 +45,7 @@ namespace {
 int64_t next_order_key = 1000000;
 
 struct RefProblem {
+    int reflect = 0;   // BoundaryEdge bits of the reflecting edges (Global::reflecting_boundaries while in use)
     int64_t nx, ny, p, N, nq;
     int64_t order_key;
     ParameterList plist;
@@ -84,6 +85,11 @@ int64_t InjectOrdinates ( int64_t nq, const double * xi, const double * eta, con
         data.weights[q] = w[q];
     }
     data.LocateOctants();
+    try {   // reflection partners, for reflecting boundaries (level-symmetric sets have them)
+        data.ComputeReflectMap();
+    } catch ( std::exception & ) {
+        data.reflect_map = nullptr;
+    }
 
     OrdinateSet::ordinate_cache.insert(
         std::make_pair( std::make_tuple( data.type, data.order, true ), data ) );
@@ -99,6 +105,13 @@ void CopyOut ( const Abstract::DensityFunction & f, double * dst, size_t n ) {
     std::memcpy( dst, f.density, n * sizeof(double) );
 }
 
+// Global::reflecting_boundaries of a problem for the duration of a call into the reference (the reference
+// reads the global in its sweeps), reset afterwards so that other problems see none.
+struct ReflectScope {
+    explicit ReflectScope ( int mask ) {  Global::reflecting_boundaries = static_cast<BoundaryEdge>( mask );  }
+    ~ReflectScope () {  Global::reflecting_boundaries = BoundaryEdge::None;  }
+};
+
 } // namespace
 
 
@@ -110,12 +123,14 @@ extern "C" {
 // (index j + (ny+2)*i), time step dt (+inf for steady state).  sweep_pattern is the reference's key
 // ("wavefront" or "sequential").  Returns an opaque handle, or nullptr on error.
 //------------------------------------------------------------------------------------------------------------
-void * ref_create ( int64_t nx, int64_t ny, double ax, double bx, double ay, double by, int64_t p,
-                    int64_t nq, const double * xi, const double * eta, const double * w,
-                    const double * sigma_t, const double * sigma_s, double dt,
-                    const char * sweep_pattern, double si_abs_tol, int64_t si_max_its ) {
+void * ref_create_reflecting ( int64_t nx, int64_t ny, double ax, double bx, double ay, double by, int64_t p,
+                               int64_t nq, const double * xi, const double * eta, const double * w,
+                               const double * sigma_t, const double * sigma_s, double dt,
+                               const char * sweep_pattern, double si_abs_tol, int64_t si_max_its, int reflect ) {
     try {
+        ReflectScope scope( reflect );   // SweepPatternUniCart decides on sequential quadrants when built
         auto * P = new RefProblem();
+        P->reflect = reflect;
         P->nx = nx; P->ny = ny; P->p = p; P->N = (p + 1) * (p + 1); P->nq = nq; P->dt = dt;
 
         Global::DG_degree = p;
@@ -170,11 +185,21 @@ void * ref_create ( int64_t nx, int64_t ny, double ax, double bx, double ay, dou
     }
 }
 
+// The same without reflecting boundaries (vacuum or given inflow on every edge).
+void * ref_create ( int64_t nx, int64_t ny, double ax, double bx, double ay, double by, int64_t p,
+                    int64_t nq, const double * xi, const double * eta, const double * w,
+                    const double * sigma_t, const double * sigma_s, double dt,
+                    const char * sweep_pattern, double si_abs_tol, int64_t si_max_its ) {
+    return ref_create_reflecting( nx, ny, ax, bx, ay, by, p, nq, xi, eta, w, sigma_t, sigma_s, dt, sweep_pattern,
+                                  si_abs_tol, si_max_its, 0 );
+}
+
 void ref_destroy ( void * h ) { delete static_cast<RefProblem *>(h); }
 
 // SweepOperator::Apply on psi_inout (halo layout, source in / psi out).  *seconds = wall time of Apply.
 int ref_apply ( void * h, double * psi_inout, double dt, double * seconds ) {
     auto * P = static_cast<RefProblem *>(h);
+    ReflectScope scope( P->reflect );
     try {
         CopyIn( *P->psi, psi_inout, P->psi_len() );
         auto t0 = std::chrono::steady_clock::now();
@@ -190,6 +215,7 @@ int ref_apply ( void * h, double * psi_inout, double dt, double * seconds ) {
 // previous ref_apply (the data is re-loaded before each one so every sweep sees the same source).
 int ref_apply_timed ( void * h, const double * source, double dt, int64_t reps, double * seconds ) {
     auto * P = static_cast<RefProblem *>(h);
+    ReflectScope scope( P->reflect );
     try {
         double total = 0.0;
         for ( int64_t r = 0; r < reps; ++r ) {
@@ -207,6 +233,7 @@ int ref_apply_timed ( void * h, const double * source, double dt, int64_t reps, 
 // phi <- beta*phi + alpha*P psi over interior cells (TransportOperator::Pmv with OpDomain::Interior).
 int ref_pmv ( void * h, double alpha, double beta, const double * psi, double * phi ) {
     auto * P = static_cast<RefProblem *>(h);
+    ReflectScope scope( P->reflect );
     try {
         CopyIn( *P->psi, psi, P->psi_len() );
         CopyIn( *P->phi, phi, P->phi_len() );
@@ -219,6 +246,7 @@ int ref_pmv ( void * h, double alpha, double beta, const double * psi, double * 
 // psi <- beta*psi + alpha*S phi over interior cells with sigma_s (TransportOperator::Smv).
 int ref_smv ( void * h, double alpha, double beta, const double * phi, double * psi ) {
     auto * P = static_cast<RefProblem *>(h);
+    ReflectScope scope( P->reflect );
     try {
         CopyIn( *P->psi, psi, P->psi_len() );
         CopyIn( *P->phi, phi, P->phi_len() );
@@ -231,6 +259,7 @@ int ref_smv ( void * h, double alpha, double beta, const double * phi, double * 
 // y <- beta*y + alpha*L x with sigma_t (TransportOperator::Lmv, out-of-place form).
 int ref_lmv ( void * h, double alpha, double beta, const double * x, double * y ) {
     auto * P = static_cast<RefProblem *>(h);
+    ReflectScope scope( P->reflect );
     try {
         CopyIn( *P->psi, x, P->psi_len() );
         CopyIn( *P->aux, y, P->psi_len() );
@@ -244,6 +273,7 @@ int ref_lmv ( void * h, double alpha, double beta, const double * x, double * y 
 // return.  *iters and *err report the iteration count and the final absolute l2 change of phi.
 int ref_si_solve ( void * h, double * source_inout, double dt, int64_t * iters, double * seconds ) {
     auto * P = static_cast<RefProblem *>(h);
+    ReflectScope scope( P->reflect );
     try {
         CopyIn( *P->aux, source_inout, P->psi_len() );
         P->si->SetInitialGuess( nullptr );
@@ -268,6 +298,7 @@ int ref_si_solve ( void * h, double * source_inout, double dt, int64_t * iters, 
 int ref_idc_steps ( void * h, double * psi_inout, const double * source, double dt, int64_t steps,
                     int64_t num_nodes, int64_t num_corr, double si_abs_tol, int64_t si_max_its ) {
     auto * P = static_cast<RefProblem *>(h);
+    ReflectScope scope( P->reflect );
     try {
         ParameterList pl = P->plist;
         char buf[64];
@@ -302,6 +333,7 @@ int ref_idc_steps ( void * h, double * psi_inout, const double * source, double 
 // halo layout: the reference's .sd2 file.
 int ref_write_sd ( void * h, const double * phi, const char * path ) {
     auto * P = static_cast<RefProblem *>(h);
+    ReflectScope scope( P->reflect );
     try {
         CopyIn( *P->phi, phi, P->phi_len() );
         P->phi->WriteToDisk( std::string( path ) );
@@ -313,6 +345,7 @@ int ref_write_sd ( void * h, const double * phi, const char * path ) {
 // layout: the reference's .af2 file.
 int ref_write_af ( void * h, const double * psi, const char * path ) {
     auto * P = static_cast<RefProblem *>(h);
+    ReflectScope scope( P->reflect );
     try {
         CopyIn( *P->psi, psi, P->psi_len() );
         P->psi->WriteToDisk( std::string( path ) );

@@ -94,9 +94,10 @@ public:
     void Sweep ( const OrdinateFlux & source, OrdinateFlux & result, const RKDG::CrossSection & sigma,
                  const RKDG::OrdinateFlux * const /* initial_condition: not used by a direct sweep */ ) const override {
 
-        if ( this->sweep_octants_in_sequence )   // reflecting boundaries (SweepPatternUniCart.cpp:46-88)
-            throw std::runtime_error( "gpu-wavefront: reflecting boundaries are not supported" );
-
+        // reflecting boundaries (SweepPatternUniCart.cpp:46-88): the library sweeps the quadrants in the same
+        // sequence and reflects between them; the BoundaryEdge bits are the ABI's IDC_EDGE_* bits
+        idc_check( idc_set_reflecting( this->ctx, static_cast<int32_t>( Global::reflecting_boundaries ) & 15 ),
+                   "idc_set_reflecting" );
         idc_check( idc_set_sigma( this->ctx, sigma.PointerAtCell( 0, 0 ), nullptr, IDC_LOC_HOST ), "idc_set_sigma" );
         const double dt = this->sw_op.sweep_cell_solve->GetDt();   // set by SweepOperator::Apply
         if ( &source == &result ) {

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from conftest import gpu_available, rel_err, to_oracle
-from idcsweep.problems import lattice, random_problem
+from idcsweep.problems import lattice, lognormal, random_problem
 from oracle.bindings import REFERENCE_GPU_SO, Reference
 
 pytestmark = pytest.mark.skipif(not os.path.exists(REFERENCE_GPU_SO),
@@ -66,4 +66,18 @@ def test_reference_idc_integrator_through_plugin(plugged):
     for pattern in ("wavefront", "gpu-wavefront"):
         with plugged.open(to_oracle(P), P.dt, pattern=pattern, abs_tol=1e-13, max_its=100000) as h:
             out[pattern] = h.idc_steps(psi0, P.source, P.dt, 2, 4, 3, si_abs_tol=1e-13)
+    assert rel_err(out["gpu-wavefront"], out["wavefront"]) < 1e-11
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("edges", [1, 2 | 4, 15])
+def test_reference_source_iteration_with_reflecting_edges_through_plugin(plugged, edges):
+    """The reference's SISolver::Solve with reflecting edges (sequential quadrants, ReflectBoundaries between
+    them): gpu-wavefront against wavefront."""
+    P = lognormal(20, 1, 8, seed=7, c_range=(0.3, 0.9), dt=0.3)
+    out = {}
+    for pattern in ("wavefront", "gpu-wavefront"):
+        with plugged.open(to_oracle(P), P.dt, pattern=pattern, abs_tol=1e-12, max_its=5000, reflect=edges) as h:
+            psi = h.source_iteration(P.source, P.dt)
+            out[pattern] = h.pmv(psi)
     assert rel_err(out["gpu-wavefront"], out["wavefront"]) < 1e-11
