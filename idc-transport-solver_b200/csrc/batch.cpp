@@ -79,6 +79,7 @@ Status Batch::add(Context *c) {
     if (!c->have_ordinates || !c->have_sigma) return bad(IDC_ERR_STATE, "batch member without ordinates or sigma");
     if (!c->modal_family()) return bad(IDC_ERR_UNSUPPORTED, "batched sweeps need the modal kernel");
     if (c->reflect_mask) return bad(IDC_ERR_UNSUPPORTED, "batched sweeps with reflecting boundaries");
+    if (c->high_order_sigma()) return bad(IDC_ERR_UNSUPPORTED, "batched sweeps with high-order cross sections");
     if (!members.empty() && c->device != members[0]->device) return bad(IDC_ERR_ARG, "batch members on different GPUs");
     members.push_back(c);
     release();

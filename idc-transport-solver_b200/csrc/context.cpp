@@ -56,6 +56,11 @@ Context::~Context() {
     cudaFree(d_w);
     cudaFree(d_sigma_t);
     cudaFree(d_sigma_s);
+    cudaFree(d_sig_mom_);
+    cudaFree(d_tens_t_);
+    cudaFree(d_tens_s_);
+    cudaFree(d_cat_t_);
+    cudaFree(d_work_psi_);
     cudaFree(d_items);
     cudaFree(d_sync);
     cudaFree(d_phi_part);
@@ -148,6 +153,8 @@ Status Context::set_ordinates(int64_t nq_in, const double *xi, const double *eta
         cudaFree(d_reflect_vec_);
         d_reflect_vec_ = nullptr;
         reflect_vec_len_ = 0;
+        cudaFree(d_work_psi_);
+        d_work_psi_ = nullptr;
     }
     nq = nq_in;
     for (int k = 0; k < 5; ++k) quad[k] = qb[k];
@@ -200,6 +207,30 @@ Status Context::set_reflecting(int mask) {
         }
     }
     return Status::ok();
+}
+
+// A sweep whose source carries the scattering term with high-order cross sections: the term is formed by the
+// tensor Smv into the array first, as the reference's solvers apply Smv into the array before Apply
+// (SISolver.cpp:226-232, PETScPeierlsSolver.cpp:504-505 and :551-552), then the array is swept in place.
+Status Context::sweep_tensor_source(const double *src, double *out, double dt, double *phi, int precision,
+                                    const double *phi_scatter, double scatter_scale) {
+    double *w = out;
+    if (!w) {
+        if (!d_work_psi_) {
+            if (capturing) return bad(IDC_ERR_STATE, "work array allocation inside a stream capture");
+            IDC_TRY_CUDA(cudaMalloc(&d_work_psi_, sizeof(double) * psi_len()));
+        }
+        w = d_work_psi_;
+    }
+    if (src) {
+        if (w != src)
+            IDC_TRY_CUDA(cudaMemcpyAsync(w, src, sizeof(double) * psi_len(), cudaMemcpyDeviceToDevice, stream));
+    } else {
+        IDC_TRY_CUDA(cudaMemsetAsync(w, 0, sizeof(double) * psi_len(), stream));
+    }
+    IDC_TRY_CUDA(launch_smv_tensor(dims(), scatter_scale, 1.0, d_tens_s_, phi_scatter, w, stream));
+    launches += 1;
+    return sweep(w, out, dt, phi, precision);
 }
 
 // A sweep with reflecting boundaries, as the reference's SweepPatternUniCartWavefront::Sweep makes it
@@ -309,12 +340,56 @@ Status Context::source_iteration_reflecting(const double *src, double *psi_out, 
     return Status::ok();
 }
 
+namespace {
+
+// The integrals over [-1, 1] of P_a P_b P_c for degrees a, b, c < P (Global::TPI, utils/global.cpp:67-110, which
+// evaluates them by Gauss-Legendre quadrature): here from the monomial coefficients of the Legendre polynomials
+// (Bonnet's recurrence) and the exact monomial integrals 2 / (k + 1) for even k; values below 5e-16 are zero,
+// as the reference clears them.
+TripleProducts triple_products(int P) {
+    double c[3][3] = {{1, 0, 0}, {0, 1, 0}, {-0.5, 0, 1.5}};   // P_0, P_1, P_2 by powers of x
+    TripleProducts t{};
+    for (int a = 0; a < P; ++a)
+        for (int b = 0; b < P; ++b)
+            for (int cc = 0; cc < P; ++cc) {
+                double v = 0.0;
+                for (int i = 0; i < 3; ++i)
+                    for (int j = 0; j < 3; ++j)
+                        for (int k = 0; k < 3; ++k) {
+                            const int deg = i + j + k;
+                            if (deg % 2 == 0) v += c[a][i] * c[b][j] * c[cc][k] * (2.0 / (deg + 1));
+                        }
+                t.v[a + P * (b + P * cc)] = std::fabs(v) < 5e-16 ? 0.0 : v;
+            }
+    return t;
+}
+
+}  // namespace
+
 Status Context::set_sigma(const double *sigma_t, const double *sigma_s, int loc) {
     if (!sigma_t) return bad(IDC_ERR_ARG, "set_sigma: sigma_t is null");
     IDC_TRY_CUDA(cudaSetDevice(device));
     if (!d_sigma_t) IDC_TRY_CUDA(cudaMalloc(&d_sigma_t, sizeof(double) * sig_len()));
     if (!d_sigma_s) IDC_TRY_CUDA(cudaMalloc(&d_sigma_s, sizeof(double) * sig_len()));
     const cudaMemcpyKind kind = loc == IDC_LOC_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    if (high_order_sigma()) {   // Legendre moments [cell][u][v] of both cross sections
+        const size_t nm = sig_len() * N, nt = sig_len() * N * N;
+        if (!d_sig_mom_) IDC_TRY_CUDA(cudaMalloc(&d_sig_mom_, sizeof(double) * nm));
+        if (!d_tens_t_) IDC_TRY_CUDA(cudaMalloc(&d_tens_t_, sizeof(double) * nt));
+        if (!d_tens_s_) IDC_TRY_CUDA(cudaMalloc(&d_tens_s_, sizeof(double) * nt));
+        if (!d_cat_t_) IDC_TRY_CUDA(cudaMalloc(&d_cat_t_, sizeof(double) * nt));
+        const TripleProducts tpi = triple_products(P);
+        IDC_TRY_CUDA(cudaMemcpyAsync(d_sig_mom_, sigma_t, sizeof(double) * nm, kind, stream));
+        IDC_TRY_CUDA(launch_sigma_tensor(dims(), d_sig_mom_, tpi, dx * dy / 4.0, d_sigma_t, d_tens_t_, d_cat_t_, stream));
+        if (sigma_s)
+            IDC_TRY_CUDA(cudaMemcpyAsync(d_sig_mom_, sigma_s, sizeof(double) * nm, kind, stream));
+        else
+            IDC_TRY_CUDA(cudaMemsetAsync(d_sig_mom_, 0, sizeof(double) * nm, stream));
+        IDC_TRY_CUDA(launch_sigma_tensor(dims(), d_sig_mom_, tpi, 0.0, d_sigma_s, d_tens_s_, nullptr, stream));
+        IDC_TRY_CUDA(cudaStreamSynchronize(stream));
+        have_sigma = true;
+        return Status::ok();
+    }
     IDC_TRY_CUDA(cudaMemcpy(d_sigma_t, sigma_t, sizeof(double) * sig_len(), kind));
     if (sigma_s)
         IDC_TRY_CUDA(cudaMemcpy(d_sigma_s, sigma_s, sizeof(double) * sig_len(), kind));
@@ -337,6 +412,7 @@ Status Context::set_tiling(int G, int R) {
 // the lane kernel, else the modal kernel), and without a tile shape the lane kernel; the lane kernel
 // sweeps in FP64 only, the FP32 modes run on the modal kernel.  IDC_SWEEP_KERNEL fixes another kernel.
 int Context::kernel_for(int precision) const {
+    if (high_order_sigma()) return kWarp;   // the elimination kernel takes a full cell matrix
     if (kernel != kLane) return kernel;
     if (tune_seg > 0 && tune_wn > 0) return kModal;
     return sweep_lane_supports(P, precision, tune_seg > 0 ? tune_seg : 4) ? kLane : kModal;
@@ -359,6 +435,7 @@ Status Context::set_tile_shape(int s, int w) {
 
 // Candidate tile shapes, timed with CUDA events on this problem (best of three sweeps after a warm-up).
 Status Context::autotune(const double *src, double dt, int precision, int *seg_out, int *wn_out) {
+    if (high_order_sigma()) return bad(IDC_ERR_UNSUPPORTED, "high-order cross sections use the elimination kernel");
     if (!modal_family()) return bad(IDC_ERR_UNSUPPORTED, "the autotuner tunes the lane and modal kernels");
     IDC_TRY(ensure_psi_buffers(1));
     IDC_TRY(ensure_phi_buffers(1));
@@ -649,6 +726,13 @@ Status Context::sweep(const double *src, double *out, double dt, double *phi, in
         return bad(IDC_ERR_UNSUPPORTED, "the transposed sweep needs the modal kernel in FP64 or refined precision");
     if (src2 && (adjoint || !modal_family() || !src))
         return bad(IDC_ERR_UNSUPPORTED, "a second source needs a forward modal sweep with a first source");
+    if (high_order_sigma()) {
+        if (precision != IDC_PREC_FP64)
+            return bad(IDC_ERR_UNSUPPORTED, "high-order cross sections: FP64 sweeps (the elimination kernel)");
+        if (adjoint || src2)
+            return bad(IDC_ERR_UNSUPPORTED, "high-order cross sections: forward sweeps with one source only");
+        if (phi_scatter) return sweep_tensor_source(src, out, dt, phi, precision, phi_scatter, scatter_scale);
+    }
     if (reflect_mask && !in_reflect_)
         return sweep_reflecting(src, out, dt, phi, precision, phi_scatter, scatter_scale, adjoint, src2);
     IDC_TRY(build_schedule(precision));
@@ -689,6 +773,7 @@ Status Context::sweep(const double *src, double *out, double dt, double *phi, in
     a.out = out;
     a.sigma_t = d_sigma_t;
     a.sigma_s = d_sigma_s;
+    a.sigma_t_mat = high_order_sigma() ? d_cat_t_ : nullptr;
     a.phi_scatter = phi_scatter;
     a.scatter_scale = scatter_scale;
     a.phi = phi;
@@ -824,7 +909,10 @@ Status Context::smv(double alpha, double beta, const double *phi, double *psi) {
     if (!have_ordinates) return bad(IDC_ERR_STATE, "smv before idc_set_ordinates");
     if (!have_sigma) return bad(IDC_ERR_STATE, "smv before idc_set_sigma");
     IDC_TRY_CUDA(cudaSetDevice(device));
-    IDC_TRY_CUDA(launch_smv(dims(), alpha, beta, d_sigma_s, phi, psi, stream));
+    if (high_order_sigma())
+        IDC_TRY_CUDA(launch_smv_tensor(dims(), alpha, beta, d_tens_s_, phi, psi, stream));
+    else
+        IDC_TRY_CUDA(launch_smv(dims(), alpha, beta, d_sigma_s, phi, psi, stream));
     launches += 1;
     return Status::ok();
 }
@@ -833,19 +921,22 @@ Status Context::lmv(double alpha, double beta, const double *x, double *y) {
     if (!have_ordinates) return bad(IDC_ERR_STATE, "lmv before idc_set_ordinates");
     if (!have_sigma) return bad(IDC_ERR_STATE, "lmv before idc_set_sigma");
     IDC_TRY_CUDA(cudaSetDevice(device));
-    IDC_TRY_CUDA(launch_lmv(dims(), alpha, beta, d_sigma_t, d_xi, d_eta, x, y, stream));
+    IDC_TRY_CUDA(launch_lmv(dims(), alpha, beta, d_sigma_t, d_xi, d_eta, x, y, stream, 0.0, nullptr, nullptr,
+                            high_order_sigma() ? d_tens_t_ : nullptr));
     launches += 1;
     return Status::ok();
 }
 
 // res = (L - S P) psi given phi = P psi: Lmv(1, 0) then Smv(-1, 1) in one pass over psi, rounded alike
 Status Context::transport_residual(const double *psi, const double *phi, double *res) {
-    IDC_TRY_CUDA(launch_lmv(dims(), 1.0, 0.0, d_sigma_t, d_xi, d_eta, psi, res, stream, -1.0, d_sigma_s, phi));
+    IDC_TRY_CUDA(launch_lmv(dims(), 1.0, 0.0, d_sigma_t, d_xi, d_eta, psi, res, stream, -1.0, d_sigma_s, phi,
+                            high_order_sigma() ? d_tens_t_ : nullptr, high_order_sigma() ? d_tens_s_ : nullptr));
     launches += 1;
     return Status::ok();
 }
 
 Status Context::lmv_transpose(double alpha, double beta, const double *x, double *y) {
+    if (high_order_sigma()) return bad(IDC_ERR_UNSUPPORTED, "the transposed operators with high-order cross sections");
     IDC_TRY_CUDA(cudaSetDevice(device));
     IDC_TRY_CUDA(launch_lmv_transpose(dims(), alpha, beta, d_sigma_t, d_xi, d_eta, d_w, x, y, stream));
     launches += 1;
@@ -853,6 +944,7 @@ Status Context::lmv_transpose(double alpha, double beta, const double *x, double
 }
 
 Status Context::transport_residual_transpose(const double *z, double *y, double *zsum) {
+    if (high_order_sigma()) return bad(IDC_ERR_UNSUPPORTED, "the transposed operators with high-order cross sections");
     if (!d_ones_) {
         std::vector<double> ones((size_t)nq, 1.0);
         IDC_TRY_CUDA(cudaMalloc(&d_ones_, sizeof(double) * nq));

@@ -132,6 +132,14 @@ public:
     double *d_xi = nullptr, *d_eta = nullptr, *d_w = nullptr;
     double *d_sigma_t = nullptr, *d_sigma_s = nullptr;
     bool have_ordinates = false, have_sigma = false;
+    // high-order cross sections (desc.sigma_degree = p): d_sigma_t / d_sigma_s hold the cell averages (the DSA
+    // preconditioner's coefficients); the operators use the tensors T (launch_sigma_tensor) and CalcA's term
+    bool high_order_sigma() const { return desc.sigma_degree > 0; }
+    double *d_sig_mom_ = nullptr;                               // staging of one set of moments
+    double *d_tens_t_ = nullptr, *d_tens_s_ = nullptr, *d_cat_t_ = nullptr;
+    double *d_work_psi_ = nullptr;   // psi-sized array in which a sweep's scattering source is formed
+    Status sweep_tensor_source(const double *src, double *out, double dt, double *phi, int precision,
+                               const double *phi_scatter, double scatter_scale);
 
     // sweep schedule
     SweepTiling tiling;

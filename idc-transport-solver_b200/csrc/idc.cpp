@@ -139,6 +139,7 @@ Status Context::idc_integrate(double *psi, const double *Q, double dt, int64_t s
     if (!(dt > 0) || !std::isfinite(dt)) return bad(IDC_ERR_ARG, "IDC needs a finite positive dt");
     if (steps < 0) return bad(IDC_ERR_ARG, "negative step count");
     if (reflect_mask) return bad(IDC_ERR_UNSUPPORTED, "IDC time stepping with reflecting boundaries");
+    if (high_order_sigma()) return bad(IDC_ERR_UNSUPPORTED, "IDC time stepping with high-order cross sections");
     if (scattering != 0 && scattering != 1) return bad(IDC_ERR_ARG, "scattering must be 0 (explicit) or 1 (implicit)");
     if (!modal_family()) return bad(IDC_ERR_UNSUPPORTED, "IDC needs the modal sweep kernel");
     std::vector<double> t, W;

@@ -43,6 +43,8 @@ struct SweepArgs {
     double *out;               // psi (written); may equal src (in-place sweep).  Warp kernel: null = not stored
     const double *sigma_t;     // (nx+2)(ny+2), piecewise constant
     const double *sigma_s;     // (nx+2)(ny+2) or null: fused isotropic scattering source (elimination kernels)
+    const double *sigma_t_mat; // high-order cross sections (warp kernel, FP64): per cell the N x N term of CalcA,
+                               // dx dy / 4 (2d+1)(2e+1) T(d,e; u,v), added to the cell matrix; null: sigma_t per cell
     const double *phi_scatter; // fused scattering source, or null.  Elimination kernels: phi (scaled by sigma_s
                                // / (4 pi) in the kernel).  Modal forward sweep: the per-cell moments
                                // sigma_s phi / (4 pi) of launch_scatter_moments.  Transposed modal sweep: mu
@@ -161,10 +163,29 @@ cudaError_t launch_pmv(const GridDims &g, double alpha, double beta, const doubl
                        double *phi, cudaStream_t s);
 cudaError_t launch_smv(const GridDims &g, double alpha, double beta, const double *sigma_s, const double *phi,
                        double *psi, cudaStream_t s);
-// y = beta y + alpha L x (+ gamma sigma_s phi_sc / (4 pi) when phi_sc is given: Lmv and Smv in one pass)
+// y = beta y + alpha L x (+ gamma sigma_s phi_sc / (4 pi) when phi_sc is given: Lmv and Smv in one pass).
+// tensor_t / tensor_s (high-order cross sections): the per-cell tensors T of launch_sigma_tensor take the place
+// of sigma_t / sigma_s (the reference's sigma.DG_degree > 0 branches)
 cudaError_t launch_lmv(const GridDims &g, double alpha, double beta, const double *sigma_t, const double *xi,
                        const double *eta, const double *x, double *y, cudaStream_t s, double gamma = 0.0,
-                       const double *sigma_s = nullptr, const double *phi_sc = nullptr);
+                       const double *sigma_s = nullptr, const double *phi_sc = nullptr,
+                       const double *tensor_t = nullptr, const double *tensor_s = nullptr);
+
+// High-order cross sections (the reference's CrossSection with DG_degree = p, objects/RKDG/CrossSection.cpp).
+// tpi[a + P (b + P c)] = integral over [-1, 1] of P_a P_b P_c (Global::TPI, utils/global.cpp:67-110).
+struct TripleProducts {
+    double v[27];
+};
+// Per cell (ghost cells included) from the Legendre moments mom[cell][u][v]: avg[cell] = mom(0, 0) (the cell
+// average), tensor[cell][r][c] = T(d,e; u,v) = sum_{m,n} mom(m,n) TPI(d,u,m) TPI(e,v,n) (CrossSection::
+// ComputeTensor, :141-230), r = e + P d, c = v + P u, and, when cat is given, cat[cell][r][c] =
+// dxdy4 (2d+1)(2e+1) T(d,e; u,v), the cell-matrix term of CalcA (SweepLinearSolveSpec.cpp:298-318).
+cudaError_t launch_sigma_tensor(const GridDims &g, const double *mom, const TripleProducts &tpi, double dxdy4,
+                                double *avg, double *tensor, double *cat, cudaStream_t s);
+// psi(q,i,j,(d,e)) = beta psi + alpha (2d+1)(2e+1)/(16 pi) sum_{u,v} T(d,e; u,v) phi(u,v) on interior cells:
+// TransportOperator::Smv with sigma.DG_degree > 0 (operators/RKDG/TransportOperator.cpp:367-386)
+cudaError_t launch_smv_tensor(const GridDims &g, double alpha, double beta, const double *tensor_s,
+                              const double *phi, double *psi, cudaStream_t s);
 // y = beta y + alpha L^T x on interior cells (+ gamma w_q sigma_s zsum / (4 pi) when zsum = sum_q x_q is given:
 // gamma = -1 gives (L - S P)^T x); ghost cells of x are not read as unknowns, ghost cells of y not written
 cudaError_t launch_lmv_transpose(const GridDims &g, double alpha, double beta, const double *sigma_t, const double *xi,

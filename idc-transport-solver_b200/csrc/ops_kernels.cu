@@ -65,9 +65,12 @@ __global__ void smv_kernel(GridDims g, double alpha, double beta, const double *
 // round it (the IDC residual (L - S P) psi in one pass over psi).
 // (Omega.grad + sigma_t) x at one interior (cell, ordinate): TransportOperator::Lmv, :1215-1480 (piecewise
 // constant sigma), with x's dofs of the cell at x + base and its upwind neighbours' at +-istride, +-plane.
+// With tens (high-order cross sections) the absorption term is 1/4 (2d+1)(2e+1) sum_{u,v} T(d,e; u,v) x(u,v)
+// (TransportOperator::Lmv, :1335-1359) in place of s x(d,e).
 template <int P>
 __device__ __forceinline__ void lmv_point(const GridDims &g, const double *__restrict__ x, size_t base, size_t istride,
-                                          size_t plane, double xi, double eta, double s, double (&x3)[P * P]) {
+                                          size_t plane, double xi, double eta, double s, double (&x3)[P * P],
+                                          const double *__restrict__ tens = nullptr) {
     constexpr int N = P * P;
     const bool xneg = xi <= 0.0, yneg = eta <= 0.0;
     const double *X0 = x + base;
@@ -80,8 +83,21 @@ __device__ __forceinline__ void lmv_point(const GridDims &g, const double *__res
         x1[k] = X1[k];
         x2[k] = X2[k];
     }
+    if (tens) {
 #pragma unroll
-    for (int k = 0; k < N; ++k) x3[k] = s * x0[k];
+        for (int d = 0; d < P; ++d)
+#pragma unroll
+            for (int e = 0; e < P; ++e) {
+                double acc = 0.0;
+#pragma unroll
+                for (int c = 0; c < N; ++c)
+                    acc += 0.25 * double(2 * d + 1) * double(2 * e + 1) * tens[(e + P * d) * N + c] * x0[c];
+                x3[e + P * d] = acc;
+            }
+    } else {
+#pragma unroll
+        for (int k = 0; k < N; ++k) x3[k] = s * x0[k];
+    }
     double cv = xi / g.dx;
 #pragma unroll
     for (int d = 0; d < P; ++d)
@@ -304,7 +320,8 @@ template <int P, typename IDX>
 __global__ void lmv_kernel(GridDims g, double alpha, double beta, const double *__restrict__ sigma_t,
                            const double *__restrict__ xi_a, const double *__restrict__ eta_a,
                            const double *__restrict__ x, double *__restrict__ y, double gamma,
-                           const double *__restrict__ sigma_s, const double *__restrict__ phi_sc) {
+                           const double *__restrict__ sigma_s, const double *__restrict__ phi_sc,
+                           const double *__restrict__ tensor_t, const double *__restrict__ tensor_s) {
     constexpr int N = P * P;
     const size_t plane = (size_t)g.nq * N;
     const size_t istride = (size_t)(g.ny + 2) * plane;
@@ -315,20 +332,93 @@ __global__ void lmv_kernel(GridDims g, double alpha, double beta, const double *
         const int i = 1 + (int)(cell / (IDX)g.ny), j = 1 + (int)(cell - (cell / (IDX)g.ny) * (IDX)g.ny);
         const double xi = xi_a[q], eta = eta_a[q];
         const size_t base = (size_t)i * istride + (size_t)j * plane + (size_t)q * N;
+        const size_t cidx = (size_t)i * (g.ny + 2) + j;
         double x3[N];
-        lmv_point<P>(g, x, base, istride, plane, xi, eta, sigma_t[(size_t)i * (g.ny + 2) + j], x3);
+        lmv_point<P>(g, x, base, istride, plane, xi, eta, tensor_t ? 0.0 : sigma_t[cidx], x3,
+                     tensor_t ? tensor_t + cidx * N * N : nullptr);
         double *Y = y + base;
         if (!phi_sc) {
 #pragma unroll
             for (int k = 0; k < N; ++k) Y[k] = beta == 0.0 ? alpha * x3[k] : beta * Y[k] + alpha * x3[k];
         } else {
-            const size_t cidx = (size_t)i * (g.ny + 2) + j;
-            const double ss = sigma_s[cidx];
+            double sc[N];   // the scattering source of Smv(gamma, 1) at this cell
+            if (tensor_s) {
+                const double *T = tensor_s + cidx * N * N;
+#pragma unroll
+                for (int d = 0; d < P; ++d)
+#pragma unroll
+                    for (int e = 0; e < P; ++e) {
+                        double acc = 0.0;
+#pragma unroll
+                        for (int c = 0; c < N; ++c) acc += T[(e + P * d) * N + c] * phi_sc[cidx * N + c];
+                        sc[e + P * d] = (acc * (double((2 * d + 1) * (2 * e + 1)) / (16.0 * M_PI))) * gamma;
+                    }
+            } else {
+                const double ss = sigma_s[cidx];
+#pragma unroll
+                for (int k = 0; k < N; ++k) sc[k] = (ss * phi_sc[cidx * N + k] / (4.0 * M_PI)) * gamma;
+            }
 #pragma unroll
             for (int k = 0; k < N; ++k) {
                 const double lv = beta == 0.0 ? __dmul_rn(alpha, x3[k]) : beta * Y[k] + alpha * x3[k];
-                Y[k] = __dadd_rn(lv, (ss * phi_sc[cidx * N + k] / (4.0 * M_PI)) * gamma);
+                Y[k] = __dadd_rn(lv, sc[k]);
             }
+        }
+    }
+}
+
+// One thread per cell of the halo-padded grid: see launch_sigma_tensor.
+template <int P>
+__global__ void sigma_tensor_kernel(GridDims g, const double *__restrict__ mom, TripleProducts tpi, double dxdy4,
+                                    double *__restrict__ avg, double *__restrict__ tensor, double *__restrict__ cat) {
+    constexpr int N = P * P;
+    const size_t cells = (size_t)(g.nx + 2) * (g.ny + 2);
+    for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < cells; c += (size_t)gridDim.x * blockDim.x) {
+        const double *m = mom + c * N;
+        avg[c] = m[0];
+#pragma unroll
+        for (int d = 0; d < P; ++d)
+#pragma unroll
+            for (int e = 0; e < P; ++e)
+#pragma unroll
+                for (int u = 0; u < P; ++u)
+#pragma unroll
+                    for (int v = 0; v < P; ++v) {
+                        // ComputeTensor's sum over the moments (mu, nu) in its order, each term (m TPI) TPI
+                        double t = 0.0;
+#pragma unroll
+                        for (int mu = 0; mu < P; ++mu)
+#pragma unroll
+                            for (int nu = 0; nu < P; ++nu)
+                                t += m[nu + P * mu] * tpi.v[d + P * (u + P * mu)] * tpi.v[e + P * (v + P * nu)];
+                        const size_t at = c * N * N + (size_t)(e + P * d) * N + (v + P * u);
+                        tensor[at] = t;
+                        if (cat) cat[at] = dxdy4 * double(2 * d + 1) * double(2 * e + 1) * t;
+                    }
+    }
+}
+
+// One thread per (interior cell, dof (d,e)): the cell's scattering value for (d,e), written to every ordinate.
+template <int P>
+__global__ void smv_tensor_kernel(GridDims g, double alpha, double beta, const double *__restrict__ tensor_s,
+                                  const double *__restrict__ phi, double *__restrict__ psi) {
+    constexpr int N = P * P;
+    const size_t total = (size_t)g.nx * g.ny * N;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const int k = (int)(t % N);
+        const size_t cell = t / N;
+        const int i = 1 + (int)(cell / g.ny), j = 1 + (int)(cell % g.ny);
+        const size_t cidx = (size_t)i * (g.ny + 2) + j;
+        const int d = k / P, e = k - (k / P) * P;
+        const double *T = tensor_s + cidx * N * N + (size_t)k * N;
+        double acc = 0.0;
+#pragma unroll
+        for (int c = 0; c < N; ++c) acc += T[c] * phi[cidx * N + c];
+        const double v = (acc * (double((2 * d + 1) * (2 * e + 1)) / (16.0 * M_PI))) * alpha;
+        double *out = psi + cidx * (size_t)g.nq * N + k;
+        for (int q = 0; q < g.nq; ++q) {
+            double *o = out + (size_t)q * N;
+            *o = beta == 0.0 ? v : beta * *o + v;   // beta = 0: psi is not read
         }
     }
 }
@@ -640,13 +730,13 @@ cudaError_t launch_smv(const GridDims &g, double alpha, double beta, const doubl
 template <int P>
 static void lmv_p(const GridDims &g, size_t n, double alpha, double beta, const double *sigma_t, const double *xi,
                   const double *eta, const double *x, double *y, double gamma, const double *sigma_s,
-                  const double *phi_sc, cudaStream_t s) {
+                  const double *phi_sc, const double *tensor_t, const double *tensor_s, cudaStream_t s) {
     if (n < (size_t)INT32_MAX)
         lmv_kernel<P, int32_t><<<blocks_for(n), kThreads, 0, s>>>(g, alpha, beta, sigma_t, xi, eta, x, y, gamma, sigma_s,
-                                                                   phi_sc);
+                                                                   phi_sc, tensor_t, tensor_s);
     else
         lmv_kernel<P, size_t><<<blocks_for(n), kThreads, 0, s>>>(g, alpha, beta, sigma_t, xi, eta, x, y, gamma, sigma_s,
-                                                                  phi_sc);
+                                                                  phi_sc, tensor_t, tensor_s);
 }
 
 template <int P>
@@ -702,12 +792,36 @@ cudaError_t launch_reflect_ghosts(const GridDims &g, int mask, const double *xi,
 
 cudaError_t launch_lmv(const GridDims &g, double alpha, double beta, const double *sigma_t, const double *xi,
                        const double *eta, const double *x, double *y, cudaStream_t s, double gamma,
-                       const double *sigma_s, const double *phi_sc) {
+                       const double *sigma_s, const double *phi_sc, const double *tensor_t, const double *tensor_s) {
     const size_t n = (size_t)g.nx * g.ny * g.nq;
     switch (g.P) {
-        case 1: lmv_p<1>(g, n, alpha, beta, sigma_t, xi, eta, x, y, gamma, sigma_s, phi_sc, s); break;
-        case 2: lmv_p<2>(g, n, alpha, beta, sigma_t, xi, eta, x, y, gamma, sigma_s, phi_sc, s); break;
-        case 3: lmv_p<3>(g, n, alpha, beta, sigma_t, xi, eta, x, y, gamma, sigma_s, phi_sc, s); break;
+        case 1: lmv_p<1>(g, n, alpha, beta, sigma_t, xi, eta, x, y, gamma, sigma_s, phi_sc, tensor_t, tensor_s, s); break;
+        case 2: lmv_p<2>(g, n, alpha, beta, sigma_t, xi, eta, x, y, gamma, sigma_s, phi_sc, tensor_t, tensor_s, s); break;
+        case 3: lmv_p<3>(g, n, alpha, beta, sigma_t, xi, eta, x, y, gamma, sigma_s, phi_sc, tensor_t, tensor_s, s); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sigma_tensor(const GridDims &g, const double *mom, const TripleProducts &tpi, double dxdy4,
+                                double *avg, double *tensor, double *cat, cudaStream_t s) {
+    const size_t cells = (size_t)(g.nx + 2) * (g.ny + 2);
+    switch (g.P) {
+        case 1: sigma_tensor_kernel<1><<<blocks_for(cells), kThreads, 0, s>>>(g, mom, tpi, dxdy4, avg, tensor, cat); break;
+        case 2: sigma_tensor_kernel<2><<<blocks_for(cells), kThreads, 0, s>>>(g, mom, tpi, dxdy4, avg, tensor, cat); break;
+        case 3: sigma_tensor_kernel<3><<<blocks_for(cells), kThreads, 0, s>>>(g, mom, tpi, dxdy4, avg, tensor, cat); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_smv_tensor(const GridDims &g, double alpha, double beta, const double *tensor_s,
+                              const double *phi, double *psi, cudaStream_t s) {
+    const size_t n = (size_t)g.nx * g.ny * g.P * g.P;
+    switch (g.P) {
+        case 1: smv_tensor_kernel<1><<<blocks_for(n), kThreads, 0, s>>>(g, alpha, beta, tensor_s, phi, psi); break;
+        case 2: smv_tensor_kernel<2><<<blocks_for(n), kThreads, 0, s>>>(g, alpha, beta, tensor_s, phi, psi); break;
+        case 3: smv_tensor_kernel<3><<<blocks_for(n), kThreads, 0, s>>>(g, alpha, beta, tensor_s, phi, psi); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

@@ -258,8 +258,24 @@ __device__ void compute_warp(const SweepArgs &a, const SweepItem &item, const La
                 for (int k = 0; k < N; ++k) src[k] += a.scatter_scale * (sv * cp[2 + k] / (4.0 * M_PI));
             }
             build_cell_rhs<P>(B, src, xup, yup, a.dx, a.dy, xi, eta, xneg, yneg);
-            const double sdiag = (cp[0] + a.inv_dt) * a.dx * a.dy;
-            cell_solve<P, MODE>(x, B, xc, ec, xneg, yneg, sdiag, a.n_refine);
+            if (MODE == 0 && a.sigma_t_mat) {
+                // high-order cross sections: CalcA's tensor branch (SweepLinearSolveSpec.cpp:298-318), the
+                // dx dy / dt diagonal and then the cell's N x N absorption term
+                const int ic = xneg ? a.nx - c : 1 + c;
+                const double *Mt = a.sigma_t_mat + ((size_t)ic * (a.ny + 2) + j) * N * N;
+                double A[N][N];
+                build_cell_matrix<P, double>(A, xc, ec, xneg, yneg, a.dx * a.dy * a.inv_dt);
+#pragma unroll
+                for (int r = 0; r < N; ++r)
+#pragma unroll
+                    for (int cc = 0; cc < N; ++cc) A[r][cc] += __ldg(Mt + r * N + cc);
+#pragma unroll
+                for (int k = 0; k < N; ++k) x[k] = B[k];
+                ge_solve<P, double>(A, x);
+            } else {
+                const double sdiag = (cp[0] + a.inv_dt) * a.dx * a.dy;
+                cell_solve<P, MODE>(x, B, xc, ec, xneg, yneg, sdiag, a.n_refine);
+            }
             if (a.out) {
                 double *dst = a.out + cell;
 #pragma unroll

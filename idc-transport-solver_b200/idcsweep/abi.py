@@ -165,12 +165,14 @@ class SweepContext:
     """One grid on one GPU: the device-side counterpart of SweepOperator<RKDG::OrdinateFlux> plus the
     TransportOperator and SISolver routines that operate on its arrays."""
 
-    def __init__(self, nx: int, ny: int, p: int, ax=0.0, bx=1.0, ay=0.0, by=1.0, device: int = 0):
+    def __init__(self, nx: int, ny: int, p: int, ax=0.0, bx=1.0, ay=0.0, by=1.0, device: int = 0,
+                 sigma_degree: int = 0):
+        """sigma_degree: 0 for one cross-section value per cell, p for (p+1)^2 Legendre moments per cell."""
         lib = load_library()
         self._lib = lib
         self.nx, self.ny, self.p = int(nx), int(ny), int(p)
         self.N = (self.p + 1) ** 2
-        desc = ProblemDesc(self.nx, self.ny, ax, bx, ay, by, self.p, 0, device, 0)
+        desc = ProblemDesc(self.nx, self.ny, ax, bx, ay, by, self.p, int(sigma_degree), device, 0)
         h = C.c_void_p()
         _check(lib.idc_ctx_create(C.byref(desc), C.byref(h)), "idc_ctx_create")
         self._h = h

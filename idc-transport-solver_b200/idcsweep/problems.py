@@ -31,8 +31,8 @@ class Problem:
     eta: np.ndarray
     w: np.ndarray
     quad: np.ndarray
-    sigma_t: np.ndarray          # (nx+2)*(ny+2)
-    sigma_s: np.ndarray          # (nx+2)*(ny+2)
+    sigma_t: np.ndarray          # (nx+2)*(ny+2), times (p+1)^2 Legendre moments when sigma_degree = p
+    sigma_s: np.ndarray          # the same layout as sigma_t
     source: np.ndarray           # psi-shaped angular source (nx+2, ny+2, nq, p+1, p+1)
     ax: float = 0.0
     bx: float = 1.0
@@ -40,6 +40,7 @@ class Problem:
     by: float = 1.0
     dt: float = math.inf
     meta: dict = field(default_factory=dict)
+    sigma_degree: int = 0        # 0: one value per cell; p: the cross sections' Legendre moments [cell][u][v]
 
     @property
     def nq(self):
@@ -192,6 +193,36 @@ def random_problem(nx: int, ny: int, p: int, sn: int, seed: int, dt: float = mat
     return Problem(nx, ny, p, xi, eta, w, qb, np.ascontiguousarray(st.ravel()), np.ascontiguousarray(ss.ravel()),
                    np.ascontiguousarray(src), 0.0, 1.0 * nx / max(nx, ny) * 2.0, 0.0, 1.0 * ny / max(nx, ny) * 2.0,
                    dt, {"kind": "random", "sn": sn, "seed": seed})
+
+
+def smooth_sigma(n: int, p: int, sn: int, seed: int, dt: float = math.inf, c_range=(0.3, 0.8),
+                 inflow: bool = True) -> Problem:
+    """High-order cross sections (sigma_degree = p): smooth positive sigma_t(x, y) = 1.5 + sin/cos modes of random
+    phase (values in [0.4, 2.6]) and sigma_s = c(x, y) sigma_t(x, y) with a smooth scattering ratio in c_range, both
+    projected onto the cells' Legendre moments (ComputeProjection); random angular source and inflow values as
+    random_problem draws them.  Domain [0, 2]^2."""
+    rng = np.random.default_rng(seed)
+    ph = rng.uniform(0.0, 2.0 * np.pi, 4)
+    xi, eta, w, qb = level_symmetric_2d(sn)
+    nq = xi.size
+
+    def st(x, y):
+        return 1.5 + 0.6 * np.sin(2.1 * x + ph[0]) * np.cos(1.7 * y + ph[1]) + 0.5 * np.sin(3.3 * x * y + ph[2])
+
+    def cr(x, y):
+        return c_range[0] + (c_range[1] - c_range[0]) * 0.5 * (1.0 + np.sin(1.3 * x - 2.2 * y + ph[3]))
+
+    mt = project(st, n, n, 0.0, 2.0, 0.0, 2.0, p, limiter=False)
+    ms = project(lambda x, y: cr(x, y) * st(x, y), n, n, 0.0, 2.0, 0.0, 2.0, p, limiter=False)
+    src = rng.uniform(-0.5, 1.0, (n + 2, n + 2, nq, p + 1, p + 1))
+    if not inflow:
+        src[0, :] = 0.0
+        src[-1, :] = 0.0
+        src[:, 0] = 0.0
+        src[:, -1] = 0.0
+    return Problem(n, n, p, xi, eta, w, qb, np.ascontiguousarray(mt.ravel()), np.ascontiguousarray(ms.ravel()),
+                   np.ascontiguousarray(src), 0.0, 2.0, 0.0, 2.0, dt,
+                   {"kind": "smooth-sigma", "sn": sn, "seed": seed}, sigma_degree=p)
 
 
 def detector_window(P: Problem, cells: int = 16, cx: float = 2.0 / 3.0, cy: float = 0.5) -> np.ndarray:

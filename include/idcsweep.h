@@ -57,7 +57,7 @@ typedef struct idc_problem_desc {
     int64_t nx, ny;          /* interior cells in x and y (DomainDecomposition nx(0), nx(1))            */
     double ax, bx, ay, by;   /* domain [ax,bx] x [ay,by]; dx = (bx-ax)/nx, dy = (by-ay)/ny              */
     int64_t dg_degree;       /* DG degree p of psi and phi (Global::DG_degree); 0..2 supported          */
-    int64_t sigma_degree;    /* DG degree of the cross sections; 0 (piecewise constant) supported       */
+    int64_t sigma_degree;    /* DG degree of the cross sections: 0 (piecewise constant) or dg_degree    */
     int32_t device;          /* CUDA device ordinal                                                     */
     int32_t flags;           /* reserved, must be 0                                                     */
 } idc_problem_desc;
@@ -79,9 +79,17 @@ int idc_ctx_destroy(idc_ctx *ctx);
 int idc_set_ordinates(idc_ctx *ctx, int64_t nq, const double *xi, const double *eta, const double *w,
                       const int64_t quad_bounds[5]);
 
-/* Installs piecewise-constant sigma_t and sigma_s on the halo-padded cell grid (loc as above).
- * sigma_s may be NULL (treated as zero).  These are the CrossSection arguments of
- * SweepOperator::Apply and ImplicitSolver::Solve. */
+/* Installs sigma_t and sigma_s on the halo-padded cell grid (loc as above): one value per cell when
+ * sigma_degree = 0, or, when sigma_degree = dg_degree (high-order cross sections), the (p+1)^2 Legendre
+ * moments of each cell, [cell][u][v] as the CrossSection's DensityFunction array holds them.  sigma_s may
+ * be NULL (treated as zero).  These are the CrossSection arguments of SweepOperator::Apply and
+ * ImplicitSolver::Solve.  High-order cross sections enter as the reference's tensor branches do: the cell
+ * matrix of CalcA (linear_solvers/RKDG/SweepCellSolve/SweepLinearSolveSpec.cpp:298-318), Smv and Lmv
+ * (operators/RKDG/TransportOperator.cpp:367-386, :1335-1359), with the tensor of Legendre triple products of
+ * CrossSection::ComputeTensor (objects/RKDG/CrossSection.cpp:141-230).  They run on the elimination kernel in
+ * FP64: sweeps, idc_smv, idc_lmv, source iteration and GMRES (its DSA preconditioner uses the cell averages);
+ * FP32 sweeps, transposed operators, IDC time stepping, batches and reflecting edges return
+ * IDC_ERR_UNSUPPORTED. */
 int idc_set_sigma(idc_ctx *ctx, const double *sigma_t, const double *sigma_s, int loc);
 
 /* Tile shape of the persistent sweep kernel: G ordinates x R rows per thread block (0 = automatic).

@@ -154,6 +154,8 @@ class Reference:
                                    C.c_double, C.c_int64]
         lib.ref_create_reflecting.restype = C.c_void_p
         lib.ref_create_reflecting.argtypes = lib.ref_create.argtypes + [C.c_int]
+        lib.ref_create_ex.restype = C.c_void_p
+        lib.ref_create_ex.argtypes = lib.ref_create.argtypes + [C.c_int, C.c_int]
         lib.ref_destroy.argtypes = [C.c_void_p]
         lib.ref_apply.argtypes = [C.c_void_p, _dp, C.c_double, _dp]
         lib.ref_apply_timed.argtypes = [C.c_void_p, _dp, C.c_double, C.c_int64, _dp]
@@ -171,12 +173,13 @@ class Reference:
         self.lib = lib
 
     def open(self, P: Problem, dt: float = np.inf, pattern: str = "wavefront", abs_tol=1e-10, max_its=500,
-             reflect: int = 0):
+             reflect: int = 0, sigma_degree: int = 0):
         """reflect: the reflecting edges as the reference's BoundaryEdge bits (X_Min 1, X_Max 2, Y_Min 4,
-        Y_Max 8); with any, the reference sweeps the quadrants in sequence and reflects between them."""
+        Y_Max 8); with any, the reference sweeps the quadrants in sequence and reflects between them.
+        sigma_degree: 0, or p when P.sigma_t / P.sigma_s hold (p+1)^2 Legendre moments per cell."""
         keep = [np.ascontiguousarray(a, np.float64) for a in (P.xi, P.eta, P.w, P.sigma_t, P.sigma_s)]
-        h = self.lib.ref_create_reflecting(P.nx, P.ny, P.ax, P.bx, P.ay, P.by, P.p, P.nq, *[_p(a) for a in keep],
-                                           dt, pattern.encode(), abs_tol, max_its, int(reflect))
+        h = self.lib.ref_create_ex(P.nx, P.ny, P.ax, P.bx, P.ay, P.by, P.p, P.nq, *[_p(a) for a in keep],
+                                   dt, pattern.encode(), abs_tol, max_its, int(reflect), int(sigma_degree))
         if not h:
             raise RuntimeError("ref_create failed")
         return _RefHandle(self.lib, h, P, keep)

@@ -46,6 +46,7 @@ int64_t next_order_key = 1000000;
 
 struct RefProblem {
     int reflect = 0;   // BoundaryEdge bits of the reflecting edges (Global::reflecting_boundaries while in use)
+    int sigma_degree = 0;   // DG degree of the cross sections: 0 (piecewise constant) or p
     int64_t nx, ny, p, N, nq;
     int64_t order_key;
     ParameterList plist;
@@ -59,7 +60,9 @@ struct RefProblem {
 
     size_t psi_len() const { return (size_t)(nx + 2) * (ny + 2) * nq * N; }
     size_t phi_len() const { return (size_t)(nx + 2) * (ny + 2) * N; }
-    size_t sig_len() const { return (size_t)(nx + 2) * (ny + 2); }
+    size_t sig_len() const {   // values per cross section: one per cell, or (p+1)^2 Legendre moments
+        return (size_t)(nx + 2) * (ny + 2) * (sigma_degree ? N : 1);
+    }
 };
 
 // Installs (xi, eta, w) in the reference's ordinate cache under a fresh key and returns that key.
@@ -123,14 +126,20 @@ extern "C" {
 // (index j + (ny+2)*i), time step dt (+inf for steady state).  sweep_pattern is the reference's key
 // ("wavefront" or "sequential").  Returns an opaque handle, or nullptr on error.
 //------------------------------------------------------------------------------------------------------------
-void * ref_create_reflecting ( int64_t nx, int64_t ny, double ax, double bx, double ay, double by, int64_t p,
-                               int64_t nq, const double * xi, const double * eta, const double * w,
-                               const double * sigma_t, const double * sigma_s, double dt,
-                               const char * sweep_pattern, double si_abs_tol, int64_t si_max_its, int reflect ) {
+// reflect: BoundaryEdge bits of reflecting edges; sigma_degree: 0, or p for high-order cross sections given as
+// (p+1)^2 Legendre moments per cell ([cell][u][v], the DensityFunction layout), as Init configures them when the
+// deck does not ask for piecewise-constant cross sections (utils/init.cpp:740-745).
+void * ref_create_ex ( int64_t nx, int64_t ny, double ax, double bx, double ay, double by, int64_t p,
+                       int64_t nq, const double * xi, const double * eta, const double * w,
+                       const double * sigma_t, const double * sigma_s, double dt,
+                       const char * sweep_pattern, double si_abs_tol, int64_t si_max_its, int reflect,
+                       int sigma_degree ) {
     try {
+        if ( sigma_degree != 0 && sigma_degree != p ) throw std::runtime_error( "sigma_degree must be 0 or p" );
         ReflectScope scope( reflect );   // SweepPatternUniCart decides on sequential quadrants when built
         auto * P = new RefProblem();
         P->reflect = reflect;
+        P->sigma_degree = sigma_degree;
         P->nx = nx; P->ny = ny; P->p = p; P->N = (p + 1) * (p + 1); P->nq = nq; P->dt = dt;
 
         Global::DG_degree = p;
@@ -158,8 +167,8 @@ void * ref_create_reflecting ( int64_t nx, int64_t ny, double ax, double bx, dou
         // default-construct + Reconfigure, the way Init builds them (utils/init.cpp:741-750)
         P->sigma_t.reset( new RKDG::CrossSection() );
         P->sigma_s.reset( new RKDG::CrossSection() );
-        P->sigma_t->Reconfigure( *P->dd, 0 );
-        P->sigma_s->Reconfigure( *P->dd, 0 );
+        P->sigma_t->Reconfigure( *P->dd, sigma_degree );
+        P->sigma_s->Reconfigure( *P->dd, sigma_degree );
         CopyIn( *P->sigma_t, sigma_t, P->sig_len() );
         CopyIn( *P->sigma_s, sigma_s, P->sig_len() );
         P->sigma_t->ComputeTensor();
@@ -183,6 +192,15 @@ void * ref_create_reflecting ( int64_t nx, int64_t ny, double ax, double bx, dou
         std::fprintf( stderr, "ref_create: %s\n", e.what() );
         return nullptr;
     }
+}
+
+// Piecewise-constant cross sections.
+void * ref_create_reflecting ( int64_t nx, int64_t ny, double ax, double bx, double ay, double by, int64_t p,
+                               int64_t nq, const double * xi, const double * eta, const double * w,
+                               const double * sigma_t, const double * sigma_s, double dt,
+                               const char * sweep_pattern, double si_abs_tol, int64_t si_max_its, int reflect ) {
+    return ref_create_ex( nx, ny, ax, bx, ay, by, p, nq, xi, eta, w, sigma_t, sigma_s, dt, sweep_pattern,
+                          si_abs_tol, si_max_its, reflect, 0 );
 }
 
 // The same without reflecting boundaries (vacuum or given inflow on every edge).

@@ -54,10 +54,20 @@ class SweepOperator<OrdinateFlux>::SweepPatternGPU : public SweepOperator<Ordina
 
 protected:
 
-    // The context is created once per SweepOperator: the grid and the ordinate set are fixed for its life.
+    // The grid and the ordinate set are fixed for the SweepOperator's life.  The context is made here for
+    // piecewise-constant cross sections (so a missing GPU fails the pattern's construction, as the reference
+    // reports errors) and made again at a sweep whose cross sections have the flux's DG degree.
     SweepPatternGPU ( const SweepOperator<OrdinateFlux> & op, const ParameterList & input_list )
         : SweepPatternUniCart( op, input_list ) {
 
+        make_context( 0 );
+    }
+
+    void make_context ( int64_t sigma_degree ) const {
+
+        if ( this->ctx ) idc_ctx_destroy( this->ctx );
+        this->ctx = nullptr;
+        const SweepOperator<OrdinateFlux> & op = this->sw_op;
         idc_problem_desc d {};
         d.nx = op.nx(0);
         d.ny = op.nx(1);
@@ -66,10 +76,11 @@ protected:
         d.ay = op.ax(1);
         d.by = op.bx(1);
         d.dg_degree = Global::DG_degree;
-        d.sigma_degree = 0;
+        d.sigma_degree = sigma_degree;
         d.device = 0;
         d.flags = 0;
         idc_check( idc_ctx_create( &d, &this->ctx ), "idc_ctx_create" );
+        this->ctx_sigma_degree = sigma_degree;
 
         const int64_t nq = op.nq();
         std::vector<double> xi( nq ), eta( nq ), w( nq );
@@ -85,7 +96,7 @@ protected:
 
 public:
 
-    ~SweepPatternGPU ( void ) override {  idc_ctx_destroy( this->ctx );  }
+    ~SweepPatternGPU ( void ) override {  if ( this->ctx ) idc_ctx_destroy( this->ctx );  }
 
     static const std::string Descriptor ( void ) {  return "gpu-wavefront";  }
     const std::string GetDescriptor ( void ) const override {  return Descriptor();  }
@@ -93,6 +104,8 @@ public:
     // SweepPattern::Sweep: result <- L^{-1} source with the inflow values in the ghost cells of `source`.
     void Sweep ( const OrdinateFlux & source, OrdinateFlux & result, const RKDG::CrossSection & sigma,
                  const RKDG::OrdinateFlux * const /* initial_condition: not used by a direct sweep */ ) const override {
+
+        if ( !this->ctx || this->ctx_sigma_degree != sigma.DG_degree ) make_context( sigma.DG_degree );
 
         // reflecting boundaries (SweepPatternUniCart.cpp:46-88): the library sweeps the quadrants in the same
         // sequence and reflects between them; the BoundaryEdge bits are the ABI's IDC_EDGE_* bits
@@ -111,7 +124,8 @@ public:
 
 private:
 
-    idc_ctx * ctx = nullptr;
+    mutable idc_ctx * ctx = nullptr;
+    mutable int64_t ctx_sigma_degree = -1;
 };
 
 

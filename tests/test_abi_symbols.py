@@ -47,8 +47,8 @@ def test_descriptor_validation_before_device():
     assert lib.idc_ctx_create(C.byref(bad), C.byref(h)) == abi.IDC_ERR_ARG
     p3 = abi.ProblemDesc(4, 4, 0.0, 1.0, 0.0, 1.0, 3, 0, 0, 0)
     assert lib.idc_ctx_create(C.byref(p3), C.byref(h)) == abi.IDC_ERR_UNSUPPORTED
-    hi = abi.ProblemDesc(4, 4, 0.0, 1.0, 0.0, 1.0, 1, 1, 0, 0)
-    assert lib.idc_ctx_create(C.byref(hi), C.byref(h)) == abi.IDC_ERR_UNSUPPORTED
+    hi = abi.ProblemDesc(4, 4, 0.0, 1.0, 0.0, 1.0, 1, 2, 0, 0)   # cross sections: degree 0 or the DG degree
+    assert lib.idc_ctx_create(C.byref(hi), C.byref(h)) == abi.IDC_ERR_ARG
     empty = abi.ProblemDesc(4, 4, 1.0, 1.0, 0.0, 1.0, 1, 0, 0, 0)
     assert lib.idc_ctx_create(C.byref(empty), C.byref(h)) == abi.IDC_ERR_ARG
 

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from conftest import gpu_available, rel_err, to_oracle
-from idcsweep.problems import lattice, lognormal, random_problem
+from idcsweep.problems import lattice, lognormal, random_problem, smooth_sigma
 from oracle.bindings import REFERENCE_GPU_SO, Reference
 
 pytestmark = pytest.mark.skipif(not os.path.exists(REFERENCE_GPU_SO),
@@ -78,6 +78,20 @@ def test_reference_source_iteration_with_reflecting_edges_through_plugin(plugged
     out = {}
     for pattern in ("wavefront", "gpu-wavefront"):
         with plugged.open(to_oracle(P), P.dt, pattern=pattern, abs_tol=1e-12, max_its=5000, reflect=edges) as h:
+            psi = h.source_iteration(P.source, P.dt)
+            out[pattern] = h.pmv(psi)
+    assert rel_err(out["gpu-wavefront"], out["wavefront"]) < 1e-11
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("p", [1, 2])
+def test_reference_source_iteration_with_high_order_cross_sections_through_plugin(plugged, p):
+    """The reference's SISolver::Solve with CrossSection objects of DG degree p: gpu-wavefront (which makes its
+    context with the cross sections' degree) against wavefront."""
+    P = smooth_sigma(12, p, 4, seed=11 + p, dt=0.4)
+    out = {}
+    for pattern in ("wavefront", "gpu-wavefront"):
+        with plugged.open(to_oracle(P), P.dt, pattern=pattern, abs_tol=1e-12, max_its=5000, sigma_degree=p) as h:
             psi = h.source_iteration(P.source, P.dt)
             out[pattern] = h.pmv(psi)
     assert rel_err(out["gpu-wavefront"], out["wavefront"]) < 1e-11
