@@ -679,6 +679,15 @@ int idc_set_spin_limit(idc_ctx *ctx, int64_t polls) {
     ABI_GUARD_END
 }
 
+int idc_set_periodic(idc_ctx *ctx, int32_t periodic) {
+    ABI_GUARD_BEGIN
+    if (!ctx) return fail(IDC_ERR_ARG, "null context");
+    if (periodic != 0 && periodic != 1) return fail(IDC_ERR_ARG, "idc_set_periodic: 0 or 1");
+    ABI_TRY(ctx->impl.set_periodic(periodic == 1));
+    return IDC_OK;
+    ABI_GUARD_END
+}
+
 int idc_set_reflecting(idc_ctx *ctx, int32_t edges) {
     ABI_GUARD_BEGIN
     if (!ctx) return fail(IDC_ERR_ARG, "null context");

@@ -80,6 +80,7 @@ Status Batch::add(Context *c) {
     if (!c->modal_family()) return bad(IDC_ERR_UNSUPPORTED, "batched sweeps need the modal kernel");
     if (c->reflect_mask) return bad(IDC_ERR_UNSUPPORTED, "batched sweeps with reflecting boundaries");
     if (c->high_order_sigma()) return bad(IDC_ERR_UNSUPPORTED, "batched sweeps with high-order cross sections");
+    if (c->periodic_) return bad(IDC_ERR_UNSUPPORTED, "batched solves on a periodic grid");
     if (!members.empty() && c->device != members[0]->device) return bad(IDC_ERR_ARG, "batch members on different GPUs");
     members.push_back(c);
     release();

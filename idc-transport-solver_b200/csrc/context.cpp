@@ -196,6 +196,7 @@ Status Context::update_reflect_map() {
 
 Status Context::set_reflecting(int mask) {
     if (mask < 0 || mask > 15) return bad(IDC_ERR_ARG, "reflecting edges: bits 1 x-min, 2 x-max, 4 y-min, 8 y-max");
+    if (mask && periodic_) return bad(IDC_ERR_UNSUPPORTED, "reflecting edges on a periodic grid");
     IDC_TRY_CUDA(cudaSetDevice(device));
     const int old = reflect_mask;
     reflect_mask = mask;
@@ -294,8 +295,46 @@ Status Context::reflect_quadrants(double *w, double dt, double *phi, int precisi
 }
 
 Status Context::reflect_ghosts(double *psi, double *packed, bool to_packed) {
-    IDC_TRY_CUDA(launch_reflect_ghosts(dims(), reflect_mask, d_xi, d_eta, psi, packed, to_packed, stream));
+    IDC_TRY_CUDA(launch_reflect_ghosts(dims(), ghost_mask(), d_xi, d_eta, psi, packed, to_packed, stream));
     launches += 1;
+    return Status::ok();
+}
+
+Status Context::set_periodic(bool on) {
+    if (on && reflect_mask) return bad(IDC_ERR_UNSUPPORTED, "reflecting edges on a periodic grid");
+    periodic_ = on;
+    return Status::ok();
+}
+
+// SISolver::Solve with Global::periodic: psi starts at zero, and each iteration first synchronises the halos
+// that the last sweep left dirty (SISolver.cpp:223; SynchronizeHalos copies the opposite interior edge into
+// every ghost cell of the four edges, objects/Abstract/DensityFunction.cpp:927-960), then copies the source
+// with OpDomain::Interior | OpDomain::Boundary, which on a periodic grid is the interior alone
+// (DomainDecomposition::DetermineOffsets, objects/DomainDecomposition.cpp:271-330).  The sweep then reads the
+// last iterate's periodic images as its inflow.
+Status Context::source_iteration_periodic(const double *src, double *psi_out, double dt, double abs_tol,
+                                          int64_t max_its, int precision, int64_t *iters, double *err) {
+    if (src == psi_out) return bad(IDC_ERR_ARG, "source iteration: source and psi must be different arrays");
+    IDC_TRY(ensure_phi_buffers(2));
+    double *phi_cur = phi_buf(0), *phi_last = phi_buf(1);
+    IDC_TRY_CUDA(cudaMemsetAsync(phi_cur, 0, sizeof(double) * phi_len(), stream));
+    IDC_TRY_CUDA(cudaMemsetAsync(phi_last, 0, sizeof(double) * phi_len(), stream));
+    IDC_TRY_CUDA(cudaMemsetAsync(psi_out, 0, sizeof(double) * psi_len(), stream));
+    int64_t it = 0;
+    double e = INFINITY;
+    while (it < max_its && e > abs_tol) {
+        ++it;
+        std::swap(phi_cur, phi_last);
+        if (it > 1) IDC_TRY_CUDA(launch_periodic_halos(dims(), psi_out, stream));
+        IDC_TRY_CUDA(launch_copy_interior(dims(), src, psi_out, stream));
+        launches += it > 1 ? 2 : 1;
+        IDC_TRY(smv(1.0, 1.0, phi_last, psi_out));
+        IDC_TRY(sweep(psi_out, psi_out, dt, phi_cur, precision));
+        IDC_TRY(l2dist(phi_cur, phi_last, &e));
+        IDC_TRY(check_device_error());
+    }
+    if (iters) *iters = it;
+    if (err) *err = e;
     return Status::ok();
 }
 
@@ -921,6 +960,17 @@ Status Context::lmv(double alpha, double beta, const double *x, double *y) {
     if (!have_ordinates) return bad(IDC_ERR_STATE, "lmv before idc_set_ordinates");
     if (!have_sigma) return bad(IDC_ERR_STATE, "lmv before idc_set_sigma");
     IDC_TRY_CUDA(cudaSetDevice(device));
+    if (periodic_) {   // the upwind neighbours across an edge are the opposite edge's cells (Lmv synchronises
+                       // its input's halos first, TransportOperator.cpp:1232): a copy of x with its halos synced
+        if (!d_work_psi_) {
+            if (capturing) return bad(IDC_ERR_STATE, "work array allocation inside a stream capture");
+            IDC_TRY_CUDA(cudaMalloc(&d_work_psi_, sizeof(double) * psi_len()));
+        }
+        IDC_TRY_CUDA(cudaMemcpyAsync(d_work_psi_, x, sizeof(double) * psi_len(), cudaMemcpyDeviceToDevice, stream));
+        IDC_TRY_CUDA(launch_periodic_halos(dims(), d_work_psi_, stream));
+        launches += 1;
+        x = d_work_psi_;
+    }
     IDC_TRY_CUDA(launch_lmv(dims(), alpha, beta, d_sigma_t, d_xi, d_eta, x, y, stream, 0.0, nullptr, nullptr,
                             high_order_sigma() ? d_tens_t_ : nullptr));
     launches += 1;
@@ -936,6 +986,7 @@ Status Context::transport_residual(const double *psi, const double *phi, double 
 }
 
 Status Context::lmv_transpose(double alpha, double beta, const double *x, double *y) {
+    if (periodic_ || reflect_mask) return bad(IDC_ERR_UNSUPPORTED, "the transposed operators with periodic or reflecting edges");
     if (high_order_sigma()) return bad(IDC_ERR_UNSUPPORTED, "the transposed operators with high-order cross sections");
     IDC_TRY_CUDA(cudaSetDevice(device));
     IDC_TRY_CUDA(launch_lmv_transpose(dims(), alpha, beta, d_sigma_t, d_xi, d_eta, d_w, x, y, stream));
@@ -973,6 +1024,7 @@ Status Context::l2dist(const double *a, const double *b, double *out_host) {
 Status Context::source_iteration(const double *src, double *psi_out, double dt, double abs_tol, int64_t max_its,
                                  int precision, int64_t *iters, double *err) {
     if (reflect_mask) return source_iteration_reflecting(src, psi_out, dt, abs_tol, max_its, precision, iters, err);
+    if (periodic_) return source_iteration_periodic(src, psi_out, dt, abs_tol, max_its, precision, iters, err);
     IDC_TRY(ensure_phi_buffers(2));
     double *phi_cur = phi_buf(0), *phi_last = phi_buf(1);
     IDC_TRY_CUDA(cudaMemsetAsync(phi_cur, 0, sizeof(double) * phi_len(), stream));

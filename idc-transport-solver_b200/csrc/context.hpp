@@ -206,9 +206,18 @@ public:
     Status reflect_ghosts(double *psi, double *packed, bool to_packed);
     Status source_iteration_reflecting(const double *src, double *psi_out, double dt, double abs_tol,
                                        int64_t max_its, int precision, int64_t *iters, double *err);
-    Status apply_peierls_reflecting(const double *x, double *y, double *tmp, double dt, int precision);
-    Status gmres_peierls_reflecting(const double *src, double *psi_out, double dt, double abs_tol, int restart,
-                                    int64_t max_its, int precision, int64_t *iters, double *resid);
+    // periodic boundaries (idc_set_periodic, the reference's Global::periodic): the sweep reads the ghost
+    // cells as given; source iteration and GMRES carry them from the opposite edges between sweeps
+    bool periodic_ = false;
+    Status set_periodic(bool on);
+    Status source_iteration_periodic(const double *src, double *psi_out, double dt, double abs_tol,
+                                     int64_t max_its, int precision, int64_t *iters, double *err);
+    // edges whose ghost values the solvers carry: the reflecting ones, or all four when periodic
+    int ghost_mask() const { return periodic_ ? 15 : reflect_mask; }
+    Status boundary_sweep(double *w, double dt, double *phi, int precision);
+    Status apply_peierls_boundary(const double *x, double *y, double *tmp, double dt, int precision);
+    Status gmres_peierls_boundary(const double *src, double *psi_out, double dt, double abs_tol, int restart,
+                                  int64_t max_its, int precision, int64_t *iters, double *resid);
 
     double *d_krylov = nullptr;    // GMRES basis, (restart + 1) phi-sized vectors (+ restart for flexible GMRES)
     int precond_kind = 0;          // 0 none, 1 DSA (right preconditioner of the forward Peierls GMRES)

@@ -140,6 +140,7 @@ Status Context::idc_integrate(double *psi, const double *Q, double dt, int64_t s
     if (steps < 0) return bad(IDC_ERR_ARG, "negative step count");
     if (reflect_mask) return bad(IDC_ERR_UNSUPPORTED, "IDC time stepping with reflecting boundaries");
     if (high_order_sigma()) return bad(IDC_ERR_UNSUPPORTED, "IDC time stepping with high-order cross sections");
+    if (periodic_) return bad(IDC_ERR_UNSUPPORTED, "IDC time stepping on a periodic grid");
     if (scattering != 0 && scattering != 1) return bad(IDC_ERR_ARG, "scattering must be 0 (explicit) or 1 (implicit)");
     if (!modal_family()) return bad(IDC_ERR_UNSUPPORTED, "IDC needs the modal sweep kernel");
     std::vector<double> t, W;

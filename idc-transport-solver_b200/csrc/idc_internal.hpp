@@ -201,6 +201,12 @@ cudaError_t launch_weighted_broadcast(const GridDims &g, const double *w, const 
 // (x) or (-1)^e (y)
 cudaError_t launch_reflect_boundaries(const GridDims &g, int mask, const double *xi, const double *eta,
                                       const int *rmap, double *psi, cudaStream_t s);
+// Periodic boundaries (DensityFunction::SynchronizeHalos with Global::periodic, objects/Abstract/
+// DensityFunction.cpp:927-960): every value of the edge cells' ghosts from the opposite interior edge,
+// (0, j) <- (nx, j), (nx+1, j) <- (1, j), (i, 0) <- (i, ny), (i, ny+1) <- (i, 1); corner cells untouched.
+cudaError_t launch_periodic_halos(const GridDims &g, double *psi, cudaStream_t s);
+// dst <- src on interior cells only (Copy over OpDomain::Interior); ghost cells of dst untouched
+cudaError_t launch_copy_interior(const GridDims &g, const double *src, double *dst, cudaStream_t s);
 // The ghost values of the reflecting edges' entering ordinates, packed edge after edge (x-min, x-max, y-min, y-max
 // of `mask`), each edge [cell][q][dof]; the entries of ordinates leaving through an edge are 0 in the pack.
 // to_packed: packed <- ghosts; else ghosts <- packed (0 for leaving ordinates, and for all when packed is null).

@@ -285,6 +285,39 @@ __global__ void reflect_kernel(GridDims g, int mask, const double *__restrict__ 
     }
 }
 
+// One thread per (edge cell, value of the cell): see launch_periodic_halos.
+__global__ void periodic_halos_kernel(GridDims g, double *__restrict__ psi) {
+    const size_t per = (size_t)g.nq * g.P * g.P;   // values of a cell: every ordinate's dofs
+    const size_t nxe = (size_t)g.ny * per, nye = (size_t)g.nx * per;
+    const size_t total = nxe + nye;
+    const size_t istride = (size_t)(g.ny + 2) * per;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        if (t < nye) {   // the y edges of column i: (i, 0) <- (i, ny), (i, ny + 1) <- (i, 1)
+            const size_t i = 1 + t / per, l = t % per;
+            double *col = psi + i * istride + l;
+            col[0] = col[(size_t)g.ny * per];
+            col[(size_t)(g.ny + 1) * per] = col[per];
+        } else {         // the x edges of row j: (0, j) <- (nx, j), (nx + 1, j) <- (1, j)
+            const size_t r = t - nye, j = 1 + r / per, l = r % per;
+            double *row = psi + j * per + l;
+            row[0] = row[(size_t)g.nx * istride];
+            row[(size_t)(g.nx + 1) * istride] = row[istride];
+        }
+    }
+}
+
+// One thread per interior value: see launch_copy_interior.
+__global__ void copy_interior_kernel(GridDims g, const double *__restrict__ src, double *__restrict__ dst) {
+    const size_t per = (size_t)g.nq * g.P * g.P;
+    const size_t total = (size_t)g.nx * g.ny * per;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const size_t cell = t / per, l = t % per;
+        const size_t i = 1 + cell / g.ny, j = 1 + cell % g.ny;
+        const size_t at = (i * (g.ny + 2) + j) * per + l;
+        dst[at] = src[at];
+    }
+}
+
 // One thread per (edge cell, ordinate, dof) of the reflecting edges, packed edge after edge (x-min, x-max, y-min,
 // y-max; absent edges take no room): see launch_reflect_ghosts.
 __global__ void reflect_ghosts_kernel(GridDims g, int mask, const double *__restrict__ xi,
@@ -774,6 +807,18 @@ cudaError_t launch_reflect_boundaries(const GridDims &g, int mask, const double 
                                       const int *rmap, double *psi, cudaStream_t s) {
     const size_t total = 2 * (size_t)(g.nx + g.ny) * g.nq * g.P * g.P;
     reflect_kernel<<<blocks_for(total), kThreads, 0, s>>>(g, mask, xi, eta, rmap, psi);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_periodic_halos(const GridDims &g, double *psi, cudaStream_t s) {
+    const size_t total = (size_t)(g.nx + g.ny) * g.nq * g.P * g.P;
+    periodic_halos_kernel<<<blocks_for(total), kThreads, 0, s>>>(g, psi);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_copy_interior(const GridDims &g, const double *src, double *dst, cudaStream_t s) {
+    const size_t total = (size_t)g.nx * g.ny * g.nq * g.P * g.P;
+    copy_interior_kernel<<<blocks_for(total), kThreads, 0, s>>>(g, src, dst);
     return cudaGetLastError();
 }
 

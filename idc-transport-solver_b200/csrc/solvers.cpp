@@ -191,43 +191,54 @@ Status Context::gmres(Op apply, const double *b, double *x, double abs_tol, int 
     return Status::ok();
 }
 
-// The Peierls operator with reflecting edges, on x = [phi; g], g the reflecting edges' ghost values at the start
-// of a sweep (packed as launch_reflect_ghosts packs them): the sequential-quadrant sweep of the scattering
-// source S phi with vacuum inflow on the other edges and g on the reflecting ones, y = x - [P psi; g(psi)], g(psi)
-// the ghost values that the sweep leaves.  Source iteration with reflecting edges is the fixed-point iteration
-// of exactly this map (the reflections of one sweep are the next sweep's inflow), so GMRES on it reaches the
-// source-iteration fixed point for every set of reflecting edges.  The reference's Peierls operator
-// (PETScPeierlsSolver.cpp:529-572) starts every sweep from zero ghost cells instead (Smv over OpDomain::All of
-// a scalar flux unpacked with zero halos): the same solution where the quadrant order reaches every reflection
-// partner before it is read (x-min and y-min edges), a different one elsewhere.
-Status Context::apply_peierls_reflecting(const double *x, double *y, double *tmp, double dt, int precision) {
-    const size_t np = phi_len(), n = np + reflect_ghost_len(dims(), reflect_mask);
-    double *w = d_reflect_;
-    IDC_TRY_CUDA(cudaMemsetAsync(w, 0, sizeof(double) * psi_len(), stream));
-    IDC_TRY(reflect_ghosts(w, const_cast<double *>(x) + np, false));
-    IDC_TRY_CUDA(launch_smv(dims(), 1.0, 1.0, d_sigma_s, x, w, stream));
-    IDC_TRY(reflect_quadrants(w, dt, tmp, precision));
-    IDC_TRY(reflect_ghosts(w, tmp + np, true));
-    IDC_TRY_CUDA(launch_axpby(1.0, x, 0.0, y, n, stream));
-    IDC_TRY_CUDA(launch_axpby(-1.0, tmp, 1.0, y, n, stream));
-    launches += 3;
+// The sweep of a prepared array w in place with the boundary treatment of source iteration: with reflecting
+// edges the quadrants in sequence with the reflections between them (the reflections of the last quadrant are
+// the ghost values it leaves); on a periodic grid one sweep, then the halos synchronised from the opposite edges.
+Status Context::boundary_sweep(double *w, double dt, double *phi, int precision) {
+    if (reflect_mask) return reflect_quadrants(w, dt, phi, precision);
+    IDC_TRY(sweep(w, w, dt, phi, precision));
+    IDC_TRY_CUDA(launch_periodic_halos(dims(), w, stream));
+    launches += 1;
     return Status::ok();
 }
 
-// GMRES on (I - K) [phi; g] = b with K the map above and b the sweep of Q (its own inflow on the other edges,
-// zero reflecting ghost values); then psi is the sweep of Q + S phi with g in the reflecting ghost cells.
-Status Context::gmres_peierls_reflecting(const double *src, double *psi_out, double dt, double abs_tol, int restart,
-                                         int64_t max_its, int precision, int64_t *iters_out, double *resid_out) {
+// The Peierls operator with reflecting or periodic edges, on x = [phi; g], g the ghost values of those edges'
+// entering ordinates at the start of a sweep (packed as launch_reflect_ghosts packs them): the boundary sweep
+// of the scattering source S phi with vacuum inflow on the other edges and g on these, y = x - [P psi; g(psi)],
+// g(psi) the ghost values that the sweep leaves.  Source iteration with such edges is the fixed-point iteration
+// of exactly this map (the ghost values left by one sweep are the next sweep's inflow), so GMRES on it reaches
+// the source-iteration fixed point.  The reference's Peierls operator (PETScPeierlsSolver.cpp:529-572) starts
+// every sweep from zero ghost cells instead (Smv over OpDomain::All of a scalar flux unpacked with zero halos):
+// the same solution only where one sweep needs no ghost value from the sweep before (reflecting x-min and y-min
+// edges), a different one elsewhere (other reflecting edges, periodic grids).
+Status Context::apply_peierls_boundary(const double *x, double *y, double *tmp, double dt, int precision) {
+    const size_t np = phi_len(), n = np + reflect_ghost_len(dims(), ghost_mask());
+    double *w = d_reflect_;
+    IDC_TRY_CUDA(cudaMemsetAsync(w, 0, sizeof(double) * psi_len(), stream));
+    IDC_TRY(reflect_ghosts(w, const_cast<double *>(x) + np, false));
+    IDC_TRY(smv(1.0, 1.0, x, w));
+    IDC_TRY(boundary_sweep(w, dt, tmp, precision));
+    IDC_TRY(reflect_ghosts(w, tmp + np, true));
+    IDC_TRY_CUDA(launch_axpby(1.0, x, 0.0, y, n, stream));
+    IDC_TRY_CUDA(launch_axpby(-1.0, tmp, 1.0, y, n, stream));
+    launches += 2;
+    return Status::ok();
+}
+
+// GMRES on (I - K) [phi; g] = b with K the map above and b the boundary sweep of Q (its own inflow on the other
+// edges, zero ghost values on these); then psi is the boundary sweep of Q + S phi with g in those ghost cells.
+Status Context::gmres_peierls_boundary(const double *src, double *psi_out, double dt, double abs_tol, int restart,
+                                       int64_t max_its, int precision, int64_t *iters_out, double *resid_out) {
     if (precision == IDC_PREC_FP32_IR)
-        return bad(IDC_ERR_UNSUPPORTED, "reflecting boundaries: GMRES with FP64 or FP32 sweeps");
-    if (kernel_for(precision) != kLane)
+        return bad(IDC_ERR_UNSUPPORTED, "reflecting or periodic edges: GMRES with FP64 or FP32 sweeps");
+    if (reflect_mask && kernel_for(precision) != kLane)
         return bad(IDC_ERR_UNSUPPORTED,
                    "reflecting boundaries need the lane kernel: FP64 or FP32 sweeps at a lane tile shape");
     if (allreduce_fn)
-        return bad(IDC_ERR_UNSUPPORTED, "reflecting boundaries with ordinates partitioned over ranks");
-    const size_t np = phi_len(), ng = reflect_ghost_len(dims(), reflect_mask), n = np + ng;
+        return bad(IDC_ERR_UNSUPPORTED, "reflecting or periodic edges with ordinates partitioned over ranks");
+    const size_t np = phi_len(), ng = reflect_ghost_len(dims(), ghost_mask()), n = np + ng;
     if (capturing && (!d_reflect_ || reflect_vec_len_ < 3 * n))
-        return bad(IDC_ERR_STATE, "reflecting-solve buffer allocation inside a stream capture");
+        return bad(IDC_ERR_STATE, "boundary-solve buffer allocation inside a stream capture");
     if (!d_reflect_) IDC_TRY_CUDA(cudaMalloc(&d_reflect_, sizeof(double) * psi_len()));
     if (reflect_vec_len_ < 3 * n) {
         cudaFree(d_reflect_vec_);
@@ -240,18 +251,17 @@ Status Context::gmres_peierls_reflecting(const double *src, double *psi_out, dou
     double *w = d_reflect_;
     IDC_TRY_CUDA(cudaMemcpyAsync(w, src, sizeof(double) * psi_len(), cudaMemcpyDeviceToDevice, stream));
     IDC_TRY(reflect_ghosts(w, nullptr, false));
-    IDC_TRY(reflect_quadrants(w, dt, b, precision));
+    IDC_TRY(boundary_sweep(w, dt, b, precision));
     IDC_TRY(reflect_ghosts(w, b + np, true));
     bool converged = false;
     double resid = 0.0;
-    auto op = [&](const double *in, double *out) { return apply_peierls_reflecting(in, out, tmp, dt, precision); };
+    auto op = [&](const double *in, double *out) { return apply_peierls_boundary(in, out, tmp, dt, precision); };
     IDC_TRY(gmres(op, b, x, abs_tol, restart, max_its, iters_out, &resid, &converged, precond_kind == 1 ? 1 : 0,
                   ng));
     IDC_TRY_CUDA(cudaMemcpyAsync(psi_out, src, sizeof(double) * psi_len(), cudaMemcpyDeviceToDevice, stream));
     IDC_TRY(reflect_ghosts(psi_out, x + np, false));
-    IDC_TRY_CUDA(launch_smv(dims(), 1.0, 1.0, d_sigma_s, x, psi_out, stream));
-    launches += 1;
-    IDC_TRY(reflect_quadrants(psi_out, dt, nullptr, precision));
+    IDC_TRY(smv(1.0, 1.0, x, psi_out));
+    IDC_TRY(boundary_sweep(psi_out, dt, nullptr, precision));
     IDC_TRY(check_device_error());
     if (resid_out) *resid_out = resid;
     if (!converged)
@@ -264,8 +274,8 @@ Status Context::gmres_peierls_reflecting(const double *src, double *psi_out, dou
 Status Context::gmres_peierls(const double *src, double *psi_out, double dt, double abs_tol, int restart,
                               int64_t max_its, int precision, int64_t *iters_out, double *resid_out) {
     if (!use_warp_kernel) return bad(IDC_ERR_UNSUPPORTED, "GMRES needs the warp-pipelined sweep kernel");
-    if (reflect_mask)
-        return gmres_peierls_reflecting(src, psi_out, dt, abs_tol, restart, max_its, precision, iters_out, resid_out);
+    if (reflect_mask || periodic_)
+        return gmres_peierls_boundary(src, psi_out, dt, abs_tol, restart, max_its, precision, iters_out, resid_out);
     if (precision == IDC_PREC_FP32_IR) return gmres_peierls_ir(src, psi_out, dt, abs_tol, restart, max_its, iters_out,
                                                                resid_out);
     IDC_TRY(ensure_phi_buffers(6));
@@ -350,6 +360,8 @@ Status Context::set_preconditioner(int kind, int inner_steps) {
 // y = x - S^T L^{-T} P^T x: one transposed sweep with the fused source w_q x, no psi stored, the unweighted
 // moment sums scaled by sigma_s / (4 pi).
 Status Context::apply_peierls_adjoint(const double *x, double *y, double *tmp_phi, double dt, int precision) {
+    if (periodic_ || reflect_mask)
+        return bad(IDC_ERR_UNSUPPORTED, "adjoint solves with periodic or reflecting edges");
     IDC_TRY(sweep(nullptr, nullptr, dt, tmp_phi, precision, x, 1.0, true));
     IDC_TRY_CUDA(launch_adjoint_scatter(dims(), d_sigma_s, x, tmp_phi, y, stream));
     launches += 1;

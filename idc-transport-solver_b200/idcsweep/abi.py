@@ -50,7 +50,7 @@ EXPORTED_SYMBOLS = (
     "idc_batch_add", "idc_batch_sweep", "idc_batch_autotune", "idc_batch_last_timing", "idc_batch_destroy",
     "idc_batch_set_shape", "idc_batch_get_shape", "idc_sweep_out_many", "idc_adjoint_transient",
     "idc_set_spin_limit", "idc_batch_gmres_solve", "idc_set_allreduce", "idc_adjoint_idc", "idc_lmv_transpose",
-    "idc_set_reflecting",
+    "idc_set_reflecting", "idc_set_periodic",
 )
 
 
@@ -105,6 +105,7 @@ def load_library(path: str = LIB_PATH):
                                     C.c_int32, C.c_int64, C.c_int, vp, vp, vp, vp, _dp, C.c_int, C.POINTER(C.c_int64)]
     lib.idc_lmv_transpose.argtypes = [vp, C.c_double, C.c_double, vp, vp, C.c_int]
     lib.idc_set_reflecting.argtypes = [vp, C.c_int32]
+    lib.idc_set_periodic.argtypes = [vp, C.c_int32]
     lib.idc_sweep_out.argtypes = [vp, vp, vp, C.c_double, vp, C.c_int, C.c_int]
     lib.idc_sweep_out_many.argtypes = [vp, C.c_int64, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.c_double,
                                        C.c_int, C.c_int]
@@ -350,6 +351,10 @@ class SweepContext:
         """Device pointers: y <- beta y + alpha L^T x (interior cells)."""
         _check(self._lib.idc_lmv_transpose(self._h, float(alpha), float(beta), C.c_void_p(int(x_ptr)),
                                            C.c_void_p(int(y_ptr)), LOC_DEVICE), "idc_lmv_transpose")
+
+    def set_periodic(self, on: bool = True):
+        """Periodic boundaries on all four edges (the reference's `periodic` key)."""
+        _check(self._lib.idc_set_periodic(self._h, 1 if on else 0), "idc_set_periodic")
 
     def set_reflecting(self, edges: int = 0):
         """Reflecting edges: EDGE_X_MIN | EDGE_X_MAX | EDGE_Y_MIN | EDGE_Y_MAX (0: none)."""

@@ -383,6 +383,17 @@ int idc_set_spin_limit(idc_ctx *ctx, int64_t polls);
  * point for every edge set.  FP64 and FP32 sweeps (the lane kernel); IDC_PREC_FP32_IR, transposed sweeps,
  * IDC time stepping, batches and ordinate-partitioned solves with reflecting boundaries return
  * IDC_ERR_UNSUPPORTED. */
+/* Periodic boundaries (the reference's Global::periodic, deck key `periodic`): 1 = on, 0 = off (the default).
+ * A sweep reads the ghost cells as given, as the reference's does.  idc_source_iteration follows
+ * SISolver::Solve on a periodic grid: psi starts at zero; from the second iteration on, each iteration first
+ * fills the ghost cells of the four edges with the opposite interior edge's values (DensityFunction::
+ * SynchronizeHalos, objects/Abstract/DensityFunction.cpp:927-960) and then copies the source into the interior
+ * cells only.  idc_gmres_solve adds the edges' incoming ghost values to its unknowns and reaches the same fixed
+ * point.  idc_lmv uses the opposite edges' cells as the upwind neighbours across an edge (Lmv synchronises its
+ * input's halos first).  Reflecting edges, IDC_PREC_FP32_IR, adjoint solves, transposed operators, IDC time
+ * stepping, batches and, for GMRES, ordinate-partitioned solves return IDC_ERR_UNSUPPORTED on a periodic grid. */
+int idc_set_periodic(idc_ctx *ctx, int32_t periodic);
+
 #define IDC_EDGE_X_MIN 1
 #define IDC_EDGE_X_MAX 2
 #define IDC_EDGE_Y_MIN 4

@@ -155,7 +155,7 @@ class Reference:
         lib.ref_create_reflecting.restype = C.c_void_p
         lib.ref_create_reflecting.argtypes = lib.ref_create.argtypes + [C.c_int]
         lib.ref_create_ex.restype = C.c_void_p
-        lib.ref_create_ex.argtypes = lib.ref_create.argtypes + [C.c_int, C.c_int]
+        lib.ref_create_ex.argtypes = lib.ref_create.argtypes + [C.c_int, C.c_int, C.c_int]
         lib.ref_destroy.argtypes = [C.c_void_p]
         lib.ref_apply.argtypes = [C.c_void_p, _dp, C.c_double, _dp]
         lib.ref_apply_timed.argtypes = [C.c_void_p, _dp, C.c_double, C.c_int64, _dp]
@@ -173,13 +173,15 @@ class Reference:
         self.lib = lib
 
     def open(self, P: Problem, dt: float = np.inf, pattern: str = "wavefront", abs_tol=1e-10, max_its=500,
-             reflect: int = 0, sigma_degree: int = 0):
+             reflect: int = 0, sigma_degree: int = 0, periodic: bool = False):
         """reflect: the reflecting edges as the reference's BoundaryEdge bits (X_Min 1, X_Max 2, Y_Min 4,
         Y_Max 8); with any, the reference sweeps the quadrants in sequence and reflects between them.
-        sigma_degree: 0, or p when P.sigma_t / P.sigma_s hold (p+1)^2 Legendre moments per cell."""
+        sigma_degree: 0, or p when P.sigma_t / P.sigma_s hold (p+1)^2 Legendre moments per cell.
+        periodic: the reference's Global::periodic (halos synchronised from the opposite edges)."""
         keep = [np.ascontiguousarray(a, np.float64) for a in (P.xi, P.eta, P.w, P.sigma_t, P.sigma_s)]
         h = self.lib.ref_create_ex(P.nx, P.ny, P.ax, P.bx, P.ay, P.by, P.p, P.nq, *[_p(a) for a in keep],
-                                   dt, pattern.encode(), abs_tol, max_its, int(reflect), int(sigma_degree))
+                                   dt, pattern.encode(), abs_tol, max_its, int(reflect), int(sigma_degree),
+                                   1 if periodic else 0)
         if not h:
             raise RuntimeError("ref_create failed")
         return _RefHandle(self.lib, h, P, keep)

@@ -47,6 +47,7 @@ int64_t next_order_key = 1000000;
 struct RefProblem {
     int reflect = 0;   // BoundaryEdge bits of the reflecting edges (Global::reflecting_boundaries while in use)
     int sigma_degree = 0;   // DG degree of the cross sections: 0 (piecewise constant) or p
+    bool periodic = false;  // Global::periodic while in use
     int64_t nx, ny, p, N, nq;
     int64_t order_key;
     ParameterList plist;
@@ -108,11 +109,18 @@ void CopyOut ( const Abstract::DensityFunction & f, double * dst, size_t n ) {
     std::memcpy( dst, f.density, n * sizeof(double) );
 }
 
-// Global::reflecting_boundaries of a problem for the duration of a call into the reference (the reference
-// reads the global in its sweeps), reset afterwards so that other problems see none.
+// Global::reflecting_boundaries and Global::periodic of a problem for the duration of a call into the
+// reference (it reads the globals in its sweeps, halo operations and solvers), reset afterwards so that other
+// problems see neither.
 struct ReflectScope {
-    explicit ReflectScope ( int mask ) {  Global::reflecting_boundaries = static_cast<BoundaryEdge>( mask );  }
-    ~ReflectScope () {  Global::reflecting_boundaries = BoundaryEdge::None;  }
+    explicit ReflectScope ( int mask, bool periodic = false ) {
+        Global::reflecting_boundaries = static_cast<BoundaryEdge>( mask );
+        Global::periodic = periodic;
+    }
+    ~ReflectScope () {
+        Global::reflecting_boundaries = BoundaryEdge::None;
+        Global::periodic = false;
+    }
 };
 
 } // namespace
@@ -126,19 +134,21 @@ extern "C" {
 // (index j + (ny+2)*i), time step dt (+inf for steady state).  sweep_pattern is the reference's key
 // ("wavefront" or "sequential").  Returns an opaque handle, or nullptr on error.
 //------------------------------------------------------------------------------------------------------------
-// reflect: BoundaryEdge bits of reflecting edges; sigma_degree: 0, or p for high-order cross sections given as
+// reflect: BoundaryEdge bits of reflecting edges; periodic: Global::periodic (deck key `periodic`);
+// sigma_degree: 0, or p for high-order cross sections given as
 // (p+1)^2 Legendre moments per cell ([cell][u][v], the DensityFunction layout), as Init configures them when the
 // deck does not ask for piecewise-constant cross sections (utils/init.cpp:740-745).
 void * ref_create_ex ( int64_t nx, int64_t ny, double ax, double bx, double ay, double by, int64_t p,
                        int64_t nq, const double * xi, const double * eta, const double * w,
                        const double * sigma_t, const double * sigma_s, double dt,
                        const char * sweep_pattern, double si_abs_tol, int64_t si_max_its, int reflect,
-                       int sigma_degree ) {
+                       int sigma_degree, int periodic ) {
     try {
         if ( sigma_degree != 0 && sigma_degree != p ) throw std::runtime_error( "sigma_degree must be 0 or p" );
-        ReflectScope scope( reflect );   // SweepPatternUniCart decides on sequential quadrants when built
+        ReflectScope scope( reflect, periodic != 0 );   // SweepPatternUniCart decides on sequential quadrants when built
         auto * P = new RefProblem();
         P->reflect = reflect;
+        P->periodic = periodic != 0;
         P->sigma_degree = sigma_degree;
         P->nx = nx; P->ny = ny; P->p = p; P->N = (p + 1) * (p + 1); P->nq = nq; P->dt = dt;
 
@@ -200,7 +210,7 @@ void * ref_create_reflecting ( int64_t nx, int64_t ny, double ax, double bx, dou
                                const double * sigma_t, const double * sigma_s, double dt,
                                const char * sweep_pattern, double si_abs_tol, int64_t si_max_its, int reflect ) {
     return ref_create_ex( nx, ny, ax, bx, ay, by, p, nq, xi, eta, w, sigma_t, sigma_s, dt, sweep_pattern,
-                          si_abs_tol, si_max_its, reflect, 0 );
+                          si_abs_tol, si_max_its, reflect, 0, 0 );
 }
 
 // The same without reflecting boundaries (vacuum or given inflow on every edge).
@@ -217,7 +227,7 @@ void ref_destroy ( void * h ) { delete static_cast<RefProblem *>(h); }
 // SweepOperator::Apply on psi_inout (halo layout, source in / psi out).  *seconds = wall time of Apply.
 int ref_apply ( void * h, double * psi_inout, double dt, double * seconds ) {
     auto * P = static_cast<RefProblem *>(h);
-    ReflectScope scope( P->reflect );
+    ReflectScope scope( P->reflect, P->periodic );
     try {
         CopyIn( *P->psi, psi_inout, P->psi_len() );
         auto t0 = std::chrono::steady_clock::now();
@@ -233,7 +243,7 @@ int ref_apply ( void * h, double * psi_inout, double dt, double * seconds ) {
 // previous ref_apply (the data is re-loaded before each one so every sweep sees the same source).
 int ref_apply_timed ( void * h, const double * source, double dt, int64_t reps, double * seconds ) {
     auto * P = static_cast<RefProblem *>(h);
-    ReflectScope scope( P->reflect );
+    ReflectScope scope( P->reflect, P->periodic );
     try {
         double total = 0.0;
         for ( int64_t r = 0; r < reps; ++r ) {
@@ -251,7 +261,7 @@ int ref_apply_timed ( void * h, const double * source, double dt, int64_t reps, 
 // phi <- beta*phi + alpha*P psi over interior cells (TransportOperator::Pmv with OpDomain::Interior).
 int ref_pmv ( void * h, double alpha, double beta, const double * psi, double * phi ) {
     auto * P = static_cast<RefProblem *>(h);
-    ReflectScope scope( P->reflect );
+    ReflectScope scope( P->reflect, P->periodic );
     try {
         CopyIn( *P->psi, psi, P->psi_len() );
         CopyIn( *P->phi, phi, P->phi_len() );
@@ -264,7 +274,7 @@ int ref_pmv ( void * h, double alpha, double beta, const double * psi, double * 
 // psi <- beta*psi + alpha*S phi over interior cells with sigma_s (TransportOperator::Smv).
 int ref_smv ( void * h, double alpha, double beta, const double * phi, double * psi ) {
     auto * P = static_cast<RefProblem *>(h);
-    ReflectScope scope( P->reflect );
+    ReflectScope scope( P->reflect, P->periodic );
     try {
         CopyIn( *P->psi, psi, P->psi_len() );
         CopyIn( *P->phi, phi, P->phi_len() );
@@ -277,7 +287,7 @@ int ref_smv ( void * h, double alpha, double beta, const double * phi, double * 
 // y <- beta*y + alpha*L x with sigma_t (TransportOperator::Lmv, out-of-place form).
 int ref_lmv ( void * h, double alpha, double beta, const double * x, double * y ) {
     auto * P = static_cast<RefProblem *>(h);
-    ReflectScope scope( P->reflect );
+    ReflectScope scope( P->reflect, P->periodic );
     try {
         CopyIn( *P->psi, x, P->psi_len() );
         CopyIn( *P->aux, y, P->psi_len() );
@@ -291,7 +301,7 @@ int ref_lmv ( void * h, double alpha, double beta, const double * x, double * y 
 // return.  *iters and *err report the iteration count and the final absolute l2 change of phi.
 int ref_si_solve ( void * h, double * source_inout, double dt, int64_t * iters, double * seconds ) {
     auto * P = static_cast<RefProblem *>(h);
-    ReflectScope scope( P->reflect );
+    ReflectScope scope( P->reflect, P->periodic );
     try {
         CopyIn( *P->aux, source_inout, P->psi_len() );
         P->si->SetInitialGuess( nullptr );
@@ -316,7 +326,7 @@ int ref_si_solve ( void * h, double * source_inout, double dt, int64_t * iters, 
 int ref_idc_steps ( void * h, double * psi_inout, const double * source, double dt, int64_t steps,
                     int64_t num_nodes, int64_t num_corr, double si_abs_tol, int64_t si_max_its ) {
     auto * P = static_cast<RefProblem *>(h);
-    ReflectScope scope( P->reflect );
+    ReflectScope scope( P->reflect, P->periodic );
     try {
         ParameterList pl = P->plist;
         char buf[64];
@@ -351,7 +361,7 @@ int ref_idc_steps ( void * h, double * psi_inout, const double * source, double 
 // halo layout: the reference's .sd2 file.
 int ref_write_sd ( void * h, const double * phi, const char * path ) {
     auto * P = static_cast<RefProblem *>(h);
-    ReflectScope scope( P->reflect );
+    ReflectScope scope( P->reflect, P->periodic );
     try {
         CopyIn( *P->phi, phi, P->phi_len() );
         P->phi->WriteToDisk( std::string( path ) );
@@ -363,7 +373,7 @@ int ref_write_sd ( void * h, const double * phi, const char * path ) {
 // layout: the reference's .af2 file.
 int ref_write_af ( void * h, const double * psi, const char * path ) {
     auto * P = static_cast<RefProblem *>(h);
-    ReflectScope scope( P->reflect );
+    ReflectScope scope( P->reflect, P->periodic );
     try {
         CopyIn( *P->psi, psi, P->psi_len() );
         P->psi->WriteToDisk( std::string( path ) );

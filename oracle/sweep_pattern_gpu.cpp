@@ -111,6 +111,7 @@ public:
         // sequence and reflects between them; the BoundaryEdge bits are the ABI's IDC_EDGE_* bits
         idc_check( idc_set_reflecting( this->ctx, static_cast<int32_t>( Global::reflecting_boundaries ) & 15 ),
                    "idc_set_reflecting" );
+        idc_check( idc_set_periodic( this->ctx, Global::periodic ? 1 : 0 ), "idc_set_periodic" );
         idc_check( idc_set_sigma( this->ctx, sigma.PointerAtCell( 0, 0 ), nullptr, IDC_LOC_HOST ), "idc_set_sigma" );
         const double dt = this->sw_op.sweep_cell_solve->GetDt();   // set by SweepOperator::Apply
         if ( &source == &result ) {
@@ -120,6 +121,9 @@ public:
             idc_check( idc_sweep_out( this->ctx, source.PointerAtCell( 0, 0 ), result.PointerAtCell( 0, 0 ), dt,
                                       nullptr, IDC_PREC_FP64, IDC_LOC_HOST ), "idc_sweep_out" );
         }
+        // the reference's patterns leave the halos dirty on a periodic grid (SweepPatternUniCartWavefront.cpp:324-331),
+        // so the next reader synchronises them
+        if ( Global::periodic ) result.MarkAllHalosDirty();
     }
 
 private:

@@ -95,3 +95,17 @@ def test_reference_source_iteration_with_high_order_cross_sections_through_plugi
             psi = h.source_iteration(P.source, P.dt)
             out[pattern] = h.pmv(psi)
     assert rel_err(out["gpu-wavefront"], out["wavefront"]) < 1e-11
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("p", [1, 2])
+def test_reference_source_iteration_on_a_periodic_grid_through_plugin(plugged, p):
+    """The reference's SISolver::Solve with Global::periodic (halos synchronised between iterations; the plugin
+    leaves them dirty after its sweep, as the reference's patterns do): gpu-wavefront against wavefront."""
+    P = lognormal(14, p, 4, seed=13 + p, c_range=(0.3, 0.8), dt=0.4)
+    out = {}
+    for pattern in ("wavefront", "gpu-wavefront"):
+        with plugged.open(to_oracle(P), P.dt, pattern=pattern, abs_tol=1e-12, max_its=5000, periodic=True) as h:
+            psi = h.source_iteration(P.source, P.dt)
+            out[pattern] = h.pmv(psi)
+    assert rel_err(out["gpu-wavefront"], out["wavefront"]) < 1e-11
