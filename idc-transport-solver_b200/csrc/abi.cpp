@@ -142,7 +142,7 @@ int idc_ctx_create(const idc_problem_desc *desc, idc_ctx **out) {
         !std::isfinite(desc->by - desc->ay))
         return fail(IDC_ERR_ARG, "idc_ctx_create: empty or non-finite domain");
     if (desc->dg_degree < 0) return fail(IDC_ERR_ARG, "idc_ctx_create: negative DG degree");
-    if (desc->dg_degree > 2) return fail(IDC_ERR_UNSUPPORTED, "idc_ctx_create: DG degree > 2 not implemented");
+    if (desc->dg_degree > 3) return fail(IDC_ERR_UNSUPPORTED, "idc_ctx_create: DG degree > 3 not implemented");
     if (desc->sigma_degree != 0 && desc->sigma_degree != desc->dg_degree)
         return fail(IDC_ERR_ARG, "idc_ctx_create: sigma_degree must be 0 (piecewise constant) or the DG degree");
     if (desc->flags != 0) return fail(IDC_ERR_ARG, "idc_ctx_create: flags must be 0");

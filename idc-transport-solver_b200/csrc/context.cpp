@@ -386,15 +386,15 @@ namespace {
 // (Bonnet's recurrence) and the exact monomial integrals 2 / (k + 1) for even k; values below 5e-16 are zero,
 // as the reference clears them.
 TripleProducts triple_products(int P) {
-    double c[3][3] = {{1, 0, 0}, {0, 1, 0}, {-0.5, 0, 1.5}};   // P_0, P_1, P_2 by powers of x
+    const double c[4][4] = {{1, 0, 0, 0}, {0, 1, 0, 0}, {-0.5, 0, 1.5, 0}, {0, -1.5, 0, 2.5}};   // P_0..P_3
     TripleProducts t{};
     for (int a = 0; a < P; ++a)
         for (int b = 0; b < P; ++b)
             for (int cc = 0; cc < P; ++cc) {
                 double v = 0.0;
-                for (int i = 0; i < 3; ++i)
-                    for (int j = 0; j < 3; ++j)
-                        for (int k = 0; k < 3; ++k) {
+                for (int i = 0; i < 4; ++i)
+                    for (int j = 0; j < 4; ++j)
+                        for (int k = 0; k < 4; ++k) {
                             const int deg = i + j + k;
                             if (deg % 2 == 0) v += c[a][i] * c[b][j] * c[cc][k] * (2.0 / (deg + 1));
                         }
@@ -451,7 +451,7 @@ Status Context::set_tiling(int G, int R) {
 // the lane kernel, else the modal kernel), and without a tile shape the lane kernel; the lane kernel
 // sweeps in FP64 only, the FP32 modes run on the modal kernel.  IDC_SWEEP_KERNEL fixes another kernel.
 int Context::kernel_for(int precision) const {
-    if (high_order_sigma()) return kWarp;   // the elimination kernel takes a full cell matrix
+    if (high_order_sigma() || P > 3) return kWarp;   // the elimination kernel takes a full cell matrix
     if (kernel != kLane) return kernel;
     if (tune_seg > 0 && tune_wn > 0) return kModal;
     return sweep_lane_supports(P, precision, tune_seg > 0 ? tune_seg : 4) ? kLane : kModal;
@@ -593,6 +593,11 @@ Status Context::build_schedule(int precision) {
             G = (qmax + nch - 1) / nch;
         }
         if (active == kModal) wn = sweep_modal_fit_wn(P, precision, wn, G, seg);
+        if (active == kWarp) {   // fewer warps per block where the rings outgrow shared memory (DG degree 3)
+            int limit = 0;
+            IDC_TRY_CUDA(cudaDeviceGetAttribute(&limit, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+            while (wn > 1 && sweep_warp_smem_bytes(P, wn, G, seg) > (size_t)limit) --wn;
+        }
         R = wn * (32 / seg);
     } else {
         const int max_threads = 320;
@@ -765,6 +770,8 @@ Status Context::sweep(const double *src, double *out, double dt, double *phi, in
         return bad(IDC_ERR_UNSUPPORTED, "the transposed sweep needs the modal kernel in FP64 or refined precision");
     if (src2 && (adjoint || !modal_family() || !src))
         return bad(IDC_ERR_UNSUPPORTED, "a second source needs a forward modal sweep with a first source");
+    if (P > 3 && precision != IDC_PREC_FP64)
+        return bad(IDC_ERR_UNSUPPORTED, "DG degree 3: FP64 sweeps (the elimination kernel)");
     if (high_order_sigma()) {
         if (precision != IDC_PREC_FP64)
             return bad(IDC_ERR_UNSUPPORTED, "high-order cross sections: FP64 sweeps (the elimination kernel)");

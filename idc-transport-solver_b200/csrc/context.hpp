@@ -156,7 +156,9 @@ public:
     int active = kLane;            // the kernel the current schedule was built for (kernel_for(precision))
     bool use_warp_kernel = true;   // kernel is kWarp, kModal or kLane (same trace protocol)
     // the modal cell arithmetic (modal or lane kernel): the transposed sweep, IDC, batches
-    bool modal_family() const { return kernel == kModal || kernel == kLane; }
+    // the lane and modal kernels (their cell arithmetic diagonalises a Kronecker cell matrix): DG degree <= 2,
+    // piecewise-constant cross sections
+    bool modal_family() const { return (kernel == kModal || kernel == kLane) && P <= 3 && !high_order_sigma(); }
     int kernel_for(int precision) const;
     int seg = 0, wn = 0;           // warp kernel tiling
     double *d_trace = nullptr;     // warp / modal kernel: per-item last-row traces (sentinel-armed)

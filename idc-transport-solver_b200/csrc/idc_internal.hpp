@@ -174,7 +174,7 @@ cudaError_t launch_lmv(const GridDims &g, double alpha, double beta, const doubl
 // High-order cross sections (the reference's CrossSection with DG_degree = p, objects/RKDG/CrossSection.cpp).
 // tpi[a + P (b + P c)] = integral over [-1, 1] of P_a P_b P_c (Global::TPI, utils/global.cpp:67-110).
 struct TripleProducts {
-    double v[27];
+    double v[64];   // P <= 4
 };
 // Per cell (ghost cells included) from the Legendre moments mom[cell][u][v]: avg[cell] = mom(0, 0) (the cell
 // average), tensor[cell][r][c] = T(d,e; u,v) = sum_{m,n} mom(m,n) TPI(d,u,m) TPI(e,v,n) (CrossSection::

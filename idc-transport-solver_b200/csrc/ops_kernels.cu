@@ -843,6 +843,7 @@ cudaError_t launch_lmv(const GridDims &g, double alpha, double beta, const doubl
         case 1: lmv_p<1>(g, n, alpha, beta, sigma_t, xi, eta, x, y, gamma, sigma_s, phi_sc, tensor_t, tensor_s, s); break;
         case 2: lmv_p<2>(g, n, alpha, beta, sigma_t, xi, eta, x, y, gamma, sigma_s, phi_sc, tensor_t, tensor_s, s); break;
         case 3: lmv_p<3>(g, n, alpha, beta, sigma_t, xi, eta, x, y, gamma, sigma_s, phi_sc, tensor_t, tensor_s, s); break;
+        case 4: lmv_p<4>(g, n, alpha, beta, sigma_t, xi, eta, x, y, gamma, sigma_s, phi_sc, tensor_t, tensor_s, s); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -855,6 +856,7 @@ cudaError_t launch_sigma_tensor(const GridDims &g, const double *mom, const Trip
         case 1: sigma_tensor_kernel<1><<<blocks_for(cells), kThreads, 0, s>>>(g, mom, tpi, dxdy4, avg, tensor, cat); break;
         case 2: sigma_tensor_kernel<2><<<blocks_for(cells), kThreads, 0, s>>>(g, mom, tpi, dxdy4, avg, tensor, cat); break;
         case 3: sigma_tensor_kernel<3><<<blocks_for(cells), kThreads, 0, s>>>(g, mom, tpi, dxdy4, avg, tensor, cat); break;
+        case 4: sigma_tensor_kernel<4><<<blocks_for(cells), kThreads, 0, s>>>(g, mom, tpi, dxdy4, avg, tensor, cat); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -867,6 +869,7 @@ cudaError_t launch_smv_tensor(const GridDims &g, double alpha, double beta, cons
         case 1: smv_tensor_kernel<1><<<blocks_for(n), kThreads, 0, s>>>(g, alpha, beta, tensor_s, phi, psi); break;
         case 2: smv_tensor_kernel<2><<<blocks_for(n), kThreads, 0, s>>>(g, alpha, beta, tensor_s, phi, psi); break;
         case 3: smv_tensor_kernel<3><<<blocks_for(n), kThreads, 0, s>>>(g, alpha, beta, tensor_s, phi, psi); break;
+        case 4: smv_tensor_kernel<4><<<blocks_for(n), kThreads, 0, s>>>(g, alpha, beta, tensor_s, phi, psi); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

@@ -125,7 +125,7 @@ __device__ __forceinline__ double pick(const double (&v)[N], int k) {
 
 // Source prefetch depth (cells ahead per lane): enough to cover HBM latency under load with the
 // per-step time of each DG degree, within the shared-memory budget.
-__host__ __device__ constexpr int prefetch_depth(int P) { return P == 3 ? 4 : 8; }
+__host__ __device__ constexpr int prefetch_depth(int P) { return P >= 4 ? 3 : P == 3 ? 4 : 8; }
 
 struct Layout {
     uint64_t *full, *empty;   // [Wn+1][kS]
@@ -510,6 +510,7 @@ cudaError_t launch_sweep_warp(int P, int precision, const SweepArgs &args, int g
         case 1: IDC_WDISPATCH(1, launch_t, args, grid, smem, stream);
         case 2: IDC_WDISPATCH(2, launch_t, args, grid, smem, stream);
         case 3: IDC_WDISPATCH(3, launch_t, args, grid, smem, stream);
+        case 4: return precision == 0 ? launch_t<4, 0>(args, grid, smem, stream) : cudaErrorInvalidValue;
         default: return cudaErrorInvalidValue;
     }
 }
@@ -519,6 +520,7 @@ cudaError_t sweep_warp_occupancy(int P, int precision, int threads, size_t smem,
         case 1: IDC_WDISPATCH(1, occ_t, threads, smem, blocks_per_sm);
         case 2: IDC_WDISPATCH(2, occ_t, threads, smem, blocks_per_sm);
         case 3: IDC_WDISPATCH(3, occ_t, threads, smem, blocks_per_sm);
+        case 4: return precision == 0 ? occ_t<4, 0>(threads, smem, blocks_per_sm) : cudaErrorInvalidValue;
         default: return cudaErrorInvalidValue;
     }
 }

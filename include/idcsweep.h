@@ -56,7 +56,8 @@ typedef struct idc_ctx idc_ctx;
 typedef struct idc_problem_desc {
     int64_t nx, ny;          /* interior cells in x and y (DomainDecomposition nx(0), nx(1))            */
     double ax, bx, ay, by;   /* domain [ax,bx] x [ay,by]; dx = (bx-ax)/nx, dy = (by-ay)/ny              */
-    int64_t dg_degree;       /* DG degree p of psi and phi (Global::DG_degree); 0..2 supported          */
+    int64_t dg_degree;       /* DG degree p of psi and phi (Global::DG_degree): 0..3; 3 runs on the     */
+                             /* elimination kernel in FP64 (no FP32, transposed, IDC or batched sweeps) */
     int64_t sigma_degree;    /* DG degree of the cross sections: 0 (piecewise constant) or dg_degree    */
     int32_t device;          /* CUDA device ordinal                                                     */
     int32_t flags;           /* reserved, must be 0                                                     */

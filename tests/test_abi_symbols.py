@@ -45,8 +45,8 @@ def test_descriptor_validation_before_device():
     h = C.c_void_p()
     bad = abi.ProblemDesc(0, 4, 0.0, 1.0, 0.0, 1.0, 1, 0, 0, 0)
     assert lib.idc_ctx_create(C.byref(bad), C.byref(h)) == abi.IDC_ERR_ARG
-    p3 = abi.ProblemDesc(4, 4, 0.0, 1.0, 0.0, 1.0, 3, 0, 0, 0)
-    assert lib.idc_ctx_create(C.byref(p3), C.byref(h)) == abi.IDC_ERR_UNSUPPORTED
+    p4 = abi.ProblemDesc(4, 4, 0.0, 1.0, 0.0, 1.0, 4, 0, 0, 0)   # DG degree <= 3
+    assert lib.idc_ctx_create(C.byref(p4), C.byref(h)) == abi.IDC_ERR_UNSUPPORTED
     hi = abi.ProblemDesc(4, 4, 0.0, 1.0, 0.0, 1.0, 1, 2, 0, 0)   # cross sections: degree 0 or the DG degree
     assert lib.idc_ctx_create(C.byref(hi), C.byref(h)) == abi.IDC_ERR_ARG
     empty = abi.ProblemDesc(4, 4, 1.0, 1.0, 0.0, 1.0, 1, 0, 0, 0)
