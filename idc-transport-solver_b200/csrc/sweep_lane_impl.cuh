@@ -169,25 +169,39 @@ __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.p
 // The consumer caught up with its producer (a value of column s still held the sentinel): wait, bounded,
 // until the producer has written column s.  Waiting for no more than that keeps the lag between row blocks
 // at its minimum (measured on B200: waiting for two more columns of slack, to wait less often, made the
-// 256x256 Q2 S16 sweep 10-20% slower).  Returns the poll count so far, or -1 if the wait gave up or another
-// warp has failed (the error word is then set).  Out of line: the hot loop stays small; every argument is a
-// register.
+// 256x256 Q2 S16 sweep 10-20% slower).  The poll that finds the column complete has read its values, which
+// are returned with the poll count, so the consumer does not load them again (one L2 round trip less on the
+// row-block handoff); polls = -1 if the wait gave up or another warp has failed (the error word is then
+// set).  Out of line: the hot loop stays small; every argument is a register.
 template <int P>
-__device__ __noinline__ long long wait_for_producer(const double *dep_trace, int s, bool reader, int G, int *error,
-                                                    long long spin_limit, long long polls, int lane) {
+struct ProducerWait {
+    long long polls;
+    double v[P];   // column s as the last poll read it; 0.0 in lanes that do not read (as load_trace gives)
+};
+template <int P>
+__device__ __noinline__ ProducerWait<P> wait_for_producer(const double *dep_trace, int s, bool reader, int G,
+                                                          int *error, long long spin_limit, long long polls,
+                                                          int lane) {
     const double *col = dep_trace + (size_t)s * G * P;
+    ProducerWait<P> r;
     for (;;) {
         bool still = false;
-        if (reader) {
 #pragma unroll
-            for (int m = 0; m < P; ++m) still |= is_sentinel(ld_relaxed_f64(col + m));
+        for (int m = 0; m < P; ++m) {
+            r.v[m] = ld_relaxed_f64_if(col + m, reader);
+            still |= reader && is_sentinel(r.v[m]);
         }
-        if (!__any_sync(kFullMask, still)) return polls;
+        r.polls = polls;
+        if (!__any_sync(kFullMask, still)) return r;
         ++polls;
-        if ((polls & 63) == 63 && ld_relaxed(error) != kDevOk) return -1;
+        if ((polls & 63) == 63 && ld_relaxed(error) != kDevOk) {
+            r.polls = -1;
+            return r;
+        }
         if (polls > spin_limit) {
             if (lane == 0) atomicCAS(error, kDevOk, kDevTimeout);
-            return -1;
+            r.polls = -1;
+            return r;
         }
         __nanosleep(64);
     }
@@ -437,11 +451,13 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
             bool bad = false;
 #pragma unroll
             for (int m = 0; m < P; ++m) bad |= reader && s < nx && is_sentinel(tnext[m]);
-            if (__any_sync(kFullMask, bad)) {   // caught up with the producer: wait for two columns of slack
-                polls = wait_for_producer<P>(dep_trace, s, reader, a.G, a.error, a.spin_limit,
-                                             polls, lane);
+            if (__any_sync(kFullMask, bad)) {   // caught up with the producer: wait for column s
+                const ProducerWait<P> w =
+                    wait_for_producer<P>(dep_trace, s, reader, a.G, a.error, a.spin_limit, polls, lane);
+                polls = w.polls;
                 if (polls < 0) break;
-                load_trace(s, tnext);
+#pragma unroll
+                for (int m = 0; m < P; ++m) tnext[m] = w.v[m];
             }
         }
         {   // re-arm the consumed column for the next sweep
