@@ -271,14 +271,64 @@ Status Context::sweep_reflecting(const double *src, double *out, double dt, doub
     return reflect_quadrants(w, dt, phi, precision);
 }
 
+// The reference's quadrant sequence 3, 2, 1, 0 (a reflection after each) in as few launches as give the same
+// result.  Quadrant k (0: xi > 0, eta > 0; 1: xi > 0, eta < 0; 2: xi < 0, eta > 0; 3: xi < 0, eta < 0) reads
+// ghost cells on its x-inflow edge (x-min if xi > 0) and y-inflow edge (y-min if eta > 0); where that edge
+// reflects, the reference hands it the mirror of partner quadrant k ^ 2 (x) or k ^ 1 (y) as the partner stands
+// after the quadrants swept before k.  Launch levels L (a reflection after each launch) keep that when
+//   * a partner swept before k in the reference is in an earlier launch: L(k) > L(partner);
+//   * a partner swept after k is not in an earlier launch: L(partner) >= L(k) (k must see it unswept);
+//   * k other than the first quadrant, 3, with a reflecting inflow is not in the first launch: the first
+//     launch reads the input's ghost cells, k reads a reflection.
+// Quadrants of one launch read nothing another of them writes, and the reflection after a launch is that of
+// the current interior, as after the reference's last quadrant.  The least levels meeting these (a fixed
+// point; quadrant 3 stays at 0) give, e.g., all edges: {3}, {2, 1}, {0}; x-min: {3, 2}, {1, 0}; y-min: {3, 1},
+// {2, 0}.  Returns the launches' quadrant masks in order.
+static std::vector<int> reflect_launches(int mask) {
+    auto before = [](int p, int k) { return p > k; };   // the reference sweeps 3, 2, 1, 0
+    int L[4] = {0, 0, 0, 0};
+    for (int k = 0; k < 4; ++k) {
+        const int xedge = (k & 2) ? 2 : 1, yedge = (k & 1) ? 8 : 4;   // xi < 0: x-max; eta < 0: y-max
+        if (k != 3 && (mask & (xedge | yedge))) L[k] = 1;
+    }
+    for (bool changed = true; changed;) {
+        changed = false;
+        for (int k = 0; k < 4; ++k) {
+            const int xedge = (k & 2) ? 2 : 1, yedge = (k & 1) ? 8 : 4;
+            for (int e = 0; e < 2; ++e) {
+                if (!(mask & (e == 0 ? xedge : yedge))) continue;
+                const int p = e == 0 ? (k ^ 2) : (k ^ 1);
+                if (before(p, k) && L[k] < L[p] + 1) {
+                    L[k] = L[p] + 1;
+                    changed = true;
+                }
+                if (!before(p, k) && L[p] < L[k]) {
+                    L[p] = L[k];
+                    changed = true;
+                }
+            }
+        }
+    }
+    std::vector<int> groups;
+    for (int level = 0; level < 4; ++level) {
+        int m = 0;
+        for (int k = 0; k < 4; ++k)
+            if (L[k] == level) m |= 1 << k;
+        if (m) groups.push_back(m);
+    }
+    return groups;
+}
+
 // The sequential-quadrant sweep proper, in place on a prepared array w; phi (optional) gets the moments of
 // all four quadrants.
 Status Context::reflect_quadrants(double *w, double dt, double *phi, int precision) {
     in_reflect_ = true;
     Status st = Status::ok();
-    for (int quad : {3, 2, 1, 0}) {
-        quad_mask_ = 1 << quad;
-        skip_reduce_ = quad != 0;   // the chunk partials of every quadrant are summed after the last
+    const std::vector<int> launches_q = reflect_launches(reflect_mask);
+    for (size_t g = 0; g < launches_q.size(); ++g) {
+        const int mask = launches_q[g];
+        quad_mask_ = mask;
+        skip_reduce_ = g + 1 < launches_q.size();   // the chunk partials of every quadrant are summed after the last
         st = sweep(w, w, dt, phi, precision);
         if (!st.good()) break;
         cudaError_t e = launch_reflect_boundaries(dims(), reflect_mask, d_xi, d_eta, d_rmap, w, stream);
