@@ -139,10 +139,13 @@ Status Context::idc_integrate(double *psi, const double *Q, double dt, int64_t s
     if (!(dt > 0) || !std::isfinite(dt)) return bad(IDC_ERR_ARG, "IDC needs a finite positive dt");
     if (steps < 0) return bad(IDC_ERR_ARG, "negative step count");
     if (reflect_mask) return bad(IDC_ERR_UNSUPPORTED, "IDC time stepping with reflecting boundaries");
-    if (high_order_sigma()) return bad(IDC_ERR_UNSUPPORTED, "IDC time stepping with high-order cross sections");
     if (periodic_) return bad(IDC_ERR_UNSUPPORTED, "IDC time stepping on a periodic grid");
     if (scattering != 0 && scattering != 1) return bad(IDC_ERR_ARG, "scattering must be 0 (explicit) or 1 (implicit)");
-    if (!modal_family()) return bad(IDC_ERR_UNSUPPORTED, "IDC needs the modal sweep kernel");
+    // explicit scattering: the lane or modal kernel's second source and the fused correction kernel (piecewise-
+    // constant sigma, DG degree <= 2); implicit scattering (GMRES substeps) takes every input the solver takes
+    if (scattering == 0 && !modal_family())
+        return bad(IDC_ERR_UNSUPPORTED, "IDC with explicit scattering needs the lane or modal kernel (DG degree <= 2, "
+                                        "piecewise-constant cross sections); implicit scattering takes these inputs");
     std::vector<double> t, W;
     idc_nodes_and_weights(M, t, W);
 

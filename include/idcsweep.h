@@ -206,10 +206,12 @@ enum { IDC_SCATTER_EXPLICIT = 0, IDC_SCATTER_IMPLICIT = 1 };
  * non-hybrid update form: IDCIntegrator::Step_Nonhybrid, ComputeResiduals, ComputeSource
  * (time_integrators/RKDG/idc.cpp:846-955, 1657-1740) and SetNodes (:2305-2381).
  * scattering = IDC_SCATTER_IMPLICIT: every substep solves (1/(h dt) + L - S P) with the GPU GMRES
- * (abs_tol, restart, max_its), as the reference does with its implicit solver.
+ * (abs_tol, restart, max_its), as the reference does with its implicit solver; high-order cross sections
+ * and DG degree 3 are taken here.
  * scattering = IDC_SCATTER_EXPLICIT (IMEX): every substep is one sweep with the scattering lagged to the
  * previous node and corrected by the deferred-correction iterations; with use_graph a step is captured
- * once as a CUDA graph and replayed.  Quadrature sums and residuals are FP64; `precision` selects the
+ * once as a CUDA graph and replayed (lane or modal kernel: DG degree <= 2, piecewise-constant cross
+ * sections).  Reflecting edges and periodic grids return IDC_ERR_UNSUPPORTED.  Quadrature sums and residuals are FP64; `precision` selects the
  * sweep arithmetic.  *sweeps receives the number of sweeps performed. */
 int idc_idc_integrate(idc_ctx *ctx, double *psi_inout, const double *source, double dt, int64_t steps,
                       int32_t num_nodes, int32_t num_corrections, int scattering, int precision, double abs_tol,

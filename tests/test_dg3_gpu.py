@@ -106,3 +106,16 @@ def test_unsupported_at_dg_degree_3():
             with abi.Batch() as b:
                 b.add(ctx)
         assert e.value.code == abi.IDC_ERR_UNSUPPORTED
+
+
+def test_implicit_idc_matches_reference_integrator(ref):
+    """IDC time stepping with implicit scattering at DG degree 3 against the reference's IDCIntegrator."""
+    P = random_problem(6, 7, 3, 4, seed=31, dt=0.05, inflow=False, sigma_range=(0.5, 4.0))
+    psi0 = np.zeros(P.psi_shape())
+    psi0[1:-1, 1:-1] = 0.05
+    with ref.open(to_oracle(P), P.dt, abs_tol=1e-14, max_its=100000) as h:
+        want = h.idc_steps(psi0, P.source, P.dt, 2, 3, 2, si_abs_tol=1e-14)
+    with _ctx(P) as ctx:
+        psi = psi0.copy()
+        ctx.idc_integrate(psi, P.source, P.dt, 2, 3, 2, abi.SCATTER_IMPLICIT, abi.PREC_FP64, abs_tol=1e-14)
+    assert rel_err(psi[1:-1, 1:-1], want[1:-1, 1:-1]) < 1e-10

@@ -119,3 +119,18 @@ def test_unsupported_with_high_order_cross_sections():
             with abi.Batch() as b:
                 b.add(ctx)
         assert e.value.code == abi.IDC_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("p", [1, 2])
+def test_implicit_idc_matches_reference_integrator(ref, p):
+    """IDC time stepping with implicit scattering (GMRES substeps) against the reference's own IDCIntegrator
+    (update form, Gauss-Lobatto nodes, SISolver substeps) with degree-p cross sections."""
+    P = smooth_sigma(8, p, 4, seed=50 + p, dt=0.05, inflow=False)
+    psi0 = np.zeros(P.psi_shape())
+    psi0[1:-1, 1:-1] = 0.05
+    with ref.open(to_oracle(P), P.dt, abs_tol=1e-14, max_its=100000, sigma_degree=p) as h:
+        want = h.idc_steps(psi0, P.source, P.dt, 2, 3, 2, si_abs_tol=1e-14)
+    with _ctx(P) as ctx:
+        psi = psi0.copy()
+        ctx.idc_integrate(psi, P.source, P.dt, 2, 3, 2, abi.SCATTER_IMPLICIT, abi.PREC_FP64, abs_tol=1e-14)
+    assert rel_err(psi[1:-1, 1:-1], want[1:-1, 1:-1]) < 1e-10
