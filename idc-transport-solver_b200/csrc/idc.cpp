@@ -138,9 +138,10 @@ Status Context::idc_integrate(double *psi, const double *Q, double dt, int64_t s
     if (K < 0 || K > 16) return bad(IDC_ERR_ARG, "IDC corrections must be in 0..16");
     if (!(dt > 0) || !std::isfinite(dt)) return bad(IDC_ERR_ARG, "IDC needs a finite positive dt");
     if (steps < 0) return bad(IDC_ERR_ARG, "negative step count");
-    if (reflect_mask) return bad(IDC_ERR_UNSUPPORTED, "IDC time stepping with reflecting boundaries");
-    if (periodic_) return bad(IDC_ERR_UNSUPPORTED, "IDC time stepping on a periodic grid");
     if (scattering != 0 && scattering != 1) return bad(IDC_ERR_ARG, "scattering must be 0 (explicit) or 1 (implicit)");
+    if (scattering == 0 && (reflect_mask || periodic_))
+        return bad(IDC_ERR_UNSUPPORTED, "IDC with explicit scattering on reflecting or periodic edges; implicit "
+                                        "scattering takes them");
     // explicit scattering: the lane or modal kernel's second source and the fused correction kernel (piecewise-
     // constant sigma, DG degree <= 2); implicit scattering (GMRES substeps) takes every input the solver takes
     if (scattering == 0 && !modal_family())
@@ -299,6 +300,16 @@ Status Context::idc_integrate(double *psi, const double *Q, double dt, int64_t s
     } else {
         // implicit: GMRES per substep (host-driven; the reference's Step_Nonhybrid, update form)
         for (int64_t s = 0; s < steps; ++s) {
+            // the step's initial stage with its boundary ghosts made consistent, as Step_Nonhybrid reflects it
+            // (idc.cpp:855-859) and Lmv synchronises periodic halos before reading them; the stages the
+            // substep solves return carry their reflections or periodic images already
+            if (reflect_mask) {
+                IDC_TRY_CUDA(launch_reflect_boundaries(dims(), reflect_mask, d_xi, d_eta, d_rmap, stage(0), stream));
+                launches += 1;
+            } else if (periodic_) {
+                IDC_TRY_CUDA(launch_periodic_halos(dims(), stage(0), stream));
+                launches += 1;
+            }
             for (int n = 1; n < M; ++n) {
                 const double h = t[n] - t[n - 1];
                 IDC_TRY(source(n, false, false));

@@ -88,9 +88,9 @@ int idc_set_ordinates(idc_ctx *ctx, int64_t nq, const double *xi, const double *
  * matrix of CalcA (linear_solvers/RKDG/SweepCellSolve/SweepLinearSolveSpec.cpp:298-318), Smv and Lmv
  * (operators/RKDG/TransportOperator.cpp:367-386, :1335-1359), with the tensor of Legendre triple products of
  * CrossSection::ComputeTensor (objects/RKDG/CrossSection.cpp:141-230).  They run on the elimination kernel in
- * FP64: sweeps, idc_smv, idc_lmv, source iteration and GMRES (its DSA preconditioner uses the cell averages);
- * FP32 sweeps, transposed operators, IDC time stepping, batches and reflecting edges return
- * IDC_ERR_UNSUPPORTED. */
+ * FP64: sweeps, idc_smv, idc_lmv, source iteration, GMRES (its DSA preconditioner uses the cell averages)
+ * and IDC time stepping with implicit scattering; FP32 sweeps, transposed operators, explicit-scattering
+ * IDC, batches and reflecting edges return IDC_ERR_UNSUPPORTED. */
 int idc_set_sigma(idc_ctx *ctx, const double *sigma_t, const double *sigma_s, int loc);
 
 /* Tile shape of the persistent sweep kernel: G ordinates x R rows per thread block (0 = automatic).
@@ -383,8 +383,10 @@ int idc_set_spin_limit(idc_ctx *ctx, int64_t polls);
  * the last reflection.  idc_source_iteration follows SISolver::Solve: psi starts at zero and the reflecting
  * edges' ghost cells are not copied from the source, so each sweep reads the reflections of the last.
  * idc_gmres_solve adds the reflecting edges' incoming ghost values to its unknowns and reaches the same fixed
- * point for every edge set.  FP64 and FP32 sweeps (the lane kernel); IDC_PREC_FP32_IR, transposed sweeps,
- * IDC time stepping, batches and ordinate-partitioned solves with reflecting boundaries return
+ * point for every edge set.  IDC time stepping with implicit scattering reflects each step's initial stage, as
+ * IDCIntegrator::Step_Nonhybrid does (time_integrators/RKDG/idc.cpp:855-859), and solves every substep this
+ * way.  FP64 and FP32 sweeps (the lane kernel); IDC_PREC_FP32_IR, transposed sweeps, explicit-scattering
+ * IDC, batches and ordinate-partitioned solves with reflecting boundaries return
  * IDC_ERR_UNSUPPORTED. */
 /* Periodic boundaries (the reference's Global::periodic, deck key `periodic`): 1 = on, 0 = off (the default).
  * A sweep reads the ghost cells as given, as the reference's does.  idc_source_iteration follows
@@ -393,8 +395,10 @@ int idc_set_spin_limit(idc_ctx *ctx, int64_t polls);
  * SynchronizeHalos, objects/Abstract/DensityFunction.cpp:927-960) and then copies the source into the interior
  * cells only.  idc_gmres_solve adds the edges' incoming ghost values to its unknowns and reaches the same fixed
  * point.  idc_lmv uses the opposite edges' cells as the upwind neighbours across an edge (Lmv synchronises its
- * input's halos first).  Reflecting edges, IDC_PREC_FP32_IR, adjoint solves, transposed operators, IDC time
- * stepping, batches and, for GMRES, ordinate-partitioned solves return IDC_ERR_UNSUPPORTED on a periodic grid. */
+ * input's halos first).  IDC time stepping with implicit scattering synchronises each step's initial stage
+ * and solves every substep this way.  Reflecting edges, IDC_PREC_FP32_IR, adjoint solves, transposed
+ * operators, explicit-scattering IDC, batches and, for GMRES, ordinate-partitioned solves return
+ * IDC_ERR_UNSUPPORTED on a periodic grid. */
 int idc_set_periodic(idc_ctx *ctx, int32_t periodic);
 
 #define IDC_EDGE_X_MIN 1

@@ -100,7 +100,7 @@ def test_reflecting_rejections():
             ctx.gmres_solve(P.source.copy(), P.dt, precision=abi.PREC_FP32_IR)
         assert e.value.code == abi.IDC_ERR_UNSUPPORTED
         with pytest.raises(abi.IdcError) as e:
-            ctx.idc_integrate(P.source.copy(), P.source, 0.1, 1, 3, 1, abi.SCATTER_IMPLICIT)
+            ctx.idc_integrate(P.source.copy(), P.source, 0.1, 1, 3, 1, abi.SCATTER_EXPLICIT)   # implicit: supported
         assert e.value.code == abi.IDC_ERR_UNSUPPORTED
         with pytest.raises(abi.IdcError) as e:
             with abi.Batch() as b:
