@@ -109,3 +109,31 @@ def test_reference_source_iteration_on_a_periodic_grid_through_plugin(plugged, p
             psi = h.source_iteration(P.source, P.dt)
             out[pattern] = h.pmv(psi)
     assert rel_err(out["gpu-wavefront"], out["wavefront"]) < 1e-11
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("reflect,periodic", [(15, False), (0, True)])
+def test_reference_idc_integrator_with_boundaries_through_plugin(plugged, reflect, periodic):
+    """IDCIntegrator::Step with reflecting edges (it reflects each step's initial stage) or on a periodic grid,
+    its SISolver substeps sweeping on the GPU: gpu-wavefront against wavefront."""
+    P = random_problem(10, 9, 1, 4, seed=62, dt=0.05, inflow=False, sigma_range=(0.5, 4.0))
+    psi0 = np.zeros(P.psi_shape())
+    psi0[1:-1, 1:-1] = 0.05
+    out = {}
+    for pattern in ("wavefront", "gpu-wavefront"):
+        with plugged.open(to_oracle(P), P.dt, pattern=pattern, abs_tol=1e-13, max_its=100000, reflect=reflect,
+                          periodic=periodic) as h:
+            out[pattern] = h.idc_steps(psi0, P.source, P.dt, 2, 3, 2, si_abs_tol=1e-13)
+    assert rel_err(out["gpu-wavefront"], out["wavefront"]) < 1e-11
+
+
+@pytest.mark.gpu
+def test_reference_source_iteration_at_dg_degree_3_through_plugin(plugged):
+    """The reference's SISolver::Solve at DG degree 3 (its sweep on the GPU's elimination kernel)."""
+    P = random_problem(9, 8, 3, 4, seed=63, dt=0.3, inflow=True, sigma_range=(0.5, 4.0))
+    out = {}
+    for pattern in ("wavefront", "gpu-wavefront"):
+        with plugged.open(to_oracle(P), P.dt, pattern=pattern, abs_tol=1e-12, max_its=5000) as h:
+            psi = h.source_iteration(P.source, P.dt)
+            out[pattern] = h.pmv(psi)
+    assert rel_err(out["gpu-wavefront"], out["wavefront"]) < 1e-11
