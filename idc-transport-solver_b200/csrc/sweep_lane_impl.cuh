@@ -317,60 +317,69 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
     const bool tin_ok = reader && tin != nullptr;
     double *out_trace = a.trace + (size_t)it_index * a.trace_stride + (size_t)o * P;
     const bool writer = has_consumer && rr == Rw - 1 && o < item.q_count;
-    auto load_trace = [&](int c, double (&v)[P]) {
+    auto load_trace = [&](int c, long long off, double (&v)[P]) {   // off = c * tin_col
         const bool p = tin_ok && c < nx;
-        const double *ptr = p ? tin + (size_t)c * tin_col : valid_addr;
+        const double *ptr = p ? tin + off : valid_addr;
 #pragma unroll
         for (int m = 0; m < P; ++m) v[m] = ld_relaxed_f64_if(ptr + m, p);
     };
 
-    // step t's inputs into stage t % D, one cp.async group per step; a cell outside the row gets zeros
-    auto prefetch = [&](int t) {
+    // Column addresses advance by a fixed stride per step: the prefetch of step t reads column t - rr, whose
+    // cell index (xi0 + xis (t - rr)) cstride + j and psi offset are kept running (prefetches come in step order).
+    const long long dcol = (long long)xis * (long long)cstride;   // cells between consecutive columns
+    const long long dsoff = dcol * (long long)plane;              // psi doubles between them
+    long long pf_cidx = ((long long)xi0 - (long long)xis * rr) * (long long)cstride + j;   // step 0's column
+    long long pf_soff = pf_cidx * (long long)plane + (long long)q * N;
+
+    // step t's inputs into stage slot = t % D, one cp.async group per step; a cell outside the row gets zeros
+    auto prefetch = [&](int t, int slot) {
         const int c = t - rr;
         const bool in = row_valid && c >= 0 && c < nx;
-        const size_t cidx = in ? (size_t)(xi0 + xis * c) * cstride + j : 0;
-        double *d = stage + (size_t)(t % D) * 32 * N;
+        const size_t cidx = in ? (size_t)pf_cidx : 0;
+        double *d = stage + (size_t)slot * 32 * N;
         if constexpr (PHI) {   // the cell's packed modal source of this quadrant (the same for the row segment)
             const double *g = a.modal_src + (cidx * 4 + quadrant) * N;
 #pragma unroll
             for (int k = 0; k < N; ++k) cp_async8_zfill(d + k, g + k, in && act);
         } else {
             const bool ps = in && act && a.src != nullptr;
-            const double *g = ps ? a.src + cidx * plane + (size_t)q * N : valid_addr;
+            const double *g = ps ? a.src + pf_soff : valid_addr;
 #pragma unroll
             for (int k = 0; k < N; ++k) cp_async8_zfill(d + k, g + k, ps);
         }
         if constexpr (SRC2) {
-            double *d2 = stage2 + (size_t)(t % D) * 32 * N;
-            const double *g2 = (in && act) ? a.src2 + cidx * plane + (size_t)q * N : valid_addr;
+            double *d2 = stage2 + (size_t)slot * 32 * N;
+            const double *g2 = (in && act) ? a.src2 + pf_soff : valid_addr;
 #pragma unroll
             for (int k = 0; k < N; ++k) cp_async8_zfill(d2 + k, g2 + k, in && act);
         }
-        cp_async8_zfill(sig + (size_t)(t % D) * 32, a.sigma_t + cidx, in);
+        cp_async8_zfill(sig + (size_t)slot * 32, a.sigma_t + cidx, in);
         if (has_scatter) {   // lane o == 0 of a row copies the cell's fused scattering moments (one copy per row)
             const bool pm = in && o == 0;
             const double *gm = pm ? a.phi_scatter + cidx * N : valid_addr;
-            double *dm = mom + (size_t)(t % D) * Rw * N;
+            double *dm = mom + (size_t)slot * Rw * N;
 #pragma unroll
             for (int k = 0; k < N; ++k) cp_async8_if(dm + k, gm + k, pm);
         }
         cp_commit();
+        pf_cidx += dcol;
+        pf_soff += dsoff;
     };
 
     // step t's raw inputs from its landed stage: the source (with the second source and the fused scattering
     // source) and sigma_t + 1/dt
-    auto load_inputs = [&](int t, double (&src)[N], double &st) {
-        const double *sp = stage + (size_t)(t % D) * 32 * N;
+    auto load_inputs = [&](int slot, double (&src)[N], double &st) {   // slot = t % D of step t
+        const double *sp = stage + (size_t)slot * 32 * N;
 #pragma unroll
         for (int k = 0; k < N; ++k) src[k] = sp[k];
         if constexpr (SRC2) {
-            const double *sp2 = stage2 + (size_t)(t % D) * 32 * N;
+            const double *sp2 = stage2 + (size_t)slot * 32 * N;
 #pragma unroll
             for (int k = 0; k < N; ++k) src[k] = fma(a.src2_scale, sp2[k], src[k]);
         }
-        st = sig[(size_t)(t % D) * 32] + a.inv_dt;
+        st = sig[(size_t)slot * 32] + a.inv_dt;
         if (has_scatter) {   // lane o == 0's copy of the cell's moments, handed to its row segment
-            const double *mp = mom + (size_t)(t % D) * Rw * N;
+            const double *mp = mom + (size_t)slot * Rw * N;
 #pragma unroll
             for (int k = 0; k < N; ++k) {
                 const double mk = __shfl_sync(kFullMask, o == 0 ? mp[k] : 0.0, rr * SEG);
@@ -415,21 +424,28 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
     // prologue: stages 0 .. D-1 in flight, step 0 prepared, step 1's raw inputs loaded, row 0's trace of
     // column 0 loaded
 #pragma unroll
-    for (int t = 0; t < D - 1; ++t) prefetch(t);
+    for (int t = 0; t < D - 1; ++t) prefetch(t, t);
     cp_wait<D - 2>();
     TC S[N];
     ModalRecip<P, TC> r;
     {
         double src0[N], st0;
-        load_inputs(0, src0, st0);
+        load_inputs(0, src0, st0);   // slot 0
         transform(src0, st0, S, r);
     }
     double srcn[N], stn;
     cp_wait<D - 3>();
-    load_inputs(1, srcn, stn);
-    prefetch(D - 1);
+    load_inputs(1, srcn, stn);   // slot 1
+    prefetch(D - 1, D - 1);
     double tnext[P];
-    load_trace(0, tnext);
+    load_trace(0, 0, tnext);
+    // per-step running values of the loop: the stage slots of steps s + D (= s % D) and s + 2, the trace column
+    // offsets s * tcol and (s + 1) * tin_col, and the finish column (s - rr - 1)'s cell index and psi offset
+    int sl = 0, sl2 = 2 % D;
+    long long s_tcol = 0, lt_off = (long long)tin_col;
+    const long long out_lag = (long long)(Rw - 1) * (long long)tcol;
+    long long fin_cidx = ((long long)xi0 - (long long)xis * (rr + 1)) * (long long)cstride + j;
+    long long fin_ooff = fin_cidx * (long long)plane + (long long)item.q_begin * N;
     TC gprev[P], Zp[N];
 #pragma unroll
     for (int m = 0; m < P; ++m) gprev[m] = TC(0);
@@ -462,13 +478,13 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
         }
         {   // re-arm the consumed column for the next sweep
             const bool p = has_dep && reader && s < nx;
-            double *ptr = p ? dep_trace + (size_t)s * tcol : out_trace;
+            double *ptr = p ? dep_trace + s_tcol : out_trace;
 #pragma unroll
             for (int m = 0; m < P; ++m) st_relaxed_f64_if(ptr + m, sentinel_value(), p);
         }
 #pragma unroll
         for (int m = 0; m < P; ++m) g[m] = (rr == 0) ? TC(tnext[m]) : g[m];
-        load_trace(s + 1, tnext);
+        load_trace(s + 1, lt_off, tnext);
 
         // ---- the chain of step s ----
         TC Z[N], fn[P], gout[P];
@@ -483,7 +499,7 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
         {   // traces out: relaxed stores, each value its own flag
             const int cout = s - (Rw - 1);
             const bool p = writer && cout >= 0 && cout < nx;
-            double *ptr = p ? out_trace + (size_t)cout * tcol : out_trace;
+            double *ptr = p ? out_trace + (s_tcol - out_lag) : out_trace;
 #pragma unroll
             for (int m = 0; m < P; ++m) st_relaxed_f64_if(ptr + m, double(gout[m]), p);
         }
@@ -492,7 +508,7 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
         {   // (at s = 0 nothing is valid: Zp is zero and no store is made)
             const int cp = c - 1;
             const bool inrow = row_valid && cp >= 0 && cp < nx;
-            const size_t cidx = inrow ? (size_t)(xi0 + xis * cp) * cstride + j : 0;
+            const size_t cidx = inrow ? (size_t)fin_cidx : 0;
             TC x[N];
             if constexpr (PHI) {
 #pragma unroll
@@ -523,7 +539,7 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
             __syncwarp();
             if constexpr (!PHI) {   // row rr's segment: one bulk copy by lane o == 0
                 const bool pb = bulk_out && o == 0 && inrow;
-                double *dst = pb ? a.out + cidx * plane + (size_t)item.q_begin * N : out_trace;
+                double *dst = pb ? a.out + fin_ooff : out_trace;
                 bulk_store_if(dst, ob + (size_t)rr * SEG * N, (unsigned)(item.q_count * N * sizeof(double)), pb);
                 bulk_commit();
             }
@@ -561,8 +577,14 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
         // ---- step s + 2's raw inputs (copied D - 2 iterations ago), the copies of step s + D ----
         if (lane_out) store_psi_lanes(s - 1);
         cp_wait<D - 3>();
-        load_inputs(s + 2, srcn, stn);
-        prefetch(s + D);   // into the stage of step s (read two iterations ago)
+        load_inputs(sl2, srcn, stn);   // step s + 2
+        prefetch(s + D, sl);           // into the stage of step s (read two iterations ago)
+        sl = sl + 1 == D ? 0 : sl + 1;
+        sl2 = sl2 + 1 == D ? 0 : sl2 + 1;
+        s_tcol += (long long)tcol;
+        lt_off += (long long)tin_col;
+        fin_cidx += dcol;
+        fin_ooff += dsoff;
     }
     cp_wait<0>();
     bulk_wait<0>();
