@@ -57,8 +57,10 @@ public:
     Status l2dist(const double *a, const double *b, double *out_host);
     Status source_iteration(const double *src, double *psi_out, double dt, double abs_tol, int64_t max_its,
                             int precision, int64_t *iters, double *err);
+    // phi_guess (optional, moment-sized, device): GMRES starts from it instead of zero (reflecting or periodic
+    // edges and IDC_PREC_FP32_IR start from zero)
     Status gmres_peierls(const double *src, double *psi_out, double dt, double abs_tol, int restart, int64_t max_its,
-                         int precision, int64_t *iters, double *resid);
+                         int precision, int64_t *iters, double *resid, const double *phi_guess = nullptr);
     Status apply_peierls(const double *x, double *y, double *tmp_phi, double dt, int precision);
     // precision IDC_PREC_FP32_IR of gmres_peierls: FP32 Krylov solves inside FP64 iterative refinement
     Status gmres_peierls_ir(const double *src, double *psi_out, double dt, double abs_tol, int restart,
@@ -71,7 +73,7 @@ public:
     template <typename Op>
     Status gmres(Op apply, const double *b, double *x, double abs_tol, int restart, int64_t max_its, int64_t *iters,
                  double *resid, bool *converged, int dsa_mode = 0,   // 0 none, 1 DSA, 2 transposed DSA
-                 size_t n_extra = 0);
+                 size_t n_extra = 0, bool warm = false);   // warm: x holds the initial guess
     Status set_preconditioner(int kind, int inner_steps);   // 0 none, 1 DSA
     // IDC time integration (idc.cpp): psi (device, in/out) advanced `steps` steps of size dt with M
     // Gauss-Lobatto nodes and K corrections; scattering 0 = explicit (IMEX, one sweep per substep, CUDA

@@ -298,7 +298,9 @@ Status Context::idc_integrate(double *psi, const double *Q, double dt, int64_t s
         }
         IDC_TRY(check_device_error());
     } else {
-        // implicit: GMRES per substep (host-driven; the reference's Step_Nonhybrid, update form)
+        // implicit: GMRES per substep (host-driven; the reference's Step_Nonhybrid, update form); a guess costs
+        // one operator application where it is used
+        const bool warm_start = !(reflect_mask || periodic_ || precision == IDC_PREC_FP32_IR);
         for (int64_t s = 0; s < steps; ++s) {
             // the step's initial stage with its boundary ghosts made consistent, as Step_Nonhybrid reflects it
             // (idc.cpp:855-859) and Lmv synchronises periodic halos before reading them; the stages the
@@ -310,23 +312,27 @@ Status Context::idc_integrate(double *psi, const double *Q, double dt, int64_t s
                 IDC_TRY_CUDA(launch_periodic_halos(dims(), stage(0), stream));
                 launches += 1;
             }
+            // GMRES starts from the previous node's moments in the prediction and from the same node's moments one
+            // level down in the corrections (the reference's source iteration keeps its psi between substeps)
             for (int n = 1; n < M; ++n) {
                 const double h = t[n] - t[n - 1];
                 IDC_TRY(source(n, false, false));
+                IDC_TRY(pmv(1.0, 0.0, stage(n - 1), phi(n)));
                 int64_t its = 0;
                 double r = 0;
-                IDC_TRY(gmres_peierls(src, stage(n), h * dt, abs_tol, restart, max_its, precision, &its, &r));
-                sweeps += its + 2;
+                IDC_TRY(gmres_peierls(src, stage(n), h * dt, abs_tol, restart, max_its, precision, &its, &r, phi(n)));
+                sweeps += its + (warm_start ? 3 : 2);
             }
             for (int p = 0; p < K; ++p) {
                 for (int l = 0; l < M; ++l) IDC_TRY(residual(l));
-                for (int n = 1; n < M; ++n) {
+                for (int n = 1; n < M; ++n) {   // phi(n) = P stage(n) of the level before (residual)
                     const double h = t[n] - t[n - 1];
                     IDC_TRY(source(n, true, false));
                     int64_t its = 0;
                     double r = 0;
-                    IDC_TRY(gmres_peierls(src, stage(n), h * dt, abs_tol, restart, max_its, precision, &its, &r));
-                    sweeps += its + 2;
+                    IDC_TRY(gmres_peierls(src, stage(n), h * dt, abs_tol, restart, max_its, precision, &its, &r,
+                                          phi(n)));
+                    sweeps += its + (warm_start ? 3 : 2);
                 }
             }
             IDC_TRY_CUDA(cudaMemcpyAsync(stage(0), stage(M - 1), sizeof(double) * np, cudaMemcpyDeviceToDevice, stream));
@@ -392,8 +398,8 @@ Status Context::adjoint_idc(const double *psi0, const double *Q, double dt, int6
     double *lam = adj_idc_bufs_[b0 + 3 * M], *tmp = adj_idc_bufs_[b0 + 3 * M + 1];
     double *src = adj_idc_bufs_[b0 + 3 * M + 2], *pbar = adj_idc_bufs_[b0 + 3 * M + 3];
     double *inbar = adj_idc_bufs_[b0 + 3 * M + 4], *zsum = adj_idc_bufs_[b0 + 3 * M + 5];   // zsum: moment-sized use
-    IDC_TRY(ensure_phi_buffers(11));
-    double *Lam = phi_buf(9), *phi = phi_buf(10);
+    IDC_TRY(ensure_phi_buffers(16));   // 15: the warm-start moments of each solve
+    double *Lam = phi_buf(9), *phi = phi_buf(10), *guess = phi_buf(15);
     int64_t nsolve = 0;
     // stage ghost cells hold the inflow (Q's ghost cells), as in idc_integrate; the solves write interiors only
     for (int p = 0; p <= K; ++p)
@@ -413,9 +419,12 @@ Status Context::adjoint_idc(const double *psi0, const double *Q, double dt, int6
             }
         IDC_TRY_CUDA(launch_idc_source(dims(), tm, Q, src, stream));
         launches += 1;
+        // GMRES from the moments idc_integrate starts from: the previous node's stage (prediction), the same
+        // node's stage one level down (corrections)
+        IDC_TRY(pmv(1.0, 0.0, p == 0 ? stage(0, n - 1) : stage(p - 1, n), guess));
         int64_t its = 0;
         double r = 0.0;
-        IDC_TRY(gmres_peierls(src, stage(p, n), h * dt, abs_tol, restart, max_its, precision, &its, &r));
+        IDC_TRY(gmres_peierls(src, stage(p, n), h * dt, abs_tol, restart, max_its, precision, &its, &r, guess));
         ++nsolve;
         return Status::ok();
     };

@@ -60,7 +60,8 @@ Status Context::apply_peierls(const double *x, double *y, double *tmp_phi, doubl
 // linear) and x = Z y.
 template <typename Op>
 Status Context::gmres(Op apply, const double *b, double *x, double abs_tol, int restart, int64_t max_its,
-                      int64_t *iters_out, double *resid_out, bool *converged_out, int dsa_mode, size_t n_extra) {
+                      int64_t *iters_out, double *resid_out, bool *converged_out, int dsa_mode, size_t n_extra,
+                      bool warm) {
     const bool dsa = dsa_mode != 0;
     if (restart < 1 || restart > 60) return bad(IDC_ERR_ARG, "gmres restart must be in 1..60");
     const size_t n = phi_len() + n_extra;
@@ -92,9 +93,14 @@ Status Context::gmres(Op apply, const double *b, double *x, double abs_tol, int 
         launches += 2;
     }
 
-    IDC_TRY_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, stream));
-    // r = b - A x = b for the zero initial guess
-    IDC_TRY_CUDA(cudaMemcpyAsync(Vc(0), b, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream));
+    if (warm) {   // r = b - A x for the caller's initial guess
+        IDC_TRY(apply(x, Vc(0)));
+        IDC_TRY_CUDA(launch_axpby(1.0, b, -1.0, Vc(0), n, stream));
+        launches += 1;
+    } else {      // r = b - A x = b for the zero initial guess
+        IDC_TRY_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, stream));
+        IDC_TRY_CUDA(cudaMemcpyAsync(Vc(0), b, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream));
+    }
     double beta = 0.0;
     IDC_TRY(dot_host(Vc(0), Vc(0), n, &beta));
     beta = std::sqrt(beta);
@@ -272,7 +278,8 @@ Status Context::gmres_peierls_boundary(const double *src, double *psi_out, doubl
 
 // (I - P L^{-1} S) phi = P L^{-1} Q (PETScPeierlsSolver.cpp:423-572), then psi = L^{-1}(S phi + Q).
 Status Context::gmres_peierls(const double *src, double *psi_out, double dt, double abs_tol, int restart,
-                              int64_t max_its, int precision, int64_t *iters_out, double *resid_out) {
+                              int64_t max_its, int precision, int64_t *iters_out, double *resid_out,
+                              const double *phi_guess) {
     if (!use_warp_kernel) return bad(IDC_ERR_UNSUPPORTED, "GMRES needs the warp-pipelined sweep kernel");
     if (reflect_mask || periodic_)
         return gmres_peierls_boundary(src, psi_out, dt, abs_tol, restart, max_its, precision, iters_out, resid_out);
@@ -285,7 +292,10 @@ Status Context::gmres_peierls(const double *src, double *psi_out, double dt, dou
     bool converged = false;
     double resid = 0.0;
     auto op = [&](const double *in, double *out) { return apply_peierls(in, out, tmp, dt, precision); };
-    IDC_TRY(gmres(op, b, x, abs_tol, restart, max_its, iters_out, &resid, &converged, precond_kind == 1 ? 1 : 0));
+    if (phi_guess)
+        IDC_TRY_CUDA(cudaMemcpyAsync(x, phi_guess, sizeof(double) * phi_len(), cudaMemcpyDeviceToDevice, stream));
+    IDC_TRY(gmres(op, b, x, abs_tol, restart, max_its, iters_out, &resid, &converged, precond_kind == 1 ? 1 : 0, 0,
+                  phi_guess != nullptr));
     // psi = L^{-1} (S phi + Q)  (PETScPeierlsSolver.cpp:504-505)
     IDC_TRY(sweep(src, psi_out, dt, nullptr, precision, x, 1.0));
     IDC_TRY(check_device_error());
@@ -464,11 +474,11 @@ Status Context::adjoint_transient(const double *psi0, const double *Q, double dt
     auto seg = [&](int64_t k) { return transient_bufs_[(size_t)(M + k - 1)]; };   // k = 1..K
     double *lam = transient_bufs_[(size_t)(M + K)], *b = transient_bufs_[(size_t)(M + K + 1)];
     double *src = transient_bufs_[(size_t)(M + K + 2)];
-    IDC_TRY(ensure_phi_buffers(11));
+    IDC_TRY(ensure_phi_buffers(16));   // 15: the warm-start moments of each step's solve
     double *Lam = phi_buf(9), *phi = phi_buf(10);
     int64_t nsolve = 0;
 
-    // one step: out = A^{-1} (in / dt + Q)
+    // one step: out = A^{-1} (in / dt + Q), GMRES from the moments of `in` (the previous step's solution)
     auto step = [&](const double *in, double *out) -> Status {
         IdcTerms tm{};
         tm.n = 1;
@@ -476,9 +486,10 @@ Status Context::adjoint_transient(const double *psi0, const double *Q, double dt
         tm.c[0] = 1.0 / dt;
         IDC_TRY_CUDA(launch_idc_source(dims(), tm, Q, src, stream));
         launches += 1;
+        IDC_TRY(pmv(1.0, 0.0, in, phi_buf(15)));
         int64_t its = 0;
         double r = 0.0;
-        IDC_TRY(gmres_peierls(src, out, dt, abs_tol, restart, max_its, precision, &its, &r));
+        IDC_TRY(gmres_peierls(src, out, dt, abs_tol, restart, max_its, precision, &its, &r, phi_buf(15)));
         ++nsolve;
         return Status::ok();
     };
