@@ -56,6 +56,8 @@ Context::~Context() {
     cudaFree(d_w);
     cudaFree(d_sigma_t);
     cudaFree(d_sigma_s);
+    cudaFree(other_sched_.d_items);
+    cudaFree(other_sched_.d_trace);
     cudaFree(d_sig_mom_);
     cudaFree(d_tens_t_);
     cudaFree(d_tens_s_);
@@ -159,8 +161,7 @@ Status Context::set_ordinates(int64_t nq_in, const double *xi, const double *eta
     nq = nq_in;
     for (int k = 0; k < 5; ++k) quad[k] = qb[k];
     have_ordinates = true;
-    n_items = 0;   // schedule rebuilt lazily
-    occupancy_precision = -1;
+    invalidate_schedules();   // rebuilt lazily
     if (reflect_mask) return update_reflect_map();
     return Status::ok();
 }
@@ -492,8 +493,7 @@ Status Context::set_tiling(int G, int R) {
     if (G < 0 || R < 0) return bad(IDC_ERR_ARG, "set_tiling: negative tile size");
     user_G = G;
     user_R = R;
-    n_items = 0;
-    occupancy_precision = -1;
+    invalidate_schedules();
     return Status::ok();
 }
 
@@ -517,8 +517,7 @@ Status Context::set_tile_shape(int s, int w) {
         tune_seg = s;
         tune_wn = w;
     }
-    n_items = 0;
-    occupancy_precision = -1;
+    invalidate_schedules();
     return Status::ok();
 }
 
@@ -617,6 +616,26 @@ static void choose_warp_tiling(int qmax, int user_G, int user_rows, int max_wn, 
 }
 
 // Work items in row-block-major order: (row block, quadrant, ordinate chunk).
+void Context::use_schedule(int variant) {
+    if (variant == sched_variant_) return;
+    ScheduleSlot &o = other_sched_;
+    std::swap(tiling, o.tiling);
+    std::swap(d_items, o.d_items);
+    std::swap(d_trace, o.d_trace);
+    std::swap(trace_len, o.trace_len);
+    std::swap(smem, o.smem);
+    std::swap(n_items, o.n_items);
+    std::swap(items_per_rb, o.items_per_rb);
+    for (int k = 0; k < 5; ++k) std::swap(quad_slots[k], o.quad_slots[k]);
+    std::swap(seg, o.seg);
+    std::swap(wn, o.wn);
+    std::swap(active, o.active);
+    std::swap(grid, o.grid);
+    std::swap(block, o.block);
+    std::swap(occupancy_precision, o.occupancy_precision);
+    sched_variant_ = variant;
+}
+
 Status Context::build_schedule(int precision) {
     if (n_items > 0 && occupancy_precision == precision) return Status::ok();
     int qmax = 0;
@@ -626,7 +645,8 @@ Status Context::build_schedule(int precision) {
     active = kernel_for(precision);
     const int max_wn = active == kModal ? sweep_modal_max_wn(P) : active == kLane ? 1 : 7;
     const bool modal_like = active == kModal || active == kLane;
-    if (use_warp_kernel && tune_seg > 0) {
+    // a fixed or autotuned tile shape is the full sweeps'; the moments-only sweeps keep the default rule
+    if (use_warp_kernel && tune_seg > 0 && sched_variant_ == 0) {
         seg = tune_seg;
         if (active == kLane && !sweep_lane_supports(P, precision, seg)) seg = 16;
         wn = tune_wn > 0 ? std::min(tune_wn, max_wn) : (active == kModal ? sweep_modal_default_wn(P) : 1);
@@ -637,6 +657,13 @@ Status Context::build_schedule(int precision) {
     } else if (use_warp_kernel) {
         choose_warp_tiling(qmax, user_G, user_R, max_wn, active == kModal ? sweep_modal_default_wn(P) : max_wn,
                            modal_like, &G, &seg, &wn);
+        if (active == kLane && sched_variant_ == 0 && P == 3 && user_G == 0 && user_R == 0) {
+            // full lane sweeps at DG degree 2: 16-wide segments (fewer row blocks, 16-wide moment sums) were the
+            // fastest at S8, S12 and S16 on 256^2 grids, ahead of the narrower segments of the lane-occupancy rule
+            seg = 16;
+            const int nch = (qmax + seg - 1) / seg;
+            G = (qmax + nch - 1) / nch;
+        }
         if (active == kLane && !sweep_lane_supports(P, precision, seg)) {   // 32 lanes: 16 and two chunks
             seg = 16;
             const int nch = (qmax + seg - 1) / seg;
@@ -700,13 +727,20 @@ Status Context::build_schedule(int precision) {
 
     IDC_TRY_CUDA(cudaSetDevice(device));
     cudaFree(d_items);
-    cudaFree(d_sync);
     d_items = nullptr;
-    d_sync = nullptr;
     IDC_TRY_CUDA(cudaMalloc(&d_items, sizeof(SweepItem) * items.size()));
     IDC_TRY_CUDA(cudaMemcpy(d_items, items.data(), sizeof(SweepItem) * items.size(), cudaMemcpyHostToDevice));
-    IDC_TRY_CUDA(cudaMalloc(&d_sync, sizeof(int) * (2 + items.size())));
-    IDC_TRY_CUDA(cudaMemset(d_sync, 0, sizeof(int) * (2 + items.size())));
+    if (sync_cap_ < 2 + items.size()) {   // shared by both schedules: the larger one's progress flags
+        int err_word = 0;
+        if (d_sync) IDC_TRY_CUDA(cudaMemcpy(&err_word, d_sync + 1, sizeof(int), cudaMemcpyDeviceToHost));
+        cudaFree(d_sync);
+        d_sync = nullptr;
+        sync_cap_ = 0;
+        IDC_TRY_CUDA(cudaMalloc(&d_sync, sizeof(int) * (2 + items.size())));
+        sync_cap_ = 2 + items.size();
+        IDC_TRY_CUDA(cudaMemset(d_sync, 0, sizeof(int) * sync_cap_));
+        IDC_TRY_CUDA(cudaMemcpy(d_sync + 1, &err_word, sizeof(int), cudaMemcpyHostToDevice));   // kept until checked
+    }
 
     if (use_warp_kernel) {
         cudaFree(d_trace);
@@ -801,6 +835,9 @@ Status Context::check_device_error() {
         IDC_TRY_CUDA(cudaMemsetAsync(d_sync + 1, 0, sizeof(int), stream));
         if (d_trace)
             IDC_TRY_CUDA(launch_fill_u64(reinterpret_cast<unsigned long long *>(d_trace), trace_len, kTraceSentinel, stream));
+        if (other_sched_.d_trace)   // the other variant's schedule: its sweeps may have been the abandoned ones
+            IDC_TRY_CUDA(launch_fill_u64(reinterpret_cast<unsigned long long *>(other_sched_.d_trace),
+                                         other_sched_.trace_len, kTraceSentinel, stream));
         IDC_TRY_CUDA(cudaStreamSynchronize(stream));
         return bad(IDC_ERR_TIMEOUT, "a device-side wait gave up (bounded spin); the sweep was abandoned");
     }
@@ -831,6 +868,7 @@ Status Context::sweep(const double *src, double *out, double dt, double *phi, in
     }
     if (reflect_mask && !in_reflect_)
         return sweep_reflecting(src, out, dt, phi, precision, phi_scatter, scatter_scale, adjoint, src2);
+    use_schedule((!src && !out && phi && !adjoint && !src2 && moments_fast_path) ? 1 : 0);
     IDC_TRY(build_schedule(precision));
     IDC_TRY_CUDA(cudaSetDevice(device));
 

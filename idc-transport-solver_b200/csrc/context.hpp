@@ -181,6 +181,29 @@ public:
     int grid = 0, block = 0;
     size_t smem = 0;
     int occupancy_precision = -1;
+    size_t sync_cap_ = 0;          // ints allocated at d_sync (shared by both schedules below)
+    // Two cached schedules, one per sweep variant: 0 = sweeps with a source or a psi output, 1 = the moments-only
+    // Krylov sweeps (no source, psi not stored).  They want different tile widths (the full lane sweep at DG
+    // degree 2 is fastest with 16-wide segments, the moments-only one with narrow ones), and GMRES alternates
+    // between them, so the members above hold the current variant's schedule and `other_sched_` the other's;
+    // `use_schedule` swaps them.  d_sync (the error word and progress flags) is shared.
+    struct ScheduleSlot {
+        SweepTiling tiling{};
+        SweepItem *d_items = nullptr;
+        double *d_trace = nullptr;
+        size_t trace_len = 0, smem = 0;
+        int n_items = 0, items_per_rb = 0, quad_slots[5] = {0, 0, 0, 0, 0}, seg = 0, wn = 0, active = 3, grid = 0,
+            block = 0, occupancy_precision = -1;
+    };
+    ScheduleSlot other_sched_;
+    int sched_variant_ = 0;
+    void use_schedule(int variant);
+    void invalidate_schedules() {
+        n_items = 0;
+        occupancy_precision = -1;
+        other_sched_.n_items = 0;
+        other_sched_.occupancy_precision = -1;
+    }
 
     float last_sweep_ms = 0.f;
     bool capturing = false;   // a CUDA graph capture is open on `stream`: no timing events, no host syncs
