@@ -149,6 +149,21 @@ Status Context::idc_integrate(double *psi, const double *Q, double dt, int64_t s
                                         "piecewise-constant cross sections); implicit scattering takes these inputs");
     std::vector<double> t, W;
     idc_nodes_and_weights(M, t, W);
+    // The IMEX sweeps (a second source and the scattering term) at DG degree 1 are faster on the modal kernel
+    // than on the lane kernel's second-source instance (measured per step: 512^2 Q1 S12 23.3-23.7 ms against
+    // 28-34 ms; 256^2 Q1 S12 7.8-8.6 against 10.5-11.8 ms; at degree 2 the lane kernel's default is the
+    // fastest).  Without a tile shape of the caller's the integration runs on the modal (8, 5) shape and the
+    // default comes back when it returns, on every path.
+    struct TileRestore {
+        Context *c = nullptr;
+        ~TileRestore() {
+            if (c) c->set_tile_shape(0, 0);
+        }
+    } tile_restore;
+    if (scattering == 0 && P == 2 && tune_seg == 0 && tune_wn == 0) {
+        IDC_TRY(set_tile_shape(8, 5));
+        tile_restore.c = this;
+    }
 
     // buffers: M stages, M residuals, one source (psi-sized); M moments, M previous-level moments, one
     // scattering combination (moment-sized)
