@@ -657,10 +657,11 @@ Status Context::build_schedule(int precision) {
     } else if (use_warp_kernel) {
         choose_warp_tiling(qmax, user_G, user_R, max_wn, active == kModal ? sweep_modal_default_wn(P) : max_wn,
                            modal_like, &G, &seg, &wn);
-        if (active == kLane && sched_variant_ == 0 && P == 3 && user_G == 0 && user_R == 0) {
-            // full lane sweeps at DG degree 2: 16-wide segments (fewer row blocks, 16-wide moment sums) were the
-            // fastest at S8, S12 and S16 on 256^2 grids, ahead of the narrower segments of the lane-occupancy rule
-            seg = 16;
+        if (active == kLane && sched_variant_ == 0 && user_G == 0 && user_R == 0 && (P == 3 || (P == 2 && qmax <= 24))) {
+            // full lane sweeps: at DG degree 2 16-wide segments (fewer row blocks, 16-wide moment sums) were the
+            // fastest at S8, S12 and S16 on 256^2 grids; at degree 1 8-wide ones for up to 24 ordinates per quadrant
+            // (S8, S12: 4-7% ahead of 4-wide, also on the 64^2 lattice), while S16's 36 keep the 4-wide rule
+            seg = P == 3 ? 16 : 8;
             const int nch = (qmax + seg - 1) / seg;
             G = (qmax + nch - 1) / nch;
         }

@@ -234,7 +234,7 @@ int idc_sweep_fused(idc_ctx *ctx, const double *source, double *result, double d
  * rows; seg 4, 8 or 16; FP64 sweeps); warps 1..7 the modal kernel with that many compute warps stacked per
  * thread block (at most 5 at DG degree 2 and 7 below, fewer if the shape's shared memory would not fit).
  * 0, 0 restores the default (the lane kernel for FP64, the modal kernel for the FP32 modes; 16-wide lane
- * segments at DG degree 2).  The shape applies to sweeps with a source or a psi output; the moments-only
+ * segments at DG degree 2, 8-wide at degree 1 for up to 24 ordinates per quadrant).  The shape applies to sweeps with a source or a psi output; the moments-only
  * sweeps of the Krylov iterations keep their own default (narrow segments, which suit them).  Results do
  * not depend on it beyond the last bits of the moments. */
 int idc_set_tile_shape(idc_ctx *ctx, int32_t seg, int32_t warps);
