@@ -240,7 +240,7 @@ int idc_sweep_fused(idc_ctx *ctx, const double *source, double *result, double d
 int idc_set_tile_shape(idc_ctx *ctx, int32_t seg, int32_t warps);
 
 /* Autotuner: times every tile shape of both kernels on this context's problem with `source` (device psi
- * array) and keeps the fastest (reported in *seg, *warps; warps = 0: the lane kernel). */
+ * array; plain sweeps: the IMEX sweeps of idc_idc_integrate may prefer another shape) and keeps the fastest (reported in *seg, *warps; warps = 0: the lane kernel). */
 int idc_autotune(idc_ctx *ctx, const double *source, double dt, int precision, int32_t *seg, int32_t *warps);
 
 /* A batch of independent problems (contexts on one GPU) swept together: one persistent launch per DG
