@@ -455,8 +455,13 @@ def extra_batched(abi, torch, dev, n_problems=64):
             for c in ctxs:
                 b.add(c)
             S, O, F = [x.data_ptr() for x in srcs], [x.data_ptr() for x in outs], [x.data_ptr() for x in phis]
+            for _ in range(2):
+                b.sweep(S, O, F, math.inf, abi.PREC_FP64)
+            default_ms = min((b.sweep(S, O, F, math.inf, abi.PREC_FP64), b.last_ms())[1] for _ in range(3))
+            default_shapes = {f"dg{p}": list(b.get_shape(p, abi.PREC_FP64)) for p in (1, 2)}
             b.autotune(S, O, math.inf, abi.PREC_FP64)
-            res = {}
+            res = {"fp64_default_shapes": {"device_ms": default_ms, "shapes_seg_warps": default_shapes},
+                   "fp64_shapes_seg_warps": {f"dg{p}": list(b.get_shape(p, abi.PREC_FP64)) for p in (1, 2)}}
             for name, prec in (("fp64", abi.PREC_FP64), ("fp32_refined", abi.PREC_FP32_REFINED)):
                 for _ in range(2):
                     b.sweep(S, O, F, math.inf, prec)

@@ -36,10 +36,14 @@ Status bad(int code, const std::string &m) {
     return s;
 }
 
-// Default shape: the narrowest segment with the best lane use, the single problem's default warps.
-void default_shape(int P, int qmax, int *seg, int *wn) {
+// Default shape: the single problem's default kernel and rule.  FP64: the lane kernel (warps = 0) with 16-wide
+// segments at DG degree 2, 8-wide at degree 1 for up to 24 ordinates per quadrant, else the narrowest segment
+// with the best lane use.  FP32_REFINED: the modal kernel, narrowest best segment, its default warps.
+void default_shape(int P, int precision, int qmax, int *seg, int *wn) {
+    const bool lane = precision == IDC_PREC_FP64;
     double best = -1.0;
     for (int cand : {4, 8, 16, 32}) {
+        if (lane && cand == 32) break;
         const int nch = (qmax + cand - 1) / cand;
         const double eff = (double)qmax / (nch * cand);
         if (eff > best + 1e-9) {
@@ -47,7 +51,8 @@ void default_shape(int P, int qmax, int *seg, int *wn) {
             *seg = cand;
         }
     }
-    *wn = sweep_modal_default_wn(P);
+    if (lane && (P == 3 || (P == 2 && qmax <= 24))) *seg = P == 3 ? 16 : 8;
+    *wn = lane ? 0 : sweep_modal_default_wn(P);
 }
 
 int qmax_of(const Context &c) {
@@ -90,8 +95,11 @@ Status Batch::add(Context *c) {
 Status Batch::build_group(Group &g, int precision) {
     Context &c0 = *members[g.members[0]];
     g.G = g.seg;
-    g.wn = sweep_modal_fit_wn(c0.P, precision, g.wn, g.G, g.seg);
-    const int seg = g.seg, wn = g.wn, rw = 32 / seg, rows_cta = wn * rw;
+    const bool lane = g.wn == 0;   // the lane kernel (FP64): one warp per item, 32 / seg rows
+    if (lane && (precision != IDC_PREC_FP64 || !sweep_lane_supports(c0.P, 0, g.seg)))
+        return bad(IDC_ERR_UNSUPPORTED, "batched lane sweeps: FP64, seg 4, 8 or 16");
+    if (!lane) g.wn = sweep_modal_fit_wn(c0.P, precision, g.wn, g.G, g.seg);
+    const int seg = g.seg, wn = g.wn, rw = 32 / seg, rows_cta = lane ? rw : wn * rw;
     std::vector<std::vector<SweepItem>> per(g.members.size());
     std::vector<int> nrb(g.members.size()), ipr(g.members.size());
     for (size_t m = 0; m < g.members.size(); ++m) {
@@ -150,10 +158,17 @@ Status Batch::build_group(Group &g, int precision) {
         IDC_TRY_CUDA(cudaMalloc(&g.inflow[m], sizeof(double) * (size_t)(c.nx + c.ny) * c.nq * c.P));
     }
     int per_sm = 0;
-    g.smem = sweep_modal_smem_bytes(c0.P, precision, wn, g.G, seg);
-    IDC_TRY_CUDA(sweep_modal_occupancy(c0.P, precision, seg, sweep_modal_threads(c0.P, wn), g.smem, &per_sm));
-    if (per_sm < 1) return bad(IDC_ERR_UNSUPPORTED, "batched sweep kernel does not fit on an SM");
-    g.grid = std::min(g.n_items, per_sm * c0.num_sms);
+    if (lane) {   // shared memory fixed per kernel instance (set by the launcher); one item per warp at a time
+        g.smem = 0;
+        IDC_TRY_CUDA(sweep_lane_batched_occupancy(c0.P, seg, &per_sm));
+        if (per_sm < 1) return bad(IDC_ERR_UNSUPPORTED, "batched sweep kernel does not fit on an SM");
+        g.grid = std::min((g.n_items + sweep_lane_warps() - 1) / sweep_lane_warps(), per_sm * c0.num_sms);
+    } else {
+        g.smem = sweep_modal_smem_bytes(c0.P, precision, wn, g.G, seg);
+        IDC_TRY_CUDA(sweep_modal_occupancy(c0.P, precision, seg, sweep_modal_threads(c0.P, wn), g.smem, &per_sm));
+        if (per_sm < 1) return bad(IDC_ERR_UNSUPPORTED, "batched sweep kernel does not fit on an SM");
+        g.grid = std::min(g.n_items, per_sm * c0.num_sms);
+    }
     g.precision = precision;
     IDC_TRY_CUDA(cudaStreamSynchronize(stream()));
     return Status::ok();
@@ -190,7 +205,7 @@ Status Batch::launch_group(Group &g, const double *const *srcs, double *const *o
         a.n_refine = 1;
         a.seg = g.seg;
         a.wn = g.wn;
-        a.R = g.wn * (32 / g.seg);
+        a.R = (g.wn == 0 ? 1 : g.wn) * (32 / g.seg);
         a.trace = g.trace[m];
         a.trace_stride = (size_t)c.nx * g.G * c.P;
         a.next_item = g.d_sync;
@@ -233,7 +248,10 @@ Status Batch::launch_group(Group &g, const double *const *srcs, double *const *o
         IDC_TRY_CUDA(launch_batched_helpers(c0.P, g.precision != IDC_PREC_FP32_REFINED, g.d_table, (int)table.size(),
                                             true, false, st));
     IDC_TRY_CUDA(cudaMemsetAsync(g.d_sync, 0, sizeof(int), st));
-    IDC_TRY_CUDA(launch_sweep_modal_batched(c0.P, g.precision, launch, g.d_table, g.grid, g.smem, st));
+    if (g.wn == 0)
+        IDC_TRY_CUDA(launch_sweep_lane_batched(c0.P, launch, g.d_table, g.grid, st));
+    else
+        IDC_TRY_CUDA(launch_sweep_modal_batched(c0.P, g.precision, launch, g.d_table, g.grid, g.smem, st));
     if (any_phi)
         IDC_TRY_CUDA(launch_batched_helpers(c0.P, false, g.d_table, (int)table.size(), false, true, st));
     return Status::ok();
@@ -262,7 +280,7 @@ Status Batch::sweep(const double *const *srcs, double *const *outs, const double
                 g.seg = tuned[key].first;
                 g.wn = std::min(tuned[key].second, sweep_modal_max_wn(P));
             } else {
-                default_shape(P, qmax, &g.seg, &g.wn);
+                default_shape(P, precision, qmax, &g.seg, &g.wn);
             }
             g.precision = precision;
             groups.push_back(g);
@@ -536,8 +554,10 @@ Status Batch::set_shape(int P, int precision, int seg, int wn) {
     if (seg == 0 && wn == 0) {
         tuned.erase(key);
     } else {
-        if ((seg != 4 && seg != 8 && seg != 16 && seg != 32) || wn < 1 || wn > 7)
-            return bad(IDC_ERR_ARG, "batch tile shape: seg must be 4, 8, 16 or 32 and wn in 1..7");
+        const bool lane = wn == 0 && precision == IDC_PREC_FP64 && (seg == 4 || seg == 8 || seg == 16);
+        if (!lane && ((seg != 4 && seg != 8 && seg != 16 && seg != 32) || wn < 1 || wn > 7))
+            return bad(IDC_ERR_ARG, "batch tile shape: seg 4, 8, 16 or 32 with wn in 1..7 (the modal kernel), or "
+                                    "seg 4, 8 or 16 with wn 0 (the lane kernel, FP64)");
         tuned[key] = {seg, wn};
     }
     release();
@@ -558,7 +578,7 @@ void Batch::get_shape(int P, int precision, int *seg, int *wn) const {
         *seg = *wn = 0;
         return;
     }
-    default_shape(P, qmax, seg, wn);
+    default_shape(P, precision, qmax, seg, wn);
 }
 
 Status Batch::autotune(const double *const *srcs, double *const *outs, double dt, int precision) {
@@ -569,21 +589,27 @@ Status Batch::autotune(const double *const *srcs, double *const *outs, double dt
         if (!any) continue;
         float best = 1e30f;
         std::pair<int, int> bsh{0, 0};
+        // the modal kernel's shapes, and in FP64 the lane kernel's (wn 0)
+        std::vector<std::pair<int, int>> cands;
         for (int cs : {4, 8, 16, 32})
-            for (int cw = std::max(1, sweep_modal_max_wn(P) - 3); cw <= sweep_modal_max_wn(P); ++cw) {
-                tuned[std::make_pair(P, precision)] = {cs, cw};
-                release();
-                float ms = 1e30f;
-                for (int rep = 0; rep < 4; ++rep) {   // one warm-up, then the best of three
-                    IDC_TRY(sweep(srcs, outs, nullptr, 1.0, nullptr, dt, precision));
-                    if (rep > 0) ms = std::min(ms, last_ms);
-                }
-                // the timing covers every degree's launch; the other degrees' shapes stay fixed meanwhile
-                if (ms < best) {
-                    best = ms;
-                    bsh = {cs, cw};
-                }
+            for (int cw = std::max(1, sweep_modal_max_wn(P) - 3); cw <= sweep_modal_max_wn(P); ++cw)
+                cands.push_back({cs, cw});
+        if (precision == IDC_PREC_FP64)
+            for (int cs : {4, 8, 16}) cands.push_back({cs, 0});
+        for (const auto &cand : cands) {
+            tuned[std::make_pair(P, precision)] = cand;
+            release();
+            float ms = 1e30f;
+            for (int rep = 0; rep < 4; ++rep) {   // one warm-up, then the best of three
+                IDC_TRY(sweep(srcs, outs, nullptr, 1.0, nullptr, dt, precision));
+                if (rep > 0) ms = std::min(ms, last_ms);
             }
+            // the timing covers every degree's launch; the other degrees' shapes stay fixed meanwhile
+            if (ms < best) {
+                best = ms;
+                bsh = cand;
+            }
+        }
         tuned[std::make_pair(P, precision)] = bsh;
         release();
     }

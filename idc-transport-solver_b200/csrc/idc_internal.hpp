@@ -106,6 +106,11 @@ constexpr int kModalSolutionSlots = 4;   // modal kernel: step results in flight
 // sweep_lane_warps() warps.  Same arguments and trace protocol as the modal kernel.
 bool sweep_lane_supports(int P, int precision, int seg);
 int sweep_lane_warps();
+// A batch's FP64 forward sweep on the lane kernel: the items of several problems of one DG degree (`table`:
+// one SweepArgs per problem on the device; items name their problem and carry problem-local indices)
+cudaError_t launch_sweep_lane_batched(int P, const SweepArgs &args, const SweepArgs *table, int grid,
+                                      cudaStream_t stream);
+cudaError_t sweep_lane_batched_occupancy(int P, int seg, int *blocks_per_sm);
 cudaError_t launch_sweep_lane(int P, int precision, const SweepArgs &args, int grid, cudaStream_t stream);
 cudaError_t sweep_lane_occupancy(int P, int seg, bool src2, int *blocks_per_sm);
 

@@ -159,6 +159,47 @@ cudaError_t launch_reduce_modal_partials(const GridDims &g, const double *part, 
     return cudaGetLastError();
 }
 
+namespace {
+template <int P>
+cudaError_t launch_batched_p(int seg, const SweepArgs &args, const SweepArgs *table, int grid, cudaStream_t stream) {
+    switch (seg) {
+        case 4: return lane::launch_batched<P, 4>(args, table, grid, stream);
+        case 8: return lane::launch_batched<P, 8>(args, table, grid, stream);
+        case 16: return lane::launch_batched<P, 16>(args, table, grid, stream);
+        default: return cudaErrorInvalidValue;
+    }
+}
+template <int P>
+cudaError_t occupancy_batched_p(int seg, int *n) {
+    switch (seg) {
+        case 4: return lane::occupancy_batched<P, 4>(n);
+        case 8: return lane::occupancy_batched<P, 8>(n);
+        case 16: return lane::occupancy_batched<P, 16>(n);
+        default: return cudaErrorInvalidValue;
+    }
+}
+}  // namespace
+
+cudaError_t launch_sweep_lane_batched(int P, const SweepArgs &args, const SweepArgs *table, int grid,
+                                      cudaStream_t stream) {
+    if (args.G > args.seg || args.R != 32 / args.seg || !table) return cudaErrorInvalidValue;
+    switch (P) {
+        case 1: return launch_batched_p<1>(args.seg, args, table, grid, stream);
+        case 2: return launch_batched_p<2>(args.seg, args, table, grid, stream);
+        case 3: return launch_batched_p<3>(args.seg, args, table, grid, stream);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t sweep_lane_batched_occupancy(int P, int seg, int *blocks_per_sm) {
+    switch (P) {
+        case 1: return occupancy_batched_p<1>(seg, blocks_per_sm);
+        case 2: return occupancy_batched_p<2>(seg, blocks_per_sm);
+        case 3: return occupancy_batched_p<3>(seg, blocks_per_sm);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 cudaError_t sweep_lane_occupancy(int P, int seg, bool src2, int *blocks_per_sm) {
     switch (P) {
         case 1: return occ_p<1>(seg, src2, blocks_per_sm);

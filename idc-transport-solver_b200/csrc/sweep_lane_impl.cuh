@@ -590,9 +590,16 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
     bulk_wait<0>();
 }
 
-template <int P, int SEG, bool ADJ, bool SRC2, bool PHI, typename TC>
-__global__ void __launch_bounds__(kWarps * 32, 1) sweep_lane_kernel(const SweepArgs a) {
+// BATCHED: the items of several problems in one launch (a batch's problems of one DG degree, FP64 forward
+// sweeps); each item names its problem in `table` and carries its index within that problem (`local`: its trace
+// row and moment slot, `dep` is local too).  A warp copies its item's entry into shared memory; a problem left
+// out of the launch (`skip`) has its items return at once.
+template <int P, int SEG, bool ADJ, bool SRC2, bool PHI, typename TC, bool BATCHED>
+__global__ void __launch_bounds__(kWarps * 32, 1) sweep_lane_kernel(const SweepArgs a,
+                                                                    const SweepArgs *__restrict__ table) {
+    static_assert(sizeof(SweepArgs) % 8 == 0, "SweepArgs is copied in 8-byte words");
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(16) SweepArgs s_args[BATCHED ? kWarps : 1];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double *wsm = reinterpret_cast<double *>(smem_raw) + warp_doubles(P, SEG, SRC2) * warp;
     for (;;) {
@@ -603,23 +610,53 @@ __global__ void __launch_bounds__(kWarps * 32, 1) sweep_lane_kernel(const SweepA
         }
         it = __shfl_sync(kFullMask, it, 0);
         if (it >= a.n_items) return;
-        run_item<P, SEG, ADJ, SRC2, PHI, TC>(a, a.items[it], it, wsm, lane);
+        const SweepItem item = a.items[it];
+        if constexpr (BATCHED) {
+            const unsigned long long *sw = reinterpret_cast<const unsigned long long *>(table + item.problem);
+            unsigned long long *dw = reinterpret_cast<unsigned long long *>(&s_args[warp]);
+            for (int k = lane; k < (int)(sizeof(SweepArgs) / 8); k += 32) dw[k] = sw[k];
+            __syncwarp();
+            if (!s_args[warp].skip) run_item<P, SEG, ADJ, SRC2, PHI, TC>(s_args[warp], item, item.local, wsm, lane);
+            __syncwarp();   // every lane is done with the entry before the next item's copy
+        } else {
+            run_item<P, SEG, ADJ, SRC2, PHI, TC>(a, item, it, wsm, lane);
+        }
     }
 }
 
 template <int P, int SEG, bool ADJ, bool SRC2, bool PHI = false, typename TC = double>
 cudaError_t launch(const SweepArgs &args, int grid, cudaStream_t stream) {
-    auto kern = sweep_lane_kernel<P, SEG, ADJ, SRC2, PHI, TC>;
+    auto kern = sweep_lane_kernel<P, SEG, ADJ, SRC2, PHI, TC, false>;
     const size_t smem = block_smem_bytes(P, SEG, SRC2);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    kern<<<grid, kWarps * 32, smem, stream>>>(args);
+    kern<<<grid, kWarps * 32, smem, stream>>>(args, nullptr);
     return cudaGetLastError();
+}
+
+// A batch's FP64 forward sweep (items of several problems; `table` on the device, one entry per problem)
+template <int P, int SEG>
+cudaError_t launch_batched(const SweepArgs &args, const SweepArgs *table, int grid, cudaStream_t stream) {
+    auto kern = sweep_lane_kernel<P, SEG, false, false, false, double, true>;
+    const size_t smem = block_smem_bytes(P, SEG, false);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    kern<<<grid, kWarps * 32, smem, stream>>>(args, table);
+    return cudaGetLastError();
+}
+
+template <int P, int SEG>
+cudaError_t occupancy_batched(int *blocks_per_sm) {
+    auto kern = sweep_lane_kernel<P, SEG, false, false, false, double, true>;
+    const size_t smem = block_smem_bytes(P, SEG, false);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kern, kWarps * 32, smem);
 }
 
 template <int P, int SEG, bool ADJ, bool SRC2>
 cudaError_t occupancy(int *blocks_per_sm) {
-    auto kern = sweep_lane_kernel<P, SEG, ADJ, SRC2, false, double>;
+    auto kern = sweep_lane_kernel<P, SEG, ADJ, SRC2, false, double, false>;
     const size_t smem = block_smem_bytes(P, SEG, SRC2);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;

@@ -256,7 +256,9 @@ int idc_batch_sweep(idc_batch *b, const double *const *sources, double *const *r
 int idc_batch_autotune(idc_batch *b, const double *const *sources, double *const *results, double dt, int precision);
 int idc_batch_last_timing(idc_batch *b, double *ms);
 /* The tile shape a batch uses for its problems of DG degree dg_degree at `precision` (what the autotuner
- * picked, the default, or what was set; set 0, 0 to return to the default). */
+ * picked, the default, or what was set; set 0, 0 to return to the default).  seg 4, 8, 16 or 32 with warps
+ * 1..7 is the modal kernel; in FP64, seg 4, 8 or 16 with warps = 0 is the lane kernel (one warp per row
+ * block).  The autotuner tries both. */
 int idc_batch_set_shape(idc_batch *b, int dg_degree, int precision, int32_t seg, int32_t warps);
 int idc_batch_get_shape(idc_batch *b, int dg_degree, int precision, int32_t *seg, int32_t *warps);
 /* GMRES(restart) to abs_tol on every member's Peierls system at once (each member's problem as

@@ -52,6 +52,68 @@ def test_batched_sweep_matches_individual_sweeps(prec):
             c.close()
 
 
+@pytest.mark.parametrize("seg", [4, 8, 16])
+def test_batched_lane_shapes_match_individual_sweeps(seg):
+    """The lane kernel run over a batch (tile shape (seg, 0), FP64): every member's psi bitwise its own sweep's,
+    phi to rounding, with a reused batch and members of both degrees."""
+    probs = [P for P in _problems() if P.dt == np.inf]
+    ctxs = [_ctx(P) for P in probs]
+    try:
+        srcs = [torch.from_numpy(P.source).cuda() for P in probs]
+        outs = [torch.zeros_like(s) for s in srcs]
+        phis = [torch.zeros(P.phi_shape(), dtype=torch.float64, device="cuda") for P in probs]
+        with abi.Batch() as b:
+            for c in ctxs:
+                b.add(c)
+            for p in (1, 2):
+                b.set_shape(p, abi.PREC_FP64, seg, 0)
+                assert b.get_shape(p, abi.PREC_FP64) == (seg, 0)
+            for _ in range(2):
+                b.sweep([s.data_ptr() for s in srcs], [o.data_ptr() for o in outs], [f.data_ptr() for f in phis],
+                        np.inf)
+            with pytest.raises(abi.IdcError) as e:   # the lane kernel has no FP32 form
+                b.set_shape(1, abi.PREC_FP32_REFINED, seg, 0)
+            assert e.value.code == abi.IDC_ERR_ARG
+        for j, c in enumerate(ctxs):
+            want = torch.zeros_like(srcs[j])
+            wphi = torch.zeros_like(phis[j])
+            c.sweep_out(srcs[j].data_ptr(), want.data_ptr(), np.inf, wphi.data_ptr(), loc=abi.LOC_DEVICE)
+            assert torch.equal(outs[j][1:-1, 1:-1], want[1:-1, 1:-1])
+            assert rel_err(phis[j].cpu().numpy(), wphi.cpu().numpy()) < 1e-14
+    finally:
+        for c in ctxs:
+            c.close()
+
+
+def test_batched_gmres_on_lane_shapes():
+    """Batched GMRES + DSA with the lane kernel's shapes (converged members skipped inside its launches): the
+    members' own solutions."""
+    probs = [random_problem(12, 9, 1, 4, seed=31), lognormal(40, 2, 8, seed=32, c_range=(0.3, 0.99)),
+             lognormal(24, 1, 12, seed=33, c_range=(0.5, 0.95))]
+    tol = 1e-10
+    ctxs = [_ctx(P) for P in probs]
+    try:
+        want = []
+        for P, c in zip(probs, ctxs):
+            c.set_preconditioner(abi.PRECOND_DSA, 20)
+            psi = P.source.copy()
+            c.gmres_solve(psi, P.dt, abs_tol=tol, restart=10, max_its=2000)
+            want.append(psi)
+        psis = [torch.from_numpy(P.source).cuda() for P in probs]
+        with abi.Batch() as b:
+            for c in ctxs:
+                b.add(c)
+            b.set_shape(1, abi.PREC_FP64, 16, 0)
+            b.set_shape(2, abi.PREC_FP64, 8, 0)
+            its, res = b.gmres_solve([x.data_ptr() for x in psis], np.inf, abs_tol=tol, restart=10, max_its=2000)
+        for k in range(len(probs)):
+            assert res[k] <= tol
+            assert rel_err(psis[k].cpu().numpy(), want[k]) < 1e-8
+    finally:
+        for c in ctxs:
+            c.close()
+
+
 def test_autotuners_keep_results():
     probs = _problems()[:3]
     ctxs = [_ctx(P) for P in probs]
