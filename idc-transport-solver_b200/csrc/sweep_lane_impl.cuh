@@ -545,22 +545,25 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
             }
             // the moments of row rr: sums of the SEG weighted values in fixed trees, one partial per ordinate
             // chunk (added in a fixed order by the reduction kernel: bitwise reproducible).  16-wide segments
-            // sum moment k = o in ordinate order from the shared buffer; narrower ones by a shuffle butterfly
-            // (measured on B200: each is the faster one at its width).
+            // sum moment k = o from the shared buffer in a pairwise tree over ordinate order (the sequential
+            // sum's 15 dependent adds cost 4% of the 256x256 Q2 S16 sweep on B200); narrower ones by a shuffle
+            // butterfly (measured on B200: each is the faster one at its width).
             const bool pp = inrow && phi_base != nullptr;
             double *pt = pp ? phi_base + cidx * N : out_trace;
             if constexpr (SEG >= 16) {
                 const int k = o < N ? o : N - 1;
                 const double2 *mv = reinterpret_cast<const double2 *>(mbuf + k * kMomStride + rr * SEG);
-                double2 v = mv[0];
-                double sum = v.x + v.y;
+                double part[SEG / 2];   // a pairwise tree in ordinate order: 4 dependent adds, not 15
 #pragma unroll
-                for (int h = 1; h < SEG / 2; ++h) {
-                    v = mv[h];
-                    sum += v.x;
-                    sum += v.y;
+                for (int h = 0; h < SEG / 2; ++h) {
+                    const double2 v = mv[h];
+                    part[h] = v.x + v.y;
                 }
-                st_f64_if(pt + k, sum, pp && o < N);
+#pragma unroll
+                for (int w = SEG / 4; w >= 1; w /= 2)
+#pragma unroll
+                    for (int h = 0; h < w; ++h) part[h] = part[2 * h] + part[2 * h + 1];
+                st_f64_if(pt + k, part[0], pp && o < N);
             } else {
 #pragma unroll
                 for (int k = 0; k < N; ++k) x[k] = wv * x[k];
