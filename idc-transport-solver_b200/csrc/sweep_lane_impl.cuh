@@ -67,6 +67,11 @@ constexpr int kWarps = 4;    // warps per thread block: one per SM sub-partition
 constexpr int kStages = 6;   // stages in shared memory: a step's inputs are copied this many steps minus one ahead
 constexpr int kOutBufs = 2;  // psi leaves through a ring of this many per-warp buffers
 constexpr int kMomStride = 34;   // doubles per moment index k in the moment buffer (32 lanes + 2: conflict-free sums)
+// Polls of a producer's trace column in flight at once, by DG degree + 1.  Measured on B200 (interleaved A/B):
+// three at DG degree 1 (512x512 Q1 S12 1.039 -> 0.952 ms; two gained nothing), one at DG degree 2 (three
+// cost 2-3% there: 256x256 Q2 S16 0.695 -> 0.714 ms).
+template <int P>
+constexpr int kPollDepth = P >= 3 ? 1 : 3;
 
 // Doubles per (column, ordinate) slot of the trace buffer.
 __host__ __device__ constexpr int trace_slot(int P) { return P; }
@@ -184,26 +189,38 @@ __device__ __noinline__ ProducerWait<P> wait_for_producer(const double *dep_trac
                                                           int lane) {
     const double *col = dep_trace + (size_t)s * G * P;
     ProducerWait<P> r;
-    for (;;) {
-        bool still = false;
+    // kPollDepth<P> polls in flight: each check waits for the oldest while the others travel, and a checked
+    // poll is reissued at once, so the polls reach L2 about a round trip / kPollDepth<P> apart
+    double v[kPollDepth<P>][P];
 #pragma unroll
-        for (int m = 0; m < P; ++m) {
-            r.v[m] = ld_relaxed_f64_if(col + m, reader);
-            still |= reader && is_sentinel(r.v[m]);
+    for (int d = 0; d < kPollDepth<P>; ++d)
+#pragma unroll
+        for (int m = 0; m < P; ++m) v[d][m] = ld_relaxed_f64_if(col + m, reader);
+    for (;;) {
+#pragma unroll
+        for (int d = 0; d < kPollDepth<P>; ++d) {
+            bool still = false;
+#pragma unroll
+            for (int m = 0; m < P; ++m) still |= reader && is_sentinel(v[d][m]);
+            r.polls = polls;
+            if (!__any_sync(kFullMask, still)) {
+#pragma unroll
+                for (int m = 0; m < P; ++m) r.v[m] = v[d][m];
+                return r;
+            }
+            ++polls;
+            if ((polls & 63) == 63 && ld_relaxed(error) != kDevOk) {
+                r.polls = -1;
+                return r;
+            }
+            if (polls > spin_limit) {
+                if (lane == 0) atomicCAS(error, kDevOk, kDevTimeout);
+                r.polls = -1;
+                return r;
+            }
+#pragma unroll
+            for (int m = 0; m < P; ++m) v[d][m] = ld_relaxed_f64_if(col + m, reader);
         }
-        r.polls = polls;
-        if (!__any_sync(kFullMask, still)) return r;
-        ++polls;
-        if ((polls & 63) == 63 && ld_relaxed(error) != kDevOk) {
-            r.polls = -1;
-            return r;
-        }
-        if (polls > spin_limit) {
-            if (lane == 0) atomicCAS(error, kDevOk, kDevTimeout);
-            r.polls = -1;
-            return r;
-        }
-        __nanosleep(64);
     }
 }
 
