@@ -67,9 +67,12 @@ constexpr int kWarps = 4;    // warps per thread block: one per SM sub-partition
 constexpr int kStages = 6;   // stages in shared memory: a step's inputs are copied this many steps minus one ahead
 constexpr int kOutBufs = 2;  // psi leaves through a ring of this many per-warp buffers
 constexpr int kMomStride = 34;   // doubles per moment index k in the moment buffer (32 lanes + 2: conflict-free sums)
-// Polls of a producer's trace column in flight at once, by DG degree + 1.  Measured on B200 (interleaved A/B):
-// three at DG degree 1 (512x512 Q1 S12 1.039 -> 0.952 ms; two gained nothing), one at DG degree 2 (three
-// cost 2-3% there: 256x256 Q2 S16 0.695 -> 0.714 ms).
+// Polls per round of the producer wait below, by DG degree + 1, chosen by measurement on B200 (interleaved
+// A/B).  At DG degree 1 the three-poll form is 6-8% faster (512x512 Q1 S12 1.015-1.039 -> 0.950 ms; two: no
+// gain).  ptxas places its poll array in local memory (a 48-byte stack frame), so its loads do not stay in
+// flight together as the loop is written; variants with the polls in registers (overlapping), with one poll
+// and a 256 ns sleep, or waiting for 2 or 4 columns of slack all lose the gain (1.02-1.18 ms), so where the
+// gain comes from is not established.  At DG degree 2 three polls cost 2-3% (0.695 -> 0.714 ms): one.
 template <int P>
 constexpr int kPollDepth = P >= 3 ? 1 : 3;
 
@@ -189,8 +192,7 @@ __device__ __noinline__ ProducerWait<P> wait_for_producer(const double *dep_trac
                                                           int lane) {
     const double *col = dep_trace + (size_t)s * G * P;
     ProducerWait<P> r;
-    // kPollDepth<P> polls in flight: each check waits for the oldest while the others travel, and a checked
-    // poll is reissued at once, so the polls reach L2 about a round trip / kPollDepth<P> apart
+    // kPollDepth<P> polls per round: each checked poll is reissued at once
     double v[kPollDepth<P>][P];
 #pragma unroll
     for (int d = 0; d < kPollDepth<P>; ++d)
