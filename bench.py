@@ -300,11 +300,11 @@ def extra_idc(abi, torch, dev, steps=10):
         psi = torch.zeros(P.psi_shape(), dtype=torch.float64, device=f"cuda:{dev}")
         src = torch.from_numpy(P.source).to(f"cuda:{dev}")
         for name, prec in (("fp64", abi.PREC_FP64), ("fp32_refined", abi.PREC_FP32_REFINED)):
-            # the autotuner times plain sweeps; the IMEX sweeps (a second source and the scattering term) at Q1
-            # run faster on the modal kernel, which the library's default takes for them, so FP64 keeps it
+            # the autotuner times plain sweeps; the library's default picks the IMEX sweeps' kernel by grid size
+            # (512^2 at Q1: the lane kernel, 8-wide segments), so FP64 keeps it
             if prec == abi.PREC_FP64:
                 c.set_tile_shape(0, 0)
-                out.setdefault("tile_shape", {})[name] = "default (IMEX at Q1: modal, seg 8, 5 warps)"
+                out.setdefault("tile_shape", {})[name] = "default (IMEX at Q1 512^2: lane, seg 8)"
             else:
                 out.setdefault("tile_shape", {})[name] = c.autotune(src.data_ptr(), P.dt, prec)
             c.idc_integrate(psi.data_ptr(), src.data_ptr(), P.dt, 2, 4, 3, abi.SCATTER_EXPLICIT, prec, use_graph=True,

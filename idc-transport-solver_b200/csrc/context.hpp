@@ -126,6 +126,8 @@ public:
     double dx = 0, dy = 0;
     int device = 0;
     int num_sms = 0;
+    int lane_src2_blocks_[2] = {-1, -1};   // resident blocks per SM of the lane kernel's second-source
+                                           // instance at DG degree 1, segments 8 and 4 (-1: not queried yet)
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 

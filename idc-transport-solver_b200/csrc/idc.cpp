@@ -17,6 +17,7 @@
 // The quadrature sums, residuals and sources are FP64; `precision` selects the sweep arithmetic.
 #include "context.hpp"
 
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -149,20 +150,30 @@ Status Context::idc_integrate(double *psi, const double *Q, double dt, int64_t s
                                         "piecewise-constant cross sections); implicit scattering takes these inputs");
     std::vector<double> t, W;
     idc_nodes_and_weights(M, t, W);
-    // The IMEX sweeps (a second source and the scattering term) at DG degree 1 are faster on the modal kernel
-    // than on the lane kernel's second-source instance (measured per step: 512^2 Q1 S12 23.3-23.7 ms against
-    // 28-34 ms; 256^2 Q1 S12 7.8-8.6 against 10.5-11.8 ms; at degree 2 the lane kernel's default is the
-    // fastest).  Without a tile shape of the caller's the integration runs on the modal (8, 5) shape and the
-    // default comes back when it returns, on every path.
+    // The IMEX sweeps (a second source and the scattering term) at DG degree 1 run on the lane kernel's default
+    // shape when its work queue has an item for every resident warp, else on the modal (8, 5) shape.  Measured
+    // per step (lattice, Q1 S12): 512^2 (1536 lane items for 1184 resident warps) lane 22.2 ms, modal 23.7 ms;
+    // 256^2 (768 items) lane 8.9 ms, modal 7.7 ms.  Without a tile shape of the caller's, the modal shape is
+    // set for the call and the default comes back when it returns, on every path (the schedules are rebuilt:
+    // ~0.8 ms per call at these sizes).
     struct TileRestore {
         Context *c = nullptr;
         ~TileRestore() {
             if (c) c->set_tile_shape(0, 0);
         }
     } tile_restore;
-    if (scattering == 0 && P == 2 && tune_seg == 0 && tune_wn == 0) {
-        IDC_TRY(set_tile_shape(8, 5));
-        tile_restore.c = this;
+    if (scattering == 0 && P == 2 && tune_seg == 0 && tune_wn == 0 && kernel_for(precision) == kLane) {
+        int counts[4], qmax = 0;
+        for (int k = 0; k < 4; ++k) qmax = std::max(qmax, counts[k] = (int)(quad[k + 1] - quad[k]));
+        const int seg = qmax <= 24 ? 8 : 4, rows = 32 / seg;
+        int64_t items = 0;
+        for (int k = 0; k < 4; ++k) items += (int64_t)((counts[k] + seg - 1) / seg) * ((ny + rows - 1) / rows);
+        int &per_sm = lane_src2_blocks_[seg == 8 ? 0 : 1];   // queried once per context
+        if (per_sm < 0) IDC_TRY_CUDA(sweep_lane_occupancy(P, seg, true, &per_sm));
+        if (items < (int64_t)per_sm * sweep_lane_warps() * num_sms) {
+            IDC_TRY(set_tile_shape(8, 5));
+            tile_restore.c = this;
+        }
     }
 
     // buffers: M stages, M residuals, one source (psi-sized); M moments, M previous-level moments, one

@@ -211,8 +211,10 @@ enum { IDC_SCATTER_EXPLICIT = 0, IDC_SCATTER_IMPLICIT = 1 };
  * scattering = IDC_SCATTER_EXPLICIT (IMEX): every substep is one sweep with the scattering lagged to the
  * previous node and corrected by the deferred-correction iterations; with use_graph a step is captured
  * once as a CUDA graph and replayed (lane or modal kernel: DG degree <= 2, piecewise-constant cross
- * sections; at DG degree 1, unless idc_set_tile_shape fixed a shape, the step runs on the modal kernel's
- * (8, 5) shape, the faster one for these sweeps, and the context's default shape returns afterwards).  Reflecting edges and periodic grids return IDC_ERR_UNSUPPORTED.  Quadrature sums and residuals are FP64; `precision` selects the
+ * sections; at DG degree 1, unless idc_set_tile_shape fixed a shape, a grid too small to give the lane
+ * kernel an item for every resident warp runs the step on the modal kernel's (8, 5) shape, the faster one
+ * there, and the context's default shape returns afterwards).  Reflecting edges and periodic grids return
+ * IDC_ERR_UNSUPPORTED.  Quadrature sums and residuals are FP64; `precision` selects the
  * sweep arithmetic.  *sweeps receives the number of sweeps performed. */
 int idc_idc_integrate(idc_ctx *ctx, double *psi_inout, const double *source, double dt, int64_t steps,
                       int32_t num_nodes, int32_t num_corrections, int scattering, int precision, double abs_tol,
