@@ -63,6 +63,38 @@ __global__ void smv_kernel(GridDims g, double alpha, double beta, const double *
 // sigma).  One thread per (interior cell, ordinate).  With phi_sc, the scattering term of Smv is added in
 // the same pass, y += (sigma_s phi_sc / (4 pi)) gamma, rounded as Lmv followed by Smv(gamma, 1) would
 // round it (the IDC residual (L - S P) psi in one pass over psi).
+// v = p[0 .. n): 16-byte loads when n is even and `wide` (p 16-byte aligned), else 8-byte loads.  A cell's
+// dofs of one ordinate start on a 16-byte boundary of an aligned array when n is even (DG degree 1).
+template <int n>
+__device__ __forceinline__ void load_dofs(const double *__restrict__ p, double (&v)[n], bool wide) {
+    if constexpr (n % 2 == 0) {
+        if (wide) {
+#pragma unroll
+            for (int h = 0; h < n / 2; ++h) {
+                const double2 t = reinterpret_cast<const double2 *>(p)[h];
+                v[2 * h] = t.x;
+                v[2 * h + 1] = t.y;
+            }
+            return;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < n; ++k) v[k] = p[k];
+}
+template <int n>
+__device__ __forceinline__ void store_dofs(double *__restrict__ p, const double (&v)[n], bool wide) {
+    if constexpr (n % 2 == 0) {
+        if (wide) {
+#pragma unroll
+            for (int h = 0; h < n / 2; ++h) reinterpret_cast<double2 *>(p)[h] = make_double2(v[2 * h], v[2 * h + 1]);
+            return;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < n; ++k) p[k] = v[k];
+}
+__device__ __forceinline__ bool aligned16(const void *p) { return ((size_t)p & 15) == 0; }
+
 // (Omega.grad + sigma_t) x at one interior (cell, ordinate): TransportOperator::Lmv, :1215-1480 (piecewise
 // constant sigma), with x's dofs of the cell at x + base and its upwind neighbours' at +-istride, +-plane.
 // With tens (high-order cross sections) the absorption term is 1/4 (2d+1)(2e+1) sum_{u,v} T(d,e; u,v) x(u,v)
@@ -77,12 +109,10 @@ __device__ __forceinline__ void lmv_point(const GridDims &g, const double *__res
     const double *X1 = x + base + (xneg ? (ptrdiff_t)istride : -(ptrdiff_t)istride);
     const double *X2 = x + base + (yneg ? (ptrdiff_t)plane : -(ptrdiff_t)plane);
     double x0[N], x1[N], x2[N];
-#pragma unroll
-    for (int k = 0; k < N; ++k) {
-        x0[k] = X0[k];
-        x1[k] = X1[k];
-        x2[k] = X2[k];
-    }
+    const bool wide = aligned16(x);
+    load_dofs<N>(X0, x0, wide);
+    load_dofs<N>(X1, x1, wide);
+    load_dofs<N>(X2, x2, wide);
     if (tens) {
 #pragma unroll
         for (int d = 0; d < P; ++d)
@@ -484,8 +514,7 @@ __global__ void __launch_bounds__(kThreads, P <= 2 ? 2 : 1)
     const double st = sigma_t[cidx];
     double acc[M - 1][N];
     double q0[N];
-#pragma unroll
-    for (int k = 0; k < N; ++k) q0[k] = t.Q[base + k];
+    load_dofs<N>(t.Q + base, q0, aligned16(t.Q));
 #pragma unroll
     for (int n = 0; n < M - 1; ++n)
 #pragma unroll
@@ -494,7 +523,8 @@ __global__ void __launch_bounds__(kThreads, P <= 2 ? 2 : 1)
     for (int l = 0; l < M; ++l) {
         double x3[N];
         lmv_point<P>(g, t.stage[l], base, istride, plane, xi, eta, st, x3);
-        const double *sm = t.scat[l] + cidx * N;
+        double sm[N];
+        load_dofs<N>(t.scat[l] + cidx * N, sm, aligned16(t.scat[l]));
 #pragma unroll
         for (int k = 0; k < N; ++k) {
             const double r = __dadd_rn(__dmul_rn(1.0, x3[k]), sm[k] * -1.0);
@@ -503,9 +533,7 @@ __global__ void __launch_bounds__(kThreads, P <= 2 ? 2 : 1)
         }
     }
 #pragma unroll
-    for (int n = 0; n < M - 1; ++n)
-#pragma unroll
-        for (int k = 0; k < N; ++k) t.out[n + 1][base + k] = acc[n][k];
+    for (int n = 0; n < M - 1; ++n) store_dofs<N>(t.out[n + 1] + base, acc[n], aligned16(t.out[n + 1]));
 }
 
 // out = sigma_s phi / (4 pi) on interior cells, rounded as TransportOperator::Smv rounds its scattering term

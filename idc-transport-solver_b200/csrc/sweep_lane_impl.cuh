@@ -150,6 +150,23 @@ __device__ __forceinline__ double ld_relaxed_f64_if(const double *p, bool pred) 
 __device__ __forceinline__ void cp_async8_zfill(void *dst, const void *src, bool pred) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(saddr(dst)), "l"(src), "r"(pred ? 8 : 0));
 }
+// 16-byte cp.async (through L2) with the same zero fill; dst and src 16-byte aligned
+__device__ __forceinline__ void cp_async16_zfill(void *dst, const void *src, bool pred) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(saddr(dst)), "l"(src), "r"(pred ? 16 : 0));
+}
+// n doubles (n even: 16-byte copies when `wide`, both addresses then 16-byte aligned; else 8-byte copies)
+template <int n>
+__device__ __forceinline__ void cp_async_doubles(double *dst, const double *src, bool pred, bool wide) {
+    if constexpr (n % 2 == 0) {
+        if (wide) {
+#pragma unroll
+            for (int h = 0; h < n / 2; ++h) cp_async16_zfill(dst + 2 * h, src + 2 * h, pred);
+            return;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < n; ++k) cp_async8_zfill(dst + k, src + k, pred);
+}
 __device__ __forceinline__ void cp_async8_if(void *dst, const void *src, bool pred) {
     asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %2, 0;\n\t@q cp.async.ca.shared.global [%0], [%1], 8;\n\t}" ::"r"(
                      saddr(dst)),
@@ -350,7 +367,14 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
     long long pf_cidx = ((long long)xi0 - (long long)xis * rr) * (long long)cstride + j;   // step 0's column
     long long pf_soff = pf_cidx * (long long)plane + (long long)q * N;
 
-    // step t's inputs into stage slot = t % D, one cp.async group per step; a cell outside the row gets zeros
+    // step t's inputs into stage slot = t % D, one cp.async group per step; a cell outside the row gets zeros.
+    // With an even number of dofs per cell (DG degree 1) every (cell, ordinate) block starts on a 16-byte
+    // boundary of an aligned array, and the copies are 16 bytes wide (half the copy instructions; measured on
+    // B200 at DG degree 1: see the lane kernel's notes); the stage slots are 16-byte aligned by layout.
+    const bool wide_ok = N % 2 == 0 && ((size_t)valid_addr & 15) == 0;
+    const bool src16 = wide_ok && ((size_t)a.src & 15) == 0;
+    const bool src2_16 = wide_ok && (!SRC2 || ((size_t)a.src2 & 15) == 0);
+    const bool modal16 = wide_ok && (!PHI || ((size_t)a.modal_src & 15) == 0);
     auto prefetch = [&](int t, int slot) {
         const int c = t - rr;
         const bool in = row_valid && c >= 0 && c < nx;
@@ -358,19 +382,16 @@ __device__ __forceinline__ void run_item(const SweepArgs &a, const SweepItem &it
         double *d = stage + (size_t)slot * 32 * N;
         if constexpr (PHI) {   // the cell's packed modal source of this quadrant (the same for the row segment)
             const double *g = a.modal_src + (cidx * 4 + quadrant) * N;
-#pragma unroll
-            for (int k = 0; k < N; ++k) cp_async8_zfill(d + k, g + k, in && act);
+            cp_async_doubles<N>(d, g, in && act, modal16);
         } else {
             const bool ps = in && act && a.src != nullptr;
             const double *g = ps ? a.src + pf_soff : valid_addr;
-#pragma unroll
-            for (int k = 0; k < N; ++k) cp_async8_zfill(d + k, g + k, ps);
+            cp_async_doubles<N>(d, g, ps, src16);
         }
         if constexpr (SRC2) {
             double *d2 = stage2 + (size_t)slot * 32 * N;
             const double *g2 = (in && act) ? a.src2 + pf_soff : valid_addr;
-#pragma unroll
-            for (int k = 0; k < N; ++k) cp_async8_zfill(d2 + k, g2 + k, in && act);
+            cp_async_doubles<N>(d2, g2, in && act, src2_16);
         }
         cp_async8_zfill(sig + (size_t)slot * 32, a.sigma_t + cidx, in);
         if (has_scatter) {   // lane o == 0 of a row copies the cell's fused scattering moments (one copy per row)
