@@ -638,6 +638,13 @@ void Context::use_schedule(int variant) {
 
 Status Context::build_schedule(int precision) {
     if (n_items > 0 && occupancy_precision == precision) return Status::ok();
+    // the lane kernel's schedule does not depend on the precision (the same tiling rules, traces and grid for
+    // its FP64 and FP32 instances): a switch between them, as FP32 Krylov sweeps inside FP64 refinement make
+    // on every refinement pass, keeps it instead of reallocating and re-arming the traces
+    if (n_items > 0 && active == kLane && kernel_for(precision) == kLane) {
+        occupancy_precision = precision;
+        return Status::ok();
+    }
     int qmax = 0;
     for (int k = 0; k < 4; ++k) qmax = std::max<int>(qmax, (int)(quad[k + 1] - quad[k]));
     if (qmax == 0) return bad(IDC_ERR_ARG, "no ordinates");
