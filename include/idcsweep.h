@@ -165,9 +165,9 @@ int idc_source_iteration(idc_ctx *ctx, double *source_inout, double dt, double a
  * one fixed file-scope device array of about 96 KiB that every GPU loading the library keeps until the
  * process exits; problems needing more than IDC_NOALLOC_MAX_ITEMS work items, or more than
  * IDC_NOALLOC_MAX_ORDINATES ordinates, are rejected with IDC_ERR_ARG (use idc_sweep_out for those).
- * The first call on a device looks up that array's device address (cudaGetSymbolAddress); make that
- * first call before any stream capture.  All calls share the array and it keeps the last call's
- * contents; each call clears the parts that must start at zero.  Calls whose kernels overlap on the GPU
+ * The first call on a device looks up that array's device address (cudaGetSymbolAddress).  All calls
+ * share the array and it keeps the last call's contents; each call clears the parts that must start at
+ * zero.  Calls whose kernels overlap on the GPU
  * would race on it: calls from one process are serialised by a lock, and the call returns only after its
  * work on `stream` (a cudaStream_t, NULL for the default stream) has finished.  The caller's current
  * device is restored on return. */
