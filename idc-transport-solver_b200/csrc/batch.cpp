@@ -82,7 +82,9 @@ void Batch::release() {
 Status Batch::add(Context *c) {
     if (!c) return bad(IDC_ERR_ARG, "null context");
     if (!c->have_ordinates || !c->have_sigma) return bad(IDC_ERR_STATE, "batch member without ordinates or sigma");
-    if (!c->modal_family()) return bad(IDC_ERR_UNSUPPORTED, "batched sweeps need the modal kernel");
+    if (!c->modal_family())
+        return bad(IDC_ERR_UNSUPPORTED, "batched sweeps need the lane or modal kernel (DG degree <= 2, piecewise-"
+                                        "constant cross sections)");
     if (c->reflect_mask) return bad(IDC_ERR_UNSUPPORTED, "batched sweeps with reflecting boundaries");
     if (c->high_order_sigma()) return bad(IDC_ERR_UNSUPPORTED, "batched sweeps with high-order cross sections");
     if (c->periodic_) return bad(IDC_ERR_UNSUPPORTED, "batched solves on a periodic grid");

@@ -73,3 +73,22 @@ def test_solver_entry_points_reject_null_arguments():
     assert lib.idc_adjoint_transient(None, None, None, 0.1, 3, None, 0, 1e-8, 30, 10, 0, None, None, None, None,
                                      C.byref(jv), 0, C.byref(ns)) == abi.IDC_ERR_ARG
     assert b"null" in lib.idc_last_error_message()
+
+
+def test_batch_tile_shapes_validated_without_a_device():
+    """idc_batch_set_shape: the modal kernel's shapes (seg 4..32, warps 1..7) at any precision, the lane
+    kernel's (seg 4, 8 or 16, warps 0) in FP64 only; anything else is IDC_ERR_ARG; 0, 0 restores the default
+    (none for a degree without members)."""
+    with abi.Batch() as b:
+        b.set_shape(1, abi.PREC_FP64, 8, 0)
+        assert b.get_shape(1, abi.PREC_FP64) == (8, 0)
+        b.set_shape(2, abi.PREC_FP32_REFINED, 32, 5)
+        assert b.get_shape(2, abi.PREC_FP32_REFINED) == (32, 5)
+        for args in ((1, abi.PREC_FP32_REFINED, 8, 0), (1, abi.PREC_FP64, 32, 0), (1, abi.PREC_FP64, 12, 3),
+                     (1, abi.PREC_FP64, 8, 8), (2, abi.PREC_FP64, 16, -1)):
+            with pytest.raises(abi.IdcError) as e:
+                b.set_shape(*args)
+            assert e.value.code == abi.IDC_ERR_ARG
+        assert b.get_shape(1, abi.PREC_FP64) == (8, 0)   # a rejected shape leaves the set one
+        b.set_shape(1, abi.PREC_FP64, 0, 0)
+        assert b.get_shape(1, abi.PREC_FP64) == (0, 0)
