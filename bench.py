@@ -213,6 +213,10 @@ def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        # torchrun sets OMP_NUM_THREADS=1 for every rank; the other ranks exit without work, so rank 0 takes
+        # every core this process may run on (set before the reference library, and its OpenMP, is loaded)
+        os.environ["OMP_NUM_THREADS"] = str(len(os.sched_getaffinity(0)))
     P = problem(0, args.nx)
     steps = max(1, args.steps)
     warm = max(1, args.warmup)
