@@ -223,11 +223,17 @@ def run_reference_arm(args):
     t0 = time.time()
     sec, threads, _ = time_reference_cpu(P, steps, warm)
     value = P.unknowns_per_sweep / sec
+    # the same config as the GPU arm at this N: one problem split by ordinates (strong) or one per GPU (weak)
+    cfg = bench_config(P, args.gpus)
+    scaling = "weak"
+    if args.gpus > 1 and args.mode == "partitioned":
+        cfg["parallelism"] = f"ordinates{args.gpus}"
+        scaling = "strong"
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
-        "steps": steps, "warmup": warm, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+        "steps": steps, "warmup": warm, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": scaling,
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": bench_config(P, args.gpus),
+        "config": cfg,
         "reference_path": "SweepOperator::Apply (wavefront pattern, Gaussian-elimination cell solves), FP64, "
                           "OpenMP on all host cores",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
